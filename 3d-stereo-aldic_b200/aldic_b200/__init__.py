@@ -1,0 +1,10 @@
+"""B200 (sm_100a) implementation of the 3D-Stereo-ALDIC per-subset hot path.
+
+The compute runs in the in-tree CUDA library libaldic_b200.so (C ABI:
+include/aldic_b200.h); this package is its host-side mirror of the reference's MATLAB
+interface (funIntegerSearch, LocalICGN, LocalICGNQuadtree, Subpb1, Subpb1Quadtree,
+epipolar_ICGN1, stereoReconstruction_quadtree, ...).
+"""
+from ._lib import AldicError, load as load_library  # noqa: F401
+from .api import *  # noqa: F401,F403
+from . import api, synth  # noqa: F401

@@ -1,0 +1,71 @@
+"""ctypes binding of the in-tree CUDA library ``libaldic_b200.so`` (C ABI in
+include/aldic_b200.h).  There is no CPU fallback: if the library is missing or cannot be
+loaded, every entry point raises."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libaldic_b200.so")
+
+ALDIC_OK = 0
+ALDIC_ERR_ARG = 1
+ALDIC_ERR_CUDA = 2
+ALDIC_ERR_TIMEOUT = 3
+ALDIC_ERR_STATE = 4
+
+U8, U16, F32, F64 = 0, 1, 2, 3
+SLOT_REF, SLOT_DEF = 0, 1
+UNIFORM, QUADTREE = 0, 1
+
+# Every symbol the header declares, with (restype, argtypes).
+_vp = C.c_void_p
+_i = C.c_int
+_i64 = C.c_int64
+_d = C.c_double
+SIGNATURES = {
+    "aldic_create": (_i, [C.POINTER(_vp), _i]),
+    "aldic_destroy": (None, [_vp]),
+    "aldic_last_error": (C.c_char_p, [_vp]),
+    "aldic_set_stream": (_i, [_vp, _vp]),
+    "aldic_synchronize": (_i, [_vp]),
+    "aldic_launch_count": (_i64, [_vp]),
+    "aldic_abi_version": (_i, []),
+    "aldic_load_image_raw": (_i, [_vp, _i, _vp, _i, _i, _i, _vp, _vp, _vp, _vp]),
+    "aldic_load_image": (_i, [_vp, _i, _vp, _i, _i]),
+    "aldic_set_mask": (_i, [_vp, _vp, _i, _i]),
+    "aldic_compute_gradients": (_i, [_vp]),
+    "aldic_set_gradients": (_i, [_vp, _vp, _vp, _i, _i]),
+    "aldic_get_state": (_i, [_vp, _i, _vp]),
+    "aldic_interp2": (_i, [_vp, _i, _i64, _vp, _vp, _vp]),
+    "aldic_search_grid": (_i, [_vp, _vp, _i, _i, C.POINTER(_i), C.POINTER(_i)]),
+    "aldic_integer_search": (_i, [_vp, _vp, _vp, _vp, _i, _i, _vp, _vp, _vp, _vp, _vp]),
+    "aldic_local_icgn": (_i, [_vp, _i, _i64, _vp, _vp, _i, _d, _vp, _vp, _vp, _vp, _vp]),
+    "aldic_subpb1": (_i, [_vp, _i, _i64, _vp, _vp, _vp, _vp, _vp, _i, _vp, _d, _d, _vp, _vp]),
+    "aldic_epipolar_icgn": (_i, [_vp, _i64, _vp, _i, _d, _vp]),
+    "aldic_triangulate": (_i, [_vp, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+}
+
+_LIB = None
+
+
+class AldicError(RuntimeError):
+    pass
+
+
+def load(path: str | None = None):
+    """Load the library once; raise AldicError (never fall back) when it is absent."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise AldicError(f"CUDA library not built: {p} (run __graft_entry__.build() or make -C 3d-stereo-aldic_b200)")
+    lib = C.CDLL(p)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _LIB = lib
+    return lib

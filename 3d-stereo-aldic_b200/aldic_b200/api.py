@@ -1,0 +1,460 @@
+"""Host-side mirror of the reference's MATLAB interface for the per-subset hot path,
+running on the B200 through the C ABI of libaldic_b200.so.
+
+Function names, argument meaning, array layouts and per-subset status codes follow the
+reference (func/, func_quadtree/): images are column-major M x N (numpy order='F', dim 1
+= image x), coordinates 1-based, U interleaved [u1 v1 ...], F interleaved
+[F11 F21 F12 F22 ...], HtempPar n x 21, ConvItPerEle codes (iterations / 101 / 102 / 103
+/ -1).
+
+Arrays may be numpy (host) or CUDA torch tensors (device); device arrays keep the call
+asynchronous on the context's stream.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import time
+
+import numpy as np
+
+from . import _lib
+from ._lib import AldicError
+
+__all__ = [
+    "Context", "default_context", "funNormalizeImg", "funImgGradient", "ba_interp2_spline", "funIntegerSearch",
+    "LocalICGN", "LocalICGNQuadtree", "Subpb1", "Subpb1Quadtree", "epipolar_ICGN1",
+    "stereoReconstruction_quadtree", "bad_points_local", "bad_points_subpb1",
+]
+
+
+def _is_torch(x):
+    return hasattr(x, "data_ptr") and hasattr(x, "is_cuda")
+
+
+class _Keep:
+    """Holds converted numpy buffers alive for the duration of a call."""
+
+    def __init__(self):
+        self.items = []
+
+    def ptr(self, x, dtype, order="F"):
+        if x is None:
+            return None
+        if _is_torch(x):
+            if not x.is_contiguous():
+                raise AldicError("device tensors must be contiguous")
+            return C.c_void_p(x.data_ptr())
+        a = np.asarray(x, dtype=dtype)
+        a = np.ascontiguousarray(a.ravel(order=order)) if a.ndim > 1 else np.ascontiguousarray(a)
+        self.items.append(a)
+        return C.c_void_p(a.ctypes.data)
+
+    def out(self, n, dtype):
+        a = np.empty(n, dtype=dtype)
+        self.items.append(a)
+        return a, C.c_void_p(a.ctypes.data)
+
+
+def _np_dtype_code(a):
+    dt = a.dtype if hasattr(a, "dtype") else np.asarray(a).dtype
+    name = str(dt).replace("torch.", "")
+    return {"uint8": _lib.U8, "uint16": _lib.U16, "float32": _lib.F32, "float64": _lib.F64}[name]
+
+
+class Context:
+    """One device context: a CUDA stream, the resident frame (REF/DEF images, mask,
+    gradients) and the scratch buffers of the batched solvers."""
+
+    def __init__(self, device: int = 0):
+        self.lib = _lib.load()
+        h = C.c_void_p()
+        rc = self.lib.aldic_create(C.byref(h), int(device))
+        if rc != _lib.ALDIC_OK:
+            raise AldicError(f"aldic_create(device={device}) failed with code {rc} (no usable CUDA device?)")
+        self.h = h
+        self.device = device
+        self.M = self.N = None
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.aldic_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc, what):
+        if rc != _lib.ALDIC_OK:
+            msg = self.lib.aldic_last_error(self.h)
+            raise AldicError(f"{what}: code {rc}: {msg.decode() if msg else ''}")
+
+    # ------------------------------------------------------------------ frame
+    def set_stream(self, stream_handle):
+        self._check(self.lib.aldic_set_stream(self.h, C.c_void_p(stream_handle or 0)), "aldic_set_stream")
+
+    def synchronize(self):
+        self._check(self.lib.aldic_synchronize(self.h), "aldic_synchronize")
+
+    @property
+    def launches(self):
+        return int(self.lib.aldic_launch_count(self.h))
+
+    def load_image_raw(self, slot, img, gridx, gridy, mask=None, want_stats=True):
+        k = _Keep()
+        M, N = img.shape
+        gx = np.asarray(gridx, dtype=np.int32).ravel()
+        gy = np.asarray(gridy, dtype=np.int32).ravel()
+        ms = np.empty(2) if want_stats else None
+        dtype_code = _np_dtype_code(img)
+        npdt = {0: np.uint8, 1: np.uint16, 2: np.float32, 3: np.float64}[dtype_code]
+        rc = self.lib.aldic_load_image_raw(self.h, slot, k.ptr(img, npdt), dtype_code, M, N,
+                                           C.c_void_p(gx.ctypes.data), C.c_void_p(gy.ctypes.data),
+                                           k.ptr(mask, np.float64),
+                                           None if ms is None else C.c_void_p(ms.ctypes.data))
+        self._check(rc, "aldic_load_image_raw")
+        self.M, self.N = M, N
+        return ms
+
+    def load_image(self, slot, img):
+        k = _Keep()
+        M, N = img.shape
+        self._check(self.lib.aldic_load_image(self.h, slot, k.ptr(img, np.float64), M, N), "aldic_load_image")
+        self.M, self.N = M, N
+
+    def set_mask(self, mask):
+        k = _Keep()
+        self._check(self.lib.aldic_set_mask(self.h, k.ptr(mask, np.float64), self.M, self.N), "aldic_set_mask")
+
+    def compute_gradients(self):
+        self._check(self.lib.aldic_compute_gradients(self.h), "aldic_compute_gradients")
+
+    def set_gradients(self, dfdx, dfdy):
+        k = _Keep()
+        M6, N6 = dfdx.shape
+        self._check(self.lib.aldic_set_gradients(self.h, k.ptr(dfdx, np.float64), k.ptr(dfdy, np.float64), M6, N6),
+                    "aldic_set_gradients")
+
+    def get_state(self, what):
+        shape = (self.M, self.N) if what in (0, 1) else (self.M - 6, self.N - 6)
+        out = np.empty(shape[0] * shape[1])
+        self._check(self.lib.aldic_get_state(self.h, what, C.c_void_p(out.ctypes.data)), "aldic_get_state")
+        return out.reshape(shape, order="F")
+
+    # ------------------------------------------------------------ primitives
+    def interp2(self, slot, X, Y):
+        k = _Keep()
+        X = np.asarray(X, dtype=np.float64)
+        n = X.size
+        Z, zp = k.out(n, np.float64)
+        self._check(self.lib.aldic_interp2(self.h, slot, n, k.ptr(X, np.float64, "C"), k.ptr(Y, np.float64, "C"), zp),
+                    "aldic_interp2")
+        return Z.reshape(X.shape)
+
+    def search_grid(self, gridx, gridy, winsize, step):
+        gx = np.asarray(gridx, dtype=np.int32).ravel()
+        gy = np.asarray(gridy, dtype=np.int32).ravel()
+        nx, ny = C.c_int(), C.c_int()
+        self._check(self.lib.aldic_search_grid(C.c_void_p(gx.ctypes.data), C.c_void_p(gy.ctypes.data), int(winsize),
+                                               int(step), C.byref(nx), C.byref(ny)), "aldic_search_grid")
+        return nx.value, ny.value
+
+    def integer_search(self, search, gridx, gridy, winsize, step, out=None):
+        """Whole-field search on the resident REF/DEF images.  Returns dict of nY x nX
+        arrays (host), or fills `out` (dict of device tensors) asynchronously."""
+        s = np.asarray(search, dtype=np.int32).ravel()
+        if s.size == 1:
+            s = np.array([s[0], s[0]], dtype=np.int32)
+        gx = np.asarray(gridx, dtype=np.int32).ravel()
+        gy = np.asarray(gridy, dtype=np.int32).ravel()
+        nx, ny = self.search_grid(gx, gy, winsize, step)
+        k = _Keep()
+        if out is None:
+            bufs = {name: k.out(nx * ny, np.float64) for name in ("x", "y", "u", "v", "phi")}
+            ptrs = [bufs[nm][1] for nm in ("x", "y", "u", "v", "phi")]
+        else:
+            ptrs = [C.c_void_p(out[nm].data_ptr()) for nm in ("x", "y", "u", "v", "phi")]
+        rc = self.lib.aldic_integer_search(self.h, C.c_void_p(s.ctypes.data), C.c_void_p(gx.ctypes.data),
+                                           C.c_void_p(gy.ctypes.data), int(winsize), int(step), *ptrs)
+        self._check(rc, "aldic_integer_search")
+        if out is not None:
+            return out
+        return {nm: bufs[nm][0].reshape((ny, nx), order="F") for nm in ("x", "y", "u", "v", "phi")}
+
+    def local_icgn(self, variant, coords, U0, winsize, tol, want_H=True, want_mark=True, out=None):
+        k = _Keep()
+        n = int(coords.shape[0])
+        if out is None:
+            U, up = k.out(2 * n, np.float64)
+            F, fp = k.out(4 * n, np.float64)
+            H, hp = k.out(21 * n, np.float64) if want_H else (None, None)
+            conv, cp = k.out(n, np.int32)
+            mark, mp = k.out(n, np.uint8) if (want_mark and variant == _lib.QUADTREE) else (None, None)
+        else:
+            up, fp = C.c_void_p(out["U"].data_ptr()), C.c_void_p(out["F"].data_ptr())
+            hp = C.c_void_p(out["H"].data_ptr()) if out.get("H") is not None else None
+            cp = C.c_void_p(out["conv"].data_ptr())
+            mp = C.c_void_p(out["mark"].data_ptr()) if out.get("mark") is not None else None
+        rc = self.lib.aldic_local_icgn(self.h, int(variant), n, k.ptr(coords, np.float64), k.ptr(U0, np.float64, "C"),
+                                       int(winsize), float(tol), up, fp, hp, cp, mp)
+        self._check(rc, "aldic_local_icgn")
+        if out is not None:
+            return out
+        return dict(U=U, F=F, H=None if H is None else H.reshape((n, 21), order="F"), conv=conv, markHole=mark)
+
+    def subpb1(self, variant, coords, UOld, FOld, vdual, mu, tol, winsize=0, winsize_list=None, HPar=None):
+        k = _Keep()
+        n = int(coords.shape[0])
+        U, up = k.out(2 * n, np.float64)
+        conv, cp = k.out(n, np.int32)
+        wl = None if winsize_list is None else k.ptr(winsize_list, np.int32)
+        rc = self.lib.aldic_subpb1(self.h, int(variant), n, k.ptr(coords, np.float64), k.ptr(UOld, np.float64, "C"),
+                                   k.ptr(FOld, np.float64, "C"), k.ptr(vdual, np.float64, "C"), wl, int(winsize),
+                                   k.ptr(HPar, np.float64), float(mu), float(tol), up, cp)
+        self._check(rc, "aldic_subpb1")
+        return dict(U=U, conv=conv)
+
+    def epipolar_icgn(self, pts, winsize, tol):
+        k = _Keep()
+        n = int(pts.shape[0])
+        z, zp = k.out(n, np.float64)
+        self._check(self.lib.aldic_epipolar_icgn(self.h, n, k.ptr(pts, np.float64), int(winsize), float(tol), zp),
+                    "aldic_epipolar_icgn")
+        return z
+
+    def triangulate(self, pairs, KL, KR, R, T, out=None):
+        k = _Keep()
+        n = int(pairs.shape[0])
+        if out is None:
+            xyz, xp = k.out(3 * n, np.float64)
+            err, ep = k.out(n, np.float64)
+        else:
+            xp, ep = C.c_void_p(out["xyz"].data_ptr()), C.c_void_p(out["err"].data_ptr())
+        rc = self.lib.aldic_triangulate(self.h, n, k.ptr(pairs, np.float64), k.ptr(KL, np.float64),
+                                        k.ptr(KR, np.float64), k.ptr(R, np.float64), k.ptr(np.ravel(T), np.float64),
+                                        xp, ep)
+        self._check(rc, "aldic_triangulate")
+        if out is not None:
+            return out
+        return xyz.reshape((n, 3), order="F"), err
+
+
+_CTX = {}
+
+
+def default_context(device: int = 0) -> Context:
+    if device not in _CTX:
+        _CTX[device] = Context(device)
+    return _CTX[device]
+
+
+# ==================================================================================
+# MATLAB-signature mirrors
+# ==================================================================================
+def funNormalizeImg(Img, gridxyROIRange, ctx: Context | None = None):
+    """[ImgNormalized, gridxyROIRange] = funNormalizeImg(Img, gridxyROIRange)
+    (func/funNormalizeImg.m:1-127).  Img: list of raw images."""
+    ctx = ctx or default_context()
+    gx = list(gridxyROIRange["gridx"])
+    gy = list(gridxyROIRange["gridy"])
+    M, N = Img[0].shape
+    gx = [max(gx[0], 1), min(gx[1], M)]
+    gy = [max(gy[0], 1), min(gy[1], N)]
+    out = []
+    for im in Img:
+        ctx.load_image_raw(_lib.SLOT_DEF, im, gx, gy)
+        out.append(ctx.get_state(1))
+    return out, {"gridx": gx, "gridy": gy}
+
+
+def funImgGradient(ImgRef, ImgDef=None, ImgRefMask=None, ctx: Context | None = None):
+    """Df = funImgGradient(ImgRef, ImgDef, ImgRefMask) (func/funImgGradient.m:50-83)."""
+    ctx = ctx or default_context()
+    ImgRef = np.asarray(ImgRef, dtype=np.float64)
+    M, N = ImgRef.shape
+    ctx.load_image(_lib.SLOT_REF, ImgRef)
+    mask = np.ones((M, N)) if ImgRefMask is None else np.asarray(ImgRefMask, dtype=np.float64)
+    ctx.set_mask(mask)
+    ctx.compute_gradients()
+    return {"DfDx": ctx.get_state(2), "DfDy": ctx.get_state(3), "ImgRefMask": mask, "DfCropWidth": 3,
+            "imgSize": (M, N), "DfAxis": [4, M - 3, 4, N - 3]}
+
+
+def ba_interp2_spline(F, X, Y, method="cubicspline", ctx: Context | None = None):
+    """Z = ba_interp2_spline(F, X, Y) (ba_interp2_spline.cpp:418-435); X = dim-2 and
+    Y = dim-1 coordinates (1-based)."""
+    ctx = ctx or default_context()
+    ctx.load_image(_lib.SLOT_DEF, np.asarray(F, dtype=np.float64))
+    return ctx.interp2(_lib.SLOT_DEF, X, Y)
+
+
+def funIntegerSearch(f, g, tempSizeOfSearchRegion, gridx, gridy, winsize, winstepsize, tempNoOfInitPt=0,
+                     ctx: Context | None = None):
+    """[x, y, u, v, cc] = funIntegerSearch(f, g, search, gridx, gridy, winsize, step, 0)
+    (func/funIntegerSearch.m:2-98).  Only the whole-field mode (0) is on the device."""
+    if tempNoOfInitPt != 0:
+        raise AldicError("funIntegerSearch: only the whole-field mode (tempNoOfInitPt = 0) is implemented")
+    ctx = ctx or default_context()
+    ctx.load_image(_lib.SLOT_REF, np.asarray(f, dtype=np.float64))
+    ctx.load_image(_lib.SLOT_DEF, np.asarray(g, dtype=np.float64))
+    w = int(np.ravel(winsize)[0])
+    st = int(np.ravel(winstepsize)[0])
+    r = ctx.integer_search(tempSizeOfSearchRegion, gridx, gridy, w, st)
+    return r["x"], r["y"], r["u"], r["v"], {"max": r["phi"], "A": []}
+
+
+def _load_frame(ctx, Df, ImgRef, ImgDef, mask):
+    ctx.load_image(_lib.SLOT_REF, np.asarray(ImgRef, dtype=np.float64))
+    ctx.load_image(_lib.SLOT_DEF, np.asarray(ImgDef, dtype=np.float64))
+    ctx.set_mask(None if mask is None else np.asarray(mask, dtype=np.float64))
+    ctx.set_gradients(np.asarray(Df["DfDx"], dtype=np.float64), np.asarray(Df["DfDy"], dtype=np.float64))
+
+
+def bad_points_local(conv, rule="quadtree"):
+    """Bad-point rules after the local IC-GN loop: codes < 0 or > 99 plus the iteration
+    outlier test (func_quadtree/LocalICGNQuadtree.m:169-192: > max(mu + sigma, 6) with a
+    normal fit; func/LocalICGN.m:170-182: > mean + 0.15 std).  Returns (bad index array,
+    LocalICGNBadPtNum)."""
+    conv = np.asarray(conv)
+    n = conv.size
+    bad = (conv < 0) | (conv > 99)
+    row3 = int(np.sum(conv == 102))
+    num = int(np.sum(bad)) - row3
+    good = ~bad
+    if rule == "quadtree":
+        if good.sum() >= 3:
+            mu = conv[good].mean()
+            sd = conv[good].std(ddof=1)   # fitdist 'Normal' sigma (unbiased std)
+        else:
+            mu, sd = np.inf, 0.0
+        thr = max(mu + sd, 6)
+    else:
+        mu = conv[good].mean() if good.any() else np.nan
+        sd = conv[good].std(ddof=1) if good.sum() > 1 else np.nan
+        thr = mu + 0.15 * sd
+    bad = bad | (conv > thr)
+    return np.nonzero(bad)[0], num if n else 0
+
+
+def bad_points_subpb1(conv):
+    """Subpb1Quadtree.m:130-143 rules: codes < 0 or > 99, plus > max(mean + 0.25 std, 10)."""
+    conv = np.asarray(conv)
+    bad = (conv < 0) | (conv > 99)
+    row3 = int(np.sum(conv == 102))
+    num = int(np.sum(bad)) - row3
+    good = ~bad
+    mu = conv[good].mean() if good.any() else np.nan
+    sd = conv[good].std(ddof=1) if good.sum() > 1 else np.nan
+    bad = bad | (conv > max(mu + 0.25 * sd, 10))
+    return np.nonzero(bad)[0], num
+
+
+def LocalICGN(U0, coordinatesFEM, Df, ImgRef, ImgDef, DICpara, ICGNmethod="GaussNewton", tol=1e-3,
+              shapeFunctionOrder=1, ctx: Context | None = None):
+    """[U, F, HtempPar, LocalTime, ConvItPerEle, LocalICGNBadPtNum] = LocalICGN(...)
+    (func/LocalICGN.m).  The device runs the loop body (:64-164); the bad-point marking
+    (:166-189) follows; bad points are returned as NaN (the natural-neighbour fill of
+    :198-220 is left to the caller)."""
+    if shapeFunctionOrder != 1:
+        raise AldicError("only the first-order shape function is implemented (as in the reference)")
+    ctx = ctx or default_context()
+    _load_frame(ctx, Df, ImgRef, ImgDef, None)
+    t0 = time.perf_counter()
+    r = ctx.local_icgn(_lib.UNIFORM, np.asarray(coordinatesFEM, dtype=np.float64), U0, DICpara["winsize"], tol)
+    local_time = time.perf_counter() - t0
+    U, F, conv = r["U"].copy(), r["F"].copy(), r["conv"]
+    bad, num = bad_points_local(conv, rule="uniform")
+    U[2 * bad] = np.nan
+    U[2 * bad + 1] = np.nan
+    for k in range(4):
+        F[4 * bad + k] = np.nan
+    return U, F, r["H"], local_time, conv, num
+
+
+def LocalICGNQuadtree(U0, coordinatesFEM, Df, ImgRef, ImgDef, DICpara, ICGNmethod="GaussNewton", tol=1e-3,
+                      shapeFunctionOrder=1, ctx: Context | None = None):
+    """[U, F, HtempPar, LocalTime, ConvItPerEle, LocalICGNBadPtNum, markCoordHoleStrain]
+    = LocalICGNQuadtree(...) (func_quadtree/LocalICGNQuadtree.m).  Device loop body
+    (:67-164), then the bad-point rules (:167-202); bad points are NaN (the region-wise
+    fill of :208-325 is left to the caller)."""
+    if shapeFunctionOrder != 1:
+        raise AldicError("only the first-order shape function is implemented (as in the reference)")
+    ctx = ctx or default_context()
+    _load_frame(ctx, Df, ImgRef, ImgDef, Df.get("ImgRefMask"))
+    t0 = time.perf_counter()
+    r = ctx.local_icgn(_lib.QUADTREE, np.asarray(coordinatesFEM, dtype=np.float64), U0, DICpara["winsize"], tol)
+    local_time = time.perf_counter() - t0
+    U, F, conv = r["U"].copy(), r["F"].copy(), r["conv"]
+    bad, num = bad_points_local(conv, rule="quadtree")
+    U[2 * bad] = np.nan
+    U[2 * bad + 1] = np.nan
+    mark = np.nonzero(r["markHole"] == 1)[0]
+    return U, F, r["H"], local_time, conv, num, mark
+
+
+def Subpb1Quadtree(UOld, FOld, udual, vdual, coordinatesFEM, Df, ImgRef, ImgDef, mu, beta, HPar, ALSolveStep,
+                   DICpara, ICGNmethod="GaussNewton", tol=1e-2, ctx: Context | None = None):
+    """[U, HPar, ALSub1Time, ConvItPerEle, LocalICGNBadPtNum] = Subpb1Quadtree(...)
+    (func_quadtree/Subpb1Quadtree.m).  Device loop body (:71-126), then the bad-point rules
+    (:130-149); bad points are NaN."""
+    ctx = ctx or default_context()
+    _load_frame(ctx, Df, ImgRef, ImgDef, Df.get("ImgRefMask"))
+    n = np.asarray(coordinatesFEM).shape[0]
+    wl = DICpara.get("winsize_List")
+    if wl is None:
+        wl = np.full((n, 2), DICpara["winsize"], dtype=np.int32)
+    t0 = time.perf_counter()
+    r = ctx.subpb1(_lib.QUADTREE, np.asarray(coordinatesFEM, dtype=np.float64), UOld, FOld, vdual, mu, tol,
+                   winsize=int(DICpara["winsize"]), winsize_list=np.asarray(wl, dtype=np.int32))
+    t = time.perf_counter() - t0
+    U, conv = r["U"].copy(), r["conv"]
+    bad, num = bad_points_subpb1(conv)
+    U[2 * bad] = np.nan
+    U[2 * bad + 1] = np.nan
+    return U, HPar, t, conv, num
+
+
+def Subpb1(UOld, FOld, udual, vdual, coordinatesFEM, Df, ImgRef, ImgDef, mu, beta, HPar, ALSolveStep, DICpara,
+           ICGNmethod="GaussNewton", tol=1e-2, ctx: Context | None = None):
+    """Uniform-mesh Subpb1 (func/Subpb1.m with func/funICGN_Subpb1.m); HPar is the n x 21
+    Hessian array of LocalICGN (zeros at ALSolveStep 1, as the reference passes)."""
+    ctx = ctx or default_context()
+    _load_frame(ctx, Df, ImgRef, ImgDef, None)
+    n = np.asarray(coordinatesFEM).shape[0]
+    H = np.zeros((n, 21)) if (HPar is None or ALSolveStep <= 1) else np.asarray(HPar, dtype=np.float64)
+    t0 = time.perf_counter()
+    r = ctx.subpb1(_lib.UNIFORM, np.asarray(coordinatesFEM, dtype=np.float64), UOld, FOld, vdual, mu, tol,
+                   winsize=int(DICpara["winsize"]), HPar=H)
+    t = time.perf_counter() - t0
+    U, conv = r["U"].copy(), r["conv"]
+    bad, num = bad_points_subpb1(conv)
+    U[2 * bad] = np.nan
+    U[2 * bad + 1] = np.nan
+    return U, HPar, t, conv, num
+
+
+def epipolar_ICGN1(pointCandidate, Df, ImgRef, ImgDef, winsize, tol, ICGNmethod="GaussNewton",
+                   ctx: Context | None = None):
+    """ZNSSD = epipolar_ICGN1(pointCandidate, Df, ImgRef, ImgDef, winsize, tol)
+    (func/epipolar_ICGN1.m), batched over the rows of pointCandidate (n x 2)."""
+    ctx = ctx or default_context()
+    _load_frame(ctx, Df, ImgRef, ImgDef, None)
+    pts = np.atleast_2d(np.asarray(pointCandidate, dtype=np.float64))
+    return ctx.epipolar_icgn(pts, winsize, tol)
+
+
+def stereoReconstruction_quadtree(matchedPairs, cameraParams, ctx: Context | None = None):
+    """[FinalResult, reprojectionErrors] = stereoReconstruction_quadtree(matchedPairs, cameraParams)
+    (func_quadtree/stereoReconstruction_quadtree.m).  matchedPairs: list of n x 4 arrays;
+    cameraParams: dict with KL, KR (3x3), R (3x3), T (3,), zero distortion."""
+    ctx = ctx or default_context()
+    coords, errs = [], []
+    for pts in matchedPairs:
+        xyz, err = ctx.triangulate(np.asarray(pts, dtype=np.float64), cameraParams["KL"], cameraParams["KR"],
+                                   cameraParams["R"], cameraParams["T"])
+        coords.append(xyz)
+        errs.append(err)
+    final = {"Coordinates": coords, "Displacement": [c - coords[0] for c in coords]}
+    return final, errs

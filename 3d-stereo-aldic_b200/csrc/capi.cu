@@ -1,0 +1,644 @@
+// C ABI of the ALDIC B200 library: context (stream, device frame, scratch), argument
+// staging between host and device memory, and the batched entry points declared in
+// include/aldic_b200.h.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/aldic_b200.h"
+#include "kernels.h"
+
+using namespace aldic;
+
+namespace {
+
+// Device scratch arena: bump allocation per call, reset at the start of every call.
+// Growth synchronises the stream first, so earlier work never sees freed memory.
+struct Arena {
+  char* base = nullptr;
+  size_t cap = 0, used = 0;
+};
+
+}  // namespace
+
+struct aldic_ctx {
+  int device = 0;
+  cudaStream_t own = nullptr;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  int64_t launches = 0;
+  // device frame
+  int M = 0, N = 0;
+  float* img[2] = {nullptr, nullptr};
+  bool img_ok[2] = {false, false};
+  uint8_t* mask = nullptr;
+  bool has_mask = false;
+  float* gx = nullptr;
+  float* gy = nullptr;
+  bool grad_ok = false;
+  bool grad_from_mask = false;  // gradients computed here (they depend on the mask)
+  // persistent scratch
+  double* stats = nullptr;  // 4 doubles: sum, sum sq dev, mean, std
+  double* partials = nullptr;
+  unsigned int* counter = nullptr;
+  int npartials = 0;
+  int* qcount = nullptr;
+  double* I1 = nullptr;
+  double* I2 = nullptr;
+  size_t ii_cap = 0;
+  Arena arena;
+  // outputs to copy back at the end of a call
+  struct Back {
+    void* host;
+    const void* dev;
+    size_t bytes;
+  };
+  std::vector<Back> back;
+};
+
+namespace {
+
+int fail(aldic_ctx* c, int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  if (c) c->err = buf;
+  return code;
+}
+
+int cuda_fail(aldic_ctx* c, cudaError_t e, const char* what) {
+  return fail(c, ALDIC_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define CK(call)                                         \
+  do {                                                   \
+    cudaError_t e_ = (call);                             \
+    if (e_ != cudaSuccess) return cuda_fail(c, e_, #call); \
+  } while (0)
+
+bool is_device_ptr(const void* p) {
+  if (!p) return false;
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+}
+
+int arena_reserve(aldic_ctx* c, size_t bytes) {
+  if (c->arena.cap >= bytes) return ALDIC_OK;
+  CK(cudaStreamSynchronize(c->stream));
+  if (c->arena.base) CK(cudaFree(c->arena.base));
+  c->arena.base = nullptr;
+  size_t cap = bytes + bytes / 2 + (1 << 20);
+  CK(cudaMalloc(&c->arena.base, cap));
+  c->arena.cap = cap;
+  return ALDIC_OK;
+}
+
+void* arena_take(aldic_ctx* c, size_t bytes) {
+  const size_t off = (c->arena.used + 255) & ~size_t(255);
+  c->arena.used = off + bytes;
+  return c->arena.base + off;
+}
+
+// Staging plan: the caller lists every array argument with its size, then the arena is
+// sized once and host arrays are copied in (inputs) or scheduled for copy-back (outputs).
+struct Arg {
+  const void* user;
+  size_t bytes;
+  bool output;
+  void* dev;
+};
+
+int stage(aldic_ctx* c, std::vector<Arg*> args) {
+  c->arena.used = 0;
+  c->back.clear();
+  size_t need = 0;
+  for (Arg* a : args)
+    if (a->user && !is_device_ptr(a->user) && a->bytes) need += ((a->bytes + 255) & ~size_t(255)) + 256;
+  int rc = arena_reserve(c, need);
+  if (rc) return rc;
+  for (Arg* a : args) {
+    if (!a->user || a->bytes == 0) {
+      a->dev = nullptr;
+      continue;
+    }
+    if (is_device_ptr(a->user)) {
+      a->dev = const_cast<void*>(a->user);
+      continue;
+    }
+    a->dev = arena_take(c, a->bytes);
+    if (a->output) {
+      c->back.push_back({const_cast<void*>(a->user), a->dev, a->bytes});
+    } else {
+      CK(cudaMemcpyAsync(a->dev, a->user, a->bytes, cudaMemcpyHostToDevice, c->stream));
+    }
+  }
+  return ALDIC_OK;
+}
+
+// Copy host outputs back and wait for them; otherwise leave the work in flight.
+int finish(aldic_ctx* c, int launched) {
+  c->launches += launched;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(c, e, "kernel launch");
+  for (auto& b : c->back) CK(cudaMemcpyAsync(b.host, b.dev, b.bytes, cudaMemcpyDeviceToHost, c->stream));
+  if (!c->back.empty()) CK(cudaStreamSynchronize(c->stream));
+  c->back.clear();
+  return ALDIC_OK;
+}
+
+int ensure_frame(aldic_ctx* c, int M, int N) {
+  if (M < 8 || N < 8) return fail(c, ALDIC_ERR_ARG, "image must be at least 8 x 8 (got %d x %d)", M, N);
+  if (c->M == M && c->N == N && c->img[0]) return ALDIC_OK;
+  CK(cudaStreamSynchronize(c->stream));
+  for (int s = 0; s < 2; ++s)
+    if (c->img[s]) CK(cudaFree(c->img[s]));
+  if (c->mask) CK(cudaFree(c->mask));
+  if (c->gx) CK(cudaFree(c->gx));
+  if (c->gy) CK(cudaFree(c->gy));
+  const size_t npx = (size_t)M * N, ng = (size_t)(M - 6) * (N - 6);
+  for (int s = 0; s < 2; ++s) CK(cudaMalloc(&c->img[s], npx * sizeof(float)));
+  CK(cudaMalloc(&c->mask, npx));
+  CK(cudaMalloc(&c->gx, ng * sizeof(float)));
+  CK(cudaMalloc(&c->gy, ng * sizeof(float)));
+  c->M = M;
+  c->N = N;
+  c->img_ok[0] = c->img_ok[1] = false;
+  c->has_mask = false;
+  c->grad_ok = false;
+  return ALDIC_OK;
+}
+
+int need_frame(aldic_ctx* c, bool grads) {
+  if (!c->img_ok[0] || !c->img_ok[1]) return fail(c, ALDIC_ERR_STATE, "reference and deformed images must be loaded");
+  if (grads && !c->grad_ok) return fail(c, ALDIC_ERR_STATE, "gradients not set (aldic_compute_gradients / aldic_set_gradients)");
+  return ALDIC_OK;
+}
+
+FrameDev frame_of(aldic_ctx* c) {
+  FrameDev f;
+  f.ref = c->img[0];
+  f.def = c->img[1];
+  f.mask = c->has_mask ? c->mask : nullptr;
+  f.gx = c->gx;
+  f.gy = c->gy;
+  f.M = c->M;
+  f.N = c->N;
+  return f;
+}
+
+size_t dtype_size(int dt) {
+  switch (dt) {
+    case ALDIC_U8: return 1;
+    case ALDIC_U16: return 2;
+    case ALDIC_F32: return 4;
+    case ALDIC_F64: return 8;
+    default: return 0;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int aldic_abi_version(void) { return 1; }
+
+int aldic_create(aldic_ctx** out, int device) {
+  if (!out) return ALDIC_ERR_ARG;
+  *out = nullptr;
+  aldic_ctx* c = new aldic_ctx();
+  c->device = device;
+  cudaError_t e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking);
+  if (e == cudaSuccess) {
+    c->stream = c->own;
+    c->npartials = 148 * 8;
+    e = cudaMalloc(&c->stats, 8 * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&c->partials, c->npartials * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&c->counter, 64);
+    if (e == cudaSuccess) e = cudaMemset(c->counter, 0, 64);
+    if (e == cudaSuccess) e = cudaMalloc(&c->qcount, 64);
+  }
+  if (e != cudaSuccess) {
+    delete c;
+    return ALDIC_ERR_CUDA;
+  }
+  *out = c;
+  return ALDIC_OK;
+}
+
+void aldic_destroy(aldic_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  void* bufs[] = {c->img[0], c->img[1], c->mask, c->gx, c->gy, c->stats, c->partials, c->counter, c->qcount,
+                  c->I1, c->I2, c->arena.base};
+  for (void* b : bufs)
+    if (b) cudaFree(b);
+  if (c->own) cudaStreamDestroy(c->own);
+  delete c;
+}
+
+const char* aldic_last_error(const aldic_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+int aldic_set_stream(aldic_ctx* c, void* stream) {
+  if (!c) return ALDIC_ERR_ARG;
+  c->stream = stream ? (cudaStream_t)stream : c->own;
+  return ALDIC_OK;
+}
+
+int aldic_synchronize(aldic_ctx* c) {
+  if (!c) return ALDIC_ERR_ARG;
+  CK(cudaStreamSynchronize(c->stream));
+  return ALDIC_OK;
+}
+
+int64_t aldic_launch_count(const aldic_ctx* c) { return c ? c->launches : -1; }
+
+int aldic_load_image_raw(aldic_ctx* c, int slot, const void* img, int dtype, int M, int N, const int* gridx,
+                         const int* gridy, const double* mask, double* mean_std) {
+  if (!c) return ALDIC_ERR_ARG;
+  if (slot != 0 && slot != 1) return fail(c, ALDIC_ERR_ARG, "slot must be ALDIC_SLOT_REF or ALDIC_SLOT_DEF");
+  const size_t es = dtype_size(dtype);
+  if (!img || !es) return fail(c, ALDIC_ERR_ARG, "image pointer or dtype invalid");
+  if (!gridx || !gridy) return fail(c, ALDIC_ERR_ARG, "gridx/gridy required");
+  int rc = ensure_frame(c, M, N);
+  if (rc) return rc;
+  // ROI clamp (funNormalizeImg.m:112-115)
+  int gx0 = gridx[0] < 1 ? 1 : gridx[0], gx1 = gridx[1] > M ? M : gridx[1];
+  int gy0 = gridy[0] < 1 ? 1 : gridy[0], gy1 = gridy[1] > N ? N : gridy[1];
+  if (gx1 < gx0 || gy1 < gy0 || (long long)(gx1 - gx0 + 1) * (gy1 - gy0 + 1) < 2)
+    return fail(c, ALDIC_ERR_ARG, "ROI must hold at least two pixels");
+  const size_t npx = (size_t)M * N;
+  Arg ai{img, npx * es, false, nullptr}, am{mask, mask ? npx * sizeof(double) : 0, false, nullptr};
+  Arg ams{mean_std, mean_std ? 2 * sizeof(double) : 0, true, nullptr};
+  rc = stage(c, {&ai, &am, &ams});
+  if (rc) return rc;
+  int launched = 0;
+  uint8_t* mk = nullptr;
+  if (am.dev) {
+    mk = (uint8_t*)arena_take(c, npx);
+    launched += launch_mask_binarize((const double*)am.dev, (long long)npx, mk, c->stream);
+  }
+  launched += launch_normalize(ai.dev, dtype, M, N, gx0 - 1, gx1, gy0 - 1, gy1, mk, c->img[slot], c->stats,
+                               c->partials, c->npartials, c->counter, c->stream);
+  if (ams.dev) CK(cudaMemcpyAsync(ams.dev, c->stats + 2, 2 * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  c->img_ok[slot] = true;
+  if (slot == 0) c->grad_ok = false;
+  return finish(c, launched);
+}
+
+int aldic_load_image(aldic_ctx* c, int slot, const double* img, int M, int N) {
+  if (!c) return ALDIC_ERR_ARG;
+  if (slot != 0 && slot != 1) return fail(c, ALDIC_ERR_ARG, "slot must be ALDIC_SLOT_REF or ALDIC_SLOT_DEF");
+  if (!img) return fail(c, ALDIC_ERR_ARG, "image pointer is NULL");
+  int rc = ensure_frame(c, M, N);
+  if (rc) return rc;
+  const size_t npx = (size_t)M * N;
+  Arg ai{img, npx * sizeof(double), false, nullptr};
+  rc = stage(c, {&ai});
+  if (rc) return rc;
+  const int l = launch_f64_to_f32((const double*)ai.dev, (long long)npx, c->img[slot], c->stream);
+  c->img_ok[slot] = true;
+  if (slot == 0) c->grad_ok = false;
+  return finish(c, l);
+}
+
+int aldic_set_mask(aldic_ctx* c, const double* mask, int M, int N) {
+  if (!c) return ALDIC_ERR_ARG;
+  if (c->M != M || c->N != N) return fail(c, ALDIC_ERR_ARG, "mask size %d x %d differs from the frame", M, N);
+  if (!mask) {
+    c->has_mask = false;
+    if (c->grad_from_mask) c->grad_ok = false;
+    return ALDIC_OK;
+  }
+  const size_t npx = (size_t)M * N;
+  Arg am{mask, npx * sizeof(double), false, nullptr};
+  int rc = stage(c, {&am});
+  if (rc) return rc;
+  const int l = launch_mask_binarize((const double*)am.dev, (long long)npx, c->mask, c->stream);
+  c->has_mask = true;
+  if (c->grad_from_mask) c->grad_ok = false;  // device-computed gradients carry the old mask
+  return finish(c, l);
+}
+
+int aldic_compute_gradients(aldic_ctx* c) {
+  if (!c) return ALDIC_ERR_ARG;
+  if (!c->img_ok[0]) return fail(c, ALDIC_ERR_STATE, "reference image not loaded");
+  c->arena.used = 0;
+  c->back.clear();
+  const int l = launch_gradient(c->img[0], c->has_mask ? c->mask : nullptr, c->M, c->N, c->gx, c->gy, c->stream);
+  c->grad_ok = true;
+  c->grad_from_mask = true;
+  return finish(c, l);
+}
+
+int aldic_set_gradients(aldic_ctx* c, const double* dfdx, const double* dfdy, int M6, int N6) {
+  if (!c) return ALDIC_ERR_ARG;
+  if (!dfdx || !dfdy) return fail(c, ALDIC_ERR_ARG, "gradient pointers are NULL");
+  if (M6 != c->M - 6 || N6 != c->N - 6)
+    return fail(c, ALDIC_ERR_ARG, "gradients must be (M-6) x (N-6) = %d x %d", c->M - 6, c->N - 6);
+  const size_t ng = (size_t)M6 * N6;
+  Arg ax{dfdx, ng * sizeof(double), false, nullptr}, ay{dfdy, ng * sizeof(double), false, nullptr};
+  int rc = stage(c, {&ax, &ay});
+  if (rc) return rc;
+  int l = launch_f64_to_f32((const double*)ax.dev, (long long)ng, c->gx, c->stream);
+  l += launch_f64_to_f32((const double*)ay.dev, (long long)ng, c->gy, c->stream);
+  c->grad_ok = true;
+  c->grad_from_mask = false;
+  return finish(c, l);
+}
+
+int aldic_get_state(aldic_ctx* c, int what, double* out) {
+  if (!c || !out) return ALDIC_ERR_ARG;
+  const float* src = nullptr;
+  size_t n = 0;
+  if (what == 0 || what == 1) {
+    if (!c->img_ok[what]) return fail(c, ALDIC_ERR_STATE, "image slot %d not loaded", what);
+    src = c->img[what];
+    n = (size_t)c->M * c->N;
+  } else if (what == 2 || what == 3) {
+    if (!c->grad_ok) return fail(c, ALDIC_ERR_STATE, "gradients not set");
+    src = what == 2 ? c->gx : c->gy;
+    n = (size_t)(c->M - 6) * (c->N - 6);
+  } else {
+    return fail(c, ALDIC_ERR_ARG, "unknown state %d", what);
+  }
+  Arg ao{out, n * sizeof(double), true, nullptr};
+  int rc = stage(c, {&ao});
+  if (rc) return rc;
+  return finish(c, launch_f32_to_f64(src, (long long)n, (double*)ao.dev, c->stream));
+}
+
+int aldic_interp2(aldic_ctx* c, int slot, int64_t n, const double* X, const double* Y, double* Z) {
+  if (!c) return ALDIC_ERR_ARG;
+  if (slot != 0 && slot != 1) return fail(c, ALDIC_ERR_ARG, "bad slot");
+  if (!c->img_ok[slot]) return fail(c, ALDIC_ERR_STATE, "image slot %d not loaded", slot);
+  if (n < 0 || (n > 0 && (!X || !Y || !Z))) return fail(c, ALDIC_ERR_ARG, "bad point arrays");
+  if (n == 0) return ALDIC_OK;
+  Arg ax{X, n * sizeof(double), false, nullptr}, ay{Y, n * sizeof(double), false, nullptr};
+  Arg az{Z, n * sizeof(double), true, nullptr};
+  int rc = stage(c, {&ax, &ay, &az});
+  if (rc) return rc;
+  const int l = launch_interp_points(c->img[slot], c->M, c->N, n, (const double*)ax.dev, (const double*)ay.dev,
+                                     (double*)az.dev, c->stream);
+  return finish(c, l);
+}
+
+int aldic_search_grid(const int* gridx, const int* gridy, int winsize, int step, int* nx, int* ny) {
+  if (!gridx || !gridy || !nx || !ny || step <= 0 || winsize < 0) return ALDIC_ERR_ARG;
+  const int ex = gridx[1] - winsize - step, ey = gridy[1] - winsize - step;
+  *nx = ex >= gridx[0] ? (ex - gridx[0]) / step + 1 : 0;
+  *ny = ey >= gridy[0] ? (ey - gridy[0]) / step + 1 : 0;
+  return ALDIC_OK;
+}
+
+int aldic_integer_search(aldic_ctx* c, const int* search, const int* gridx, const int* gridy, int winsize, int step,
+                         double* x, double* y, double* u, double* v, double* phi) {
+  if (!c) return ALDIC_ERR_ARG;
+  int rc = need_frame(c, false);
+  if (rc) return rc;
+  if (!search || !gridx || !gridy) return fail(c, ALDIC_ERR_ARG, "search/gridx/gridy required");
+  if (winsize < 2 || step < 1) return fail(c, ALDIC_ERR_ARG, "winsize >= 2 and step >= 1 required");
+  if (search[0] < 0 || search[1] < 0) return fail(c, ALDIC_ERR_ARG, "search region must be non-negative");
+  if ((size_t)(winsize + 1) * (winsize + 1) > 120 * 120)
+    return fail(c, ALDIC_ERR_ARG, "winsize %d too large for the device search", winsize);
+  int nx, ny;
+  aldic_search_grid(gridx, gridy, winsize, step, &nx, &ny);
+  const size_t n = (size_t)nx * ny;
+  if (n == 0) return ALDIC_OK;
+  if (!x || !y || !u || !v || !phi) return fail(c, ALDIC_ERR_ARG, "output arrays required");
+  const size_t iin = (size_t)(c->M + 1) * (c->N + 1);
+  if (c->ii_cap < iin) {
+    CK(cudaStreamSynchronize(c->stream));
+    if (c->I1) CK(cudaFree(c->I1));
+    if (c->I2) CK(cudaFree(c->I2));
+    c->I1 = c->I2 = nullptr;
+    CK(cudaMalloc(&c->I1, iin * sizeof(double)));
+    CK(cudaMalloc(&c->I2, iin * sizeof(double)));
+    c->ii_cap = iin;
+  }
+  Arg ox{x, n * 8, true, nullptr}, oy{y, n * 8, true, nullptr}, ou{u, n * 8, true, nullptr};
+  Arg ov{v, n * 8, true, nullptr}, op{phi, n * 8, true, nullptr};
+  rc = stage(c, {&ox, &oy, &ou, &ov, &op});
+  if (rc) return rc;
+  SearchArgs a;
+  a.f = c->img[0];
+  a.g = c->img[1];
+  a.M = c->M;
+  a.N = c->N;
+  a.s0 = search[0];
+  a.s1 = search[1];
+  a.gx0 = gridx[0];
+  a.gx1 = gridx[1];
+  a.gy0 = gridy[0];
+  a.gy1 = gridy[1];
+  a.winsize = winsize;
+  a.step = step;
+  a.nx = nx;
+  a.ny = ny;
+  a.x = (double*)ox.dev;
+  a.y = (double*)oy.dev;
+  a.u = (double*)ou.dev;
+  a.v = (double*)ov.dev;
+  a.phi = (double*)op.dev;
+  a.I1 = c->I1;
+  a.I2 = c->I2;
+  return finish(c, launch_search(a, c->stream));
+}
+
+static int icgn_common(aldic_ctx* c, int variant, int64_t n, const double* coords, const double* U0, int winsize,
+                       double tol, double* U, double* F, double* H, int32_t* conv, uint8_t* mark, double* znssd) {
+  int rc = need_frame(c, true);
+  if (rc) return rc;
+  if (n < 0) return fail(c, ALDIC_ERR_ARG, "n < 0");
+  if (n == 0) return ALDIC_OK;
+  if (n > (1LL << 30)) return fail(c, ALDIC_ERR_ARG, "too many subsets");
+  if (winsize < 2 || winsize > 200) return fail(c, ALDIC_ERR_ARG, "winsize %d out of range [2, 200]", winsize);
+  if (!coords) return fail(c, ALDIC_ERR_ARG, "coords required");
+  const bool epi = (variant == 2);
+  if (!epi && (!U0 || !U || !F || !conv)) return fail(c, ALDIC_ERR_ARG, "U0, U, F and conv are required");
+  if (epi && !znssd) return fail(c, ALDIC_ERR_ARG, "znssd output required");
+  // largest enlarged window (funICGN.m:61 / funICGNQuadtree.m:70)
+  int wmax;
+  const double w = winsize, Nw = (w + 1) * (w + 1);
+  if (variant == 1) {
+    // masked count < 0.4 (w+1)^2, so the growth factor is below sqrt(1/0.6)
+    wmax = (int)(2 * std::ceil(std::sqrt(1.0 / 0.6) * w / 2)) + 2;
+  } else {
+    wmax = (int)std::round(std::sqrt(2.0) * w);
+  }
+  if (wmax < winsize) wmax = winsize;
+  if (icgn_smem_bytes(wmax) > 200 * 1024) return fail(c, ALDIC_ERR_ARG, "winsize %d too large for shared memory", winsize);
+  const size_t qbytes = (size_t)2 * n * 3 * sizeof(int);
+  Arg ac{coords, (size_t)n * 2 * 8, false, nullptr}, au0{epi ? nullptr : U0, epi ? 0 : (size_t)n * 2 * 8, false, nullptr};
+  Arg au{U, epi ? 0 : (size_t)n * 2 * 8, true, nullptr}, af{F, epi ? 0 : (size_t)n * 4 * 8, true, nullptr};
+  Arg ah{H, H ? (size_t)n * 21 * 8 : 0, true, nullptr};
+  Arg acv{conv, conv ? (size_t)n * 4 : 0, true, nullptr};
+  Arg am{mark, mark ? (size_t)n : 0, true, nullptr};
+  Arg az{znssd, znssd ? (size_t)n * 8 : 0, true, nullptr};
+  // the work queue comes from the arena too: reserve room for it with the staged arguments
+  c->arena.used = 0;
+  rc = arena_reserve(c, qbytes + 4096 + (size_t)n * (2 + 2 + 2 + 4 + 21 + 1 + 1) * 8 + 8192);
+  if (rc) return rc;
+  rc = stage(c, {&ac, &au0, &au, &af, &ah, &acv, &am, &az});
+  if (rc) return rc;
+  IcgnArgs a;
+  a.fr = frame_of(c);
+  a.variant = variant;
+  a.n = n;
+  a.coords = (const double*)ac.dev;
+  a.U0 = (const double*)au0.dev;
+  a.winsize = winsize;
+  a.tol = tol;
+  a.max_iter = epi ? 30 : 100;
+  a.crop = epi ? 4 : 3;
+  a.U = (double*)au.dev;
+  a.F = (double*)af.dev;
+  a.H = (double*)ah.dev;
+  a.conv = (int*)acv.dev;
+  a.mark = (uint8_t*)am.dev;
+  a.znssd = (double*)az.dev;
+  a.queue = (int*)arena_take(c, qbytes);
+  a.qcount = c->qcount;
+  return finish(c, launch_icgn(a, wmax, c->stream));
+}
+
+int aldic_local_icgn(aldic_ctx* c, int variant, int64_t n, const double* coords, const double* U0, int winsize,
+                     double tol, double* U, double* F, double* H, int32_t* conv, uint8_t* markHole) {
+  if (!c) return ALDIC_ERR_ARG;
+  if (variant != ALDIC_UNIFORM && variant != ALDIC_QUADTREE) return fail(c, ALDIC_ERR_ARG, "bad variant %d", variant);
+  return icgn_common(c, variant, n, coords, U0, winsize, tol, U, F, H, conv,
+                     variant == ALDIC_QUADTREE ? markHole : nullptr, nullptr);
+}
+
+int aldic_epipolar_icgn(aldic_ctx* c, int64_t n, const double* pts, int winsize, double tol, double* znssd) {
+  if (!c) return ALDIC_ERR_ARG;
+  return icgn_common(c, 2, n, pts, nullptr, winsize, tol, nullptr, nullptr, nullptr, nullptr, nullptr, znssd);
+}
+
+int aldic_subpb1(aldic_ctx* c, int variant, int64_t n, const double* coords, const double* UOld, const double* FOld,
+                 const double* vdual, const int32_t* winsize_list, int winsize, const double* HPar, double mu,
+                 double tol, double* U, int32_t* conv) {
+  if (!c) return ALDIC_ERR_ARG;
+  int rc = need_frame(c, true);
+  if (rc) return rc;
+  if (variant != ALDIC_UNIFORM && variant != ALDIC_QUADTREE) return fail(c, ALDIC_ERR_ARG, "bad variant %d", variant);
+  if (n < 0) return fail(c, ALDIC_ERR_ARG, "n < 0");
+  if (n == 0) return ALDIC_OK;
+  if (!coords || !UOld || !FOld || !vdual || !U || !conv) return fail(c, ALDIC_ERR_ARG, "missing array argument");
+  if (variant == ALDIC_QUADTREE && !winsize_list) return fail(c, ALDIC_ERR_ARG, "winsize_list required (quadtree)");
+  // nominal bucket size and the largest enlarged window
+  int wl_max = winsize;
+  if (variant == ALDIC_QUADTREE) {
+    std::vector<int32_t> wl((size_t)n * 2);
+    if (is_device_ptr(winsize_list)) {
+      CK(cudaMemcpyAsync(wl.data(), winsize_list, wl.size() * 4, cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+    } else {
+      std::memcpy(wl.data(), winsize_list, wl.size() * 4);
+    }
+    wl_max = 0;
+    for (int32_t v : wl) {
+      if (v < 2 || v > 200) return fail(c, ALDIC_ERR_ARG, "winsize_list entry %d out of range [2, 200]", (int)v);
+      wl_max = v > wl_max ? v : wl_max;
+    }
+    if (winsize < 2) winsize = wl_max;
+  }
+  if (winsize < 2 || winsize > 200) return fail(c, ALDIC_ERR_ARG, "winsize %d out of range", winsize);
+  int wmx, wmy;
+  {
+    const double w = wl_max, Nw = (w + 1) * (w + 1);
+    (void)Nw;
+    if (variant == ALDIC_QUADTREE) {
+      // both enlargement factors are below sqrt(1/0.6) (masked count < 0.4 of the window)
+      wmx = wmy = (int)(2 * std::ceil(std::sqrt(1.0 / 0.6) * w / 2)) + 2;
+    } else {
+      wmx = wmy = (int)std::round(std::sqrt(2.0) * w);
+    }
+    if (wmx < wl_max) wmx = wl_max;
+    if (wmy < wl_max) wmy = wl_max;
+  }
+  if (sub1_smem_bytes(wmx, wmy) > 200 * 1024) return fail(c, ALDIC_ERR_ARG, "winsize too large for shared memory");
+  const size_t qbytes = (size_t)2 * n * 4 * sizeof(int);
+  Arg ac{coords, (size_t)n * 16, false, nullptr}, auo{UOld, (size_t)n * 16, false, nullptr};
+  Arg afo{FOld, (size_t)n * 32, false, nullptr}, avd{vdual, (size_t)n * 16, false, nullptr};
+  Arg awl{variant == ALDIC_QUADTREE ? winsize_list : nullptr, variant == ALDIC_QUADTREE ? (size_t)n * 8 : 0, false,
+          nullptr};
+  Arg ahp{variant == ALDIC_UNIFORM ? HPar : nullptr, (variant == ALDIC_UNIFORM && HPar) ? (size_t)n * 21 * 8 : 0,
+          false, nullptr};
+  Arg au{U, (size_t)n * 16, true, nullptr}, acv{conv, (size_t)n * 4, true, nullptr};
+  c->arena.used = 0;
+  rc = arena_reserve(c, qbytes + (size_t)n * (2 + 2 + 4 + 2 + 1 + 21 + 2 + 1) * 8 + 16384);
+  if (rc) return rc;
+  rc = stage(c, {&ac, &auo, &afo, &avd, &awl, &ahp, &au, &acv});
+  if (rc) return rc;
+  Sub1Args a;
+  a.fr = frame_of(c);
+  a.variant = variant;
+  a.n = n;
+  a.coords = (const double*)ac.dev;
+  a.UOld = (const double*)auo.dev;
+  a.FOld = (const double*)afo.dev;
+  a.vdual = (const double*)avd.dev;
+  a.winsize_list = (const int*)awl.dev;
+  a.winsize = winsize;
+  a.HPar = (const double*)ahp.dev;
+  a.mu = mu;
+  a.tol = tol;
+  a.U = (double*)au.dev;
+  a.conv = (int*)acv.dev;
+  a.queue = (int*)arena_take(c, qbytes);
+  a.qcount = c->qcount;
+  return finish(c, launch_subpb1(a, wmx, wmy, c->stream));
+}
+
+int aldic_triangulate(aldic_ctx* c, int64_t n, const double* pairs, const double* KL, const double* KR,
+                      const double* R, const double* T, double* xyz, double* reproj_err) {
+  if (!c) return ALDIC_ERR_ARG;
+  if (n < 0) return fail(c, ALDIC_ERR_ARG, "n < 0");
+  if (n == 0) return ALDIC_OK;
+  if (!pairs || !KL || !KR || !R || !T || !xyz) return fail(c, ALDIC_ERR_ARG, "missing array argument");
+  // camera matrices (small, always read on the host): MATLAB column-major 3x3 inputs
+  double kl[9], kr[9], r[9], tt[3];
+  const double* srcs[4] = {KL, KR, R, T};
+  double* dsts[4] = {kl, kr, r, tt};
+  const int cnts[4] = {9, 9, 9, 3};
+  for (int i = 0; i < 4; ++i) {
+    if (is_device_ptr(srcs[i])) {
+      CK(cudaMemcpy(dsts[i], srcs[i], cnts[i] * 8, cudaMemcpyDeviceToHost));
+    } else {
+      std::memcpy(dsts[i], srcs[i], cnts[i] * 8);
+    }
+  }
+  double P[24];  // PL (3x4 row-major) then PR
+  for (int row = 0; row < 3; ++row)
+    for (int col = 0; col < 4; ++col) {
+      // PL = KL [I | 0]
+      P[row * 4 + col] = col < 3 ? kl[row + 3 * col] : 0.0;
+      // PR = KR [R | T]
+      double s = 0;
+      for (int k = 0; k < 3; ++k) s += kr[row + 3 * k] * (col < 3 ? r[k + 3 * col] : tt[k]);
+      P[12 + row * 4 + col] = s;
+    }
+  Arg ap{pairs, (size_t)n * 32, false, nullptr}, ax{xyz, (size_t)n * 24, true, nullptr};
+  Arg ae{reproj_err, reproj_err ? (size_t)n * 8 : 0, true, nullptr};
+  Arg aP{P, sizeof(P), false, nullptr};
+  int rc = stage(c, {&ap, &ax, &ae, &aP});
+  if (rc) return rc;
+  const double* Pd = (const double*)aP.dev;
+  return finish(c, launch_triangulate(n, (const double*)ap.dev, Pd, Pd + 12, (double*)ax.dev, (double*)ae.dev,
+                                      c->stream));
+}
+
+}  // extern "C"

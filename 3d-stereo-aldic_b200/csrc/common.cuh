@@ -1,0 +1,211 @@
+// Shared device helpers for the ALDIC B200 kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define ALDIC_NAN __longlong_as_double(0x7ff8000000000000LL)
+
+namespace aldic {
+
+// ---------------------------------------------------------------------------------
+// Local 4x4 B-spline stencil of ba_interp2_spline.cpp:235-331 in separable form.
+// The reference evaluates A = BC*Q*BC^T and sum a_ij tr^i tc^j; since the stencil is the
+// outer product of one cubic basis per axis, the same value is
+//   sum_r w_r(tr) * sum_c w_c(tc) * Q[r][c]
+// with w(t) = [(-33t + 57t^2 - 24t^3), (56 - 3t - 117t^2 + 64t^3),
+//              (45t + 75t^2 - 64t^3),  (-9t - 15t^2 + 24t^3)] / 56,
+// the rows of BC = B*C (B the cubic B-spline basis, C the truncated prefilter inverse
+// [71 -19 5 -1; ...]/56).  The weights sum to 1 and w(0) = [0 1 0 0].
+// ---------------------------------------------------------------------------------
+__device__ __forceinline__ void bspline_weights(float t, float w[4]) {
+  const float k = 1.0f / 56.0f;
+  w[0] = k * (t * fmaf(t, fmaf(t, -24.0f, 57.0f), -33.0f));
+  w[1] = k * fmaf(t, fmaf(t, fmaf(t, 64.0f, -117.0f), -3.0f), 56.0f);
+  w[2] = k * (t * fmaf(t, fmaf(t, -64.0f, 75.0f), 45.0f));
+  w[3] = k * (t * fmaf(t, fmaf(t, 24.0f, -15.0f), -9.0f));
+}
+
+// Interpolate the column-major M-row image `img` with tap 0 at 0-based (r0, c0), all 16
+// taps in bounds, fractions tr (dim 1) and tc (dim 2).
+__device__ __forceinline__ float stencil16(const float* __restrict__ img, int M, int r0, int c0, float tr, float tc) {
+  float wr[4], wc[4];
+  bspline_weights(tr, wr);
+  bspline_weights(tc, wc);
+  const float* p = img + (size_t)r0 + (size_t)c0 * M;
+  float acc = 0.f;
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    const float* q = p + (size_t)c * M;
+    float col = wr[0] * __ldg(q);
+    col = fmaf(wr[1], __ldg(q + 1), col);
+    col = fmaf(wr[2], __ldg(q + 2), col);
+    col = fmaf(wr[3], __ldg(q + 3), col);
+    acc = fmaf(wc[c], col, acc);
+  }
+  return acc;
+}
+
+// Clamped version for arbitrary points (the MEX clamps taps to the image edge,
+// ba_interp2_spline.cpp:60-66).
+__device__ __forceinline__ float stencil16_clamped(const float* __restrict__ img, int M, int N, int r0, int c0, float tr,
+                                                   float tc) {
+  float wr[4], wc[4];
+  bspline_weights(tr, wr);
+  bspline_weights(tc, wc);
+  float acc = 0.f;
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    const int cc = min(max(c0 + c, 0), N - 1);
+    float col = 0.f;
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const int rr = min(max(r0 + r, 0), M - 1);
+      col = fmaf(wr[r], __ldg(img + (size_t)rr + (size_t)cc * M), col);
+    }
+    acc = fmaf(wc[c], col, acc);
+  }
+  return acc;
+}
+
+// ---------------------------------------------------------------------------------
+// Reductions
+// ---------------------------------------------------------------------------------
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Block-wide sums of K doubles per thread; result in out[0..K) (shared), visible to all
+// threads after return.  scratch must hold (NT/32)*K doubles.
+template <int K, int NT>
+__device__ __forceinline__ void block_sum(double (&v)[K], double* scratch, double* out) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const double s = warp_sum(v[k]);
+    if (lane == 0) scratch[warp * K + k] = s;
+  }
+  __syncthreads();
+  if (threadIdx.x < K) {
+    double s = 0;
+#pragma unroll
+    for (int w = 0; w < NT / 32; ++w) s += scratch[w * K + threadIdx.x];
+    out[threadIdx.x] = s;
+  }
+  __syncthreads();
+}
+
+// ---------------------------------------------------------------------------------
+// bwselect: connected component of `on` pixels (rows x cols, column-major, u8) that
+// contains the 0-based seed (sr, sc), 4- or 8-connected, into `lab` (u8).  Iterated
+// in-place propagation until no pixel changes; bounded by rows*cols sweeps (every
+// productive sweep adds at least one pixel).  All threads of the block must call it.
+// ---------------------------------------------------------------------------------
+__device__ inline void flood_select(const uint8_t* on, uint8_t* lab, int rows, int cols, int sr, int sc, int conn,
+                             int* flag) {
+  const int npx = rows * cols;
+  for (int p = threadIdx.x; p < npx; p += blockDim.x) lab[p] = 0;
+  __syncthreads();
+  const bool seed_ok = sr >= 0 && sr < rows && sc >= 0 && sc < cols && on[sr + sc * rows];
+  if (!seed_ok) {
+    __syncthreads();
+    return;
+  }
+  if (threadIdx.x == 0) lab[sr + sc * rows] = 1;
+  __syncthreads();
+  for (int sweep = 0; sweep < npx; ++sweep) {
+    int changed = 0;
+    for (int p = threadIdx.x; p < npx; p += blockDim.x) {
+      if (lab[p] || !on[p]) continue;
+      const int r = p % rows, c = p / rows;
+      bool hit = false;
+      if (r > 0 && lab[p - 1]) hit = true;
+      if (r + 1 < rows && lab[p + 1]) hit = true;
+      if (c > 0 && lab[p - rows]) hit = true;
+      if (c + 1 < cols && lab[p + rows]) hit = true;
+      if (!hit && conn == 8) {
+        if (r > 0 && c > 0 && lab[p - 1 - rows]) hit = true;
+        if (r + 1 < rows && c > 0 && lab[p + 1 - rows]) hit = true;
+        if (r > 0 && c + 1 < cols && lab[p - 1 + rows]) hit = true;
+        if (r + 1 < rows && c + 1 < cols && lab[p + 1 + rows]) hit = true;
+      }
+      if (hit) {
+        lab[p] = 1;
+        changed = 1;
+      }
+    }
+    if (!__syncthreads_or(changed)) break;
+  }
+  (void)flag;
+}
+
+// MATLAB round(): half away from zero.
+__device__ __forceinline__ double mround(double x) { return round(x); }
+
+// Inverse-compositional update P <- P o dP^-1 (func/funICGN.m:289-307).  Returns false
+// when det(dP) == 0.
+__device__ __forceinline__ bool compose_inverse(double P[6], const double d[6]) {
+  const double det = (1 + d[0]) * (1 + d[3]) - d[1] * d[2];
+  if (!(det != 0)) return false;
+  const double t1 = (-d[0] - d[0] * d[3] + d[1] * d[2]) / det;
+  const double t2 = -d[1] / det;
+  const double t3 = -d[2] / det;
+  const double t4 = (-d[3] - d[0] * d[3] + d[1] * d[2]) / det;
+  const double t5 = (-d[4] - d[3] * d[4] + d[2] * d[5]) / det;
+  const double t6 = (-d[5] - d[0] * d[5] + d[1] * d[4]) / det;
+  const double a00 = 1 + P[0], a01 = P[2], a02 = P[4];
+  const double a10 = P[1], a11 = 1 + P[3], a12 = P[5];
+  const double n00 = a00 * (1 + t1) + a01 * t2;
+  const double n10 = a10 * (1 + t1) + a11 * t2;
+  const double n01 = a00 * t3 + a01 * (1 + t4);
+  const double n11 = a10 * t3 + a11 * (1 + t4);
+  const double n02 = a00 * t5 + a01 * t6 + a02;
+  const double n12 = a10 * t5 + a11 * t6 + a12;
+  P[0] = n00 - 1;
+  P[1] = n10;
+  P[2] = n01;
+  P[3] = n11 - 1;
+  P[4] = n02;
+  P[5] = n12;
+  return true;
+}
+
+// x = A^-1 b for an n x n (n <= 6) column-major system, Gaussian elimination with
+// partial pivoting in FP64 (mldivide's general path; a zero pivot yields Inf/NaN).
+__device__ inline void solve_small(int n, const double* Ain, const double* bin, double* x) {
+  double A[36], b[6];
+  for (int i = 0; i < n * n; ++i) A[i] = Ain[i];
+  for (int i = 0; i < n; ++i) b[i] = bin[i];
+  for (int k = 0; k < n; ++k) {
+    int piv = k;
+    double best = fabs(A[k + k * n]);
+    for (int i = k + 1; i < n; ++i)
+      if (fabs(A[i + k * n]) > best) {
+        best = fabs(A[i + k * n]);
+        piv = i;
+      }
+    if (piv != k) {
+      for (int j = 0; j < n; ++j) {
+        const double t = A[k + j * n];
+        A[k + j * n] = A[piv + j * n];
+        A[piv + j * n] = t;
+      }
+      const double t = b[k];
+      b[k] = b[piv];
+      b[piv] = t;
+    }
+    for (int i = k + 1; i < n; ++i) {
+      const double l = A[i + k * n] / A[k + k * n];
+      for (int j = k; j < n; ++j) A[i + j * n] -= l * A[k + j * n];
+      b[i] -= l * b[k];
+    }
+  }
+  for (int i = n - 1; i >= 0; --i) {
+    double s = b[i];
+    for (int j = i + 1; j < n; ++j) s -= A[i + j * n] * x[j];
+    x[i] = s / A[i + i * n];
+  }
+}
+
+}  // namespace aldic

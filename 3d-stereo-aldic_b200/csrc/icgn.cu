@@ -1,0 +1,1029 @@
+// Batched local IC-GN (6-DOF, first-order shape function) and the ALDIC Subpb1
+// augmented-Lagrangian local step on the B200.
+//
+// Structure of one batched call (all subsets of one frame):
+//   1. classify kernel, one warp per subset: coordinate rounding, window bounds, the
+//      zero-count rules of the reference (funICGN.m:57-68, funICGNQuadtree.m:61-79,
+//      funICGN_Subpb1quadtree.m:68-89), final window size.  Subsets that end here
+//      (solver error -> -1, too much masked -> 102) are written out; the others are
+//      appended to one of two work queues: nominal window size, or enlarged window.
+//   2. solve kernel per queue, persistent (grid = resident CTAs), one CTA of NT threads
+//      per subset.  The subset's f, f_x, f_y live in shared memory for the whole solve;
+//      each Gauss-Newton iteration interpolates g with the local 4x4 B-spline stencil
+//      (FP32), accumulates the b-vector statistics in one pass (FP32 per thread, FP64
+//      across threads), and thread 0 does the FP64 6x6 update and inverse composition.
+//      Masked (quadtree) subsets additionally run the bwselect flood fills in shared
+//      memory.
+//
+// The single-pass b-vector: with fn = (f - mean_f)/bf the reference's
+//   b_k = bf * sum_p J_k(p) [fn(p) - (g(p) - mean_g)/bg]
+// equals bf * (A_k - (C_k - mean_g * B_k) / bg) with A_k = sum J_k fn, B_k = sum J_k
+// (constant per subset) and C_k = sum J_k g (per iteration); mean_g and bg come from
+// sum g, sum g^2 over the same pass.
+#include "common.cuh"
+#include "kernels.h"
+
+namespace aldic {
+
+constexpr int kNT = 128;  // threads per solve CTA
+
+struct SolveCtl {
+  double P[6];
+  double Hinv[36];
+  double H[21];
+  double A[6], B[6];
+  double meanf, bf, sabsf;
+  double normNew, normAbs, normInit;
+  double gsum_prev;
+  double znssd;
+  float pf[4], f5, f6;
+  int base_r, base_c;  // 0-based tap-0 row/col offsets: x0 + n5 - 2, y0 + n6 - 2
+  int step, go, status, need_mask, fbw8_ready, done_error;
+};
+
+__device__ __forceinline__ bool is_intd(double v) { return floor(v) == v && fabs(v) < 1e9; }
+
+// Window [x0 - wx/2, x0 + wx/2] x [y0 - wy/2, y0 + wy/2] (1-based) inside the image and,
+// if need_grad, inside the gradient arrays shifted by crop.
+__device__ __forceinline__ bool window_ok(const FrameDev& fr, double x0, double y0, double wx, double wy, bool need_grad,
+                                          int crop) {
+  const double r0 = x0 - wx / 2, r1 = x0 + wx / 2, c0 = y0 - wy / 2, c1 = y0 + wy / 2;
+  if (!is_intd(r0) || !is_intd(r1) || !is_intd(c0) || !is_intd(c1)) return false;
+  if (r0 < 1 || r1 > fr.M || c0 < 1 || c1 > fr.N) return false;
+  if (need_grad) {
+    if (r0 - crop < 1 || r1 - crop > fr.M - 6 || c0 - crop < 1 || c1 - crop > fr.N - 6) return false;
+  }
+  return true;
+}
+
+// Any corner of the warped window outside [3, M-2] x [3, N-2] (func/funICGN.m:121-124);
+// the warp is affine so the extremes are at the corners.  Non-finite -> outside.
+__device__ __forceinline__ bool warped_oob(const FrameDev& fr, const double P[6], double x0, double y0, double hx,
+                                           double hy) {
+  bool oob = false;
+  for (int cx = -1; cx <= 1; cx += 2)
+    for (int cy = -1; cy <= 1; cy += 2) {
+      const double dx = cx * hx, dy = cy * hy;
+      const double u = (1 + P[0]) * dx + P[2] * dy + (x0 + P[4]);
+      const double v = P[1] * dx + (1 + P[3]) * dy + (y0 + P[5]);
+      if (!(u >= 3 && u <= fr.M - 2 && v >= 3 && v <= fr.N - 2)) oob = true;
+    }
+  return oob;
+}
+
+// Per-iteration FP32 warp coefficients: u22 - (x0 + n5) = dx + P1 dx + P3 dy + f5 with
+// n5 = round(P5), f5 = P5 - n5, so the coordinate keeps full FP32 precision relative to
+// the subset centre.
+__device__ __forceinline__ void prep_coeffs(SolveCtl& c, double x0, double y0) {
+  const double n5 = mround(c.P[4]), n6 = mround(c.P[5]);
+  c.pf[0] = (float)c.P[0];
+  c.pf[1] = (float)c.P[1];
+  c.pf[2] = (float)c.P[2];
+  c.pf[3] = (float)c.P[3];
+  c.f5 = (float)(c.P[4] - n5);
+  c.f6 = (float)(c.P[5] - n6);
+  c.base_r = (int)(x0 + n5) - 2;
+  c.base_c = (int)(y0 + n6) - 2;
+}
+
+// Interpolate g at window pixel (dx, dy) with the current coefficients.
+__device__ __forceinline__ float warp_g(const FrameDev& fr, const SolveCtl& c, float dx, float dy) {
+  const float lx = dx + fmaf(c.pf[0], dx, fmaf(c.pf[2], dy, c.f5));
+  const float ly = dy + fmaf(c.pf[3], dy, fmaf(c.pf[1], dx, c.f6));
+  const float ix = floorf(lx), iy = floorf(ly);
+  return stencil16(fr.def, fr.M, c.base_r + (int)ix, c.base_c + (int)iy, lx - ix, ly - iy);
+}
+
+// Gauss-Jordan inverse of a 6x6 (column-major) with partial pivoting, FP64.
+__device__ void invert6(const double* Hin, double* Hinv) {
+  double A[36], I[36];
+  for (int k = 0; k < 36; ++k) {
+    A[k] = Hin[k];
+    I[k] = (k % 7 == 0) ? 1.0 : 0.0;
+  }
+  for (int k = 0; k < 6; ++k) {
+    int piv = k;
+    double best = fabs(A[k + 6 * k]);
+    for (int i = k + 1; i < 6; ++i)
+      if (fabs(A[i + 6 * k]) > best) {
+        best = fabs(A[i + 6 * k]);
+        piv = i;
+      }
+    if (piv != k)
+      for (int j = 0; j < 6; ++j) {
+        double t = A[k + 6 * j];
+        A[k + 6 * j] = A[piv + 6 * j];
+        A[piv + 6 * j] = t;
+        t = I[k + 6 * j];
+        I[k + 6 * j] = I[piv + 6 * j];
+        I[piv + 6 * j] = t;
+      }
+    const double d = A[k + 6 * k];
+    for (int j = 0; j < 6; ++j) {
+      A[k + 6 * j] /= d;
+      I[k + 6 * j] /= d;
+    }
+    for (int i = 0; i < 6; ++i) {
+      if (i == k) continue;
+      const double l = A[i + 6 * k];
+      for (int j = 0; j < 6; ++j) {
+        A[i + 6 * j] -= l * A[k + 6 * j];
+        I[i + 6 * j] -= l * I[k + 6 * j];
+      }
+    }
+  }
+  for (int k = 0; k < 36; ++k) Hinv[k] = I[k];
+}
+
+// ================================================================================
+// classify kernel (one warp per subset)
+// ================================================================================
+__global__ void icgn_classify_kernel(IcgnArgs a) {
+  const long long t = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (t >= a.n) return;
+  const FrameDev& fr = a.fr;
+  double x0 = a.coords[t], y0 = a.coords[a.n + t];
+  const bool quad = (a.variant == 1);
+  if (quad) {
+    x0 = mround(x0);
+    y0 = mround(y0);
+  }
+  const double w = a.winsize;
+  const double Nw = (w + 1) * (w + 1);
+  int status = 0;  // 0 active, -1 error, 102 masked-out
+  double wfin = w;
+  uint8_t mark = 0;
+  // zero counts over the nominal window
+  const bool img_ok = window_ok(fr, x0, y0, w, w, false, a.crop);
+  const bool grad_ok = img_ok && window_ok(fr, x0, y0, w, w, true, a.crop);
+  long long cnt = 0;
+  if (img_ok) {
+    const int W1 = (int)w + 1;
+    const int r0 = (int)(x0 - w / 2) - 1, c0 = (int)(y0 - w / 2) - 1;
+    for (int p = lane; p < W1 * W1; p += 32) {
+      const int aa = p % W1, bb = p / W1;
+      const size_t k = (size_t)(r0 + aa) + (size_t)(c0 + bb) * fr.M;
+      if (quad) {
+        const float f = fr.ref[k];
+        const bool mk = fr.mask ? (fr.mask[k] != 0) : true;
+        cnt += (!mk || f == 0.f);
+      } else if (grad_ok) {
+        const size_t kg = (size_t)(r0 + aa - a.crop) + (size_t)(c0 + bb - a.crop) * (fr.M - 6);
+        cnt += (fr.gx[kg] == 0.f);
+      }
+    }
+    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+  }
+  if (quad) mark = (!img_ok || cnt > 0.6 * Nw) ? 1 : 0;
+  if (!grad_ok) {
+    status = -1;
+  } else if (quad) {
+    if (cnt < 0.4 * Nw) {
+      if (cnt > 0) {
+        wfin = 2 * ceil(sqrt(Nw / (Nw - (double)cnt)) * w / 2);
+        if (!window_ok(fr, x0, y0, wfin, wfin, true, a.crop)) status = -1;
+      }
+    } else {
+      status = 102;
+    }
+  } else {
+    if (cnt < 0.5 * Nw) {
+      if (cnt > 0.1 * Nw) {
+        wfin = mround(1.4142135623730951 * w);
+        if (!window_ok(fr, x0, y0, wfin, wfin, true, a.crop)) status = -1;
+      }
+    } else {
+      status = 102;
+    }
+  }
+  if (lane != 0) return;
+  if (quad && a.mark) a.mark[t] = mark;
+  if (status == 0) {
+    const int bucket = (wfin == w) ? 0 : 1;
+    const int pos = atomicAdd(&a.qcount[bucket], 1);
+    int* q = a.queue + 3 * ((long long)bucket * a.n + pos);
+    q[0] = (int)t;
+    q[1] = (int)wfin;
+    q[2] = (quad && cnt > 0) ? 1 : 0;
+    return;
+  }
+  // finished here
+  if (a.variant == 2) {
+    a.znssd[t] = ALDIC_NAN;
+    if (a.conv) a.conv[t] = status;
+    return;
+  }
+  a.conv[t] = status;
+  if (status == -1) {
+    a.U[2 * t] = ALDIC_NAN;
+    a.U[2 * t + 1] = ALDIC_NAN;
+    for (int k = 0; k < 4; ++k) a.F[4 * t + k] = ALDIC_NAN;
+  } else {  // 102: U = U0, F = 0
+    a.U[2 * t] = a.U0[2 * t];
+    a.U[2 * t + 1] = a.U0[2 * t + 1];
+    for (int k = 0; k < 4; ++k) a.F[4 * t + k] = 0.0;
+  }
+  if (a.H)
+    for (int k = 0; k < 21; ++k) a.H[t + a.n * k] = 0.0;
+}
+
+// ================================================================================
+// 6-DOF solve kernel
+// ================================================================================
+struct SolveSmem {
+  float* f;
+  float* gx;
+  float* gy;
+  float* g;
+  uint8_t* on;    // f-mask pixel on (quadtree)
+  uint8_t* lab;   // flood-fill output (bw4, then per-iteration g region)
+  uint8_t* tmp;   // flood-fill input
+  uint8_t* fbw8;  // 8-connected f-mask region (g-mask fallback)
+};
+
+__device__ __forceinline__ SolveSmem carve(unsigned char* base, int npx) {
+  SolveSmem s;
+  s.f = reinterpret_cast<float*>(base);
+  s.gx = s.f + npx;
+  s.gy = s.gx + npx;
+  s.g = s.gy + npx;
+  uint8_t* u = reinterpret_cast<uint8_t*>(s.g + npx);
+  s.on = u;
+  s.lab = u + npx;
+  s.tmp = u + 2 * npx;
+  s.fbw8 = u + 3 * npx;
+  return s;
+}
+
+__global__ void __launch_bounds__(kNT) icgn_solve_kernel(IcgnArgs a, int bucket) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ SolveCtl c;
+  __shared__ double red[(kNT / 32) * 40];
+  __shared__ double sums[40];
+  const int tid = threadIdx.x;
+  const FrameDev& fr = a.fr;
+  const bool quad = (a.variant == 1);
+  const bool epi = (a.variant == 2);
+  const int count = a.qcount[bucket];
+  const int gM = fr.M - 6;
+  for (int qi = blockIdx.x; qi < count; qi += gridDim.x) {
+    const int* q = a.queue + 3 * ((long long)bucket * a.n + qi);
+    const long long t = q[0];
+    const int w = q[1];
+    const bool masked = q[2] != 0;
+    const int W1 = w + 1, npx = W1 * W1;
+    const int half = w / 2;
+    double x0 = a.coords[t], y0 = a.coords[a.n + t];
+    if (quad) {
+      x0 = mround(x0);
+      y0 = mround(y0);
+    }
+    const int seed = (int)floor((w + 1) / 2.0) - 1;
+    SolveSmem s = carve(smem_raw, npx);
+    // ---- load the subset window ----
+    {
+      const int r0 = (int)x0 - half - 1, c0 = (int)y0 - half - 1;
+      for (int p = tid; p < npx; p += kNT) {
+        const int aa = p % W1, bb = p / W1;
+        const size_t k = (size_t)(r0 + aa) + (size_t)(c0 + bb) * fr.M;
+        const size_t kg = (size_t)(r0 + aa - a.crop) + (size_t)(c0 + bb - a.crop) * gM;
+        float f = fr.ref[k];
+        uint8_t on = 1;
+        if (quad && fr.mask) {
+          on = fr.mask[k] != 0;
+          if (!on) f = 0.f;
+        }
+        s.f[p] = f;
+        s.gx[p] = fr.gx[kg];
+        s.gy[p] = fr.gy[kg];
+        s.on[p] = on;
+      }
+    }
+    __syncthreads();
+    if (masked) {
+      // bwselect(logical(mask), seed, seed, 4) restricts f, fx, fy (funICGNQuadtree.m:83-88)
+      flood_select(s.on, s.lab, W1, W1, seed, seed, 4, nullptr);
+      for (int p = tid; p < npx; p += kNT)
+        if (!s.lab[p]) {
+          s.f[p] = 0.f;
+          s.gx[p] = 0.f;
+          s.gy[p] = 0.f;
+        }
+      __syncthreads();
+    }
+    // ---- setup sums: H (21), sum J f (6), sum J (6), f stats (3), sum |f| (1) ----
+    {
+      float h[21], jf[6], jb[6], fs = 0.f, fs2 = 0.f, fn = 0.f, fab = 0.f;
+#pragma unroll
+      for (int k = 0; k < 21; ++k) h[k] = 0.f;
+#pragma unroll
+      for (int k = 0; k < 6; ++k) {
+        jf[k] = 0.f;
+        jb[k] = 0.f;
+      }
+      for (int p = tid; p < npx; p += kNT) {
+        const float dx = (float)(p % W1 - half), dy = (float)(p / W1 - half);
+        const float gxv = s.gx[p], gyv = s.gy[p], f = s.f[p];
+        const float J[6] = {gxv * dx, gyv * dx, gxv * dy, gyv * dy, gxv, gyv};
+        int k = 0;
+#pragma unroll
+        for (int i = 0; i < 6; ++i)
+#pragma unroll
+          for (int j = i; j < 6; ++j) h[k++] = fmaf(J[i], J[j], h[k]);
+#pragma unroll
+        for (int i = 0; i < 6; ++i) {
+          jf[i] = fmaf(J[i], f, jf[i]);
+          jb[i] += J[i];
+        }
+        const bool sel = quad ? (fabsf(f) > 1e-10f) : true;
+        if (sel) {
+          fs += f;
+          fs2 = fmaf(f, f, fs2);
+          fn += 1.f;
+        }
+        fab += fabsf(f);
+      }
+      double v[37];
+#pragma unroll
+      for (int k = 0; k < 21; ++k) v[k] = h[k];
+#pragma unroll
+      for (int k = 0; k < 6; ++k) {
+        v[21 + k] = jf[k];
+        v[27 + k] = jb[k];
+      }
+      v[33] = fs;
+      v[34] = fs2;
+      v[35] = fn;
+      v[36] = fab;
+      block_sum<37, kNT>(v, red, sums);
+    }
+    if (tid == 0) {
+      double H[36];
+      int k = 0;
+      for (int i = 0; i < 6; ++i)
+        for (int j = i; j < 6; ++j) {
+          H[i + 6 * j] = sums[k];
+          H[j + 6 * i] = sums[k];
+          ++k;
+        }
+      // packed lower triangle by columns == upper triangle by rows
+      k = 0;
+      for (int col = 0; col < 6; ++col)
+        for (int row = col; row < 6; ++row) c.H[k++] = H[row + 6 * col];
+      invert6(H, c.Hinv);
+      const double n = sums[35];
+      if (n > 0) {
+        c.meanf = sums[33] / n;
+        c.bf = sqrt(fmax(sums[34] - sums[33] * sums[33] / n, 0.0));
+      } else {
+        c.meanf = ALDIC_NAN;
+        c.bf = ALDIC_NAN;
+      }
+      for (int i = 0; i < 6; ++i) {
+        c.B[i] = sums[27 + i];
+        c.A[i] = (sums[21 + i] - c.meanf * c.B[i]) / c.bf;
+      }
+      c.sabsf = sums[36];
+      c.P[0] = c.P[1] = c.P[2] = c.P[3] = 0.0;
+      if (epi) {
+        c.P[4] = 0.0;
+        c.P[5] = 0.0;
+      } else {
+        c.P[4] = a.U0[2 * t];
+        c.P[5] = a.U0[2 * t + 1];
+      }
+      c.normNew = 1.0;
+      c.normAbs = 1.0;
+      c.normInit = 0.0;
+      c.step = 0;
+      c.status = 0;
+      c.fbw8_ready = 0;
+      c.done_error = 0;
+      c.gsum_prev = 0.0;
+      c.znssd = ALDIC_NAN;
+    }
+    __syncthreads();
+    // ---- Gauss-Newton iterations ----
+    const int q_nt = kNT / W1, r_nt = kNT % W1;
+    while (true) {
+      if (tid == 0) {
+        int go = (c.step <= a.max_iter && c.normNew > a.tol && c.normAbs > a.tol) ? 1 : 0;
+        if (go) {
+          c.step += 1;
+          if (quad && masked && c.step > 1) {
+            // funICGNQuadtree.m:139-145 re-derives the subset size without re-slicing f
+            const double w0 = a.winsize;
+            const double wn = 2 * ceil(sqrt((w0 + 1) * (w0 + 1) / c.gsum_prev) * w / 2);
+            if (wn != (double)w) {
+              if (!window_ok(fr, x0, y0, wn, wn, false, a.crop)) {
+                c.done_error = 1;
+              } else if (warped_oob(fr, c.P, x0, y0, wn / 2, wn / 2)) {
+                c.normNew = 1e6;
+              } else {
+                c.done_error = 1;  // array size mismatch in the reference
+              }
+              go = 0;
+            }
+          }
+          if (go && warped_oob(fr, c.P, x0, y0, half, half)) {
+            c.normNew = 1e6;
+            go = 0;
+          }
+          if (go) prep_coeffs(c, x0, y0);
+        }
+        c.go = go;
+      }
+      __syncthreads();
+      if (!c.go) break;
+      // pass 1: interpolate, single-pass sums
+      float C[6] = {0, 0, 0, 0, 0, 0}, S1 = 0.f, S2 = 0.f, ns = 0.f, nz = 0.f, fg = 0.f;
+      {
+        int aa = tid % W1, bb = tid / W1;
+        for (int p = tid; p < npx; p += kNT) {
+          const float dx = (float)(aa - half), dy = (float)(bb - half);
+          const float g = warp_g(fr, c, dx, dy);
+          s.g[p] = g;
+          const float ag = s.gx[p] * g, bg = s.gy[p] * g;
+          C[0] = fmaf(ag, dx, C[0]);
+          C[1] = fmaf(bg, dx, C[1]);
+          C[2] = fmaf(ag, dy, C[2]);
+          C[3] = fmaf(bg, dy, C[3]);
+          C[4] += ag;
+          C[5] += bg;
+          const bool sel = quad ? (fabsf(g) > 1e-10f) : true;
+          if (sel) {
+            S1 += g;
+            S2 = fmaf(g, g, S2);
+            ns += 1.f;
+          }
+          nz += (g == 0.f) ? 1.f : 0.f;
+          if (epi) fg = fmaf(s.f[p], g, fg);
+          aa += r_nt;
+          bb += q_nt;
+          if (aa >= W1) {
+            aa -= W1;
+            bb += 1;
+          }
+        }
+      }
+      double v[11] = {C[0], C[1], C[2], C[3], C[4], C[5], S1, S2, ns, nz, fg};
+      block_sum<11, kNT>(v, red, sums);
+      const bool run_mask = quad && (masked || sums[9] > 0);
+      if (run_mask) {
+        // g region: bwselect(logical(g), seed, seed, 8); if it covers the window, the
+        // 8-connected f-mask region instead (funICGNQuadtree.m:170-182)
+        for (int p = tid; p < npx; p += kNT) s.tmp[p] = (s.g[p] != 0.f);
+        __syncthreads();
+        flood_select(s.tmp, s.lab, W1, W1, seed, seed, 8, nullptr);
+        int allon = 1;
+        for (int p = tid; p < npx; p += kNT) allon &= s.lab[p];
+        allon = __syncthreads_and(allon);
+        const uint8_t* gm = s.lab;
+        if (allon) {
+          if (!c.fbw8_ready) {
+            flood_select(s.on, s.fbw8, W1, W1, seed, seed, 8, nullptr);
+            if (tid == 0) c.fbw8_ready = 1;
+          }
+          gm = s.fbw8;
+        }
+        __syncthreads();
+        float C2[6] = {0, 0, 0, 0, 0, 0}, T1 = 0.f, T2 = 0.f, tn = 0.f, gs = 0.f;
+        for (int p = tid; p < npx; p += kNT) {
+          const float dx = (float)(p % W1 - half), dy = (float)(p / W1 - half);
+          const float g = gm[p] ? s.g[p] : 0.f;
+          const float ag = s.gx[p] * g, bg = s.gy[p] * g;
+          C2[0] = fmaf(ag, dx, C2[0]);
+          C2[1] = fmaf(bg, dx, C2[1]);
+          C2[2] = fmaf(ag, dy, C2[2]);
+          C2[3] = fmaf(bg, dy, C2[3]);
+          C2[4] += ag;
+          C2[5] += bg;
+          if (fabsf(g) > 1e-10f) {
+            T1 += g;
+            T2 = fmaf(g, g, T2);
+            tn += 1.f;
+          }
+          gs += gm[p] ? 1.f : 0.f;
+        }
+        double v2[10] = {C2[0], C2[1], C2[2], C2[3], C2[4], C2[5], T1, T2, tn, gs};
+        block_sum<10, kNT>(v2, red, sums);
+        if (tid == 0) c.gsum_prev = sums[9];
+      }
+      if (tid == 0) {
+        const double n = sums[8];
+        double meang, bg;
+        if (n > 0) {
+          meang = sums[6] / n;
+          bg = sqrt(fmax(sums[7] - sums[6] * sums[6] / n, 0.0));
+        } else {
+          meang = ALDIC_NAN;
+          bg = ALDIC_NAN;
+        }
+        double b[6];
+        for (int i = 0; i < 6; ++i) b[i] = c.bf * (c.A[i] - (sums[i] - meang * c.B[i]) / bg);
+        if (epi) c.znssd = 2.0 - 2.0 * (sums[10] - c.meanf * sums[6]) / (c.bf * bg);
+        double nn = 0;
+        for (int i = 0; i < 6; ++i) nn += b[i] * b[i];
+        c.normNew = sqrt(nn);
+        c.normAbs = c.normNew;
+        if (c.step == 1) c.normInit = c.normNew;
+        if (c.normInit > a.tol) c.normNew = c.normNew / c.normInit;
+        else c.normNew = 0.0;
+        if (!(c.normNew < a.tol || c.normAbs < a.tol)) {
+          double dP[6];
+          for (int i = 0; i < 6; ++i) {
+            double acc = 0;
+            for (int j = 0; j < 6; ++j) acc += c.Hinv[i + 6 * j] * b[j];
+            dP[i] = -acc;
+          }
+          if (!compose_inverse(c.P, dP)) {
+            c.step = a.max_iter + 1000;  // leave the loop (det(dP) == 0)
+            c.status = 1;
+          } else if (epi) {
+            c.P[4] = 0.0;
+            c.P[5] = 0.0;
+          }
+        }
+      }
+      __syncthreads();
+    }
+    // ---- finalize ----
+    if (tid == 0) {
+      int step = c.step;
+      if (c.status == 1) step -= 1000;  // restore the count at the det == 0 break
+      if (!(c.normNew < a.tol || c.normAbs < a.tol)) step = a.max_iter + 1;
+      if (isnan(c.normNew)) step = a.max_iter + 1;
+      if (quad && c.sabsf < 1e-6) step = a.max_iter + 3;
+      if (epi) {
+        a.znssd[t] = c.done_error ? ALDIC_NAN : c.znssd;
+        if (a.conv) a.conv[t] = c.done_error ? -1 : step;
+      } else if (c.done_error) {
+        a.conv[t] = -1;
+        a.U[2 * t] = ALDIC_NAN;
+        a.U[2 * t + 1] = ALDIC_NAN;
+        for (int k = 0; k < 4; ++k) a.F[4 * t + k] = ALDIC_NAN;
+        if (a.H)
+          for (int k = 0; k < 21; ++k) a.H[t + a.n * k] = 0.0;
+      } else {
+        a.conv[t] = step;
+        a.U[2 * t] = c.P[4];
+        a.U[2 * t + 1] = c.P[5];
+        for (int k = 0; k < 4; ++k) a.F[4 * t + k] = c.P[k];
+        if (a.H)
+          for (int k = 0; k < 21; ++k) a.H[t + a.n * k] = c.H[k];
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ================================================================================
+// Subpb1: classify + solve
+// ================================================================================
+__global__ void subpb1_classify_kernel(Sub1Args a) {
+  const long long t = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (t >= a.n) return;
+  const FrameDev& fr = a.fr;
+  const bool quad = (a.variant == 1);
+  double x0 = a.coords[t], y0 = a.coords[a.n + t];
+  double wx, wy;
+  if (quad) {
+    x0 = mround(x0);
+    y0 = mround(y0);
+    wx = a.winsize_list[t];
+    wy = a.winsize_list[a.n + t];
+  } else {
+    wx = wy = a.winsize;
+  }
+  int status = 0;
+  const bool ok = window_ok(fr, x0, y0, wx, wy, true, 3);
+  long long cnt = 0;
+  if (ok) {
+    const int R = (int)wx + 1, Cc = (int)wy + 1;
+    const int r0 = (int)(x0 - wx / 2) - 1, c0 = (int)(y0 - wy / 2) - 1;
+    for (int p = lane; p < R * Cc; p += 32) {
+      const int aa = p % R, bb = p / R;
+      const size_t k = (size_t)(r0 + aa) + (size_t)(c0 + bb) * fr.M;
+      if (quad) {
+        const bool mk = fr.mask ? (fr.mask[k] != 0) : true;
+        cnt += (!mk || fr.ref[k] == 0.f);
+      } else {
+        cnt += (fr.gx[(size_t)(r0 + aa - 3) + (size_t)(c0 + bb - 3) * (fr.M - 6)] == 0.f);
+      }
+    }
+    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+  }
+  double wxf = wx, wyf = wy;
+  if (!ok) {
+    status = -1;
+  } else if (quad) {
+    const double Nw = (wx + 1) * (wy + 1);
+    if (cnt < 0.4 * Nw) {
+      if (cnt > 0) {
+        wxf = 2 * ceil(sqrt((wx + 1) * (wy + 1) / ((wx + 1) * (wy + 1) - (double)cnt)) * wx / 2);
+        wyf = 2 * ceil(sqrt((wxf + 1) * (wy + 1) / ((wxf + 1) * (wy + 1) - (double)cnt)) * wy / 2);
+        if (!window_ok(fr, x0, y0, wxf, wyf, true, 3)) status = -1;
+      }
+    } else {
+      status = 102;
+    }
+  } else {
+    const double Nw = (wx + 1) * (wx + 1);
+    if (cnt < 0.5 * Nw) {
+      if (cnt > 0.1 * Nw) {
+        wxf = wyf = mround(1.4142135623730951 * wx);
+        if (!window_ok(fr, x0, y0, wxf, wyf, true, 3)) status = -1;
+      }
+    } else {
+      status = 102;
+    }
+  }
+  if (lane != 0) return;
+  if (status == 0) {
+    const bool nominal = (wxf == a.winsize && wyf == a.winsize);
+    const int bucket = nominal ? 0 : 1;
+    const int pos = atomicAdd(&a.qcount[bucket], 1);
+    int* q = a.queue + 4 * ((long long)bucket * a.n + pos);
+    q[0] = (int)t;
+    q[1] = (int)wxf;
+    q[2] = (int)wyf;
+    q[3] = (quad && cnt > 0) ? 1 : 0;
+    return;
+  }
+  if (status == -1) {
+    a.conv[t] = quad ? 0 : -1;
+    a.U[2 * t] = ALDIC_NAN;
+    a.U[2 * t + 1] = ALDIC_NAN;
+  } else {
+    a.conv[t] = 102;
+    a.U[2 * t] = a.UOld[2 * t];
+    a.U[2 * t + 1] = a.UOld[2 * t + 1];
+  }
+}
+
+struct Sub1Ctl {
+  double P[6];
+  double H2[4];
+  double A[2], B[2];
+  double meanf, bf, sabsf;
+  double normNew, normAbs, normInit;
+  float pf[4], f5, f6;
+  int base_r, base_c;
+  int step, go, status, fbw8_ready;
+};
+
+// Shared-memory arrays of one Subpb1 subset: f (= ImgRef .* mask), fx, fy, g as floats;
+// on (mask pixel set), cur (the region that currently restricts f, fx, fy: bw4 after
+// set-up, the last g region after a masked iteration), tmp/glab (flood fill of g), fbw8.
+struct Sub1Smem {
+  float *f, *gx, *gy, *g;
+  uint8_t *on, *cur, *tmp, *glab, *fbw8;
+};
+
+__device__ __forceinline__ Sub1Smem carve_sub1(unsigned char* base, int npx) {
+  Sub1Smem s;
+  s.f = reinterpret_cast<float*>(base);
+  s.gx = s.f + npx;
+  s.gy = s.gx + npx;
+  s.g = s.gy + npx;
+  uint8_t* u = reinterpret_cast<uint8_t*>(s.g + npx);
+  s.on = u;
+  s.cur = u + npx;
+  s.tmp = u + 2 * npx;
+  s.glab = u + 3 * npx;
+  s.fbw8 = u + 4 * npx;
+  return s;
+}
+
+// Derive mean_f, bf, H2, A, B from f-side sums v = [H0 H1 H2 JF0 JF1 JB0 JB1 fs fs2 fn fab].
+__device__ __forceinline__ void sub1_fside(Sub1Ctl& c, const double* v, bool use_sum_h, const double* hstore,
+                                           double mu) {
+  const double n = v[9];
+  if (n > 0) {
+    c.meanf = v[7] / n;
+    c.bf = sqrt(fmax(v[8] - v[7] * v[7] / n, 0.0));
+  } else {
+    c.meanf = ALDIC_NAN;
+    c.bf = ALDIC_NAN;
+  }
+  const double h0 = use_sum_h ? v[0] : hstore[0];
+  const double h1 = use_sum_h ? v[1] : hstore[1];
+  const double h2 = use_sum_h ? v[2] : hstore[2];
+  const double s2 = 2.0 / (c.bf * c.bf);
+  c.H2[0] = h0 * s2 + mu;
+  c.H2[1] = h1 * s2;
+  c.H2[2] = h1 * s2;
+  c.H2[3] = h2 * s2 + mu;
+  for (int i = 0; i < 2; ++i) {
+    c.B[i] = v[5 + i];
+    c.A[i] = (v[3 + i] - c.meanf * c.B[i]) / c.bf;
+  }
+  c.sabsf = v[10];
+}
+
+__global__ void __launch_bounds__(kNT) subpb1_solve_kernel(Sub1Args a, int bucket) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ Sub1Ctl c;
+  __shared__ double red[(kNT / 32) * 16];
+  __shared__ double sums[16];
+  const int tid = threadIdx.x;
+  const FrameDev& fr = a.fr;
+  const bool quad = (a.variant == 1);
+  const int count = a.qcount[bucket];
+  const int gM = fr.M - 6;
+  for (int qi = blockIdx.x; qi < count; qi += gridDim.x) {
+    const int* q = a.queue + 4 * ((long long)bucket * a.n + qi);
+    const long long t = q[0];
+    const int wx = q[1], wy = q[2];
+    const bool masked = q[3] != 0;
+    const int R = wx + 1, Cc = wy + 1, npx = R * Cc;
+    const int hx = wx / 2, hy = wy / 2;
+    double x0 = a.coords[t], y0 = a.coords[a.n + t];
+    if (quad) {
+      x0 = mround(x0);
+      y0 = mround(y0);
+    }
+    // bwselect(BW, c, r): column seed from winsize_x, row seed from winsize_y
+    // (funICGN_Subpb1quadtree.m:93)
+    const int sc = (int)floor((wx + 1) / 2.0) - 1;
+    const int sr = (int)floor((wy + 1) / 2.0) - 1;
+    Sub1Smem s = carve_sub1(smem_raw, npx);
+    {
+      const int r0 = (int)x0 - hx - 1, c0 = (int)y0 - hy - 1;
+      for (int p = tid; p < npx; p += kNT) {
+        const int aa = p % R, bb = p / R;
+        const size_t k = (size_t)(r0 + aa) + (size_t)(c0 + bb) * fr.M;
+        const size_t kg = (size_t)(r0 + aa - 3) + (size_t)(c0 + bb - 3) * gM;
+        float f = fr.ref[k];
+        uint8_t on = 1;
+        if (quad && fr.mask) {
+          on = fr.mask[k] != 0;
+          if (!on) f = 0.f;
+        }
+        s.f[p] = f;
+        s.gx[p] = fr.gx[kg];
+        s.gy[p] = fr.gy[kg];
+        s.on[p] = on;
+        s.cur[p] = 1;
+      }
+    }
+    __syncthreads();
+    if (masked) {
+      flood_select(s.on, s.cur, R, Cc, sr, sc, 4, nullptr);  // cur = bw4
+      __syncthreads();
+    }
+    // f-side sums restricted by cur: H(3), sum J f (2), sum J (2), f stats (3), sum|f|
+    {
+      float h0 = 0, h1 = 0, h2 = 0, jf0 = 0, jf1 = 0, jb0 = 0, jb1 = 0, fs = 0, fs2 = 0, fn = 0, fab = 0;
+      for (int p = tid; p < npx; p += kNT) {
+        const float m = s.cur[p] ? 1.f : 0.f;
+        const float gxv = s.gx[p] * m, gyv = s.gy[p] * m, f = s.f[p] * m;
+        h0 = fmaf(gxv, gxv, h0);
+        h1 = fmaf(gxv, gyv, h1);
+        h2 = fmaf(gyv, gyv, h2);
+        jf0 = fmaf(gxv, f, jf0);
+        jf1 = fmaf(gyv, f, jf1);
+        jb0 += gxv;
+        jb1 += gyv;
+        const bool sel = quad ? (fabsf(f) > 1e-10f) : true;
+        if (sel) {
+          fs += f;
+          fs2 = fmaf(f, f, fs2);
+          fn += 1.f;
+        }
+        fab += fabsf(f);
+      }
+      double v[11] = {h0, h1, h2, jf0, jf1, jb0, jb1, fs, fs2, fn, fab};
+      block_sum<11, kNT>(v, red, sums);
+    }
+    if (tid == 0) {
+      double hs[3] = {0, 0, 0};
+      if (!quad && a.HPar) {  // stored Hessian block H(5:6,5:6) (funICGN_Subpb1.m:35)
+        hs[0] = a.HPar[t + a.n * 18];
+        hs[1] = a.HPar[t + a.n * 19];
+        hs[2] = a.HPar[t + a.n * 20];
+      }
+      sub1_fside(c, sums, quad, hs, a.mu);
+      c.P[0] = a.FOld[4 * t];
+      c.P[1] = a.FOld[4 * t + 1];
+      c.P[2] = a.FOld[4 * t + 2];
+      c.P[3] = a.FOld[4 * t + 3];
+      c.P[4] = a.UOld[2 * t];
+      c.P[5] = a.UOld[2 * t + 1];
+      c.normNew = 1.0;
+      c.normAbs = 1.0;
+      c.normInit = 0.0;
+      c.step = 0;
+      c.status = 0;
+      c.fbw8_ready = 0;
+    }
+    __syncthreads();
+    const double uo0 = a.UOld[2 * t], uo1 = a.UOld[2 * t + 1];
+    const double vd0 = a.vdual[2 * t], vd1 = a.vdual[2 * t + 1];
+    while (true) {
+      if (tid == 0) {
+        int go = (c.step <= 100 && c.normNew > a.tol && c.normAbs > a.tol) ? 1 : 0;
+        if (go) {
+          c.step += 1;
+          if (warped_oob(fr, c.P, x0, y0, hx, hy)) {
+            c.normNew = 1e6;
+            go = 0;
+          } else {
+            const double n5 = mround(c.P[4]), n6 = mround(c.P[5]);
+            c.pf[0] = (float)c.P[0];
+            c.pf[1] = (float)c.P[1];
+            c.pf[2] = (float)c.P[2];
+            c.pf[3] = (float)c.P[3];
+            c.f5 = (float)(c.P[4] - n5);
+            c.f6 = (float)(c.P[5] - n6);
+            c.base_r = (int)(x0 + n5) - 2;
+            c.base_c = (int)(y0 + n6) - 2;
+          }
+        }
+        c.go = go;
+      }
+      __syncthreads();
+      if (!c.go) break;
+      // pass 1: g and the g-side sums with the current f-side region
+      float C0 = 0, C1 = 0, S1 = 0, S2 = 0, ns = 0, nz = 0;
+      for (int p = tid; p < npx; p += kNT) {
+        const float dx = (float)(p % R - hx), dy = (float)(p / R - hy);
+        const float lx = dx + fmaf(c.pf[0], dx, fmaf(c.pf[2], dy, c.f5));
+        const float ly = dy + fmaf(c.pf[3], dy, fmaf(c.pf[1], dx, c.f6));
+        const float ix = floorf(lx), iy = floorf(ly);
+        const float g = stencil16(fr.def, fr.M, c.base_r + (int)ix, c.base_c + (int)iy, lx - ix, ly - iy);
+        s.g[p] = g;
+        const float m = s.cur[p] ? 1.f : 0.f;
+        C0 = fmaf(s.gx[p] * m, g, C0);
+        C1 = fmaf(s.gy[p] * m, g, C1);
+        const bool sel = quad ? (fabsf(g) > 1e-10f) : true;
+        if (sel) {
+          S1 += g;
+          S2 = fmaf(g, g, S2);
+          ns += 1.f;
+        }
+        nz += (g == 0.f) ? 1.f : 0.f;
+      }
+      double gv[6] = {C0, C1, S1, S2, ns, nz};
+      block_sum<6, kNT>(gv, red, sums);
+      double Cg[2] = {sums[0], sums[1]}, Sg1 = sums[2], Sg2 = sums[3], Sgn = sums[4];
+      const bool run_mask = quad && (masked || sums[5] > 0);
+      __syncthreads();
+      if (run_mask) {
+        // funICGN_Subpb1quadtree.m:158-193: 4-connected g region, fallback to the
+        // 8-connected f-mask region; f, fx, fy, H, mean_f, bf recomputed on it.
+        for (int p = tid; p < npx; p += kNT) s.tmp[p] = (s.g[p] != 0.f);
+        __syncthreads();
+        flood_select(s.tmp, s.glab, R, Cc, sr, sc, 4, nullptr);
+        int allon = 1;
+        for (int p = tid; p < npx; p += kNT) allon &= s.glab[p];
+        allon = __syncthreads_and(allon);
+        if (allon && !c.fbw8_ready) {
+          flood_select(s.on, s.fbw8, R, Cc, sr, sc, 8, nullptr);
+          __syncthreads();
+          if (tid == 0) c.fbw8_ready = 1;
+        }
+        const uint8_t* gm = allon ? s.fbw8 : s.glab;
+        float h0 = 0, h1 = 0, h2 = 0, jf0 = 0, jf1 = 0, jb0 = 0, jb1 = 0, fs = 0, fs2 = 0, fn = 0, fab = 0;
+        float c0 = 0, c1 = 0, t1 = 0, t2 = 0, tn = 0;
+        for (int p = tid; p < npx; p += kNT) {
+          const uint8_t mk = gm[p];
+          s.cur[p] = mk;
+          const float m = mk ? 1.f : 0.f;
+          const float gxv = s.gx[p] * m, gyv = s.gy[p] * m, f = s.f[p] * m, g = s.g[p] * m;
+          h0 = fmaf(gxv, gxv, h0);
+          h1 = fmaf(gxv, gyv, h1);
+          h2 = fmaf(gyv, gyv, h2);
+          jf0 = fmaf(gxv, f, jf0);
+          jf1 = fmaf(gyv, f, jf1);
+          jb0 += gxv;
+          jb1 += gyv;
+          if (fabsf(f) > 1e-10f) {
+            fs += f;
+            fs2 = fmaf(f, f, fs2);
+            fn += 1.f;
+          }
+          fab += fabsf(f);
+          c0 = fmaf(gxv, g, c0);
+          c1 = fmaf(gyv, g, c1);
+          if (fabsf(g) > 1e-10f) {
+            t1 += g;
+            t2 = fmaf(g, g, t2);
+            tn += 1.f;
+          }
+        }
+        double v[16] = {h0, h1, h2, jf0, jf1, jb0, jb1, fs, fs2, fn, fab, c0, c1, t1, t2, tn};
+        block_sum<16, kNT>(v, red, sums);
+        if (tid == 0) sub1_fside(c, sums, true, nullptr, a.mu);
+        Cg[0] = sums[11];
+        Cg[1] = sums[12];
+        Sg1 = sums[13];
+        Sg2 = sums[14];
+        Sgn = sums[15];
+      }
+      if (tid == 0) {
+        double meang, bg;
+        if (Sgn > 0) {
+          meang = Sg1 / Sgn;
+          bg = sqrt(fmax(Sg2 - Sg1 * Sg1 / Sgn, 0.0));
+        } else {
+          meang = ALDIC_NAN;
+          bg = ALDIC_NAN;
+        }
+        double b[2];
+        for (int i = 0; i < 2; ++i) b[i] = c.bf * (c.A[i] - (Cg[i] - meang * c.B[i]) / bg);
+        const double s2 = 2.0 / (c.bf * c.bf);
+        const double tb[2] = {b[0] * s2 + a.mu * (c.P[4] - uo0 - vd0), b[1] * s2 + a.mu * (c.P[5] - uo1 - vd1)};
+        const double dmax = fmax(c.H2[0], c.H2[3]);
+        const double tH[4] = {c.H2[0] + 1e-3 * dmax, c.H2[1], c.H2[2], c.H2[3] + 1e-3 * dmax};
+        const double nb[2] = {-tb[0], -tb[1]};
+        double d56[2];
+        solve_small(2, tH, nb, d56);
+        c.normNew = sqrt(tb[0] * tb[0] + tb[1] * tb[1]);
+        c.normAbs = c.normNew;
+        if (c.step == 1) c.normInit = c.normNew;
+        if (c.normInit > a.tol) c.normNew = c.normNew / c.normInit;
+        else c.normNew = 0.0;
+        if (!(c.normNew < a.tol || c.normAbs < a.tol)) {
+          const double dP[6] = {0, 0, 0, 0, d56[0], d56[1]};
+          if (!compose_inverse(c.P, dP)) {
+            c.step += 1000;
+            c.status = 1;
+          }
+        }
+      }
+      __syncthreads();
+    }
+    if (tid == 0) {
+      int step = c.step;
+      if (c.status == 1) step -= 1000;
+      if (!(c.normNew < a.tol || c.normAbs < a.tol)) step = 101;
+      if (isnan(c.normNew)) step = 101;
+      if (quad && c.sabsf < 1e-6) step = 103;
+      a.conv[t] = step;
+      a.U[2 * t] = c.P[4];
+      a.U[2 * t + 1] = c.P[5];
+    }
+    __syncthreads();
+  }
+}
+
+// ================================================================================
+// host launchers
+// ================================================================================
+static int occupancy_grid(const void* fn, size_t smem) {
+  int dev = 0, sms = 148, per_sm = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kNT, smem);
+  if (per_sm < 1) per_sm = 1;
+  return sms * per_sm;
+}
+
+size_t icgn_smem_bytes(int w) { return (size_t)(w + 1) * (w + 1) * (4 * sizeof(float) + 4); }
+size_t sub1_smem_bytes(int wx, int wy) { return (size_t)(wx + 1) * (wy + 1) * (4 * sizeof(float) + 5); }
+
+int launch_icgn(const IcgnArgs& a, int wmax_enlarged, cudaStream_t st) {
+  int launches = 0;
+  cudaMemsetAsync(a.qcount, 0, 2 * sizeof(int), st);
+  const long long threads = a.n * 32;
+  const int cb = 256;
+  icgn_classify_kernel<<<(unsigned)((threads + cb - 1) / cb), cb, 0, st>>>(a);
+  ++launches;
+  for (int bucket = 0; bucket < 2; ++bucket) {
+    const int w = bucket == 0 ? a.winsize : wmax_enlarged;
+    const size_t smem = icgn_smem_bytes(w);
+    cudaFuncSetAttribute(icgn_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int grid = occupancy_grid((const void*)icgn_solve_kernel, smem);
+    if (bucket == 1) grid = grid < 296 ? grid : 296;
+    if ((long long)grid > a.n) grid = (int)a.n;
+    if (grid < 1) grid = 1;
+    icgn_solve_kernel<<<grid, kNT, smem, st>>>(a, bucket);
+    ++launches;
+  }
+  return launches;
+}
+
+int launch_subpb1(const Sub1Args& a, int wmax_x, int wmax_y, cudaStream_t st) {
+  int launches = 0;
+  cudaMemsetAsync(a.qcount, 0, 2 * sizeof(int), st);
+  const long long threads = a.n * 32;
+  const int cb = 256;
+  subpb1_classify_kernel<<<(unsigned)((threads + cb - 1) / cb), cb, 0, st>>>(a);
+  ++launches;
+  for (int bucket = 0; bucket < 2; ++bucket) {
+    const size_t smem = bucket == 0 ? sub1_smem_bytes(a.winsize, a.winsize) : sub1_smem_bytes(wmax_x, wmax_y);
+    cudaFuncSetAttribute(subpb1_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int grid = occupancy_grid((const void*)subpb1_solve_kernel, smem);
+    if (bucket == 1) grid = grid < 296 ? grid : 296;
+    if ((long long)grid > a.n) grid = (int)a.n;
+    if (grid < 1) grid = 1;
+    subpb1_solve_kernel<<<grid, kNT, smem, st>>>(a, bucket);
+    ++launches;
+  }
+  return launches;
+}
+
+}  // namespace aldic

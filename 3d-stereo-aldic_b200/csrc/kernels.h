@@ -1,0 +1,94 @@
+// Internal kernel interfaces of the ALDIC B200 library (not part of the public C ABI).
+#pragma once
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+namespace aldic {
+
+// Device-resident frame: normalised images (FP32, column-major M x N), binary mask
+// (u8, may be null = all ones) and the cropped gradients ((M-6) x (N-6), FP32).
+struct FrameDev {
+  const float* ref;
+  const float* def;
+  const uint8_t* mask;
+  const float* gx;
+  const float* gy;
+  int M, N;
+};
+
+struct IcgnArgs {
+  FrameDev fr;
+  int variant;  // 0 uniform (funICGN), 1 quadtree (funICGNQuadtree), 2 epipolar (epipolar_ICGN1)
+  long long n;
+  const double* coords;  // n x 2
+  const double* U0;      // 2n
+  int winsize;
+  double tol;
+  int max_iter;  // 100, or 30 for the epipolar variant
+  int crop;      // gradient offset: 3 (DfCropWidth) or 4 (DfAxis start)
+  double* U;     // 2n
+  double* F;     // 4n
+  double* H;     // n x 21 or null
+  int* conv;     // n
+  uint8_t* mark; // n or null
+  double* znssd; // n (epipolar)
+  int* queue;    // 2 buckets x n x 3 ints
+  int* qcount;   // 2
+};
+
+struct Sub1Args {
+  FrameDev fr;
+  int variant;  // 0 uniform (funICGN_Subpb1), 1 quadtree (funICGN_Subpb1quadtree)
+  long long n;
+  const double* coords;
+  const double* UOld;
+  const double* FOld;
+  const double* vdual;
+  const int* winsize_list;  // n x 2 (quadtree)
+  int winsize;              // uniform winsize / nominal bucket size
+  const double* HPar;       // n x 21 (uniform)
+  double mu, tol;
+  double* U;
+  int* conv;
+  int* queue;   // 2 buckets x n x 4 ints
+  int* qcount;  // 2
+};
+
+struct SearchArgs {
+  const float* f;  // normalised REF
+  const float* g;  // normalised DEF
+  int M, N;
+  int s0, s1;      // tempSizeOfSearchRegion
+  int gx0, gx1, gy0, gy1;  // gridx, gridy (1-based)
+  int winsize, step;
+  int nx, ny;
+  double* x;
+  double* y;
+  double* u;
+  double* v;
+  double* phi;
+  double* I1;  // (M+1) x (N+1) integral images of g and g^2 (scratch)
+  double* I2;
+};
+
+// launchers return the number of kernels they enqueued (or < 0 on argument errors)
+int launch_normalize(const void* img, int dtype, int M, int N, int gx0, int gx1, int gy0, int gy1,
+                     const uint8_t* mask, float* out, double* stats, double* partials, int npartials,
+                     unsigned int* counter, cudaStream_t st);
+int launch_f64_to_f32(const double* in, long long n, float* out, cudaStream_t st);
+int launch_f32_to_f64(const float* in, long long n, double* out, cudaStream_t st);
+int launch_mask_binarize(const double* in, long long n, uint8_t* out, cudaStream_t st);
+int launch_gradient(const float* img, const uint8_t* mask, int M, int N, float* gx, float* gy, cudaStream_t st);
+int launch_interp_points(const float* img, int M, int N, long long n, const double* X, const double* Y, double* Z,
+                         cudaStream_t st);
+size_t icgn_smem_bytes(int w);
+size_t sub1_smem_bytes(int wx, int wy);
+int launch_icgn(const IcgnArgs& a, int wmax_enlarged, cudaStream_t st);
+int launch_subpb1(const Sub1Args& a, int wmax_x, int wmax_y, cudaStream_t st);
+size_t search_smem_bytes(int winsize, int s0, int s1);
+int launch_search(const SearchArgs& a, cudaStream_t st);
+int launch_triangulate(long long n, const double* pairs, const double* PL, const double* PR, double* xyz,
+                       double* err, cudaStream_t st);
+
+}  // namespace aldic

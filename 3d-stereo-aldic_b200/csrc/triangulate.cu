@@ -1,0 +1,108 @@
+// Per-point stereo triangulation (func_quadtree/stereoReconstruction_quadtree.m:30-52,
+// which calls MATLAB's triangulate: linear DLT solved by SVD).  FP64 throughout: the
+// 4x4 homogeneous system is ill-conditioned at small stereo angles.
+#include "common.cuh"
+#include "kernels.h"
+
+namespace aldic {
+
+// One-sided (Hestenes) Jacobi SVD of a 4x4 matrix A (row-major a[r][c]); returns the
+// right singular vector of the smallest singular value in x.
+__device__ void smallest_right_singular(double a[4][4], double x[4]) {
+  double V[4][4];
+  for (int r = 0; r < 4; ++r)
+    for (int c = 0; c < 4; ++c) V[r][c] = (r == c) ? 1.0 : 0.0;
+  for (int sweep = 0; sweep < 40; ++sweep) {
+    double off = 0.0;
+    for (int p = 0; p < 3; ++p)
+      for (int q = p + 1; q < 4; ++q) {
+        double alpha = 0, beta = 0, gamma = 0;
+        for (int r = 0; r < 4; ++r) {
+          alpha += a[r][p] * a[r][p];
+          beta += a[r][q] * a[r][q];
+          gamma += a[r][p] * a[r][q];
+        }
+        const double scale = sqrt(alpha * beta);
+        if (!(scale > 0)) continue;
+        const double rel = fabs(gamma) / scale;
+        if (rel > off) off = rel;
+        if (rel < 1e-17) continue;
+        const double zeta = (beta - alpha) / (2.0 * gamma);
+        const double t = (zeta >= 0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+        const double cs = 1.0 / sqrt(1.0 + t * t), sn = cs * t;
+        for (int r = 0; r < 4; ++r) {
+          const double ap = a[r][p], aq = a[r][q];
+          a[r][p] = cs * ap - sn * aq;
+          a[r][q] = sn * ap + cs * aq;
+          const double vp = V[r][p], vq = V[r][q];
+          V[r][p] = cs * vp - sn * vq;
+          V[r][q] = sn * vp + cs * vq;
+        }
+      }
+    if (off < 1e-15) break;
+  }
+  int kmin = 0;
+  double smin = INFINITY;
+  for (int c = 0; c < 4; ++c) {
+    double s = 0;
+    for (int r = 0; r < 4; ++r) s += a[r][c] * a[r][c];
+    if (s < smin) {
+      smin = s;
+      kmin = c;
+    }
+  }
+  for (int r = 0; r < 4; ++r) x[r] = V[r][kmin];
+}
+
+// pairs: n x 4 column-major [xL yL xR yR]; PL, PR: 3x4 row-major; xyz: n x 3 col-major.
+__global__ void triangulate_kernel(long long n, const double* __restrict__ pairs, const double* __restrict__ PLg,
+                                   const double* __restrict__ PRg, double* __restrict__ xyz,
+                                   double* __restrict__ err) {
+  __shared__ double PL[12], PR[12];
+  if (threadIdx.x < 12) {
+    PL[threadIdx.x] = PLg[threadIdx.x];
+    PR[threadIdx.x] = PRg[threadIdx.x];
+  }
+  __syncthreads();
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+    const double x1 = pairs[k], y1 = pairs[n + k], x2 = pairs[2 * n + k], y2 = pairs[3 * n + k];
+    if (!(isfinite(x1) && isfinite(y1) && isfinite(x2) && isfinite(y2))) {
+      xyz[k] = xyz[n + k] = xyz[2 * n + k] = ALDIC_NAN;
+      if (err) err[k] = ALDIC_NAN;
+      continue;
+    }
+    double A[4][4];
+    for (int c = 0; c < 4; ++c) {
+      A[0][c] = x1 * PL[8 + c] - PL[c];
+      A[1][c] = y1 * PL[8 + c] - PL[4 + c];
+      A[2][c] = x2 * PR[8 + c] - PR[c];
+      A[3][c] = y2 * PR[8 + c] - PR[4 + c];
+    }
+    double X[4];
+    smallest_right_singular(A, X);
+    const double X0 = X[0] / X[3], X1 = X[1] / X[3], X2 = X[2] / X[3];
+    xyz[k] = X0;
+    xyz[n + k] = X1;
+    xyz[2 * n + k] = X2;
+    if (err) {
+      const double lz = PL[8] * X0 + PL[9] * X1 + PL[10] * X2 + PL[11];
+      const double lx = (PL[0] * X0 + PL[1] * X1 + PL[2] * X2 + PL[3]) / lz;
+      const double ly = (PL[4] * X0 + PL[5] * X1 + PL[6] * X2 + PL[7]) / lz;
+      const double rz = PR[8] * X0 + PR[9] * X1 + PR[10] * X2 + PR[11];
+      const double rx = (PR[0] * X0 + PR[1] * X1 + PR[2] * X2 + PR[3]) / rz;
+      const double ry = (PR[4] * X0 + PR[5] * X1 + PR[6] * X2 + PR[7]) / rz;
+      err[k] = 0.5 * (hypot(lx - x1, ly - y1) + hypot(rx - x2, ry - y2));
+    }
+  }
+}
+
+int launch_triangulate(long long n, const double* pairs, const double* PL, const double* PR, double* xyz,
+                       double* err, cudaStream_t st) {
+  if (n <= 0) return 0;
+  long long g = (n + 127) / 128;
+  if (g > 148 * 16) g = 148 * 16;
+  triangulate_kernel<<<(unsigned)g, 128, 0, st>>>(n, pairs, PL, PR, xyz, err);
+  return 1;
+}
+
+}  // namespace aldic

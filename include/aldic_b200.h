@@ -1,0 +1,145 @@
+/*
+ * aldic_b200.h -- C ABI of the B200 (sm_100a) implementation of the 3D-Stereo-ALDIC
+ * per-subset hot path: image preparation, whole-field integer (ZNCC) search, local
+ * IC-GN with the local bicubic B-spline stencil (uniform and quadtree/masked), the
+ * ALDIC Subpb1 augmented-Lagrangian local step, the epipolar IC-GN candidate score and
+ * per-point stereo triangulation.
+ *
+ * Conventions follow the MATLAB reference so that a MEX shim can pass mxArray data
+ * pointers straight through:
+ *   - images are column-major M x N (dim 1 = image x, because the reference transposes
+ *     images at load), element (i, j) at i + j*M;
+ *   - pixel coordinates are 1-based;
+ *   - coordinatesFEM is n x 2 column-major; U is 2n interleaved [u1 v1 u2 v2 ...];
+ *     F is 4n interleaved [F11 F21 F12 F22 ...]; H is n x 21 column-major (the packed
+ *     lower triangle [H(1:6) H(8:12) H(15:18) H(22:24) H(29:30) H(36)]).
+ *
+ * Every array argument may be host or device memory (checked with
+ * cudaPointerGetAttributes).  A call whose outputs are all device memory is
+ * asynchronous on the context's stream; a call with any host output returns after the
+ * results are in host memory.  The library never frees caller memory.
+ *
+ * Return value: ALDIC_OK or an error code; aldic_last_error() gives the message.
+ * Per-subset outcomes are in-band as in the reference: the iteration count when
+ * converged, 101 (not converged / out of image / NaN), 102 (too much of the subset
+ * masked), 103 (all-zero reference subset), -1 (the reference solver raised an error).
+ */
+#ifndef ALDIC_B200_H
+#define ALDIC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ALDIC_OK 0
+#define ALDIC_ERR_ARG 1
+#define ALDIC_ERR_CUDA 2
+#define ALDIC_ERR_TIMEOUT 3
+#define ALDIC_ERR_STATE 4
+
+/* element types of raw images */
+#define ALDIC_U8 0
+#define ALDIC_U16 1
+#define ALDIC_F32 2
+#define ALDIC_F64 3
+
+/* image slots of a context */
+#define ALDIC_SLOT_REF 0
+#define ALDIC_SLOT_DEF 1
+
+/* solver variants */
+#define ALDIC_UNIFORM 0  /* LocalICGN / Subpb1 (func/funICGN.m, func/funICGN_Subpb1.m) */
+#define ALDIC_QUADTREE 1 /* LocalICGNQuadtree / Subpb1Quadtree (masked solvers) */
+
+typedef struct aldic_ctx aldic_ctx;
+
+/* Create a context on CUDA device `device`; it owns a stream and device buffers. */
+int aldic_create(aldic_ctx** ctx, int device);
+void aldic_destroy(aldic_ctx* ctx);
+const char* aldic_last_error(const aldic_ctx* ctx);
+/* Run subsequent work on `stream` (a cudaStream_t); NULL restores the context's own. */
+int aldic_set_stream(aldic_ctx* ctx, void* stream);
+int aldic_synchronize(aldic_ctx* ctx);
+/* Number of kernels this context has launched since creation. */
+int64_t aldic_launch_count(const aldic_ctx* ctx);
+int aldic_abi_version(void);
+
+/* ---------------------------------------------------------------- frame state ---- */
+/* funNormalizeImg (func/funNormalizeImg.m:109-127) of a raw image into `slot`:
+ * (img - mean_ROI) / std_ROI, FP64 statistics over gridx x gridy (1-based inclusive,
+ * clamped to the image), stored as FP32 on the device.  If `mask` (M x N, nonzero = in)
+ * is given the stored image is additionally multiplied by it, as TemporalMatch
+ * (func/TemporalMatch_quadtree_ST1.m:47-48) does.  mean_std (2 doubles, may be NULL)
+ * receives the statistics. */
+int aldic_load_image_raw(aldic_ctx* ctx, int slot, const void* img, int dtype, int M, int N, const int* gridx,
+                         const int* gridy, const double* mask, double* mean_std);
+/* Store an already-normalised image (the ImgRef / ImgDef arguments of the MATLAB
+ * solvers) into `slot`. */
+int aldic_load_image(aldic_ctx* ctx, int slot, const double* img, int M, int N);
+/* Df.ImgRefMask (M x N; NULL = all ones).  Values are binarised (nonzero -> 1). */
+int aldic_set_mask(aldic_ctx* ctx, const double* mask, int M, int N);
+/* funImgGradient (func/funImgGradient.m:50-78) of the REF slot on the device:
+ * 7-tap central differences, crop 3, times the mask. */
+int aldic_compute_gradients(aldic_ctx* ctx);
+/* Df.DfDx / Df.DfDy given by the caller, (M-6) x (N-6). */
+int aldic_set_gradients(aldic_ctx* ctx, const double* dfdx, const double* dfdy, int M6, int N6);
+/* Read back device state as doubles: what = 0 REF image, 1 DEF image, 2 DfDx, 3 DfDy. */
+int aldic_get_state(aldic_ctx* ctx, int what, double* out);
+
+/* ---------------------------------------------------------- interpolation ------- */
+/* ba_interp2_spline(F, X, Y) (ba_interp2_spline.cpp:418-435, local 4x4 stencil
+ * :235-331) on the image in `slot`: X is the dim-2 and Y the dim-1 coordinate. */
+int aldic_interp2(aldic_ctx* ctx, int slot, int64_t n, const double* X, const double* Y, double* Z);
+
+/* ------------------------------------------------------- integer search --------- */
+/* Grid size of funIntegerSearchWholeField (func/funIntegerSearch.m:106-107). */
+int aldic_search_grid(const int* gridx, const int* gridy, int winsize, int step, int* nx, int* ny);
+/* funIntegerSearch(f, g, search, gridx, gridy, winsize, step, 0)
+ * (func/funIntegerSearch.m:2-98,100-203) with f = REF slot and g = DEF slot:
+ * per grid subset ZNCC (normxcorr2) over the border-clamped search window, crop, and
+ * findpeak (func/findpeak.m) with the 1e-3 px rounding.  search = [s0 s1]
+ * (tempSizeOfSearchRegion; expanded to [left right up down] = [s0 s1 s0 s1]).
+ * Outputs x, y, u, v, phi are nY x nX column-major; failed subsets give NaN. */
+int aldic_integer_search(aldic_ctx* ctx, const int* search, const int* gridx, const int* gridy, int winsize,
+                         int step, double* x, double* y, double* u, double* v, double* phi);
+
+/* --------------------------------------------------------- local IC-GN ---------- */
+/* Loop body of LocalICGN (variant ALDIC_UNIFORM; func/LocalICGN.m:64-164 with
+ * func/funICGN.m) or LocalICGNQuadtree (ALDIC_QUADTREE;
+ * func_quadtree/LocalICGNQuadtree.m:67-164 with func_quadtree/funICGNQuadtree.m):
+ * first-order IC-GN, Gauss-Newton, maxIter 100, on the REF/DEF slots, gradients and
+ * mask of the context.  H (n x 21) and markHole (n, quadtree only) may be NULL. */
+int aldic_local_icgn(aldic_ctx* ctx, int variant, int64_t n, const double* coords, const double* U0, int winsize,
+                     double tol, double* U, double* F, double* H, int32_t* conv, uint8_t* markHole);
+
+/* Loop body of Subpb1 (ALDIC_UNIFORM; func/Subpb1.m with func/funICGN_Subpb1.m, Hessian
+ * block H(5:6,5:6) from HPar n x 21) or Subpb1Quadtree (ALDIC_QUADTREE;
+ * func_quadtree/Subpb1Quadtree.m:71-126 with func_quadtree/funICGN_Subpb1quadtree.m,
+ * per-subset winsize_List n x 2): the ALDIC augmented-Lagrangian translation step with
+ * F fixed at FOld.  vdual is 2n interleaved.  A solver error gives U = NaN and
+ * conv = -1 (uniform) or 0 (quadtree), as the two drivers store. */
+int aldic_subpb1(aldic_ctx* ctx, int variant, int64_t n, const double* coords, const double* UOld,
+                 const double* FOld, const double* vdual, const int32_t* winsize_list, int winsize,
+                 const double* HPar, double mu, double tol, double* U, int32_t* conv);
+
+/* epipolar_ICGN1 (func/epipolar_ICGN1.m:1-253) for n candidate points pts (n x 2):
+ * IC-GN from P = 0 with the translation held at 0, at most 30 iterations, gradient
+ * offset Df.DfAxis(1) = 4; znssd = ZNSSD of the final iteration (NaN on failure). */
+int aldic_epipolar_icgn(aldic_ctx* ctx, int64_t n, const double* pts, int winsize, double tol, double* znssd);
+
+/* -------------------------------------------------------- triangulation --------- */
+/* triangulatePoints (func_quadtree/stereoReconstruction_quadtree.m:30-52): per row of
+ * pairs (n x 4 column-major [xL yL xR yR]) the DLT of P_L = K_L [I | 0] and
+ * P_R = K_R [R | T], solved in FP64 by SVD; xyz (n x 3) and the mean two-view
+ * reprojection error; rows with non-finite input give NaN.  KL, KR, R are 3 x 3
+ * column-major (MATLAB), T has 3 entries. */
+int aldic_triangulate(aldic_ctx* ctx, int64_t n, const double* pairs, const double* KL, const double* KR,
+                      const double* R, const double* T, double* xyz, double* reproj_err);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ALDIC_B200_H */

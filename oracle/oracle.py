@@ -1,0 +1,268 @@
+"""ctypes front end of the FP64 CPU oracle (test infrastructure only).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline / reference legs import
+this module, as the checker.  The product path (the CUDA library under
+3d-stereo-aldic_b200/) never calls it.
+
+Arrays follow the reference's MATLAB layouts: images are column-major M x N (numpy
+``order='F'``), coordinates are 1-based, U is interleaved [u1 v1 ...], F is interleaved
+[F11 F21 F12 F22 ...], H is n x 21.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+_REF = None
+
+_dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_up = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
+
+
+def build(force: bool = False) -> None:
+    """Compile liboracle.so (and _ref/ when the reference sources are present)."""
+    so = os.path.join(_HERE, "liboracle.so")
+    src = os.path.join(_HERE, "aldic_oracle.cpp")
+    if force or not os.path.exists(so) or os.path.getmtime(so) < os.path.getmtime(src):
+        subprocess.check_call(["make", "-s", "-C", _HERE])
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build()
+        L = C.CDLL(path)
+        L.orc_interp.argtypes = [_dp, C.c_int, C.c_int, _dp, _dp, C.c_long, _dp]
+        L.orc_normalize.argtypes = [_dp, C.c_int, C.c_int, _ip, _ip, _dp, _dp]
+        L.orc_gradient.argtypes = [_dp, C.c_void_p, C.c_int, C.c_int, _dp, _dp]
+        L.orc_local_icgn.argtypes = [C.c_int, _dp, _dp, C.c_void_p, _dp, _dp, C.c_int, C.c_int, C.c_long, _dp,
+                                     _dp, C.c_int, C.c_double, _dp, _dp, _dp, _ip, C.c_void_p, C.c_int]
+        L.orc_subpb1.argtypes = [C.c_int, _dp, _dp, C.c_void_p, _dp, _dp, C.c_int, C.c_int, C.c_long, _dp, _dp,
+                                 _dp, _dp, C.c_void_p, C.c_int, C.c_void_p, C.c_double, C.c_double, _dp, _ip,
+                                 C.c_int]
+        L.orc_epipolar_icgn.argtypes = [_dp, _dp, _dp, _dp, C.c_int, C.c_int, C.c_long, _dp, C.c_int, C.c_double,
+                                        _dp, _ip, C.c_int]
+        L.orc_search_grid.argtypes = [_ip, _ip, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        L.orc_integer_search.argtypes = [_dp, _dp, C.c_int, C.c_int, _ip, _ip, _ip, C.c_int, C.c_int, _dp, _dp,
+                                         _dp, _dp, _dp, C.c_void_p, C.c_int]
+        L.orc_findpeak.argtypes = [_dp, C.c_int, C.c_int, _dp]
+        L.orc_normxcorr2.argtypes = [_dp, C.c_int, C.c_int, _dp, C.c_int, C.c_int, _dp]
+        L.orc_normxcorr2.restype = C.c_int
+        L.orc_bwselect.argtypes = [_up, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _up]
+        _LIB = L
+    return _LIB
+
+
+def ref_lib():
+    """The reference's own ba_interp2_spline.cpp built under _ref/ (None if absent)."""
+    global _REF
+    if _REF is None:
+        path = os.path.join(_HERE, "_ref", "libref_interp.so")
+        if not os.path.exists(path):
+            return None
+        R = C.CDLL(path)
+        R.ref_interp2.argtypes = [_dp, C.c_long, C.c_long, _dp, _dp, C.c_long, _dp]
+        R.ref_interp2.restype = C.c_int
+        _REF = R
+    return _REF
+
+
+def _f64(a):
+    """Column-major image -> contiguous buffer in MATLAB memory order."""
+    return np.ascontiguousarray(np.asarray(a, dtype=np.float64).ravel(order="F"))
+
+
+def _flat(a, dtype=np.float64):
+    return np.ascontiguousarray(np.asarray(a, dtype=dtype).ravel())
+
+
+def interp(F, X, Y):
+    """ba_interp2_spline(F, X, Y): X is the dim-2 and Y the dim-1 coordinate (1-based)."""
+    F = np.asarray(F, dtype=np.float64)
+    M, N = F.shape
+    X = _flat(X)
+    Y = _flat(Y)
+    out = np.empty_like(X)
+    lib().orc_interp(_f64(F), M, N, X, Y, X.size, out)
+    return out
+
+
+def ref_interp(F, X, Y):
+    R = ref_lib()
+    if R is None:
+        raise RuntimeError("reference interpolation library not built")
+    F = np.asarray(F, dtype=np.float64)
+    M, N = F.shape
+    X = _flat(X)
+    Y = _flat(Y)
+    out = np.empty_like(X)
+    if R.ref_interp2(_f64(F), M, N, X, Y, X.size, out) != 0:
+        raise RuntimeError("reference MEX raised an error")
+    return out
+
+
+def normalize(img, gridx, gridy):
+    img = np.asarray(img, dtype=np.float64)
+    M, N = img.shape
+    out = np.empty(M * N)
+    ms = np.empty(2)
+    lib().orc_normalize(_f64(img), M, N, _flat(gridx, np.int32), _flat(gridy, np.int32), out, ms)
+    return out.reshape((M, N), order="F"), ms
+
+
+def gradient(img, mask=None):
+    img = np.asarray(img, dtype=np.float64)
+    M, N = img.shape
+    gx = np.empty((M - 6) * (N - 6))
+    gy = np.empty_like(gx)
+    mk = None if mask is None else _f64(mask)
+    lib().orc_gradient(_f64(img), None if mk is None else mk.ctypes.data, M, N, gx, gy)
+    return gx.reshape((M - 6, N - 6), order="F"), gy.reshape((M - 6, N - 6), order="F")
+
+
+class Frame:
+    """Reference/deformed images plus gradients, in the reference's layout."""
+
+    def __init__(self, ref, deff, mask, dfdx, dfdy):
+        ref = np.asarray(ref, dtype=np.float64)
+        self.M, self.N = ref.shape
+        self.ref = _f64(ref)
+        self.deff = _f64(deff)
+        self.mask = None if mask is None else _f64(mask)
+        self.dfdx = _f64(dfdx)
+        self.dfdy = _f64(dfdy)
+
+    def _mask_ptr(self):
+        return None if self.mask is None else self.mask.ctypes.data
+
+
+def local_icgn(frame: Frame, coords, U0, winsize, tol, variant=1, nthreads=0):
+    """Loop body of LocalICGN (variant 0) / LocalICGNQuadtree (variant 1)."""
+    coords = np.asarray(coords, dtype=np.float64)
+    n = coords.shape[0]
+    U = np.empty(2 * n)
+    F = np.empty(4 * n)
+    H = np.empty(21 * n)
+    conv = np.empty(n, dtype=np.int32)
+    mark = np.zeros(n, dtype=np.uint8)
+    lib().orc_local_icgn(variant, frame.ref, frame.deff, frame._mask_ptr(), frame.dfdx, frame.dfdy, frame.M, frame.N,
+                         n, _f64(coords), _flat(U0), int(winsize), float(tol), U, F, H, conv,
+                         mark.ctypes.data if variant == 1 else None, nthreads)
+    return dict(U=U, F=F, H=H.reshape((n, 21), order="F"), conv=conv, markHole=mark)
+
+
+def subpb1(frame: Frame, coords, UOld, FOld, vdual, mu, tol, winsize=None, winsize_list=None, HPar=None,
+           variant=1, nthreads=0):
+    """Loop body of Subpb1 (variant 0) / Subpb1Quadtree (variant 1)."""
+    coords = np.asarray(coords, dtype=np.float64)
+    n = coords.shape[0]
+    U = np.empty(2 * n)
+    conv = np.empty(n, dtype=np.int32)
+    wl = None
+    if variant == 1:
+        wl = np.ascontiguousarray(np.asarray(winsize_list, dtype=np.int32).ravel(order="F"))
+    hp = None if HPar is None else _f64(HPar)
+    lib().orc_subpb1(variant, frame.ref, frame.deff, frame._mask_ptr(), frame.dfdx, frame.dfdy, frame.M, frame.N, n,
+                     _f64(coords), _flat(UOld), _flat(FOld), _flat(vdual), None if wl is None else wl.ctypes.data,
+                     int(winsize or 0), None if hp is None else hp.ctypes.data, float(mu), float(tol), U, conv,
+                     nthreads)
+    return dict(U=U, conv=conv)
+
+
+def epipolar_icgn(frame: Frame, pts, winsize, tol, nthreads=0):
+    pts = np.asarray(pts, dtype=np.float64)
+    n = pts.shape[0]
+    z = np.empty(n)
+    conv = np.empty(n, dtype=np.int32)
+    lib().orc_epipolar_icgn(frame.ref, frame.deff, frame.dfdx, frame.dfdy, frame.M, frame.N, n, _f64(pts),
+                            int(winsize), float(tol), z, conv, nthreads)
+    return z, conv
+
+
+def search_grid(gridx, gridy, winsize, step):
+    nx = C.c_int()
+    ny = C.c_int()
+    lib().orc_search_grid(_flat(gridx, np.int32), _flat(gridy, np.int32), int(winsize), int(step), C.byref(nx),
+                          C.byref(ny))
+    return nx.value, ny.value
+
+
+def integer_search(f, g, search, gridx, gridy, winsize, step, nthreads=0, want_qf=True):
+    """funIntegerSearch(f, g, search, gridx, gridy, winsize, step, 0): returns x, y, u, v, phi, qf."""
+    f = np.asarray(f, dtype=np.float64)
+    M, N = f.shape
+    nx, ny = search_grid(gridx, gridy, winsize, step)
+    outs = [np.empty(nx * ny) for _ in range(5)]
+    qf = np.empty(2 * nx * ny) if want_qf else None
+    s = np.asarray(search, dtype=np.int32).ravel()
+    if s.size == 1:
+        s = np.array([s[0], s[0]], dtype=np.int32)
+    lib().orc_integer_search(_f64(f), _f64(g), M, N, _flat(s, np.int32), _flat(gridx, np.int32),
+                             _flat(gridy, np.int32), int(winsize), int(step), *outs,
+                             None if qf is None else qf.ctypes.data, nthreads)
+    x, y, u, v, phi = [o.reshape((ny, nx), order="F") for o in outs]
+    return dict(x=x, y=y, u=u, v=v, phi=phi, qf=None if qf is None else qf.reshape((nx * ny, 2), order="F"))
+
+
+def findpeak(f):
+    f = np.asarray(f, dtype=np.float64)
+    out = np.empty(3)
+    lib().orc_findpeak(_f64(f), f.shape[0], f.shape[1], out)
+    return out  # xpeak (column), ypeak (row), max_f
+
+
+def normxcorr2(T, A):
+    T = np.asarray(T, dtype=np.float64)
+    A = np.asarray(A, dtype=np.float64)
+    m, n = T.shape
+    ma, na = A.shape
+    out = np.empty((ma + m - 1) * (na + n - 1))
+    if lib().orc_normxcorr2(_f64(T), m, n, _f64(A), ma, na, out) != 0:
+        raise ValueError("normxcorr2: template larger than image or constant")
+    return out.reshape((ma + m - 1, na + n - 1), order="F")
+
+
+def bwselect(bw, r, c, conn):
+    """Connected component containing the 0-based seed (r, c)."""
+    bw = np.asarray(bw, dtype=np.uint8)
+    rows, cols = bw.shape
+    out = np.empty(rows * cols, dtype=np.uint8)
+    lib().orc_bwselect(_flat(bw.ravel(order="F"), np.uint8), rows, cols, int(r), int(c), int(conn), out)
+    return out.reshape((rows, cols), order="F")
+
+
+def triangulate(pairs, KL, KR, R, T):
+    """DLT triangulation (stereoReconstruction_quadtree.m:30-52 via MATLAB triangulate):
+    P_L = K_L [I | 0], P_R = K_R [R | T]; per finite row the homogeneous 4x4 system is
+    solved by SVD (smallest right singular vector).  Returns xyz (n x 3) and the mean
+    reprojection error of the two views (NaN rows where the input is not finite)."""
+    pairs = np.asarray(pairs, dtype=np.float64)
+    PL = np.asarray(KL, dtype=np.float64) @ np.hstack([np.eye(3), np.zeros((3, 1))])
+    PR = np.asarray(KR, dtype=np.float64) @ np.hstack([np.asarray(R, np.float64), np.asarray(T, np.float64).reshape(3, 1)])
+    n = pairs.shape[0]
+    xyz = np.full((n, 3), np.nan)
+    err = np.full(n, np.nan)
+    ok = np.all(np.isfinite(pairs), axis=1)
+    p = pairs[ok]
+    if p.size:
+        A = np.stack([p[:, 0:1] * PL[2] - PL[0], p[:, 1:2] * PL[2] - PL[1],
+                      p[:, 2:3] * PR[2] - PR[0], p[:, 3:4] * PR[2] - PR[1]], axis=1)
+        _, _, Vt = np.linalg.svd(A)
+        X = Vt[:, -1, :]
+        X = X[:, :3] / X[:, 3:4]
+        Xh = np.hstack([X, np.ones((X.shape[0], 1))])
+        pl = Xh @ PL.T
+        pr = Xh @ PR.T
+        el = np.hypot(pl[:, 0] / pl[:, 2] - p[:, 0], pl[:, 1] / pl[:, 2] - p[:, 1])
+        er = np.hypot(pr[:, 0] / pr[:, 2] - p[:, 2], pr[:, 1] / pr[:, 2] - p[:, 3])
+        xyz[ok] = X
+        err[ok] = 0.5 * (el + er)
+    return xyz, err
