@@ -37,12 +37,17 @@ class _Keep:
     def __init__(self):
         self.items = []
 
-    def ptr(self, x, dtype, order="F"):
+    def ptr(self, x, dtype, order="F", numel=None):
         if x is None:
             return None
         if _is_torch(x):
-            if not x.is_contiguous():
-                raise AldicError("device tensors must be contiguous")
+            if not x.is_cuda or not x.is_contiguous():
+                raise AldicError("device arrays must be contiguous CUDA tensors")
+            want = str(np.dtype(dtype))
+            if str(x.dtype).replace("torch.", "") != want:
+                raise AldicError(f"device array has dtype {x.dtype}, expected {want}")
+            if numel is not None and x.numel() < numel:
+                raise AldicError(f"device array holds {x.numel()} elements, {numel} required")
             return C.c_void_p(x.data_ptr())
         a = np.asarray(x, dtype=dtype)
         a = np.ascontiguousarray(a.ravel(order=order)) if a.ndim > 1 else np.ascontiguousarray(a)
@@ -53,6 +58,28 @@ class _Keep:
         a = np.empty(n, dtype=dtype)
         self.items.append(a)
         return a, C.c_void_p(a.ctypes.data)
+
+
+def _count(x, per_row):
+    """Number of rows of an n x per_row MATLAB array: numpy (n, per_row), or a CUDA tensor
+    of shape (per_row, n) (the same column-major memory)."""
+    if _is_torch(x):
+        if x.dim() != 2 or x.shape[0] != per_row:
+            raise AldicError(f"device arrays of n x {per_row} MATLAB data are passed as ({per_row}, n) tensors")
+        return int(x.shape[1])
+    a = np.asarray(x)
+    if a.ndim != 2 or a.shape[1] != per_row:
+        raise AldicError(f"expected an n x {per_row} array, got shape {a.shape}")
+    return int(a.shape[0])
+
+
+def _img_shape(img, shape):
+    """(M, N) of a column-major image: numpy arrays carry it; CUDA tensors need shape=."""
+    if _is_torch(img):
+        if shape is None or img.numel() != shape[0] * shape[1]:
+            raise AldicError("device images need shape=(M, N) matching their element count")
+        return int(shape[0]), int(shape[1])
+    return img.shape
 
 
 def _np_dtype_code(a):
@@ -93,6 +120,11 @@ class Context:
 
     # ------------------------------------------------------------------ frame
     def set_stream(self, stream_handle):
+        """Run on this cudaStream_t.  None restores the context's own stream; the legacy
+        default stream is cudaStreamLegacy (1), not 0."""
+        if stream_handle == 0:
+            raise AldicError("stream handle 0 means 'the context's own stream'; pass a created stream "
+                             "(e.g. torch.cuda.Stream()) or cudaStreamLegacy (1)")
         self._check(self.lib.aldic_set_stream(self.h, C.c_void_p(stream_handle or 0)), "aldic_set_stream")
 
     def synchronize(self):
@@ -102,17 +134,17 @@ class Context:
     def launches(self):
         return int(self.lib.aldic_launch_count(self.h))
 
-    def load_image_raw(self, slot, img, gridx, gridy, mask=None, want_stats=True):
+    def load_image_raw(self, slot, img, gridx, gridy, mask=None, want_stats=True, shape=None):
         k = _Keep()
-        M, N = img.shape
+        M, N = _img_shape(img, shape)
         gx = np.asarray(gridx, dtype=np.int32).ravel()
         gy = np.asarray(gridy, dtype=np.int32).ravel()
         ms = np.empty(2) if want_stats else None
         dtype_code = _np_dtype_code(img)
         npdt = {0: np.uint8, 1: np.uint16, 2: np.float32, 3: np.float64}[dtype_code]
-        rc = self.lib.aldic_load_image_raw(self.h, slot, k.ptr(img, npdt), dtype_code, M, N,
+        rc = self.lib.aldic_load_image_raw(self.h, slot, k.ptr(img, npdt, numel=M * N), dtype_code, M, N,
                                            C.c_void_p(gx.ctypes.data), C.c_void_p(gy.ctypes.data),
-                                           k.ptr(mask, np.float64),
+                                           k.ptr(mask, np.float64, numel=M * N),
                                            None if ms is None else C.c_void_p(ms.ctypes.data))
         self._check(rc, "aldic_load_image_raw")
         self.M, self.N = M, N
@@ -175,7 +207,7 @@ class Context:
             bufs = {name: k.out(nx * ny, np.float64) for name in ("x", "y", "u", "v", "phi")}
             ptrs = [bufs[nm][1] for nm in ("x", "y", "u", "v", "phi")]
         else:
-            ptrs = [C.c_void_p(out[nm].data_ptr()) for nm in ("x", "y", "u", "v", "phi")]
+            ptrs = [k.ptr(out[nm], np.float64, numel=nx * ny) for nm in ("x", "y", "u", "v", "phi")]
         rc = self.lib.aldic_integer_search(self.h, C.c_void_p(s.ctypes.data), C.c_void_p(gx.ctypes.data),
                                            C.c_void_p(gy.ctypes.data), int(winsize), int(step), *ptrs)
         self._check(rc, "aldic_integer_search")
@@ -185,7 +217,7 @@ class Context:
 
     def local_icgn(self, variant, coords, U0, winsize, tol, want_H=True, want_mark=True, out=None):
         k = _Keep()
-        n = int(coords.shape[0])
+        n = _count(coords, 2)
         if out is None:
             U, up = k.out(2 * n, np.float64)
             F, fp = k.out(4 * n, np.float64)
@@ -193,12 +225,14 @@ class Context:
             conv, cp = k.out(n, np.int32)
             mark, mp = k.out(n, np.uint8) if (want_mark and variant == _lib.QUADTREE) else (None, None)
         else:
-            up, fp = C.c_void_p(out["U"].data_ptr()), C.c_void_p(out["F"].data_ptr())
-            hp = C.c_void_p(out["H"].data_ptr()) if out.get("H") is not None else None
-            cp = C.c_void_p(out["conv"].data_ptr())
-            mp = C.c_void_p(out["mark"].data_ptr()) if out.get("mark") is not None else None
-        rc = self.lib.aldic_local_icgn(self.h, int(variant), n, k.ptr(coords, np.float64), k.ptr(U0, np.float64, "C"),
-                                       int(winsize), float(tol), up, fp, hp, cp, mp)
+            up = k.ptr(out["U"], np.float64, numel=2 * n)
+            fp = k.ptr(out["F"], np.float64, numel=4 * n)
+            hp = k.ptr(out.get("H"), np.float64, numel=21 * n)
+            cp = k.ptr(out["conv"], np.int32, numel=n)
+            mp = k.ptr(out.get("mark"), np.uint8, numel=n)
+        rc = self.lib.aldic_local_icgn(self.h, int(variant), n, k.ptr(coords, np.float64, numel=2 * n),
+                                       k.ptr(U0, np.float64, "C", numel=2 * n), int(winsize), float(tol), up, fp, hp,
+                                       cp, mp)
         self._check(rc, "aldic_local_icgn")
         if out is not None:
             return out
@@ -206,7 +240,7 @@ class Context:
 
     def subpb1(self, variant, coords, UOld, FOld, vdual, mu, tol, winsize=0, winsize_list=None, HPar=None):
         k = _Keep()
-        n = int(coords.shape[0])
+        n = _count(coords, 2)
         U, up = k.out(2 * n, np.float64)
         conv, cp = k.out(n, np.int32)
         wl = None if winsize_list is None else k.ptr(winsize_list, np.int32)
@@ -218,7 +252,7 @@ class Context:
 
     def epipolar_icgn(self, pts, winsize, tol):
         k = _Keep()
-        n = int(pts.shape[0])
+        n = _count(pts, 2)
         z, zp = k.out(n, np.float64)
         self._check(self.lib.aldic_epipolar_icgn(self.h, n, k.ptr(pts, np.float64), int(winsize), float(tol), zp),
                     "aldic_epipolar_icgn")
@@ -226,13 +260,14 @@ class Context:
 
     def triangulate(self, pairs, KL, KR, R, T, out=None):
         k = _Keep()
-        n = int(pairs.shape[0])
+        n = _count(pairs, 4)
         if out is None:
             xyz, xp = k.out(3 * n, np.float64)
             err, ep = k.out(n, np.float64)
         else:
-            xp, ep = C.c_void_p(out["xyz"].data_ptr()), C.c_void_p(out["err"].data_ptr())
-        rc = self.lib.aldic_triangulate(self.h, n, k.ptr(pairs, np.float64), k.ptr(KL, np.float64),
+            xp = k.ptr(out["xyz"], np.float64, numel=3 * n)
+            ep = k.ptr(out.get("err"), np.float64, numel=n)
+        rc = self.lib.aldic_triangulate(self.h, n, k.ptr(pairs, np.float64, numel=4 * n), k.ptr(KL, np.float64),
                                         k.ptr(KR, np.float64), k.ptr(R, np.float64), k.ptr(np.ravel(T), np.float64),
                                         xp, ep)
         self._check(rc, "aldic_triangulate")

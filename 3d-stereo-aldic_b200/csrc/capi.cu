@@ -621,7 +621,8 @@ int aldic_triangulate(aldic_ctx* c, int64_t n, const double* pairs, const double
       std::memcpy(dsts[i], srcs[i], cnts[i] * 8);
     }
   }
-  double P[24];  // PL (3x4 row-major) then PR
+  CamPair cams;  // PL (3x4 row-major) then PR
+  double* P = cams.P;
   for (int row = 0; row < 3; ++row)
     for (int col = 0; col < 4; ++col) {
       // PL = KL [I | 0]
@@ -633,12 +634,37 @@ int aldic_triangulate(aldic_ctx* c, int64_t n, const double* pairs, const double
     }
   Arg ap{pairs, (size_t)n * 32, false, nullptr}, ax{xyz, (size_t)n * 24, true, nullptr};
   Arg ae{reproj_err, reproj_err ? (size_t)n * 8 : 0, true, nullptr};
-  Arg aP{P, sizeof(P), false, nullptr};
-  int rc = stage(c, {&ap, &ax, &ae, &aP});
+  int rc = stage(c, {&ap, &ax, &ae});
   if (rc) return rc;
-  const double* Pd = (const double*)aP.dev;
-  return finish(c, launch_triangulate(n, (const double*)ap.dev, Pd, Pd + 12, (double*)ax.dev, (double*)ae.dev,
-                                      c->stream));
+  return finish(c, launch_triangulate(n, (const double*)ap.dev, cams, (double*)ax.dev, (double*)ae.dev, c->stream));
+}
+
+int aldic_measure_fp32_peak(aldic_ctx* c, double* tflops) {
+  if (!c || !tflops) return ALDIC_ERR_ARG;
+  int dev = 0, sms = 148;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  c->arena.used = 0;
+  int rc = arena_reserve(c, 4096);
+  if (rc) return rc;
+  float* out = (float*)arena_take(c, 64);
+  const int threads = 256, blocks = sms * 8, iters = 2048;
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  launch_fp32_probe(blocks, threads, 64, out, c->stream);  // warm-up
+  CK(cudaEventRecord(e0, c->stream));
+  launch_fp32_probe(blocks, threads, iters, out, c->stream);
+  CK(cudaEventRecord(e1, c->stream));
+  CK(cudaEventSynchronize(e1));
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  c->launches += 2;
+  const double flops = 2.0 * 8 * 16 * (double)iters * threads * blocks;
+  *tflops = flops / (ms * 1e-3) / 1e12;
+  return ALDIC_OK;
 }
 
 }  // extern "C"

@@ -88,7 +88,11 @@ int launch_icgn(const IcgnArgs& a, int wmax_enlarged, cudaStream_t st);
 int launch_subpb1(const Sub1Args& a, int wmax_x, int wmax_y, cudaStream_t st);
 size_t search_smem_bytes(int winsize, int s0, int s1);
 int launch_search(const SearchArgs& a, cudaStream_t st);
-int launch_triangulate(long long n, const double* pairs, const double* PL, const double* PR, double* xyz,
-                       double* err, cudaStream_t st);
+struct CamPair {
+  double P[24];  // P_L = K_L [I | 0] then P_R = K_R [R | T], each 3x4 row-major
+};
+int launch_triangulate(long long n, const double* pairs, const CamPair& cams, double* xyz, double* err,
+                       cudaStream_t st);
+int launch_fp32_probe(int blocks, int threads, int iters, float* out, cudaStream_t st);
 
 }  // namespace aldic

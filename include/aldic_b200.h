@@ -139,6 +139,11 @@ int aldic_epipolar_icgn(aldic_ctx* ctx, int64_t n, const double* pts, int winsiz
 int aldic_triangulate(aldic_ctx* ctx, int64_t n, const double* pairs, const double* KL, const double* KR,
                       const double* R, const double* T, double* xyz, double* reproj_err);
 
+/* ------------------------------------------------------------- diagnostics ------- */
+/* Measured FP32 FMA throughput of the current device (TFLOP/s), the denominator the
+ * library's compute-bound kernels are reported against.  Not part of the reference. */
+int aldic_measure_fp32_peak(aldic_ctx* ctx, double* tflops);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1124,6 +1124,57 @@ void orc_search_grid(const int* gridx, const int* gridy, int winsize, int step, 
 // crop [w : end-w+1], findpeak; search = tempSizeOfSearchRegion as passed (length 2,
 // expanded to [left right up down] = [s0 s1 s0 s1] at :12).  Outputs are nY x nX
 // column-major (x, y, u, v, phi) and qf (nX*nY x 2, normalised as :184-187).
+// One subset of funIntegerSearchWholeField (func/funIntegerSearch.m:134-176): template
+// top-left (ii, jj) 1-based; gridx_end/gridy_end are gridx(end)/gridy(end) used by the
+// right/down clamps.  out5 = [u v phi pce ppe] (NaN / Inf on failure).
+static void search_one(const double* f, const double* g, int M, int N, const int* search, int gridx_end,
+                       int gridy_end, int ii, int jj, int w, double* out5) {
+  int L = search[0], R = search[1], Uu = search[0], D = search[1];
+  if (ii - L < 1) L = ii - 1;
+  if (jj - Uu < 1) Uu = jj - 1;
+  if (ii + w + R > M) R = gridx_end - ii - w - 1;
+  if (jj + w + D > N) D = gridy_end - jj - w - 1;
+  L = std::max(L, 0);
+  R = std::max(R, 0);
+  Uu = std::max(Uu, 0);
+  D = std::max(D, 0);
+  out5[0] = out5[1] = out5[2] = kNaN;
+  out5[3] = out5[4] = INFINITY;
+  const int m = w + 1;
+  const int ar0 = ii - L, ar1 = ii + w + R, ac0 = jj - Uu, ac1 = jj + w + D;
+  if (!(ii >= 1 && ii + w <= M && jj >= 1 && jj + w <= N && ar0 >= 1 && ar1 <= M && ac0 >= 1 && ac1 <= N)) return;
+  std::vector<double> T((size_t)m * m), A((size_t)(ar1 - ar0 + 1) * (ac1 - ac0 + 1));
+  for (int b = 0; b < m; ++b)
+    for (int a = 0; a < m; ++a) T[a + (size_t)b * m] = f[(ii - 1 + a) + (size_t)(jj - 1 + b) * M];
+  const int ma = ar1 - ar0 + 1, na = ac1 - ac0 + 1;
+  for (int b = 0; b < na; ++b)
+    for (int a = 0; a < ma; ++a) A[a + (size_t)b * ma] = g[(ar0 - 1 + a) + (size_t)(ac0 - 1 + b) * M];
+  std::vector<double> cc;
+  if (!normxcorr2(T.data(), m, m, A.data(), ma, na, &cc)) return;
+  qfactors(cc, &out5[3], &out5[4]);
+  const int R2 = ma + m - 1, C2 = na + m - 1;
+  const int cr = R2 - 2 * w + 2, ccn = C2 - 2 * w + 2;
+  std::vector<double> crop((size_t)cr * ccn);
+  for (int b = 0; b < ccn; ++b)
+    for (int a = 0; a < cr; ++a) crop[a + (size_t)b * cr] = cc[(w - 1 + a) + (size_t)(w - 1 + b) * R2];
+  double xp, yp, mf;
+  findpeak(crop.data(), cr, ccn, &xp, &yp, &mf);
+  out5[0] = yp - 2 - L;
+  out5[1] = xp - 2 - Uu;
+  out5[2] = mf;
+}
+
+// A list of grid subsets (template top-lefts ii[k], jj[k]) searched in parallel, for
+// sampled checks and CPU timing; out is n x 5 row-major [u v phi pce ppe].
+void orc_search_list(const double* f, const double* g, int M, int N, const int* search, int gridx_end,
+                     int gridy_end, long n, const int* ii, const int* jj, int w, double* out, int nthreads) {
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#endif
+#pragma omp parallel for schedule(dynamic, 1)
+  for (long k = 0; k < n; ++k) search_one(f, g, M, N, search, gridx_end, gridy_end, ii[k], jj[k], w, out + 5 * k);
+}
+
 void orc_integer_search(const double* f, const double* g, int M, int N, const int* search, const int* gridx,
                         const int* gridy, int winsize, int step, double* x, double* y, double* u, double* v,
                         double* phi, double* qf, int nthreads) {
@@ -1131,7 +1182,6 @@ void orc_integer_search(const double* f, const double* g, int M, int N, const in
   orc_search_grid(gridx, gridy, winsize, step, &nX, &nY);
   const long n = (long)nX * nY;
   const int w = winsize;
-  const int reg0[4] = {search[0], search[1], search[0], search[1]};
   std::vector<double> q0(n), q1(n);
 #ifdef _OPENMP
   if (nthreads > 0) omp_set_num_threads(nthreads);
@@ -1140,42 +1190,9 @@ void orc_integer_search(const double* f, const double* g, int M, int N, const in
   for (long t = 0; t < n; ++t) {
     const int i = (int)(t % nX), j = (int)(t / nX);
     const int ii = gridx[0] + i * step, jj = gridy[0] + j * step;
-    int L = reg0[0], R = reg0[1], Uu = reg0[2], D = reg0[3];
-    if (ii - L < 1) L = ii - 1;
-    if (jj - Uu < 1) Uu = jj - 1;
-    if (ii + w + R > M) R = gridx[1] - ii - w - 1;
-    if (jj + w + D > N) D = gridy[1] - jj - w - 1;
-    L = std::max(L, 0);
-    R = std::max(R, 0);
-    Uu = std::max(Uu, 0);
-    D = std::max(D, 0);
-    double uu = kNaN, vv = kNaN, pp = kNaN, qa = INFINITY, qb = INFINITY;
-    const int m = w + 1;
-    const int ar0 = ii - L, ar1 = ii + w + R, ac0 = jj - Uu, ac1 = jj + w + D;
-    bool ok = (ii >= 1 && ii + w <= M && jj >= 1 && jj + w <= N && ar0 >= 1 && ar1 <= M && ac0 >= 1 && ac1 <= N);
-    if (ok) {
-      std::vector<double> T((size_t)m * m), A((size_t)(ar1 - ar0 + 1) * (ac1 - ac0 + 1));
-      for (int b = 0; b < m; ++b)
-        for (int a = 0; a < m; ++a) T[a + (size_t)b * m] = f[(ii - 1 + a) + (size_t)(jj - 1 + b) * M];
-      const int ma = ar1 - ar0 + 1, na = ac1 - ac0 + 1;
-      for (int b = 0; b < na; ++b)
-        for (int a = 0; a < ma; ++a) A[a + (size_t)b * ma] = g[(ar0 - 1 + a) + (size_t)(ac0 - 1 + b) * M];
-      std::vector<double> cc;
-      if (normxcorr2(T.data(), m, m, A.data(), ma, na, &cc)) {
-        qfactors(cc, &qa, &qb);
-        const int R2 = ma + m - 1, C2 = na + m - 1;
-        // crop rows w..R2-w+1, cols w..C2-w+1 (1-based)
-        const int cr = R2 - 2 * w + 2, ccn = C2 - 2 * w + 2;
-        std::vector<double> crop((size_t)cr * ccn);
-        for (int b = 0; b < ccn; ++b)
-          for (int a = 0; a < cr; ++a) crop[a + (size_t)b * cr] = cc[(w - 1 + a) + (size_t)(w - 1 + b) * R2];
-        double xp, yp, mf;
-        findpeak(crop.data(), cr, ccn, &xp, &yp, &mf);
-        uu = yp - 2 - L;
-        vv = xp - 2 - Uu;
-        pp = mf;
-      }
-    }
+    double r5[5];
+    search_one(f, g, M, N, search, gridx[1], gridy[1], ii, jj, w, r5);
+    const double uu = r5[0], vv = r5[1], pp = r5[2], qa = r5[3], qb = r5[4];
     const long o = j + (long)i * nY;
     u[o] = uu;
     v[o] = vv;

@@ -53,6 +53,8 @@ def lib():
         L.orc_search_grid.argtypes = [_ip, _ip, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.orc_integer_search.argtypes = [_dp, _dp, C.c_int, C.c_int, _ip, _ip, _ip, C.c_int, C.c_int, _dp, _dp,
                                          _dp, _dp, _dp, C.c_void_p, C.c_int]
+        L.orc_search_list.argtypes = [_dp, _dp, C.c_int, C.c_int, _ip, C.c_int, C.c_int, C.c_long, _ip, _ip,
+                                      C.c_int, _dp, C.c_int]
         L.orc_findpeak.argtypes = [_dp, C.c_int, C.c_int, _dp]
         L.orc_normxcorr2.argtypes = [_dp, C.c_int, C.c_int, _dp, C.c_int, C.c_int, _dp]
         L.orc_normxcorr2.restype = C.c_int
@@ -210,6 +212,22 @@ def integer_search(f, g, search, gridx, gridy, winsize, step, nthreads=0, want_q
                              None if qf is None else qf.ctypes.data, nthreads)
     x, y, u, v, phi = [o.reshape((ny, nx), order="F") for o in outs]
     return dict(x=x, y=y, u=u, v=v, phi=phi, qf=None if qf is None else qf.reshape((nx * ny, 2), order="F"))
+
+
+def search_list(f, g, search, gridx_end, gridy_end, ii, jj, winsize, nthreads=0):
+    """Selected subsets of funIntegerSearchWholeField: template top-lefts (ii, jj),
+    gridx(end)/gridy(end) of the run they belong to.  Returns n x 5 [u v phi pce ppe]."""
+    f = np.asarray(f, dtype=np.float64)
+    M, N = f.shape
+    ii = _flat(ii, np.int32)
+    jj = _flat(jj, np.int32)
+    s = np.asarray(search, dtype=np.int32).ravel()
+    if s.size == 1:
+        s = np.array([s[0], s[0]], dtype=np.int32)
+    out = np.empty(5 * ii.size)
+    lib().orc_search_list(_f64(f), _f64(g), M, N, _flat(s, np.int32), int(gridx_end), int(gridy_end), ii.size,
+                          ii, jj, int(winsize), out, nthreads)
+    return out.reshape(-1, 5)
 
 
 def findpeak(f):

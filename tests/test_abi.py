@@ -1,0 +1,78 @@
+"""CPU tests of the C ABI boundary: the library loads, exports every symbol that
+include/aldic_b200.h declares, and fails loudly (no CPU fallback) without a device."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "aldic_b200.h")
+
+
+def header_functions():
+    txt = open(HEADER).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(aldic_[a-z0-9_]+)\s*\(", txt)))
+
+
+def test_library_exports_every_declared_symbol():
+    import aldic_b200
+
+    lib = aldic_b200.load_library()
+    names = header_functions()
+    assert len(names) >= 20
+    for name in names:
+        assert hasattr(lib, name), name
+    from aldic_b200 import _lib
+
+    assert set(names) == set(_lib.SIGNATURES), "ctypes signatures out of sync with the header"
+
+
+def test_abi_version_and_grid_without_device():
+    import aldic_b200
+
+    lib = aldic_b200.load_library()
+    assert lib.aldic_abi_version() == 1
+    gx = np.array([1, 512], dtype=np.int32)
+    gy = np.array([1, 512], dtype=np.int32)
+    nx, ny = C.c_int(), C.c_int()
+    rc = lib.aldic_search_grid(C.c_void_p(gx.ctypes.data), C.c_void_p(gy.ctypes.data), 30, 16, C.byref(nx),
+                               C.byref(ny))
+    assert rc == 0 and (nx.value, ny.value) == (30, 30)  # XList = 1:16:466 (funIntegerSearch.m:106)
+
+
+def test_grid_matches_oracle():
+    import aldic_b200
+    import oracle as O
+
+    lib = aldic_b200.load_library()
+    for gx, gy, w, st in (([1, 2048], [1, 2048], 40, 10), ([5, 300], [9, 280], 20, 7), ([1, 60], [1, 60], 40, 30)):
+        a = np.array(gx, dtype=np.int32)
+        b = np.array(gy, dtype=np.int32)
+        nx, ny = C.c_int(), C.c_int()
+        lib.aldic_search_grid(C.c_void_p(a.ctypes.data), C.c_void_p(b.ctypes.data), w, st, C.byref(nx), C.byref(ny))
+        assert (nx.value, ny.value) == O.search_grid(gx, gy, w, st)
+
+
+def test_no_cpu_fallback_without_gpu():
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    import aldic_b200
+
+    with pytest.raises(aldic_b200.AldicError):
+        aldic_b200.Context(0)
+    with pytest.raises(aldic_b200.AldicError):
+        aldic_b200.ba_interp2_spline(np.zeros((10, 10)), [1.0], [1.0])
+
+
+def test_null_context_is_rejected():
+    import aldic_b200
+
+    lib = aldic_b200.load_library()
+    assert lib.aldic_compute_gradients(None) == 1
+    assert lib.aldic_local_icgn(None, 1, 0, None, None, 30, 1e-3, None, None, None, None, None) == 1
+    assert lib.aldic_last_error(None) == b"null context"
