@@ -50,6 +50,7 @@ struct aldic_ctx {
   int* qcount = nullptr;
   double* I1 = nullptr;
   double* I2 = nullptr;
+  double* iitot = nullptr;
   size_t ii_cap = 0;
   Arena arena;
   // outputs to copy back at the end of a call
@@ -242,7 +243,7 @@ void aldic_destroy(aldic_ctx* c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   void* bufs[] = {c->img[0], c->img[1], c->mask, c->gx, c->gy, c->stats, c->partials, c->counter, c->qcount,
-                  c->I1, c->I2, c->arena.base};
+                  c->I1, c->I2, c->iitot, c->arena.base};
   for (void* b : bufs)
     if (b) cudaFree(b);
   if (c->own) cudaStreamDestroy(c->own);
@@ -411,8 +412,8 @@ int aldic_integer_search(aldic_ctx* c, const int* search, const int* gridx, cons
   if (!search || !gridx || !gridy) return fail(c, ALDIC_ERR_ARG, "search/gridx/gridy required");
   if (winsize < 2 || step < 1) return fail(c, ALDIC_ERR_ARG, "winsize >= 2 and step >= 1 required");
   if (search[0] < 0 || search[1] < 0) return fail(c, ALDIC_ERR_ARG, "search region must be non-negative");
-  if ((size_t)(winsize + 1) * (winsize + 1) > 120 * 120)
-    return fail(c, ALDIC_ERR_ARG, "winsize %d too large for the device search", winsize);
+  if (winsize > 120) return fail(c, ALDIC_ERR_ARG, "winsize %d too large for the device search", winsize);
+  if (search[0] + search[1] > 2000) return fail(c, ALDIC_ERR_ARG, "search region too large");
   int nx, ny;
   aldic_search_grid(gridx, gridy, winsize, step, &nx, &ny);
   const size_t n = (size_t)nx * ny;
@@ -423,9 +424,11 @@ int aldic_integer_search(aldic_ctx* c, const int* search, const int* gridx, cons
     CK(cudaStreamSynchronize(c->stream));
     if (c->I1) CK(cudaFree(c->I1));
     if (c->I2) CK(cudaFree(c->I2));
-    c->I1 = c->I2 = nullptr;
+    if (c->iitot) CK(cudaFree(c->iitot));
+    c->I1 = c->I2 = c->iitot = nullptr;
     CK(cudaMalloc(&c->I1, iin * sizeof(double)));
     CK(cudaMalloc(&c->I2, iin * sizeof(double)));
+    CK(cudaMalloc(&c->iitot, search_tot_bytes(c->M, c->N)));
     c->ii_cap = iin;
   }
   Arg ox{x, n * 8, true, nullptr}, oy{y, n * 8, true, nullptr}, ou{u, n * 8, true, nullptr};
@@ -454,6 +457,7 @@ int aldic_integer_search(aldic_ctx* c, const int* search, const int* gridx, cons
   a.phi = (double*)op.dev;
   a.I1 = c->I1;
   a.I2 = c->I2;
+  a.tot = c->iitot;
   return finish(c, launch_search(a, c->stream));
 }
 

@@ -96,6 +96,24 @@ __device__ __forceinline__ void block_sum(double (&v)[K], double* scratch, doubl
   __syncthreads();
 }
 
+// Block-wide sums for a runtime number of warps (scratch holds nwarps*K doubles).
+template <int K>
+__device__ __forceinline__ void block_sum_dyn(double (&v)[K], double* scratch, double* out, int nwarps) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const double s = warp_sum(v[k]);
+    if (lane == 0) scratch[warp * K + k] = s;
+  }
+  __syncthreads();
+  if (threadIdx.x < K) {
+    double s = 0;
+    for (int w = 0; w < nwarps; ++w) s += scratch[w * K + threadIdx.x];
+    out[threadIdx.x] = s;
+  }
+  __syncthreads();
+}
+
 // ---------------------------------------------------------------------------------
 // bwselect: connected component of `on` pixels (rows x cols, column-major, u8) that
 // contains the 0-based seed (sr, sc), 4- or 8-connected, into `lab` (u8).  Iterated

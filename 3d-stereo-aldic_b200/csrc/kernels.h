@@ -68,8 +68,9 @@ struct SearchArgs {
   double* u;
   double* v;
   double* phi;
-  double* I1;  // (M+1) x (N+1) integral images of g and g^2 (scratch)
+  double* I1;   // (M+1) x (N+1) integral images of g and g^2 (scratch)
   double* I2;
+  double* tot;  // row-pass chunk totals (scratch, search_tot_bytes)
 };
 
 // launchers return the number of kernels they enqueued (or < 0 on argument errors)
@@ -87,6 +88,7 @@ size_t sub1_smem_bytes(int wx, int wy);
 int launch_icgn(const IcgnArgs& a, int wmax_enlarged, cudaStream_t st);
 int launch_subpb1(const Sub1Args& a, int wmax_x, int wmax_y, cudaStream_t st);
 size_t search_smem_bytes(int winsize, int s0, int s1);
+size_t search_tot_bytes(int M, int N);
 int launch_search(const SearchArgs& a, cudaStream_t st);
 struct CamPair {
   double P[24];  // P_L = K_L [I | 0] then P_R = K_R [R | T], each 3x4 row-major

@@ -18,50 +18,101 @@
 
 namespace aldic {
 
-constexpr int SNT = 256;  // threads per search CTA
-constexpr int STA = 64;   // shift tile rows
-constexpr int STB = 64;   // shift tile columns
 
 __host__ __device__ inline int round_up8(int v) { return (v + 7) & ~7; }
+__host__ __device__ inline int round_up16(int v) { return (v + 15) & ~15; }
 
-// Column prefix sums: II(r+1, c+1) = sum_{r' <= r} g(r', c) (and of g^2); II is
+// Integral images of g and g^2 in FP64: II(r, c) = sum over rows < r and columns < c;
 // (M+1) x (N+1) column-major, row 0 and column 0 zero.
+//
+// Pass 1 (one warp per image column, coalesced): column prefix sums by warp scans.
 __global__ void integral_cols_kernel(const float* __restrict__ g, int M, int N, double* __restrict__ I1,
                                      double* __restrict__ I2) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   const size_t ld = (size_t)M + 1;
-  if (c > N) return;
-  if (c == 0) {
-    for (int r = 0; r <= M; ++r) {
-      I1[r] = 0.0;
-      I2[r] = 0.0;
+  if (warp > N) return;
+  double* c1 = I1 + (size_t)warp * ld;
+  double* c2 = I2 + (size_t)warp * ld;
+  if (warp == 0) {  // column 0 is zero
+    for (int r = lane; r <= M; r += 32) {
+      c1[r] = 0.0;
+      c2[r] = 0.0;
     }
     return;
   }
-  double s1 = 0, s2 = 0;
-  I1[(size_t)c * ld] = 0.0;
-  I2[(size_t)c * ld] = 0.0;
-  const float* col = g + (size_t)(c - 1) * M;
-  for (int r = 0; r < M; ++r) {
-    const double v = col[r];
-    s1 += v;
-    s2 += v * v;
-    I1[(size_t)(r + 1) + (size_t)c * ld] = s1;
-    I2[(size_t)(r + 1) + (size_t)c * ld] = s2;
+  const float* col = g + (size_t)(warp - 1) * M;
+  if (lane == 0) {
+    c1[0] = 0.0;
+    c2[0] = 0.0;
+  }
+  double carry1 = 0.0, carry2 = 0.0;
+  for (int r0 = 0; r0 < M; r0 += 32) {
+    const int r = r0 + lane;
+    const double v = r < M ? (double)col[r] : 0.0;
+    double s1 = v, s2 = v * v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const double t1 = __shfl_up_sync(0xffffffffu, s1, o), t2 = __shfl_up_sync(0xffffffffu, s2, o);
+      if (lane >= o) {
+        s1 += t1;
+        s2 += t2;
+      }
+    }
+    s1 += carry1;
+    s2 += carry2;
+    if (r < M) {
+      c1[r + 1] = s1;
+      c2[r + 1] = s2;
+    }
+    carry1 = __shfl_sync(0xffffffffu, s1, 31);
+    carry2 = __shfl_sync(0xffffffffu, s2, 31);
   }
 }
 
-// Row prefix of the column prefixes -> full integral image.
-__global__ void integral_rows_kernel(int M, int N, double* __restrict__ I1, double* __restrict__ I2) {
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r > M) return;
+constexpr int kRowChunk = 64;  // columns per thread in the row pass
+
+// Pass 2a: within each chunk of kRowChunk columns, prefix along the row (one thread per
+// (row, chunk); consecutive threads take consecutive rows: coalesced).  Chunk totals go
+// to tot (nchunk x (M+1)).
+__global__ void integral_rows_local_kernel(int M, int N, double* __restrict__ I1, double* __restrict__ I2,
+                                           double* __restrict__ tot) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const int rows = M + 1;
+  const int nchunk = (N + kRowChunk - 1) / kRowChunk;
+  if (t >= (long long)rows * nchunk) return;
+  const int r = (int)(t % rows), ch = (int)(t / rows);
   const size_t ld = (size_t)M + 1;
+  const int c0 = 1 + ch * kRowChunk, c1 = min(N, c0 + kRowChunk - 1);
   double s1 = 0, s2 = 0;
-  for (int c = 1; c <= N; ++c) {
+  for (int c = c0; c <= c1; ++c) {
     s1 += I1[r + c * ld];
     s2 += I2[r + c * ld];
     I1[r + c * ld] = s1;
     I2[r + c * ld] = s2;
+  }
+  tot[2 * ((size_t)ch * rows + r)] = s1;
+  tot[2 * ((size_t)ch * rows + r) + 1] = s2;
+}
+
+// Pass 2b: add the totals of the preceding chunks of the row.
+__global__ void integral_rows_fix_kernel(int M, int N, double* __restrict__ I1, double* __restrict__ I2,
+                                         const double* __restrict__ tot) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const int rows = M + 1;
+  const int nchunk = (N + kRowChunk - 1) / kRowChunk;
+  if (t >= (long long)rows * nchunk) return;
+  const int r = (int)(t % rows), ch = (int)(t / rows);
+  if (ch == 0) return;
+  double o1 = 0, o2 = 0;
+  for (int k = 0; k < ch; ++k) {
+    o1 += tot[2 * ((size_t)k * rows + r)];
+    o2 += tot[2 * ((size_t)k * rows + r) + 1];
+  }
+  const size_t ld = (size_t)M + 1;
+  const int c0 = 1 + ch * kRowChunk, c1 = min(N, c0 + kRowChunk - 1);
+  for (int c = c0; c <= c1; ++c) {
+    I1[r + c * ld] += o1;
+    I2[r + c * ld] += o2;
   }
 }
 
@@ -118,25 +169,43 @@ __device__ __forceinline__ double matlab_eps_d(double x) {
   return nextafter(x, INFINITY) - x;
 }
 
-__global__ void __launch_bounds__(SNT, 2) ncc_search_kernel(SearchArgs a) {
+// Shared-memory layout of one subset: the centred template (TR x W1, rows >= W1 zero)
+// and the padded search window Dpad restricted to the current strip of shift columns
+// (DR x DC, zero outside the cut-out window D).
+struct SearchLayout {
+  int W1, TR, DR, DC, strip_b;  // strip_b = shift columns covered per strip
+};
+
+__host__ __device__ inline SearchLayout search_layout(int w, int na_max, int strip_b) {
+  SearchLayout L;
+  L.W1 = w + 1;
+  L.TR = round_up8(L.W1);
+  L.DR = (round_up8(na_max) + L.TR - 1) | 1;  // rows a0 .. a0 + TR + 6 for every 8-row block
+  L.strip_b = strip_b;
+  L.DC = round_up16(strip_b) + w;               // columns b + j for b < round_up16(strip_b)
+  return L;
+}
+
+// One CTA per subset (grid-stride).  Each warp task covers 32 shift rows (4 lanes x 8
+// consecutive rows) x 16 shift columns (8 lanes x the column pair b, b + 8): with an odd
+// leading dimension the 32 lanes of every window load hit 32 different banks.
+__global__ void __launch_bounds__(512, 1) ncc_search_kernel(SearchArgs a, int strip_b, int na_max) {
   const double* __restrict__ I1 = a.I1;
   const double* __restrict__ I2 = a.I2;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ double red[(SNT / 32) * 10];
+  __shared__ double red[16 * 10];
   __shared__ double sums[10];
-  __shared__ float sbest[SNT / 32];
-  __shared__ int sidx[SNT / 32];
+  __shared__ float sbest[16];
+  __shared__ int sidx[16];
   __shared__ double s_tmean, s_denT, s_tolz;
   __shared__ int s_peak;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int w = a.winsize, W1 = w + 1;
-  const int TR = round_up8(W1);
-  const int DR = (STA + TR) | 1;  // odd leading dimension: conflict-free column loads
-  const int DC = STB + w;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+  const int w = a.winsize;
+  const SearchLayout Ly = search_layout(w, na_max, strip_b);
+  const int W1 = Ly.W1, TR = Ly.TR, DR = Ly.DR, DC = Ly.DC;
   const size_t ld = (size_t)a.M + 1;
-  float* Tp = reinterpret_cast<float*>(smem_raw);  // TR x W1 (rows >= W1 are zero)
-  float* Dt = Tp + TR * W1;                         // DR x DC tile of the padded window
-  float* den_t = Dt + (size_t)DR * DC;              // STA x STB
+  float* Tp = reinterpret_cast<float*>(smem_raw);
+  float* Dt = Tp + TR * W1;
   const long long n = (long long)a.nx * a.ny;
   for (long long t = blockIdx.x; t < n; t += gridDim.x) {
     const SubsetGeom s = subset_geom(a, t);
@@ -146,23 +215,23 @@ __global__ void __launch_bounds__(SNT, 2) ncc_search_kernel(SearchArgs a) {
       a.x[o] = (s.ii + s.ii + w) / 2.0;
       a.y[o] = (s.jj + s.jj + w) / 2.0;
     }
-    if (!s.ok) {
+    if (!s.ok || s.na > na_max) {
       if (tid == 0) a.u[o] = a.v[o] = a.phi[o] = ALDIC_NAN;
       continue;
     }
     // ---- template: mean, centred FP32 copy, FP64 norm ----
     {
       double v[1] = {0};
-      for (int p = tid; p < W1 * W1; p += SNT) {
+      for (int p = tid; p < W1 * W1; p += blockDim.x) {
         const int i = p % W1, j = p / W1;
         v[0] += (double)a.f[(size_t)(s.ii - 1 + i) + (size_t)(s.jj - 1 + j) * a.M];
       }
-      block_sum<1, SNT>(v, red, sums);
+      block_sum_dyn<1>(v, red, sums, nwarps);
       if (tid == 0) s_tmean = sums[0] / (double)(W1 * W1);
       __syncthreads();
       const double tm = s_tmean;
       double ss[1] = {0};
-      for (int p = tid; p < TR * W1; p += SNT) {
+      for (int p = tid; p < TR * W1; p += blockDim.x) {
         const int i = p % TR, j = p / TR;
         float tv = 0.f;
         if (i < W1) {
@@ -172,7 +241,7 @@ __global__ void __launch_bounds__(SNT, 2) ncc_search_kernel(SearchArgs a) {
         }
         Tp[i + j * TR] = tv;
       }
-      block_sum<1, SNT>(ss, red, sums);
+      block_sum_dyn<1>(ss, red, sums, nwarps);
       if (tid == 0) s_denT = sqrt(sums[0]);
       __syncthreads();
     }
@@ -183,10 +252,10 @@ __global__ void __launch_bounds__(SNT, 2) ncc_search_kernel(SearchArgs a) {
       continue;
     }
     const double nwin = (double)W1 * W1;
-    // ---- pre-pass: largest denominator over the crop (normxcorr2 zero threshold) ----
+    // ---- largest denominator over the crop (normxcorr2 zero threshold) ----
     {
       double dmax = 0;
-      for (int k = tid; k < s.na * s.nb; k += SNT) {
+      for (int k = tid; k < s.na * s.nb; k += blockDim.x) {
         double S1, S2;
         window_sums(s, w, k % s.na, k / s.na, I1, I2, ld, &S1, &S2);
         dmax = fmax(dmax, denT * sqrt(fmax(S2 - S1 * S1 / nwin, 0.0)));
@@ -196,106 +265,98 @@ __global__ void __launch_bounds__(SNT, 2) ncc_search_kernel(SearchArgs a) {
       __syncthreads();
       if (tid == 0) {
         double m = 0;
-        for (int i = 0; i < SNT / 32; ++i) m = fmax(m, red[i]);
+        for (int i = 0; i < nwarps; ++i) m = fmax(m, red[i]);
         s_tolz = sqrt(matlab_eps_d(m));
       }
       __syncthreads();
     }
     const double tolz = s_tolz;
-    const float one_tol = 1.4901161193847656e-08f;  // sqrt(eps(1))
     float best = -INFINITY;
     int bidx = 0x7fffffff;
-    // task of this thread inside a 64 x 64 tile: 8 shift rows x shift columns (b, b+8)
     const int la = lane & 3, lb = lane >> 2;
-    const int wa = warp & 1, wb = warp >> 1;
-    const int a0 = (wa * 4 + la) * 8;
-    const int b0 = wb * 16 + lb;
-    for (int ta0 = 0; ta0 < s.na; ta0 += STA)
-      for (int tb0 = 0; tb0 < s.nb; tb0 += STB) {
-        // load the tile of the padded window: Dpad(p, q) = g at image (dr0-1+p, dc0-1+q)
-        // inside D, zero outside
-        for (int k = tid; k < DR * DC; k += SNT) {
-          const int p = ta0 + k % DR, q = tb0 + k / DR;
-          const int r = s.dr0 - 1 + p, c = s.dc0 - 1 + q;
-          float v = 0.f;
-          if (r >= s.dr0 && r <= s.dr1 && c >= s.dc0 && c <= s.dc1) v = __ldg(a.g + (size_t)r + (size_t)c * a.M);
-          Dt[k] = v;
+    const int ablocks = (s.na + 31) / 32;
+    for (int tb0 = 0; tb0 < s.nb; tb0 += Ly.strip_b) {
+      const int nbs = min(Ly.strip_b, s.nb - tb0);
+      // padded window for this strip: Dpad(p, tb0 + q) = g at image (dr0-1+p, dc0-1+tb0+q)
+      for (int k = tid; k < DR * DC; k += blockDim.x) {
+        const int p = k % DR, q = tb0 + k / DR;
+        const int r = s.dr0 - 1 + p, c = s.dc0 - 1 + q;
+        float v = 0.f;
+        if (r >= s.dr0 && r <= s.dr1 && c >= s.dc0 && c <= s.dc1) v = __ldg(a.g + (size_t)r + (size_t)c * a.M);
+        Dt[k] = v;
+      }
+      __syncthreads();
+      const int bgroups = (nbs + 15) / 16;
+      for (int task = warp; task < ablocks * bgroups; task += nwarps) {
+        const int a0 = (task % ablocks) * 32 + la * 8;
+        const int bl = (task / ablocks) * 16 + lb;  // strip-local shift column
+        if (a0 >= s.na || bl >= nbs) continue;
+        double acc0[8], acc1[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          acc0[k] = 0.0;
+          acc1[k] = 0.0;
         }
-        for (int k = tid; k < STA * STB; k += SNT) {
-          const int aa = ta0 + k % STA, bb = tb0 + k / STA;
-          float dv = -1.f;
-          if (aa < s.na && bb < s.nb) {
+        for (int j = 0; j < W1; ++j) {
+          const float* c0 = Dt + (size_t)(bl + j) * DR + a0;
+          const float* c1 = c0 + 8 * (size_t)DR;
+          const float* tj = Tp + j * TR;
+          float p0[8], p1[8];
+#pragma unroll
+          for (int k = 0; k < 8; ++k) {
+            p0[k] = 0.f;
+            p1[k] = 0.f;
+          }
+          for (int i0 = 0; i0 < TR; i0 += 8) {
+            float w0[15], w1[15];
+#pragma unroll
+            for (int m = 0; m < 15; ++m) {
+              w0[m] = c0[i0 + m];
+              w1[m] = c1[i0 + m];
+            }
+            const float4 ta = *reinterpret_cast<const float4*>(tj + i0);
+            const float4 tb = *reinterpret_cast<const float4*>(tj + i0 + 4);
+            const float tv[8] = {ta.x, ta.y, ta.z, ta.w, tb.x, tb.y, tb.z, tb.w};
+#pragma unroll
+            for (int s8 = 0; s8 < 8; ++s8) {
+#pragma unroll
+              for (int k = 0; k < 8; ++k) {
+                p0[k] = fmaf(tv[s8], w0[k + s8], p0[k]);
+                p1[k] = fmaf(tv[s8], w1[k + s8], p1[k]);
+              }
+            }
+          }
+#pragma unroll
+          for (int k = 0; k < 8; ++k) {
+            acc0[k] += (double)p0[k];
+            acc1[k] += (double)p1[k];
+          }
+        }
+        // NCC with the zero rules, running first maximum in column-major crop order
+#pragma unroll
+        for (int half = 0; half < 2; ++half) {
+          const int bb = tb0 + bl + 8 * half;
+          if (bl + 8 * half >= nbs) continue;
+#pragma unroll
+          for (int k = 0; k < 8; ++k) {
+            const int aa = a0 + k;
+            if (aa >= s.na) continue;
             double S1, S2;
             window_sums(s, w, aa, bb, I1, I2, ld, &S1, &S2);
             const double den = denT * sqrt(fmax(S2 - S1 * S1 / nwin, 0.0));
-            dv = (den > tolz) ? (float)den : -1.f;
-          }
-          den_t[k] = dv;
-        }
-        __syncthreads();
-        if (ta0 + a0 < s.na && tb0 + b0 < s.nb) {
-          double acc0[8], acc1[8];
-#pragma unroll
-          for (int k = 0; k < 8; ++k) {
-            acc0[k] = 0.0;
-            acc1[k] = 0.0;
-          }
-          for (int j = 0; j < W1; ++j) {
-            const float* c0 = Dt + (size_t)(b0 + j) * DR + a0;
-            const float* c1 = c0 + 8 * (size_t)DR;
-            const float* tj = Tp + j * TR;
-            float p0[8], p1[8];
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-              p0[k] = 0.f;
-              p1[k] = 0.f;
-            }
-            for (int i0 = 0; i0 < TR; i0 += 8) {
-              float w0[15], w1[15];
-#pragma unroll
-              for (int m = 0; m < 15; ++m) {
-                w0[m] = c0[i0 + m];
-                w1[m] = c1[i0 + m];
-              }
-#pragma unroll
-              for (int sidx8 = 0; sidx8 < 8; ++sidx8) {
-                const float tv = tj[i0 + sidx8];
-#pragma unroll
-                for (int k = 0; k < 8; ++k) {
-                  p0[k] = fmaf(tv, w0[k + sidx8], p0[k]);
-                  p1[k] = fmaf(tv, w1[k + sidx8], p1[k]);
-                }
-              }
-            }
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-              acc0[k] += (double)p0[k];
-              acc1[k] += (double)p1[k];
-            }
-          }
-          // NCC, zero rules, running first-max in column-major crop order
-#pragma unroll
-          for (int half = 0; half < 2; ++half) {
-            const int bb = tb0 + b0 + 8 * half;
-            if (bb >= s.nb) continue;
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-              const int aa = ta0 + a0 + k;
-              if (aa >= s.na) continue;
-              const float dv = den_t[(a0 + k) + (b0 + 8 * half) * STA];
-              float cval = 0.f;
-              if (dv > 0.f) cval = (float)((half ? acc1[k] : acc0[k]) / (double)dv);
-              if (fabsf(cval) - 1.f > one_tol) cval = 0.f;
-              const int lin = aa + bb * s.na;
-              if (cval > best || (cval == best && lin < bidx)) {
-                best = cval;
-                bidx = lin;
-              }
+            float cval = 0.f;
+            if (den > tolz) cval = (float)((half ? acc1[k] : acc0[k]) / den);
+            if (fabsf(cval) - 1.f > 1.4901161193847656e-08f) cval = 0.f;
+            const int lin = aa + bb * s.na;
+            if (cval > best || (cval == best && lin < bidx)) {
+              best = cval;
+              bidx = lin;
             }
           }
         }
-        __syncthreads();
       }
+      __syncthreads();
+    }
     // ---- block argmax (max value, then smallest column-major index) ----
     for (int off = 16; off > 0; off >>= 1) {
       const float ob = __shfl_xor_sync(0xffffffffu, best, off);
@@ -313,7 +374,7 @@ __global__ void __launch_bounds__(SNT, 2) ncc_search_kernel(SearchArgs a) {
     if (tid == 0) {
       float b = sbest[0];
       int bi = sidx[0];
-      for (int i = 1; i < SNT / 32; ++i)
+      for (int i = 1; i < nwarps; ++i)
         if (sbest[i] > b || (sbest[i] == b && sidx[i] < bi)) {
           b = sbest[i];
           bi = sidx[i];
@@ -328,7 +389,7 @@ __global__ void __launch_bounds__(SNT, 2) ncc_search_kernel(SearchArgs a) {
 #pragma unroll
       for (int k = 0; k < 9; ++k) v[k] = 0.0;
       const double tm = s_tmean;
-      for (int p = tid; p < W1 * W1; p += SNT) {
+      for (int p = tid; p < W1 * W1; p += blockDim.x) {
         const int i = p % W1, j = p / W1;
         const double tv = (double)a.f[(size_t)(s.ii - 1 + i) + (size_t)(s.jj - 1 + j) * a.M] - tm;
 #pragma unroll
@@ -340,7 +401,7 @@ __global__ void __launch_bounds__(SNT, 2) ncc_search_kernel(SearchArgs a) {
           v[k] += tv * d;
         }
       }
-      block_sum<9, SNT>(v, red, sums);
+      block_sum_dyn<9>(v, red, sums, nwarps);
     }
     if (tid == 0) {
       double cc[9];
@@ -371,7 +432,7 @@ __global__ void __launch_bounds__(SNT, 2) ncc_search_kernel(SearchArgs a) {
             if (dy != 0) Sy2 += u;
           }
         const double A2 = Sx / 6.0, A3 = Sy / 6.0;
-        const double A4 = (cc[2 + 6] - cc[0 + 6] - cc[2 + 0] + cc[0 + 0]) / 4.0;
+        const double A4 = (cc[8] - cc[6] - cc[2] + cc[0]) / 4.0;
         const double A5 = Sx2 / 2.0 - S / 3.0, A6 = Sy2 / 2.0 - S / 3.0;
         const double A1 = (5.0 * S - 3.0 * (Sx2 + Sy2)) / 9.0;
         const double dd = A4 * A4 - 4 * A5 * A6;
@@ -393,32 +454,59 @@ __global__ void __launch_bounds__(SNT, 2) ncc_search_kernel(SearchArgs a) {
   }
 }
 
+// Largest crop size of any subset: interior subsets have na = s0 + s1 + 3.
+static int crop_max(int s0, int s1) { return s0 + s1 + 3; }
+
+// Columns of shifts per strip so that template + window fit in `budget` bytes.
+static int strip_columns(int w, int na_max, int nb_max, size_t budget) {
+  int sb = round_up16(nb_max);
+  while (sb > 16) {
+    const SearchLayout L = search_layout(w, na_max, sb);
+    const size_t bytes = sizeof(float) * ((size_t)L.TR * L.W1 + (size_t)L.DR * L.DC);
+    if (bytes <= budget) break;
+    sb -= 16;
+  }
+  return sb;
+}
+
 size_t search_smem_bytes(int winsize, int s0, int s1) {
-  (void)s0;
-  (void)s1;
-  const int W1 = winsize + 1;
-  const int TR = round_up8(W1);
-  const int DR = (STA + TR) | 1;
-  const int DC = STB + winsize;
-  return sizeof(float) * ((size_t)TR * W1 + (size_t)DR * DC + (size_t)STA * STB);
+  const int na = crop_max(s0, s1);
+  const int sb = strip_columns(winsize, na, na, 200 * 1024);
+  const SearchLayout L = search_layout(winsize, na, sb);
+  return sizeof(float) * ((size_t)L.TR * L.W1 + (size_t)L.DR * L.DC);
+}
+
+size_t search_tot_bytes(int M, int N) {
+  const int nchunk = (N + kRowChunk - 1) / kRowChunk;
+  return (size_t)nchunk * (M + 1) * 2 * sizeof(double);
 }
 
 int launch_search(const SearchArgs& a, cudaStream_t st) {
   const long long n = (long long)a.nx * a.ny;
   if (n <= 0) return 0;
-  integral_cols_kernel<<<(a.N + 1 + 127) / 128, 128, 0, st>>>(a.g, a.M, a.N, a.I1, a.I2);
-  integral_rows_kernel<<<(a.M + 1 + 127) / 128, 128, 0, st>>>(a.M, a.N, a.I1, a.I2);
-  const size_t smem = search_smem_bytes(a.winsize, a.s0, a.s1);
+  integral_cols_kernel<<<(unsigned)(((long long)(a.N + 1) * 32 + 255) / 256), 256, 0, st>>>(a.g, a.M, a.N, a.I1,
+                                                                                          a.I2);
+  const long long rt = (long long)(a.M + 1) * ((a.N + kRowChunk - 1) / kRowChunk);
+  integral_rows_local_kernel<<<(unsigned)((rt + 255) / 256), 256, 0, st>>>(a.M, a.N, a.I1, a.I2, a.tot);
+  integral_rows_fix_kernel<<<(unsigned)((rt + 255) / 256), 256, 0, st>>>(a.M, a.N, a.I1, a.I2, a.tot);
+  const int na = crop_max(a.s0, a.s1);
+  const int sb = strip_columns(a.winsize, na, na, 200 * 1024);
+  const SearchLayout L = search_layout(a.winsize, na, sb);
+  const size_t smem = sizeof(float) * ((size_t)L.TR * L.W1 + (size_t)L.DR * L.DC);
+  // warps: one per 32 x 16 block of shifts of an interior subset, at most 16
+  int nw = ((na + 31) / 32) * ((min(sb, na) + 15) / 16);
+  nw = nw < 2 ? 2 : (nw > 16 ? 16 : nw);
+  const int threads = nw * 32;
   cudaFuncSetAttribute(ncc_search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int dev = 0, sms = 148, per_sm = 1;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ncc_search_kernel, SNT, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ncc_search_kernel, threads, smem);
   if (per_sm < 1) per_sm = 1;
   long long grid = (long long)sms * per_sm;
   if (grid > n) grid = n;
-  ncc_search_kernel<<<(unsigned)grid, SNT, smem, st>>>(a);
-  return 3;
+  ncc_search_kernel<<<(unsigned)grid, threads, smem, st>>>(a, sb, na);
+  return 4;
 }
 
 }  // namespace aldic
