@@ -139,6 +139,25 @@ int aldic_epipolar_icgn(aldic_ctx* ctx, int64_t n, const double* pts, int winsiz
 int aldic_triangulate(aldic_ctx* ctx, int64_t n, const double* pairs, const double* KL, const double* KR,
                       const double* R, const double* T, double* xyz, double* reproj_err);
 
+/* ------------------------------------------------------ allocation-free IC-GN ---- */
+/* No counterpart in the reference.  aldic_local_icgn for callers that cannot allocate
+ * device memory (a host that owns every allocation: gpuArray buffers handed over by a
+ * MEX, a fixed memory budget or pool).  No context and no cudaMalloc/cudaFree: the work
+ * queue lives in a fixed file-scope device array sized for ALDIC_NOALLOC_MAX_SUBSETS
+ * subsets (~1.5 MB, held by every GPU that loads the library until exit).  Every array
+ * must be device memory on the current device: ref/def are the normalised FP32 images
+ * (M x N), mask is u8 (may be NULL), dfdx/dfdy are FP32 (M-6) x (N-6); the rest as
+ * aldic_local_icgn.  Work is queued on `stream` (NULL = legacy default stream) and not
+ * waited for.  n > ALDIC_NOALLOC_MAX_SUBSETS returns ALDIC_ERR_ARG.  All calls share the
+ * array, so calls that overlap on the GPU race and must be serialised by the caller; the
+ * first call on a device looks the array up (cudaGetSymbolAddress) and should come
+ * before any stream capture. */
+#define ALDIC_NOALLOC_MAX_SUBSETS 65536
+int aldic_local_icgn_noalloc(int variant, const float* ref, const float* def, const uint8_t* mask, const float* dfdx,
+                             const float* dfdy, int M, int N, int64_t n, const double* coords, const double* U0,
+                             int winsize, double tol, double* U, double* F, double* H, int32_t* conv,
+                             uint8_t* markHole, void* stream);
+
 /* ------------------------------------------------------------- diagnostics ------- */
 /* Measured FP32 FMA throughput of the current device (TFLOP/s), the denominator the
  * library's compute-bound kernels are reported against.  Not part of the reference. */
