@@ -96,6 +96,26 @@ __device__ __forceinline__ void block_sum(double (&v)[K], double* scratch, doubl
   __syncthreads();
 }
 
+// Block-wide FP64 sums of K per-thread FP32 partials, converting one value at a time so
+// that only the FP32 partials stay live (low register pressure for wide one-off sums).
+template <int K, int NT>
+__device__ __forceinline__ void block_sum_f32(float (&v)[K], double* scratch, double* out) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const double s = warp_sum((double)v[k]);
+    if (lane == 0) scratch[warp * K + k] = s;
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < K; k += NT) {
+    double s = 0;
+#pragma unroll
+    for (int w = 0; w < NT / 32; ++w) s += scratch[w * K + k];
+    out[k] = s;
+  }
+  __syncthreads();
+}
+
 // Block-wide sums for a runtime number of warps (scratch holds nwarps*K doubles).
 template <int K>
 __device__ __forceinline__ void block_sum_dyn(double (&v)[K], double* scratch, double* out, int nwarps) {

@@ -579,6 +579,298 @@ __global__ void __launch_bounds__(kNT) icgn_solve_kernel(IcgnArgs a, int bucket)
 }
 
 // ================================================================================
+// fast 6-DOF solve for subsets at the nominal window without a mask region
+// ================================================================================
+// The common case (uniform variant; quadtree subsets whose window holds no masked or zero
+// pixel): no flood fills, so shared memory holds only (f_x, f_y) per pixel (f as well for
+// the epipolar score) and a 64-thread CTA per subset keeps many subsets in flight per SM.
+// The 6x6 inverse is a cooperative Gauss-Jordan elimination (H is the symmetric positive
+// semi-definite Gauss-Newton Hessian), the b-vector and update are spread over six
+// threads.  A quadtree subset that meets an exact zero in g (a masked deformed image) needs
+// the g-region flood fill: it is handed to the general kernel's queue and restarted there.
+constexpr int kFT = 64;
+
+struct FastCtl {
+  double P[6];
+  double aug[72];  // 6 x 12 row-major [H | I] -> [I | H^-1]
+  double H21[21];  // packed upper triangle by rows == lower triangle by columns
+  double fac[6], piv;
+  double A[6], B[6], b[6], dP[6];
+  double meanf, bf, sabsf;
+  double normNew, normAbs, normInit, znssd;
+  float pf[4], f5, f6;
+  int base_r, base_c;
+  int step, go, status, requeue;
+};
+
+__global__ void __launch_bounds__(kFT, 12) icgn_fast_kernel(IcgnArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ FastCtl c;
+  __shared__ double red[(kFT / 32) * 40];
+  __shared__ double sums[40];
+  const int tid = threadIdx.x;
+  const FrameDev& fr = a.fr;
+  const bool quad = (a.variant == 1);
+  const bool epi = (a.variant == 2);
+  const int count = a.qcount[0];
+  const int gM = fr.M - 6;
+  for (int qi = blockIdx.x; qi < count; qi += gridDim.x) {
+    const int* q = a.queue + 3 * (long long)qi;
+    const long long t = q[0];
+    const int w = q[1];
+    const int W1 = w + 1, npx = W1 * W1, half = w / 2;
+    double x0 = a.coords[t], y0 = a.coords[a.n + t];
+    if (quad) {
+      x0 = mround(x0);
+      y0 = mround(y0);
+    }
+    float2* gxy = reinterpret_cast<float2*>(smem_raw);
+    float* fsm = reinterpret_cast<float*>(gxy + npx);  // epipolar only
+    // ---- load the window and the set-up sums in one pass ----
+    {
+      float h[21], jf[6], jb[6], fs = 0.f, fs2 = 0.f, fn = 0.f, fab = 0.f;
+#pragma unroll
+      for (int k = 0; k < 21; ++k) h[k] = 0.f;
+#pragma unroll
+      for (int k = 0; k < 6; ++k) {
+        jf[k] = 0.f;
+        jb[k] = 0.f;
+      }
+      const int r0 = (int)x0 - half - 1, c0 = (int)y0 - half - 1;
+      for (int p = tid; p < npx; p += kFT) {
+        const int aa = p % W1, bb = p / W1;
+        const size_t k = (size_t)(r0 + aa) + (size_t)(c0 + bb) * fr.M;
+        const size_t kg = (size_t)(r0 + aa - a.crop) + (size_t)(c0 + bb - a.crop) * gM;
+        const float f = fr.ref[k];  // a quadtree subset here has no masked pixel
+        const float gxv = fr.gx[kg], gyv = fr.gy[kg];
+        gxy[p] = make_float2(gxv, gyv);
+        if (epi) fsm[p] = f;
+        const float dx = (float)(aa - half), dy = (float)(bb - half);
+        const float J[6] = {gxv * dx, gyv * dx, gxv * dy, gyv * dy, gxv, gyv};
+        int m = 0;
+#pragma unroll
+        for (int i = 0; i < 6; ++i)
+#pragma unroll
+          for (int j = i; j < 6; ++j) h[m++] = fmaf(J[i], J[j], h[m]);
+#pragma unroll
+        for (int i = 0; i < 6; ++i) {
+          jf[i] = fmaf(J[i], f, jf[i]);
+          jb[i] += J[i];
+        }
+        if (!quad || fabsf(f) > 1e-10f) {
+          fs += f;
+          fs2 = fmaf(f, f, fs2);
+          fn += 1.f;
+        }
+        fab += fabsf(f);
+      }
+      float v[37];
+#pragma unroll
+      for (int k = 0; k < 21; ++k) v[k] = h[k];
+#pragma unroll
+      for (int k = 0; k < 6; ++k) {
+        v[21 + k] = jf[k];
+        v[27 + k] = jb[k];
+      }
+      v[33] = fs;
+      v[34] = fs2;
+      v[35] = fn;
+      v[36] = fab;
+      block_sum_f32<37, kFT>(v, red, sums);
+    }
+    // ---- [H | I] and the f statistics ----
+    for (int e = tid; e < 72; e += kFT) {
+      const int i = e / 12, j = e % 12;
+      double val;
+      if (j < 6) {
+        const int r = i < j ? i : j, cc = i < j ? j : i;  // packed upper-triangle index of (r, cc)
+        val = sums[r * 6 - r * (r - 1) / 2 + (cc - r)];
+      } else {
+        val = (j - 6 == i) ? 1.0 : 0.0;
+      }
+      c.aug[e] = val;
+    }
+    if (tid == 0) {
+      const double n = sums[35];
+      if (n > 0) {
+        c.meanf = sums[33] / n;
+        c.bf = sqrt(fmax(sums[34] - sums[33] * sums[33] / n, 0.0));
+      } else {
+        c.meanf = ALDIC_NAN;
+        c.bf = ALDIC_NAN;
+      }
+      c.sabsf = sums[36];
+      for (int k = 0; k < 21; ++k) c.H21[k] = sums[k];
+      c.P[0] = c.P[1] = c.P[2] = c.P[3] = 0.0;
+      c.P[4] = epi ? 0.0 : a.U0[2 * t];
+      c.P[5] = epi ? 0.0 : a.U0[2 * t + 1];
+      c.normNew = 1.0;
+      c.normAbs = 1.0;
+      c.normInit = 0.0;
+      c.step = 0;
+      c.status = 0;
+      c.requeue = 0;
+      c.znssd = ALDIC_NAN;
+    }
+    __syncthreads();
+    if (tid < 6) {
+      c.B[tid] = sums[27 + tid];
+      c.A[tid] = (sums[21 + tid] - c.meanf * c.B[tid]) / c.bf;
+    }
+    // Gauss-Jordan elimination without pivoting (positive definite H); a zero pivot
+    // propagates Inf/NaN as the reference's singular solve does
+    for (int k = 0; k < 6; ++k) {
+      if (tid < 6) c.fac[tid] = c.aug[tid * 12 + k];
+      if (tid == 0) c.piv = c.aug[k * 12 + k];
+      __syncthreads();
+      if (tid < 12) c.aug[k * 12 + tid] /= c.piv;
+      __syncthreads();
+      for (int e = tid; e < 72; e += kFT) {
+        const int i = e / 12, j = e % 12;
+        if (i != k) c.aug[e] -= c.fac[i] * c.aug[k * 12 + j];
+      }
+      __syncthreads();
+    }
+    // ---- Gauss-Newton iterations ----
+    const int q_nt = kFT / W1, r_nt = kFT % W1;
+    while (true) {
+      if (tid == 0) {
+        int go = (c.step <= a.max_iter && c.normNew > a.tol && c.normAbs > a.tol && !c.requeue) ? 1 : 0;
+        if (go) {
+          c.step += 1;
+          if (warped_oob(fr, c.P, x0, y0, half, half)) {
+            c.normNew = 1e6;
+            go = 0;
+          } else {
+            const double n5 = mround(c.P[4]), n6 = mround(c.P[5]);
+            c.pf[0] = (float)c.P[0];
+            c.pf[1] = (float)c.P[1];
+            c.pf[2] = (float)c.P[2];
+            c.pf[3] = (float)c.P[3];
+            c.f5 = (float)(c.P[4] - n5);
+            c.f6 = (float)(c.P[5] - n6);
+            c.base_r = (int)(x0 + n5) - 2;
+            c.base_c = (int)(y0 + n6) - 2;
+          }
+        }
+        c.go = go;
+      }
+      __syncthreads();
+      if (!c.go) break;
+      float C[6] = {0, 0, 0, 0, 0, 0}, S1 = 0.f, S2 = 0.f, ns = 0.f, nz = 0.f, fg = 0.f;
+      {
+        const float p0 = c.pf[0], p1 = c.pf[1], p2 = c.pf[2], p3 = c.pf[3], f5 = c.f5, f6 = c.f6;
+        const int br = c.base_r, bc = c.base_c;
+        int aa = tid % W1, bb = tid / W1;
+        for (int p = tid; p < npx; p += kFT) {
+          const float dx = (float)(aa - half), dy = (float)(bb - half);
+          const float lx = dx + fmaf(p0, dx, fmaf(p2, dy, f5));
+          const float ly = dy + fmaf(p3, dy, fmaf(p1, dx, f6));
+          const float ix = floorf(lx), iy = floorf(ly);
+          const float g = stencil16(fr.def, fr.M, br + (int)ix, bc + (int)iy, lx - ix, ly - iy);
+          const float2 gg = gxy[p];
+          const float ag = gg.x * g, bg = gg.y * g;
+          C[0] = fmaf(ag, dx, C[0]);
+          C[1] = fmaf(bg, dx, C[1]);
+          C[2] = fmaf(ag, dy, C[2]);
+          C[3] = fmaf(bg, dy, C[3]);
+          C[4] += ag;
+          C[5] += bg;
+          if (!quad || fabsf(g) > 1e-10f) {
+            S1 += g;
+            S2 = fmaf(g, g, S2);
+            ns += 1.f;
+          }
+          if (quad && g == 0.f) nz += 1.f;
+          if (epi) fg = fmaf(fsm[p], g, fg);
+          aa += r_nt;
+          bb += q_nt;
+          if (aa >= W1) {
+            aa -= W1;
+            bb += 1;
+          }
+        }
+      }
+      double v[11] = {C[0], C[1], C[2], C[3], C[4], C[5], S1, S2, ns, nz, fg};
+      block_sum<11, kFT>(v, red, sums);
+      if (sums[9] > 0) {  // exact zero in g: the g-region flood fill is needed
+        if (tid == 0) c.requeue = 1;
+        __syncthreads();
+        break;
+      }
+      if (tid < 6) {
+        const double n = sums[8];
+        double meang, bg;
+        if (n > 0) {
+          meang = sums[6] / n;
+          bg = sqrt(fmax(sums[7] - sums[6] * sums[6] / n, 0.0));
+        } else {
+          meang = ALDIC_NAN;
+          bg = ALDIC_NAN;
+        }
+        c.b[tid] = c.bf * (c.A[tid] - (sums[tid] - meang * c.B[tid]) / bg);
+        if (epi && tid == 0) c.znssd = 2.0 - 2.0 * (sums[10] - c.meanf * sums[6]) / (c.bf * bg);
+      }
+      __syncthreads();
+      if (tid < 6) {
+        double acc = 0;
+#pragma unroll
+        for (int j = 0; j < 6; ++j) acc += c.aug[tid * 12 + 6 + j] * c.b[j];
+        c.dP[tid] = -acc;
+      }
+      __syncthreads();
+      if (tid == 0) {
+        double nn = 0;
+        for (int i = 0; i < 6; ++i) nn += c.b[i] * c.b[i];
+        c.normNew = sqrt(nn);
+        c.normAbs = c.normNew;
+        if (c.step == 1) c.normInit = c.normNew;
+        if (c.normInit > a.tol) c.normNew = c.normNew / c.normInit;
+        else c.normNew = 0.0;
+        if (!(c.normNew < a.tol || c.normAbs < a.tol)) {
+          if (!compose_inverse(c.P, c.dP)) {
+            c.step = a.max_iter + 1000;
+            c.status = 1;
+          } else if (epi) {
+            c.P[4] = 0.0;
+            c.P[5] = 0.0;
+          }
+        }
+      }
+      __syncthreads();
+    }
+    if (tid == 0) {
+      if (c.requeue) {
+        // restart this subset in the general kernel (its queue runs after this kernel)
+        const int pos = atomicAdd(&a.qcount[1], 1);
+        int* q1 = a.queue + 3 * ((long long)a.n + pos);
+        q1[0] = (int)t;
+        q1[1] = w;
+        q1[2] = 0;
+      } else {
+        int step = c.step;
+        if (c.status == 1) step -= 1000;
+        if (!(c.normNew < a.tol || c.normAbs < a.tol)) step = a.max_iter + 1;
+        if (isnan(c.normNew)) step = a.max_iter + 1;
+        if (quad && c.sabsf < 1e-6) step = a.max_iter + 3;
+        if (epi) {
+          a.znssd[t] = c.znssd;
+          if (a.conv) a.conv[t] = step;
+        } else {
+          a.conv[t] = step;
+          a.U[2 * t] = c.P[4];
+          a.U[2 * t + 1] = c.P[5];
+          for (int k = 0; k < 4; ++k) a.F[4 * t + k] = c.P[k];
+          if (a.H)
+            for (int k = 0; k < 21; ++k) a.H[t + a.n * k] = c.H21[k];
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ================================================================================
 // Subpb1: classify + solve
 // ================================================================================
 __global__ void subpb1_classify_kernel(Sub1Args a) {
@@ -985,6 +1277,8 @@ static int occupancy_grid(const void* fn, size_t smem) {
 size_t icgn_smem_bytes(int w) { return (size_t)(w + 1) * (w + 1) * (4 * sizeof(float) + 4); }
 size_t sub1_smem_bytes(int wx, int wy) { return (size_t)(wx + 1) * (wy + 1) * (4 * sizeof(float) + 5); }
 
+size_t icgn_fast_smem_bytes(int w, bool epi) { return (size_t)(w + 1) * (w + 1) * (epi ? 12 : 8); }
+
 int launch_icgn(const IcgnArgs& a, int wmax_enlarged, cudaStream_t st) {
   int launches = 0;
   cudaMemsetAsync(a.qcount, 0, 2 * sizeof(int), st);
@@ -992,15 +1286,27 @@ int launch_icgn(const IcgnArgs& a, int wmax_enlarged, cudaStream_t st) {
   const int cb = 256;
   icgn_classify_kernel<<<(unsigned)((threads + cb - 1) / cb), cb, 0, st>>>(a);
   ++launches;
-  for (int bucket = 0; bucket < 2; ++bucket) {
-    const int w = bucket == 0 ? a.winsize : wmax_enlarged;
-    const size_t smem = icgn_smem_bytes(w);
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  {  // nominal-window subsets without a mask region
+    const size_t smem = icgn_fast_smem_bytes(a.winsize, a.variant == 2);
+    cudaFuncSetAttribute(icgn_fast_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int per_sm = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, icgn_fast_kernel, kFT, smem);
+    long long grid = (long long)sms * (per_sm < 1 ? 1 : per_sm);
+    if (grid > a.n) grid = a.n;
+    icgn_fast_kernel<<<(unsigned)grid, kFT, smem, st>>>(a);
+    ++launches;
+  }
+  {  // enlarged / masked subsets, and those handed over by the fast kernel
+    const size_t smem = icgn_smem_bytes(wmax_enlarged);
     cudaFuncSetAttribute(icgn_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int grid = occupancy_grid((const void*)icgn_solve_kernel, smem);
-    if (bucket == 1) grid = grid < 296 ? grid : 296;
+    grid = grid < 296 ? grid : 296;
     if ((long long)grid > a.n) grid = (int)a.n;
     if (grid < 1) grid = 1;
-    icgn_solve_kernel<<<grid, kNT, smem, st>>>(a, bucket);
+    icgn_solve_kernel<<<grid, kNT, smem, st>>>(a, 1);
     ++launches;
   }
   return launches;

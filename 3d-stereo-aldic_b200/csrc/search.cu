@@ -7,9 +7,10 @@
 //   * window sums sum(D), sum(D^2) of every shift come from FP64 integral images of g
 //     (computed once per call), so the partial-overlap ring of the crop (zero padding of
 //     the cut-out window) is exact;
-//   * the numerator sum((T - mean T) * D) is tiled over 64 x 64 shifts; each thread owns
-//     8 consecutive shift rows x 2 shift columns in registers, slides a 15-value register
-//     window down the template column, accumulates each template column in FP32 and
+//   * the numerator sum((T - mean T) * D): the whole zero-padded window of the subset (or a
+//     strip of its shift columns) sits in shared memory; each thread owns
+//     8 consecutive shift rows x 2 shift columns in registers, slides a 16-value register
+//     window (four 128-bit shared loads) down the template column, accumulates each template column in FP32 and
 //     adds it to FP64 accumulators (41-term FP32 partial sums);
 //   * argmax is the first maximum in column-major order (MATLAB max); the 3 x 3
 //     neighbourhood of the peak is recomputed in FP64 for the sub-pixel fit.
@@ -180,15 +181,19 @@ __host__ __device__ inline SearchLayout search_layout(int w, int na_max, int str
   SearchLayout L;
   L.W1 = w + 1;
   L.TR = round_up8(L.W1);
-  L.DR = (round_up8(na_max) + L.TR - 1) | 1;  // rows a0 .. a0 + TR + 6 for every 8-row block
+  // rows a0 .. a0 + TR + 7 of every 8-row block, leading dimension = 4 (mod 32): each
+  // quarter-warp phase of a 128-bit column load (4 row blocks x 2 columns) covers all 32
+  // banks exactly once
+  const int need = round_up8(na_max) + L.TR;
+  L.DR = need + ((4 - need) % 32 + 32) % 32;
   L.strip_b = strip_b;
   L.DC = round_up16(strip_b) + w;               // columns b + j for b < round_up16(strip_b)
   return L;
 }
 
 // One CTA per subset (grid-stride).  Each warp task covers 32 shift rows (4 lanes x 8
-// consecutive rows) x 16 shift columns (8 lanes x the column pair b, b + 8): with an odd
-// leading dimension the 32 lanes of every window load hit 32 different banks.
+// consecutive rows) x 16 shift columns (8 lanes x the column pair b, b + 8); the window
+// column of a thread is read as four 128-bit loads per 8 template rows.
 __global__ void __launch_bounds__(512, 1) ncc_search_kernel(SearchArgs a, int strip_b, int na_max) {
   const double* __restrict__ I1 = a.I1;
   const double* __restrict__ I2 = a.I2;
@@ -308,11 +313,20 @@ __global__ void __launch_bounds__(512, 1) ncc_search_kernel(SearchArgs a, int st
             p1[k] = 0.f;
           }
           for (int i0 = 0; i0 < TR; i0 += 8) {
-            float w0[15], w1[15];
+            float w0[16], w1[16];
+            const float4* v0 = reinterpret_cast<const float4*>(c0 + i0);
+            const float4* v1 = reinterpret_cast<const float4*>(c1 + i0);
 #pragma unroll
-            for (int m = 0; m < 15; ++m) {
-              w0[m] = c0[i0 + m];
-              w1[m] = c1[i0 + m];
+            for (int q = 0; q < 4; ++q) {
+              const float4 x0 = v0[q], x1 = v1[q];
+              w0[4 * q] = x0.x;
+              w0[4 * q + 1] = x0.y;
+              w0[4 * q + 2] = x0.z;
+              w0[4 * q + 3] = x0.w;
+              w1[4 * q] = x1.x;
+              w1[4 * q + 1] = x1.y;
+              w1[4 * q + 2] = x1.z;
+              w1[4 * q + 3] = x1.w;
             }
             const float4 ta = *reinterpret_cast<const float4*>(tj + i0);
             const float4 tb = *reinterpret_cast<const float4*>(tj + i0 + 4);

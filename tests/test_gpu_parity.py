@@ -170,6 +170,32 @@ def test_local_icgn_quadtree_masked_parity(ctx, hole):
     assert np.array_equal(res["U"].reshape(-1, 2)[m102], U0.reshape(-1, 2)[m102])
 
 
+def test_local_icgn_quadtree_masked_deformed_image(ctx, hole):
+    # reference frame unmasked, deformed frame zeroed inside the hole (TemporalMatch's
+    # gNormalized = ImgNormalized .* gMask): exact zeros in g start the per-iteration
+    # g-region flood fill of funICGNQuadtree.m:170-182 on subsets without any f mask
+    sc = hole
+    M, N = sc.ref.shape
+    ctx.load_image_raw(0, sc.ref, [1, M], [1, N])
+    ctx.load_image_raw(1, sc.deff, [1, M], [1, N], mask=sc.mask)
+    ctx.set_mask(None)
+    ctx.compute_gradients()
+    f, g = ctx.get_state(0), ctx.get_state(1)
+    gx, gy = ctx.get_state(2), ctx.get_state(3)
+    assert np.sum(g == 0) > 1000
+    xs = np.arange(24, 362, 7.0)
+    X, Y = np.meshgrid(xs, xs, indexing="ij")
+    coords = np.stack([X.ravel(), Y.ravel()], 1)
+    tu, tv = sc.disp(coords[:, 0], coords[:, 1])
+    U0 = np.stack([np.round(tu), np.round(tv)], 1).ravel()
+    res = ctx.local_icgn(1, coords, U0, 24, 1e-3)
+    ref = O.local_icgn(O.Frame(f, g, None, gx, gy), coords, U0, 24, 1e-3, variant=1)
+    assert np.mean(res["conv"] == ref["conv"]) >= 0.99
+    assert np.mean(_flag(res["conv"]) == _flag(ref["conv"])) >= FLAG_RATE
+    both = _flag(res["conv"]) & _flag(ref["conv"])
+    assert np.abs(res["U"] - ref["U"]).reshape(-1, 2)[both].max() < UV_TOL
+
+
 def test_subpb1_quadtree_parity(ctx, hole):
     sc = hole
     M, N = sc.ref.shape

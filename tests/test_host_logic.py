@@ -1,0 +1,53 @@
+"""Host-side driver logic mirrored from the reference (no GPU): bad-point rules of the
+local solvers and Subpb1, the search grid, and argument validation of the host API."""
+import numpy as np
+import pytest
+
+from aldic_b200 import api
+
+
+def test_bad_points_quadtree_rules():
+    # LocalICGNQuadtree.m:169-192: codes < 0 or > 99 are bad; 102 does not count in the
+    # bad number; iterations > max(mu + sigma, 6) are bad too
+    conv = np.array([3, 4, 5, 4, 3, 30, -1, 101, 102, 103, 4, 5, 6, 7])
+    bad, num = api.bad_points_local(conv, rule="quadtree")
+    good = conv[(conv >= 0) & (conv <= 99)]
+    thr = max(good.mean() + good.std(ddof=1), 6)
+    want = np.nonzero((conv < 0) | (conv > 99) | (conv > thr))[0]
+    assert np.array_equal(bad, want)
+    assert num == 4 - 1  # -1, 101, 102, 103 minus the 102
+
+
+def test_bad_points_uniform_rule():
+    conv = np.array([3, 3, 4, 10, 3, -1])
+    bad, num = api.bad_points_local(conv, rule="uniform")
+    g = conv[(conv >= 0) & (conv <= 99)]
+    thr = g.mean() + 0.15 * g.std(ddof=1)
+    assert np.array_equal(bad, np.nonzero((conv < 0) | (conv > 99) | (conv > thr))[0])
+
+
+def test_bad_points_subpb1_rule():
+    conv = np.array([2, 3, 2, 12, 0, 101])
+    bad, num = api.bad_points_subpb1(conv)
+    g = conv[(conv >= 0) & (conv <= 99)]
+    thr = max(g.mean() + 0.25 * g.std(ddof=1), 10)
+    assert np.array_equal(bad, np.nonzero((conv < 0) | (conv > 99) | (conv > thr))[0])
+    assert num == 1
+
+
+def test_few_good_points_skip_the_iteration_filter():
+    conv = np.array([3, 101, -1])
+    bad, _ = api.bad_points_local(conv, rule="quadtree")
+    assert list(bad) == [1, 2]
+
+
+def test_count_and_shape_validation():
+    with pytest.raises(api.AldicError):
+        api._count(np.zeros((5, 3)), 2)
+    assert api._count(np.zeros((5, 2)), 2) == 5
+    assert api._img_shape(np.zeros((4, 7)), None) == (4, 7)
+
+
+def test_funintegersearch_rejects_seed_mode():
+    with pytest.raises(api.AldicError):
+        api.funIntegerSearch(np.zeros((10, 10)), np.zeros((10, 10)), 3, [1, 10], [1, 10], 4, 2, 1)
