@@ -194,6 +194,7 @@ __host__ __device__ inline SearchLayout search_layout(int w, int na_max, int str
 // One CTA per subset (grid-stride).  Each warp task covers 32 shift rows (4 lanes x 8
 // consecutive rows) x 16 shift columns (8 lanes x the column pair b, b + 8); the window
 // column of a thread is read as four 128-bit loads per 8 template rows.
+template <int TRC>
 __global__ void __launch_bounds__(512, 1) ncc_search_kernel(SearchArgs a, int strip_b, int na_max) {
   const double* __restrict__ I1 = a.I1;
   const double* __restrict__ I2 = a.I2;
@@ -207,7 +208,8 @@ __global__ void __launch_bounds__(512, 1) ncc_search_kernel(SearchArgs a, int st
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
   const int w = a.winsize;
   const SearchLayout Ly = search_layout(w, na_max, strip_b);
-  const int W1 = Ly.W1, TR = Ly.TR, DR = Ly.DR, DC = Ly.DC;
+  const int W1 = Ly.W1, DR = Ly.DR, DC = Ly.DC;
+  constexpr int TR = TRC;  // == Ly.TR (checked on the host)
   const size_t ld = (size_t)a.M + 1;
   float* Tp = reinterpret_cast<float*>(smem_raw);
   float* Dt = Tp + TR * W1;
@@ -259,11 +261,11 @@ __global__ void __launch_bounds__(512, 1) ncc_search_kernel(SearchArgs a, int st
     const double nwin = (double)W1 * W1;
     // ---- largest denominator over the crop (normxcorr2 zero threshold) ----
     {
-      double dmax = 0;
+      double dmax = 0;  // largest window variance sum; sqrt is monotone
       for (int k = tid; k < s.na * s.nb; k += blockDim.x) {
         double S1, S2;
         window_sums(s, w, k % s.na, k / s.na, I1, I2, ld, &S1, &S2);
-        dmax = fmax(dmax, denT * sqrt(fmax(S2 - S1 * S1 / nwin, 0.0)));
+        dmax = fmax(dmax, S2 - S1 * S1 / nwin);
       }
       for (int off = 16; off > 0; off >>= 1) dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, off));
       if (lane == 0) red[warp] = dmax;
@@ -271,11 +273,13 @@ __global__ void __launch_bounds__(512, 1) ncc_search_kernel(SearchArgs a, int st
       if (tid == 0) {
         double m = 0;
         for (int i = 0; i < nwarps; ++i) m = fmax(m, red[i]);
-        s_tolz = sqrt(matlab_eps_d(m));
+        s_tolz = sqrt(matlab_eps_d(denT * sqrt(fmax(m, 0.0))));
       }
       __syncthreads();
     }
     const double tolz = s_tolz;
+    const double tolv = (tolz / denT) * (tolz / denT);
+    const float inv_denT = (float)(1.0 / denT);
     float best = -INFINITY;
     int bidx = 0x7fffffff;
     const int la = lane & 3, lb = lane >> 2;
@@ -312,6 +316,7 @@ __global__ void __launch_bounds__(512, 1) ncc_search_kernel(SearchArgs a, int st
             p0[k] = 0.f;
             p1[k] = 0.f;
           }
+#pragma unroll
           for (int i0 = 0; i0 < TR; i0 += 8) {
             float w0[16], w1[16];
             const float4* v0 = reinterpret_cast<const float4*>(c0 + i0);
@@ -357,9 +362,15 @@ __global__ void __launch_bounds__(512, 1) ncc_search_kernel(SearchArgs a, int st
             if (aa >= s.na) continue;
             double S1, S2;
             window_sums(s, w, aa, bb, I1, I2, ld, &S1, &S2);
-            const double den = denT * sqrt(fmax(S2 - S1 * S1 / nwin, 0.0));
+            // den = denT * sqrt(var); den > tolz  <=>  var > (tolz / denT)^2
+            const double var = fmax(S2 - S1 * S1 / nwin, 0.0);
             float cval = 0.f;
-            if (den > tolz) cval = (float)((half ? acc1[k] : acc0[k]) / den);
+            if (var > tolv) {
+              const float vf = (float)var;
+              float r = rsqrtf(vf);
+              r = r * fmaf(-0.5f * vf * r, r, 1.5f);  // one Newton step: ~1 ulp
+              cval = (float)(half ? acc1[k] : acc0[k]) * r * inv_denT;
+            }
             if (fabsf(cval) - 1.f > 1.4901161193847656e-08f) cval = 0.f;
             const int lin = aa + bb * s.na;
             if (cval > best || (cval == best && lin < bidx)) {
@@ -511,15 +522,36 @@ int launch_search(const SearchArgs& a, cudaStream_t st) {
   int nw = ((na + 31) / 32) * ((min(sb, na) + 15) / 16);
   nw = nw < 2 ? 2 : (nw > 16 ? 16 : nw);
   const int threads = nw * 32;
-  cudaFuncSetAttribute(ncc_search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  int dev = 0, sms = 148, per_sm = 1;
+  int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ncc_search_kernel, threads, smem);
-  if (per_sm < 1) per_sm = 1;
-  long long grid = (long long)sms * per_sm;
-  if (grid > n) grid = n;
-  ncc_search_kernel<<<(unsigned)grid, threads, smem, st>>>(a, sb, na);
+  auto go = [&](auto kern) {
+    int per_sm = 1;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
+    if (per_sm < 1) per_sm = 1;
+    long long grid = (long long)sms * per_sm;
+    if (grid > n) grid = n;
+    kern<<<(unsigned)grid, threads, smem, st>>>(a, sb, na);
+  };
+  switch (L.TR) {  // template rows rounded up to 8: compile-time for full unrolling
+    case 8: go(ncc_search_kernel<8>); break;
+    case 16: go(ncc_search_kernel<16>); break;
+    case 24: go(ncc_search_kernel<24>); break;
+    case 32: go(ncc_search_kernel<32>); break;
+    case 40: go(ncc_search_kernel<40>); break;
+    case 48: go(ncc_search_kernel<48>); break;
+    case 56: go(ncc_search_kernel<56>); break;
+    case 64: go(ncc_search_kernel<64>); break;
+    case 72: go(ncc_search_kernel<72>); break;
+    case 80: go(ncc_search_kernel<80>); break;
+    case 88: go(ncc_search_kernel<88>); break;
+    case 96: go(ncc_search_kernel<96>); break;
+    case 104: go(ncc_search_kernel<104>); break;
+    case 112: go(ncc_search_kernel<112>); break;
+    case 120: go(ncc_search_kernel<120>); break;
+    default: return -1;
+  }
   return 4;
 }
 
