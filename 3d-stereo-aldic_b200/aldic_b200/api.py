@@ -134,6 +134,16 @@ class Context:
     def launches(self):
         return int(self.lib.aldic_launch_count(self.h))
 
+    def set_profiling(self, on=True):
+        """Record the device time of the correlation kernel of each integer_search call."""
+        self._check(self.lib.aldic_set_profiling(self.h, 1 if on else 0), "aldic_set_profiling")
+
+    def profile_read(self):
+        """(total ms, number of recorded launches) since the last read; clears the record."""
+        ms, n = C.c_double(), C.c_int()
+        self._check(self.lib.aldic_profile_read(self.h, C.byref(ms), C.byref(n)), "aldic_profile_read")
+        return ms.value, n.value
+
     def load_image_raw(self, slot, img, gridx, gridy, mask=None, want_stats=True, shape=None):
         k = _Keep()
         M, N = _img_shape(img, shape)

@@ -52,6 +52,12 @@ struct aldic_ctx {
   double* I2 = nullptr;
   double* iitot = nullptr;
   size_t ii_cap = 0;
+  void* tscratch = nullptr;  // shared-product search scratch
+  size_t tscratch_cap = 0;
+  // profiling: event pairs around the correlation kernel of each integer search
+  bool prof = false;
+  std::vector<cudaEvent_t> prof_ev;  // 2 per record
+  int prof_n = 0;
   Arena arena;
   // outputs to copy back at the end of a call
   struct Back {
@@ -243,9 +249,10 @@ void aldic_destroy(aldic_ctx* c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   void* bufs[] = {c->img[0], c->img[1], c->mask, c->gx, c->gy, c->stats, c->partials, c->counter, c->qcount,
-                  c->I1, c->I2, c->iitot, c->arena.base};
+                  c->I1, c->I2, c->iitot, c->tscratch, c->arena.base};
   for (void* b : bufs)
     if (b) cudaFree(b);
+  for (cudaEvent_t e : c->prof_ev) cudaEventDestroy(e);
   if (c->own) cudaStreamDestroy(c->own);
   delete c;
 }
@@ -431,6 +438,15 @@ int aldic_integer_search(aldic_ctx* c, const int* search, const int* gridx, cons
     CK(cudaMalloc(&c->iitot, search_tot_bytes(c->M, c->N)));
     c->ii_cap = iin;
   }
+  const size_t tbytes = search_tile_bytes(c->M, c->N, winsize, step, nx, ny, search[0], search[1]);
+  if (tbytes > c->tscratch_cap) {
+    CK(cudaStreamSynchronize(c->stream));
+    if (c->tscratch) CK(cudaFree(c->tscratch));
+    c->tscratch = nullptr;
+    c->tscratch_cap = 0;
+    CK(cudaMalloc(&c->tscratch, tbytes));
+    c->tscratch_cap = tbytes;
+  }
   Arg ox{x, n * 8, true, nullptr}, oy{y, n * 8, true, nullptr}, ou{u, n * 8, true, nullptr};
   Arg ov{v, n * 8, true, nullptr}, op{phi, n * 8, true, nullptr};
   rc = stage(c, {&ox, &oy, &ou, &ov, &op});
@@ -458,6 +474,13 @@ int aldic_integer_search(aldic_ctx* c, const int* search, const int* gridx, cons
   a.I1 = c->I1;
   a.I2 = c->I2;
   a.tot = c->iitot;
+  a.tile_scratch = tbytes ? c->tscratch : nullptr;
+  a.ev_start = a.ev_stop = nullptr;
+  if (c->prof && 2 * (c->prof_n + 1) <= (int)c->prof_ev.size()) {
+    a.ev_start = c->prof_ev[2 * c->prof_n];
+    a.ev_stop = c->prof_ev[2 * c->prof_n + 1];
+    ++c->prof_n;
+  }
   return finish(c, launch_search(a, c->stream));
 }
 
@@ -668,6 +691,33 @@ int aldic_measure_fp32_peak(aldic_ctx* c, double* tflops) {
   c->launches += 2;
   const double flops = 2.0 * 8 * 16 * (double)iters * threads * blocks;
   *tflops = flops / (ms * 1e-3) / 1e12;
+  return ALDIC_OK;
+}
+
+int aldic_set_profiling(aldic_ctx* c, int on) {
+  if (!c) return ALDIC_ERR_ARG;
+  CK(cudaSetDevice(c->device));
+  if (on && c->prof_ev.empty()) {
+    c->prof_ev.resize(2 * 256);
+    for (cudaEvent_t& e : c->prof_ev) CK(cudaEventCreate(&e));
+  }
+  c->prof = on != 0;
+  return ALDIC_OK;
+}
+
+int aldic_profile_read(aldic_ctx* c, double* total_ms, int* launches) {
+  if (!c || !total_ms || !launches) return ALDIC_ERR_ARG;
+  CK(cudaSetDevice(c->device));
+  double tot = 0.0;
+  for (int k = 0; k < c->prof_n; ++k) {
+    CK(cudaEventSynchronize(c->prof_ev[2 * k + 1]));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, c->prof_ev[2 * k], c->prof_ev[2 * k + 1]));
+    tot += ms;
+  }
+  *total_ms = tot;
+  *launches = c->prof_n;
+  c->prof_n = 0;
   return ALDIC_OK;
 }
 

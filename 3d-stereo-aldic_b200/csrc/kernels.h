@@ -71,6 +71,8 @@ struct SearchArgs {
   double* I1;   // (M+1) x (N+1) integral images of g and g^2 (scratch)
   double* I2;
   double* tot;  // row-pass chunk totals (scratch, search_tot_bytes)
+  void* tile_scratch;  // shared-product search scratch (search_tile_bytes bytes), or null
+  cudaEvent_t ev_start, ev_stop;  // recorded around the correlation kernel when non-null
 };
 
 // launchers return the number of kernels they enqueued (or < 0 on argument errors)
@@ -90,6 +92,10 @@ int launch_subpb1(const Sub1Args& a, int wmax_x, int wmax_y, cudaStream_t st);
 size_t search_smem_bytes(int winsize, int s0, int s1);
 size_t search_tot_bytes(int M, int N);
 int launch_search(const SearchArgs& a, cudaStream_t st);
+// Shared-product search (search_tile.cu): scratch size (0 when the step / window pair has
+// no tile kernel), and the launcher (returns the launch count, or -1 when not available).
+size_t search_tile_bytes(int M, int N, int winsize, int step, int nx, int ny, int s0, int s1);
+int launch_search_tile(const SearchArgs& a, cudaStream_t st);
 struct CamPair {
   double P[24];  // P_L = K_L [I | 0] then P_R = K_R [R | T], each 3x4 row-major
 };

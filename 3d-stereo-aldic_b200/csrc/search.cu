@@ -14,14 +14,10 @@
 //     adds it to FP64 accumulators (41-term FP32 partial sums);
 //   * argmax is the first maximum in column-major order (MATLAB max); the 3 x 3
 //     neighbourhood of the peak is recomputed in FP64 for the sub-pixel fit.
-#include "common.cuh"
-#include "kernels.h"
+#include "search_common.cuh"
 
 namespace aldic {
 
-
-__host__ __device__ inline int round_up8(int v) { return (v + 7) & ~7; }
-__host__ __device__ inline int round_up16(int v) { return (v + 15) & ~15; }
 
 // Integral images of g and g^2 in FP64: II(r, c) = sum over rows < r and columns < c;
 // (M+1) x (N+1) column-major, row 0 and column 0 zero.
@@ -117,59 +113,6 @@ __global__ void integral_rows_fix_kernel(int M, int N, double* __restrict__ I1, 
   }
 }
 
-struct SubsetGeom {
-  int ii, jj;        // 1-based template top-left
-  int L, R, U, D;    // search extents
-  int na, nb;        // crop size
-  int dr0, dr1, dc0, dc1;  // 0-based inclusive extent of the cut-out window D
-  bool ok;
-};
-
-__device__ inline SubsetGeom subset_geom(const SearchArgs& a, long long t) {
-  SubsetGeom s;
-  const int i = (int)(t % a.nx), j = (int)(t / a.nx);
-  const int w = a.winsize;
-  s.ii = a.gx0 + i * a.step;
-  s.jj = a.gy0 + j * a.step;
-  // [left right up down] = [s0 s1 s0 s1] (funIntegerSearch.m:12), clamped per subset
-  // (:139-152); the right/down clamps use gridx(end)/gridy(end) as the reference does.
-  int L = a.s0, R = a.s1, U = a.s0, D = a.s1;
-  if (s.ii - L < 1) L = s.ii - 1;
-  if (s.jj - U < 1) U = s.jj - 1;
-  if (s.ii + w + R > a.M) R = a.gx1 - s.ii - w - 1;
-  if (s.jj + w + D > a.N) D = a.gy1 - s.jj - w - 1;
-  s.L = max(L, 0);
-  s.R = max(R, 0);
-  s.U = max(U, 0);
-  s.D = max(D, 0);
-  s.na = s.L + s.R + 3;
-  s.nb = s.U + s.D + 3;
-  s.dr0 = s.ii - s.L - 1;
-  s.dr1 = s.ii + w + s.R - 1;
-  s.dc0 = s.jj - s.U - 1;
-  s.dc1 = s.jj + w + s.D - 1;
-  s.ok = s.ii >= 1 && s.ii + w <= a.M && s.jj >= 1 && s.jj + w <= a.N && s.dr0 >= 0 && s.dr1 < a.M &&
-         s.dc0 >= 0 && s.dc1 < a.N;
-  return s;
-}
-
-// Window sums of the shift (a, b): the (w+1)^2 window with top-left at Dpad (a, b),
-// intersected with D (image rows dr0-1+a ..), from the integral images.
-__device__ __forceinline__ void window_sums(const SubsetGeom& s, int w, int a, int b, const double* __restrict__ I1,
-                                            const double* __restrict__ I2, size_t ld, double* S1, double* S2) {
-  const int r0 = max(s.dr0, s.dr0 - 1 + a), r1 = min(s.dr1, s.dr0 - 1 + a + w);
-  const int c0 = max(s.dc0, s.dc0 - 1 + b), c1 = min(s.dc1, s.dc0 - 1 + b + w);
-  const size_t p00 = (size_t)r0 + (size_t)c0 * ld, p10 = (size_t)(r1 + 1) + (size_t)c0 * ld;
-  const size_t p01 = (size_t)r0 + (size_t)(c1 + 1) * ld, p11 = (size_t)(r1 + 1) + (size_t)(c1 + 1) * ld;
-  *S1 = (I1[p11] - I1[p10]) - (I1[p01] - I1[p00]);
-  *S2 = (I2[p11] - I2[p10]) - (I2[p01] - I2[p00]);
-}
-
-__device__ __forceinline__ double matlab_eps_d(double x) {
-  x = fabs(x);
-  return nextafter(x, INFINITY) - x;
-}
-
 // Shared-memory layout of one subset: the centred template (TR x W1, rows >= W1 zero)
 // and the padded search window Dpad restricted to the current strip of shift columns
 // (DR x DC, zero outside the cut-out window D).
@@ -216,8 +159,7 @@ __global__ void __launch_bounds__(512, 1) ncc_search_kernel(SearchArgs a, int st
   const long long n = (long long)a.nx * a.ny;
   for (long long t = blockIdx.x; t < n; t += gridDim.x) {
     const SubsetGeom s = subset_geom(a, t);
-    const int oi = (int)(t % a.nx), oj = (int)(t / a.nx);
-    const long long o = oj + (long long)oi * a.ny;
+    const long long o = subset_out(a, t);
     if (tid == 0) {
       a.x[o] = (s.ii + s.ii + w) / 2.0;
       a.y[o] = (s.jj + s.jj + w) / 2.0;
@@ -407,75 +349,7 @@ __global__ void __launch_bounds__(512, 1) ncc_search_kernel(SearchArgs a, int st
       s_peak = bi;
     }
     __syncthreads();
-    // ---- FP64 NCC of the 3 x 3 neighbourhood of the peak ----
-    const int pa = s_peak % s.na, pb = s_peak / s.na;
-    {
-      double v[9];
-#pragma unroll
-      for (int k = 0; k < 9; ++k) v[k] = 0.0;
-      const double tm = s_tmean;
-      for (int p = tid; p < W1 * W1; p += blockDim.x) {
-        const int i = p % W1, j = p / W1;
-        const double tv = (double)a.f[(size_t)(s.ii - 1 + i) + (size_t)(s.jj - 1 + j) * a.M] - tm;
-#pragma unroll
-        for (int k = 0; k < 9; ++k) {
-          const int aa = pa + (k % 3) - 1, bb = pb + (k / 3) - 1;
-          const int r = s.dr0 - 1 + aa + i, c = s.dc0 - 1 + bb + j;
-          double d = 0.0;
-          if (r >= s.dr0 && r <= s.dr1 && c >= s.dc0 && c <= s.dc1) d = (double)a.g[(size_t)r + (size_t)c * a.M];
-          v[k] += tv * d;
-        }
-      }
-      block_sum_dyn<9>(v, red, sums, nwarps);
-    }
-    if (tid == 0) {
-      double cc[9];
-      for (int k = 0; k < 9; ++k) {
-        const int aa = pa + (k % 3) - 1, bb = pb + (k / 3) - 1;
-        cc[k] = 0.0;
-        if (aa < 0 || aa >= s.na || bb < 0 || bb >= s.nb) continue;
-        double S1, S2;
-        window_sums(s, w, aa, bb, I1, I2, ld, &S1, &S2);
-        const double den = denT * sqrt(fmax(S2 - S1 * S1 / nwin, 0.0));
-        double cv = (den > tolz) ? sums[k] / den : 0.0;
-        if (fabs(cv) - 1 > 1.4901161193847656e-08) cv = 0.0;
-        cc[k] = cv;
-      }
-      // findpeak (func/findpeak.m:27-66); xpeak = crop column, ypeak = crop row (1-based)
-      double xpeak = pb + 1, ypeak = pa + 1, maxf = cc[4];
-      const bool edge = (pb == 0 || pb == s.nb - 1 || pa == 0 || pa == s.na - 1);
-      if (!edge) {
-        // u(dx, dy) with dx = column offset, dy = row offset: cc[(dy+1) + 3 (dx+1)]
-        double S = 0, Sx = 0, Sy = 0, Sx2 = 0, Sy2 = 0;
-        for (int dx = -1; dx <= 1; ++dx)
-          for (int dy = -1; dy <= 1; ++dy) {
-            const double u = cc[(dy + 1) + 3 * (dx + 1)];
-            S += u;
-            Sx += dx * u;
-            Sy += dy * u;
-            if (dx != 0) Sx2 += u;
-            if (dy != 0) Sy2 += u;
-          }
-        const double A2 = Sx / 6.0, A3 = Sy / 6.0;
-        const double A4 = (cc[8] - cc[6] - cc[2] + cc[0]) / 4.0;
-        const double A5 = Sx2 / 2.0 - S / 3.0, A6 = Sy2 / 2.0 - S / 3.0;
-        const double A1 = (5.0 * S - 3.0 * (Sx2 + Sy2)) / 9.0;
-        const double dd = A4 * A4 - 4 * A5 * A6;
-        double xo = (-A3 * A4 + 2 * A6 * A2) / dd;
-        double yo = -1 / dd * (A4 * A2 - 2 * A5 * A3);
-        if (!(fabs(xo) > 1 || fabs(yo) > 1)) {
-          xo = round(1000 * xo) / 1000;
-          yo = round(1000 * yo) / 1000;
-          xpeak += xo;
-          ypeak += yo;
-          maxf = A1 + A2 * xo + A3 * yo + A4 * xo * yo + A5 * xo * xo + A6 * yo * yo;
-        }
-      }
-      a.u[o] = ypeak - 2 - s.L;
-      a.v[o] = xpeak - 2 - s.U;
-      a.phi[o] = maxf;
-    }
-    __syncthreads();
+    refit_peak(a, s, o, s_peak % s.na, s_peak / s.na, s_tmean, denT, tolz, red, sums);
   }
 }
 
@@ -514,6 +388,9 @@ int launch_search(const SearchArgs& a, cudaStream_t st) {
   const long long rt = (long long)(a.M + 1) * ((a.N + kRowChunk - 1) / kRowChunk);
   integral_rows_local_kernel<<<(unsigned)((rt + 255) / 256), 256, 0, st>>>(a.M, a.N, a.I1, a.I2, a.tot);
   integral_rows_fix_kernel<<<(unsigned)((rt + 255) / 256), 256, 0, st>>>(a.M, a.N, a.I1, a.I2, a.tot);
+  // shared products over tiles of subsets where a tile kernel exists for (step, w + 1)
+  const int tl = launch_search_tile(a, st);
+  if (tl >= 0) return 3 + tl;
   const int na = crop_max(a.s0, a.s1);
   const int sb = strip_columns(a.winsize, na, na, 200 * 1024);
   const SearchLayout L = search_layout(a.winsize, na, sb);
@@ -532,7 +409,9 @@ int launch_search(const SearchArgs& a, cudaStream_t st) {
     if (per_sm < 1) per_sm = 1;
     long long grid = (long long)sms * per_sm;
     if (grid > n) grid = n;
+    if (a.ev_start) cudaEventRecord(a.ev_start, st);
     kern<<<(unsigned)grid, threads, smem, st>>>(a, sb, na);
+    if (a.ev_stop) cudaEventRecord(a.ev_stop, st);
   };
   switch (L.TR) {  // template rows rounded up to 8: compile-time for full unrolling
     case 8: go(ncc_search_kernel<8>); break;

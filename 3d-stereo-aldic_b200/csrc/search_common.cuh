@@ -1,0 +1,184 @@
+// Helpers shared by the two integer-search implementations (search.cu: one CTA per
+// subset; search_tile.cu: shared products over tiles of subsets): the per-subset search
+// geometry of funIntegerSearchWholeField (func/funIntegerSearch.m:139-152), window sums
+// from the FP64 integral images, and the FP64 3 x 3 refit + findpeak (func/findpeak.m).
+#pragma once
+#include "common.cuh"
+#include "kernels.h"
+
+namespace aldic {
+
+__host__ __device__ inline int round_up8(int v) { return (v + 7) & ~7; }
+__host__ __device__ inline int round_up16(int v) { return (v + 15) & ~15; }
+
+// Search extents along one image axis for a template starting at the 1-based index
+// `start` (ii or jj): [lo hi] = [s0 s1] clamped as funIntegerSearch.m:139-152 does (the
+// high-side clamp uses gridx(end) / gridy(end), `gend`).  `ok` is the axis part of the
+// validity test: the template and the cut-out window lie inside the image.
+struct AxisGeom {
+  int lo, hi;      // L, R (rows) or U, D (columns), >= 0
+  int d0, d1;      // 0-based inclusive extent of the cut-out window along the axis
+  bool ok;
+};
+
+__host__ __device__ inline AxisGeom axis_geom(int start, int w, int s0, int s1, int size, int gend) {
+  AxisGeom g;
+  int lo = s0, hi = s1;
+  if (start - lo < 1) lo = start - 1;
+  if (start + w + hi > size) hi = gend - start - w - 1;
+  g.lo = lo > 0 ? lo : 0;
+  g.hi = hi > 0 ? hi : 0;
+  g.d0 = start - g.lo - 1;
+  g.d1 = start + w + g.hi - 1;
+  g.ok = start >= 1 && start + w <= size && g.d0 >= 0 && g.d1 < size;
+  return g;
+}
+
+struct SubsetGeom {
+  int ii, jj;        // 1-based template top-left
+  int L, R, U, D;    // search extents
+  int na, nb;        // crop size
+  int dr0, dr1, dc0, dc1;  // 0-based inclusive extent of the cut-out window D
+  bool ok;
+};
+
+// Subset t of the nx x ny grid (t = i + j nx).
+__device__ inline SubsetGeom subset_geom(const SearchArgs& a, long long t) {
+  SubsetGeom s;
+  const int i = (int)(t % a.nx), j = (int)(t / a.nx);
+  const int w = a.winsize;
+  s.ii = a.gx0 + i * a.step;
+  s.jj = a.gy0 + j * a.step;
+  const AxisGeom r = axis_geom(s.ii, w, a.s0, a.s1, a.M, a.gx1);
+  const AxisGeom c = axis_geom(s.jj, w, a.s0, a.s1, a.N, a.gy1);
+  s.L = r.lo;
+  s.R = r.hi;
+  s.U = c.lo;
+  s.D = c.hi;
+  s.na = s.L + s.R + 3;
+  s.nb = s.U + s.D + 3;
+  s.dr0 = r.d0;
+  s.dr1 = r.d1;
+  s.dc0 = c.d0;
+  s.dc1 = c.d1;
+  s.ok = r.ok && c.ok;
+  return s;
+}
+
+// Output slot of subset t = i + j nx in the x, y, u, v, phi arrays: o = j + i ny.
+__device__ __forceinline__ long long subset_out(const SearchArgs& a, long long t) {
+  return t / a.nx + (t % a.nx) * (long long)a.ny;
+}
+
+// Sums of g and g^2 over the image box rows r0..r1, columns c0..c1 (inclusive, 0-based)
+// from the (M+1) x (N+1) integral images.
+__device__ __forceinline__ void box_sums(int r0, int r1, int c0, int c1, const double* __restrict__ I1,
+                                         const double* __restrict__ I2, size_t ld, double* S1, double* S2) {
+  const size_t p00 = (size_t)r0 + (size_t)c0 * ld, p10 = (size_t)(r1 + 1) + (size_t)c0 * ld;
+  const size_t p01 = (size_t)r0 + (size_t)(c1 + 1) * ld, p11 = (size_t)(r1 + 1) + (size_t)(c1 + 1) * ld;
+  *S1 = (I1[p11] - I1[p10]) - (I1[p01] - I1[p00]);
+  *S2 = (I2[p11] - I2[p10]) - (I2[p01] - I2[p00]);
+}
+
+// Window sums of the crop shift (a, b): the (w+1)^2 window with top-left at Dpad (a, b),
+// intersected with D (image rows dr0-1+a ..), from the integral images.
+__device__ __forceinline__ void window_sums(const SubsetGeom& s, int w, int a, int b, const double* __restrict__ I1,
+                                            const double* __restrict__ I2, size_t ld, double* S1, double* S2) {
+  const int r0 = max(s.dr0, s.dr0 - 1 + a), r1 = min(s.dr1, s.dr0 - 1 + a + w);
+  const int c0 = max(s.dc0, s.dc0 - 1 + b), c1 = min(s.dc1, s.dc0 - 1 + b + w);
+  box_sums(r0, r1, c0, c1, I1, I2, ld, S1, S2);
+}
+
+__device__ __forceinline__ double matlab_eps_d(double x) {
+  x = fabs(x);
+  return nextafter(x, INFINITY) - x;
+}
+
+// Per-subset constants of the normalised cross-correlation, computed once per call.
+struct SubsetPrm {
+  double fm;     // template mean
+  double denT;   // sqrt(sum (T - mean)^2)
+  double tolz;   // normxcorr2 zero threshold on the denominator
+  double tolv;   // the same threshold on the window variance sum: (tolz / denT)^2
+  int valid;     // geometry inside the image and a non-constant template
+  int pad;
+};
+
+// FP64 NCC of the 3 x 3 neighbourhood of the crop peak (pa, pb), then findpeak
+// (func/findpeak.m:27-66) and the displacement of funIntegerSearch.m:170-190.  Called by
+// every thread of the block (block-wide reduction); thread 0 writes u, v, phi.
+__device__ inline void refit_peak(const SearchArgs& a, const SubsetGeom& s, long long o, int pa, int pb, double tm,
+                                  double denT, double tolz, double* red, double* sums) {
+  const int w = a.winsize, W1 = w + 1;
+  const size_t ld = (size_t)a.M + 1;
+  const int nwarps = blockDim.x >> 5;
+  {
+    double v[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) v[k] = 0.0;
+    for (int p = threadIdx.x; p < W1 * W1; p += blockDim.x) {
+      const int i = p % W1, j = p / W1;
+      const double tv = (double)a.f[(size_t)(s.ii - 1 + i) + (size_t)(s.jj - 1 + j) * a.M] - tm;
+#pragma unroll
+      for (int k = 0; k < 9; ++k) {
+        const int aa = pa + (k % 3) - 1, bb = pb + (k / 3) - 1;
+        const int r = s.dr0 - 1 + aa + i, c = s.dc0 - 1 + bb + j;
+        double d = 0.0;
+        if (r >= s.dr0 && r <= s.dr1 && c >= s.dc0 && c <= s.dc1) d = (double)a.g[(size_t)r + (size_t)c * a.M];
+        v[k] += tv * d;
+      }
+    }
+    block_sum_dyn<9>(v, red, sums, nwarps);
+  }
+  if (threadIdx.x == 0) {
+    const double nwin = (double)W1 * W1;
+    double cc[9];
+    for (int k = 0; k < 9; ++k) {
+      const int aa = pa + (k % 3) - 1, bb = pb + (k / 3) - 1;
+      cc[k] = 0.0;
+      if (aa < 0 || aa >= s.na || bb < 0 || bb >= s.nb) continue;
+      double S1, S2;
+      window_sums(s, w, aa, bb, a.I1, a.I2, ld, &S1, &S2);
+      const double den = denT * sqrt(fmax(S2 - S1 * S1 / nwin, 0.0));
+      double cv = (den > tolz) ? sums[k] / den : 0.0;
+      if (fabs(cv) - 1 > 1.4901161193847656e-08) cv = 0.0;
+      cc[k] = cv;
+    }
+    // findpeak; xpeak = crop column, ypeak = crop row (1-based)
+    double xpeak = pb + 1, ypeak = pa + 1, maxf = cc[4];
+    const bool edge = (pb == 0 || pb == s.nb - 1 || pa == 0 || pa == s.na - 1);
+    if (!edge) {
+      // u(dx, dy) with dx = column offset, dy = row offset: cc[(dy+1) + 3 (dx+1)]
+      double S = 0, Sx = 0, Sy = 0, Sx2 = 0, Sy2 = 0;
+      for (int dx = -1; dx <= 1; ++dx)
+        for (int dy = -1; dy <= 1; ++dy) {
+          const double u = cc[(dy + 1) + 3 * (dx + 1)];
+          S += u;
+          Sx += dx * u;
+          Sy += dy * u;
+          if (dx != 0) Sx2 += u;
+          if (dy != 0) Sy2 += u;
+        }
+      const double A2 = Sx / 6.0, A3 = Sy / 6.0;
+      const double A4 = (cc[8] - cc[6] - cc[2] + cc[0]) / 4.0;
+      const double A5 = Sx2 / 2.0 - S / 3.0, A6 = Sy2 / 2.0 - S / 3.0;
+      const double A1 = (5.0 * S - 3.0 * (Sx2 + Sy2)) / 9.0;
+      const double dd = A4 * A4 - 4 * A5 * A6;
+      double xo = (-A3 * A4 + 2 * A6 * A2) / dd;
+      double yo = -1 / dd * (A4 * A2 - 2 * A5 * A3);
+      if (!(fabs(xo) > 1 || fabs(yo) > 1)) {
+        xo = round(1000 * xo) / 1000;
+        yo = round(1000 * yo) / 1000;
+        xpeak += xo;
+        ypeak += yo;
+        maxf = A1 + A2 * xo + A3 * yo + A4 * xo * yo + A5 * xo * xo + A6 * yo * yo;
+      }
+    }
+    a.u[o] = ypeak - 2 - s.L;
+    a.v[o] = xpeak - 2 - s.U;
+    a.phi[o] = maxf;
+  }
+  __syncthreads();
+}
+
+}  // namespace aldic

@@ -1,0 +1,693 @@
+// Whole-field integer search with shared products: the same results as the per-subset
+// normxcorr2 of funIntegerSearchWholeField (func/funIntegerSearch.m:100-203, findpeak at
+// :170-190), computed for tiles of grid subsets at once.
+//
+// The numerator of the NCC of subset s at the shift d = (da, db) is
+//     sum over the (w+1)^2 window W_s of (f - fm_s)(x) g(x + d),
+// and the windows of neighbouring grid subsets overlap ((w+1) / step times along each axis
+// for w = 40, step = 10).  For a tile of TI x 8 subsets and one shift, every product
+// f(x) g(x + d) of the tile is formed once and summed in blocks of `step` columns and rows
+// (each window is Q = (w+1) / step whole blocks plus REM = (w+1) mod step leading rows /
+// columns of the next block), instead of once per overlapping window:
+//   pass 1  each thread owns one tile row x and 8 consecutive shift columns db and walks the
+//           tile's columns with a sliding register window of g (128-bit shared loads); the
+//           block sums give, per row, the row-band sums RB(x, j, d) over the columns of
+//           window j;
+//   pass 2  each thread owns (window column j, shift column db) and walks the rows of half
+//           of the tile's window rows; block sums over rows give the window sums N(i, j, d).
+// The window mean and variance sums of g come from a per-position map (full windows) and a
+// per-subset table (the ring of partial windows at the crop border, where normxcorr2 zero-
+// pads the cut-out window), both built from the FP64 integral images.  A ring shift drops
+// the excluded template row (one RB value) and / or column (a per-subset table of column
+// products) from the window sum.  The argmax (first maximum in column-major crop order) is
+// refit in FP64 on the 3 x 3 neighbourhood, as the per-subset kernel does.
+#include "search_common.cuh"
+
+namespace aldic {
+
+namespace {
+
+constexpr int kTileThreads = 256;
+constexpr int kTJ = 8;     // subset columns per tile
+constexpr int kDBC = 16;   // shift columns per chunk (2 groups of 8)
+constexpr int kRing = 128; // rows of the circular g buffer
+
+// Smallest m >= n with m = 4 (mod 8): row strides of 128-bit loads across consecutive
+// rows then hit 8 distinct 16-byte bank groups per quarter warp.
+constexpr int pad4odd(int n) { return ((n + 3) / 4 % 2 == 1) ? (n + 3) / 4 * 4 : (n + 3) / 4 * 4 + 4; }
+
+template <int ST, int W1, int TI>
+struct TileShape {
+  static constexpr int Q = W1 / ST, REM = W1 % ST;
+  static constexpr int FR = (TI - 1) * ST + W1;      // tile rows
+  static constexpr int FC = (kTJ - 1) * ST + W1;     // tile columns
+  static constexpr int FCP = pad4odd(FC);            // row stride of F (row-major)
+  static constexpr int GCP = pad4odd(FC + 18);       // row stride of the g ring (row-major)
+  static constexpr int FRP = pad4odd(FR);            // row stride of RB (one row per (j, d))
+  static constexpr int H0 = (TI + 1) / 2;            // subset rows of the first pass-2 half
+  static constexpr int NSUB = TI * kTJ;
+  static constexpr size_t smem_bytes =
+      sizeof(float) * ((size_t)FR * FCP + (size_t)kRing * GCP + (size_t)kTJ * kDBC * FRP);
+  static_assert(Q >= 1, "step must not exceed the window");
+  static_assert(FR <= kRing - 1, "tile rows must leave one free ring row");
+};
+
+template <int ST, int W1>
+struct TileFor {
+  static constexpr int TI = (kRing - 1 - W1) / ST + 1;  // as many subset rows as fit 127 tile rows
+};
+
+struct TileScratch {
+  float2* map;       // MW x NW: (window mean of g, 1 / sqrt(window variance sum)) per position
+  double* V;         // MW x NW: window variance sum S2 - S1^2 / n
+  double* H;         // MW x ny: max of V over the non-ring shift columns of grid column j
+  SubsetPrm* prm;    // nx * ny
+  float2* ringv;     // nx * ny x 4 NDA: (mean, 1/sqrt(variance sum)) of the partial windows
+  float* cx;         // nx * ny x 2 NDA: products of the excluded template column
+  int* best;         // nx * ny: crop index of the first maximum
+};
+
+inline size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+
+inline size_t scratch_layout(int M, int N, int W1, int nx, int ny, int nda, char* base, TileScratch* sc) {
+  const size_t MW = (size_t)(M - W1 + 1), NW = (size_t)(N - W1 + 1), n = (size_t)nx * ny;
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    char* p = base ? base + off : nullptr;
+    off += align256(bytes);
+    return p;
+  };
+  char* pm = take(MW * NW * sizeof(float2));
+  char* pv = take(MW * NW * sizeof(double));
+  char* ph = take(MW * (size_t)ny * sizeof(double));
+  char* pp = take(n * sizeof(SubsetPrm));
+  char* pr = take(n * 4 * (size_t)nda * sizeof(float2));
+  char* pc = take(n * 2 * (size_t)nda * sizeof(float));
+  char* pb = take(n * sizeof(int));
+  if (sc) {
+    sc->map = (float2*)pm;
+    sc->V = (double*)pv;
+    sc->H = (double*)ph;
+    sc->prm = (SubsetPrm*)pp;
+    sc->ringv = (float2*)pr;
+    sc->cx = (float*)pc;
+    sc->best = (int*)pb;
+  }
+  return off;
+}
+
+__device__ __forceinline__ float rsqrt_from(double v) { return v > 0 ? (float)(1.0 / sqrt(v)) : INFINITY; }
+
+// Centring constant of the tile with origin (i0, j0): the mean of its valid template means
+// (a fixed summation order, so every kernel computes the same float).
+__device__ inline float tile_centre(const SubsetPrm* __restrict__ prm, int nx, int ny, int i0, int j0, int TI) {
+  double s = 0.0;
+  int c = 0;
+  for (int q = 0; q < TI * kTJ; ++q) {
+    const int i = i0 + q % TI, j = j0 + q / TI;
+    if (i < nx && j < ny) {
+      const SubsetPrm& P = prm[i + (long long)j * nx];
+      if (P.valid) {
+        s += P.fm;
+        ++c;
+      }
+    }
+  }
+  return c ? (float)(s / c) : 0.f;
+}
+
+}  // namespace
+
+// Window mean and variance sum of g for every full (w+1)^2 window position (x, y) (top-left,
+// 0-based), with the same integral-image expression as window_sums.
+__global__ void window_map_kernel(const double* __restrict__ I1, const double* __restrict__ I2, int M, int N,
+                                  int W1, float2* __restrict__ map, double* __restrict__ V) {
+  const int MW = M - W1 + 1, NW = N - W1 + 1;
+  const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (p >= (long long)MW * NW) return;
+  const int x = (int)(p % MW), y = (int)(p / MW);
+  double S1, S2;
+  box_sums(x, x + W1 - 1, y, y + W1 - 1, I1, I2, (size_t)M + 1, &S1, &S2);
+  const double nwin = (double)W1 * W1;
+  const double v = S2 - S1 * S1 / nwin;
+  V[p] = v;
+  map[p] = make_float2((float)(S1 / nwin), rsqrt_from(v));
+}
+
+// H(x, j) = max(0, max over the non-ring shift columns db in [-U_j, D_j] of V(x, jj-1+db)).
+__global__ void window_rowmax_kernel(SearchArgs a, const double* __restrict__ V, double* __restrict__ H) {
+  const int W1 = a.winsize + 1, MW = a.M - W1 + 1;
+  const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (p >= (long long)MW * a.ny) return;
+  const int x = (int)(p % MW), j = (int)(p / MW);
+  const int jj = a.gy0 + j * a.step;
+  const AxisGeom c = axis_geom(jj, a.winsize, a.s0, a.s1, a.N, a.gy1);
+  double m = 0.0;
+  if (c.ok)
+    for (int db = -c.lo; db <= c.hi; ++db) m = fmax(m, V[x + (size_t)(jj - 1 + db) * MW]);
+  H[p] = m;
+}
+
+// One warp per subset: template mean and norm, the window sums of the ring of partial
+// windows, the largest window variance sum over the crop (normxcorr2 zero threshold) and
+// validity; writes x, y and the NaN outputs of invalid subsets.
+__global__ void subset_prep_kernel(SearchArgs a, const double* __restrict__ H, SubsetPrm* __restrict__ prm,
+                                   float2* __restrict__ ringv) {
+  const int lane = threadIdx.x & 31;
+  const long long t = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const long long n = (long long)a.nx * a.ny;
+  if (t >= n) return;
+  const SubsetGeom s = subset_geom(a, t);
+  const long long o = subset_out(a, t);
+  const int w = a.winsize, W1 = w + 1;
+  const int nda = a.s0 + a.s1 + 3;
+  if (lane == 0) {
+    a.x[o] = (s.ii + s.ii + w) / 2.0;
+    a.y[o] = (s.jj + s.jj + w) / 2.0;
+  }
+  SubsetPrm P;
+  P.fm = P.denT = P.tolz = P.tolv = 0.0;
+  P.valid = 0;
+  P.pad = 0;
+  if (s.ok) {
+    double sum = 0.0;
+    for (int p = lane; p < W1 * W1; p += 32)
+      sum += (double)a.f[(size_t)(s.ii - 1 + p % W1) + (size_t)(s.jj - 1 + p / W1) * a.M];
+    const double fm = warp_sum(sum) / (double)(W1 * W1);
+    double ss = 0.0;
+    for (int p = lane; p < W1 * W1; p += 32) {
+      const double d = (double)a.f[(size_t)(s.ii - 1 + p % W1) + (size_t)(s.jj - 1 + p / W1) * a.M] - fm;
+      ss += d * d;
+    }
+    const double denT = sqrt(warp_sum(ss));
+    if (denT != 0) {
+      const int MW = a.M - W1 + 1;
+      const int j = (int)(t / a.nx);
+      const size_t ld = (size_t)a.M + 1;
+      const double nwin = (double)W1 * W1;
+      float2* rv = ringv + t * 4 * (long long)nda;
+      double m = 0.0;
+      for (int da = -s.L + lane; da <= s.R; da += 32) m = fmax(m, H[(size_t)(s.ii - 1 + da) + (size_t)j * MW]);
+      // the ring of partial windows: a in {0, na-1} for every b, b in {0, nb-1} for every a
+      for (int k = lane; k < 2 * s.nb; k += 32) {
+        double S1, S2;
+        const int side = k & 1, bb = k >> 1;
+        window_sums(s, w, side ? s.na - 1 : 0, bb, a.I1, a.I2, ld, &S1, &S2);
+        const double v = S2 - S1 * S1 / nwin;
+        m = fmax(m, v);
+        rv[side * nda + bb] = make_float2((float)(S1 / nwin), rsqrt_from(v));
+      }
+      for (int k = lane; k < 2 * s.na; k += 32) {
+        double S1, S2;
+        const int side = k & 1, aa = k >> 1;
+        window_sums(s, w, aa, side ? s.nb - 1 : 0, a.I1, a.I2, ld, &S1, &S2);
+        const double v = S2 - S1 * S1 / nwin;
+        m = fmax(m, v);
+        rv[(2 + side) * nda + aa] = make_float2((float)(S1 / nwin), rsqrt_from(v));
+      }
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, off));
+      P.fm = fm;
+      P.denT = denT;
+      P.tolz = sqrt(matlab_eps_d(denT * sqrt(fmax(m, 0.0))));
+      P.tolv = (P.tolz / denT) * (P.tolz / denT);
+      P.valid = 1;
+    }
+  }
+  if (lane == 0) {
+    prm[t] = P;
+    if (!P.valid) a.u[o] = a.v[o] = a.phi[o] = ALDIC_NAN;
+  }
+}
+
+// One warp per subset: for the two ring shift columns (b = 0: db = -U-1, template column 0;
+// b = nb-1: db = D+1, template column w) and every shift row, the sum over the template
+// rows of (f - cf) g at that column — the products a ring window drops.  f is centred by
+// the tile constant cf and g is zero outside the image, exactly as the tile kernel holds
+// them.
+__global__ void ring_column_kernel(SearchArgs a, const SubsetPrm* __restrict__ prm, int TI, float* __restrict__ cx) {
+  const int lane = threadIdx.x & 31;
+  const long long t = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const long long n = (long long)a.nx * a.ny;
+  if (t >= n || !prm[t].valid) return;
+  const int i = (int)(t % a.nx), j = (int)(t / a.nx);
+  const SubsetGeom s = subset_geom(a, t);
+  const float cf = tile_centre(prm, a.nx, a.ny, i - i % TI, j - j % kTJ, TI);
+  const int W1 = a.winsize + 1, DA0 = -a.s0 - 1, nda = a.s0 + a.s1 + 3;
+  const int X = s.ii - 1, Y = s.jj - 1;
+  float* out = cx + t * 2 * (long long)nda;
+  for (int side = 0; side < 2; ++side) {
+    const int c = Y + (side ? W1 - 1 : 0);
+    const int cg = c + (side ? s.D + 1 : -s.U - 1);
+    for (int k = lane; k < nda; k += 32) {
+      const int aa = DA0 + k + s.L + 1;
+      if (aa < 0 || aa >= s.na) continue;
+      float acc = 0.f;
+      for (int r = 0; r < W1; ++r) {
+        const float fv = __ldg(a.f + (size_t)(X + r) + (size_t)c * a.M) - cf;
+        const int xg = X + r + DA0 + k;
+        float gv = 0.f;
+        if (xg >= 0 && xg < a.M && cg >= 0 && cg < a.N) gv = __ldg(a.g + (size_t)xg + (size_t)cg * a.M);
+        acc = fmaf(fv, gv, acc);
+      }
+      out[side * nda + k] = acc;
+    }
+  }
+}
+
+// Pass 1 for one tile row: row-band sums RB(x, j, t) = sum over the columns c of window j
+// of F(x, c) G(x + da, c + db0 + t), t = 0..7.  frow = F row x, grow = ring row of x + da
+// at column db0 (both 16-byte aligned), rbx = RB at (j = 0, t = 0) for row x.
+template <int ST, int W1, int FC, int FRP>
+__device__ __forceinline__ void row_band_sums(const float* __restrict__ frow, const float* __restrict__ grow,
+                                              float* __restrict__ rbx) {
+  constexpr int Q = W1 / ST, REM = W1 % ST, NB = (FC + ST - 1) / ST;
+  constexpr int NGG = (FC + 7 + 3) / 4;  // 4-column groups of g covering columns 0 .. FC+6
+  constexpr int NFG = (FC + 3) / 4;
+  float g[4 * NGG], f[4 * NFG];
+  float Bk[NB][8];
+  float acc[8], P[8];
+#pragma unroll
+  for (int u = 0; u < 2; ++u) {
+    const float4 q = *reinterpret_cast<const float4*>(grow + 4 * u);
+    g[4 * u] = q.x;
+    g[4 * u + 1] = q.y;
+    g[4 * u + 2] = q.z;
+    g[4 * u + 3] = q.w;
+  }
+#pragma unroll
+  for (int c = 0; c < FC; ++c) {
+    const int kc = c / ST, cc = c % ST;
+    if (c % 4 == 0) {
+      const float4 q = *reinterpret_cast<const float4*>(frow + c);
+      f[c] = q.x;
+      f[c + 1] = q.y;
+      f[c + 2] = q.z;
+      f[c + 3] = q.w;
+    }
+    if ((c + 7) % 4 == 0 && (c + 7) / 4 >= 2) {
+      const int u = (c + 7) / 4;
+      const float4 q = *reinterpret_cast<const float4*>(grow + 4 * u);
+      g[4 * u] = q.x;
+      g[4 * u + 1] = q.y;
+      g[4 * u + 2] = q.z;
+      g[4 * u + 3] = q.w;
+    }
+    if (cc == 0) {
+#pragma unroll
+      for (int t = 0; t < 8; ++t) acc[t] = P[t] = 0.f;
+    }
+    const float fv = f[c];
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+      if (cc < REM)
+        P[t] = fmaf(fv, g[c + t], P[t]);
+      else
+        acc[t] = fmaf(fv, g[c + t], acc[t]);
+    }
+    if (cc == ST - 1 || c == FC - 1) {
+#pragma unroll
+      for (int t = 0; t < 8; ++t) Bk[kc][t] = acc[t] + P[t];
+      if (REM > 0) {
+        // window j = kc - Q: Q whole blocks j..j+Q-1 and the first REM columns of block kc
+        if (kc >= Q && kc - Q < kTJ) {
+          const int j = kc - Q;
+#pragma unroll
+          for (int t = 0; t < 8; ++t) {
+            float s = Bk[j][t];
+#pragma unroll
+            for (int b = 1; b < Q; ++b) s += Bk[j + b][t];
+            rbx[(j * kDBC + t) * FRP] = s + P[t];
+          }
+        }
+      } else {
+        if (kc >= Q - 1 && kc - Q + 1 < kTJ) {
+          const int j = kc - Q + 1;
+#pragma unroll
+          for (int t = 0; t < 8; ++t) {
+            float s = Bk[j][t];
+#pragma unroll
+            for (int b = 1; b < Q; ++b) s += Bk[j + b][t];
+            rbx[(j * kDBC + t) * FRP] = s;
+          }
+        }
+      }
+    }
+  }
+}
+
+// Pass 2 walk: window sums N[e] of NS consecutive window rows starting at tile row R0, from
+// one RB row (rb = RB + (j, d) row, 16-byte aligned) by block sums over rows.
+template <int ST, int W1, int NS, int R0>
+__device__ __forceinline__ void column_sums(const float* __restrict__ rb, float (&N)[NS]) {
+  constexpr int Q = W1 / ST, REM = W1 % ST;
+  constexpr int NBV = NS - 1 + Q + (REM > 0 ? 1 : 0);
+  constexpr int ROWS = (NS - 1) * ST + W1;
+  float v[ROWS + 3];
+#pragma unroll
+  for (int i = 0; i < ROWS; ++i) {
+    const int r = R0 + i, m = r & 3, j0 = i - m;
+    const bool in4 = (j0 >= 0) && (j0 + 3 < ROWS);  // covered by an aligned 128-bit load at j0
+    if (in4) {
+      if (m == 0) {
+        const float4 q = *reinterpret_cast<const float4*>(rb + r);
+        v[i] = q.x;
+        v[i + 1] = q.y;
+        v[i + 2] = q.z;
+        v[i + 3] = q.w;
+      }
+    } else {
+      v[i] = rb[r];
+    }
+  }
+  float BV[NBV], PV[NBV];
+#pragma unroll
+  for (int k = 0; k < NBV; ++k) BV[k] = PV[k] = 0.f;
+#pragma unroll
+  for (int r = 0; r < ROWS; ++r) {
+    if (r % ST < REM)
+      PV[r / ST] += v[r];
+    else
+      BV[r / ST] += v[r];
+  }
+#pragma unroll
+  for (int e = 0; e < NS; ++e) {
+    float s = BV[e] + PV[e];
+#pragma unroll
+    for (int b = 1; b < Q; ++b) s += BV[e + b] + PV[e + b];
+    if (REM > 0) s += PV[e + Q];
+    N[e] = s;
+  }
+}
+
+template <int ST, int W1, int TI>
+__global__ void __launch_bounds__(kTileThreads, 1)
+    ncc_tile_kernel(SearchArgs a, const float2* __restrict__ map, const double* __restrict__ Vmap,
+                    const SubsetPrm* __restrict__ prm, const float2* __restrict__ ringv,
+                    const float* __restrict__ cxv, int* __restrict__ best) {
+  using S = TileShape<ST, W1, TI>;
+  constexpr int FR = S::FR, FC = S::FC, FCP = S::FCP, GCP = S::GCP, FRP = S::FRP, H0 = S::H0, NSUB = S::NSUB;
+  constexpr int GC = FC + kDBC - 1;  // g columns a chunk needs
+  extern __shared__ __align__(16) float smf[];
+  float* Ft = smf;                  // FR x FCP: f - cf, row-major
+  float* Gt = Ft + FR * FCP;        // kRing x GCP: g, ring over rows, row-major
+  float* RB = Gt + kRing * GCP;     // (kTJ * kDBC) x FRP: one row per (window column, shift column)
+  __shared__ float p_kf[NSUB], p_invden[NSUB], p_sqtolv[NSUB];
+  __shared__ double p_tolv[NSUB];
+  __shared__ int p_ok[NSUB];
+  __shared__ int r_L[TI], r_na[TI], r_d0[TI], r_d1[TI], c_U[kTJ], c_nb[kTJ], c_d0[kTJ], c_d1[kTJ];
+  __shared__ float s_cf;
+
+  const int tid = threadIdx.x;
+  const int w = W1 - 1;
+  const int ntx = (a.nx + TI - 1) / TI;
+  const int i0 = (int)(blockIdx.x % ntx) * TI, j0 = (int)(blockIdx.x / ntx) * kTJ;
+  const int X0 = a.gx0 - 1 + i0 * ST, Y0 = a.gy0 - 1 + j0 * ST;  // 0-based tile origin
+  const int DA0 = -a.s0 - 1, NDA = a.s0 + a.s1 + 3;               // shifts, both axes
+  const int MW = a.M - W1 + 1;
+  const double nwin = (double)W1 * W1;
+  const size_t ld = (size_t)a.M + 1;
+
+  // ---- per-subset constants and geometry ----
+  if (tid == 0) s_cf = tile_centre(prm, a.nx, a.ny, i0, j0, TI);
+  if (tid >= 32 && tid < 32 + TI) {
+    const int il = tid - 32, i = i0 + il;
+    const AxisGeom r = axis_geom(a.gx0 + i * a.step, w, a.s0, a.s1, a.M, a.gx1);
+    r_L[il] = r.lo;
+    r_na[il] = i < a.nx ? r.lo + r.hi + 3 : 0;
+    r_d0[il] = r.d0;
+    r_d1[il] = r.d1;
+  } else if (tid >= 64 && tid < 64 + kTJ) {
+    const int jl = tid - 64, j = j0 + jl;
+    const AxisGeom c = axis_geom(a.gy0 + j * a.step, w, a.s0, a.s1, a.N, a.gy1);
+    c_U[jl] = c.lo;
+    c_nb[jl] = j < a.ny ? c.lo + c.hi + 3 : 0;
+    c_d0[jl] = c.d0;
+    c_d1[jl] = c.d1;
+  }
+  __syncthreads();
+  const float cf = s_cf;
+  for (int q = tid; q < NSUB; q += kTileThreads) {
+    const int i = i0 + q % TI, j = j0 + q / TI;
+    int ok = 0;
+    if (i < a.nx && j < a.ny) {
+      const SubsetPrm P = prm[i + (long long)j * a.nx];
+      ok = P.valid;
+      p_tolv[q] = P.tolv;
+      p_kf[q] = (float)(nwin * (P.fm - (double)cf));
+      p_invden[q] = ok ? (float)(1.0 / P.denT) : 0.f;
+      p_sqtolv[q] = (float)sqrt(P.tolv);
+    }
+    p_ok[q] = ok;
+  }
+  // ---- f tile, centred ----
+  for (int idx = tid; idx < FR * FCP; idx += kTileThreads) {
+    const int x = idx / FCP, c = idx % FCP;
+    float v = 0.f;
+    if (c < FC && X0 + x < a.M && Y0 + c < a.N) v = __ldg(a.f + (size_t)(X0 + x) + (size_t)(Y0 + c) * a.M) - cf;
+    Ft[idx] = v;
+  }
+
+  // pass-2 roles and running first maxima
+  const int half = tid >> 7, jl = (tid >> 4) & (kTJ - 1), dl = tid & (kDBC - 1);
+  const int il0 = half ? H0 : 0, ns = half ? TI - H0 : H0;
+  const float* rbrow = RB + (jl * kDBC + dl) * FRP;
+  float bv[H0];
+  int bl[H0];
+#pragma unroll
+  for (int e = 0; e < H0; ++e) {
+    bv[e] = -INFINITY;
+    bl[e] = 0x7fffffff;
+  }
+
+  for (int dbc = 0; dbc < NDA; dbc += kDBC) {
+    __syncthreads();
+    // g buffer for this chunk: ring rows 0..FR-1 = tile rows DA0 + rel, columns from db = DA0 + dbc
+    const int gy0 = Y0 + DA0 + dbc;
+    for (int idx = tid; idx < FR * GCP; idx += kTileThreads) {
+      const int rel = idx / GCP, col = idx % GCP;
+      const int x = X0 + DA0 + rel, y = gy0 + col;
+      float v = 0.f;
+      if (col < GC && x >= 0 && x < a.M && y >= 0 && y < a.N) v = __ldg(a.g + (size_t)x + (size_t)y * a.M);
+      Gt[idx] = v;
+    }
+    for (int idx = FR * GCP + tid; idx < kRing * GCP; idx += kTileThreads) Gt[idx] = 0.f;
+    __syncthreads();
+    const int dbr = dbc + dl, db = DA0 + dbr;
+    for (int k = 0; k < NDA; ++k) {
+      const int da = DA0 + k;
+      // ---- epilogue operands of this shift, fetched before pass 1 hides their latency ----
+      int st[H0];
+      float2 pf[H0];
+      float pcx[H0];
+#pragma unroll
+      for (int e = 0; e < H0; ++e) {
+        st[e] = 0;
+        pf[e] = make_float2(0.f, 0.f);
+        pcx[e] = 0.f;
+        if (e >= ns || dbr >= NDA) continue;
+        const int il = il0 + e, q = il + jl * TI;
+        if (!p_ok[q]) continue;
+        const int aa = da + r_L[il] + 1, bb = db + c_U[jl] + 1, na = r_na[il], nb = c_nb[jl];
+        if (aa < 0 || aa >= na || bb < 0 || bb >= nb) continue;
+        const bool ra = aa == 0 || aa == na - 1, rbg = bb == 0 || bb == nb - 1;
+        if (!ra && !rbg) {
+          pf[e] = __ldg(map + (size_t)(X0 + il * ST + da) + (size_t)(Y0 + jl * ST + db) * MW);
+          st[e] = 1;
+        } else {
+          const long long t = (long long)(i0 + il) + (long long)(j0 + jl) * a.nx;
+          const float2* rv = ringv + t * 4 * NDA;
+          pf[e] = ra ? __ldg(rv + (aa == 0 ? 0 : NDA) + bb) : __ldg(rv + (bb == 0 ? 2 : 3) * NDA + aa);
+          if (rbg) pcx[e] = __ldg(cxv + t * 2 * NDA + (bb == 0 ? 0 : NDA) + k);
+          st[e] = 2 | (ra ? 4 : 0) | (rbg ? 8 : 0) | (aa == 0 ? 16 : 0) | (bb == 0 ? 32 : 0);
+        }
+      }
+      // the ring row of shift row k + 1 goes to the one slot pass 1 does not read
+      float nrow = 0.f;
+      if (k + 1 < NDA && tid < GC) {
+        const int x = X0 + DA0 + k + FR, y = gy0 + tid;
+        if (x >= 0 && x < a.M && y >= 0 && y < a.N) nrow = __ldg(a.g + (size_t)x + (size_t)y * a.M);
+      }
+      // ---- pass 1 ----
+      {
+        const int grp = tid >> 7, x = tid & 127;
+        if (x < FR)
+          row_band_sums<ST, W1, FC, FRP>(Ft + x * FCP, Gt + ((x + k) & (kRing - 1)) * GCP + grp * 8,
+                                         RB + (grp * 8) * FRP + x);
+      }
+      if (k + 1 < NDA && tid < GCP) Gt[((k + FR) & (kRing - 1)) * GCP + tid] = nrow;
+      __syncthreads();
+      // ---- pass 2 ----
+      if (dbr < NDA) {
+        float N[H0];
+        if (half == 0) {
+          column_sums<ST, W1, H0, 0>(rbrow, N);
+        } else {
+          float N1[TI - H0 > 0 ? TI - H0 : 1];
+          column_sums<ST, W1, (TI - H0 > 0 ? TI - H0 : 1), H0 * ST>(rbrow, N1);
+#pragma unroll
+          for (int e = 0; e < TI - H0; ++e) N[e] = N1[e];
+        }
+#pragma unroll
+        for (int e = 0; e < H0; ++e) {
+          const int sf = st[e];
+          if (!sf) continue;
+          const int il = il0 + e, q = il + jl * TI;
+          float C = N[e];
+          if (sf & 2) {  // partial window: drop the template row / column whose partner is outside D
+            const int rx = (sf & 16) ? il * ST : il * ST + W1 - 1;
+            const int cxc = (sf & 32) ? jl * ST : jl * ST + W1 - 1;
+            if (sf & 4) C -= rbrow[rx];
+            if (sf & 8) {
+              C -= pcx[e];
+              if (sf & 4) C += Ft[rx * FCP + cxc] * Gt[((rx + k) & (kRing - 1)) * GCP + cxc + dl];
+            }
+          }
+          const float2 v = pf[e];
+          const float num = C - p_kf[q] * v.x;
+          float cval;
+          if (v.y * p_sqtolv[q] < 0.5f) {
+            cval = num * v.y * p_invden[q];
+          } else {  // near the zero threshold: decide it on the FP64 variance sum
+            const int aa = da + r_L[il] + 1, bb = db + c_U[jl] + 1;
+            double var;
+            if (sf & 2) {
+              SubsetGeom sg;
+              sg.dr0 = r_d0[il];
+              sg.dr1 = r_d1[il];
+              sg.dc0 = c_d0[jl];
+              sg.dc1 = c_d1[jl];
+              double S1, S2;
+              window_sums(sg, w, aa, bb, a.I1, a.I2, ld, &S1, &S2);
+              var = fmax(S2 - S1 * S1 / nwin, 0.0);
+            } else {
+              var = fmax(Vmap[(size_t)(X0 + il * ST + da) + (size_t)(Y0 + jl * ST + db) * MW], 0.0);
+            }
+            cval = var > p_tolv[q] ? num * (float)(1.0 / sqrt(var)) * p_invden[q] : 0.f;
+          }
+          if (fabsf(cval) - 1.f > 1.4901161193847656e-08f) cval = 0.f;
+          const int lin = (da + r_L[il] + 1) + (db + c_U[jl] + 1) * r_na[il];
+          if (cval > bv[e] || (cval == bv[e] && lin < bl[e])) {
+            bv[e] = cval;
+            bl[e] = lin;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  // ---- first maximum per subset over the 16 shift-column lanes ----
+  float* rv = RB;
+  int* ri = reinterpret_cast<int*>(RB + NSUB * kDBC);
+#pragma unroll
+  for (int e = 0; e < H0; ++e) {
+    if (e >= ns) break;
+    const int q = (il0 + e) + jl * TI;
+    rv[q * kDBC + dl] = bv[e];
+    ri[q * kDBC + dl] = bl[e];
+  }
+  __syncthreads();
+  for (int q = tid; q < NSUB; q += kTileThreads) {
+    if (!p_ok[q]) continue;
+    float b = rv[q * kDBC];
+    int bi = ri[q * kDBC];
+    for (int l = 1; l < kDBC; ++l) {
+      const float v = rv[q * kDBC + l];
+      const int li = ri[q * kDBC + l];
+      if (v > b || (v == b && li < bi)) {
+        b = v;
+        bi = li;
+      }
+    }
+    const int i = i0 + q % TI, j = j0 + q / TI;
+    best[i + (long long)j * a.nx] = bi == 0x7fffffff ? 0 : bi;
+  }
+}
+
+// FP64 refit + findpeak at the argmax of every valid subset (one CTA per subset).
+__global__ void __launch_bounds__(128) subset_refit_kernel(SearchArgs a, const SubsetPrm* __restrict__ prm,
+                                                           const int* __restrict__ best) {
+  __shared__ double red[4 * 9];
+  __shared__ double sums[9];
+  const long long n = (long long)a.nx * a.ny;
+  for (long long t = blockIdx.x; t < n; t += gridDim.x) {
+    const SubsetPrm P = prm[t];
+    if (!P.valid) continue;
+    const SubsetGeom s = subset_geom(a, t);
+    const int bi = best[t];
+    refit_peak(a, s, subset_out(a, t), bi % s.na, bi / s.na, P.fm, P.denT, P.tolz, red, sums);
+  }
+}
+
+namespace {
+
+struct TileEntry {
+  int TI;
+  int (*launch)(const SearchArgs&, const TileScratch&, cudaStream_t);
+};
+
+template <int ST, int W1>
+int launch_tile(const SearchArgs& a, const TileScratch& sc, cudaStream_t st) {
+  constexpr int TI = TileFor<ST, W1>::TI;
+  using S = TileShape<ST, W1, TI>;
+  auto kern = ncc_tile_kernel<ST, W1, TI>;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::smem_bytes) != cudaSuccess)
+    return -1;
+  const long long tiles = (long long)((a.nx + TI - 1) / TI) * ((a.ny + kTJ - 1) / kTJ);
+  kern<<<(unsigned)tiles, kTileThreads, S::smem_bytes, st>>>(a, sc.map, sc.V, sc.prm, sc.ringv, sc.cx, sc.best);
+  return 0;
+}
+
+template <int ST, int W1>
+TileEntry entry() {
+  return TileEntry{TileFor<ST, W1>::TI, launch_tile<ST, W1>};
+}
+
+// The step / window pairs with a tile kernel (others use the per-subset kernel).
+bool tile_entry(int step, int W1, TileEntry* e) {
+  switch (step * 1000 + W1) {
+    case 10 * 1000 + 41: *e = entry<10, 41>(); return true;
+    case 16 * 1000 + 31: *e = entry<16, 31>(); return true;
+    case 16 * 1000 + 33: *e = entry<16, 33>(); return true;
+    case 12 * 1000 + 21: *e = entry<12, 21>(); return true;
+    case 9 * 1000 + 17: *e = entry<9, 17>(); return true;
+    case 8 * 1000 + 33: *e = entry<8, 33>(); return true;
+    default: return false;
+  }
+}
+
+}  // namespace
+
+size_t search_tile_bytes(int M, int N, int winsize, int step, int nx, int ny, int s0, int s1) {
+  const int W1 = winsize + 1;
+  TileEntry e;
+  if (!tile_entry(step, W1, &e) || M < W1 || N < W1 || nx <= 0 || ny <= 0) return 0;
+  return scratch_layout(M, N, W1, nx, ny, s0 + s1 + 3, nullptr, nullptr);
+}
+
+int launch_search_tile(const SearchArgs& a, cudaStream_t st) {
+  const int W1 = a.winsize + 1;
+  TileEntry e;
+  if (!tile_entry(a.step, W1, &e) || !a.tile_scratch || a.M < W1 || a.N < W1) return -1;
+  const int nda = a.s0 + a.s1 + 3;
+  TileScratch sc;
+  scratch_layout(a.M, a.N, W1, a.nx, a.ny, nda, (char*)a.tile_scratch, &sc);
+  const long long n = (long long)a.nx * a.ny;
+  const long long npos = (long long)(a.M - W1 + 1) * (a.N - W1 + 1);
+  window_map_kernel<<<(unsigned)((npos + 255) / 256), 256, 0, st>>>(a.I1, a.I2, a.M, a.N, W1, sc.map, sc.V);
+  const long long nh = (long long)(a.M - W1 + 1) * a.ny;
+  window_rowmax_kernel<<<(unsigned)((nh + 255) / 256), 256, 0, st>>>(a, sc.V, sc.H);
+  subset_prep_kernel<<<(unsigned)((n * 32 + 255) / 256), 256, 0, st>>>(a, sc.H, sc.prm, sc.ringv);
+  ring_column_kernel<<<(unsigned)((n * 32 + 255) / 256), 256, 0, st>>>(a, sc.prm, e.TI, sc.cx);
+  if (a.ev_start) cudaEventRecord(a.ev_start, st);
+  if (e.launch(a, sc, st) != 0) return -1;
+  if (a.ev_stop) cudaEventRecord(a.ev_stop, st);
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const long long grid = n < (long long)sms * 8 ? n : (long long)sms * 8;
+  subset_refit_kernel<<<(unsigned)grid, 128, 0, st>>>(a, sc.prm, sc.best);
+  return 6;
+}
+
+}  // namespace aldic

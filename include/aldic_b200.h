@@ -162,6 +162,12 @@ int aldic_local_icgn_noalloc(int variant, const float* ref, const float* def, co
 /* Measured FP32 FMA throughput of the current device (TFLOP/s), the denominator the
  * library's compute-bound kernels are reported against.  Not part of the reference. */
 int aldic_measure_fp32_peak(aldic_ctx* ctx, double* tflops);
+/* Device time of the correlation kernel of every aldic_integer_search call while profiling
+ * is on (CUDA events recorded on the context's stream around that one launch; up to 256
+ * calls are kept).  aldic_profile_read waits for the recorded events, returns their total
+ * time and count, and clears the record.  A measurement hook; not part of the reference. */
+int aldic_set_profiling(aldic_ctx* ctx, int on);
+int aldic_profile_read(aldic_ctx* ctx, double* total_ms, int* launches);
 
 #ifdef __cplusplus
 }

@@ -111,6 +111,40 @@ def test_integer_search_edge_cases(ctx):
     assert np.isnan(ctx.integer_search([3, 7], [1, 200], [1, 180], 20, 12)["u"][0, 0])
 
 
+@pytest.mark.parametrize("w,st,search,grid", [
+    (40, 10, (12, 12), ([1, 330], [1, 300])),   # shared-product tile kernel, the stereo workload's shape
+    (40, 10, (3, 9), ([7, 322], [4, 290])),     # same, rectangular search and border clamps
+    (32, 16, (8, 8), ([1, 330], [1, 300])),     # tile kernel with REM = 1, Q = 2
+    (24, 7, (5, 6), ([1, 330], [1, 300])),      # no tile kernel for this pair: per-subset kernel
+])
+def test_integer_search_parity_paths(ctx, w, st, search, grid):
+    sc = synth.temporal_affine(M=330, N=300, n_speckles=1500, u=3.4, v=-2.7)
+    _load_raw(ctx, sc)
+    f, g = ctx.get_state(0), ctx.get_state(1)
+    r = ctx.integer_search(list(search), grid[0], grid[1], w, st)
+    ro = O.integer_search(f, g, list(search), grid[0], grid[1], w, st)
+    assert np.array_equal(r["x"], ro["x"]) and np.array_equal(r["y"], ro["y"])
+    assert np.array_equal(np.isnan(r["u"]), np.isnan(ro["u"]))
+    ok = np.isfinite(ro["u"])
+    assert ok.sum() > 50
+    assert np.array_equal(r["u"][ok], ro["u"][ok]) and np.array_equal(r["v"][ok], ro["v"][ok])
+    assert np.max(np.abs(r["phi"][ok] - ro["phi"][ok])) < 1e-6
+
+
+def test_search_profiling_hook(ctx, affine):
+    _load_raw(ctx, affine)
+    M, N = affine.ref.shape
+    ctx.set_profiling(True)
+    ctx.profile_read()
+    ctx.integer_search([10, 10], [1, M], [1, N], 30, 16)
+    ctx.integer_search([10, 10], [1, M], [1, N], 30, 16)
+    ms, n = ctx.profile_read()
+    ctx.set_profiling(False)
+    assert n == 2 and ms > 0
+    ctx.integer_search([10, 10], [1, M], [1, N], 30, 16)
+    assert ctx.profile_read() == (0.0, 0)
+
+
 @pytest.mark.parametrize("variant", [0, 1])
 def test_local_icgn_parity_affine(ctx, affine, variant):
     sc = affine
