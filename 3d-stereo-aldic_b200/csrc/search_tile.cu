@@ -380,6 +380,185 @@ __device__ __forceinline__ void column_sums(const float* __restrict__ rb, float 
   }
 }
 
+// Pass 1 with packed FP32 pairs (even steps): the same row-band sums as row_band_sums.
+// At an even column c the 8 products f(c) g(c + t) are 4 pairs t = (0,1) .. (6,7) of
+// aligned g pairs; at an odd column, t = (1,2) .. (5,6) are aligned pairs and t = 0, 7
+// scalars.  Even and odd columns accumulate separately (E and O) and are added at the
+// block end; the first REM columns of a block (P) seed the remaining columns' sums.
+template <int ST, int W1, int FC, int FRP>
+__device__ __forceinline__ void row_band_sums_x2(const float* __restrict__ frow, const float* __restrict__ grow,
+                                                 float* __restrict__ rbx) {
+  static_assert(ST % 2 == 0, "blocks must start on even columns");
+  constexpr int Q = W1 / ST, REM = W1 % ST, NB = (FC + ST - 1) / ST;
+  constexpr int NGG = (FC + 7 + 3) / 4;  // 4-column groups of g covering columns 0 .. FC+6
+  constexpr int NFG = (FC + 3) / 4;
+  constexpr int E_A0 = (REM + 1) / 2 * 2;  // first even column of a block outside P
+  constexpr int O_A0 = REM / 2 * 2 + 1;    // first odd column of a block outside P
+  float2 gp[2 * NGG];                      // gp[m] = (g(2m), g(2m+1))
+  float f[4 * NFG];
+  float2 B[NB][4], S2[NB][4];              // block sums and sums of consecutive block pairs, t pairs
+  float2 PE[4], AE[4], PO[3], AO[3];
+  float PO0 = 0.f, PO7 = 0.f, AO0 = 0.f, AO7 = 0.f;
+#pragma unroll
+  for (int u = 0; u < 2; ++u) {
+    const float4 q = *reinterpret_cast<const float4*>(grow + 4 * u);
+    gp[2 * u] = make_float2(q.x, q.y);
+    gp[2 * u + 1] = make_float2(q.z, q.w);
+  }
+#pragma unroll
+  for (int c = 0; c < FC; ++c) {
+    const int kc = c / ST, cc = c % ST;
+    if (c % 4 == 0) {
+      const float4 q = *reinterpret_cast<const float4*>(frow + c);
+      f[c] = q.x;
+      f[c + 1] = q.y;
+      f[c + 2] = q.z;
+      f[c + 3] = q.w;
+    }
+    if ((c + 7) % 4 == 0 && (c + 7) / 4 >= 2) {
+      const int u = (c + 7) / 4;
+      const float4 q = *reinterpret_cast<const float4*>(grow + 4 * u);
+      gp[2 * u] = make_float2(q.x, q.y);
+      gp[2 * u + 1] = make_float2(q.z, q.w);
+    }
+    const float2 ff = make_float2(f[c], f[c]);
+    if (cc % 2 == 0) {
+      const int m = c / 2;  // gp[m + i] = (g(c + 2i), g(c + 2i + 1))
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        if (cc < REM)
+          PE[i] = (cc == 0) ? fmul2(ff, gp[m + i]) : ffma2(ff, gp[m + i], PE[i]);
+        else if (cc == E_A0)
+          AE[i] = (REM > 0) ? ffma2(ff, gp[m + i], PE[i]) : fmul2(ff, gp[m + i]);
+        else
+          AE[i] = ffma2(ff, gp[m + i], AE[i]);
+      }
+    } else {
+      const int m = (c + 1) / 2;  // gp[m + i] = (g(c + 1 + 2i), g(c + 2 + 2i))
+      const float g0 = gp[m - 1].y, g7 = gp[m + 3].x;
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        if (cc < REM)
+          PO[i] = (cc == 1) ? fmul2(ff, gp[m + i]) : ffma2(ff, gp[m + i], PO[i]);
+        else if (cc == O_A0)
+          AO[i] = (REM > 1) ? ffma2(ff, gp[m + i], PO[i]) : fmul2(ff, gp[m + i]);
+        else
+          AO[i] = ffma2(ff, gp[m + i], AO[i]);
+      }
+      if (cc < REM) {
+        PO0 = (cc == 1) ? f[c] * g0 : fmaf(f[c], g0, PO0);
+        PO7 = (cc == 1) ? f[c] * g7 : fmaf(f[c], g7, PO7);
+      } else if (cc == O_A0) {
+        AO0 = (REM > 1) ? fmaf(f[c], g0, PO0) : f[c] * g0;
+        AO7 = (REM > 1) ? fmaf(f[c], g7, PO7) : f[c] * g7;
+      } else {
+        AO0 = fmaf(f[c], g0, AO0);
+        AO7 = fmaf(f[c], g7, AO7);
+      }
+    }
+    if (cc == ST - 1 || c == FC - 1) {
+      // P of this block (first REM columns) as t pairs
+      float2 P[4];
+      if (REM > 1) {
+        P[0] = make_float2(PE[0].x + PO0, PE[0].y + PO[0].x);
+        P[1] = make_float2(PE[1].x + PO[0].y, PE[1].y + PO[1].x);
+        P[2] = make_float2(PE[2].x + PO[1].y, PE[2].y + PO[2].x);
+        P[3] = make_float2(PE[3].x + PO[2].y, PE[3].y + PO7);
+      } else if (REM == 1) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) P[i] = PE[i];
+      }
+      if (cc == ST - 1) {  // a whole block: its sum (P alone where no column of a parity follows it)
+        float2 e[4], o[3];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) e[i] = (E_A0 < ST) ? AE[i] : PE[i];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) o[i] = (O_A0 < ST) ? AO[i] : PO[i];
+        const float o0 = (O_A0 < ST) ? AO0 : PO0, o7 = (O_A0 < ST) ? AO7 : PO7;
+        B[kc][0] = make_float2(e[0].x + o0, e[0].y + o[0].x);
+        B[kc][1] = make_float2(e[1].x + o[0].y, e[1].y + o[1].x);
+        B[kc][2] = make_float2(e[2].x + o[1].y, e[2].y + o[2].x);
+        B[kc][3] = make_float2(e[3].x + o[2].y, e[3].y + o7);
+        if (kc >= 1) {
+#pragma unroll
+          for (int i = 0; i < 4; ++i) S2[kc - 1][i] = fadd2(B[kc - 1][i], B[kc][i]);
+        }
+      }
+      // window j ends in this block: Q whole blocks j..j+Q-1 (+ the first REM columns of block kc)
+      const int j = REM > 0 ? kc - Q : kc - Q + 1;
+      if (j >= 0 && j < kTJ) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          float2 s = (Q >= 2) ? S2[j][i] : B[j][i];
+#pragma unroll
+          for (int b = 2; b < Q; b += 2) s = fadd2(s, (b + 1 < Q) ? S2[j + b][i] : B[j + b][i]);
+          if (REM > 0) s = fadd2(s, P[i]);
+          rbx[(j * kDBC + 2 * i) * FRP] = s.x;
+          rbx[(j * kDBC + 2 * i + 1) * FRP] = s.y;
+        }
+      }
+    }
+  }
+}
+
+// Pass 2 with packed pairs of rows (even steps; R0 even): window sums as column_sums.
+template <int ST, int W1, int NS, int R0>
+__device__ __forceinline__ void column_sums_x2(const float* __restrict__ rb, float (&N)[NS]) {
+  static_assert(ST % 2 == 0 && R0 % 2 == 0, "row pairs must align with blocks");
+  constexpr int Q = W1 / ST, REM = W1 % ST;
+  constexpr int NBV = NS - 1 + Q + (REM > 0 ? 1 : 0);
+  constexpr int ROWS = (NS - 1) * ST + W1;
+  constexpr int NP = (ROWS + 1) / 2;
+  float2 v[NP + 2];
+#pragma unroll
+  for (int p = 0; p < NP; ++p) {
+    const int r = R0 + 2 * p;  // even
+    if (r % 4 == 0 && 2 * p + 3 < ROWS) {
+      const float4 q = *reinterpret_cast<const float4*>(rb + r);
+      v[p] = make_float2(q.x, q.y);
+      v[p + 1] = make_float2(q.z, q.w);
+    } else if (r % 4 == 2 && p >= 1 && 2 * (p - 1) + 3 < ROWS) {
+      // loaded with the previous 128-bit load
+    } else if (2 * p + 1 < ROWS) {
+      v[p] = *reinterpret_cast<const float2*>(rb + r);
+    } else {
+      v[p] = make_float2(rb[r], 0.f);
+    }
+  }
+  float Bs[NBV], Ps[NBV];
+#pragma unroll
+  for (int kb = 0; kb < NBV; ++kb) {
+    const int r0 = kb * ST;  // even
+    float pv = 0.f;          // first REM rows
+#pragma unroll
+    for (int r = 0; r < REM; ++r) {
+      const float x = ((r0 + r) % 2) ? v[(r0 + r) / 2].y : v[(r0 + r) / 2].x;
+      pv = (r == 0) ? x : pv + x;
+    }
+    Ps[kb] = pv;
+    if (r0 + ST <= ROWS) {  // whole block: pair tree over ST / 2 row pairs
+      float2 t[ST / 2];
+#pragma unroll
+      for (int i = 0; i < ST / 2; ++i) t[i] = v[r0 / 2 + i];
+#pragma unroll
+      for (int h = 1; h < ST / 2; h *= 2)
+#pragma unroll
+        for (int i = 0; i + h < ST / 2; i += 2 * h) t[i] = fadd2(t[i], t[i + h]);
+      Bs[kb] = t[0].x + t[0].y;
+    } else {
+      Bs[kb] = 0.f;
+    }
+  }
+#pragma unroll
+  for (int e = 0; e < NS; ++e) {
+    float s = Bs[e];
+#pragma unroll
+    for (int b = 1; b < Q; ++b) s += Bs[e + b];
+    if (REM > 0) s += Ps[e + Q];
+    N[e] = s;
+  }
+}
+
 template <int ST, int W1, int TI>
 __global__ void __launch_bounds__(kTileThreads, 1)
     ncc_tile_kernel(SearchArgs a, const float2* __restrict__ map, const double* __restrict__ Vmap,
@@ -511,9 +690,14 @@ __global__ void __launch_bounds__(kTileThreads, 1)
       // ---- pass 1 ----
       {
         const int grp = tid >> 7, x = tid & 127;
-        if (x < FR)
-          row_band_sums<ST, W1, FC, FRP>(Ft + x * FCP, Gt + ((x + k) & (kRing - 1)) * GCP + grp * 8,
-                                         RB + (grp * 8) * FRP + x);
+        if (x < FR) {
+          if constexpr (ST % 2 == 0)
+            row_band_sums_x2<ST, W1, FC, FRP>(Ft + x * FCP, Gt + ((x + k) & (kRing - 1)) * GCP + grp * 8,
+                                              RB + (grp * 8) * FRP + x);
+          else
+            row_band_sums<ST, W1, FC, FRP>(Ft + x * FCP, Gt + ((x + k) & (kRing - 1)) * GCP + grp * 8,
+                                           RB + (grp * 8) * FRP + x);
+        }
       }
       if (k + 1 < NDA && tid < GCP) Gt[((k + FR) & (kRing - 1)) * GCP + tid] = nrow;
       __syncthreads();
@@ -521,10 +705,16 @@ __global__ void __launch_bounds__(kTileThreads, 1)
       if (dbr < NDA) {
         float N[H0];
         if (half == 0) {
-          column_sums<ST, W1, H0, 0>(rbrow, N);
+          if constexpr (ST % 2 == 0)
+            column_sums_x2<ST, W1, H0, 0>(rbrow, N);
+          else
+            column_sums<ST, W1, H0, 0>(rbrow, N);
         } else {
           float N1[TI - H0 > 0 ? TI - H0 : 1];
-          column_sums<ST, W1, (TI - H0 > 0 ? TI - H0 : 1), H0 * ST>(rbrow, N1);
+          if constexpr (ST % 2 == 0)
+            column_sums_x2<ST, W1, (TI - H0 > 0 ? TI - H0 : 1), H0 * ST>(rbrow, N1);
+          else
+            column_sums<ST, W1, (TI - H0 > 0 ? TI - H0 : 1), H0 * ST>(rbrow, N1);
 #pragma unroll
           for (int e = 0; e < TI - H0; ++e) N[e] = N1[e];
         }
