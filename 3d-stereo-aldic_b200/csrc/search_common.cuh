@@ -104,81 +104,120 @@ struct SubsetPrm {
   int pad;
 };
 
-// FP64 NCC of the 3 x 3 neighbourhood of the crop peak (pa, pb), then findpeak
-// (func/findpeak.m:27-66) and the displacement of funIntegerSearch.m:170-190.  Called by
-// every thread of the block (block-wide reduction); thread 0 writes u, v, phi.
+// FP64 NCC at crop shift (aa, bb) from its numerator sum((T - mean) D): the normxcorr2
+// zero rules (denominator threshold tolz, |C| - 1 > sqrt(eps(1)) -> 0); 0 outside the crop.
+__device__ inline double ncc_at(const SearchArgs& a, const SubsetGeom& s, int aa, int bb, double num, double denT,
+                                double tolz) {
+  if (aa < 0 || aa >= s.na || bb < 0 || bb >= s.nb) return 0.0;
+  const int w = a.winsize, W1 = w + 1;
+  double S1, S2;
+  window_sums(s, w, aa, bb, a.I1, a.I2, (size_t)a.M + 1, &S1, &S2);
+  const double den = denT * sqrt(fmax(S2 - S1 * S1 / ((double)W1 * W1), 0.0));
+  double cv = (den > tolz) ? num / den : 0.0;
+  if (fabs(cv) - 1 > 1.4901161193847656e-08) cv = 0.0;
+  return cv;
+}
+
+// findpeak (func/findpeak.m:27-66) on the 3 x 3 NCC values around the crop peak (pa, pb),
+// cc[(row offset + 1) + 3 (column offset + 1)], and the displacement of
+// funIntegerSearch.m:170-190 written to slot o.
+__device__ inline void findpeak_store(const SearchArgs& a, const SubsetGeom& s, long long o, int pa, int pb,
+                                      const double (&cc)[9]) {
+  // xpeak = crop column, ypeak = crop row (1-based)
+  double xpeak = pb + 1, ypeak = pa + 1, maxf = cc[4];
+  const bool edge = (pb == 0 || pb == s.nb - 1 || pa == 0 || pa == s.na - 1);
+  if (!edge) {
+    // u(dx, dy) with dx = column offset, dy = row offset: cc[(dy+1) + 3 (dx+1)]
+    double S = 0, Sx = 0, Sy = 0, Sx2 = 0, Sy2 = 0;
+    for (int dx = -1; dx <= 1; ++dx)
+      for (int dy = -1; dy <= 1; ++dy) {
+        const double u = cc[(dy + 1) + 3 * (dx + 1)];
+        S += u;
+        Sx += dx * u;
+        Sy += dy * u;
+        if (dx != 0) Sx2 += u;
+        if (dy != 0) Sy2 += u;
+      }
+    const double A2 = Sx / 6.0, A3 = Sy / 6.0;
+    const double A4 = (cc[8] - cc[6] - cc[2] + cc[0]) / 4.0;
+    const double A5 = Sx2 / 2.0 - S / 3.0, A6 = Sy2 / 2.0 - S / 3.0;
+    const double A1 = (5.0 * S - 3.0 * (Sx2 + Sy2)) / 9.0;
+    const double dd = A4 * A4 - 4 * A5 * A6;
+    double xo = (-A3 * A4 + 2 * A6 * A2) / dd;
+    double yo = -1 / dd * (A4 * A2 - 2 * A5 * A3);
+    if (!(fabs(xo) > 1 || fabs(yo) > 1)) {
+      xo = round(1000 * xo) / 1000;
+      yo = round(1000 * yo) / 1000;
+      xpeak += xo;
+      ypeak += yo;
+      maxf = A1 + A2 * xo + A3 * yo + A4 * xo * yo + A5 * xo * xo + A6 * yo * yo;
+    }
+  }
+  a.u[o] = ypeak - 2 - s.L;
+  a.v[o] = xpeak - 2 - s.U;
+  a.phi[o] = maxf;
+}
+
+// Per-thread FP64 numerator partials of the 3 x 3 neighbourhood of (pa, pb): template
+// elements p = first, first + stride, ...
+__device__ __forceinline__ void peak_partials(const SearchArgs& a, const SubsetGeom& s, int pa, int pb, double tm,
+                                              int first, int stride, double (&v)[9]) {
+  const int W1 = a.winsize + 1;
+#pragma unroll
+  for (int k = 0; k < 9; ++k) v[k] = 0.0;
+  int i = first % W1, j = first / W1;
+  const int di = stride % W1, dj = stride / W1;
+  for (int p = first; p < W1 * W1; p += stride) {
+    const double tv = (double)a.f[(size_t)(s.ii - 1 + i) + (size_t)(s.jj - 1 + j) * a.M] - tm;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      const int r = s.dr0 - 2 + pa + (k % 3) + i, c = s.dc0 - 2 + pb + (k / 3) + j;
+      double d = 0.0;
+      if (r >= s.dr0 && r <= s.dr1 && c >= s.dc0 && c <= s.dc1) d = (double)a.g[(size_t)r + (size_t)c * a.M];
+      v[k] += tv * d;
+    }
+    i += di;
+    j += dj;
+    if (i >= W1) {
+      i -= W1;
+      ++j;
+    }
+  }
+}
+
+// Block version: every thread of the block calls it; thread 0 writes u, v, phi.
 __device__ inline void refit_peak(const SearchArgs& a, const SubsetGeom& s, long long o, int pa, int pb, double tm,
                                   double denT, double tolz, double* red, double* sums) {
-  const int w = a.winsize, W1 = w + 1;
-  const size_t ld = (size_t)a.M + 1;
-  const int nwarps = blockDim.x >> 5;
   {
     double v[9];
-#pragma unroll
-    for (int k = 0; k < 9; ++k) v[k] = 0.0;
-    for (int p = threadIdx.x; p < W1 * W1; p += blockDim.x) {
-      const int i = p % W1, j = p / W1;
-      const double tv = (double)a.f[(size_t)(s.ii - 1 + i) + (size_t)(s.jj - 1 + j) * a.M] - tm;
-#pragma unroll
-      for (int k = 0; k < 9; ++k) {
-        const int aa = pa + (k % 3) - 1, bb = pb + (k / 3) - 1;
-        const int r = s.dr0 - 1 + aa + i, c = s.dc0 - 1 + bb + j;
-        double d = 0.0;
-        if (r >= s.dr0 && r <= s.dr1 && c >= s.dc0 && c <= s.dc1) d = (double)a.g[(size_t)r + (size_t)c * a.M];
-        v[k] += tv * d;
-      }
-    }
-    block_sum_dyn<9>(v, red, sums, nwarps);
+    peak_partials(a, s, pa, pb, tm, threadIdx.x, blockDim.x, v);
+    block_sum_dyn<9>(v, red, sums, blockDim.x >> 5);
   }
   if (threadIdx.x == 0) {
-    const double nwin = (double)W1 * W1;
     double cc[9];
-    for (int k = 0; k < 9; ++k) {
-      const int aa = pa + (k % 3) - 1, bb = pb + (k / 3) - 1;
-      cc[k] = 0.0;
-      if (aa < 0 || aa >= s.na || bb < 0 || bb >= s.nb) continue;
-      double S1, S2;
-      window_sums(s, w, aa, bb, a.I1, a.I2, ld, &S1, &S2);
-      const double den = denT * sqrt(fmax(S2 - S1 * S1 / nwin, 0.0));
-      double cv = (den > tolz) ? sums[k] / den : 0.0;
-      if (fabs(cv) - 1 > 1.4901161193847656e-08) cv = 0.0;
-      cc[k] = cv;
-    }
-    // findpeak; xpeak = crop column, ypeak = crop row (1-based)
-    double xpeak = pb + 1, ypeak = pa + 1, maxf = cc[4];
-    const bool edge = (pb == 0 || pb == s.nb - 1 || pa == 0 || pa == s.na - 1);
-    if (!edge) {
-      // u(dx, dy) with dx = column offset, dy = row offset: cc[(dy+1) + 3 (dx+1)]
-      double S = 0, Sx = 0, Sy = 0, Sx2 = 0, Sy2 = 0;
-      for (int dx = -1; dx <= 1; ++dx)
-        for (int dy = -1; dy <= 1; ++dy) {
-          const double u = cc[(dy + 1) + 3 * (dx + 1)];
-          S += u;
-          Sx += dx * u;
-          Sy += dy * u;
-          if (dx != 0) Sx2 += u;
-          if (dy != 0) Sy2 += u;
-        }
-      const double A2 = Sx / 6.0, A3 = Sy / 6.0;
-      const double A4 = (cc[8] - cc[6] - cc[2] + cc[0]) / 4.0;
-      const double A5 = Sx2 / 2.0 - S / 3.0, A6 = Sy2 / 2.0 - S / 3.0;
-      const double A1 = (5.0 * S - 3.0 * (Sx2 + Sy2)) / 9.0;
-      const double dd = A4 * A4 - 4 * A5 * A6;
-      double xo = (-A3 * A4 + 2 * A6 * A2) / dd;
-      double yo = -1 / dd * (A4 * A2 - 2 * A5 * A3);
-      if (!(fabs(xo) > 1 || fabs(yo) > 1)) {
-        xo = round(1000 * xo) / 1000;
-        yo = round(1000 * yo) / 1000;
-        xpeak += xo;
-        ypeak += yo;
-        maxf = A1 + A2 * xo + A3 * yo + A4 * xo * yo + A5 * xo * xo + A6 * yo * yo;
-      }
-    }
-    a.u[o] = ypeak - 2 - s.L;
-    a.v[o] = xpeak - 2 - s.U;
-    a.phi[o] = maxf;
+    for (int k = 0; k < 9; ++k) cc[k] = ncc_at(a, s, pa + (k % 3) - 1, pb + (k / 3) - 1, sums[k], denT, tolz);
+    findpeak_store(a, s, o, pa, pb, cc);
   }
   __syncthreads();
+}
+
+// Warp version: the 32 lanes of one warp call it; the 9 NCC values are formed by lanes
+// 0..8 in parallel and lane 0 writes u, v, phi.
+__device__ inline void refit_peak_warp(const SearchArgs& a, const SubsetGeom& s, long long o, int pa, int pb,
+                                       double tm, double denT, double tolz) {
+  const int lane = threadIdx.x & 31;
+  double v[9];
+  peak_partials(a, s, pa, pb, tm, lane, 32, v);
+#pragma unroll
+  for (int k = 0; k < 9; ++k) v[k] = warp_sum(v[k]);
+  double mine = 0.0;
+#pragma unroll
+  for (int k = 0; k < 9; ++k)
+    if (lane == k) mine = ncc_at(a, s, pa + (k % 3) - 1, pb + (k / 3) - 1, v[k], denT, tolz);
+  double cc[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) cc[k] = __shfl_sync(0xffffffffu, mine, k);
+  if (lane == 0) findpeak_store(a, s, o, pa, pb, cc);
 }
 
 }  // namespace aldic

@@ -65,6 +65,7 @@ struct TileScratch {
   float2* ringv;     // nx * ny x 4 NDA: (mean, 1/sqrt(variance sum)) of the partial windows
   float* cx;         // nx * ny x 2 NDA: products of the excluded template column
   int* best;         // nx * ny: crop index of the first maximum
+  float* cf;         // one centring constant per tile
 };
 
 inline size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
@@ -84,7 +85,9 @@ inline size_t scratch_layout(int M, int N, int W1, int nx, int ny, int nda, char
   char* pr = take(n * 4 * (size_t)nda * sizeof(float2));
   char* pc = take(n * 2 * (size_t)nda * sizeof(float));
   char* pb = take(n * sizeof(int));
+  char* pf = take(n * sizeof(float));  // >= the number of tiles
   if (sc) {
+    sc->cf = (float*)pf;
     sc->map = (float2*)pm;
     sc->V = (double*)pv;
     sc->H = (double*)ph;
@@ -225,14 +228,15 @@ __global__ void subset_prep_kernel(SearchArgs a, const double* __restrict__ H, S
 // rows of (f - cf) g at that column — the products a ring window drops.  f is centred by
 // the tile constant cf and g is zero outside the image, exactly as the tile kernel holds
 // them.
-__global__ void ring_column_kernel(SearchArgs a, const SubsetPrm* __restrict__ prm, int TI, float* __restrict__ cx) {
+__global__ void ring_column_kernel(SearchArgs a, const SubsetPrm* __restrict__ prm, int TI,
+                                   const float* __restrict__ tcf, float* __restrict__ cx) {
   const int lane = threadIdx.x & 31;
   const long long t = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
   const long long n = (long long)a.nx * a.ny;
   if (t >= n || !prm[t].valid) return;
   const int i = (int)(t % a.nx), j = (int)(t / a.nx);
   const SubsetGeom s = subset_geom(a, t);
-  const float cf = tile_centre(prm, a.nx, a.ny, i - i % TI, j - j % kTJ, TI);
+  const float cf = tcf[i / TI + (j / kTJ) * ((a.nx + TI - 1) / TI)];
   const int W1 = a.winsize + 1, DA0 = -a.s0 - 1, nda = a.s0 + a.s1 + 3;
   const int X = s.ii - 1, Y = s.jj - 1;
   float* out = cx + t * 2 * (long long)nda;
@@ -563,7 +567,7 @@ template <int ST, int W1, int TI>
 __global__ void __launch_bounds__(kTileThreads, 1)
     ncc_tile_kernel(SearchArgs a, const float2* __restrict__ map, const double* __restrict__ Vmap,
                     const SubsetPrm* __restrict__ prm, const float2* __restrict__ ringv,
-                    const float* __restrict__ cxv, int* __restrict__ best) {
+                    const float* __restrict__ cxv, const float* __restrict__ tcf, int* __restrict__ best) {
   using S = TileShape<ST, W1, TI>;
   constexpr int FR = S::FR, FC = S::FC, FCP = S::FCP, GCP = S::GCP, FRP = S::FRP, H0 = S::H0, NSUB = S::NSUB;
   constexpr int GC = FC + kDBC - 1;  // g columns a chunk needs
@@ -588,7 +592,7 @@ __global__ void __launch_bounds__(kTileThreads, 1)
   const size_t ld = (size_t)a.M + 1;
 
   // ---- per-subset constants and geometry ----
-  if (tid == 0) s_cf = tile_centre(prm, a.nx, a.ny, i0, j0, TI);
+  if (tid == 0) s_cf = tcf[blockIdx.x];
   if (tid >= 32 && tid < 32 + TI) {
     const int il = tid - 32, i = i0 + il;
     const AxisGeom r = axis_geom(a.gx0 + i * a.step, w, a.s0, a.s1, a.M, a.gx1);
@@ -794,19 +798,24 @@ __global__ void __launch_bounds__(kTileThreads, 1)
   }
 }
 
-// FP64 refit + findpeak at the argmax of every valid subset (one CTA per subset).
-__global__ void __launch_bounds__(128) subset_refit_kernel(SearchArgs a, const SubsetPrm* __restrict__ prm,
+// FP64 refit + findpeak at the argmax of every valid subset (one warp per subset).
+__global__ void __launch_bounds__(256) subset_refit_kernel(SearchArgs a, const SubsetPrm* __restrict__ prm,
                                                            const int* __restrict__ best) {
-  __shared__ double red[4 * 9];
-  __shared__ double sums[9];
-  const long long n = (long long)a.nx * a.ny;
-  for (long long t = blockIdx.x; t < n; t += gridDim.x) {
-    const SubsetPrm P = prm[t];
-    if (!P.valid) continue;
-    const SubsetGeom s = subset_geom(a, t);
-    const int bi = best[t];
-    refit_peak(a, s, subset_out(a, t), bi % s.na, bi / s.na, P.fm, P.denT, P.tolz, red, sums);
-  }
+  const long long t = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  if (t >= (long long)a.nx * a.ny) return;
+  const SubsetPrm P = prm[t];
+  if (!P.valid) return;
+  const SubsetGeom s = subset_geom(a, t);
+  const int bi = best[t];
+  refit_peak_warp(a, s, subset_out(a, t), bi % s.na, bi / s.na, P.fm, P.denT, P.tolz);
+}
+
+// Centring constant of every tile (tile_centre), one thread per tile.
+__global__ void tile_centre_kernel(int nx, int ny, int TI, const SubsetPrm* __restrict__ prm, float* __restrict__ cf) {
+  const int ntx = (nx + TI - 1) / TI, nty = (ny + kTJ - 1) / kTJ;
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= ntx * nty) return;
+  cf[b] = tile_centre(prm, nx, ny, (b % ntx) * TI, (b / ntx) * kTJ, TI);
 }
 
 namespace {
@@ -824,7 +833,7 @@ int launch_tile(const SearchArgs& a, const TileScratch& sc, cudaStream_t st) {
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::smem_bytes) != cudaSuccess)
     return -1;
   const long long tiles = (long long)((a.nx + TI - 1) / TI) * ((a.ny + kTJ - 1) / kTJ);
-  kern<<<(unsigned)tiles, kTileThreads, S::smem_bytes, st>>>(a, sc.map, sc.V, sc.prm, sc.ringv, sc.cx, sc.best);
+  kern<<<(unsigned)tiles, kTileThreads, S::smem_bytes, st>>>(a, sc.map, sc.V, sc.prm, sc.ringv, sc.cx, sc.cf, sc.best);
   return 0;
 }
 
@@ -868,16 +877,14 @@ int launch_search_tile(const SearchArgs& a, cudaStream_t st) {
   const long long nh = (long long)(a.M - W1 + 1) * a.ny;
   window_rowmax_kernel<<<(unsigned)((nh + 255) / 256), 256, 0, st>>>(a, sc.V, sc.H);
   subset_prep_kernel<<<(unsigned)((n * 32 + 255) / 256), 256, 0, st>>>(a, sc.H, sc.prm, sc.ringv);
-  ring_column_kernel<<<(unsigned)((n * 32 + 255) / 256), 256, 0, st>>>(a, sc.prm, e.TI, sc.cx);
+  const int ntiles = ((a.nx + e.TI - 1) / e.TI) * ((a.ny + kTJ - 1) / kTJ);
+  tile_centre_kernel<<<(ntiles + 127) / 128, 128, 0, st>>>(a.nx, a.ny, e.TI, sc.prm, sc.cf);
+  ring_column_kernel<<<(unsigned)((n * 32 + 255) / 256), 256, 0, st>>>(a, sc.prm, e.TI, sc.cf, sc.cx);
   if (a.ev_start) cudaEventRecord(a.ev_start, st);
   if (e.launch(a, sc, st) != 0) return -1;
   if (a.ev_stop) cudaEventRecord(a.ev_stop, st);
-  int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const long long grid = n < (long long)sms * 8 ? n : (long long)sms * 8;
-  subset_refit_kernel<<<(unsigned)grid, 128, 0, st>>>(a, sc.prm, sc.best);
-  return 6;
+  subset_refit_kernel<<<(unsigned)((n * 32 + 255) / 256), 256, 0, st>>>(a, sc.prm, sc.best);
+  return 7;
 }
 
 }  // namespace aldic
