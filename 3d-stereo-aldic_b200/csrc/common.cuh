@@ -101,6 +101,43 @@ __device__ __forceinline__ float2 fadd2(float2 a, float2 b) {
   return d;
 }
 
+// Two stencils at once with packed FP32 pairs (.x: point a, .y: point b); each lane's
+// result is bit-identical to stencil16 at that point.
+__device__ __forceinline__ void bspline_weights_x2(float2 t, float2 w[4]) {
+  const float2 k = make_float2(1.0f / 56.0f, 1.0f / 56.0f);
+  w[0] = fmul2(k, fmul2(t, ffma2(t, ffma2(t, make_float2(-24.0f, -24.0f), make_float2(57.0f, 57.0f)),
+                                 make_float2(-33.0f, -33.0f))));
+  w[1] = fmul2(k, ffma2(t, ffma2(t, ffma2(t, make_float2(64.0f, 64.0f), make_float2(-117.0f, -117.0f)),
+                                 make_float2(-3.0f, -3.0f)),
+                        make_float2(56.0f, 56.0f)));
+  w[2] = fmul2(k, fmul2(t, ffma2(t, ffma2(t, make_float2(-64.0f, -64.0f), make_float2(75.0f, 75.0f)),
+                                 make_float2(45.0f, 45.0f))));
+  w[3] = fmul2(k, fmul2(t, ffma2(t, ffma2(t, make_float2(24.0f, 24.0f), make_float2(-15.0f, -15.0f)),
+                                 make_float2(-9.0f, -9.0f))));
+}
+
+__device__ __forceinline__ float2 stencil16_x2(const float* __restrict__ img, int M, int ia, int ib, float2 tr,
+                                               float2 tc) {
+  // ia, ib: element index of tap 0 (r0 + c0 M) of the two points
+  float2 wr[4], wc[4];
+  bspline_weights_x2(tr, wr);
+  bspline_weights_x2(tc, wc);
+  const float* pa = img + ia;
+  const float* pb = img + ib;
+  float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    const float* qa = pa + c * M;
+    const float* qb = pb + c * M;
+    float2 col = fmul2(wr[0], make_float2(__ldg(qa), __ldg(qb)));
+    col = ffma2(wr[1], make_float2(__ldg(qa + 1), __ldg(qb + 1)), col);
+    col = ffma2(wr[2], make_float2(__ldg(qa + 2), __ldg(qb + 2)), col);
+    col = ffma2(wr[3], make_float2(__ldg(qa + 3), __ldg(qb + 3)), col);
+    acc = ffma2(wc[c], col, acc);
+  }
+  return acc;
+}
+
 // ---------------------------------------------------------------------------------
 // Reductions
 // ---------------------------------------------------------------------------------

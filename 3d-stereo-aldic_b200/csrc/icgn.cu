@@ -26,6 +26,7 @@
 namespace aldic {
 
 constexpr int kNT = 128;  // threads per solve CTA
+constexpr int kSlowSubset = 2;  // queue-1 flag of a subset restarted by the 4-warp pass
 
 struct SolveCtl {
   double P[6];
@@ -271,6 +272,7 @@ __global__ void __launch_bounds__(kNT) icgn_solve_kernel(IcgnArgs a, int bucket)
     const int* q = a.queue + 3 * ((long long)bucket * a.n + qi);
     const long long t = q[0];
     const int w = q[1];
+    if (q[2] == kSlowSubset) continue;  // restarted by the 4-warp pass
     const bool masked = q[2] != 0;
     const int W1 = w + 1, npx = W1 * W1;
     const int half = w / 2;
@@ -582,40 +584,96 @@ __global__ void __launch_bounds__(kNT) icgn_solve_kernel(IcgnArgs a, int bucket)
 // fast 6-DOF solve for subsets at the nominal window without a mask region
 // ================================================================================
 // The common case (uniform variant; quadtree subsets whose window holds no masked or zero
-// pixel): no flood fills, so shared memory holds only (f_x, f_y) per pixel (f as well for
-// the epipolar score) and a 64-thread CTA per subset keeps many subsets in flight per SM.
-// The 6x6 inverse is a cooperative Gauss-Jordan elimination (H is the symmetric positive
-// semi-definite Gauss-Newton Hessian), the b-vector and update are spread over six
-// threads.  A quadtree subset that meets an exact zero in g (a masked deformed image) needs
-// the g-region flood fill: it is handed to the general kernel's queue and restarted there.
-constexpr int kFT = 64;
+// pixel) needs no flood fill, so a group of NW warps solves one subset with no shared image
+// buffer.  Every thread walks its share of the window pixels; the sums are warp shuffles
+// (FP32 per thread, FP64 across lanes) plus, for NW > 1, one fixed-order FP64 sum of the
+// NW warp totals behind a named barrier of the group, so every thread holds the same
+// totals and runs the same FP64 Gauss-Newton control redundantly: there is no other
+// barrier per iteration.  The gradients f_x, f_y are re-read from the L1-resident gradient
+// images each iteration.  The 6x6 inverse is a per-group [H | I] Gauss-Jordan elimination
+// without pivoting by the group's first warp (H is the symmetric positive semi-definite
+// Gauss-Newton Hessian; a zero pivot propagates Inf/NaN as the reference's singular solve
+// does).
+//
+// The main pass (NW = 1, queue 0) gives each subset at most kWarpIterCap iterations: the
+// few subsets that need more (most never converge and run to max_iter) would otherwise
+// keep single warps running long after the rest of the grid.  They go to queue 1 flagged
+// kSlowSubset and restart from the beginning in the 4-warp pass (NW = 4), which runs each
+// iteration about four times faster.  A quadtree subset that meets an exact zero in g (a
+// masked deformed image) needs the g-region flood fill: it is handed to the general kernel
+// through queue 1 and restarted there.
+constexpr int kWT = 256;  // threads per CTA: 8 / NW subset groups
+constexpr int kWarpIterCap = 16;
 
-struct FastCtl {
-  double P[6];
-  double aug[72];  // 6 x 12 row-major [H | I] -> [I | H^-1]
-  double H21[21];  // packed upper triangle by rows == lower triangle by columns
-  double fac[6], piv;
-  double A[6], B[6], b[6], dP[6];
-  double meanf, bf, sabsf;
-  double normNew, normAbs, normInit, znssd;
-  float pf[4], f5, f6;
-  int base_r, base_c;
-  int step, go, status, requeue;
-};
+template <int NW>
+__device__ __forceinline__ void group_bar(int id) {
+  if (NW == 1)
+    __syncwarp();
+  else
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(32 * NW) : "memory");
+}
 
-__global__ void __launch_bounds__(kFT, 12) icgn_fast_kernel(IcgnArgs a) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ FastCtl c;
-  __shared__ double red[(kFT / 32) * 40];
-  __shared__ double sums[40];
-  const int tid = threadIdx.x;
+// Sum of v over the group, left in every thread of the group (FP64; the NW warp totals
+// are added in warp order).  red holds NW * K doubles of the group.
+template <int NW, int K>
+__device__ __forceinline__ void group_sum(double (&v)[K], double* red, int gw, int lane, int bar) {
+#pragma unroll
+  for (int k = 0; k < K; ++k) v[k] = warp_sum(v[k]);
+  if (NW == 1) return;
+  if (lane < K) {
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+      if (lane == k) red[gw * K + k] = v[k];
+  }
+  group_bar<NW>(bar);
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    double s = red[k];
+#pragma unroll
+    for (int u = 1; u < NW; ++u) s += red[u * K + k];
+    v[k] = s;
+  }
+  group_bar<NW>(bar);
+}
+
+template <int NW, bool SLOW>
+__global__ void __launch_bounds__(kWT, 2) icgn_group_kernel(IcgnArgs a) {
+  constexpr int NG = kWT / (32 * NW);  // subset groups per CTA
+  constexpr int GT = 32 * NW;          // threads per group
+  __shared__ double s_aug[NG][72];     // 6 x 12 row-major [H | I] -> [I | H^-1]
+  __shared__ double s_ab[NG][12];      // A (0..5), B (6..11)
+  __shared__ double s_h[NG][21];       // packed upper triangle by rows
+  __shared__ double s_fac[NG][6];      // elimination factors of the current pivot column
+  __shared__ double s_red[NG][NW * 21];
+  const int lane = threadIdx.x & 31, grp = threadIdx.x / GT, gw = (threadIdx.x % GT) >> 5;
+  const int gt = threadIdx.x % GT, bar = 1 + grp;
+  double* aug = s_aug[grp];
+  double* AB = s_ab[grp];
+  double* red = s_red[grp];
   const FrameDev& fr = a.fr;
   const bool quad = (a.variant == 1);
   const bool epi = (a.variant == 2);
-  const int count = a.qcount[0];
+  __shared__ int s_qi[NG];
+  const int count = a.qcount[SLOW ? 1 : 0];
   const int gM = fr.M - 6;
-  for (int qi = blockIdx.x; qi < count; qi += gridDim.x) {
-    const int* q = a.queue + 3 * (long long)qi;
+  int* next = a.qcount + (SLOW ? 3 : 2);  // work counter of this pass (zeroed with the queues)
+  while (true) {
+    // the group's next queue entry (dynamic: slow subsets do not pile up on one group)
+    int qi = 0;
+    if (gt == 0) qi = atomicAdd(next, 1);
+    if (NW == 1) {
+      qi = __shfl_sync(0xffffffffu, qi, 0);
+    } else {
+      if (gt == 0) s_qi[grp] = qi;
+      group_bar<NW>(bar);
+      qi = s_qi[grp];
+    }
+    if (qi >= count) break;
+    const int* q = a.queue + 3 * ((SLOW ? a.n : 0) + qi);
+    if (SLOW && q[2] != kSlowSubset) {
+      group_bar<NW>(bar);
+      continue;
+    }
     const long long t = q[0];
     const int w = q[1];
     const int W1 = w + 1, npx = W1 * W1, half = w / 2;
@@ -624,9 +682,10 @@ __global__ void __launch_bounds__(kFT, 12) icgn_fast_kernel(IcgnArgs a) {
       x0 = mround(x0);
       y0 = mround(y0);
     }
-    float2* gxy = reinterpret_cast<float2*>(smem_raw);
-    float* fsm = reinterpret_cast<float*>(gxy + npx);  // epipolar only
-    // ---- load the window and the set-up sums in one pass ----
+    const int r0 = (int)x0 - half - 1, c0 = (int)y0 - half - 1;
+    const int q_nt = GT / W1, r_nt = GT % W1;
+    // ---- set-up sums in one pass over the window ----
+    double meanf, bf, sabsf;
     {
       float h[21], jf[6], jb[6], fs = 0.f, fs2 = 0.f, fn = 0.f, fab = 0.f;
 #pragma unroll
@@ -636,15 +695,12 @@ __global__ void __launch_bounds__(kFT, 12) icgn_fast_kernel(IcgnArgs a) {
         jf[k] = 0.f;
         jb[k] = 0.f;
       }
-      const int r0 = (int)x0 - half - 1, c0 = (int)y0 - half - 1;
-      for (int p = tid; p < npx; p += kFT) {
-        const int aa = p % W1, bb = p / W1;
-        const size_t k = (size_t)(r0 + aa) + (size_t)(c0 + bb) * fr.M;
-        const size_t kg = (size_t)(r0 + aa - a.crop) + (size_t)(c0 + bb - a.crop) * gM;
+      int aa = gt % W1, bb = gt / W1;
+      for (int p = gt; p < npx; p += GT) {
+        const int k = (r0 + aa) + (c0 + bb) * fr.M;
+        const int kg = (r0 + aa - a.crop) + (c0 + bb - a.crop) * gM;
         const float f = fr.ref[k];  // a quadtree subset here has no masked pixel
         const float gxv = fr.gx[kg], gyv = fr.gy[kg];
-        gxy[p] = make_float2(gxv, gyv);
-        if (epi) fsm[p] = f;
         const float dx = (float)(aa - half), dy = (float)(bb - half);
         const float J[6] = {gxv * dx, gyv * dx, gxv * dy, gyv * dy, gxv, gyv};
         int m = 0;
@@ -663,113 +719,168 @@ __global__ void __launch_bounds__(kFT, 12) icgn_fast_kernel(IcgnArgs a) {
           fn += 1.f;
         }
         fab += fabsf(f);
-      }
-      float v[37];
-#pragma unroll
-      for (int k = 0; k < 21; ++k) v[k] = h[k];
-#pragma unroll
-      for (int k = 0; k < 6; ++k) {
-        v[21 + k] = jf[k];
-        v[27 + k] = jb[k];
-      }
-      v[33] = fs;
-      v[34] = fs2;
-      v[35] = fn;
-      v[36] = fab;
-      block_sum_f32<37, kFT>(v, red, sums);
-    }
-    // ---- [H | I] and the f statistics ----
-    for (int e = tid; e < 72; e += kFT) {
-      const int i = e / 12, j = e % 12;
-      double val;
-      if (j < 6) {
-        const int r = i < j ? i : j, cc = i < j ? j : i;  // packed upper-triangle index of (r, cc)
-        val = sums[r * 6 - r * (r - 1) / 2 + (cc - r)];
-      } else {
-        val = (j - 6 == i) ? 1.0 : 0.0;
-      }
-      c.aug[e] = val;
-    }
-    if (tid == 0) {
-      const double n = sums[35];
-      if (n > 0) {
-        c.meanf = sums[33] / n;
-        c.bf = sqrt(fmax(sums[34] - sums[33] * sums[33] / n, 0.0));
-      } else {
-        c.meanf = ALDIC_NAN;
-        c.bf = ALDIC_NAN;
-      }
-      c.sabsf = sums[36];
-      for (int k = 0; k < 21; ++k) c.H21[k] = sums[k];
-      c.P[0] = c.P[1] = c.P[2] = c.P[3] = 0.0;
-      c.P[4] = epi ? 0.0 : a.U0[2 * t];
-      c.P[5] = epi ? 0.0 : a.U0[2 * t + 1];
-      c.normNew = 1.0;
-      c.normAbs = 1.0;
-      c.normInit = 0.0;
-      c.step = 0;
-      c.status = 0;
-      c.requeue = 0;
-      c.znssd = ALDIC_NAN;
-    }
-    __syncthreads();
-    if (tid < 6) {
-      c.B[tid] = sums[27 + tid];
-      c.A[tid] = (sums[21 + tid] - c.meanf * c.B[tid]) / c.bf;
-    }
-    // Gauss-Jordan elimination without pivoting (positive definite H); a zero pivot
-    // propagates Inf/NaN as the reference's singular solve does
-    for (int k = 0; k < 6; ++k) {
-      if (tid < 6) c.fac[tid] = c.aug[tid * 12 + k];
-      if (tid == 0) c.piv = c.aug[k * 12 + k];
-      __syncthreads();
-      if (tid < 12) c.aug[k * 12 + tid] /= c.piv;
-      __syncthreads();
-      for (int e = tid; e < 72; e += kFT) {
-        const int i = e / 12, j = e % 12;
-        if (i != k) c.aug[e] -= c.fac[i] * c.aug[k * 12 + j];
-      }
-      __syncthreads();
-    }
-    // ---- Gauss-Newton iterations ----
-    const int q_nt = kFT / W1, r_nt = kFT % W1;
-    while (true) {
-      if (tid == 0) {
-        int go = (c.step <= a.max_iter && c.normNew > a.tol && c.normAbs > a.tol && !c.requeue) ? 1 : 0;
-        if (go) {
-          c.step += 1;
-          if (warped_oob(fr, c.P, x0, y0, half, half)) {
-            c.normNew = 1e6;
-            go = 0;
-          } else {
-            const double n5 = mround(c.P[4]), n6 = mround(c.P[5]);
-            c.pf[0] = (float)c.P[0];
-            c.pf[1] = (float)c.P[1];
-            c.pf[2] = (float)c.P[2];
-            c.pf[3] = (float)c.P[3];
-            c.f5 = (float)(c.P[4] - n5);
-            c.f6 = (float)(c.P[5] - n6);
-            c.base_r = (int)(x0 + n5) - 2;
-            c.base_c = (int)(y0 + n6) - 2;
-          }
+        aa += r_nt;
+        bb += q_nt;
+        if (aa >= W1) {
+          aa -= W1;
+          bb += 1;
         }
-        c.go = go;
       }
-      __syncthreads();
-      if (!c.go) break;
+      {
+        double v[4] = {fs, fs2, fn, fab};
+        group_sum<NW, 4>(v, red, gw, lane, bar);
+        sabsf = v[3];
+        if (v[2] > 0) {
+          meanf = v[0] / v[2];
+          bf = sqrt(fmax(v[1] - v[0] * v[0] / v[2], 0.0));
+        } else {
+          meanf = ALDIC_NAN;
+          bf = ALDIC_NAN;
+        }
+      }
+      {
+        double v[12];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+          v[k] = jb[k];
+          v[6 + k] = jf[k];
+        }
+        group_sum<NW, 12>(v, red, gw, lane, bar);
+        if (gt < 6) {
+#pragma unroll
+          for (int k = 0; k < 6; ++k)
+            if (gt == k) {
+              AB[6 + k] = v[k];
+              AB[k] = (v[6 + k] - meanf * v[k]) / bf;
+            }
+        }
+      }
+      {
+        double v[21];
+#pragma unroll
+        for (int k = 0; k < 21; ++k) v[k] = h[k];
+        group_sum<NW, 21>(v, red, gw, lane, bar);
+        if (gt < 21) {
+#pragma unroll
+          for (int k = 0; k < 21; ++k)
+            if (gt == k) s_h[grp][k] = v[k];
+        }
+      }
+    }
+    group_bar<NW>(bar);
+    if (gw == 0) {
+      for (int e = lane; e < 72; e += 32) {
+        const int i = e / 12, j = e % 12;
+        double val;
+        if (j < 6) {
+          const int r = i < j ? i : j, cc = i < j ? j : i;  // packed upper-triangle index of (r, cc)
+          val = s_h[grp][r * 6 - r * (r - 1) / 2 + (cc - r)];
+        } else {
+          val = (j - 6 == i) ? 1.0 : 0.0;
+        }
+        aug[e] = val;
+      }
+      __syncwarp();
+      for (int k = 0; k < 6; ++k) {
+        if (lane < 6) s_fac[grp][lane] = aug[lane * 12 + k];
+        const double piv = aug[k * 12 + k];
+        __syncwarp();
+        if (lane < 12) aug[k * 12 + lane] /= piv;
+        __syncwarp();
+        for (int e = lane; e < 72; e += 32) {
+          const int i = e / 12, j = e % 12;
+          if (i != k) aug[e] -= s_fac[grp][i] * aug[k * 12 + j];
+        }
+        __syncwarp();
+      }
+    }
+    group_bar<NW>(bar);
+    // ---- Gauss-Newton iterations (control replicated in every thread) ----
+    double P[6] = {0.0, 0.0, 0.0, 0.0, epi ? 0.0 : a.U0[2 * t], epi ? 0.0 : a.U0[2 * t + 1]};
+    double normNew = 1.0, normAbs = 1.0, normInit = 0.0, znssd = ALDIC_NAN;
+    int step = 0, status = 0, requeue = -1;
+    while (step <= a.max_iter && normNew > a.tol && normAbs > a.tol) {
+      if (!SLOW && step >= kWarpIterCap) {  // a slow subset: restarted by the 4-warp pass
+        requeue = kSlowSubset;
+        break;
+      }
+      step += 1;
+      if (warped_oob(fr, P, x0, y0, half, half)) {
+        normNew = 1e6;
+        break;
+      }
+      const double n5 = mround(P[4]), n6 = mround(P[5]);
+      const float p0 = (float)P[0], p1 = (float)P[1], p2 = (float)P[2], p3 = (float)P[3];
+      const float f5 = (float)(P[4] - n5), f6 = (float)(P[5] - n6);
+      const int br = (int)(x0 + n5) - 2, bc = (int)(y0 + n6) - 2;
       float C[6] = {0, 0, 0, 0, 0, 0}, S1 = 0.f, S2 = 0.f, ns = 0.f, nz = 0.f, fg = 0.f;
       {
-        const float p0 = c.pf[0], p1 = c.pf[1], p2 = c.pf[2], p3 = c.pf[3], f5 = c.f5, f6 = c.f6;
-        const int br = c.base_r, bc = c.base_c;
-        int aa = tid % W1, bb = tid / W1;
-        for (int p = tid; p < npx; p += kFT) {
+        // pixels in pairs (p, p + GT) with packed FP32 pairs; a last unpaired pixel alone
+        float2 C2[6], S12 = make_float2(0.f, 0.f), S22 = make_float2(0.f, 0.f), fg2 = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) C2[k] = make_float2(0.f, 0.f);
+        const float2 pp0 = make_float2(p0, p0), pp1 = make_float2(p1, p1), pp2 = make_float2(p2, p2);
+        const float2 pp3 = make_float2(p3, p3), ff5 = make_float2(f5, f5), ff6 = make_float2(f6, f6);
+        int aa = gt % W1, bb = gt / W1;
+        int p = gt;
+        for (; p + GT < npx; p += 2 * GT) {
+          int ab = aa + r_nt, bbb = bb + q_nt;
+          if (ab >= W1) {
+            ab -= W1;
+            bbb += 1;
+          }
+          const float2 dx = make_float2((float)(aa - half), (float)(ab - half));
+          const float2 dy = make_float2((float)(bb - half), (float)(bbb - half));
+          const float2 lx = fadd2(dx, ffma2(pp0, dx, ffma2(pp2, dy, ff5)));
+          const float2 ly = fadd2(dy, ffma2(pp3, dy, ffma2(pp1, dx, ff6)));
+          const float ixa = floorf(lx.x), ixb = floorf(lx.y), iya = floorf(ly.x), iyb = floorf(ly.y);
+          const float2 tr = make_float2(lx.x - ixa, lx.y - ixb), tc = make_float2(ly.x - iya, ly.y - iyb);
+          const int ia = (br + (int)ixa) + (bc + (int)iya) * fr.M, ib = (br + (int)ixb) + (bc + (int)iyb) * fr.M;
+          const float2 g = stencil16_x2(fr.def, fr.M, ia, ib, tr, tc);
+          const int ka = (r0 + aa - a.crop) + (c0 + bb - a.crop) * gM;
+          const int kb = (r0 + ab - a.crop) + (c0 + bbb - a.crop) * gM;
+          const float2 ag = fmul2(make_float2(fr.gx[ka], fr.gx[kb]), g);
+          const float2 bg = fmul2(make_float2(fr.gy[ka], fr.gy[kb]), g);
+          C2[0] = ffma2(ag, dx, C2[0]);
+          C2[1] = ffma2(bg, dx, C2[1]);
+          C2[2] = ffma2(ag, dy, C2[2]);
+          C2[3] = ffma2(bg, dy, C2[3]);
+          C2[4] = fadd2(C2[4], ag);
+          C2[5] = fadd2(C2[5], bg);
+          if (!quad) {
+            S12 = fadd2(S12, g);
+            S22 = ffma2(g, g, S22);
+          } else {
+            if (fabsf(g.x) > 1e-10f) {
+              S1 += g.x;
+              S2 = fmaf(g.x, g.x, S2);
+              ns += 1.f;
+            }
+            if (fabsf(g.y) > 1e-10f) {
+              S1 += g.y;
+              S2 = fmaf(g.y, g.y, S2);
+              ns += 1.f;
+            }
+            nz += (g.x == 0.f ? 1.f : 0.f) + (g.y == 0.f ? 1.f : 0.f);
+          }
+          if (epi)
+            fg2 = ffma2(make_float2(fr.ref[(r0 + aa) + (c0 + bb) * fr.M], fr.ref[(r0 + ab) + (c0 + bbb) * fr.M]), g,
+                        fg2);
+          aa = ab + r_nt;
+          bb = bbb + q_nt;
+          if (aa >= W1) {
+            aa -= W1;
+            bb += 1;
+          }
+        }
+        if (p < npx) {  // the last, unpaired pixel
           const float dx = (float)(aa - half), dy = (float)(bb - half);
           const float lx = dx + fmaf(p0, dx, fmaf(p2, dy, f5));
           const float ly = dy + fmaf(p3, dy, fmaf(p1, dx, f6));
           const float ix = floorf(lx), iy = floorf(ly);
           const float g = stencil16(fr.def, fr.M, br + (int)ix, bc + (int)iy, lx - ix, ly - iy);
-          const float2 gg = gxy[p];
-          const float ag = gg.x * g, bg = gg.y * g;
+          const int kg = (r0 + aa - a.crop) + (c0 + bb - a.crop) * gM;
+          const float ag = fr.gx[kg] * g, bg = fr.gy[kg] * g;
           C[0] = fmaf(ag, dx, C[0]);
           C[1] = fmaf(bg, dx, C[1]);
           C[2] = fmaf(ag, dy, C[2]);
@@ -782,91 +893,88 @@ __global__ void __launch_bounds__(kFT, 12) icgn_fast_kernel(IcgnArgs a) {
             ns += 1.f;
           }
           if (quad && g == 0.f) nz += 1.f;
-          if (epi) fg = fmaf(fsm[p], g, fg);
-          aa += r_nt;
-          bb += q_nt;
-          if (aa >= W1) {
-            aa -= W1;
-            bb += 1;
-          }
+          if (epi) fg = fmaf(fr.ref[(r0 + aa) + (c0 + bb) * fr.M], g, fg);
         }
+#pragma unroll
+        for (int k = 0; k < 6; ++k) C[k] += C2[k].x + C2[k].y;
+        if (!quad) {
+          S1 += S12.x + S12.y;
+          S2 += S22.x + S22.y;
+          ns = (float)((npx - gt + GT - 1) / GT);  // pixels of this thread
+        }
+        if (epi) fg += fg2.x + fg2.y;
       }
       double v[11] = {C[0], C[1], C[2], C[3], C[4], C[5], S1, S2, ns, nz, fg};
-      block_sum<11, kFT>(v, red, sums);
-      if (sums[9] > 0) {  // exact zero in g: the g-region flood fill is needed
-        if (tid == 0) c.requeue = 1;
-        __syncthreads();
+      group_sum<NW, 11>(v, red, gw, lane, bar);
+      if (v[9] > 0) {  // exact zero in g: the g-region flood fill is needed
+        requeue = 0;
         break;
       }
-      if (tid < 6) {
-        const double n = sums[8];
-        double meang, bg;
-        if (n > 0) {
-          meang = sums[6] / n;
-          bg = sqrt(fmax(sums[7] - sums[6] * sums[6] / n, 0.0));
-        } else {
-          meang = ALDIC_NAN;
-          bg = ALDIC_NAN;
-        }
-        c.b[tid] = c.bf * (c.A[tid] - (sums[tid] - meang * c.B[tid]) / bg);
-        if (epi && tid == 0) c.znssd = 2.0 - 2.0 * (sums[10] - c.meanf * sums[6]) / (c.bf * bg);
+      double meang, bgn;
+      if (v[8] > 0) {
+        meang = v[6] / v[8];
+        bgn = sqrt(fmax(v[7] - v[6] * v[6] / v[8], 0.0));
+      } else {
+        meang = ALDIC_NAN;
+        bgn = ALDIC_NAN;
       }
-      __syncthreads();
-      if (tid < 6) {
+      if (epi) znssd = 2.0 - 2.0 * (v[10] - meanf * v[6]) / (bf * bgn);
+      double b[6];
+#pragma unroll
+      for (int k = 0; k < 6; ++k) b[k] = bf * (AB[k] - (v[k] - meang * AB[6 + k]) / bgn);
+      double dP[6];
+#pragma unroll
+      for (int i = 0; i < 6; ++i) {
         double acc = 0;
 #pragma unroll
-        for (int j = 0; j < 6; ++j) acc += c.aug[tid * 12 + 6 + j] * c.b[j];
-        c.dP[tid] = -acc;
+        for (int j = 0; j < 6; ++j) acc += aug[i * 12 + 6 + j] * b[j];
+        dP[i] = -acc;
       }
-      __syncthreads();
-      if (tid == 0) {
-        double nn = 0;
-        for (int i = 0; i < 6; ++i) nn += c.b[i] * c.b[i];
-        c.normNew = sqrt(nn);
-        c.normAbs = c.normNew;
-        if (c.step == 1) c.normInit = c.normNew;
-        if (c.normInit > a.tol) c.normNew = c.normNew / c.normInit;
-        else c.normNew = 0.0;
-        if (!(c.normNew < a.tol || c.normAbs < a.tol)) {
-          if (!compose_inverse(c.P, c.dP)) {
-            c.step = a.max_iter + 1000;
-            c.status = 1;
-          } else if (epi) {
-            c.P[4] = 0.0;
-            c.P[5] = 0.0;
-          }
+      double nn = 0;
+#pragma unroll
+      for (int i = 0; i < 6; ++i) nn += b[i] * b[i];
+      normNew = sqrt(nn);
+      normAbs = normNew;
+      if (step == 1) normInit = normNew;
+      if (normInit > a.tol) normNew = normNew / normInit;
+      else normNew = 0.0;
+      if (!(normNew < a.tol || normAbs < a.tol)) {
+        if (!compose_inverse(P, dP)) {
+          step = a.max_iter + 1000;
+          status = 1;
+        } else if (epi) {
+          P[4] = 0.0;
+          P[5] = 0.0;
         }
       }
-      __syncthreads();
     }
-    if (tid == 0) {
-      if (c.requeue) {
-        // restart this subset in the general kernel (its queue runs after this kernel)
+    if (gt == 0) {
+      if (requeue >= 0) {
+        // restart this subset in a later pass (they run after this kernel)
         const int pos = atomicAdd(&a.qcount[1], 1);
         int* q1 = a.queue + 3 * ((long long)a.n + pos);
         q1[0] = (int)t;
         q1[1] = w;
-        q1[2] = 0;
+        q1[2] = requeue;
       } else {
-        int step = c.step;
-        if (c.status == 1) step -= 1000;
-        if (!(c.normNew < a.tol || c.normAbs < a.tol)) step = a.max_iter + 1;
-        if (isnan(c.normNew)) step = a.max_iter + 1;
-        if (quad && c.sabsf < 1e-6) step = a.max_iter + 3;
+        if (status == 1) step -= 1000;
+        if (!(normNew < a.tol || normAbs < a.tol)) step = a.max_iter + 1;
+        if (isnan(normNew)) step = a.max_iter + 1;
+        if (quad && sabsf < 1e-6) step = a.max_iter + 3;
         if (epi) {
-          a.znssd[t] = c.znssd;
+          a.znssd[t] = znssd;
           if (a.conv) a.conv[t] = step;
         } else {
           a.conv[t] = step;
-          a.U[2 * t] = c.P[4];
-          a.U[2 * t + 1] = c.P[5];
-          for (int k = 0; k < 4; ++k) a.F[4 * t + k] = c.P[k];
+          a.U[2 * t] = P[4];
+          a.U[2 * t + 1] = P[5];
+          for (int k = 0; k < 4; ++k) a.F[4 * t + k] = P[k];
           if (a.H)
-            for (int k = 0; k < 21; ++k) a.H[t + a.n * k] = c.H21[k];
+            for (int k = 0; k < 21; ++k) a.H[t + a.n * k] = s_h[grp][k];
         }
       }
     }
-    __syncthreads();
+    group_bar<NW>(bar);
   }
 }
 
@@ -1277,11 +1385,10 @@ static int occupancy_grid(const void* fn, size_t smem) {
 size_t icgn_smem_bytes(int w) { return (size_t)(w + 1) * (w + 1) * (4 * sizeof(float) + 4); }
 size_t sub1_smem_bytes(int wx, int wy) { return (size_t)(wx + 1) * (wy + 1) * (4 * sizeof(float) + 5); }
 
-size_t icgn_fast_smem_bytes(int w, bool epi) { return (size_t)(w + 1) * (w + 1) * (epi ? 12 : 8); }
 
 int launch_icgn(const IcgnArgs& a, int wmax_enlarged, cudaStream_t st) {
   int launches = 0;
-  cudaMemsetAsync(a.qcount, 0, 2 * sizeof(int), st);
+  cudaMemsetAsync(a.qcount, 0, 4 * sizeof(int), st);  // 2 queue counts, 2 work counters
   const long long threads = a.n * 32;
   const int cb = 256;
   icgn_classify_kernel<<<(unsigned)((threads + cb - 1) / cb), cb, 0, st>>>(a);
@@ -1289,15 +1396,20 @@ int launch_icgn(const IcgnArgs& a, int wmax_enlarged, cudaStream_t st) {
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  {  // nominal-window subsets without a mask region
-    const size_t smem = icgn_fast_smem_bytes(a.winsize, a.variant == 2);
-    cudaFuncSetAttribute(icgn_fast_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  {  // nominal-window subsets without a mask region: one warp per subset, then the slow ones
     int per_sm = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, icgn_fast_kernel, kFT, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, icgn_group_kernel<1, false>, kWT, 0);
     long long grid = (long long)sms * (per_sm < 1 ? 1 : per_sm);
-    if (grid > a.n) grid = a.n;
-    icgn_fast_kernel<<<(unsigned)grid, kFT, smem, st>>>(a);
-    ++launches;
+    const long long need = (a.n + 7) / 8;
+    if (grid > need) grid = need;
+    icgn_group_kernel<1, false><<<(unsigned)grid, kWT, 0, st>>>(a);
+    per_sm = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, icgn_group_kernel<4, true>, kWT, 0);
+    grid = (long long)sms * (per_sm < 1 ? 1 : per_sm);
+    const long long need4 = (a.n + 1) / 2;
+    if (grid > need4) grid = need4;
+    icgn_group_kernel<4, true><<<(unsigned)grid, kWT, 0, st>>>(a);
+    launches += 2;
   }
   {  // enlarged / masked subsets, and those handed over by the fast kernel
     const size_t smem = icgn_smem_bytes(wmax_enlarged);

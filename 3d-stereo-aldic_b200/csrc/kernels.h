@@ -34,7 +34,7 @@ struct IcgnArgs {
   uint8_t* mark; // n or null
   double* znssd; // n (epipolar)
   int* queue;    // 2 buckets x n x 3 ints
-  int* qcount;   // 2
+  int* qcount;   // 4: queue counts of the 2 buckets, work counters of the 2 warp-group passes
 };
 
 struct Sub1Args {
