@@ -403,29 +403,43 @@ __device__ __forceinline__ void row_band_sums_x2(const float* __restrict__ frow,
   float2 B[NB][4], S2[NB][4];              // block sums and sums of consecutive block pairs, t pairs
   float2 PE[4], AE[4], PO[3], AO[3];
   float PO0 = 0.f, PO7 = 0.f, AO0 = 0.f, AO7 = 0.f;
+  float2 ffn;
+  // loads run one 4-column group ahead of their first use
 #pragma unroll
-  for (int u = 0; u < 2; ++u) {
+  for (int u = 0; u < 3 && u < NGG; ++u) {
     const float4 q = *reinterpret_cast<const float4*>(grow + 4 * u);
     gp[2 * u] = make_float2(q.x, q.y);
     gp[2 * u + 1] = make_float2(q.z, q.w);
   }
 #pragma unroll
+  for (int u = 0; u < 2 && u < NFG; ++u) {
+    const float4 q = *reinterpret_cast<const float4*>(frow + 4 * u);
+    f[4 * u] = q.x;
+    f[4 * u + 1] = q.y;
+    f[4 * u + 2] = q.z;
+    f[4 * u + 3] = q.w;
+  }
+  ffn = make_float2(f[0], f[0]);
+#pragma unroll
   for (int c = 0; c < FC; ++c) {
     const int kc = c / ST, cc = c % ST;
-    if (c % 4 == 0) {
-      const float4 q = *reinterpret_cast<const float4*>(frow + c);
-      f[c] = q.x;
-      f[c + 1] = q.y;
-      f[c + 2] = q.z;
-      f[c + 3] = q.w;
+    if (c % 4 == 0 && c / 4 + 2 < NFG) {  // f group needed at column c + 8
+      const int u = c / 4 + 2;
+      const float4 q = *reinterpret_cast<const float4*>(frow + 4 * u);
+      f[4 * u] = q.x;
+      f[4 * u + 1] = q.y;
+      f[4 * u + 2] = q.z;
+      f[4 * u + 3] = q.w;
     }
-    if ((c + 7) % 4 == 0 && (c + 7) / 4 >= 2) {
-      const int u = (c + 7) / 4;
+    if ((c + 11) % 4 == 0 && (c + 11) / 4 >= 3 && (c + 11) / 4 < NGG) {  // g group first needed at column c + 4
+      const int u = (c + 11) / 4;
       const float4 q = *reinterpret_cast<const float4*>(grow + 4 * u);
       gp[2 * u] = make_float2(q.x, q.y);
       gp[2 * u + 1] = make_float2(q.z, q.w);
     }
-    const float2 ff = make_float2(f[c], f[c]);
+    // (f, f) pair of this column, built one column ahead
+    const float2 ff = ffn;
+    if (c + 1 < FC) ffn = make_float2(f[c + 1], f[c + 1]);
     if (cc % 2 == 0) {
       const int m = c / 2;  // gp[m + i] = (g(c + 2i), g(c + 2i + 1))
 #pragma unroll
