@@ -167,8 +167,31 @@ __device__ __forceinline__ void peak_partials(const SearchArgs& a, const SubsetG
   for (int k = 0; k < 9; ++k) v[k] = 0.0;
   int i = first % W1, j = first / W1;
   const int di = stride % W1, dj = stride / W1;
+  const float* fb = a.f + (s.ii - 1) + (size_t)(s.jj - 1) * a.M;
+  const float* gb = a.g + (s.dr0 - 2 + pa) + (size_t)(s.dc0 - 2 + pb) * a.M;
+  if (pa >= 2 && pa <= s.na - 3 && pb >= 2 && pb <= s.nb - 3) {
+    // the 3 x 3 shifts are whole windows inside D: no zero padding
+    for (int p = first; p < W1 * W1; p += stride) {
+      const int o = i + j * a.M;
+      const double tv = (double)fb[o] - tm;
+      const float* q = gb + o;
+#pragma unroll
+      for (int cb = 0; cb < 3; ++cb) {
+        const float* qc = q + cb * a.M;
+#pragma unroll
+        for (int rb = 0; rb < 3; ++rb) v[rb + 3 * cb] += tv * (double)qc[rb];
+      }
+      i += di;
+      j += dj;
+      if (i >= W1) {
+        i -= W1;
+        ++j;
+      }
+    }
+    return;
+  }
   for (int p = first; p < W1 * W1; p += stride) {
-    const double tv = (double)a.f[(size_t)(s.ii - 1 + i) + (size_t)(s.jj - 1 + j) * a.M] - tm;
+    const double tv = (double)fb[i + (size_t)j * a.M] - tm;
 #pragma unroll
     for (int k = 0; k < 9; ++k) {
       const int r = s.dr0 - 2 + pa + (k % 3) + i, c = s.dc0 - 2 + pb + (k / 3) + j;

@@ -101,24 +101,6 @@ inline size_t scratch_layout(int M, int N, int W1, int nx, int ny, int nda, char
 
 __device__ __forceinline__ float rsqrt_from(double v) { return v > 0 ? (float)(1.0 / sqrt(v)) : INFINITY; }
 
-// Centring constant of the tile with origin (i0, j0): the mean of its valid template means
-// (a fixed summation order, so every kernel computes the same float).
-__device__ inline float tile_centre(const SubsetPrm* __restrict__ prm, int nx, int ny, int i0, int j0, int TI) {
-  double s = 0.0;
-  int c = 0;
-  for (int q = 0; q < TI * kTJ; ++q) {
-    const int i = i0 + q % TI, j = j0 + q / TI;
-    if (i < nx && j < ny) {
-      const SubsetPrm& P = prm[i + (long long)j * nx];
-      if (P.valid) {
-        s += P.fm;
-        ++c;
-      }
-    }
-  }
-  return c ? (float)(s / c) : 0.f;
-}
-
 }  // namespace
 
 // Window mean and variance sum of g for every full (w+1)^2 window position (x, y) (top-left,
@@ -824,12 +806,33 @@ __global__ void __launch_bounds__(256) subset_refit_kernel(SearchArgs a, const S
   refit_peak_warp(a, s, subset_out(a, t), bi % s.na, bi / s.na, P.fm, P.denT, P.tolz);
 }
 
-// Centring constant of every tile (tile_centre), one thread per tile.
+// Centring constant of every tile: the mean of its valid template means (one warp per
+// tile; the lanes' partial sums are added in lane order by lane 0, a fixed order shared by
+// every launch).
 __global__ void tile_centre_kernel(int nx, int ny, int TI, const SubsetPrm* __restrict__ prm, float* __restrict__ cf) {
   const int ntx = (nx + TI - 1) / TI, nty = (ny + kTJ - 1) / kTJ;
-  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  const int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (b >= ntx * nty) return;
-  cf[b] = tile_centre(prm, nx, ny, (b % ntx) * TI, (b / ntx) * kTJ, TI);
+  const int i0 = (b % ntx) * TI, j0 = (b / ntx) * kTJ;
+  double s = 0.0;
+  int c = 0;
+  for (int q = lane; q < TI * kTJ; q += 32) {
+    const int i = i0 + q % TI, j = j0 + q / TI;
+    if (i < nx && j < ny) {
+      const SubsetPrm& P = prm[i + (long long)j * nx];
+      if (P.valid) {
+        s += P.fm;
+        ++c;
+      }
+    }
+  }
+  double ts = 0.0;
+  int tc = 0;
+  for (int l = 0; l < 32; ++l) {
+    ts += __shfl_sync(0xffffffffu, s, l);
+    tc += __shfl_sync(0xffffffffu, c, l);
+  }
+  if (lane == 0) cf[b] = tc ? (float)(ts / tc) : 0.f;
 }
 
 namespace {
@@ -892,7 +895,7 @@ int launch_search_tile(const SearchArgs& a, cudaStream_t st) {
   window_rowmax_kernel<<<(unsigned)((nh + 255) / 256), 256, 0, st>>>(a, sc.V, sc.H);
   subset_prep_kernel<<<(unsigned)((n * 32 + 255) / 256), 256, 0, st>>>(a, sc.H, sc.prm, sc.ringv);
   const int ntiles = ((a.nx + e.TI - 1) / e.TI) * ((a.ny + kTJ - 1) / kTJ);
-  tile_centre_kernel<<<(ntiles + 127) / 128, 128, 0, st>>>(a.nx, a.ny, e.TI, sc.prm, sc.cf);
+  tile_centre_kernel<<<(ntiles * 32 + 255) / 256, 256, 0, st>>>(a.nx, a.ny, e.TI, sc.prm, sc.cf);
   ring_column_kernel<<<(unsigned)((n * 32 + 255) / 256), 256, 0, st>>>(a, sc.prm, e.TI, sc.cf, sc.cx);
   if (a.ev_start) cudaEventRecord(a.ev_start, st);
   if (e.launch(a, sc, st) != 0) return -1;
