@@ -66,6 +66,7 @@ struct TileScratch {
   float* cx;         // nx * ny x 2 NDA: products of the excluded template column
   int* best;         // nx * ny: crop index of the first maximum
   float* cf;         // one centring constant per tile
+  double* rr;        // nx x 2 sides x 4 x (N+1): integral-image rows of the top / bottom ring windows
 };
 
 inline size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
@@ -86,7 +87,9 @@ inline size_t scratch_layout(int M, int N, int W1, int nx, int ny, int nda, char
   char* pc = take(n * 2 * (size_t)nda * sizeof(float));
   char* pb = take(n * sizeof(int));
   char* pf = take(n * sizeof(float));  // >= the number of tiles
+  char* prr = take((size_t)nx * 8 * (size_t)(N + 1) * sizeof(double));
   if (sc) {
+    sc->rr = (double*)prr;
     sc->cf = (float*)pf;
     sc->map = (float2*)pm;
     sc->V = (double*)pv;
@@ -133,11 +136,32 @@ __global__ void window_rowmax_kernel(SearchArgs a, const double* __restrict__ V,
   H[p] = m;
 }
 
+// Rows r0 and r1 + 1 of both integral images for the top (a = 0) and bottom (a = na-1)
+// ring windows of grid row i, whose rows [r0, r1] depend on i alone: stored contiguously
+// so that the window sums along a ring row read consecutive addresses.
+__global__ void ring_rows_kernel(SearchArgs a, double* __restrict__ rr) {
+  const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const int N1 = a.N + 1;
+  if (p >= (long long)a.nx * 2 * N1) return;
+  const int c = (int)(p % N1), side = (int)((p / N1) % 2), i = (int)(p / (2 * (long long)N1));
+  const int w = a.winsize;
+  const AxisGeom g = axis_geom(a.gx0 + i * a.step, w, a.s0, a.s1, a.M, a.gx1);
+  if (!g.ok) return;
+  const int na = g.lo + g.hi + 3, aa = side ? na - 1 : 0;
+  const int r0 = max(g.d0, g.d0 - 1 + aa), r1 = min(g.d1, g.d0 - 1 + aa + w);
+  const size_t ld = (size_t)a.M + 1;
+  double* out = rr + ((size_t)i * 2 + side) * 4 * N1;
+  out[c] = a.I1[(size_t)r0 + c * ld];
+  out[N1 + c] = a.I1[(size_t)(r1 + 1) + c * ld];
+  out[2 * N1 + c] = a.I2[(size_t)r0 + c * ld];
+  out[3 * N1 + c] = a.I2[(size_t)(r1 + 1) + c * ld];
+}
+
 // One warp per subset: template mean and norm, the window sums of the ring of partial
 // windows, the largest window variance sum over the crop (normxcorr2 zero threshold) and
 // validity; writes x, y and the NaN outputs of invalid subsets.
-__global__ void subset_prep_kernel(SearchArgs a, const double* __restrict__ H, SubsetPrm* __restrict__ prm,
-                                   float2* __restrict__ ringv) {
+__global__ void subset_prep_kernel(SearchArgs a, const double* __restrict__ H, const double* __restrict__ rr,
+                                   SubsetPrm* __restrict__ prm, float2* __restrict__ ringv) {
   const int lane = threadIdx.x & 31;
   const long long t = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
   const long long n = (long long)a.nx * a.ny;
@@ -174,13 +198,19 @@ __global__ void subset_prep_kernel(SearchArgs a, const double* __restrict__ H, S
       double m = 0.0;
       for (int da = -s.L + lane; da <= s.R; da += 32) m = fmax(m, H[(size_t)(s.ii - 1 + da) + (size_t)j * MW]);
       // the ring of partial windows: a in {0, na-1} for every b, b in {0, nb-1} for every a
-      for (int k = lane; k < 2 * s.nb; k += 32) {
-        double S1, S2;
-        const int side = k & 1, bb = k >> 1;
-        window_sums(s, w, side ? s.na - 1 : 0, bb, a.I1, a.I2, ld, &S1, &S2);
-        const double v = S2 - S1 * S1 / nwin;
-        m = fmax(m, v);
-        rv[side * nda + bb] = make_float2((float)(S1 / nwin), rsqrt_from(v));
+      const int N1 = a.N + 1;
+      const int i = (int)(t % a.nx);
+      for (int side = 0; side < 2; ++side) {
+        // the same expression as window_sums, from the extracted rows r0 and r1 + 1
+        const double* R = rr + ((size_t)i * 2 + side) * 4 * N1;
+        for (int bb = lane; bb < s.nb; bb += 32) {
+          const int c0 = max(s.dc0, s.dc0 - 1 + bb), c1 = min(s.dc1, s.dc0 - 1 + bb + w);
+          const double S1 = (R[N1 + c1 + 1] - R[N1 + c0]) - (R[c1 + 1] - R[c0]);
+          const double S2 = (R[3 * N1 + c1 + 1] - R[3 * N1 + c0]) - (R[2 * N1 + c1 + 1] - R[2 * N1 + c0]);
+          const double v = S2 - S1 * S1 / nwin;
+          m = fmax(m, v);
+          rv[side * nda + bb] = make_float2((float)(S1 / nwin), rsqrt_from(v));
+        }
       }
       for (int k = lane; k < 2 * s.na; k += 32) {
         double S1, S2;
@@ -893,7 +923,9 @@ int launch_search_tile(const SearchArgs& a, cudaStream_t st) {
   window_map_kernel<<<(unsigned)((npos + 255) / 256), 256, 0, st>>>(a.I1, a.I2, a.M, a.N, W1, sc.map, sc.V);
   const long long nh = (long long)(a.M - W1 + 1) * a.ny;
   window_rowmax_kernel<<<(unsigned)((nh + 255) / 256), 256, 0, st>>>(a, sc.V, sc.H);
-  subset_prep_kernel<<<(unsigned)((n * 32 + 255) / 256), 256, 0, st>>>(a, sc.H, sc.prm, sc.ringv);
+  const long long nrr = (long long)a.nx * 2 * (a.N + 1);
+  ring_rows_kernel<<<(unsigned)((nrr + 255) / 256), 256, 0, st>>>(a, sc.rr);
+  subset_prep_kernel<<<(unsigned)((n * 32 + 255) / 256), 256, 0, st>>>(a, sc.H, sc.rr, sc.prm, sc.ringv);
   const int ntiles = ((a.nx + e.TI - 1) / e.TI) * ((a.ny + kTJ - 1) / kTJ);
   tile_centre_kernel<<<(ntiles * 32 + 255) / 256, 256, 0, st>>>(a.nx, a.ny, e.TI, sc.prm, sc.cf);
   ring_column_kernel<<<(unsigned)((n * 32 + 255) / 256), 256, 0, st>>>(a, sc.prm, e.TI, sc.cf, sc.cx);
@@ -901,7 +933,7 @@ int launch_search_tile(const SearchArgs& a, cudaStream_t st) {
   if (e.launch(a, sc, st) != 0) return -1;
   if (a.ev_stop) cudaEventRecord(a.ev_stop, st);
   subset_refit_kernel<<<(unsigned)((n * 32 + 255) / 256), 256, 0, st>>>(a, sc.prm, sc.best);
-  return 7;
+  return 8;
 }
 
 }  // namespace aldic
