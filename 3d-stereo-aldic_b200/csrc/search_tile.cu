@@ -52,14 +52,26 @@ struct TileShape {
   static_assert(FR <= kRing - 1, "tile rows must leave one free ring row");
 };
 
+// Shared memory per CTA: the dynamic buffers plus the static per-subset arrays (a bound).
+template <int ST, int W1, int TI>
+constexpr size_t tile_total_smem() {
+  return TileShape<ST, W1, TI>::smem_bytes + (size_t)TI * kTJ * 40 + 1024;
+}
+
+// Subset rows per tile: as many as fit 127 tile rows and the 227 KB of shared memory a CTA
+// may use.
 template <int ST, int W1>
 struct TileFor {
-  static constexpr int TI = (kRing - 1 - W1) / ST + 1;  // as many subset rows as fit 127 tile rows
+  static constexpr int TI0 = (kRing - 1 - W1) / ST + 1;
+  static constexpr int TI = tile_total_smem<ST, W1, TI0>() <= 232448 ? TI0
+                            : tile_total_smem<ST, W1, TI0 - 1>() <= 232448 ? TI0 - 1
+                                                                          : TI0 - 2;
+  static_assert(tile_total_smem<ST, W1, TI>() <= 232448, "tile does not fit shared memory");
 };
 
 struct TileScratch {
-  float2* map;       // MW x NW: (window mean of g, 1 / sqrt(window variance sum)) per position
-  double* V;         // MW x NW: window variance sum S2 - S1^2 / n
+  float2* map;       // MW x NW row-major (x * NW + y): (window mean of g, 1 / sqrt(variance sum))
+  double* V;         // MW x NW row-major: window variance sum S2 - S1^2 / n
   double* H;         // MW x ny: max of V over the non-ring shift columns of grid column j
   SubsetPrm* prm;    // nx * ny
   float2* ringv;     // nx * ny x 4 NDA: (mean, 1/sqrt(variance sum)) of the partial windows
@@ -113,7 +125,7 @@ __global__ void window_map_kernel(const double* __restrict__ I1, const double* _
   const int MW = M - W1 + 1, NW = N - W1 + 1;
   const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= (long long)MW * NW) return;
-  const int x = (int)(p % MW), y = (int)(p / MW);
+  const int x = (int)(p / NW), y = (int)(p % NW);  // row-major: consecutive shift columns adjacent
   double S1, S2;
   box_sums(x, x + W1 - 1, y, y + W1 - 1, I1, I2, (size_t)M + 1, &S1, &S2);
   const double nwin = (double)W1 * W1;
@@ -124,7 +136,7 @@ __global__ void window_map_kernel(const double* __restrict__ I1, const double* _
 
 // H(x, j) = max(0, max over the non-ring shift columns db in [-U_j, D_j] of V(x, jj-1+db)).
 __global__ void window_rowmax_kernel(SearchArgs a, const double* __restrict__ V, double* __restrict__ H) {
-  const int W1 = a.winsize + 1, MW = a.M - W1 + 1;
+  const int W1 = a.winsize + 1, MW = a.M - W1 + 1, NW = a.N - W1 + 1;
   const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= (long long)MW * a.ny) return;
   const int x = (int)(p % MW), j = (int)(p / MW);
@@ -132,7 +144,7 @@ __global__ void window_rowmax_kernel(SearchArgs a, const double* __restrict__ V,
   const AxisGeom c = axis_geom(jj, a.winsize, a.s0, a.s1, a.N, a.gy1);
   double m = 0.0;
   if (c.ok)
-    for (int db = -c.lo; db <= c.hi; ++db) m = fmax(m, V[x + (size_t)(jj - 1 + db) * MW]);
+    for (int db = -c.lo; db <= c.hi; ++db) m = fmax(m, V[(size_t)x * NW + (jj - 1 + db)]);
   H[p] = m;
 }
 
@@ -605,6 +617,8 @@ __global__ void __launch_bounds__(kTileThreads, 1)
   __shared__ double p_tolv[NSUB];
   __shared__ int p_ok[NSUB];
   __shared__ int r_L[TI], r_na[TI], r_d0[TI], r_d1[TI], c_U[kTJ], c_nb[kTJ], c_d0[kTJ], c_d1[kTJ];
+  __shared__ int r_aoff[TI];   // crop row of shift row k: aa = k + r_aoff
+  __shared__ int p_na[NSUB];   // crop rows of a valid subset, 0 for an invalid one
   __shared__ float s_cf;
 
   const int tid = threadIdx.x;
@@ -613,7 +627,7 @@ __global__ void __launch_bounds__(kTileThreads, 1)
   const int i0 = (int)(blockIdx.x % ntx) * TI, j0 = (int)(blockIdx.x / ntx) * kTJ;
   const int X0 = a.gx0 - 1 + i0 * ST, Y0 = a.gy0 - 1 + j0 * ST;  // 0-based tile origin
   const int DA0 = -a.s0 - 1, NDA = a.s0 + a.s1 + 3;               // shifts, both axes
-  const int MW = a.M - W1 + 1;
+  const int NW = a.N - W1 + 1;
   const double nwin = (double)W1 * W1;
   const size_t ld = (size_t)a.M + 1;
 
@@ -624,6 +638,7 @@ __global__ void __launch_bounds__(kTileThreads, 1)
     const AxisGeom r = axis_geom(a.gx0 + i * a.step, w, a.s0, a.s1, a.M, a.gx1);
     r_L[il] = r.lo;
     r_na[il] = i < a.nx ? r.lo + r.hi + 3 : 0;
+    r_aoff[il] = DA0 + r.lo + 1;
     r_d0[il] = r.d0;
     r_d1[il] = r.d1;
   } else if (tid >= 64 && tid < 64 + kTJ) {
@@ -649,6 +664,8 @@ __global__ void __launch_bounds__(kTileThreads, 1)
     }
     p_ok[q] = ok;
   }
+  __syncthreads();
+  for (int q = tid; q < NSUB; q += kTileThreads) p_na[q] = p_ok[q] ? r_na[q % TI] : 0;
   // ---- f tile, centred ----
   for (int idx = tid; idx < FR * FCP; idx += kTileThreads) {
     const int x = idx / FCP, c = idx % FCP;
@@ -682,7 +699,12 @@ __global__ void __launch_bounds__(kTileThreads, 1)
     }
     for (int idx = FR * GCP + tid; idx < kRing * GCP; idx += kTileThreads) Gt[idx] = 0.f;
     __syncthreads();
+    // this thread's shift column for the chunk: crop column bb of its window column jl
     const int dbr = dbc + dl, db = DA0 + dbr;
+    const int bb = db + c_U[jl] + 1, nbv = c_nb[jl];
+    const bool bok = dbr < NDA && bb >= 0 && bb < nbv;
+    const bool rbg = bb == 0 || bb == nbv - 1;
+    const long long mcol = (long long)(X0 + DA0) * NW + (Y0 + jl * ST + db);  // map index of (il = 0, k = 0)
     for (int k = 0; k < NDA; ++k) {
       const int da = DA0 + k;
       // ---- epilogue operands of this shift, fetched before pass 1 hides their latency ----
@@ -694,14 +716,13 @@ __global__ void __launch_bounds__(kTileThreads, 1)
         st[e] = 0;
         pf[e] = make_float2(0.f, 0.f);
         pcx[e] = 0.f;
-        if (e >= ns || dbr >= NDA) continue;
-        const int il = il0 + e, q = il + jl * TI;
-        if (!p_ok[q]) continue;
-        const int aa = da + r_L[il] + 1, bb = db + c_U[jl] + 1, na = r_na[il], nb = c_nb[jl];
-        if (aa < 0 || aa >= na || bb < 0 || bb >= nb) continue;
-        const bool ra = aa == 0 || aa == na - 1, rbg = bb == 0 || bb == nb - 1;
+        if (!bok || e >= ns) continue;
+        const int il = il0 + e;
+        const int na = p_na[il + jl * TI], aa = k + r_aoff[il];
+        if ((unsigned)aa >= (unsigned)na) continue;
+        const bool ra = aa == 0 || aa == na - 1;
         if (!ra && !rbg) {
-          pf[e] = __ldg(map + (size_t)(X0 + il * ST + da) + (size_t)(Y0 + jl * ST + db) * MW);
+          pf[e] = __ldg(map + (mcol + (long long)(il * ST + k) * NW));
           st[e] = 1;
         } else {
           const long long t = (long long)(i0 + il) + (long long)(j0 + jl) * a.nx;
@@ -769,7 +790,7 @@ __global__ void __launch_bounds__(kTileThreads, 1)
           if (v.y * p_sqtolv[q] < 0.5f) {
             cval = num * v.y * p_invden[q];
           } else {  // near the zero threshold: decide it on the FP64 variance sum
-            const int aa = da + r_L[il] + 1, bb = db + c_U[jl] + 1;
+            const int aa = k + r_aoff[il];
             double var;
             if (sf & 2) {
               SubsetGeom sg;
@@ -781,15 +802,16 @@ __global__ void __launch_bounds__(kTileThreads, 1)
               window_sums(sg, w, aa, bb, a.I1, a.I2, ld, &S1, &S2);
               var = fmax(S2 - S1 * S1 / nwin, 0.0);
             } else {
-              var = fmax(Vmap[(size_t)(X0 + il * ST + da) + (size_t)(Y0 + jl * ST + db) * MW], 0.0);
+              var = fmax(Vmap[mcol + (long long)(il * ST + k) * NW], 0.0);
             }
             cval = var > p_tolv[q] ? num * (float)(1.0 / sqrt(var)) * p_invden[q] : 0.f;
           }
           if (fabsf(cval) - 1.f > 1.4901161193847656e-08f) cval = 0.f;
-          const int lin = (da + r_L[il] + 1) + (db + c_U[jl] + 1) * r_na[il];
-          if (cval > bv[e] || (cval == bv[e] && lin < bl[e])) {
+          // a thread meets each subset's crop indices lin = aa + bb na in increasing order
+          // (aa grows with k, bb with the chunk), so the first maximum is the first strict one
+          if (cval > bv[e]) {
             bv[e] = cval;
-            bl[e] = lin;
+            bl[e] = (k + r_aoff[il]) + bb * p_na[q];
           }
         }
       }
@@ -870,6 +892,7 @@ namespace {
 struct TileEntry {
   int TI;
   int (*launch)(const SearchArgs&, const TileScratch&, cudaStream_t);
+  bool (*fits)();
 };
 
 template <int ST, int W1>
@@ -884,9 +907,20 @@ int launch_tile(const SearchArgs& a, const TileScratch& sc, cudaStream_t st) {
   return 0;
 }
 
+// Whether the tile kernel's shared memory (static + dynamic) fits this device.
+template <int ST, int W1>
+bool tile_fits() {
+  constexpr int TI = TileFor<ST, W1>::TI;
+  cudaFuncAttributes fa;
+  int dev = 0, optin = 0;
+  return cudaFuncGetAttributes(&fa, ncc_tile_kernel<ST, W1, TI>) == cudaSuccess && cudaGetDevice(&dev) == cudaSuccess &&
+         cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) == cudaSuccess &&
+         fa.sharedSizeBytes + TileShape<ST, W1, TI>::smem_bytes <= (size_t)optin;
+}
+
 template <int ST, int W1>
 TileEntry entry() {
-  return TileEntry{TileFor<ST, W1>::TI, launch_tile<ST, W1>};
+  return TileEntry{TileFor<ST, W1>::TI, launch_tile<ST, W1>, tile_fits<ST, W1>};
 }
 
 // The step / window pairs with a tile kernel (others use the per-subset kernel).
@@ -914,7 +948,7 @@ size_t search_tile_bytes(int M, int N, int winsize, int step, int nx, int ny, in
 int launch_search_tile(const SearchArgs& a, cudaStream_t st) {
   const int W1 = a.winsize + 1;
   TileEntry e;
-  if (!tile_entry(a.step, W1, &e) || !a.tile_scratch || a.M < W1 || a.N < W1) return -1;
+  if (!tile_entry(a.step, W1, &e) || !a.tile_scratch || a.M < W1 || a.N < W1 || !e.fits()) return -1;
   const int nda = a.s0 + a.s1 + 3;
   TileScratch sc;
   scratch_layout(a.M, a.N, W1, a.nx, a.ny, nda, (char*)a.tile_scratch, &sc);
