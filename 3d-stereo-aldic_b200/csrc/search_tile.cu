@@ -769,49 +769,68 @@ __global__ void __launch_bounds__(kTileThreads, 1)
 #pragma unroll
           for (int e = 0; e < TI - H0; ++e) N[e] = N1[e];
         }
+        // fast path, branch-free: interior shifts whose variance sum is well above the
+        // zero threshold; the others (ring shifts, near-threshold variance) are flagged
+        unsigned slow = 0;
 #pragma unroll
         for (int e = 0; e < H0; ++e) {
-          const int sf = st[e];
-          if (!sf) continue;
-          const int il = il0 + e, q = il + jl * TI;
-          float C = N[e];
-          if (sf & 2) {  // partial window: drop the template row / column whose partner is outside D
-            const int rx = (sf & 16) ? il * ST : il * ST + W1 - 1;
-            const int cxc = (sf & 32) ? jl * ST : jl * ST + W1 - 1;
-            if (sf & 4) C -= rbrow[rx];
-            if (sf & 8) {
-              C -= pcx[e];
-              if (sf & 4) C += Ft[rx * FCP + cxc] * Gt[((rx + k) & (kRing - 1)) * GCP + cxc + dl];
-            }
-          }
+          if (e >= ns) break;  // the second half has TI - H0 subset rows
+          const int q = il0 + e + jl * TI;
           const float2 v = pf[e];
-          const float num = C - p_kf[q] * v.x;
-          float cval;
-          if (v.y * p_sqtolv[q] < 0.5f) {
-            cval = num * v.y * p_invden[q];
-          } else {  // near the zero threshold: decide it on the FP64 variance sum
-            const int aa = k + r_aoff[il];
-            double var;
-            if (sf & 2) {
-              SubsetGeom sg;
-              sg.dr0 = r_d0[il];
-              sg.dr1 = r_d1[il];
-              sg.dc0 = c_d0[jl];
-              sg.dc1 = c_d1[jl];
-              double S1, S2;
-              window_sums(sg, w, aa, bb, a.I1, a.I2, ld, &S1, &S2);
-              var = fmax(S2 - S1 * S1 / nwin, 0.0);
-            } else {
-              var = fmax(Vmap[mcol + (long long)(il * ST + k) * NW], 0.0);
-            }
-            cval = var > p_tolv[q] ? num * (float)(1.0 / sqrt(var)) * p_invden[q] : 0.f;
-          }
+          const bool fast = st[e] == 1 && v.y * p_sqtolv[q] < 0.5f;
+          if (st[e] != 0 && !fast) slow |= 1u << e;
+          float cval = (N[e] - p_kf[q] * v.x) * v.y * p_invden[q];
           if (fabsf(cval) - 1.f > 1.4901161193847656e-08f) cval = 0.f;
           // a thread meets each subset's crop indices lin = aa + bb na in increasing order
           // (aa grows with k, bb with the chunk), so the first maximum is the first strict one
-          if (cval > bv[e]) {
+          if (fast && cval > bv[e]) {
             bv[e] = cval;
-            bl[e] = (k + r_aoff[il]) + bb * p_na[q];
+            bl[e] = (k + r_aoff[il0 + e]) + bb * p_na[q];
+          }
+        }
+        if (slow) {
+#pragma unroll
+          for (int e = 0; e < H0; ++e) {
+            if (!((slow >> e) & 1u)) continue;
+            const int sf = st[e];
+            const int il = il0 + e, q = il + jl * TI;
+            float C = N[e];
+            if (sf & 2) {  // partial window: drop the template row / column whose partner is outside D
+              const int rx = (sf & 16) ? il * ST : il * ST + W1 - 1;
+              const int cxc = (sf & 32) ? jl * ST : jl * ST + W1 - 1;
+              if (sf & 4) C -= rbrow[rx];
+              if (sf & 8) {
+                C -= pcx[e];
+                if (sf & 4) C += Ft[rx * FCP + cxc] * Gt[((rx + k) & (kRing - 1)) * GCP + cxc + dl];
+              }
+            }
+            const float2 v = pf[e];
+            const float num = C - p_kf[q] * v.x;
+            float cval;
+            if (v.y * p_sqtolv[q] < 0.5f) {
+              cval = num * v.y * p_invden[q];
+            } else {  // near the zero threshold: decide it on the FP64 variance sum
+              const int aa = k + r_aoff[il];
+              double var;
+              if (sf & 2) {
+                SubsetGeom sg;
+                sg.dr0 = r_d0[il];
+                sg.dr1 = r_d1[il];
+                sg.dc0 = c_d0[jl];
+                sg.dc1 = c_d1[jl];
+                double S1, S2;
+                window_sums(sg, w, aa, bb, a.I1, a.I2, ld, &S1, &S2);
+                var = fmax(S2 - S1 * S1 / nwin, 0.0);
+              } else {
+                var = fmax(Vmap[mcol + (long long)(il * ST + k) * NW], 0.0);
+              }
+              cval = var > p_tolv[q] ? num * (float)(1.0 / sqrt(var)) * p_invden[q] : 0.f;
+            }
+            if (fabsf(cval) - 1.f > 1.4901161193847656e-08f) cval = 0.f;
+            if (cval > bv[e]) {
+              bv[e] = cval;
+              bl[e] = (k + r_aoff[il]) + bb * p_na[q];
+            }
           }
         }
       }
