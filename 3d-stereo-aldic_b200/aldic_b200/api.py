@@ -248,16 +248,25 @@ class Context:
             return out
         return dict(U=U, F=F, H=None if H is None else H.reshape((n, 21), order="F"), conv=conv, markHole=mark)
 
-    def subpb1(self, variant, coords, UOld, FOld, vdual, mu, tol, winsize=0, winsize_list=None, HPar=None):
+    def subpb1(self, variant, coords, UOld, FOld, vdual, mu, tol, winsize=0, winsize_list=None, HPar=None, out=None):
+        """Subpb1 / Subpb1Quadtree local step.  With `out` (dict of CUDA tensors U (2n), conv (n))
+        and device inputs the call stays on the device and returns `out` asynchronously."""
         k = _Keep()
         n = _count(coords, 2)
-        U, up = k.out(2 * n, np.float64)
-        conv, cp = k.out(n, np.int32)
-        wl = None if winsize_list is None else k.ptr(winsize_list, np.int32)
-        rc = self.lib.aldic_subpb1(self.h, int(variant), n, k.ptr(coords, np.float64), k.ptr(UOld, np.float64, "C"),
-                                   k.ptr(FOld, np.float64, "C"), k.ptr(vdual, np.float64, "C"), wl, int(winsize),
+        if out is None:
+            U, up = k.out(2 * n, np.float64)
+            conv, cp = k.out(n, np.int32)
+        else:
+            up = k.ptr(out["U"], np.float64, numel=2 * n)
+            cp = k.ptr(out["conv"], np.int32, numel=n)
+        wl = None if winsize_list is None else k.ptr(winsize_list, np.int32, numel=2 * n)  # n x 2 (wx, wy)
+        rc = self.lib.aldic_subpb1(self.h, int(variant), n, k.ptr(coords, np.float64, numel=2 * n),
+                                   k.ptr(UOld, np.float64, "C", numel=2 * n), k.ptr(FOld, np.float64, "C", numel=4 * n),
+                                   k.ptr(vdual, np.float64, "C", numel=2 * n), wl, int(winsize),
                                    k.ptr(HPar, np.float64), float(mu), float(tol), up, cp)
         self._check(rc, "aldic_subpb1")
+        if out is not None:
+            return out
         return dict(U=U, conv=conv)
 
     def epipolar_icgn(self, pts, winsize, tol):

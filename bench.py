@@ -40,6 +40,8 @@ UNIT = "subsets/s"
 # workload description
 # ----------------------------------------------------------------------------------
 def workload_params(name):
+    if name == "quadtree2048":
+        return dict(size=2048, w=32, step=16, s_temp=10, tol_temp=1e-3, mu=1e-3, admm=3)
     if name == "stereo2048":
         return dict(size=2048, w=40, step=10, s_stereo=70, s_temp=10, tol_stereo=1e-3, tol_temp=1e-2)
     if name == "stereo1024":  # same geometry at half the resolution (profiling case)
@@ -401,7 +403,10 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="stereo2048", choices=["stereo2048", "stereo1024"])
+    ap.add_argument("--workload", default="stereo2048",
+                    choices=["stereo2048", "stereo1024", "temporal512", "quadtree2048"],
+                    help="stereo2048: the headline stereo + temporal + triangulation step; temporal512 and "
+                         "quadtree2048: the 2D and quadtree/Subpb1 configurations (separate JSON lines)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--ref-per-pass", type=int, default=200)
@@ -418,6 +423,10 @@ def main():
     if args.impl == "reference":
         if rank == 0:
             run_reference(args, P)
+        return
+    if args.workload in ("temporal512", "quadtree2048"):
+        if rank == 0:
+            run_aux(args, P)
         return
 
     import torch
@@ -541,6 +550,207 @@ def main():
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+# ----------------------------------------------------------------------------------
+# the 2D temporal (512^2) and quadtree ALDIC (2048^2, hole + notch, Subpb1) workloads
+# ----------------------------------------------------------------------------------
+def quadtree_nodes(M, N, mask, margin):
+    """A quadtree-like node set: spacing 8 px within 640 px of the mask edge (hole and notch),
+    16 px within 960 px, 32 px elsewhere (mesh generation is host work in the reference; this stands in
+    for GenerateQuadtreeMesh).  Returns coords (n x 2, 1-based) and the local spacing."""
+    from scipy import ndimage
+
+    edge_dist = np.where(mask > 0, ndimage.distance_transform_edt(mask > 0), ndimage.distance_transform_edt(mask == 0))
+    pts, sp = [], []
+    for s, lo, hi in ((8, 0, 640), (16, 640, 960), (32, 960, 1e9)):
+        xs = np.arange(margin, M - margin + 1, s, dtype=np.float64)
+        ys = np.arange(margin, N - margin + 1, s, dtype=np.float64)
+        X, Y = np.meshgrid(xs, ys, indexing="ij")
+        d = edge_dist[X.astype(int) - 1, Y.astype(int) - 1]
+        inside = mask[X.astype(int) - 1, Y.astype(int) - 1] > 0
+        keep = (d >= lo) & (d < hi) & (inside | (d < 8))
+        pts.append(np.stack([X[keep], Y[keep]], 1))
+        sp.append(np.full(int(keep.sum()), s))
+    coords = np.concatenate(pts)
+    coords, idx = np.unique(coords, axis=0, return_index=True)
+    return coords, np.concatenate(sp)[idx]
+
+
+def run_aux(args, P):
+    """temporal512: LocalICGN on a 512^2 affine pair, FFT-search init.
+    quadtree2048 (config 2): masked quadtree LocalICGNQuadtree + 3 Subpb1Quadtree steps on a
+    2048^2 plate with a hole and an edge notch.  Device-resident; verified on the oracle."""
+    import torch
+
+    import aldic_b200 as A
+    from aldic_b200 import synth
+
+    dev = torch.device("cuda:0")
+    torch.cuda.set_device(dev)
+    T = torch
+    f64 = dict(dtype=T.float64, device=dev)
+    quad = args.workload == "quadtree2048"
+    if quad:
+        sc = synth.plate_with_hole(seed=args.seed, size=2048, hole_r=300.0, peak=5.0, sin_amp=0.5, sin_wl=200.0)
+        mask = sc.mask
+    else:
+        sc = synth.temporal_affine(seed=args.seed)
+        mask = None
+    M, N = sc.ref.shape
+    w, st = P["w"], P["step"]
+    gx, gy = [1, M], [1, N]
+    # search grid (XList rule) and the solve mesh
+    gcoords, nx, ny = grid_coords(M, N, w, st)
+    if quad:
+        coords_np, spacing = quadtree_nodes(M, N, mask, margin=w // 2 + P["s_temp"] + 8)
+        wl_np = np.clip(2 * spacing, 16, 64).astype(np.int32)
+        wl = T.from_numpy(np.concatenate([wl_np, wl_np])).to(dev)  # n x 2 column-major (wx, wy)
+    else:
+        coords_np = gcoords
+    n = coords_np.shape[0]
+    coords = T.from_numpy(np.ascontiguousarray(coords_np.T)).to(dev)
+    raw = {k: T.from_numpy(np.asfortranarray(img).ravel(order="F").copy()).to(dev) for k, img in
+           (("ref", sc.ref), ("def", sc.deff))}
+    mask_d = None if mask is None else T.from_numpy(np.asfortranarray(mask).ravel(order="F").copy()).to(dev)
+    ctx = A.Context(0)
+    stream = T.cuda.Stream(dev)
+    ctx.set_stream(stream.cuda_stream)
+    g = nx * ny
+    b = {"x": T.empty(g, **f64), "y": T.empty(g, **f64), "u": T.empty(g, **f64), "v": T.empty(g, **f64),
+         "phi": T.empty(g, **f64), "U0": T.empty(2 * n, **f64), "U": T.empty(2 * n, **f64),
+         "F": T.empty(4 * n, **f64), "H": T.empty(21 * n, **f64), "conv": T.empty(n, dtype=T.int32, device=dev),
+         "mark": T.empty(n, dtype=T.uint8, device=dev)}
+    sub = [{"U": T.empty(2 * n, **f64), "conv": T.empty(n, dtype=T.int32, device=dev)} for _ in range(P.get("admm", 0))]
+    vdual = T.zeros(2 * n, **f64)
+    cxy = coords.t()
+    shp = (M, N)
+
+    def step():
+        with T.cuda.stream(stream):
+            ctx.load_image_raw(0, raw["ref"], gx, gy, want_stats=False, shape=shp)
+            ctx.load_image_raw(1, raw["def"], gx, gy, want_stats=False, shape=shp)
+            if quad:
+                ctx.set_mask(mask_d)
+            ctx.compute_gradients()
+            ctx.integer_search([P["s_temp"]] * 2, gx, gy, w, st, out=b)
+            # nearest search-grid node of every mesh node (Init stand-in), NaN -> 0
+            i = T.clamp(T.round((cxy[:, 0] - (1 + w / 2.0)) / st), 0, nx - 1).long()
+            j = T.clamp(T.round((cxy[:, 1] - (1 + w / 2.0)) / st), 0, ny - 1).long()
+            gidx = j + i * ny
+            b["U0"].view(n, 2).copy_(T.nan_to_num(T.stack([b["u"][gidx], b["v"][gidx]], 1), nan=0.0))
+            ctx.local_icgn(1 if quad else 0, coords, b["U0"], w, P["tol_temp"], out=b)
+            Uold = b["U"]
+            for k in range(P.get("admm", 0)):
+                ctx.subpb1(1, coords, T.nan_to_num(Uold, nan=0.0), T.nan_to_num(b["F"], nan=0.0), vdual, P["mu"],
+                           P["tol_temp"], winsize=w, winsize_list=wl, out=sub[k])
+                Uold = sub[k]["U"]
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    T.cuda.synchronize(dev)
+    clocks = ClockSampler(0)
+    l0 = ctx.launches
+    ev0, ev1 = T.cuda.Event(enable_timing=True), T.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+    ev1.record(stream)
+    T.cuda.synchronize(dev)
+    clk = clocks.stop()
+    ms_step = ev0.elapsed_time(ev1) / args.steps
+    launches = ctx.launches - l0
+    solves = n * (1 + P.get("admm", 0))
+    ver = None
+    counted = None
+    if not args.no_verify:
+        import oracle as O
+
+        O.build()
+        f, _ = O.normalize(sc.ref.astype(np.float64), gx, gy)
+        gimg, _ = O.normalize(sc.deff.astype(np.float64), gx, gy)
+        gxo, gyo = O.gradient(f, mask)
+        frame = O.Frame(f, gimg, mask, gxo, gyo)
+        rng = np.random.default_rng(args.seed)
+        pick = np.arange(n) if n <= 3000 else np.sort(rng.choice(n, 3000, replace=False))
+        U0 = b["U0"].view(n, 2).cpu().numpy()[pick].ravel()
+        U = b["U"].view(n, 2).cpu().numpy()[pick]
+        conv = b["conv"].cpu().numpy()[pick]
+        t0 = time.perf_counter()
+        ref = O.local_icgn(frame, coords_np[pick], U0, w, P["tol_temp"], variant=1 if quad else 0,
+                           nthreads=host_threads())
+        t_icgn = time.perf_counter() - t0
+        fg = (conv > 0) & (conv < 100)
+        fo = (ref["conv"] > 0) & (ref["conv"] < 100)
+        d = np.abs(U - ref["U"].reshape(-1, 2))
+        ok = fg & fo & np.all(d <= 0.01, axis=1)
+        ver = {"sample": int(len(pick)), "icgn_flag_match": float(np.mean(fg == fo)),
+               "icgn_code_match": float(np.mean(conv == ref["conv"])),
+               "icgn_uv_max_err": float(d[fg & fo].max()) if (fg & fo).any() else None,
+               "icgn_counted_fraction": float(ok.mean()), "oracle_icgn_s": t_icgn}
+        counted = ok.mean() * n
+        if quad:
+            # first ADMM step from the device's own IC-GN results
+            Uin = np.nan_to_num(b["U"].view(n, 2).cpu().numpy()[pick]).ravel()
+            Fin = np.nan_to_num(b["F"].view(n, 4).cpu().numpy()[pick]).ravel()
+            s1 = O.subpb1(frame, coords_np[pick], Uin, Fin, np.zeros(2 * len(pick)), P["mu"], P["tol_temp"],
+                          winsize=w, winsize_list=np.stack([wl_np[pick], wl_np[pick]], 1), nthreads=host_threads())
+            Us = sub[0]["U"].view(n, 2).cpu().numpy()[pick]
+            cs = sub[0]["conv"].cpu().numpy()[pick]
+            fgs = (cs > 0) & (cs < 100)
+            fos = (s1["conv"] > 0) & (s1["conv"] < 100)
+            ds = np.abs(Us - s1["U"].reshape(-1, 2))
+            ver.update({"subpb1_flag_match": float(np.mean(fgs == fos)),
+                        "subpb1_uv_max_err": float(ds[fgs & fos].max()) if (fgs & fos).any() else None})
+    cpu = None
+    if not args.no_cpu:
+        import oracle as O
+
+        O.build()
+        f, _ = O.normalize(sc.ref.astype(np.float64), gx, gy)
+        gimg, _ = O.normalize(sc.deff.astype(np.float64), gx, gy)
+        gxo, gyo = O.gradient(f, mask)
+        frame = O.Frame(f, gimg, mask, gxo, gyo)
+        U0h = b["U0"].view(n, 2).cpu().numpy()
+        Uh = np.nan_to_num(b["U"].view(n, 2).cpu().numpy())
+        Fh = np.nan_to_num(b["F"].view(n, 4).cpu().numpy())
+        rng = np.random.default_rng(args.seed + 7)
+        cpu = {"kind": "port", "unit": "subsets/s" if not quad else "subset solves/s"}
+        for threads in (host_threads(), 1):
+            ns = min(n, 900 if threads > 1 else 150)
+            pk = np.sort(rng.choice(n, ns, replace=False))
+            gpk = np.sort(rng.choice(nx * ny, min(nx * ny, 400 if threads > 1 else 60), replace=False))
+            t0 = time.perf_counter()
+            O.search_list(f, gimg, [P["s_temp"]] * 2, M, N, 1 + (gpk % nx) * st, 1 + (gpk // nx) * st, w,
+                          nthreads=threads)
+            t_search = (time.perf_counter() - t0) * (nx * ny) / len(gpk)
+            t0 = time.perf_counter()
+            O.local_icgn(frame, coords_np[pk], U0h[pk].ravel(), w, P["tol_temp"], variant=1 if quad else 0,
+                         nthreads=threads)
+            t_solve = time.perf_counter() - t0
+            if quad:
+                for _ in range(P["admm"]):
+                    O.subpb1(frame, coords_np[pk], Uh[pk].ravel(), Fh[pk].ravel(), np.zeros(2 * ns), P["mu"],
+                             P["tol_temp"], winsize=w, winsize_list=np.stack([wl_np[pk], wl_np[pk]], 1),
+                             nthreads=threads)
+                t_solve = time.perf_counter() - t0
+            t_step = t_search + t_solve * n / ns
+            per = (solves if quad else (counted if counted is not None else n)) / t_step
+            key = "value" if threads > 1 else "value_1core"
+            cpu[key] = per
+            if threads > 1:
+                cpu["cores"] = threads
+        cpu["sample"] = ("whole-field search timed on a sample of grid subsets and scaled to the grid; "
+                         "solves timed on 900 (150 on one core) mesh nodes and scaled to the mesh")
+    line = {"metric": METRIC if not quad else "subset solves/s (1 LocalICGNQuadtree + 3 Subpb1Quadtree per node)",
+            "value": (counted if (counted is not None and not quad) else solves) / (ms_step * 1e-3),
+            "unit": UNIT if not quad else "subset solves/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 (FP64 solve)", "data": "synthetic (seeded analytic speckle rendering)",
+            "config": {"workload": args.workload, "subsets": int(n), "image": [int(M), int(N)], **P},
+            "gpu_launches": int(launches), "clocks": clk, "verification": ver, "cpu_baseline": cpu}
+    print(json.dumps(line), flush=True)
+    ctx.close()
 
 
 def measure_fp32_peak(torch, dev):
