@@ -76,3 +76,12 @@ def test_null_context_is_rejected():
     assert lib.aldic_compute_gradients(None) == 1
     assert lib.aldic_local_icgn(None, 1, 0, None, None, 30, 1e-3, None, None, None, None, None) == 1
     assert lib.aldic_last_error(None) == b"null context"
+
+
+def test_package_exports_the_names_callers_use():
+    # the names __graft_entry__.smoke() and MATLAB-style callers take from the package
+    import aldic_b200 as A
+
+    assert (A.UNIFORM, A.QUADTREE) == (0, 1)
+    for name in ("Context", "AldicError", "load_library", "LocalICGNQuadtree", "funIntegerSearch", "synth"):
+        assert hasattr(A, name), name
