@@ -47,6 +47,7 @@ SIGNATURES = {
     "aldic_triangulate": (_i, [_vp, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "aldic_measure_fp32_peak": (_i, [_vp, C.POINTER(_d)]),
     "aldic_set_profiling": (_i, [_vp, _i]),
+    "aldic_set_iteration_cap": (_i, [_vp, _i]),
     "aldic_profile_read": (_i, [_vp, C.POINTER(_d), C.POINTER(_i)]),
     "aldic_local_icgn_noalloc": (_i, [_i, _vp, _vp, _vp, _vp, _vp, _i, _i, _i64, _vp, _vp, _i, _d, _vp, _vp, _vp,
                                       _vp, _vp, _vp]),

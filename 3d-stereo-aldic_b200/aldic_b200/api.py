@@ -134,6 +134,11 @@ class Context:
     def launches(self):
         return int(self.lib.aldic_launch_count(self.h))
 
+    def set_iteration_cap(self, cap):
+        """Iterations the one-warp solver pass spends on a subset before the 4-warp pass
+        restarts it (default 16)."""
+        self._check(self.lib.aldic_set_iteration_cap(self.h, int(cap)), "aldic_set_iteration_cap")
+
     def set_profiling(self, on=True):
         """Record the device time of the correlation kernel of each integer_search call."""
         self._check(self.lib.aldic_set_profiling(self.h, 1 if on else 0), "aldic_set_profiling")

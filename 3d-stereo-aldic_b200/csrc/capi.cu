@@ -54,6 +54,7 @@ struct aldic_ctx {
   size_t ii_cap = 0;
   void* tscratch = nullptr;  // shared-product search scratch
   size_t tscratch_cap = 0;
+  int warp_cap = kDefaultWarpCap;  // aldic_set_iteration_cap
   // profiling: event pairs around the correlation kernel of each integer search
   bool prof = false;
   std::vector<cudaEvent_t> prof_ev;  // 2 per record
@@ -529,6 +530,7 @@ static int icgn_common(aldic_ctx* c, int variant, int64_t n, const double* coord
   a.winsize = winsize;
   a.tol = tol;
   a.max_iter = epi ? 30 : 100;
+  a.warp_cap = c->warp_cap;
   a.crop = epi ? 4 : 3;
   a.U = (double*)au.dev;
   a.F = (double*)af.dev;
@@ -622,6 +624,7 @@ int aldic_subpb1(aldic_ctx* c, int variant, int64_t n, const double* coords, con
   a.winsize = winsize;
   a.HPar = (const double*)ahp.dev;
   a.mu = mu;
+  a.warp_cap = c->warp_cap;
   a.tol = tol;
   a.U = (double*)au.dev;
   a.conv = (int*)acv.dev;
@@ -691,6 +694,13 @@ int aldic_measure_fp32_peak(aldic_ctx* c, double* tflops) {
   c->launches += 2;
   const double flops = 2.0 * 8 * 16 * (double)iters * threads * blocks;
   *tflops = flops / (ms * 1e-3) / 1e12;
+  return ALDIC_OK;
+}
+
+int aldic_set_iteration_cap(aldic_ctx* c, int cap) {
+  if (!c) return ALDIC_ERR_ARG;
+  if (cap < 1 || cap > 1000) return fail(c, ALDIC_ERR_ARG, "iteration cap %d outside 1..1000", cap);
+  c->warp_cap = cap;
   return ALDIC_OK;
 }
 

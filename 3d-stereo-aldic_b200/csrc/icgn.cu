@@ -595,7 +595,8 @@ __global__ void __launch_bounds__(kNT) icgn_solve_kernel(IcgnArgs a, int bucket)
 // Gauss-Newton Hessian; a zero pivot propagates Inf/NaN as the reference's singular solve
 // does).
 //
-// The main pass (NW = 1, queue 0) gives each subset at most kWarpIterCap iterations: the
+// The main pass (NW = 1, queue 0) gives each subset at most warp_cap iterations (16 by
+// default): the
 // few subsets that need more (most never converge and run to max_iter) would otherwise
 // keep single warps running long after the rest of the grid.  They go to queue 1 flagged
 // kSlowSubset and restart from the beginning in the 4-warp pass (NW = 4), which runs each
@@ -603,7 +604,6 @@ __global__ void __launch_bounds__(kNT) icgn_solve_kernel(IcgnArgs a, int bucket)
 // masked deformed image) needs the g-region flood fill: it is handed to the general kernel
 // through queue 1 and restarted there.
 constexpr int kWT = 256;  // threads per CTA: 8 / NW subset groups
-constexpr int kWarpIterCap = 16;
 
 template <int NW>
 __device__ __forceinline__ void group_bar(int id) {
@@ -800,7 +800,7 @@ __global__ void __launch_bounds__(kWT, 2) icgn_group_kernel(IcgnArgs a) {
     double normNew = 1.0, normAbs = 1.0, normInit = 0.0, znssd = ALDIC_NAN;
     int step = 0, status = 0, requeue = -1;
     while (step <= a.max_iter && normNew > a.tol && normAbs > a.tol) {
-      if (!SLOW && step >= kWarpIterCap) {  // a slow subset: restarted by the 4-warp pass
+      if (!SLOW && step >= a.warp_cap) {  // a slow subset: restarted by the 4-warp pass
         requeue = kSlowSubset;
         break;
       }
@@ -950,12 +950,18 @@ __global__ void __launch_bounds__(kWT, 2) icgn_group_kernel(IcgnArgs a) {
     }
     if (gt == 0) {
       if (requeue >= 0) {
-        // restart this subset in a later pass (they run after this kernel)
-        const int pos = atomicAdd(&a.qcount[1], 1);
-        int* q1 = a.queue + 3 * ((long long)a.n + pos);
-        q1[0] = (int)t;
-        q1[1] = w;
-        q1[2] = requeue;
+        // restart this subset in a later pass (they run after this kernel).  A queue-0
+        // subset is appended to queue 1 (at most one entry each: queue 1 never holds more
+        // than n); a queue-1 subset is re-flagged in place.
+        if (SLOW) {
+          const_cast<int*>(q)[2] = requeue;
+        } else {
+          const int pos = atomicAdd(&a.qcount[1], 1);
+          int* q1 = a.queue + 3 * ((long long)a.n + pos);
+          q1[0] = (int)t;
+          q1[1] = w;
+          q1[2] = requeue;
+        }
       } else {
         if (status == 1) step -= 1000;
         if (!(normNew < a.tol || normAbs < a.tol)) step = a.max_iter + 1;
@@ -1137,7 +1143,8 @@ __global__ void __launch_bounds__(kNT) subpb1_solve_kernel(Sub1Args a, int bucke
     const int* q = a.queue + 4 * ((long long)bucket * a.n + qi);
     const long long t = q[0];
     const int wx = q[1], wy = q[2];
-    const bool masked = q[3] != 0;
+    if (q[3] == 0 || q[3] == kSlowSubset) continue;  // solved by the warp-group passes
+    const bool masked = q[3] == 1;
     const int R = wx + 1, Cc = wy + 1, npx = R * Cc;
     const int hx = wx / 2, hy = wy / 2;
     double x0 = a.coords[t], y0 = a.coords[a.n + t];
@@ -1386,6 +1393,219 @@ size_t icgn_smem_bytes(int w) { return (size_t)(w + 1) * (w + 1) * (4 * sizeof(f
 size_t sub1_smem_bytes(int wx, int wy) { return (size_t)(wx + 1) * (wy + 1) * (4 * sizeof(float) + 5); }
 
 
+// ================================================================================
+// Subpb1 for unmasked subsets: warp groups, as icgn_group_kernel
+// ================================================================================
+// Every subset without a mask region (either queue; any window size) is solved by a group of
+// NW warps with no shared image buffer and no block barrier; the FP64 control is replicated
+// in every thread.  The main pass (NW = 1) gives a subset at most warp_cap iterations and
+// hands slower ones to the 4-warp pass (queue-1 flag kSlowSubset); a quadtree subset that
+// meets an exact zero in g needs the g-region flood fill and goes to the general kernel
+// (flag kRestartGeneral).  Queue-1 entries are flagged 0 (unmasked: this kernel), 1 (masked:
+// the general kernel), kSlowSubset or kRestartGeneral.
+constexpr int kRestartGeneral = 3;
+
+template <int NW, bool SLOW>
+__global__ void __launch_bounds__(kWT, 2) subpb1_group_kernel(Sub1Args a) {
+  constexpr int NG = kWT / (32 * NW);
+  constexpr int GT = 32 * NW;
+  __shared__ double s_red[NG][NW * 11];
+  __shared__ int s_qi[NG];
+  const int lane = threadIdx.x & 31, grp = threadIdx.x / GT, gw = (threadIdx.x % GT) >> 5;
+  const int gt = threadIdx.x % GT, bar = 1 + grp;
+  double* red = s_red[grp];
+  const FrameDev& fr = a.fr;
+  const bool quad = (a.variant == 1);
+  const int c0n = SLOW ? 0 : a.qcount[0];
+  const int count = c0n + a.qcount[1];
+  const int gM = fr.M - 6;
+  int* next = a.qcount + (SLOW ? 3 : 2);
+  while (true) {
+    int qi = 0;
+    if (gt == 0) qi = atomicAdd(next, 1);
+    if (NW == 1) {
+      qi = __shfl_sync(0xffffffffu, qi, 0);
+    } else {
+      if (gt == 0) s_qi[grp] = qi;
+      group_bar<NW>(bar);
+      qi = s_qi[grp];
+    }
+    if (qi >= count) break;
+    const int* q = qi < c0n ? a.queue + 4 * (long long)qi : a.queue + 4 * (a.n + (qi - c0n));
+    if (q[3] != (SLOW ? kSlowSubset : 0)) {
+      group_bar<NW>(bar);
+      continue;
+    }
+    const long long t = q[0];
+    const int wx = q[1], wy = q[2];
+    const int R = wx + 1, Cc = wy + 1, npx = R * Cc;
+    const int hx = wx / 2, hy = wy / 2;
+    double x0 = a.coords[t], y0 = a.coords[a.n + t];
+    if (quad) {
+      x0 = mround(x0);
+      y0 = mround(y0);
+    }
+    const int r0 = (int)x0 - hx - 1, c0 = (int)y0 - hy - 1;
+    const int q_nt = GT / R, r_nt = GT % R;
+    // ---- f-side sums over the whole window ----
+    double H2[4], A2[2], B2[2], meanf, bf, sabsf;
+    {
+      float h0 = 0, h1 = 0, h2 = 0, jf0 = 0, jf1 = 0, jb0 = 0, jb1 = 0, fs = 0, fs2 = 0, fn = 0, fab = 0;
+      int aa = gt % R, bb = gt / R;
+      for (int p = gt; p < npx; p += GT) {
+        const int k = (r0 + aa) + (c0 + bb) * fr.M;
+        const int kg = (r0 + aa - 3) + (c0 + bb - 3) * gM;
+        const float f = fr.ref[k], gxv = fr.gx[kg], gyv = fr.gy[kg];
+        h0 = fmaf(gxv, gxv, h0);
+        h1 = fmaf(gxv, gyv, h1);
+        h2 = fmaf(gyv, gyv, h2);
+        jf0 = fmaf(gxv, f, jf0);
+        jf1 = fmaf(gyv, f, jf1);
+        jb0 += gxv;
+        jb1 += gyv;
+        if (!quad || fabsf(f) > 1e-10f) {
+          fs += f;
+          fs2 = fmaf(f, f, fs2);
+          fn += 1.f;
+        }
+        fab += fabsf(f);
+        aa += r_nt;
+        bb += q_nt;
+        if (aa >= R) {
+          aa -= R;
+          bb += 1;
+        }
+      }
+      double v[11] = {h0, h1, h2, jf0, jf1, jb0, jb1, fs, fs2, fn, fab};
+      group_sum<NW, 11>(v, red, gw, lane, bar);
+      Sub1Ctl c;
+      double hs[3] = {0, 0, 0};
+      if (!quad && a.HPar) {  // stored Hessian block H(5:6,5:6) (funICGN_Subpb1.m:35)
+        hs[0] = a.HPar[t + a.n * 18];
+        hs[1] = a.HPar[t + a.n * 19];
+        hs[2] = a.HPar[t + a.n * 20];
+      }
+      sub1_fside(c, v, quad, hs, a.mu);
+      for (int k = 0; k < 4; ++k) H2[k] = c.H2[k];
+      A2[0] = c.A[0];
+      A2[1] = c.A[1];
+      B2[0] = c.B[0];
+      B2[1] = c.B[1];
+      meanf = c.meanf;
+      bf = c.bf;
+      sabsf = c.sabsf;
+    }
+    (void)meanf;
+    double P[6] = {a.FOld[4 * t], a.FOld[4 * t + 1], a.FOld[4 * t + 2], a.FOld[4 * t + 3], a.UOld[2 * t],
+                   a.UOld[2 * t + 1]};
+    const double uo0 = a.UOld[2 * t], uo1 = a.UOld[2 * t + 1];
+    const double vd0 = a.vdual[2 * t], vd1 = a.vdual[2 * t + 1];
+    double normNew = 1.0, normAbs = 1.0, normInit = 0.0;
+    int step = 0, status = 0, requeue = -1;
+    while (step <= 100 && normNew > a.tol && normAbs > a.tol) {
+      if (!SLOW && step >= a.warp_cap) {
+        requeue = kSlowSubset;
+        break;
+      }
+      step += 1;
+      if (warped_oob(fr, P, x0, y0, hx, hy)) {
+        normNew = 1e6;
+        break;
+      }
+      const double n5 = mround(P[4]), n6 = mround(P[5]);
+      const float p0 = (float)P[0], p1 = (float)P[1], p2 = (float)P[2], p3 = (float)P[3];
+      const float f5 = (float)(P[4] - n5), f6 = (float)(P[5] - n6);
+      const int br = (int)(x0 + n5) - 2, bc = (int)(y0 + n6) - 2;
+      float C0 = 0, C1 = 0, S1 = 0, S2 = 0, ns = 0, nz = 0;
+      {
+        int aa = gt % R, bb = gt / R;
+        for (int p = gt; p < npx; p += GT) {
+          const float dx = (float)(aa - hx), dy = (float)(bb - hy);
+          const float lx = dx + fmaf(p0, dx, fmaf(p2, dy, f5));
+          const float ly = dy + fmaf(p3, dy, fmaf(p1, dx, f6));
+          const float ix = floorf(lx), iy = floorf(ly);
+          const float g = stencil16(fr.def, fr.M, br + (int)ix, bc + (int)iy, lx - ix, ly - iy);
+          const int kg = (r0 + aa - 3) + (c0 + bb - 3) * gM;
+          C0 = fmaf(fr.gx[kg], g, C0);
+          C1 = fmaf(fr.gy[kg], g, C1);
+          if (!quad || fabsf(g) > 1e-10f) {
+            S1 += g;
+            S2 = fmaf(g, g, S2);
+            ns += 1.f;
+          }
+          nz += (g == 0.f) ? 1.f : 0.f;
+          aa += r_nt;
+          bb += q_nt;
+          if (aa >= R) {
+            aa -= R;
+            bb += 1;
+          }
+        }
+      }
+      double v[6] = {C0, C1, S1, S2, ns, nz};
+      group_sum<NW, 6>(v, red, gw, lane, bar);
+      if (quad && v[5] > 0) {  // exact zero in g: the g-region flood fill of the general kernel
+        requeue = kRestartGeneral;
+        break;
+      }
+      double meang, bgn;
+      if (v[4] > 0) {
+        meang = v[2] / v[4];
+        bgn = sqrt(fmax(v[3] - v[2] * v[2] / v[4], 0.0));
+      } else {
+        meang = ALDIC_NAN;
+        bgn = ALDIC_NAN;
+      }
+      double b[2];
+      for (int i = 0; i < 2; ++i) b[i] = bf * (A2[i] - (v[i] - meang * B2[i]) / bgn);
+      const double s2 = 2.0 / (bf * bf);
+      const double tb[2] = {b[0] * s2 + a.mu * (P[4] - uo0 - vd0), b[1] * s2 + a.mu * (P[5] - uo1 - vd1)};
+      const double dmax = fmax(H2[0], H2[3]);
+      const double tH[4] = {H2[0] + 1e-3 * dmax, H2[1], H2[2], H2[3] + 1e-3 * dmax};
+      const double nb[2] = {-tb[0], -tb[1]};
+      double d56[2];
+      solve_small(2, tH, nb, d56);
+      normNew = sqrt(tb[0] * tb[0] + tb[1] * tb[1]);
+      normAbs = normNew;
+      if (step == 1) normInit = normNew;
+      if (normInit > a.tol) normNew = normNew / normInit;
+      else normNew = 0.0;
+      if (!(normNew < a.tol || normAbs < a.tol)) {
+        const double dP[6] = {0, 0, 0, 0, d56[0], d56[1]};
+        if (!compose_inverse(P, dP)) {
+          step += 1000;
+          status = 1;
+        }
+      }
+    }
+    if (gt == 0) {
+      if (requeue >= 0) {
+        // a queue-1 entry is re-flagged in place; a queue-0 subset is appended once, so
+        // queue 1 never holds more than n entries
+        if (qi >= c0n) {
+          const_cast<int*>(q)[3] = requeue;
+        } else {
+          const int pos = atomicAdd(&a.qcount[1], 1);
+          int* q1 = a.queue + 4 * (a.n + pos);
+          q1[0] = (int)t;
+          q1[1] = wx;
+          q1[2] = wy;
+          q1[3] = requeue;
+        }
+      } else {
+        if (status == 1) step -= 1000;
+        if (!(normNew < a.tol || normAbs < a.tol)) step = 101;
+        if (isnan(normNew)) step = 101;
+        if (quad && sabsf < 1e-6) step = 103;
+        a.conv[t] = step;
+        a.U[2 * t] = P[4];
+        a.U[2 * t + 1] = P[5];
+      }
+    }
+    group_bar<NW>(bar);
+  }
+}
+
 int launch_icgn(const IcgnArgs& a, int wmax_enlarged, cudaStream_t st) {
   int launches = 0;
   cudaMemsetAsync(a.qcount, 0, 4 * sizeof(int), st);  // 2 queue counts, 2 work counters
@@ -1426,19 +1646,37 @@ int launch_icgn(const IcgnArgs& a, int wmax_enlarged, cudaStream_t st) {
 
 int launch_subpb1(const Sub1Args& a, int wmax_x, int wmax_y, cudaStream_t st) {
   int launches = 0;
-  cudaMemsetAsync(a.qcount, 0, 2 * sizeof(int), st);
+  cudaMemsetAsync(a.qcount, 0, 4 * sizeof(int), st);  // 2 queue counts, 2 work counters
   const long long threads = a.n * 32;
   const int cb = 256;
   subpb1_classify_kernel<<<(unsigned)((threads + cb - 1) / cb), cb, 0, st>>>(a);
   ++launches;
-  for (int bucket = 0; bucket < 2; ++bucket) {
-    const size_t smem = bucket == 0 ? sub1_smem_bytes(a.winsize, a.winsize) : sub1_smem_bytes(wmax_x, wmax_y);
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  {  // unmasked subsets (both queues): one warp per subset, then the slow ones with 4
+    int per_sm = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, subpb1_group_kernel<1, false>, kWT, 0);
+    long long grid = (long long)sms * (per_sm < 1 ? 1 : per_sm);
+    const long long need = (a.n + 7) / 8;
+    if (grid > need) grid = need;
+    subpb1_group_kernel<1, false><<<(unsigned)grid, kWT, 0, st>>>(a);
+    per_sm = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, subpb1_group_kernel<4, true>, kWT, 0);
+    grid = (long long)sms * (per_sm < 1 ? 1 : per_sm);
+    const long long need4 = (a.n + 1) / 2;
+    if (grid > need4) grid = need4;
+    subpb1_group_kernel<4, true><<<(unsigned)grid, kWT, 0, st>>>(a);
+    launches += 2;
+  }
+  {  // masked subsets and restarts: the general kernel on queue 1
+    const size_t smem = sub1_smem_bytes(wmax_x, wmax_y);
     cudaFuncSetAttribute(subpb1_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int grid = occupancy_grid((const void*)subpb1_solve_kernel, smem);
-    if (bucket == 1) grid = grid < 296 ? grid : 296;
+    grid = grid < 296 ? grid : 296;
     if ((long long)grid > a.n) grid = (int)a.n;
     if (grid < 1) grid = 1;
-    subpb1_solve_kernel<<<grid, kNT, smem, st>>>(a, bucket);
+    subpb1_solve_kernel<<<grid, kNT, smem, st>>>(a, 1);
     ++launches;
   }
   return launches;

@@ -26,6 +26,7 @@ struct IcgnArgs {
   int winsize;
   double tol;
   int max_iter;  // 100, or 30 for the epipolar variant
+  int warp_cap;  // iterations the one-warp pass spends on a subset before the 4-warp pass restarts it
   int crop;      // gradient offset: 3 (DfCropWidth) or 4 (DfAxis start)
   double* U;     // 2n
   double* F;     // 4n
@@ -49,10 +50,11 @@ struct Sub1Args {
   int winsize;              // uniform winsize / nominal bucket size
   const double* HPar;       // n x 21 (uniform)
   double mu, tol;
+  int warp_cap;  // as IcgnArgs::warp_cap
   double* U;
   int* conv;
   int* queue;   // 2 buckets x n x 4 ints
-  int* qcount;  // 2
+  int* qcount;  // 4: queue counts of the 2 buckets, work counters of the 2 warp-group passes
 };
 
 struct SearchArgs {
@@ -94,6 +96,7 @@ size_t search_tot_bytes(int M, int N);
 int launch_search(const SearchArgs& a, cudaStream_t st);
 // Shared-product search (search_tile.cu): scratch size (0 when the step / window pair has
 // no tile kernel), and the launcher (returns the launch count, or -1 when not available).
+constexpr int kDefaultWarpCap = 16;  // default IcgnArgs / Sub1Args warp_cap
 size_t search_tile_bytes(int M, int N, int winsize, int step, int nx, int ny, int s0, int s1);
 int launch_search_tile(const SearchArgs& a, cudaStream_t st);
 struct CamPair {

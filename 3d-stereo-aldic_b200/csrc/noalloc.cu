@@ -112,6 +112,7 @@ extern "C" int aldic_local_icgn_noalloc(int variant, const float* ref, const flo
   a.winsize = winsize;
   a.tol = tol;
   a.max_iter = 100;
+  a.warp_cap = aldic::kDefaultWarpCap;
   a.crop = 3;
   a.U = U;
   a.F = F;

@@ -162,6 +162,11 @@ int aldic_local_icgn_noalloc(int variant, const float* ref, const float* def, co
 /* Measured FP32 FMA throughput of the current device (TFLOP/s), the denominator the
  * library's compute-bound kernels are reported against.  Not part of the reference. */
 int aldic_measure_fp32_peak(aldic_ctx* ctx, double* tflops);
+/* Iterations the one-warp-per-subset solver pass of aldic_local_icgn / aldic_subpb1 spends
+ * on a subset before a 4-warp pass restarts it from its initial guess (default 16, 1..1000).
+ * Results do not depend on it beyond FP32 summation order; it trades the tail of slow
+ * subsets against repeated work.  A tuning setting; not part of the reference. */
+int aldic_set_iteration_cap(aldic_ctx* ctx, int cap);
 /* Device time of the correlation kernel of every aldic_integer_search call while profiling
  * is on (CUDA events recorded on the context's stream around that one launch; up to 256
  * calls are kept).  aldic_profile_read waits for the recorded events, returns their total

@@ -261,6 +261,70 @@ def test_subpb1_quadtree_parity(ctx, hole):
     assert np.all(np.isnan(res["U"].reshape(-1, 2)[err]))
 
 
+def test_subpb1_quadtree_mixed_windows_and_slow_subsets(ctx, hole):
+    # per-subset windows 16 / 24 / 32 (queue 0 holds only the nominal size; the others are
+    # unmasked queue-1 subsets solved by the warp-group passes); with an iteration cap of 1
+    # every subset needing more than one iteration restarts in the 4-warp pass
+    sc = hole
+    M, N = sc.ref.shape
+    ctx.load_image_raw(0, sc.ref, [1, M], [1, N], mask=sc.mask)
+    ctx.load_image_raw(1, sc.deff, [1, M], [1, N])
+    ctx.set_mask(sc.mask)
+    ctx.compute_gradients()
+    f, g = ctx.get_state(0), ctx.get_state(1)
+    gx, gy = ctx.get_state(2), ctx.get_state(3)
+    xs = np.arange(24, 366, 9.0)
+    X, Y = np.meshgrid(xs, xs, indexing="ij")
+    coords = np.stack([X.ravel(), Y.ravel()], 1)
+    n = len(coords)
+    tu, tv = sc.disp(coords[:, 0], coords[:, 1])
+    rng = np.random.default_rng(3)
+    UOld = np.stack([tu, tv], 1).ravel() + rng.normal(0, 0.2, 2 * n)
+    FOld = np.tile([0.004, 0.0, 0.0, -0.002], n)
+    vdual = rng.normal(0, 0.05, 2 * n)
+    wsz = rng.choice([16, 24, 32], n).astype(np.int32)
+    wl = np.stack([wsz, wsz], 1)
+    ref = O.subpb1(O.Frame(f, g, sc.mask, gx, gy), coords, UOld, FOld, vdual, 1e-3, 1e-3, winsize_list=wl,
+                   variant=1)
+    assert np.sum(ref["conv"] > 1) > n // 4
+    try:
+        for cap in (16, 1):
+            ctx.set_iteration_cap(cap)
+            res = ctx.subpb1(1, coords, UOld, FOld, vdual, 1e-3, 1e-3, winsize=24, winsize_list=wl)
+            assert np.mean(res["conv"] == ref["conv"]) >= 0.98, cap
+            assert np.mean(_flag(res["conv"]) == _flag(ref["conv"])) >= FLAG_RATE, cap
+            both = _flag(res["conv"]) & _flag(ref["conv"])
+            assert np.abs(res["U"] - ref["U"]).reshape(-1, 2)[both].max() < UV_TOL, cap
+            assert np.array_equal(np.isnan(res["U"]), np.isnan(ref["U"])), cap
+    finally:
+        ctx.set_iteration_cap(16)
+
+
+def test_local_icgn_slow_subsets_restart(ctx, affine):
+    # with an iteration cap of 1 every subset that needs a second iteration is restarted by
+    # the 4-warp pass; codes and displacements still match the oracle
+    _load_raw(ctx, affine)
+    M, N = affine.ref.shape
+    f, g = ctx.get_state(0), ctx.get_state(1)
+    gx, gy = ctx.get_state(2), ctx.get_state(3)
+    r = ctx.integer_search([10, 10], [1, M], [1, N], 30, 16)
+    coords = np.stack([r["x"].T.ravel(order="F"), r["y"].T.ravel(order="F")], 1)
+    U0 = np.nan_to_num(np.stack([r["u"].T.ravel(order="F"), r["v"].T.ravel(order="F")], 1)).ravel()
+    ref = O.local_icgn(O.Frame(f, g, None, gx, gy), coords, U0, 30, 1e-3, variant=0)
+    assert np.sum(ref["conv"] > 1) > len(coords) // 2
+    try:
+        ctx.set_iteration_cap(1)
+        res = ctx.local_icgn(0, coords, U0, 30, 1e-3)
+    finally:
+        ctx.set_iteration_cap(16)
+    assert np.mean(res["conv"] == ref["conv"]) >= 0.98
+    assert np.mean(_flag(res["conv"]) == _flag(ref["conv"])) >= FLAG_RATE
+    both = _flag(res["conv"]) & _flag(ref["conv"])
+    assert np.abs(res["U"] - ref["U"]).reshape(-1, 2)[both].max() < UV_TOL
+    with pytest.raises(Exception):
+        ctx.set_iteration_cap(0)
+
+
 def test_subpb1_uniform_parity(ctx, affine):
     sc = affine
     _load_raw(ctx, sc)
