@@ -54,6 +54,23 @@ class _Keep:
         self.items.append(a)
         return C.c_void_p(a.ctypes.data)
 
+    def dst(self, x, dtype, numel):
+        """An output the library writes in place: a CUDA tensor, or a writeable contiguous
+        host numpy array of exactly `dtype` (in pinned host memory the device->host copy is
+        a direct DMA).  Anything that would need a conversion is refused, since the results
+        would land in a temporary."""
+        if x is None:
+            return None
+        if _is_torch(x):
+            return self.ptr(x, dtype, numel=numel)
+        ok = isinstance(x, np.ndarray) and x.dtype == np.dtype(dtype) and x.flags.writeable and (
+            x.flags.c_contiguous or x.flags.f_contiguous)
+        if not ok:
+            raise AldicError(f"outputs must be CUDA tensors or writeable contiguous {np.dtype(dtype)} numpy arrays")
+        if x.size < numel:
+            raise AldicError(f"output array holds {x.size} elements, {numel} required")
+        return C.c_void_p(x.ctypes.data)
+
     def out(self, n, dtype):
         a = np.empty(n, dtype=dtype)
         self.items.append(a)
@@ -210,7 +227,8 @@ class Context:
 
     def integer_search(self, search, gridx, gridy, winsize, step, out=None):
         """Whole-field search on the resident REF/DEF images.  Returns dict of nY x nX
-        arrays (host), or fills `out` (dict of device tensors) asynchronously."""
+        arrays (host), or fills `out`: a dict of CUDA tensors (asynchronously, on the
+        context's stream) or of host numpy arrays (before the call returns)."""
         s = np.asarray(search, dtype=np.int32).ravel()
         if s.size == 1:
             s = np.array([s[0], s[0]], dtype=np.int32)
@@ -222,7 +240,7 @@ class Context:
             bufs = {name: k.out(nx * ny, np.float64) for name in ("x", "y", "u", "v", "phi")}
             ptrs = [bufs[nm][1] for nm in ("x", "y", "u", "v", "phi")]
         else:
-            ptrs = [k.ptr(out[nm], np.float64, numel=nx * ny) for nm in ("x", "y", "u", "v", "phi")]
+            ptrs = [k.dst(out[nm], np.float64, nx * ny) for nm in ("x", "y", "u", "v", "phi")]
         rc = self.lib.aldic_integer_search(self.h, C.c_void_p(s.ctypes.data), C.c_void_p(gx.ctypes.data),
                                            C.c_void_p(gy.ctypes.data), int(winsize), int(step), *ptrs)
         self._check(rc, "aldic_integer_search")
@@ -240,11 +258,11 @@ class Context:
             conv, cp = k.out(n, np.int32)
             mark, mp = k.out(n, np.uint8) if (want_mark and variant == _lib.QUADTREE) else (None, None)
         else:
-            up = k.ptr(out["U"], np.float64, numel=2 * n)
-            fp = k.ptr(out["F"], np.float64, numel=4 * n)
-            hp = k.ptr(out.get("H"), np.float64, numel=21 * n)
-            cp = k.ptr(out["conv"], np.int32, numel=n)
-            mp = k.ptr(out.get("mark"), np.uint8, numel=n)
+            up = k.dst(out["U"], np.float64, 2 * n)
+            fp = k.dst(out["F"], np.float64, 4 * n)
+            hp = k.dst(out.get("H"), np.float64, 21 * n)
+            cp = k.dst(out["conv"], np.int32, n)
+            mp = k.dst(out.get("mark"), np.uint8, n)
         rc = self.lib.aldic_local_icgn(self.h, int(variant), n, k.ptr(coords, np.float64, numel=2 * n),
                                        k.ptr(U0, np.float64, "C", numel=2 * n), int(winsize), float(tol), up, fp, hp,
                                        cp, mp)
@@ -262,8 +280,8 @@ class Context:
             U, up = k.out(2 * n, np.float64)
             conv, cp = k.out(n, np.int32)
         else:
-            up = k.ptr(out["U"], np.float64, numel=2 * n)
-            cp = k.ptr(out["conv"], np.int32, numel=n)
+            up = k.dst(out["U"], np.float64, 2 * n)
+            cp = k.dst(out["conv"], np.int32, n)
         wl = None if winsize_list is None else k.ptr(winsize_list, np.int32, numel=2 * n)  # n x 2 (wx, wy)
         rc = self.lib.aldic_subpb1(self.h, int(variant), n, k.ptr(coords, np.float64, numel=2 * n),
                                    k.ptr(UOld, np.float64, "C", numel=2 * n), k.ptr(FOld, np.float64, "C", numel=4 * n),
@@ -289,8 +307,8 @@ class Context:
             xyz, xp = k.out(3 * n, np.float64)
             err, ep = k.out(n, np.float64)
         else:
-            xp = k.ptr(out["xyz"], np.float64, numel=3 * n)
-            ep = k.ptr(out.get("err"), np.float64, numel=n)
+            xp = k.dst(out["xyz"], np.float64, 3 * n)
+            ep = k.dst(out.get("err"), np.float64, n)
         rc = self.lib.aldic_triangulate(self.h, n, k.ptr(pairs, np.float64, numel=4 * n), k.ptr(KL, np.float64),
                                         k.ptr(KR, np.float64), k.ptr(R, np.float64), k.ptr(np.ravel(T), np.float64),
                                         xp, ep)

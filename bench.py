@@ -175,9 +175,14 @@ class StereoPipeline:
         # MATLAB n x 2 column-major coordinatesFEM == a (2, n) row-major device tensor
         self.coords = T.from_numpy(np.ascontiguousarray(self.coords_np.T)).to(device)
         self.ctx = {k: A.Context(device.index or 0) for k in ("S", "L", "R")}
-        self.stream = T.cuda.Stream(device)
-        for c in self.ctx.values():
-            c.set_stream(self.stream.cuda_stream)
+        # one stream per pass: the stereo pass owns the step's first and last work (the
+        # timing stream); the temporal passes fork after the stereo search and join
+        # before triangulation, so the stereo correlation kernel runs alone
+        self.streams = {k: T.cuda.Stream(device) for k in ("S", "L", "R")}
+        self.stream = self.streams["S"]
+        for k, c in self.ctx.items():
+            c.set_stream(self.streams[k].cuda_stream)
+        self.ev = {k: T.cuda.Event() for k in ("fork", "S", "L", "R")}
         n, g = self.n, self.nx * self.ny
         self.buf = {}
         for k in ("S", "L", "R"):
@@ -204,36 +209,59 @@ class StereoPipeline:
         b["U0"].copy_(T.nan_to_num(U0, nan=0.0))
 
     def step(self):
-        with self.torch.cuda.stream(self.stream):
-            self._step()
+        T, st, ev = self.torch, self.streams, self.ev
+        with T.cuda.stream(st["S"]):
+            self._stereo_search()
+        ev["fork"].record(st["S"])
+        with T.cuda.stream(st["S"]):
+            self._stereo_icgn()
+        ev["S"].record(st["S"])
+        with T.cuda.stream(st["L"]):
+            st["L"].wait_event(ev["fork"])
+            self._temporal_left()
+        ev["L"].record(st["L"])
+        with T.cuda.stream(st["R"]):
+            st["R"].wait_event(ev["fork"])
+            self._temporal_right(ev["S"])
+        ev["R"].record(st["R"])
+        with T.cuda.stream(st["S"]):
+            st["S"].wait_event(ev["L"])
+            st["S"].wait_event(ev["R"])
+            self._triangulate()
 
-    def _step(self):
-        T, P, A = self.torch, self.P, self.A
+    def _load_pair(self, c, ref, cur):
         shp = (self.M, self.N)
-        w, st = P["w"], P["step"]
-        cS, cL, cR = self.ctx["S"], self.ctx["L"], self.ctx["R"]
+        c.load_image_raw(0, self.raw[ref], self.gx, self.gy, want_stats=False, shape=shp)
+        c.load_image_raw(1, self.raw[cur], self.gx, self.gy, want_stats=False, shape=shp)
+        c.compute_gradients()
+
+    def _stereo_search(self):
         # stereo L0 -> R0
-        cS.load_image_raw(0, self.raw["L0"], self.gx, self.gy, want_stats=False, shape=shp)
-        cS.load_image_raw(1, self.raw["R0"], self.gx, self.gy, want_stats=False, shape=shp)
-        cS.compute_gradients()
-        bS = self.buf["S"]
-        cS.integer_search([P["s_stereo"]] * 2, self.gx, self.gy, w, st, out=bS)
+        P, cS, bS = self.P, self.ctx["S"], self.buf["S"]
+        self._load_pair(cS, "L0", "R0")
+        cS.integer_search([P["s_stereo"]] * 2, self.gx, self.gy, P["w"], P["step"], out=bS)
+
+    def _stereo_icgn(self):
+        P, bS = self.P, self.buf["S"]
         self._search_to_U0(bS)
-        cS.local_icgn(1, self.coords, bS["U0"], w, P["tol_stereo"], out=bS)
+        self.ctx["S"].local_icgn(1, self.coords, bS["U0"], P["w"], P["tol_stereo"], out=bS)
+
+    def _temporal_left(self):
         # temporal left L0 -> L1
-        cL.load_image_raw(0, self.raw["L0"], self.gx, self.gy, want_stats=False, shape=shp)
-        cL.load_image_raw(1, self.raw["L1"], self.gx, self.gy, want_stats=False, shape=shp)
-        cL.compute_gradients()
-        bL = self.buf["L"]
-        cL.integer_search([P["s_temp"]] * 2, self.gx, self.gy, w, st, out=bL)
+        P, cL, bL = self.P, self.ctx["L"], self.buf["L"]
+        self._load_pair(cL, "L0", "L1")
+        cL.integer_search([P["s_temp"]] * 2, self.gx, self.gy, P["w"], P["step"], out=bL)
         self._search_to_U0(bL)
-        cL.local_icgn(1, self.coords, bL["U0"], w, P["tol_temp"], out=bL)
+        cL.local_icgn(1, self.coords, bL["U0"], P["w"], P["tol_temp"], out=bL)
+
+    def _temporal_right(self, stereo_done):
         # temporal right R0 -> R1 on the stereo-matched mesh (coords + U_stereo)
-        cR.load_image_raw(0, self.raw["R0"], self.gx, self.gy, want_stats=False, shape=shp)
-        cR.load_image_raw(1, self.raw["R1"], self.gx, self.gy, want_stats=False, shape=shp)
-        cR.compute_gradients()
-        bR = self.buf["R"]
+        T, P = self.torch, self.P
+        w, st = P["w"], P["step"]
+        cR, bR, bS = self.ctx["R"], self.buf["R"], self.buf["S"]
+        self._load_pair(cR, "R0", "R1")
         cR.integer_search([P["s_temp"]] * 2, self.gx, self.gy, w, st, out=bR)
+        T.cuda.current_stream().wait_event(stereo_done)
         n = self.n
         US = bS["U"].view(n, 2)
         cxy = self.coords.t()
@@ -245,9 +273,14 @@ class StereoPipeline:
         gidx = j + i * self.ny
         bR["U0"].view(n, 2).copy_(T.nan_to_num(T.stack([bR["u"][gidx], bR["v"][gidx]], 1), nan=0.0))
         cR.local_icgn(1, self.coordsR, bR["U0"], w, P["tol_temp"], out=bR)
+
+    def _triangulate(self):
         # triangulation of frames 0 and 1
-        UL = bL["U"].view(n, 2)
-        UR = bR["U"].view(n, 2)
+        T, n, cS = self.torch, self.n, self.ctx["S"]
+        cxy = self.coords.t()
+        US = self.buf["S"]["U"].view(n, 2)
+        UL = self.buf["L"]["U"].view(n, 2)
+        UR = self.buf["R"]["U"].view(n, 2)
         p0 = T.cat([cxy, cxy + US], 1)
         p1 = T.cat([cxy + UL, cxy + US + UR], 1)
         self.pairs[0].copy_(p0.t())
@@ -769,56 +802,95 @@ def measure_fp32_peak(torch, dev):
 
 
 def e2e_measure(A, scene, P, steps, local_rank):
-    """The same pass through the public API with host (pinned) buffers: every call copies
-    its inputs host->device and its results device->host."""
+    """The same pass through the public API with host buffers: every call copies its
+    inputs host->device and its results device->host.  Frames and result buffers live in
+    pinned host memory; the three passes run as host threads on their own contexts (and
+    so their own streams), the way a caller overlaps independent passes; the right
+    temporal pass waits for the stereo result before its IC-GN."""
+    import threading
+    from concurrent.futures import ThreadPoolExecutor
+
     import torch
 
     M = N = P["size"]
     w, st = P["w"], P["step"]
     coords, nx, ny = grid_coords(M, N, w, st)
-    n = coords.shape[0]
-    imgs = {k: torch.from_numpy(np.asfortranarray(v)).pin_memory().numpy()
-            for k, v in (("L0", scene.L[0]), ("L1", scene.L[1]), ("R0", scene.R[0]), ("R1", scene.R[1]))}
-    ctx = A.Context(local_rank)
+    n, g = coords.shape[0], nx * ny
+
+    def pinned(shape, dtype=np.float64, order="C"):
+        shape = (shape,) if np.isscalar(shape) else tuple(shape)
+        nb = int(np.prod(shape)) * np.dtype(dtype).itemsize
+        raw = torch.empty(nb, dtype=torch.uint8, pin_memory=True).numpy()
+        return raw.view(dtype).reshape(shape, order=order)
+
+    imgs = {}
+    for k, v in (("L0", scene.L[0]), ("L1", scene.L[1]), ("R0", scene.R[0]), ("R1", scene.R[1])):
+        imgs[k] = pinned(v.shape, v.dtype, order="F")
+        imgs[k][...] = v
+    ctx = {k: A.Context(local_rank) for k in ("S", "L", "R")}
+    out = {k: {**{nm: pinned(g) for nm in ("x", "y", "u", "v", "phi")},
+               "U": pinned(2 * n), "F": pinned(4 * n), "H": pinned(21 * n), "conv": pinned(n, np.int32)}
+           for k in ("S", "L", "R")}
+    tri = [{"xyz": pinned(3 * n), "err": pinned(n)} for _ in range(2)]
+    U0 = {k: pinned(2 * n) for k in ("S", "L", "R")}
+    # MATLAB column-major n x 2 / n x 4 arrays: the library reads them without a repack
+    crd = pinned((n, 2), order="F")
+    crd[:] = coords
+    crdR = pinned((n, 2), order="F")
+    pairs = [pinned((n, 4), order="F") for _ in range(2)]
     gx, gy = [1, M], [1, N]
+    grid_bytes = 5 * g * 8
+    icgn_out_bytes = (2 + 4 + 21) * n * 8 + n * 4
+
+    def search(k, ref, cur, s):
+        c, o = ctx[k], out[k]
+        c.load_image_raw(0, imgs[ref], gx, gy, want_stats=False)
+        c.load_image_raw(1, imgs[cur], gx, gy, want_stats=False)
+        c.compute_gradients()
+        c.integer_search([s, s], gx, gy, w, st, out=o)
+        return o["u"].reshape((ny, nx), order="F"), o["v"].reshape((ny, nx), order="F")
+
+    stereo_done = threading.Event()
+
+    def stereo():
+        u, v = search("S", "L0", "R0", P["s_stereo"])
+        U0["S"].reshape(n, 2)[:] = np.nan_to_num(np.stack([u.T.ravel(order="F"), v.T.ravel(order="F")], 1))
+        ctx["S"].local_icgn(1, crd, U0["S"], w, P["tol_stereo"], out=out["S"])
+        stereo_done.set()
+
+    def left():
+        u, v = search("L", "L0", "L1", P["s_temp"])
+        U0["L"].reshape(n, 2)[:] = np.nan_to_num(np.stack([u.T.ravel(order="F"), v.T.ravel(order="F")], 1))
+        ctx["L"].local_icgn(1, crd, U0["L"], w, P["tol_temp"], out=out["L"])
+
+    def right():
+        u, v = search("R", "R0", "R1", P["s_temp"])
+        stereo_done.wait()
+        # right-camera mesh = left mesh + stereo match; initial guess from the nearest grid node
+        crdR[:] = coords + np.nan_to_num(out["S"]["U"].reshape(n, 2))
+        i = np.clip(np.round((crdR[:, 0] - (1 + w / 2.0)) / st), 0, nx - 1).astype(int)
+        j = np.clip(np.round((crdR[:, 1] - (1 + w / 2.0)) / st), 0, ny - 1).astype(int)
+        U0["R"].reshape(n, 2)[:] = np.nan_to_num(np.stack([u[j, i], v[j, i]], 1))
+        ctx["R"].local_icgn(1, crdR, U0["R"], w, P["tol_temp"], out=out["R"])
+
+    pool = ThreadPoolExecutor(3)
     conv_total = 0
 
     def one():
         nonlocal conv_total
-        h2d = d2h = 0
-        out = {}
-        for name, (ref, deff, s, tol, crd) in (("S", ("L0", "R0", P["s_stereo"], P["tol_stereo"], coords)),
-                                                ("L", ("L0", "L1", P["s_temp"], P["tol_temp"], coords)),
-                                                ("R", ("R0", "R1", P["s_temp"], P["tol_temp"], None))):
-            ctx.load_image_raw(0, imgs[ref], gx, gy, want_stats=False)
-            ctx.load_image_raw(1, imgs[deff], gx, gy, want_stats=False)
-            h2d += imgs[ref].nbytes + imgs[deff].nbytes
-            ctx.compute_gradients()
-            r = ctx.integer_search([s, s], gx, gy, w, st)
-            d2h += 5 * nx * ny * 8
-            u = np.nan_to_num(r["u"].T.ravel(order="F"))
-            v = np.nan_to_num(r["v"].T.ravel(order="F"))
-            if crd is None:  # right camera: mesh = left mesh + stereo match
-                crd = coords + np.nan_to_num(out["S"]["U"].reshape(-1, 2))
-                i = np.clip(np.round((crd[:, 0] - (1 + w / 2.0)) / st), 0, nx - 1).astype(int)
-                j = np.clip(np.round((crd[:, 1] - (1 + w / 2.0)) / st), 0, ny - 1).astype(int)
-                uu = r["u"][j, i]
-                vv = r["v"][j, i]
-                U0 = np.nan_to_num(np.stack([uu, vv], 1).ravel())
-            else:
-                U0 = np.stack([u, v], 1).ravel()
-            res = ctx.local_icgn(1, crd, U0, w, tol)
-            h2d += crd.nbytes + U0.nbytes
-            d2h += res["U"].nbytes + res["F"].nbytes + res["H"].nbytes + res["conv"].nbytes + res["markHole"].nbytes
-            out[name] = res
-            conv_total += int(np.sum((res["conv"] > 0) & (res["conv"] < 100)))
-        UL = out["L"]["U"].reshape(-1, 2)
-        US = out["S"]["U"].reshape(-1, 2)
-        UR = out["R"]["U"].reshape(-1, 2)
-        for pairs in (np.hstack([coords, coords + US]), np.hstack([coords + UL, coords + US + UR])):
-            xyz, err = ctx.triangulate(pairs, scene.KL, scene.KR, scene.R_rl, scene.T_rl)
-            h2d += pairs.nbytes
-            d2h += xyz.nbytes + err.nbytes
+        stereo_done.clear()
+        for f in [pool.submit(fn) for fn in (stereo, left, right)]:
+            f.result()
+        US, UL, UR = (out[k]["U"].reshape(n, 2) for k in ("S", "L", "R"))
+        pairs[0][:, :2] = coords
+        pairs[0][:, 2:] = coords + US
+        pairs[1][:, :2] = coords + UL
+        pairs[1][:, 2:] = coords + US + UR
+        for p, o in zip(pairs, tri):
+            ctx["S"].triangulate(p, scene.KL, scene.KR, scene.R_rl, scene.T_rl, out=o)
+        conv_total += sum(int(np.sum((out[k]["conv"] > 0) & (out[k]["conv"] < 100))) for k in ("S", "L", "R"))
+        h2d = 6 * imgs["L0"].nbytes + 3 * (2 * n * 8 + U0["S"].nbytes) + 2 * pairs[0].nbytes
+        d2h = 3 * (grid_bytes + icgn_out_bytes) + 2 * (tri[0]["xyz"].nbytes + tri[0]["err"].nbytes)
         return h2d, d2h
 
     one()  # warm-up
@@ -829,7 +901,9 @@ def e2e_measure(A, scene, P, steps, local_rank):
         h2d, d2h = one()
     torch.cuda.synchronize()
     ms = (time.perf_counter() - t0) * 1000 / steps
-    ctx.close()
+    pool.shutdown()
+    for c in ctx.values():
+        c.close()
     return {"ms": ms, "converged": conv_total / steps, "h2d": h2d, "d2h": d2h}
 
 

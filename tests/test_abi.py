@@ -85,3 +85,26 @@ def test_package_exports_the_names_callers_use():
     assert (A.UNIFORM, A.QUADTREE) == (0, 1)
     for name in ("Context", "AldicError", "load_library", "LocalICGNQuadtree", "funIntegerSearch", "synth"):
         assert hasattr(A, name), name
+
+
+def test_output_arrays_are_written_in_place_or_refused():
+    """Host outputs passed through `out=` must be the exact arrays the library writes:
+    a conversion would leave the results in a temporary, so it is refused."""
+    from aldic_b200.api import AldicError, _Keep
+
+    k = _Keep()
+    good = np.empty(10, dtype=np.float64)
+    assert k.dst(good, np.float64, 10).value == good.ctypes.data
+    fcol = np.empty((5, 2), dtype=np.float64, order="F")
+    assert k.dst(fcol, np.float64, 10).value == fcol.ctypes.data
+    assert k.dst(None, np.float64, 10) is None
+    bad = [np.empty(10, dtype=np.float32),            # would need a conversion
+           np.empty((10, 2), dtype=np.float64)[:, 0],  # strided view
+           np.empty(9, dtype=np.float64),             # too small
+           [0.0] * 10]                                # not an array
+    ro = np.empty(10, dtype=np.float64)
+    ro.flags.writeable = False
+    bad.append(ro)
+    for b in bad:
+        with pytest.raises(AldicError):
+            k.dst(b, np.float64, 10)

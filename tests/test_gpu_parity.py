@@ -412,6 +412,61 @@ def test_device_pointer_path_matches_host_path(A, ctx, affine):
         ctx.local_icgn(1, c_t, u_t, 30, 1e-3, out=small)
 
 
+def test_pinned_host_outputs_and_threaded_contexts(A, ctx, affine):
+    """Results written in place into pinned host arrays (out=) equal the returned arrays,
+    and three contexts driven from three host threads give the serial results."""
+    import threading
+
+    import torch
+
+    sc = affine
+    M, N = sc.ref.shape
+    _load_raw(ctx, sc)
+    ref_grid = ctx.integer_search([10, 10], [1, M], [1, N], 30, 16)
+    nY, nX = ref_grid["u"].shape
+    coords = np.stack([ref_grid["x"].T.ravel(order="F"), ref_grid["y"].T.ravel(order="F")], 1)
+    U0 = np.stack([ref_grid["u"].T.ravel(order="F"), ref_grid["v"].T.ravel(order="F")], 1).ravel()
+    ref_icgn = ctx.local_icgn(1, coords, U0, 30, 1e-3)
+    n = len(coords)
+
+    def pinned(k, dtype=np.float64):
+        return torch.empty(k, dtype=getattr(torch, np.dtype(dtype).name), pin_memory=True).numpy()
+
+    ctxs = [A.Context(0) for _ in range(3)]
+    outs = [{**{nm: pinned(nX * nY) for nm in ("x", "y", "u", "v", "phi")}, "U": pinned(2 * n),
+             "F": pinned(4 * n), "H": pinned(21 * n), "conv": pinned(n, np.int32)} for _ in range(3)]
+    errors = []
+
+    def run(i):
+        try:
+            c, o = ctxs[i], outs[i]
+            c.load_image_raw(0, sc.ref, [1, M], [1, N])
+            c.load_image_raw(1, sc.deff, [1, M], [1, N])
+            c.compute_gradients()
+            for _ in range(3):
+                assert c.integer_search([10, 10], [1, M], [1, N], 30, 16, out=o) is o
+                assert c.local_icgn(1, coords, U0, 30, 1e-3, out=o) is o
+        except Exception as e:  # reported on the main thread
+            errors.append(e)
+
+    th = [threading.Thread(target=run, args=(i,)) for i in range(3)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    for c in ctxs:
+        c.close()
+    assert not errors, errors
+    for o in outs:
+        for nm in ("u", "v", "phi"):
+            assert np.array_equal(o[nm].reshape((nY, nX), order="F"), ref_grid[nm], equal_nan=True), nm
+        assert np.array_equal(o["conv"], ref_icgn["conv"])
+        assert np.array_equal(o["U"], ref_icgn["U"], equal_nan=True)
+        assert np.array_equal(o["H"], ref_icgn["H"].ravel(order="F"), equal_nan=True)
+    with pytest.raises(A.AldicError):  # a float32 array would take the results into a temporary
+        ctx.local_icgn(1, coords, U0, 30, 1e-3, out=dict(outs[0], U=np.empty(2 * n, np.float32)))
+
+
 def test_launch_counter_and_errors(A, ctx):
     before = ctx.launches
     ctx.triangulate(np.zeros((4, 4)) + 1.0, np.eye(3), np.eye(3), np.eye(3), [1.0, 0, 0])
