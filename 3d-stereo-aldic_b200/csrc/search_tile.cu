@@ -27,46 +27,47 @@ namespace aldic {
 
 namespace {
 
-constexpr int kTileThreads = 256;
 constexpr int kTJ = 8;     // subset columns per tile
-constexpr int kDBC = 16;   // shift columns per chunk (2 groups of 8)
 constexpr int kRing = 128; // rows of the circular g buffer
 
 // Smallest m >= n with m = 4 (mod 8): row strides of 128-bit loads across consecutive
 // rows then hit 8 distinct 16-byte bank groups per quarter warp.
 constexpr int pad4odd(int n) { return ((n + 3) / 4 % 2 == 1) ? (n + 3) / 4 * 4 : (n + 3) / 4 * 4 + 4; }
 
-template <int ST, int W1, int TI>
+// DBC shift columns per chunk, in groups of 8 (one pass-1 thread group of 128 rows each).
+template <int ST, int W1, int TI, int DBC>
 struct TileShape {
   static constexpr int Q = W1 / ST, REM = W1 % ST;
+  static constexpr int NT = DBC / 8 * 128;           // threads per CTA
   static constexpr int FR = (TI - 1) * ST + W1;      // tile rows
   static constexpr int FC = (kTJ - 1) * ST + W1;     // tile columns
   static constexpr int FCP = pad4odd(FC);            // row stride of F (row-major)
-  static constexpr int GCP = pad4odd(FC + 18);       // row stride of the g ring (row-major)
+  static constexpr int GCP = pad4odd(FC + DBC + 2);  // row stride of the g ring (row-major)
   static constexpr int FRP = pad4odd(FR);            // row stride of RB (one row per (j, d))
   static constexpr int H0 = (TI + 1) / 2;            // subset rows of the first pass-2 half
   static constexpr int NSUB = TI * kTJ;
   static constexpr size_t smem_bytes =
-      sizeof(float) * ((size_t)FR * FCP + (size_t)kRing * GCP + (size_t)kTJ * kDBC * FRP);
+      sizeof(float) * ((size_t)FR * FCP + (size_t)kRing * GCP + (size_t)kTJ * DBC * FRP);
+  static_assert(DBC % 8 == 0 && DBC >= 16, "chunks hold whole groups of 8 shift columns");
   static_assert(Q >= 1, "step must not exceed the window");
   static_assert(FR <= kRing - 1, "tile rows must leave one free ring row");
 };
 
 // Shared memory per CTA: the dynamic buffers plus the static per-subset arrays (a bound).
-template <int ST, int W1, int TI>
+template <int ST, int W1, int TI, int DBC>
 constexpr size_t tile_total_smem() {
-  return TileShape<ST, W1, TI>::smem_bytes + (size_t)TI * kTJ * 40 + 1024;
+  return TileShape<ST, W1, TI, DBC>::smem_bytes + (size_t)TI * kTJ * 40 + 1024;
 }
 
 // Subset rows per tile: as many as fit 127 tile rows and the 227 KB of shared memory a CTA
 // may use.
-template <int ST, int W1>
+template <int ST, int W1, int DBC>
 struct TileFor {
   static constexpr int TI0 = (kRing - 1 - W1) / ST + 1;
-  static constexpr int TI = tile_total_smem<ST, W1, TI0>() <= 232448 ? TI0
-                            : tile_total_smem<ST, W1, TI0 - 1>() <= 232448 ? TI0 - 1
-                                                                          : TI0 - 2;
-  static_assert(tile_total_smem<ST, W1, TI>() <= 232448, "tile does not fit shared memory");
+  static constexpr int TI = tile_total_smem<ST, W1, TI0, DBC>() <= 232448 ? TI0
+                            : tile_total_smem<ST, W1, TI0 - 1, DBC>() <= 232448 ? TI0 - 1
+                                                                               : TI0 - 2;
+  static_assert(tile_total_smem<ST, W1, TI, DBC>() <= 232448, "tile does not fit shared memory");
 };
 
 struct TileScratch {
@@ -286,7 +287,7 @@ __global__ void ring_column_kernel(SearchArgs a, const SubsetPrm* __restrict__ p
 // Pass 1 for one tile row: row-band sums RB(x, j, t) = sum over the columns c of window j
 // of F(x, c) G(x + da, c + db0 + t), t = 0..7.  frow = F row x, grow = ring row of x + da
 // at column db0 (both 16-byte aligned), rbx = RB at (j = 0, t = 0) for row x.
-template <int ST, int W1, int FC, int FRP>
+template <int ST, int W1, int FC, int FRP, int DBC>
 __device__ __forceinline__ void row_band_sums(const float* __restrict__ frow, const float* __restrict__ grow,
                                               float* __restrict__ rbx) {
   constexpr int Q = W1 / ST, REM = W1 % ST, NB = (FC + ST - 1) / ST;
@@ -345,7 +346,7 @@ __device__ __forceinline__ void row_band_sums(const float* __restrict__ frow, co
             float s = Bk[j][t];
 #pragma unroll
             for (int b = 1; b < Q; ++b) s += Bk[j + b][t];
-            rbx[(j * kDBC + t) * FRP] = s + P[t];
+            rbx[(j * DBC + t) * FRP] = s + P[t];
           }
         }
       } else {
@@ -356,7 +357,7 @@ __device__ __forceinline__ void row_band_sums(const float* __restrict__ frow, co
             float s = Bk[j][t];
 #pragma unroll
             for (int b = 1; b < Q; ++b) s += Bk[j + b][t];
-            rbx[(j * kDBC + t) * FRP] = s;
+            rbx[(j * DBC + t) * FRP] = s;
           }
         }
       }
@@ -413,7 +414,7 @@ __device__ __forceinline__ void column_sums(const float* __restrict__ rb, float 
 // aligned g pairs; at an odd column, t = (1,2) .. (5,6) are aligned pairs and t = 0, 7
 // scalars.  Even and odd columns accumulate separately (E and O) and are added at the
 // block end; the first REM columns of a block (P) seed the remaining columns' sums.
-template <int ST, int W1, int FC, int FRP>
+template <int ST, int W1, int FC, int FRP, int DBC>
 __device__ __forceinline__ void row_band_sums_x2(const float* __restrict__ frow, const float* __restrict__ grow,
                                                  float* __restrict__ rbx) {
   static_assert(ST % 2 == 0, "blocks must start on even columns");
@@ -535,8 +536,8 @@ __device__ __forceinline__ void row_band_sums_x2(const float* __restrict__ frow,
 #pragma unroll
           for (int b = 2; b < Q; b += 2) s = fadd2(s, (b + 1 < Q) ? S2[j + b][i] : B[j + b][i]);
           if (REM > 0) s = fadd2(s, P[i]);
-          rbx[(j * kDBC + 2 * i) * FRP] = s.x;
-          rbx[(j * kDBC + 2 * i + 1) * FRP] = s.y;
+          rbx[(j * DBC + 2 * i) * FRP] = s.x;
+          rbx[(j * DBC + 2 * i + 1) * FRP] = s.y;
         }
       }
     }
@@ -601,18 +602,19 @@ __device__ __forceinline__ void column_sums_x2(const float* __restrict__ rb, flo
   }
 }
 
-template <int ST, int W1, int TI>
-__global__ void __launch_bounds__(kTileThreads, 1)
+template <int ST, int W1, int TI, int DBC>
+__global__ void __launch_bounds__(TileShape<ST, W1, TI, DBC>::NT, 1)
     ncc_tile_kernel(SearchArgs a, const float2* __restrict__ map, const double* __restrict__ Vmap,
                     const SubsetPrm* __restrict__ prm, const float2* __restrict__ ringv,
                     const float* __restrict__ cxv, const float* __restrict__ tcf, int* __restrict__ best) {
-  using S = TileShape<ST, W1, TI>;
+  using S = TileShape<ST, W1, TI, DBC>;
   constexpr int FR = S::FR, FC = S::FC, FCP = S::FCP, GCP = S::GCP, FRP = S::FRP, H0 = S::H0, NSUB = S::NSUB;
-  constexpr int GC = FC + kDBC - 1;  // g columns a chunk needs
+  constexpr int NT = S::NT;
+  constexpr int GC = FC + DBC - 1;  // g columns a chunk needs
   extern __shared__ __align__(16) float smf[];
   float* Ft = smf;                  // FR x FCP: f - cf, row-major
   float* Gt = Ft + FR * FCP;        // kRing x GCP: g, ring over rows, row-major
-  float* RB = Gt + kRing * GCP;     // (kTJ * kDBC) x FRP: one row per (window column, shift column)
+  float* RB = Gt + kRing * GCP;     // (kTJ * DBC) x FRP: one row per (window column, shift column)
   __shared__ float p_kf[NSUB], p_invden[NSUB], p_sqtolv[NSUB];
   __shared__ double p_tolv[NSUB];
   __shared__ int p_ok[NSUB];
@@ -651,7 +653,7 @@ __global__ void __launch_bounds__(kTileThreads, 1)
   }
   __syncthreads();
   const float cf = s_cf;
-  for (int q = tid; q < NSUB; q += kTileThreads) {
+  for (int q = tid; q < NSUB; q += NT) {
     const int i = i0 + q % TI, j = j0 + q / TI;
     int ok = 0;
     if (i < a.nx && j < a.ny) {
@@ -665,9 +667,9 @@ __global__ void __launch_bounds__(kTileThreads, 1)
     p_ok[q] = ok;
   }
   __syncthreads();
-  for (int q = tid; q < NSUB; q += kTileThreads) p_na[q] = p_ok[q] ? r_na[q % TI] : 0;
+  for (int q = tid; q < NSUB; q += NT) p_na[q] = p_ok[q] ? r_na[q % TI] : 0;
   // ---- f tile, centred ----
-  for (int idx = tid; idx < FR * FCP; idx += kTileThreads) {
+  for (int idx = tid; idx < FR * FCP; idx += NT) {
     const int x = idx / FCP, c = idx % FCP;
     float v = 0.f;
     if (c < FC && X0 + x < a.M && Y0 + c < a.N) v = __ldg(a.f + (size_t)(X0 + x) + (size_t)(Y0 + c) * a.M) - cf;
@@ -675,9 +677,9 @@ __global__ void __launch_bounds__(kTileThreads, 1)
   }
 
   // pass-2 roles and running first maxima
-  const int half = tid >> 7, jl = (tid >> 4) & (kTJ - 1), dl = tid & (kDBC - 1);
+  const int half = tid / (kTJ * DBC), jl = (tid / DBC) % kTJ, dl = tid % DBC;
   const int il0 = half ? H0 : 0, ns = half ? TI - H0 : H0;
-  const float* rbrow = RB + (jl * kDBC + dl) * FRP;
+  const float* rbrow = RB + (jl * DBC + dl) * FRP;
   float bv[H0];
   int bl[H0];
 #pragma unroll
@@ -686,18 +688,18 @@ __global__ void __launch_bounds__(kTileThreads, 1)
     bl[e] = 0x7fffffff;
   }
 
-  for (int dbc = 0; dbc < NDA; dbc += kDBC) {
+  for (int dbc = 0; dbc < NDA; dbc += DBC) {
     __syncthreads();
     // g buffer for this chunk: ring rows 0..FR-1 = tile rows DA0 + rel, columns from db = DA0 + dbc
     const int gy0 = Y0 + DA0 + dbc;
-    for (int idx = tid; idx < FR * GCP; idx += kTileThreads) {
+    for (int idx = tid; idx < FR * GCP; idx += NT) {
       const int rel = idx / GCP, col = idx % GCP;
       const int x = X0 + DA0 + rel, y = gy0 + col;
       float v = 0.f;
       if (col < GC && x >= 0 && x < a.M && y >= 0 && y < a.N) v = __ldg(a.g + (size_t)x + (size_t)y * a.M);
       Gt[idx] = v;
     }
-    for (int idx = FR * GCP + tid; idx < kRing * GCP; idx += kTileThreads) Gt[idx] = 0.f;
+    for (int idx = FR * GCP + tid; idx < kRing * GCP; idx += NT) Gt[idx] = 0.f;
     __syncthreads();
     // this thread's shift column for the chunk: crop column bb of its window column jl
     const int dbr = dbc + dl, db = DA0 + dbr;
@@ -743,10 +745,10 @@ __global__ void __launch_bounds__(kTileThreads, 1)
         const int grp = tid >> 7, x = tid & 127;
         if (x < FR) {
           if constexpr (ST % 2 == 0)
-            row_band_sums_x2<ST, W1, FC, FRP>(Ft + x * FCP, Gt + ((x + k) & (kRing - 1)) * GCP + grp * 8,
+            row_band_sums_x2<ST, W1, FC, FRP, DBC>(Ft + x * FCP, Gt + ((x + k) & (kRing - 1)) * GCP + grp * 8,
                                               RB + (grp * 8) * FRP + x);
           else
-            row_band_sums<ST, W1, FC, FRP>(Ft + x * FCP, Gt + ((x + k) & (kRing - 1)) * GCP + grp * 8,
+            row_band_sums<ST, W1, FC, FRP, DBC>(Ft + x * FCP, Gt + ((x + k) & (kRing - 1)) * GCP + grp * 8,
                                            RB + (grp * 8) * FRP + x);
         }
       }
@@ -839,22 +841,22 @@ __global__ void __launch_bounds__(kTileThreads, 1)
   }
   // ---- first maximum per subset over the 16 shift-column lanes ----
   float* rv = RB;
-  int* ri = reinterpret_cast<int*>(RB + NSUB * kDBC);
+  int* ri = reinterpret_cast<int*>(RB + NSUB * DBC);
 #pragma unroll
   for (int e = 0; e < H0; ++e) {
     if (e >= ns) break;
     const int q = (il0 + e) + jl * TI;
-    rv[q * kDBC + dl] = bv[e];
-    ri[q * kDBC + dl] = bl[e];
+    rv[q * DBC + dl] = bv[e];
+    ri[q * DBC + dl] = bl[e];
   }
   __syncthreads();
-  for (int q = tid; q < NSUB; q += kTileThreads) {
+  for (int q = tid; q < NSUB; q += NT) {
     if (!p_ok[q]) continue;
-    float b = rv[q * kDBC];
-    int bi = ri[q * kDBC];
-    for (int l = 1; l < kDBC; ++l) {
-      const float v = rv[q * kDBC + l];
-      const int li = ri[q * kDBC + l];
+    float b = rv[q * DBC];
+    int bi = ri[q * DBC];
+    for (int l = 1; l < DBC; ++l) {
+      const float v = rv[q * DBC + l];
+      const int li = ri[q * DBC + l];
       if (v > b || (v == b && li < bi)) {
         b = v;
         bi = li;
@@ -914,38 +916,39 @@ struct TileEntry {
   bool (*fits)();
 };
 
-template <int ST, int W1>
+template <int ST, int W1, int DBC>
 int launch_tile(const SearchArgs& a, const TileScratch& sc, cudaStream_t st) {
-  constexpr int TI = TileFor<ST, W1>::TI;
-  using S = TileShape<ST, W1, TI>;
-  auto kern = ncc_tile_kernel<ST, W1, TI>;
+  constexpr int TI = TileFor<ST, W1, DBC>::TI;
+  using S = TileShape<ST, W1, TI, DBC>;
+  auto kern = ncc_tile_kernel<ST, W1, TI, DBC>;
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::smem_bytes) != cudaSuccess)
     return -1;
   const long long tiles = (long long)((a.nx + TI - 1) / TI) * ((a.ny + kTJ - 1) / kTJ);
-  kern<<<(unsigned)tiles, kTileThreads, S::smem_bytes, st>>>(a, sc.map, sc.V, sc.prm, sc.ringv, sc.cx, sc.cf, sc.best);
+  kern<<<(unsigned)tiles, S::NT, S::smem_bytes, st>>>(a, sc.map, sc.V, sc.prm, sc.ringv, sc.cx, sc.cf, sc.best);
   return 0;
 }
 
 // Whether the tile kernel's shared memory (static + dynamic) fits this device.
-template <int ST, int W1>
+template <int ST, int W1, int DBC>
 bool tile_fits() {
-  constexpr int TI = TileFor<ST, W1>::TI;
+  constexpr int TI = TileFor<ST, W1, DBC>::TI;
   cudaFuncAttributes fa;
   int dev = 0, optin = 0;
-  return cudaFuncGetAttributes(&fa, ncc_tile_kernel<ST, W1, TI>) == cudaSuccess && cudaGetDevice(&dev) == cudaSuccess &&
+  return cudaFuncGetAttributes(&fa, ncc_tile_kernel<ST, W1, TI, DBC>) == cudaSuccess &&
+         cudaGetDevice(&dev) == cudaSuccess &&
          cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) == cudaSuccess &&
-         fa.sharedSizeBytes + TileShape<ST, W1, TI>::smem_bytes <= (size_t)optin;
+         fa.sharedSizeBytes + TileShape<ST, W1, TI, DBC>::smem_bytes <= (size_t)optin;
 }
 
-template <int ST, int W1>
+template <int ST, int W1, int DBC = 16>
 TileEntry entry() {
-  return TileEntry{TileFor<ST, W1>::TI, launch_tile<ST, W1>, tile_fits<ST, W1>};
+  return TileEntry{TileFor<ST, W1, DBC>::TI, launch_tile<ST, W1, DBC>, tile_fits<ST, W1, DBC>};
 }
 
 // The step / window pairs with a tile kernel (others use the per-subset kernel).
 bool tile_entry(int step, int W1, TileEntry* e) {
   switch (step * 1000 + W1) {
-    case 10 * 1000 + 41: *e = entry<10, 41>(); return true;
+    case 10 * 1000 + 41: *e = entry<10, 41, 24>(); return true;
     case 16 * 1000 + 31: *e = entry<16, 31>(); return true;
     case 16 * 1000 + 33: *e = entry<16, 33>(); return true;
     case 12 * 1000 + 21: *e = entry<12, 21>(); return true;
