@@ -71,7 +71,12 @@ __device__ __forceinline__ float stencil16_clamped(const float* __restrict__ img
 // Packed FP32 pairs (sm_100 .f32x2 instructions): one instruction, two lanes of IEEE
 // round-to-nearest results, each identical to the scalar operation.
 // ---------------------------------------------------------------------------------
-__device__ __forceinline__ float2 ffma2(float2 a, float2 b, float2 c) {
+// The host forms (same IEEE results lane by lane) serve host-side checks of the
+// functions built on them.
+__host__ __device__ __forceinline__ float2 ffma2(float2 a, float2 b, float2 c) {
+#ifndef __CUDA_ARCH__
+  return make_float2(fmaf(a.x, b.x, c.x), fmaf(a.y, b.y, c.y));
+#else
   float2 d;
   asm("{\n\t.reg .b64 ra, rb, rc, rd;\n\t"
       "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\tmov.b64 rc, {%6, %7};\n\t"
@@ -79,9 +84,13 @@ __device__ __forceinline__ float2 ffma2(float2 a, float2 b, float2 c) {
       : "=f"(d.x), "=f"(d.y)
       : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
   return d;
+#endif
 }
 
-__device__ __forceinline__ float2 fmul2(float2 a, float2 b) {
+__host__ __device__ __forceinline__ float2 fmul2(float2 a, float2 b) {
+#ifndef __CUDA_ARCH__
+  return make_float2(a.x * b.x, a.y * b.y);
+#else
   float2 d;
   asm("{\n\t.reg .b64 ra, rb, rd;\n\t"
       "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
@@ -89,9 +98,13 @@ __device__ __forceinline__ float2 fmul2(float2 a, float2 b) {
       : "=f"(d.x), "=f"(d.y)
       : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
   return d;
+#endif
 }
 
-__device__ __forceinline__ float2 fadd2(float2 a, float2 b) {
+__host__ __device__ __forceinline__ float2 fadd2(float2 a, float2 b) {
+#ifndef __CUDA_ARCH__
+  return make_float2(a.x + b.x, a.y + b.y);
+#else
   float2 d;
   asm("{\n\t.reg .b64 ra, rb, rd;\n\t"
       "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
@@ -99,6 +112,7 @@ __device__ __forceinline__ float2 fadd2(float2 a, float2 b) {
       : "=f"(d.x), "=f"(d.y)
       : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
   return d;
+#endif
 }
 
 // Two stencils at once with packed FP32 pairs (.x: point a, .y: point b); each lane's

@@ -104,6 +104,6 @@ struct CamPair {
 };
 int launch_triangulate(long long n, const double* pairs, const CamPair& cams, double* xyz, double* err,
                        cudaStream_t st);
-int launch_fp32_probe(int blocks, int threads, int iters, float* out, cudaStream_t st);
+int launch_fp32_probe(int blocks, int threads, int iters, float* out, bool packed, cudaStream_t st);
 
 }  // namespace aldic

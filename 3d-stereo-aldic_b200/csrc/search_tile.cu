@@ -415,7 +415,7 @@ __device__ __forceinline__ void column_sums(const float* __restrict__ rb, float 
 // scalars.  Even and odd columns accumulate separately (E and O) and are added at the
 // block end; the first REM columns of a block (P) seed the remaining columns' sums.
 template <int ST, int W1, int FC, int FRP, int DBC>
-__device__ __forceinline__ void row_band_sums_x2(const float* __restrict__ frow, const float* __restrict__ grow,
+__host__ __device__ __forceinline__ void row_band_sums_x2(const float* __restrict__ frow, const float* __restrict__ grow,
                                                  float* __restrict__ rbx) {
   static_assert(ST % 2 == 0, "blocks must start on even columns");
   constexpr int Q = W1 / ST, REM = W1 % ST, NB = (FC + ST - 1) / ST;
@@ -708,7 +708,6 @@ __global__ void __launch_bounds__(TileShape<ST, W1, TI, DBC>::NT, 1)
     const bool rbg = bb == 0 || bb == nbv - 1;
     const long long mcol = (long long)(X0 + DA0) * NW + (Y0 + jl * ST + db);  // map index of (il = 0, k = 0)
     for (int k = 0; k < NDA; ++k) {
-      const int da = DA0 + k;
       // ---- epilogue operands of this shift, fetched before pass 1 hides their latency ----
       int st[H0];
       float2 pf[H0];

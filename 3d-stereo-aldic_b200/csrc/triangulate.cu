@@ -124,8 +124,31 @@ __global__ void fp32_probe_kernel(int iters, float seed, float* out) {
   if (s == 123.456f) out[0] = s;  // keep the chains live
 }
 
-int launch_fp32_probe(int blocks, int threads, int iters, float* out, cudaStream_t st) {
-  fp32_probe_kernel<<<blocks, threads, 0, st>>>(iters, 0.5f, out);
+// The same loop on packed pairs (fma.rn.f32x2): 8 independent float2 chains.
+__global__ void fp32x2_probe_kernel(int iters, float seed, float* out) {
+  float2 a[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) a[i] = make_float2(seed + threadIdx.x + 2 * i, seed + threadIdx.x + 2 * i + 1);
+  const float2 m = make_float2(0.9999f, 0.9999f), c = make_float2(1e-4f, 1e-4f);
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+#pragma unroll
+      for (int j = 0; j < 8; ++j) a[j] = ffma2(a[j], m, c);
+    }
+  }
+  float s = 0.f;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) s += a[i].x + a[i].y;
+  if (s == 123.456f) out[0] = s;  // keep the chains live
+}
+
+// FMAs per thread per iteration: 128 in both forms.
+int launch_fp32_probe(int blocks, int threads, int iters, float* out, bool packed, cudaStream_t st) {
+  if (packed)
+    fp32x2_probe_kernel<<<blocks, threads, 0, st>>>(iters, 0.5f, out);
+  else
+    fp32_probe_kernel<<<blocks, threads, 0, st>>>(iters, 0.5f, out);
   return 1;
 }
 

@@ -566,8 +566,8 @@ def main():
             "roofline": {"bound": "fp32", "kernel": "ncc_tile_kernel (stereo integer search, shared products)",
                          "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
                          "frac": achieved / fp32_peak if fp32_peak else None, "traffic": None,
-                         "peak_source": "measured FP32 FMA loop on this GPU (MEASURED_PEAKS.json holds only HBM "
-                                        "and bf16 tensor peaks)",
+                         "peak_source": "measured on this GPU: the faster of a scalar FFMA and a packed FFMA2 "
+                                        "loop (MEASURED_PEAKS.json holds only HBM and bf16 tensor peaks)",
                          "algorithmic_flops_per_launch": flops, "flops_counted": "products only (2 per f*g)",
                          "direct_correlation_flops": direct_flops, "launch_ms": search_ms,
                          "launches_timed": prof_n},

@@ -159,8 +159,9 @@ int aldic_local_icgn_noalloc(int variant, const float* ref, const float* def, co
                              uint8_t* markHole, void* stream);
 
 /* ------------------------------------------------------------- diagnostics ------- */
-/* Measured FP32 FMA throughput of the current device (TFLOP/s), the denominator the
- * library's compute-bound kernels are reported against.  Not part of the reference. */
+/* Measured FP32 FMA throughput of the current device (TFLOP/s): the faster of a scalar
+ * FFMA loop and a packed FFMA2 (fma.rn.f32x2) loop, the denominator the library's
+ * compute-bound kernels are reported against.  Not part of the reference. */
 int aldic_measure_fp32_peak(aldic_ctx* ctx, double* tflops);
 /* Iterations the one-warp-per-subset solver pass of aldic_local_icgn / aldic_subpb1 spends
  * on a subset before a 4-warp pass restarts it from its initial guess (default 16, 1..1000).
