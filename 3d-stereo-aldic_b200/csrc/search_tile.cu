@@ -288,7 +288,7 @@ __global__ void ring_column_kernel(SearchArgs a, const SubsetPrm* __restrict__ p
 // of F(x, c) G(x + da, c + db0 + t), t = 0..7.  frow = F row x, grow = ring row of x + da
 // at column db0 (both 16-byte aligned), rbx = RB at (j = 0, t = 0) for row x.
 template <int ST, int W1, int FC, int FRP, int DBC>
-__device__ __forceinline__ void row_band_sums(const float* __restrict__ frow, const float* __restrict__ grow,
+__host__ __device__ __forceinline__ void row_band_sums(const float* __restrict__ frow, const float* __restrict__ grow,
                                               float* __restrict__ rbx) {
   constexpr int Q = W1 / ST, REM = W1 % ST, NB = (FC + ST - 1) / ST;
   constexpr int NGG = (FC + 7 + 3) / 4;  // 4-column groups of g covering columns 0 .. FC+6
@@ -368,7 +368,7 @@ __device__ __forceinline__ void row_band_sums(const float* __restrict__ frow, co
 // Pass 2 walk: window sums N[e] of NS consecutive window rows starting at tile row R0, from
 // one RB row (rb = RB + (j, d) row, 16-byte aligned) by block sums over rows.
 template <int ST, int W1, int NS, int R0>
-__device__ __forceinline__ void column_sums(const float* __restrict__ rb, float (&N)[NS]) {
+__host__ __device__ __forceinline__ void column_sums(const float* __restrict__ rb, float (&N)[NS]) {
   constexpr int Q = W1 / ST, REM = W1 % ST;
   constexpr int NBV = NS - 1 + Q + (REM > 0 ? 1 : 0);
   constexpr int ROWS = (NS - 1) * ST + W1;
@@ -546,7 +546,7 @@ __host__ __device__ __forceinline__ void row_band_sums_x2(const float* __restric
 
 // Pass 2 with packed pairs of rows (even steps; R0 even): window sums as column_sums.
 template <int ST, int W1, int NS, int R0>
-__device__ __forceinline__ void column_sums_x2(const float* __restrict__ rb, float (&N)[NS]) {
+__host__ __device__ __forceinline__ void column_sums_x2(const float* __restrict__ rb, float (&N)[NS]) {
   static_assert(ST % 2 == 0 && R0 % 2 == 0, "row pairs must align with blocks");
   constexpr int Q = W1 / ST, REM = W1 % ST;
   constexpr int NBV = NS - 1 + Q + (REM > 0 ? 1 : 0);
