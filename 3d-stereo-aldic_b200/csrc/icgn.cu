@@ -604,6 +604,7 @@ __global__ void __launch_bounds__(kNT) icgn_solve_kernel(IcgnArgs a, int bucket)
 // masked deformed image) needs the g-region flood fill: it is handed to the general kernel
 // through queue 1 and restarted there.
 constexpr int kWT = 256;  // threads per CTA: 8 / NW subset groups
+constexpr int kSlowNW = 4;  // warps per subset in the pass that restarts the slow subsets
 
 template <int NW>
 __device__ __forceinline__ void group_bar(int id) {
@@ -1624,11 +1625,11 @@ int launch_icgn(const IcgnArgs& a, int wmax_enlarged, cudaStream_t st) {
     if (grid > need) grid = need;
     icgn_group_kernel<1, false><<<(unsigned)grid, kWT, 0, st>>>(a);
     per_sm = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, icgn_group_kernel<4, true>, kWT, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, icgn_group_kernel<kSlowNW, true>, kWT, 0);
     grid = (long long)sms * (per_sm < 1 ? 1 : per_sm);
-    const long long need4 = (a.n + 1) / 2;
-    if (grid > need4) grid = need4;
-    icgn_group_kernel<4, true><<<(unsigned)grid, kWT, 0, st>>>(a);
+    const long long need_slow = (a.n + kWT / (32 * kSlowNW) - 1) / (kWT / (32 * kSlowNW));
+    if (grid > need_slow) grid = need_slow;
+    icgn_group_kernel<kSlowNW, true><<<(unsigned)grid, kWT, 0, st>>>(a);
     launches += 2;
   }
   {  // enlarged / masked subsets, and those handed over by the fast kernel

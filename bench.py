@@ -256,12 +256,19 @@ class StereoPipeline:
 
     def _temporal_right(self, stereo_done):
         # temporal right R0 -> R1 on the stereo-matched mesh (coords + U_stereo)
+        self._right_search()
+        self.torch.cuda.current_stream().wait_event(stereo_done)
+        self._right_icgn()
+
+    def _right_search(self):
+        P, cR = self.P, self.ctx["R"]
+        self._load_pair(cR, "R0", "R1")
+        cR.integer_search([P["s_temp"]] * 2, self.gx, self.gy, P["w"], P["step"], out=self.buf["R"])
+
+    def _right_icgn(self):
         T, P = self.torch, self.P
         w, st = P["w"], P["step"]
         cR, bR, bS = self.ctx["R"], self.buf["R"], self.buf["S"]
-        self._load_pair(cR, "R0", "R1")
-        cR.integer_search([P["s_temp"]] * 2, self.gx, self.gy, w, st, out=bR)
-        T.cuda.current_stream().wait_event(stereo_done)
         n = self.n
         US = bS["U"].view(n, 2)
         cxy = self.coords.t()
