@@ -208,6 +208,53 @@ __device__ __forceinline__ void peak_partials(const SearchArgs& a, const SubsetG
   }
 }
 
+// Warp form of the interior case of peak_partials: the same nine sums, with lane = template
+// row.  A lane walks its row along the columns, keeping the taps of the 3 x 3 shift block in
+// a sliding window, so each step loads (and widens to FP64) one template value and the
+// three g values of the newest column instead of ten values per pixel; consecutive lanes
+// read consecutive rows (coalesced).  Rows beyond the first 32 are split into column
+// parts over the lanes.
+__device__ __forceinline__ void peak_partials_warp_interior(const SearchArgs& a, const SubsetGeom& s, int pa, int pb,
+                                                            double tm, int lane, double (&v)[9]) {
+  const int W1 = a.winsize + 1;
+  const size_t M = (size_t)a.M;
+#pragma unroll
+  for (int k = 0; k < 9; ++k) v[k] = 0.0;
+  const float* fb = a.f + (s.ii - 1) + (size_t)(s.jj - 1) * M;
+  const float* gb = a.g + (s.dr0 - 2 + pa) + (size_t)(s.dc0 - 2 + pb) * M;
+  for (int r0 = 0; r0 < W1; r0 += 32) {
+    const int nr = min(32, W1 - r0), parts = 32 / nr;
+    if (lane >= parts * nr) continue;
+    const int i = r0 + lane % nr, part = lane / nr;
+    const int c0 = part * W1 / parts, c1 = (part + 1) * W1 / parts;
+    const float* fr = fb + i;
+    const float* gr = gb + i;
+    double t0[3], t1[3];
+#pragma unroll
+    for (int rb = 0; rb < 3; ++rb) {
+      t0[rb] = (double)gr[rb + (size_t)c0 * M];
+      t1[rb] = (double)gr[rb + (size_t)(c0 + 1) * M];
+    }
+    // unrolled so that several columns' loads are in flight at once (each new column is a
+    // fresh cache line for every lane)
+#pragma unroll 6
+    for (int j = c0; j < c1; ++j) {
+      double t2[3];
+#pragma unroll
+      for (int rb = 0; rb < 3; ++rb) t2[rb] = (double)gr[rb + (size_t)(j + 2) * M];
+      const double tv = (double)fr[(size_t)j * M] - tm;
+#pragma unroll
+      for (int rb = 0; rb < 3; ++rb) {
+        v[rb] += tv * t0[rb];
+        v[rb + 3] += tv * t1[rb];
+        v[rb + 6] += tv * t2[rb];
+        t0[rb] = t1[rb];
+        t1[rb] = t2[rb];
+      }
+    }
+  }
+}
+
 // Block version: every thread of the block calls it; thread 0 writes u, v, phi.
 __device__ inline void refit_peak(const SearchArgs& a, const SubsetGeom& s, long long o, int pa, int pb, double tm,
                                   double denT, double tolz, double* red, double* sums) {
@@ -230,7 +277,10 @@ __device__ inline void refit_peak_warp(const SearchArgs& a, const SubsetGeom& s,
                                        double tm, double denT, double tolz) {
   const int lane = threadIdx.x & 31;
   double v[9];
-  peak_partials(a, s, pa, pb, tm, lane, 32, v);
+  if (pa >= 2 && pa <= s.na - 3 && pb >= 2 && pb <= s.nb - 3)
+    peak_partials_warp_interior(a, s, pa, pb, tm, lane, v);
+  else
+    peak_partials(a, s, pa, pb, tm, lane, 32, v);
 #pragma unroll
   for (int k = 0; k < 9; ++k) v[k] = warp_sum(v[k]);
   double mine = 0.0;

@@ -32,6 +32,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "3d-stereo-aldic_b200"))
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
+# DRAM bytes (read + write) of one launch of the stereo search's correlation kernel, from an
+# ncu capture of that launch (dram__bytes_read.sum + dram__bytes_write.sum, mean of four
+# launches).  They are the inputs read about once each (frames, window map, ring tables).
+TILE_TRAFFIC = {"stereo2048": 299_537_408, "stereo1024": 44_464_384}
+
 METRIC = "converged IC-GN subsets/s at <=0.01 px vs FP64 oracle (FFT-search init), 1 B200"
 UNIT = "subsets/s"
 
@@ -440,7 +445,7 @@ def run_reference(args, P):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="stereo2048",
@@ -572,7 +577,10 @@ def main():
             "gpu_launches": int(launches),
             "roofline": {"bound": "fp32", "kernel": "ncc_tile_kernel (stereo integer search, shared products)",
                          "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
-                         "frac": achieved / fp32_peak if fp32_peak else None, "traffic": None,
+                         "frac": achieved / fp32_peak if fp32_peak else None,
+                         "traffic": TILE_TRAFFIC.get(args.workload), "traffic_unit": "bytes per launch",
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of this kernel "
+                                           "at this workload (separate capture)",
                          "peak_source": "measured on this GPU: the faster of a scalar FFMA and a packed FFMA2 "
                                         "loop (MEASURED_PEAKS.json holds only HBM and bf16 tensor peaks)",
                          "algorithmic_flops_per_launch": flops, "flops_counted": "products only (2 per f*g)",
