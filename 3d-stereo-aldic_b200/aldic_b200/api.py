@@ -153,7 +153,7 @@ class Context:
 
     def set_iteration_cap(self, cap):
         """Iterations the one-warp solver pass spends on a subset before the 4-warp pass
-        restarts it (default 16)."""
+        restarts it (default 8)."""
         self._check(self.lib.aldic_set_iteration_cap(self.h, int(cap)), "aldic_set_iteration_cap")
 
     def set_profiling(self, on=True):

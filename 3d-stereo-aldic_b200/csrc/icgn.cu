@@ -595,8 +595,8 @@ __global__ void __launch_bounds__(kNT) icgn_solve_kernel(IcgnArgs a, int bucket)
 // Gauss-Newton Hessian; a zero pivot propagates Inf/NaN as the reference's singular solve
 // does).
 //
-// The main pass (NW = 1, queue 0) gives each subset at most warp_cap iterations (16 by
-// default): the
+// The main pass (NW = 1, queue 0) gives each subset at most warp_cap iterations (8 by
+// default; 6-12 measured within 1 % of each other on the stereo pass, 4 and 24 slower): the
 // few subsets that need more (most never converge and run to max_iter) would otherwise
 // keep single warps running long after the rest of the grid.  They go to queue 1 flagged
 // kSlowSubset and restart from the beginning in the 4-warp pass (NW = 4), which runs each

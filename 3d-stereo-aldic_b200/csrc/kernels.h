@@ -96,7 +96,7 @@ size_t search_tot_bytes(int M, int N);
 int launch_search(const SearchArgs& a, cudaStream_t st);
 // Shared-product search (search_tile.cu): scratch size (0 when the step / window pair has
 // no tile kernel), and the launcher (returns the launch count, or -1 when not available).
-constexpr int kDefaultWarpCap = 16;  // default IcgnArgs / Sub1Args warp_cap
+constexpr int kDefaultWarpCap = 8;   // default IcgnArgs / Sub1Args warp_cap
 size_t search_tile_bytes(int M, int N, int winsize, int step, int nx, int ny, int s0, int s1);
 int launch_search_tile(const SearchArgs& a, cudaStream_t st);
 struct CamPair {

@@ -85,6 +85,10 @@ def test_package_exports_the_names_callers_use():
     assert (A.UNIFORM, A.QUADTREE) == (0, 1)
     for name in ("Context", "AldicError", "load_library", "LocalICGNQuadtree", "funIntegerSearch", "synth"):
         assert hasattr(A, name), name
+    # the Python copy of the library's default iteration cap matches the C constant
+    src = open(os.path.join(ROOT, "3d-stereo-aldic_b200", "csrc", "kernels.h")).read()
+    cap = int(re.search(r"constexpr int kDefaultWarpCap = (\d+);", src).group(1))
+    assert A.DEFAULT_ITERATION_CAP == cap
 
 
 def test_output_arrays_are_written_in_place_or_refused():

@@ -261,7 +261,7 @@ def test_subpb1_quadtree_parity(ctx, hole):
     assert np.all(np.isnan(res["U"].reshape(-1, 2)[err]))
 
 
-def test_subpb1_quadtree_mixed_windows_and_slow_subsets(ctx, hole):
+def test_subpb1_quadtree_mixed_windows_and_slow_subsets(A, ctx, hole):
     # per-subset windows 16 / 24 / 32 (queue 0 holds only the nominal size; the others are
     # unmasked queue-1 subsets solved by the warp-group passes); with an iteration cap of 1
     # every subset needing more than one iteration restarts in the 4-warp pass
@@ -297,10 +297,10 @@ def test_subpb1_quadtree_mixed_windows_and_slow_subsets(ctx, hole):
             assert np.abs(res["U"] - ref["U"]).reshape(-1, 2)[both].max() < UV_TOL, cap
             assert np.array_equal(np.isnan(res["U"]), np.isnan(ref["U"])), cap
     finally:
-        ctx.set_iteration_cap(16)
+        ctx.set_iteration_cap(A.DEFAULT_ITERATION_CAP)
 
 
-def test_local_icgn_slow_subsets_restart(ctx, affine):
+def test_local_icgn_slow_subsets_restart(A, ctx, affine):
     # with an iteration cap of 1 every subset that needs a second iteration is restarted by
     # the 4-warp pass; codes and displacements still match the oracle
     _load_raw(ctx, affine)
@@ -316,7 +316,7 @@ def test_local_icgn_slow_subsets_restart(ctx, affine):
         ctx.set_iteration_cap(1)
         res = ctx.local_icgn(0, coords, U0, 30, 1e-3)
     finally:
-        ctx.set_iteration_cap(16)
+        ctx.set_iteration_cap(A.DEFAULT_ITERATION_CAP)
     assert np.mean(res["conv"] == ref["conv"]) >= 0.98
     assert np.mean(_flag(res["conv"]) == _flag(ref["conv"])) >= FLAG_RATE
     both = _flag(res["conv"]) & _flag(ref["conv"])
