@@ -1,0 +1,123 @@
+"""Seeded synthetic stereo frame sequences rendered on the GPU (torch).
+
+The same analytic rendering as ``synth.render`` -- every speckle a Gaussian in material
+(frame-0 plane) coordinates, splatted over a square window around its projected centre, each
+pixel evaluated at its own material coordinates -- for image sizes and frame counts that a
+numpy rendering would take minutes over.  Used only to make benchmark inputs.
+
+``stereo_sequence``: the stereo rig of ``synth.stereo_pair`` (pinhole cameras, f px,
+principal point at the image centre, baseline along world x, optical axes aimed at the plane
+centre) looking at a speckled plane z = Z that is stretched progressively over the sequence
+(uniaxial in x up to ``stretch`` at the last frame, lateral contraction ``poisson`` times
+that in y) with a growing local out-of-plane bulge.  Frames are M x N uint16 images in the
+library's layout (dim 1 = image x fastest), returned as flat CUDA tensors.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import synth
+
+
+@dataclass
+class SequenceScene:
+    L: list            # per frame: flat uint16 CUDA tensor, M * N, x fastest
+    R: list
+    M: int
+    N: int
+    camL: synth.Camera
+    camR: synth.Camera
+    KL: np.ndarray     # 1-based pixel convention of the matched pairs
+    KR: np.ndarray
+    R_rl: np.ndarray
+    T_rl: np.ndarray
+    Z: float
+    params: dict
+
+    def material_to_world(self, X, Y, k):
+        """World position (mm) of material point (X, Y) of the frame-0 plane at frame k (numpy)."""
+        p = self.params
+        s = p["stretch"] * k / max(p["frames"] - 1, 1)
+        b = p["bulge"] * k / max(p["frames"] - 1, 1)
+        w = b * np.exp(-((X - p["bulge_x"]) ** 2 + (Y - p["bulge_y"]) ** 2) / p["bulge_sigma"] ** 2)
+        return np.stack([(1 + s) * X, (1 - p["poisson"] * s) * Y, self.Z + w], axis=-1)
+
+
+def stereo_sequence(frames=50, M=4096, N=3000, seed=4, f=4000.0, baseline=300.0, Z=1000.0, plane_half=(640.0, 480.0),
+                    density_px=0.0153, noise=2.0, amp=(60.0, 200.0), gain=200.0, stretch=0.08, poisson=0.3,
+                    bulge=3.0, bulge_x=60.0, bulge_y=-40.0, bulge_sigma=80.0, device="cuda") -> SequenceScene:
+    import torch
+
+    dev = torch.device(device)
+    rng = np.random.default_rng(seed)
+    yaw = math.degrees(math.atan(baseline / 2.0 / Z))
+    K = np.array([[f, 0, (M + 1) / 2.0 - 1.0], [0, f, (N + 1) / 2.0 - 1.0], [0, 0, 1.0]])
+    camL = synth.Camera(K=K, R=synth._rot_y(-yaw), C=np.array([-baseline / 2, 0.0, 0.0]))
+    camR = synth.Camera(K=K, R=synth._rot_y(+yaw), C=np.array([+baseline / 2, 0.0, 0.0]))
+    mm_per_px = Z / f
+    hx, hy = plane_half
+    n_sp = int(round(density_px * (2 * hx) * (2 * hy) / mm_per_px ** 2))
+    sp = synth.make_speckles(rng, n_sp, -hx, hx, -hy, hy, 2.0 * mm_per_px, 4.0 * mm_per_px, amp[0], amp[1])
+    params = dict(frames=frames, stretch=stretch, poisson=poisson, bulge=bulge, bulge_x=bulge_x, bulge_y=bulge_y,
+                  bulge_sigma=bulge_sigma)
+    f64 = dict(dtype=torch.float64, device=dev)
+    cx, cy = torch.tensor(sp.cx, **f64), torch.tensor(sp.cy, **f64)
+    ir2 = torch.tensor(1.0 / sp.r ** 2, **f64)
+    aa = torch.tensor(sp.a * gain, **f64)
+    # pixel grid, x fastest (the library's column-major M x N layout)
+    Yg, Xg = torch.meshgrid(torch.arange(1, N + 1, **f64), torch.arange(1, M + 1, **f64), indexing="ij")
+    Xg, Yg = Xg.reshape(-1), Yg.reshape(-1)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(seed)
+
+    def deform(X, Y, k):
+        s = stretch * k / max(frames - 1, 1)
+        b = bulge * k / max(frames - 1, 1)
+        w = b * torch.exp(-((X - bulge_x) ** 2 + (Y - bulge_y) ** 2) / bulge_sigma ** 2)
+        return (1 + s) * X, (1 - poisson * s) * Y, Z + w, s, b
+
+    def frame_img(cam, k):
+        Kt, Rt, Ct = torch.tensor(cam.K, **f64), torch.tensor(cam.R, **f64), torch.tensor(cam.C, **f64)
+        # speckle centres at frame k, projected (1-based pixel coordinates)
+        Px, Py, Pz, s, b = deform(cx, cy, k)
+        Xc = (torch.stack([Px, Py, Pz], 1) - Ct) @ Rt.T
+        p = Xc @ Kt.T
+        px, py = p[:, 0] / p[:, 2] + 1.0, p[:, 1] / p[:, 2] + 1.0
+        # material coordinates of every pixel: ray / deformed-surface intersection by fixed point
+        d = torch.stack([Xg - 1.0, Yg - 1.0, torch.ones_like(Xg)], 1) @ torch.linalg.inv(Kt).T @ Rt
+        qx = torch.zeros_like(Xg)
+        qy = torch.zeros_like(Xg)
+        zt = torch.full_like(Xg, Z)
+        for _ in range(8):
+            t = (zt - Ct[2]) / d[:, 2]
+            qx = (Ct[0] + t * d[:, 0]) / (1 + s)
+            qy = (Ct[1] + t * d[:, 1]) / (1 - poisson * s)
+            zt = Z + b * torch.exp(-((qx - bulge_x) ** 2 + (qy - bulge_y) ** 2) / bulge_sigma ** 2)
+        del d
+        img = torch.zeros(M * N, **f64)
+        ipx, ipy = torch.round(px).long(), torch.round(py).long()
+        keep = (ipx > -12) & (ipx <= M + 12) & (ipy > -12) & (ipy <= N + 12)
+        ipx, ipy, kcx, kcy, kir2, ka = ipx[keep], ipy[keep], cx[keep], cy[keep], ir2[keep], aa[keep]
+        offs = torch.arange(-12, 13, device=dev)
+        Xp = ipx[:, None] + offs[None, :]            # all 25 window columns at once
+        okx = (Xp >= 1) & (Xp <= M)
+        for dy in range(-12, 13):
+            Yp = ipy + dy
+            ok = okx & ((Yp >= 1) & (Yp <= N))[:, None]
+            lin = ((Xp - 1) + ((Yp - 1) * M)[:, None])[ok]
+            sel = ok.nonzero()[:, 0]
+            d2 = (qx[lin] - kcx[sel]) ** 2 + (qy[lin] - kcy[sel]) ** 2
+            img.index_add_(0, lin, ka[sel] * torch.exp(-d2 * kir2[sel]))
+        img += torch.randn(M * N, generator=gen, **f64) * (noise * gain)
+        return torch.clamp(torch.round(img), 0, 65535).to(torch.int32).to(torch.uint16)
+
+    Ls = [frame_img(camL, k) for k in range(frames)]
+    Rs = [frame_img(camR, k) for k in range(frames)]
+    R_rl = camR.R @ camL.R.T
+    T_rl = -camR.R @ camR.C + R_rl @ (camL.R @ camL.C)
+    K1 = np.array([[f, 0, (M + 1) / 2.0], [0, f, (N + 1) / 2.0], [0, 0, 1.0]])
+    return SequenceScene(L=Ls, R=Rs, M=M, N=N, camL=camL, camR=camR, KL=K1, KR=K1, R_rl=R_rl, T_rl=T_rl, Z=Z,
+                         params=params)

@@ -53,6 +53,9 @@ def workload_params(name):
         return dict(size=1024, w=40, step=10, s_stereo=35, s_temp=10, tol_stereo=1e-3, tol_temp=1e-2)
     if name == "temporal512":
         return dict(size=512, w=30, step=16, s_temp=10, tol_temp=1e-3)
+    if name == "sequence4096":  # 50 stereo frame pairs, 4096 x 3000 (x by y) uint16
+        return dict(M=4096, N=3000, frames=50, w=40, step=10, s_stereo=(275, 375), s_temp=10, tol_stereo=1e-3,
+                    tol_temp=1e-2, sample=64)
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -449,9 +452,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="stereo2048",
-                    choices=["stereo2048", "stereo1024", "temporal512", "quadtree2048"],
+                    choices=["stereo2048", "stereo1024", "temporal512", "quadtree2048", "sequence4096"],
                     help="stereo2048: the headline stereo + temporal + triangulation step; temporal512 and "
-                         "quadtree2048: the 2D and quadtree/Subpb1 configurations (separate JSON lines)")
+                         "quadtree2048: the 2D and quadtree/Subpb1 configurations; sequence4096: the 50-frame "
+                         "4096 x 3000 stereo sequence with per-frame latency (separate JSON lines)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--ref-per-pass", type=int, default=200)
@@ -467,7 +471,15 @@ def main():
 
     if args.impl == "reference":
         if rank == 0:
-            run_reference(args, P)
+            if args.workload == "sequence4096":
+                print(json.dumps({"impl": "reference", "unavailable": "sequence4096 times the FP64 CPU oracle on "
+                                  "its own per-frame sample (cpu_baseline of the ours line)"}), flush=True)
+            else:
+                run_reference(args, P)
+        return
+    if args.workload == "sequence4096":
+        if rank == 0:
+            run_sequence(args, P)
         return
     if args.workload in ("temporal512", "quadtree2048"):
         if rank == 0:
@@ -800,6 +812,236 @@ def run_aux(args, P):
     print(json.dumps(line), flush=True)
     ctx.close()
 
+
+def run_sequence(args, P):
+    """sequence4096 (without the learned initial guess): 50 stereo frame
+    pairs at 4096 x 3000 uint16 with the stereo rig of config 1 aimed at a plane stretched
+    progressively (8 % in x at the last frame) with a growing local bulge, rendered on the GPU.
+    Frame 0: stereo L0 -> R0 whole-field search + IC-GN (set-up, timed separately).  Frames
+    1..49, each timed alone: temporal L0 -> Lk and R0 -> Rk IC-GN on the left mesh and the
+    stereo-matched right mesh, from the previous frames' results (frame 1: whole-field
+    search), and FP64 triangulation.  Every frame is checked on the FP64 oracle (a sample
+    of subsets per camera from the device's own initial guesses) and against the rendering's
+    ground truth."""
+    import torch
+
+    import aldic_b200 as A
+    from aldic_b200 import synth, synth_gpu
+
+    T = torch
+    dev = T.device("cuda:0")
+    T.cuda.set_device(dev)
+    f64 = dict(dtype=T.float64, device=dev)
+    t0 = time.perf_counter()
+    sc = synth_gpu.stereo_sequence(frames=P["frames"], M=P["M"], N=P["N"], seed=args.seed + 3)
+    T.cuda.synchronize(dev)
+    render_s = time.perf_counter() - t0
+    M, N, K = sc.M, sc.N, P["frames"]
+    w, st = P["w"], P["step"]
+    gx, gy, shp = [1, M], [1, N], (M, N)
+    coords_np, nx, ny = grid_coords(M, N, w, st)
+    n, g = coords_np.shape[0], nx * ny
+    coords = T.from_numpy(np.ascontiguousarray(coords_np.T)).to(dev)
+    cxy = coords.t()
+    sL, sR = T.cuda.Stream(dev), T.cuda.Stream(dev)
+    cS, cL, cR = A.Context(0), A.Context(0), A.Context(0)
+    cS.set_stream(sL.cuda_stream)
+    cL.set_stream(sL.cuda_stream)
+    cR.set_stream(sR.cuda_stream)
+
+    def grid_buf():
+        return {nm: T.empty(g, **f64) for nm in ("x", "y", "u", "v", "phi")}
+
+    def icgn_buf():
+        return {"U": T.empty(2 * n, **f64), "F": T.empty(4 * n, **f64), "conv": T.empty(n, dtype=T.int32, device=dev)}
+
+    def grid_to_U0(b):
+        u = b["u"].view(nx, ny).t().contiguous().view(-1)
+        v = b["v"].view(nx, ny).t().contiguous().view(-1)
+        return T.nan_to_num(T.stack([u, v], 1).view(-1), nan=0.0)
+
+    # ---- frame 0: stereo match (set-up) ----
+    bS, oS = grid_buf(), icgn_buf()
+    U0S = T.empty(2 * n, **f64)
+    e0, e1 = T.cuda.Event(enable_timing=True), T.cuda.Event(enable_timing=True)
+    with T.cuda.stream(sL):
+        e0.record(sL)
+        cS.load_image_raw(0, sc.L[0], gx, gy, want_stats=False, shape=shp)
+        cS.load_image_raw(1, sc.R[0], gx, gy, want_stats=False, shape=shp)
+        cS.compute_gradients()
+        cS.integer_search(list(P["s_stereo"]), gx, gy, w, st, out=bS)
+        U0S.copy_(grid_to_U0(bS))
+        cS.local_icgn(1, coords, U0S, w, P["tol_stereo"], out=oS)
+        e1.record(sL)
+    T.cuda.synchronize(dev)
+    stereo_ms = e0.elapsed_time(e1)
+    US = T.nan_to_num(oS["U"].view(n, 2), nan=0.0)
+    coordsR = (cxy + US).t().contiguous()
+    # temporal contexts keep frame 0 as the reference (slot 0) and its gradients
+    with T.cuda.stream(sL):
+        cL.load_image_raw(0, sc.L[0], gx, gy, want_stats=False, shape=shp)
+        cL.compute_gradients()
+    with T.cuda.stream(sR):
+        cR.load_image_raw(0, sc.R[0], gx, gy, want_stats=False, shape=shp)
+        cR.compute_gradients()
+    T.cuda.synchronize(dev)
+    bL1, bR1 = grid_buf(), grid_buf()
+    res = {cam: [icgn_buf() for _ in range(K)] for cam in ("L", "R")}
+    U0s = {cam: [T.zeros(2 * n, **f64) for _ in range(K)] for cam in ("L", "R")}
+    xyz = [{"xyz": T.empty(3 * n, **f64), "err": T.empty(n, **f64)} for _ in range(2)]
+    pairs = T.empty((4, n), **f64)
+    for cam in ("L", "R"):
+        res[cam][0]["U"].zero_()
+        res[cam][0]["conv"].fill_(1)
+
+    def init_guess(cam, k, ctx, crd, gb):
+        """U0 of frame k: frame 1 from a whole-field search, later frames by extrapolating the
+        last two results (a subset without both falls back to the last finite one, then 0)."""
+        if k == 1:
+            ctx.integer_search([P["s_temp"]] * 2, gx, gy, w, st, out=gb)
+            if crd is None:
+                return grid_to_U0(gb)
+            xy = crd.t()
+            i = T.clamp(T.round((xy[:, 0] - (1 + w / 2.0)) / st), 0, nx - 1).long()
+            j = T.clamp(T.round((xy[:, 1] - (1 + w / 2.0)) / st), 0, ny - 1).long()
+            gidx = j + i * ny
+            return T.nan_to_num(T.stack([gb["u"][gidx], gb["v"][gidx]], 1).view(-1), nan=0.0)
+        a, b = res[cam][k - 1]["U"], res[cam][k - 2]["U"]
+        ext = 2 * a - b
+        return T.where(T.isfinite(ext), ext, T.where(T.isfinite(a), a, T.zeros_like(a)))
+
+    def frame(k):
+        start, done_r, end = (T.cuda.Event(enable_timing=True) for _ in range(3))
+        start.record(sL)
+        sR.wait_event(start)
+        with T.cuda.stream(sL):
+            cL.load_image_raw(1, sc.L[k], gx, gy, want_stats=False, shape=shp)
+            U0s["L"][k].copy_(init_guess("L", k, cL, None, bL1))
+            cL.local_icgn(1, coords, U0s["L"][k], w, P["tol_temp"], out=res["L"][k])
+        with T.cuda.stream(sR):
+            cR.load_image_raw(1, sc.R[k], gx, gy, want_stats=False, shape=shp)
+            U0s["R"][k].copy_(init_guess("R", k, cR, coordsR, bR1))
+            cR.local_icgn(1, coordsR, U0s["R"][k], w, P["tol_temp"], out=res["R"][k])
+            done_r.record(sR)
+        with T.cuda.stream(sL):
+            sL.wait_event(done_r)
+            UL, UR = res["L"][k]["U"].view(n, 2), res["R"][k]["U"].view(n, 2)
+            pairs.copy_(T.cat([cxy + UL, coordsR.t() + UR], 1).t())
+            cS.triangulate(pairs, sc.KL, sc.KR, sc.R_rl, sc.T_rl, out=xyz[k % 2])
+            end.record(sL)
+        return start, end
+
+    # warm-up: the first frames once (the timed pass starts the sequence again)
+    for k in range(1, 1 + max(args.warmup, 3)):
+        frame(k)
+    T.cuda.synchronize(dev)
+    clocks = ClockSampler(0)
+    l0 = cS.launches + cL.launches + cR.launches
+    evs = [frame(k) for k in range(1, K)]
+    T.cuda.synchronize(dev)
+    clk = clocks.stop()
+    launches = cS.launches + cL.launches + cR.launches - l0
+    lat = np.array([a.elapsed_time(b) for a, b in evs])
+    total_ms = evs[0][0].elapsed_time(evs[-1][1])
+    conv = {cam: np.stack([res[cam][k]["conv"].cpu().numpy() for k in range(K)]) for cam in ("L", "R")}
+    converged = sum(int(((conv[c][1:] > 0) & (conv[c][1:] < 100)).sum()) for c in ("L", "R"))
+
+    # ---- verification on the FP64 oracle and the rendering's ground truth (untimed) ----
+    import oracle as O
+
+    O.build()
+    nthr = host_threads()
+    rng = np.random.default_rng(5)
+    m = min(P["sample"], n)
+    pick = np.sort(rng.choice(n, m, replace=False))
+    crdL = coords_np[pick]
+    crdR = coordsR.t().cpu().numpy()[pick]
+
+    def host(img):
+        return img.to(T.int32).cpu().numpy().reshape(N, M).T.astype(np.float64)
+
+    def norm(img):
+        return O.normalize(host(img), gx, gy)[0]
+
+    fL0, fR0 = norm(sc.L[0]), norm(sc.R[0])
+    gL0, gR0 = O.gradient(fL0), O.gradient(fR0)
+    # stereo: IC-GN from the device's initial guesses, and the whole-field search on a few subsets
+    o = O.local_icgn(O.Frame(fL0, fR0, None, gL0[0], gL0[1]), crdL, U0S.view(n, 2)[pick].cpu().numpy().ravel(), w,
+                     P["tol_stereo"], variant=1, nthreads=nthr)
+    cg = oS["conv"].cpu().numpy()[pick]
+    fg_d, fg_o = (cg > 0) & (cg < 100), (o["conv"] > 0) & (o["conv"] < 100)
+    both = fg_d & fg_o
+    dU = np.abs(oS["U"].view(n, 2).cpu().numpy()[pick] - o["U"].reshape(-1, 2)).max(1)
+    qs = pick[:12]
+    pi, pj = qs % nx, qs // nx  # mesh order: XList fastest
+    sub = O.search_list(fL0, fR0, list(P["s_stereo"]), M, N, 1 + pi * st, 1 + pj * st, w, nthreads=nthr)
+    gu = bS["u"].cpu().numpy().reshape(nx, ny).T
+    gv = bS["v"].cpu().numpy().reshape(nx, ny).T
+    same = (sub[:, 0] == gu[pj, pi]) & (sub[:, 1] == gv[pj, pi])
+    same |= np.isnan(sub[:, 0]) & np.isnan(gu[pj, pi])
+    stereo_ver = {"sample": m, "flag_match": float(np.mean(fg_d == fg_o)),
+                  "uv_max_err": float(dU[both].max()) if both.any() else None,
+                  "search_sample_exact": f"{int(same.sum())}/{len(qs)}",
+                  "converged": int(((oS["conv"] > 0) & (oS["conv"] < 100)).sum())}
+    # temporal frames: every frame, both cameras
+    W0 = synth._ray_plane(sc.camL, crdL[:, 0], crdL[:, 1], sc.Z)  # frame-0 plane = material coordinates
+    per = {"flag_match": [], "uv_max_err": [], "truth_median_err": [], "truth_p95_err": []}
+    t_oracle, n_oracle = 0.0, 0
+    for k in range(1, K):
+        wk = sc.material_to_world(W0[:, 0], W0[:, 1], k)
+        uu, vv = sc.camL.project(wk)
+        Utrue = np.stack([uu + 1.0, vv + 1.0], 1) - crdL
+        fmk, emk = [], []
+        for cam, f0, g0, crd in (("L", fL0, gL0, crdL), ("R", fR0, gR0, crdR)):
+            gk = norm((sc.L if cam == "L" else sc.R)[k])
+            ta = time.perf_counter()
+            o = O.local_icgn(O.Frame(f0, gk, None, g0[0], g0[1]), crd,
+                             U0s[cam][k].view(n, 2)[pick].cpu().numpy().ravel(), w, P["tol_temp"], variant=1,
+                             nthreads=nthr)
+            t_oracle += time.perf_counter() - ta
+            n_oracle += m
+            cd = res[cam][k]["conv"].cpu().numpy()[pick]
+            Ud = res[cam][k]["U"].view(n, 2).cpu().numpy()[pick]
+            fd, fo = (cd > 0) & (cd < 100), (o["conv"] > 0) & (o["conv"] < 100)
+            fmk.append(float(np.mean(fd == fo)))
+            bo = fd & fo
+            if bo.any():
+                emk.append(float(np.abs(Ud - o["U"].reshape(-1, 2)).max(1)[bo].max()))
+            if cam == "L":
+                e = np.abs(Ud - Utrue).max(1)[fd]
+                per["truth_median_err"].append(round(float(np.median(e)), 4) if e.size else None)
+                per["truth_p95_err"].append(round(float(np.percentile(e, 95)), 4) if e.size else None)
+        per["flag_match"].append(min(fmk))
+        per["uv_max_err"].append(max(emk) if emk else None)
+    errs = [e for e in per["uv_max_err"] if e is not None]
+    line = {
+        "metric": "converged temporal IC-GN subsets/s over frames 1-49 (2 cameras), 4096x3000 stereo sequence",
+        "value": converged / (total_ms * 1e-3), "unit": "subsets/s", "n_gpus": 1, "steps": K - 1,
+        "warmup": max(args.warmup, 3), "ms_per_step": float(lat.mean()), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FP64 solve/fit/triangulation)",
+        "data": "synthetic (seeded analytic speckle rendering on the GPU)",
+        "config": {"workload": "sequence4096", "subsets_per_camera": n, "frames": K,
+                   "init": "frame 1: whole-field search [10 10]; frames 2-49: extrapolation of the last two "
+                           "results; no learned initial guess",
+                   "l2_flush": "each frame reads new 24 MB frames and 0.5 GB of per-context images / gradients",
+                   **{k: v for k, v in P.items() if k != "sample"}},
+        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                       "max": float(lat.max()), "stereo_frame0": stereo_ms},
+        "gpu_launches": int(launches),
+        "cpu_baseline": {"value": n_oracle / t_oracle if t_oracle else None, "unit": "subsets/s", "cores": nthr,
+                         "kind": "port",
+                         "sample": f"FP64 oracle IC-GN on {m} subsets per camera and frame from the device's own "
+                                   f"initial guesses, frames 1-{K - 1}"},
+        "clocks": clk,
+        "verification": {"stereo_frame0": stereo_ver, "sample_per_camera": m,
+                         "temporal_flag_match_min": min(per["flag_match"]),
+                         "temporal_uv_max_err": max(errs) if errs else None,
+                         "per_frame": per, "render_s": render_s,
+                         "converged_fraction": converged / (2.0 * n * (K - 1))},
+    }
+    print(json.dumps(line), flush=True)
+    for c in (cS, cL, cR):
+        c.close()
 
 def measure_fp32_peak(torch, dev):
     import aldic_b200 as A
