@@ -56,7 +56,7 @@ struct TileShape {
 // Shared memory per CTA: the dynamic buffers plus the static per-subset arrays (a bound).
 template <int ST, int W1, int TI, int DBC>
 constexpr size_t tile_total_smem() {
-  return TileShape<ST, W1, TI, DBC>::smem_bytes + (size_t)TI * kTJ * 40 + 1024;
+  return TileShape<ST, W1, TI, DBC>::smem_bytes + (size_t)TI * kTJ * 64 + 1024;
 }
 
 // Subset rows per tile: as many as fit 127 tile rows and the 227 KB of shared memory a CTA
@@ -621,6 +621,8 @@ __global__ void __launch_bounds__(TileShape<ST, W1, TI, DBC>::NT, 1)
   __shared__ int r_L[TI], r_na[TI], r_d0[TI], r_d1[TI], c_U[kTJ], c_nb[kTJ], c_d0[kTJ], c_d1[kTJ];
   __shared__ int r_aoff[TI];   // crop row of shift row k: aa = k + r_aoff
   __shared__ int p_na[NSUB];   // crop rows of a valid subset, 0 for an invalid one
+  __shared__ float4 p_c[NSUB]; // (kf, 1 / denT, sqrt(tolv), 0): the fast epilogue's operands, one load
+  __shared__ int2 p_g[NSUB];   // (crop row offset r_aoff, crop rows p_na): the prefetch's operands, one load
   __shared__ float s_cf;
 
   const int tid = threadIdx.x;
@@ -667,7 +669,11 @@ __global__ void __launch_bounds__(TileShape<ST, W1, TI, DBC>::NT, 1)
     p_ok[q] = ok;
   }
   __syncthreads();
-  for (int q = tid; q < NSUB; q += NT) p_na[q] = p_ok[q] ? r_na[q % TI] : 0;
+  for (int q = tid; q < NSUB; q += NT) {
+    p_na[q] = p_ok[q] ? r_na[q % TI] : 0;
+    p_c[q] = make_float4(p_kf[q], p_invden[q], p_sqtolv[q], 0.f);
+    p_g[q] = make_int2(r_aoff[q % TI], p_ok[q] ? r_na[q % TI] : 0);
+  }
   // ---- f tile, centred ----
   for (int idx = tid; idx < FR * FCP; idx += NT) {
     const int x = idx / FCP, c = idx % FCP;
@@ -707,6 +713,13 @@ __global__ void __launch_bounds__(TileShape<ST, W1, TI, DBC>::NT, 1)
     const bool bok = dbr < NDA && bb >= 0 && bb < nbv;
     const bool rbg = bb == 0 || bb == nbv - 1;
     const long long mcol = (long long)(X0 + DA0) * NW + (Y0 + jl * ST + db);  // map index of (il = 0, k = 0)
+    // crop index of shift row k of subset row e is k + lbase[e] (lin = aa + bb na)
+    int lbase[H0];
+#pragma unroll
+    for (int e = 0; e < H0; ++e) {
+      const int2 gq = p_g[(il0 + e < TI ? il0 + e : TI - 1) + jl * TI];
+      lbase[e] = gq.x + bb * gq.y;
+    }
     for (int k = 0; k < NDA; ++k) {
       // ---- epilogue operands of this shift, fetched before pass 1 hides their latency ----
       int st[H0];
@@ -719,7 +732,8 @@ __global__ void __launch_bounds__(TileShape<ST, W1, TI, DBC>::NT, 1)
         pcx[e] = 0.f;
         if (!bok || e >= ns) continue;
         const int il = il0 + e;
-        const int na = p_na[il + jl * TI], aa = k + r_aoff[il];
+        const int2 gq = p_g[il + jl * TI];
+        const int na = gq.y, aa = k + gq.x;
         if ((unsigned)aa >= (unsigned)na) continue;
         const bool ra = aa == 0 || aa == na - 1;
         if (!ra && !rbg) {
@@ -778,15 +792,16 @@ __global__ void __launch_bounds__(TileShape<ST, W1, TI, DBC>::NT, 1)
           if (e >= ns) break;  // the second half has TI - H0 subset rows
           const int q = il0 + e + jl * TI;
           const float2 v = pf[e];
-          const bool fast = st[e] == 1 && v.y * p_sqtolv[q] < 0.5f;
+          const float4 c = p_c[q];
+          const bool fast = st[e] == 1 && v.y * c.z < 0.5f;
           if (st[e] != 0 && !fast) slow |= 1u << e;
-          float cval = (N[e] - p_kf[q] * v.x) * v.y * p_invden[q];
+          float cval = (N[e] - c.x * v.x) * v.y * c.y;
           if (fabsf(cval) - 1.f > 1.4901161193847656e-08f) cval = 0.f;
           // a thread meets each subset's crop indices lin = aa + bb na in increasing order
           // (aa grows with k, bb with the chunk), so the first maximum is the first strict one
           if (fast && cval > bv[e]) {
             bv[e] = cval;
-            bl[e] = (k + r_aoff[il0 + e]) + bb * p_na[q];
+            bl[e] = k + lbase[e];
           }
         }
         if (slow) {
