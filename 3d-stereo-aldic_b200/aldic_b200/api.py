@@ -23,7 +23,7 @@ from ._lib import AldicError
 __all__ = [
     "Context", "default_context", "funNormalizeImg", "funImgGradient", "ba_interp2_spline", "funIntegerSearch",
     "LocalICGN", "LocalICGNQuadtree", "Subpb1", "Subpb1Quadtree", "epipolar_ICGN1",
-    "stereoReconstruction_quadtree", "bad_points_local", "bad_points_subpb1",
+    "stereoReconstruction_quadtree", "bad_points_local", "bad_points_subpb1", "Init",
 ]
 
 
@@ -300,6 +300,44 @@ class Context:
                     "aldic_epipolar_icgn")
         return z
 
+    def inpaint_nans(self, A, info=False):
+        """inpaint_nans(A, 4) (spring analogy).  A host array is returned as a new filled
+        array; a CUDA tensor (with shape=(m, n) implied by a 2-D tensor, column-major data)
+        is filled in place.  info=True also returns (NaN entries, CG iterations, converged)."""
+        k = _Keep()
+        nfo = (C.c_int32 * 3)()
+        if _is_torch(A):
+            if A.dim() != 2:
+                raise AldicError("device grids must be 2-D tensors (n, m) holding the column-major m x n grid")
+            n, m = A.shape  # row-major (n, m) == column-major m x n
+            rc = self.lib.aldic_inpaint_nans(self.h, int(m), int(n), k.ptr(A, np.float64), nfo if info else None)
+            self._check(rc, "aldic_inpaint_nans")
+            return (A, tuple(nfo)) if info else A
+        a = np.array(A, dtype=np.float64, order="F", copy=True)
+        m, n = a.shape
+        rc = self.lib.aldic_inpaint_nans(self.h, int(m), int(n), C.c_void_p(a.ctypes.data), nfo if info else None)
+        self._check(rc, "aldic_inpaint_nans")
+        return (a, tuple(nfo)) if info else a
+
+    def init_u0(self, u, v, out=None):
+        """Init(u, v, Phi, x, y, 0): inpaint the search grids (ny x nx, left unchanged) and
+        return U0 (2 nx ny, mesh order), or fill `out` (a CUDA tensor or host array)."""
+        k = _Keep()
+        if _is_torch(u):
+            if u.dim() != 2:
+                raise AldicError("device grids must be 2-D tensors (nx, ny) holding the column-major ny x nx grid")
+            nx, ny = u.shape
+        else:
+            ny, nx = np.shape(u)
+        if out is None:
+            U0, op = k.out(2 * nx * ny, np.float64)
+        else:
+            U0, op = out, k.dst(out, np.float64, 2 * nx * ny)
+        rc = self.lib.aldic_init_u0(self.h, int(ny), int(nx), k.ptr(u, np.float64, numel=nx * ny),
+                                    k.ptr(v, np.float64, numel=nx * ny), op)
+        self._check(rc, "aldic_init_u0")
+        return U0
+
     def triangulate(self, pairs, KL, KR, R, T, out=None):
         k = _Keep()
         n = _count(pairs, 4)
@@ -365,6 +403,16 @@ def ba_interp2_spline(F, X, Y, method="cubicspline", ctx: Context | None = None)
     ctx = ctx or default_context()
     ctx.load_image(_lib.SLOT_DEF, np.asarray(F, dtype=np.float64))
     return ctx.interp2(_lib.SLOT_DEF, X, Y)
+
+
+def Init(u, v, Phi=None, x=None, y=None, index=0, ctx: Context | None = None):
+    """Init(u, v, Phi, x, y, index) (func/Init.m).  index 0 (the stereo and temporal
+    drivers' call): inpaint_nans(., 4) of u and v and U0 in mesh order.  The spring outlier
+    passes of index 1 are not built."""
+    if index != 0:
+        raise AldicError("Init index 1 (spring outlier passes) is not built; the drivers call index 0")
+    ctx = ctx or default_context()
+    return ctx.init_u0(u, v)
 
 
 def funIntegerSearch(f, g, tempSizeOfSearchRegion, gridx, gridy, winsize, winstepsize, tempNoOfInitPt=0,

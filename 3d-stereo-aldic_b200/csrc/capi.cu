@@ -633,6 +633,93 @@ int aldic_subpb1(aldic_ctx* c, int variant, int64_t n, const double* coords, con
   return finish(c, launch_subpb1(a, wmx, wmy, c->stream));
 }
 
+int aldic_inpaint_nans(aldic_ctx* c, int m, int n, double* A, int32_t* info) {
+  if (!c) return ALDIC_ERR_ARG;
+  if (m < 0 || n < 0) return fail(c, ALDIC_ERR_ARG, "grid size %d x %d", m, n);
+  if ((long long)m * n > (1LL << 30)) return fail(c, ALDIC_ERR_ARG, "grid of %d x %d entries too large", m, n);
+  if (info) {
+    info[0] = 0;
+    info[1] = 0;
+    info[2] = 1;
+  }
+  if (m == 0 || n == 0) return ALDIC_OK;
+  if (!A) return fail(c, ALDIC_ERR_ARG, "grid pointer is NULL");
+  CK(cudaSetDevice(c->device));
+  const long long mn = (long long)m * n;
+  const size_t bytes = (size_t)mn * sizeof(double);
+  // A is both input and output: staged in, copied back
+  Arg aa{A, bytes, false, nullptr};
+  c->arena.used = 0;
+  c->back.clear();
+  const bool host = !is_device_ptr(A);
+  int rc = arena_reserve(c, (host ? bytes + 256 : 0) + inpaint_scratch_bytes(mn) + 256 + 64);
+  if (rc) return rc;
+  if (host) {
+    aa.dev = arena_take(c, bytes);
+    CK(cudaMemcpyAsync(aa.dev, A, bytes, cudaMemcpyHostToDevice, c->stream));
+    c->back.push_back({A, aa.dev, bytes});
+  } else {
+    aa.dev = A;
+  }
+  void* scratch = arena_take(c, inpaint_scratch_bytes(mn));
+  int* status = (int*)arena_take(c, 64);
+  const int l = launch_inpaint((double*)aa.dev, m, n, scratch, status, c->stream);
+  if (info) {
+    int st[3];
+    CK(cudaMemcpyAsync(st, status, sizeof(st), cudaMemcpyDeviceToHost, c->stream));
+    rc = finish(c, l);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(c->stream));
+    info[0] = st[0];
+    info[1] = st[1];
+    info[2] = st[2];
+    return ALDIC_OK;
+  }
+  return finish(c, l);
+}
+
+int aldic_init_u0(aldic_ctx* c, int ny, int nx, const double* u, const double* v, double* U0) {
+  if (!c) return ALDIC_ERR_ARG;
+  if (ny < 0 || nx < 0) return fail(c, ALDIC_ERR_ARG, "grid size %d x %d", ny, nx);
+  if ((long long)ny * nx > (1LL << 30)) return fail(c, ALDIC_ERR_ARG, "grid of %d x %d entries too large", ny, nx);
+  if (ny == 0 || nx == 0) return ALDIC_OK;
+  if (!u || !v || !U0) return fail(c, ALDIC_ERR_ARG, "missing array argument");
+  CK(cudaSetDevice(c->device));
+  const long long g = (long long)ny * nx;
+  const size_t bytes = (size_t)g * sizeof(double);
+  Arg au{u, bytes, false, nullptr}, av{v, bytes, false, nullptr}, ao{U0, 2 * bytes, true, nullptr};
+  // the staged arrays, then the two working copies and the solver scratch
+  c->arena.used = 0;
+  c->back.clear();
+  size_t need = 0;
+  for (Arg* a : {&au, &av, &ao})
+    if (!is_device_ptr(a->user)) need += ((a->bytes + 255) & ~size_t(255)) + 256;
+  need += 2 * (bytes + 256) + inpaint_scratch_bytes(g) + 512;
+  int rc = arena_reserve(c, need);
+  if (rc) return rc;
+  for (Arg* a : {&au, &av, &ao}) {
+    if (is_device_ptr(a->user)) {
+      a->dev = const_cast<void*>(a->user);
+    } else {
+      a->dev = arena_take(c, a->bytes);
+      if (a->output)
+        c->back.push_back({const_cast<void*>(a->user), a->dev, a->bytes});
+      else
+        CK(cudaMemcpyAsync(a->dev, a->user, a->bytes, cudaMemcpyHostToDevice, c->stream));
+    }
+  }
+  double* wu = (double*)arena_take(c, bytes);
+  double* wv = (double*)arena_take(c, bytes);
+  CK(cudaMemcpyAsync(wu, au.dev, bytes, cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaMemcpyAsync(wv, av.dev, bytes, cudaMemcpyDeviceToDevice, c->stream));
+  void* scratch = arena_take(c, inpaint_scratch_bytes(g));
+  int* status = (int*)arena_take(c, 64);
+  int l = launch_inpaint(wu, ny, nx, scratch, status, c->stream);
+  l += launch_inpaint(wv, ny, nx, scratch, status, c->stream);
+  l += launch_interleave_u0(wu, wv, ny, nx, (double*)ao.dev, c->stream);
+  return finish(c, l);
+}
+
 int aldic_triangulate(aldic_ctx* c, int64_t n, const double* pairs, const double* KL, const double* KR,
                       const double* R, const double* T, double* xyz, double* reproj_err) {
   if (!c) return ALDIC_ERR_ARG;

@@ -1,0 +1,193 @@
+// Initial-guess assembly of the stereo / temporal drivers: Init(u, v, Phi, x, y, 0)
+// (func/Init.m:1-2 and :85-92), i.e. inpaint_nans(u, 4) and inpaint_nans(v, 4) of the
+// integer-search grids, then U0 interleaved in mesh order.
+//
+// inpaint_nans method 4 (func/inpaint_nans.m:369-398, the "spring analogy"): every NaN
+// entry is tied by a spring of unit stiffness to each of its horizontal and vertical
+// neighbours inside the grid (each pair once), and the NaN entries take the least-squares
+// solution of "every spring at rest" with the known entries fixed.  The normal equations of
+// that system are, for every unknown i with in-grid 4-neighbours N(i),
+//     |N(i)| x_i - sum over unknown j in N(i) of x_j = sum over known j in N(i) of A_j,
+// a symmetric positive definite system (a graph Laplacian with Dirichlet values) whenever
+// every connected NaN region touches a known entry.  It is solved here by conjugate
+// gradients in FP64, matrix-free on the grid, by one CTA per grid (the unknowns are the
+// search's few failed subsets); the residual is driven to 1e-13 of the right-hand side.
+// A NaN region with no known neighbour has no unique solution: CG leaves it at 0.
+#include "common.cuh"
+#include "kernels.h"
+
+namespace aldic {
+
+namespace {
+
+constexpr int kInitThreads = 1024;
+
+// Sum over the block, returned to every thread (fixed order: warp shuffles, then the 32
+// warp totals in warp order).
+__device__ __forceinline__ double block_sum_all(double v, double* red) {
+  v = warp_sum(v);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  __syncthreads();  // red is reused call after call
+  if (lane == 0) red[wid] = v;
+  __syncthreads();
+  double s = 0.0;
+  for (int k = 0; k < (int)(blockDim.x >> 5); ++k) s += red[k];
+  return s;
+}
+
+// Grid neighbours (row-1, row+1, col-1, col+1) of linear index g in an m x n column-major grid.
+__device__ __forceinline__ int nbr(int g, int k, int m, int n) {
+  const int r = g % m, c = g / m;
+  switch (k) {
+    case 0: return r > 0 ? g - 1 : -1;
+    case 1: return r < m - 1 ? g + 1 : -1;
+    case 2: return c > 0 ? g - m : -1;
+    default: return c < n - 1 ? g + m : -1;
+  }
+}
+
+}  // namespace
+
+// One CTA per grid: A (m x n, column-major) is overwritten at its NaN entries.  Scratch:
+// map (m n ints), list (m n ints), x, r, p, q (m n doubles each).  status[0] = unknowns,
+// status[1] = CG iterations, status[2] = 1 when the residual target was met.
+__global__ void __launch_bounds__(kInitThreads) inpaint_springs_kernel(double* __restrict__ A, int m, int n,
+                                                                       int* __restrict__ map, int* __restrict__ list,
+                                                                       double* __restrict__ x, double* __restrict__ r,
+                                                                       double* __restrict__ p, double* __restrict__ q,
+                                                                       int* __restrict__ status) {
+  __shared__ double red[32];
+  __shared__ int s_count;
+  __shared__ int s_warp[32];
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
+  const int mn = m * n;
+  if (tid == 0) s_count = 0;
+  __syncthreads();
+  // ---- compaction of the NaN entries, in grid order ----
+  for (int base = 0; base < mn; base += blockDim.x) {
+    const int g = base + tid;
+    const bool unk = g < mn && isnan(A[g]);
+    const unsigned bal = __ballot_sync(0xffffffffu, unk);
+    if (lane == 0) s_warp[wid] = __popc(bal);
+    __syncthreads();
+    int before = s_count;
+    for (int k = 0; k < wid; ++k) before += s_warp[k];
+    const int pos = before + __popc(bal & ((1u << lane) - 1u));
+    if (g < mn) map[g] = unk ? pos : -1;
+    if (unk) list[pos] = g;
+    __syncthreads();
+    if (tid == 0) {
+      int t = 0;
+      for (int k = 0; k < nw; ++k) t += s_warp[k];
+      s_count += t;
+    }
+    __syncthreads();
+  }
+  const int nu = s_count;
+  if (nu == 0) {
+    if (tid == 0) {
+      status[0] = 0;
+      status[1] = 0;
+      status[2] = 1;
+    }
+    return;
+  }
+  // ---- right-hand side and the CG start x = 0, r = p = b ----
+  double bb_local = 0.0;
+  for (int u = tid; u < nu; u += blockDim.x) {
+    const int g = list[u];
+    double b = 0.0;
+    for (int k = 0; k < 4; ++k) {
+      const int h = nbr(g, k, m, n);
+      if (h >= 0 && map[h] < 0) b += A[h];
+    }
+    x[u] = 0.0;
+    r[u] = b;
+    p[u] = b;
+    bb_local += b * b;
+  }
+  const double bb = block_sum_all(bb_local, red);
+  double rr = bb;
+  const double target = 1e-26 * bb;  // |r| <= 1e-13 |b|
+  const int maxit = nu + 200 < 100000 ? nu + 200 : 100000;
+  int it = 0;
+  bool met = rr <= target;
+  while (!met && it < maxit) {
+    __syncthreads();  // p complete
+    double pq_local = 0.0;
+    for (int u = tid; u < nu; u += blockDim.x) {
+      const int g = list[u];
+      double s = 0.0;
+      int deg = 0;
+      for (int k = 0; k < 4; ++k) {
+        const int h = nbr(g, k, m, n);
+        if (h < 0) continue;
+        ++deg;
+        const int j = map[h];
+        if (j >= 0) s += p[j];
+      }
+      const double v = deg * p[u] - s;
+      q[u] = v;
+      pq_local += p[u] * v;
+    }
+    const double pq = block_sum_all(pq_local, red);
+    if (!(pq > 0.0)) break;  // singular direction (a region with no known neighbour)
+    const double alpha = rr / pq;
+    double rr_local = 0.0;
+    for (int u = tid; u < nu; u += blockDim.x) {
+      x[u] += alpha * p[u];
+      const double rn = r[u] - alpha * q[u];
+      r[u] = rn;
+      rr_local += rn * rn;
+    }
+    const double rr_new = block_sum_all(rr_local, red);
+    ++it;
+    met = rr_new <= target;
+    const double beta = rr_new / rr;
+    rr = rr_new;
+    for (int u = tid; u < nu; u += blockDim.x) p[u] = r[u] + beta * p[u];
+  }
+  __syncthreads();
+  for (int u = tid; u < nu; u += blockDim.x) A[list[u]] = x[u];
+  if (tid == 0) {
+    status[0] = nu;
+    status[1] = it;
+    status[2] = met ? 1 : 0;
+  }
+}
+
+// U0 in mesh order from the inpainted grids u, v (ny x nx column-major, the search's
+// output layout): U0(2 i - 1) = u'(i), U0(2 i) = v'(i) with i running over the transposed
+// grid, XList fastest (func/Init.m:86-92).
+__global__ void interleave_u0_kernel(const double* __restrict__ u, const double* __restrict__ v, int ny, int nx,
+                                     double* __restrict__ U0) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= (long long)nx * ny) return;
+  const int ix = (int)(i % nx), iy = (int)(i / nx);
+  const long long g = iy + (long long)ix * ny;
+  U0[2 * i] = u[g];
+  U0[2 * i + 1] = v[g];
+}
+
+size_t inpaint_scratch_bytes(long long mn) { return (size_t)mn * (2 * sizeof(int) + 4 * sizeof(double)) + 1024; }
+
+int launch_inpaint(double* A, int m, int n, void* scratch, int* status, cudaStream_t st) {
+  const long long mn = (long long)m * n;
+  char* s = (char*)scratch;
+  int* map = (int*)s;
+  int* list = map + mn;
+  double* x = (double*)(((uintptr_t)(list + mn) + 255) & ~(uintptr_t)255);
+  double* r = x + mn;
+  double* p = r + mn;
+  double* q = p + mn;
+  inpaint_springs_kernel<<<1, kInitThreads, 0, st>>>(A, m, n, map, list, x, r, p, q, status);
+  return 1;
+}
+
+int launch_interleave_u0(const double* u, const double* v, int ny, int nx, double* U0, cudaStream_t st) {
+  const long long n = (long long)nx * ny;
+  interleave_u0_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(u, v, ny, nx, U0);
+  return 1;
+}
+
+}  // namespace aldic

@@ -102,6 +102,9 @@ int launch_search_tile(const SearchArgs& a, cudaStream_t st);
 struct CamPair {
   double P[24];  // P_L = K_L [I | 0] then P_R = K_R [R | T], each 3x4 row-major
 };
+size_t inpaint_scratch_bytes(long long mn);
+int launch_inpaint(double* A, int m, int n, void* scratch, int* status, cudaStream_t st);
+int launch_interleave_u0(const double* u, const double* v, int ny, int nx, double* U0, cudaStream_t st);
 int launch_triangulate(long long n, const double* pairs, const CamPair& cams, double* xyz, double* err,
                        cudaStream_t st);
 int launch_fp32_probe(int blocks, int threads, int iters, float* out, bool packed, cudaStream_t st);

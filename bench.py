@@ -198,7 +198,7 @@ class StereoPipeline:
                            "v": T.empty(g, **f64), "phi": T.empty(g, **f64), "U0": T.empty(2 * n, **f64),
                            "U": T.empty(2 * n, **f64), "F": T.empty(4 * n, **f64), "H": T.empty(21 * n, **f64),
                            "conv": T.empty(n, dtype=T.int32, device=device),
-                           "mark": T.empty(n, dtype=T.uint8, device=device)}
+                           "mark": T.empty(n, dtype=T.uint8, device=device), "Ug": T.empty(2 * g, **f64)}
         self.coordsR = T.empty((2, n), **f64)
         self.pairs = [T.empty((4, n), **f64), T.empty((4, n), **f64)]
         self.xyz = [{"xyz": T.empty(3 * n, **f64), "err": T.empty(n, **f64)} for _ in range(2)]
@@ -207,14 +207,10 @@ class StereoPipeline:
         self.gy = [1, N]
 
 
-    def _search_to_U0(self, b):
-        """Grid search output (nY x nX column-major) -> U0 interleaved in mesh order,
-        NaN -> 0 (stand-in for Init's inpainting)."""
-        T = self.torch
-        u = b["u"].view(self.nx, self.ny).t().contiguous().view(-1)  # (ny,nx) F-order -> mesh order
-        v = b["v"].view(self.nx, self.ny).t().contiguous().view(-1)
-        U0 = T.stack([u, v], 1).view(-1)
-        b["U0"].copy_(T.nan_to_num(U0, nan=0.0))
+    def _search_to_U0(self, b, ctx, out=None):
+        """Init(u, v, Phi, x, y, 0): the search grids (nY x nX column-major) inpainted
+        (inpaint_nans(., 4)) and interleaved in mesh order, on the device."""
+        ctx.init_u0(b["u"].view(self.nx, self.ny), b["v"].view(self.nx, self.ny), out=b["U0"] if out is None else out)
 
     def step(self):
         T, st, ev = self.torch, self.streams, self.ev
@@ -251,7 +247,7 @@ class StereoPipeline:
 
     def _stereo_icgn(self):
         P, bS = self.P, self.buf["S"]
-        self._search_to_U0(bS)
+        self._search_to_U0(bS, self.ctx["S"])
         self.ctx["S"].local_icgn(1, self.coords, bS["U0"], P["w"], P["tol_stereo"], out=bS)
 
     def _temporal_left(self):
@@ -259,7 +255,7 @@ class StereoPipeline:
         P, cL, bL = self.P, self.ctx["L"], self.buf["L"]
         self._load_pair(cL, "L0", "L1")
         cL.integer_search([P["s_temp"]] * 2, self.gx, self.gy, P["w"], P["step"], out=bL)
-        self._search_to_U0(bL)
+        self._search_to_U0(bL, cL)
         cL.local_icgn(1, self.coords, bL["U0"], P["w"], P["tol_temp"], out=bL)
 
     def _temporal_right(self, stereo_done):
@@ -282,11 +278,12 @@ class StereoPipeline:
         cxy = self.coords.t()
         xyR = cxy + T.nan_to_num(US, nan=0.0)
         self.coordsR.copy_(xyR.t())
-        # nearest search-grid node of each right-image point (Init / MeshSetUp stand-in)
+        # Init over the search grid, then each right-image point takes its nearest grid node
+        # (the MeshSetUp stand-in for the stereo-matched mesh)
+        self._search_to_U0(bR, cR, out=bR["Ug"])
         i = T.clamp(T.round((xyR[:, 0] - (1 + w / 2.0)) / st), 0, self.nx - 1).long()
         j = T.clamp(T.round((xyR[:, 1] - (1 + w / 2.0)) / st), 0, self.ny - 1).long()
-        gidx = j + i * self.ny
-        bR["U0"].view(n, 2).copy_(T.nan_to_num(T.stack([bR["u"][gidx], bR["v"][gidx]], 1), nan=0.0))
+        bR["U0"].view(n, 2).copy_(bR["Ug"].view(-1, 2)[i + j * self.nx])
         cR.local_icgn(1, self.coordsR, bR["U0"], w, P["tol_temp"], out=bR)
 
     def _triangulate(self):
@@ -680,7 +677,7 @@ def run_aux(args, P):
     b = {"x": T.empty(g, **f64), "y": T.empty(g, **f64), "u": T.empty(g, **f64), "v": T.empty(g, **f64),
          "phi": T.empty(g, **f64), "U0": T.empty(2 * n, **f64), "U": T.empty(2 * n, **f64),
          "F": T.empty(4 * n, **f64), "H": T.empty(21 * n, **f64), "conv": T.empty(n, dtype=T.int32, device=dev),
-         "mark": T.empty(n, dtype=T.uint8, device=dev)}
+         "mark": T.empty(n, dtype=T.uint8, device=dev), "Ug": T.empty(2 * g, **f64)}
     sub = [{"U": T.empty(2 * n, **f64), "conv": T.empty(n, dtype=T.int32, device=dev)} for _ in range(P.get("admm", 0))]
     vdual = T.zeros(2 * n, **f64)
     cxy = coords.t()
@@ -694,11 +691,11 @@ def run_aux(args, P):
                 ctx.set_mask(mask_d)
             ctx.compute_gradients()
             ctx.integer_search([P["s_temp"]] * 2, gx, gy, w, st, out=b)
-            # nearest search-grid node of every mesh node (Init stand-in), NaN -> 0
+            # Init over the search grid, then every mesh node takes its nearest grid node
+            ctx.init_u0(b["u"].view(nx, ny), b["v"].view(nx, ny), out=b["Ug"])
             i = T.clamp(T.round((cxy[:, 0] - (1 + w / 2.0)) / st), 0, nx - 1).long()
             j = T.clamp(T.round((cxy[:, 1] - (1 + w / 2.0)) / st), 0, ny - 1).long()
-            gidx = j + i * ny
-            b["U0"].view(n, 2).copy_(T.nan_to_num(T.stack([b["u"][gidx], b["v"][gidx]], 1), nan=0.0))
+            b["U0"].view(n, 2).copy_(b["Ug"].view(-1, 2)[i + j * nx])
             ctx.local_icgn(1 if quad else 0, coords, b["U0"], w, P["tol_temp"], out=b)
             Uold = b["U"]
             for k in range(P.get("admm", 0)):
@@ -855,10 +852,11 @@ def run_sequence(args, P):
     def icgn_buf():
         return {"U": T.empty(2 * n, **f64), "F": T.empty(4 * n, **f64), "conv": T.empty(n, dtype=T.int32, device=dev)}
 
-    def grid_to_U0(b):
-        u = b["u"].view(nx, ny).t().contiguous().view(-1)
-        v = b["v"].view(nx, ny).t().contiguous().view(-1)
-        return T.nan_to_num(T.stack([u, v], 1).view(-1), nan=0.0)
+    def grid_to_U0(b, ctx):
+        """Init(u, v, Phi, x, y, 0) on the device: the search grids inpainted, mesh order."""
+        out = T.empty(2 * g, **f64)
+        ctx.init_u0(b["u"].view(nx, ny), b["v"].view(nx, ny), out=out)
+        return out
 
     # ---- frame 0: stereo match (set-up) ----
     bS, oS = grid_buf(), icgn_buf()
@@ -870,7 +868,7 @@ def run_sequence(args, P):
         cS.load_image_raw(1, sc.R[0], gx, gy, want_stats=False, shape=shp)
         cS.compute_gradients()
         cS.integer_search(list(P["s_stereo"]), gx, gy, w, st, out=bS)
-        U0S.copy_(grid_to_U0(bS))
+        U0S.copy_(grid_to_U0(bS, cS))
         cS.local_icgn(1, coords, U0S, w, P["tol_stereo"], out=oS)
         e1.record(sL)
     T.cuda.synchronize(dev)
@@ -899,13 +897,13 @@ def run_sequence(args, P):
         last two results (a subset without both falls back to the last finite one, then 0)."""
         if k == 1:
             ctx.integer_search([P["s_temp"]] * 2, gx, gy, w, st, out=gb)
+            Ug = grid_to_U0(gb, ctx)
             if crd is None:
-                return grid_to_U0(gb)
+                return Ug
             xy = crd.t()
             i = T.clamp(T.round((xy[:, 0] - (1 + w / 2.0)) / st), 0, nx - 1).long()
             j = T.clamp(T.round((xy[:, 1] - (1 + w / 2.0)) / st), 0, ny - 1).long()
-            gidx = j + i * ny
-            return T.nan_to_num(T.stack([gb["u"][gidx], gb["v"][gidx]], 1).view(-1), nan=0.0)
+            return Ug.view(-1, 2)[i + j * nx].reshape(-1)
         a, b = res[cam][k - 1]["U"], res[cam][k - 2]["U"]
         ext = 2 * a - b
         return T.where(T.isfinite(ext), ext, T.where(T.isfinite(a), a, T.zeros_like(a)))
@@ -1090,6 +1088,7 @@ def e2e_measure(A, scene, P, steps, local_rank):
            for k in ("S", "L", "R")}
     tri = [{"xyz": pinned(3 * n), "err": pinned(n)} for _ in range(2)]
     U0 = {k: pinned(2 * n) for k in ("S", "L", "R")}
+    Ug = pinned(2 * g)
     # MATLAB column-major n x 2 / n x 4 arrays: the library reads them without a repack
     crd = pinned((n, 2), order="F")
     crd[:] = coords
@@ -1111,23 +1110,25 @@ def e2e_measure(A, scene, P, steps, local_rank):
 
     def stereo():
         u, v = search("S", "L0", "R0", P["s_stereo"])
-        U0["S"].reshape(n, 2)[:] = np.nan_to_num(np.stack([u.T.ravel(order="F"), v.T.ravel(order="F")], 1))
+        ctx["S"].init_u0(u, v, out=U0["S"])
         ctx["S"].local_icgn(1, crd, U0["S"], w, P["tol_stereo"], out=out["S"])
         stereo_done.set()
 
     def left():
         u, v = search("L", "L0", "L1", P["s_temp"])
-        U0["L"].reshape(n, 2)[:] = np.nan_to_num(np.stack([u.T.ravel(order="F"), v.T.ravel(order="F")], 1))
+        ctx["L"].init_u0(u, v, out=U0["L"])
         ctx["L"].local_icgn(1, crd, U0["L"], w, P["tol_temp"], out=out["L"])
 
     def right():
         u, v = search("R", "R0", "R1", P["s_temp"])
         stereo_done.wait()
-        # right-camera mesh = left mesh + stereo match; initial guess from the nearest grid node
+        # right-camera mesh = left mesh + stereo match; initial guess: Init over the search
+        # grid, then the nearest grid node of each right-image point
+        ctx["R"].init_u0(u, v, out=Ug)
         crdR[:] = coords + np.nan_to_num(out["S"]["U"].reshape(n, 2))
         i = np.clip(np.round((crdR[:, 0] - (1 + w / 2.0)) / st), 0, nx - 1).astype(int)
         j = np.clip(np.round((crdR[:, 1] - (1 + w / 2.0)) / st), 0, ny - 1).astype(int)
-        U0["R"].reshape(n, 2)[:] = np.nan_to_num(np.stack([u[j, i], v[j, i]], 1))
+        U0["R"].reshape(n, 2)[:] = Ug.reshape(-1, 2)[i + j * nx]
         ctx["R"].local_icgn(1, crdR, U0["R"], w, P["tol_temp"], out=out["R"])
 
     pool = ThreadPoolExecutor(3)
@@ -1146,8 +1147,8 @@ def e2e_measure(A, scene, P, steps, local_rank):
         for p, o in zip(pairs, tri):
             ctx["S"].triangulate(p, scene.KL, scene.KR, scene.R_rl, scene.T_rl, out=o)
         conv_total += sum(int(np.sum((out[k]["conv"] > 0) & (out[k]["conv"] < 100))) for k in ("S", "L", "R"))
-        h2d = 6 * imgs["L0"].nbytes + 3 * (2 * n * 8 + U0["S"].nbytes) + 2 * pairs[0].nbytes
-        d2h = 3 * (grid_bytes + icgn_out_bytes) + 2 * (tri[0]["xyz"].nbytes + tri[0]["err"].nbytes)
+        h2d = 6 * imgs["L0"].nbytes + 3 * (2 * n * 8 + U0["S"].nbytes + 2 * g * 8) + 2 * pairs[0].nbytes
+        d2h = 3 * (grid_bytes + icgn_out_bytes + 2 * g * 8) + 2 * (tri[0]["xyz"].nbytes + tri[0]["err"].nbytes)
         return h2d, d2h
 
     one()  # warm-up

@@ -130,6 +130,20 @@ int aldic_subpb1(aldic_ctx* ctx, int variant, int64_t n, const double* coords, c
  * offset Df.DfAxis(1) = 4; znssd = ZNSSD of the final iteration (NaN on failure). */
 int aldic_epipolar_icgn(aldic_ctx* ctx, int64_t n, const double* pts, int winsize, double tol, double* znssd);
 
+/* ------------------------------------------------------ initial guess --------- */
+/* inpaint_nans(A, 4) (func/inpaint_nans.m:369-398, spring analogy), in place on an m x n
+ * column-major grid: the NaN entries become the least-squares solution of unit springs
+ * to their in-grid horizontal / vertical neighbours with the finite entries fixed (FP64
+ * conjugate gradients to 1e-13 of the right-hand side; a NaN region with no finite
+ * neighbour becomes 0).  info (optional, host, 3 ints): NaN entries, CG iterations,
+ * 1 when the residual target was met; passing it makes the call wait for the device. */
+int aldic_inpaint_nans(aldic_ctx* ctx, int m, int n, double* A, int32_t* info);
+
+/* Init(u, v, Phi, x, y, 0) (func/Init.m:1-2,85-92): inpaint_nans(., 4) of the search's
+ * u and v grids (ny x nx column-major, as aldic_integer_search returns them; left
+ * unchanged) and U0 (2 nx ny) interleaved [u1 v1 u2 v2 ...] in mesh order (XList fastest). */
+int aldic_init_u0(aldic_ctx* ctx, int ny, int nx, const double* u, const double* v, double* U0);
+
 /* -------------------------------------------------------- triangulation --------- */
 /* triangulatePoints (func_quadtree/stereoReconstruction_quadtree.m:30-52): per row of
  * pairs (n x 4 column-major [xL yL xR yR]) the DLT of P_L = K_L [I | 0] and

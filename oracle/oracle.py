@@ -284,3 +284,44 @@ def triangulate(pairs, KL, KR, R, T):
         xyz[ok] = X
         err[ok] = 0.5 * (el + er)
     return xyz, err
+
+
+def inpaint_nans4(A):
+    """inpaint_nans(A, 4), the spring analogy (func/inpaint_nans.m:369-398): springs from
+    every NaN entry to each in-grid horizontal / vertical neighbour (:375-381), duplicate
+    springs removed (:384), knowns moved to the right-hand side (:394) and the NaN entries
+    solved in the least-squares sense (:398; MATLAB's sparse QR, here the normal equations
+    of the same full-rank system, solved directly).  Restated in numpy / scipy."""
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spla
+
+    A = np.asarray(A, dtype=np.float64)
+    m, n = A.shape
+    flat = A.ravel(order="F").copy()
+    nan = np.flatnonzero(np.isnan(flat))
+    if nan.size == 0:
+        return A.copy()
+    r, c = nan % m, nan // m
+    pairs = []
+    for dr, dc in ((-1, 0), (1, 0), (0, -1), (0, 1)):
+        rr, cc = r + dr, c + dc
+        ok = (rr >= 0) & (rr < m) & (cc >= 0) & (cc < n)
+        pairs.append(np.stack([nan[ok], (rr + cc * m)[ok]], 1))
+    P = np.unique(np.sort(np.concatenate(pairs), 1), axis=0)
+    k = P.shape[0]
+    S = sp.csr_matrix((np.tile([1.0, -1.0], k), (np.repeat(np.arange(k), 2), P.ravel())), shape=(k, m * n))
+    known = np.flatnonzero(~np.isnan(flat))
+    rhs = -(S[:, known] @ flat[known])
+    Su = S[:, nan].tocsc()
+    x = spla.spsolve((Su.T @ Su).tocsc(), Su.T @ rhs)
+    flat[nan] = x
+    return flat.reshape((m, n), order="F")
+
+
+def init_u0(u, v):
+    """Init(u, v, Phi, x, y, 0) (func/Init.m:1-2 and :85-92): inpaint_nans(., 4) of the
+    search grids u, v (ny x nx) and U0 interleaved over the transposed grids (XList fastest)."""
+    ui, vi = inpaint_nans4(u).T.ravel(order="F"), inpaint_nans4(v).T.ravel(order="F")
+    U0 = np.empty(2 * ui.size)
+    U0[0::2], U0[1::2] = ui, vi
+    return U0

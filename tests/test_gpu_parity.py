@@ -467,6 +467,49 @@ def test_pinned_host_outputs_and_threaded_contexts(A, ctx, affine):
         ctx.local_icgn(1, coords, U0, 30, 1e-3, out=dict(outs[0], U=np.empty(2 * n, np.float32)))
 
 
+def test_inpaint_nans_and_init_parity(A, ctx):
+    """inpaint_nans(., 4) and Init(., 0) against the oracle's spring-system solve: scattered
+    NaNs, a block hole, border runs, a whole edge column; unchanged finite entries; the
+    device-tensor path; a grid without NaN; an all-NaN grid (no finite neighbour -> 0)."""
+    import torch
+
+    rng = np.random.default_rng(11)
+    for m, n in ((40, 55), (200, 200), (7, 3)):
+        G = rng.normal(size=(m, n)) * 3.0
+        G[rng.random(G.shape) < 0.1] = np.nan
+        G[m // 4:m // 2, n // 3:n // 2] = np.nan
+        G[0, : n // 2] = np.nan
+        G[:, -1] = np.nan
+        ref = O.inpaint_nans4(G)
+        got, info = ctx.inpaint_nans(G, info=True)
+        assert info[0] == int(np.isnan(G).sum()) and info[2] == 1, info
+        assert np.array_equal(got[np.isfinite(G)], G[np.isfinite(G)])
+        scale = np.abs(ref).max()
+        assert np.abs(got - ref).max() <= 1e-10 * scale, (m, n)
+        # device path, in place ((n, m) row-major tensor == column-major m x n)
+        t = torch.from_numpy(np.ascontiguousarray(G.T)).cuda()
+        ctx.inpaint_nans(t)
+        torch.cuda.synchronize()
+        assert np.abs(t.cpu().numpy().T - ref).max() <= 1e-10 * scale
+    clean = rng.normal(size=(9, 12))
+    assert np.array_equal(ctx.inpaint_nans(clean), clean)
+    assert np.array_equal(ctx.inpaint_nans(np.full((4, 5), np.nan)), np.zeros((4, 5)))
+    # Init: the search grids of a real search, with holes punched in
+    sc = synth.temporal_affine()
+    _load_raw(ctx, sc)
+    M, N = sc.ref.shape
+    r = ctx.integer_search([10, 10], [1, M], [1, N], 30, 16)
+    u, v = r["u"].copy(), r["v"].copy()
+    u[rng.random(u.shape) < 0.2] = np.nan
+    v[np.isnan(u)] = np.nan
+    u_in, v_in = u.copy(), v.copy()
+    U0 = ctx.init_u0(u, v)
+    ref = O.init_u0(u, v)
+    assert np.abs(U0 - ref).max() <= 1e-10 * np.abs(ref).max()
+    assert np.array_equal(u, u_in, equal_nan=True) and np.array_equal(v, v_in, equal_nan=True)
+    assert np.array_equal(A.Init(u, v, ctx=ctx), U0)
+
+
 def test_launch_counter_and_errors(A, ctx):
     before = ctx.launches
     ctx.triangulate(np.zeros((4, 4)) + 1.0, np.eye(3), np.eye(3), np.eye(3), [1.0, 0, 0])
