@@ -192,11 +192,14 @@ class StereoPipeline:
             c.set_stream(self.streams[k].cuda_stream)
         self.ev = {k: T.cuda.Event() for k in ("fork", "S", "L", "R")}
         n, g = self.n, self.nx * self.ny
+        # per pass: search grids, U0, the IC-GN results (U, F, codes; the per-subset Hessian
+        # H feeds only ALDIC's Subpb1 step, which this pipeline does not run, so it is not
+        # requested) and the grid-order Init output Ug
         self.buf = {}
         for k in ("S", "L", "R"):
             self.buf[k] = {"x": T.empty(g, **f64), "y": T.empty(g, **f64), "u": T.empty(g, **f64),
                            "v": T.empty(g, **f64), "phi": T.empty(g, **f64), "U0": T.empty(2 * n, **f64),
-                           "U": T.empty(2 * n, **f64), "F": T.empty(4 * n, **f64), "H": T.empty(21 * n, **f64),
+                           "U": T.empty(2 * n, **f64), "F": T.empty(4 * n, **f64),
                            "conv": T.empty(n, dtype=T.int32, device=device),
                            "mark": T.empty(n, dtype=T.uint8, device=device), "Ug": T.empty(2 * g, **f64)}
         self.coordsR = T.empty((2, n), **f64)
@@ -1083,8 +1086,10 @@ def e2e_measure(A, scene, P, steps, local_rank):
         imgs[k] = pinned(v.shape, v.dtype, order="F")
         imgs[k][...] = v
     ctx = {k: A.Context(local_rank) for k in ("S", "L", "R")}
+    # the step's results: U, F and the convergence codes (the per-subset Hessian H is an
+    # input of ALDIC's Subpb1 step only, which this pipeline does not run, so it is not read)
     out = {k: {**{nm: pinned(g) for nm in ("x", "y", "u", "v", "phi")},
-               "U": pinned(2 * n), "F": pinned(4 * n), "H": pinned(21 * n), "conv": pinned(n, np.int32)}
+               "U": pinned(2 * n), "F": pinned(4 * n), "conv": pinned(n, np.int32)}
            for k in ("S", "L", "R")}
     tri = [{"xyz": pinned(3 * n), "err": pinned(n)} for _ in range(2)]
     U0 = {k: pinned(2 * n) for k in ("S", "L", "R")}
@@ -1096,31 +1101,35 @@ def e2e_measure(A, scene, P, steps, local_rank):
     pairs = [pinned((n, 4), order="F") for _ in range(2)]
     gx, gy = [1, M], [1, N]
     grid_bytes = 5 * g * 8
-    icgn_out_bytes = (2 + 4 + 21) * n * 8 + n * 4
+    icgn_out_bytes = (2 + 4) * n * 8 + n * 4
 
-    def search(k, ref, cur, s):
+    def search(k, ref, cur, s, after=None):
         c, o = ctx[k], out[k]
         c.load_image_raw(0, imgs[ref], gx, gy, want_stats=False)
         c.load_image_raw(1, imgs[cur], gx, gy, want_stats=False)
         c.compute_gradients()
+        if after is not None:  # the temporal searches wait for the stereo search, as on the device
+            after.wait()
         c.integer_search([s, s], gx, gy, w, st, out=o)
         return o["u"].reshape((ny, nx), order="F"), o["v"].reshape((ny, nx), order="F")
 
     stereo_done = threading.Event()
+    search_done = threading.Event()
 
     def stereo():
         u, v = search("S", "L0", "R0", P["s_stereo"])
+        search_done.set()
         ctx["S"].init_u0(u, v, out=U0["S"])
         ctx["S"].local_icgn(1, crd, U0["S"], w, P["tol_stereo"], out=out["S"])
         stereo_done.set()
 
     def left():
-        u, v = search("L", "L0", "L1", P["s_temp"])
+        u, v = search("L", "L0", "L1", P["s_temp"], after=search_done)
         ctx["L"].init_u0(u, v, out=U0["L"])
         ctx["L"].local_icgn(1, crd, U0["L"], w, P["tol_temp"], out=out["L"])
 
     def right():
-        u, v = search("R", "R0", "R1", P["s_temp"])
+        u, v = search("R", "R0", "R1", P["s_temp"], after=search_done)
         stereo_done.wait()
         # right-camera mesh = left mesh + stereo match; initial guess: Init over the search
         # grid, then the nearest grid node of each right-image point
@@ -1137,6 +1146,7 @@ def e2e_measure(A, scene, P, steps, local_rank):
     def one():
         nonlocal conv_total
         stereo_done.clear()
+        search_done.clear()
         for f in [pool.submit(fn) for fn in (stereo, left, right)]:
             f.result()
         US, UL, UR = (out[k]["U"].reshape(n, 2) for k in ("S", "L", "R"))
