@@ -675,11 +675,12 @@ __global__ void __launch_bounds__(TileShape<ST, W1, TI, DBC>::NT, 1)
     p_g[q] = make_int2(r_aoff[q % TI], p_ok[q] ? r_na[q % TI] : 0);
   }
   // ---- f tile, centred ----
+  // consecutive threads take consecutive tile rows x: contiguous in the column-major image
   for (int idx = tid; idx < FR * FCP; idx += NT) {
-    const int x = idx / FCP, c = idx % FCP;
+    const int x = idx % FR, c = idx / FR;
     float v = 0.f;
     if (c < FC && X0 + x < a.M && Y0 + c < a.N) v = __ldg(a.f + (size_t)(X0 + x) + (size_t)(Y0 + c) * a.M) - cf;
-    Ft[idx] = v;
+    Ft[x * FCP + c] = v;
   }
 
   // pass-2 roles and running first maxima
@@ -699,11 +700,11 @@ __global__ void __launch_bounds__(TileShape<ST, W1, TI, DBC>::NT, 1)
     // g buffer for this chunk: ring rows 0..FR-1 = tile rows DA0 + rel, columns from db = DA0 + dbc
     const int gy0 = Y0 + DA0 + dbc;
     for (int idx = tid; idx < FR * GCP; idx += NT) {
-      const int rel = idx / GCP, col = idx % GCP;
+      const int rel = idx % FR, col = idx / FR;  // consecutive threads: consecutive image rows
       const int x = X0 + DA0 + rel, y = gy0 + col;
       float v = 0.f;
       if (col < GC && x >= 0 && x < a.M && y >= 0 && y < a.N) v = __ldg(a.g + (size_t)x + (size_t)y * a.M);
-      Gt[idx] = v;
+      Gt[rel * GCP + col] = v;
     }
     for (int idx = FR * GCP + tid; idx < kRing * GCP; idx += NT) Gt[idx] = 0.f;
     __syncthreads();
