@@ -61,30 +61,31 @@ __global__ void __launch_bounds__(kInitThreads) inpaint_springs_kernel(double* _
   __shared__ int s_warp[32];
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
   const int mn = m * n;
-  if (tid == 0) s_count = 0;
-  __syncthreads();
-  // ---- compaction of the NaN entries, in grid order ----
-  for (int base = 0; base < mn; base += blockDim.x) {
-    const int g = base + tid;
-    const bool unk = g < mn && isnan(A[g]);
-    const unsigned bal = __ballot_sync(0xffffffffu, unk);
-    if (lane == 0) s_warp[wid] = __popc(bal);
-    __syncthreads();
-    int before = s_count;
-    for (int k = 0; k < wid; ++k) before += s_warp[k];
-    const int pos = before + __popc(bal & ((1u << lane) - 1u));
-    if (g < mn) map[g] = unk ? pos : -1;
-    if (unk) list[pos] = g;
-    __syncthreads();
-    if (tid == 0) {
-      int t = 0;
-      for (int k = 0; k < nw; ++k) t += s_warp[k];
-      s_count += t;
-    }
-    __syncthreads();
+  // ---- compaction of the NaN entries, in grid order: every thread counts a contiguous
+  // range, one block scan gives the offsets, the same ranges are written ----
+  const int per = (mn + (int)blockDim.x - 1) / (int)blockDim.x;
+  const int g0 = min(mn, tid * per), g1 = min(mn, g0 + per);
+  int cnt = 0;
+  for (int g = g0; g < g1; ++g) cnt += isnan(A[g]) ? 1 : 0;
+  int incl = cnt;  // inclusive scan within the warp
+  for (int off = 1; off < 32; off <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, incl, off);
+    if (lane >= off) incl += y;
   }
+  if (lane == 31) s_warp[wid] = incl;
+  __syncthreads();
+  if (tid == 0) {
+    int run = 0;
+    for (int k = 0; k < nw; ++k) {
+      const int t = s_warp[k];
+      s_warp[k] = run;
+      run += t;
+    }
+    s_count = run;
+  }
+  __syncthreads();
   const int nu = s_count;
-  if (nu == 0) {
+  if (nu == 0) {  // nothing to fill (the common case): one read of the grid
     if (tid == 0) {
       status[0] = 0;
       status[1] = 0;
@@ -92,6 +93,13 @@ __global__ void __launch_bounds__(kInitThreads) inpaint_springs_kernel(double* _
     }
     return;
   }
+  int pos = s_warp[wid] + incl - cnt;  // exclusive offset of this thread's range
+  for (int g = g0; g < g1; ++g) {
+    const bool unk = isnan(A[g]);
+    map[g] = unk ? pos : -1;
+    if (unk) list[pos++] = g;
+  }
+  __syncthreads();
   // ---- right-hand side and the CG start x = 0, r = p = b ----
   double bb_local = 0.0;
   for (int u = tid; u < nu; u += blockDim.x) {
