@@ -18,7 +18,7 @@ ALDIC_ERR_STATE = 4
 U8, U16, F32, F64 = 0, 1, 2, 3
 SLOT_REF, SLOT_DEF = 0, 1
 UNIFORM, QUADTREE = 0, 1
-# iterations the one-warp solver pass gives a subset before the 4-warp pass restarts it, when
+# iterations the one-warp solver pass gives a subset before the multi-warp pass restarts it, when
 # aldic_set_iteration_cap has not been called (kDefaultWarpCap in csrc/kernels.h)
 DEFAULT_ITERATION_CAP = 8
 

@@ -152,7 +152,7 @@ class Context:
         return int(self.lib.aldic_launch_count(self.h))
 
     def set_iteration_cap(self, cap):
-        """Iterations the one-warp solver pass spends on a subset before the 4-warp pass
+        """Iterations the one-warp solver pass spends on a subset before the multi-warp pass
         restarts it (default 8)."""
         self._check(self.lib.aldic_set_iteration_cap(self.h, int(cap)), "aldic_set_iteration_cap")
 

@@ -26,7 +26,7 @@
 namespace aldic {
 
 constexpr int kNT = 128;  // threads per solve CTA
-constexpr int kSlowSubset = 2;  // queue-1 flag of a subset restarted by the 4-warp pass
+constexpr int kSlowSubset = 2;  // queue-1 flag of a subset restarted by the multi-warp pass
 
 struct SolveCtl {
   double P[6];
@@ -272,7 +272,7 @@ __global__ void __launch_bounds__(kNT) icgn_solve_kernel(IcgnArgs a, int bucket)
     const int* q = a.queue + 3 * ((long long)bucket * a.n + qi);
     const long long t = q[0];
     const int w = q[1];
-    if (q[2] == kSlowSubset) continue;  // restarted by the 4-warp pass
+    if (q[2] == kSlowSubset) continue;  // restarted by the multi-warp pass
     const bool masked = q[2] != 0;
     const int W1 = w + 1, npx = W1 * W1;
     const int half = w / 2;
@@ -599,12 +599,13 @@ __global__ void __launch_bounds__(kNT) icgn_solve_kernel(IcgnArgs a, int bucket)
 // default; 6-12 measured within 1 % of each other on the stereo pass, 4 and 24 slower): the
 // few subsets that need more (most never converge and run to max_iter) would otherwise
 // keep single warps running long after the rest of the grid.  They go to queue 1 flagged
-// kSlowSubset and restart from the beginning in the 4-warp pass (NW = 4), which runs each
-// iteration about four times faster.  A quadtree subset that meets an exact zero in g (a
+// kSlowSubset and restart from the beginning in the multi-warp pass (NW = kSlowNW = 2), whose
+// iterations run about twice as fast; two warps measured faster over the whole stereo step
+// than four or eight, which finish each subset sooner but crowd out the passes beside them.  A quadtree subset that meets an exact zero in g (a
 // masked deformed image) needs the g-region flood fill: it is handed to the general kernel
 // through queue 1 and restarted there.
 constexpr int kWT = 256;  // threads per CTA: 8 / NW subset groups
-constexpr int kSlowNW = 4;  // warps per subset in the pass that restarts the slow subsets
+constexpr int kSlowNW = 2;  // warps per subset in the pass that restarts the slow subsets
 
 template <int NW>
 __device__ __forceinline__ void group_bar(int id) {
@@ -801,7 +802,7 @@ __global__ void __launch_bounds__(kWT, 2) icgn_group_kernel(IcgnArgs a) {
     double normNew = 1.0, normAbs = 1.0, normInit = 0.0, znssd = ALDIC_NAN;
     int step = 0, status = 0, requeue = -1;
     while (step <= a.max_iter && normNew > a.tol && normAbs > a.tol) {
-      if (!SLOW && step >= a.warp_cap) {  // a slow subset: restarted by the 4-warp pass
+      if (!SLOW && step >= a.warp_cap) {  // a slow subset: restarted by the multi-warp pass
         requeue = kSlowSubset;
         break;
       }

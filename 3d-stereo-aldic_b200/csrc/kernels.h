@@ -26,7 +26,7 @@ struct IcgnArgs {
   int winsize;
   double tol;
   int max_iter;  // 100, or 30 for the epipolar variant
-  int warp_cap;  // iterations the one-warp pass spends on a subset before the 4-warp pass restarts it
+  int warp_cap;  // iterations the one-warp pass spends on a subset before the multi-warp pass restarts it
   int crop;      // gradient offset: 3 (DfCropWidth) or 4 (DfAxis start)
   double* U;     // 2n
   double* F;     // 4n

@@ -178,7 +178,7 @@ int aldic_local_icgn_noalloc(int variant, const float* ref, const float* def, co
  * compute-bound kernels are reported against.  Not part of the reference. */
 int aldic_measure_fp32_peak(aldic_ctx* ctx, double* tflops);
 /* Iterations the one-warp-per-subset solver pass of aldic_local_icgn / aldic_subpb1 spends
- * on a subset before a 4-warp pass restarts it from its initial guess (default 8, 1..1000).
+ * on a subset before a multi-warp pass restarts it from its initial guess (default 8, 1..1000).
  * Results do not depend on it beyond FP32 summation order; it trades the tail of slow
  * subsets against repeated work.  A tuning setting; not part of the reference. */
 int aldic_set_iteration_cap(aldic_ctx* ctx, int cap);

@@ -264,7 +264,7 @@ def test_subpb1_quadtree_parity(ctx, hole):
 def test_subpb1_quadtree_mixed_windows_and_slow_subsets(A, ctx, hole):
     # per-subset windows 16 / 24 / 32 (queue 0 holds only the nominal size; the others are
     # unmasked queue-1 subsets solved by the warp-group passes); with an iteration cap of 1
-    # every subset needing more than one iteration restarts in the 4-warp pass
+    # every subset needing more than one iteration restarts in the multi-warp pass
     sc = hole
     M, N = sc.ref.shape
     ctx.load_image_raw(0, sc.ref, [1, M], [1, N], mask=sc.mask)
@@ -302,7 +302,7 @@ def test_subpb1_quadtree_mixed_windows_and_slow_subsets(A, ctx, hole):
 
 def test_local_icgn_slow_subsets_restart(A, ctx, affine):
     # with an iteration cap of 1 every subset that needs a second iteration is restarted by
-    # the 4-warp pass; codes and displacements still match the oracle
+    # the multi-warp pass; codes and displacements still match the oracle
     _load_raw(ctx, affine)
     M, N = affine.ref.shape
     f, g = ctx.get_state(0), ctx.get_state(1)
