@@ -606,6 +606,7 @@ __global__ void __launch_bounds__(kNT) icgn_solve_kernel(IcgnArgs a, int bucket)
 // through queue 1 and restarted there.
 constexpr int kWT = 256;  // threads per CTA: 8 / NW subset groups
 constexpr int kSlowNW = 2;  // warps per subset in the pass that restarts the slow subsets
+constexpr int kSub1SlowNW = 4;  // the same for the Subpb1 step
 
 template <int NW>
 __device__ __forceinline__ void group_bar(int id) {
@@ -1664,11 +1665,11 @@ int launch_subpb1(const Sub1Args& a, int wmax_x, int wmax_y, cudaStream_t st) {
     if (grid > need) grid = need;
     subpb1_group_kernel<1, false><<<(unsigned)grid, kWT, 0, st>>>(a);
     per_sm = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, subpb1_group_kernel<4, true>, kWT, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, subpb1_group_kernel<kSub1SlowNW, true>, kWT, 0);
     grid = (long long)sms * (per_sm < 1 ? 1 : per_sm);
-    const long long need4 = (a.n + 1) / 2;
-    if (grid > need4) grid = need4;
-    subpb1_group_kernel<4, true><<<(unsigned)grid, kWT, 0, st>>>(a);
+    const long long need_slow = (a.n + kWT / (32 * kSub1SlowNW) - 1) / (kWT / (32 * kSub1SlowNW));
+    if (grid > need_slow) grid = need_slow;
+    subpb1_group_kernel<kSub1SlowNW, true><<<(unsigned)grid, kWT, 0, st>>>(a);
     launches += 2;
   }
   {  // masked subsets and restarts: the general kernel on queue 1
