@@ -34,10 +34,18 @@ constexpr int kRing = 128; // rows of the circular g buffer
 // rows then hit 8 distinct 16-byte bank groups per quarter warp.
 constexpr int pad4odd(int n) { return ((n + 3) / 4 % 2 == 1) ? (n + 3) / 4 * 4 : (n + 3) / 4 * 4 + 4; }
 
+// Dynamic shared memory of a tile: f tile, g ring, RB (the same sums as TileShape below; a
+// plain function so that sizing candidate tiles instantiates no shape).
+constexpr size_t tile_dyn_smem(int ST, int W1, int TI, int DBC) {
+  return sizeof(float) * ((size_t)((TI - 1) * ST + W1) * pad4odd((kTJ - 1) * ST + W1) +
+                          (size_t)kRing * pad4odd((kTJ - 1) * ST + W1 + DBC + 2) +
+                          (size_t)kTJ * DBC * pad4odd((TI - 1) * ST + W1));
+}
+
 // DBC shift columns per chunk, in groups of 8 (one pass-1 thread group of 128 rows each).
 template <int ST, int W1, int TI, int DBC>
 struct TileShape {
-  static constexpr int Q = W1 / ST, REM = W1 % ST;
+  static constexpr int Q = W1 / ST;
   static constexpr int NT = DBC / 8 * 128;           // threads per CTA
   static constexpr int FR = (TI - 1) * ST + W1;      // tile rows
   static constexpr int FC = (kTJ - 1) * ST + W1;     // tile columns
@@ -48,6 +56,7 @@ struct TileShape {
   static constexpr int NSUB = TI * kTJ;
   static constexpr size_t smem_bytes =
       sizeof(float) * ((size_t)FR * FCP + (size_t)kRing * GCP + (size_t)kTJ * DBC * FRP);
+  static_assert(smem_bytes == tile_dyn_smem(ST, W1, TI, DBC), "one shared-memory size");
   static_assert(DBC % 8 == 0 && DBC >= 16, "chunks hold whole groups of 8 shift columns");
   static_assert(Q >= 1, "step must not exceed the window");
   static_assert(FR <= kRing - 1, "tile rows must leave one free ring row");
@@ -56,7 +65,7 @@ struct TileShape {
 // Shared memory per CTA: the dynamic buffers plus the static per-subset arrays (a bound).
 template <int ST, int W1, int TI, int DBC>
 constexpr size_t tile_total_smem() {
-  return TileShape<ST, W1, TI, DBC>::smem_bytes + (size_t)TI * kTJ * 64 + 1024;
+  return tile_dyn_smem(ST, W1, TI, DBC) + (size_t)TI * kTJ * 64 + 1024;
 }
 
 // Subset rows per tile: as many as fit 127 tile rows and the 227 KB of shared memory a CTA
