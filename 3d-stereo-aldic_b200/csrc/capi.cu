@@ -517,7 +517,7 @@ static int icgn_common(aldic_ctx* c, int variant, int64_t n, const double* coord
   Arg az{znssd, znssd ? (size_t)n * 8 : 0, true, nullptr};
   // the work queue comes from the arena too: reserve room for it with the staged arguments
   c->arena.used = 0;
-  rc = arena_reserve(c, qbytes + 4096 + (size_t)n * (2 + 2 + 2 + 4 + 21 + 1 + 1) * 8 + 8192);
+  rc = arena_reserve(c, qbytes + 4096 + (size_t)n * (2 + 2 + 2 + 4 + 21 + 1 + 1 + 8) * 8 + 8192);
   if (rc) return rc;
   rc = stage(c, {&ac, &au0, &au, &af, &ah, &acv, &am, &az});
   if (rc) return rc;
@@ -540,6 +540,7 @@ static int icgn_common(aldic_ctx* c, int variant, int64_t n, const double* coord
   a.znssd = (double*)az.dev;
   a.queue = (int*)arena_take(c, qbytes);
   a.qcount = c->qcount;
+  a.carry = (double*)arena_take(c, (size_t)n * 8 * sizeof(double));
   return finish(c, launch_icgn(a, wmax, c->stream));
 }
 

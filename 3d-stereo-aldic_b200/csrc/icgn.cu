@@ -599,8 +599,9 @@ __global__ void __launch_bounds__(kNT) icgn_solve_kernel(IcgnArgs a, int bucket)
 // default; 6-12 measured within 1 % of each other on the stereo pass, 4 and 24 slower): the
 // few subsets that need more (most never converge and run to max_iter) would otherwise
 // keep single warps running long after the rest of the grid.  They go to queue 1 flagged
-// kSlowSubset and restart from the beginning in the multi-warp pass (NW = kSlowNW = 2), whose
-// iterations run about twice as fast; two warps measured faster over the whole stereo step
+// kSlowSubset and continue in the multi-warp pass (NW = kSlowNW = 2) from the state the warp
+// pass stored (P, the first norm, the step; without a state buffer they restart from their
+// initial guess), whose iterations run about twice as fast; two warps measured faster over the whole stereo step
 // than four or eight, which finish each subset sooner but crowd out the passes beside them.  A quadtree subset that meets an exact zero in g (a
 // masked deformed image) needs the g-region flood fill: it is handed to the general kernel
 // through queue 1 and restarted there.
@@ -802,8 +803,15 @@ __global__ void __launch_bounds__(kWT, 2) icgn_group_kernel(IcgnArgs a) {
     double P[6] = {0.0, 0.0, 0.0, 0.0, epi ? 0.0 : a.U0[2 * t], epi ? 0.0 : a.U0[2 * t + 1]};
     double normNew = 1.0, normAbs = 1.0, normInit = 0.0, znssd = ALDIC_NAN;
     int step = 0, status = 0, requeue = -1;
+    if (SLOW && a.carry) {  // continue from where the warp pass stopped: P, the first norm, the step
+      const double* cs = a.carry + 8 * t;
+#pragma unroll
+      for (int k = 0; k < 6; ++k) P[k] = cs[k];
+      normInit = cs[6];
+      step = (int)cs[7];
+    }
     while (step <= a.max_iter && normNew > a.tol && normAbs > a.tol) {
-      if (!SLOW && step >= a.warp_cap) {  // a slow subset: restarted by the multi-warp pass
+      if (!SLOW && step >= a.warp_cap) {  // a slow subset: continued by the multi-warp pass
         requeue = kSlowSubset;
         break;
       }
@@ -923,8 +931,9 @@ __global__ void __launch_bounds__(kWT, 2) icgn_group_kernel(IcgnArgs a) {
       }
       if (epi) znssd = 2.0 - 2.0 * (v[10] - meanf * v[6]) / (bf * bgn);
       double b[6];
+      const double ibgn = 1.0 / bgn;  // one FP64 division per iteration instead of six
 #pragma unroll
-      for (int k = 0; k < 6; ++k) b[k] = bf * (AB[k] - (v[k] - meang * AB[6 + k]) / bgn);
+      for (int k = 0; k < 6; ++k) b[k] = bf * (AB[k] - (v[k] - meang * AB[6 + k]) * ibgn);
       double dP[6];
 #pragma unroll
       for (int i = 0; i < 6; ++i) {
@@ -952,8 +961,15 @@ __global__ void __launch_bounds__(kWT, 2) icgn_group_kernel(IcgnArgs a) {
       }
     }
     if (gt == 0) {
+      if (requeue == kSlowSubset && a.carry) {
+        double* cs = a.carry + 8 * t;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) cs[k] = P[k];
+        cs[6] = normInit;
+        cs[7] = (double)step;
+      }
       if (requeue >= 0) {
-        // restart this subset in a later pass (they run after this kernel).  A queue-0
+        // hand this subset to a later pass (they run after this kernel).  A queue-0
         // subset is appended to queue 1 (at most one entry each: queue 1 never holds more
         // than n); a queue-1 subset is re-flagged in place.
         if (SLOW) {

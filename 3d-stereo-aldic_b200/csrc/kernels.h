@@ -36,6 +36,7 @@ struct IcgnArgs {
   double* znssd; // n (epipolar)
   int* queue;    // 2 buckets x n x 3 ints
   int* qcount;   // 4: queue counts of the 2 buckets, work counters of the 2 warp-group passes
+  double* carry; // n x 8 or null: where the warp pass left a subset it hands to the multi-warp pass
 };
 
 struct Sub1Args {

@@ -122,6 +122,7 @@ extern "C" int aldic_local_icgn_noalloc(int variant, const float* ref, const flo
   a.znssd = nullptr;
   a.queue = scratch;
   a.qcount = scratch + 2 * kMaxSubsets * 3;  // cleared by launch_icgn before the classify kernel
+  a.carry = nullptr;  // slow subsets restart from their initial guess (no state buffer here)
   aldic::launch_icgn(a, wmax, static_cast<cudaStream_t>(stream));
   return cudaGetLastError() == cudaSuccess ? ALDIC_OK : ALDIC_ERR_CUDA;
 }
