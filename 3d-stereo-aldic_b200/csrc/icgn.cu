@@ -640,8 +640,11 @@ __device__ __forceinline__ void group_sum(double (&v)[K], double* red, int gw, i
   group_bar<NW>(bar);
 }
 
+// The one-warp pass is latency-bound on its image reads: three CTAs per SM (24 warps, 80
+// registers with a few spills) measured 12 % faster than two (128 registers, no spills);
+// four (64 registers) spill too much.
 template <int NW, bool SLOW>
-__global__ void __launch_bounds__(kWT, 2) icgn_group_kernel(IcgnArgs a) {
+__global__ void __launch_bounds__(kWT, NW == 1 ? 3 : 2) icgn_group_kernel(IcgnArgs a) {
   constexpr int NG = kWT / (32 * NW);  // subset groups per CTA
   constexpr int GT = 32 * NW;          // threads per group
   __shared__ double s_aug[NG][72];     // 6 x 12 row-major [H | I] -> [I | H^-1]
