@@ -182,7 +182,7 @@ __global__ void ring_rows_kernel(SearchArgs a, double* __restrict__ rr) {
 // One warp per subset: template mean and norm, the window sums of the ring of partial
 // windows, the largest window variance sum over the crop (normxcorr2 zero threshold) and
 // validity; writes x, y and the NaN outputs of invalid subsets.
-__global__ void subset_prep_kernel(SearchArgs a, const double* __restrict__ H, const double* __restrict__ rr,
+__global__ void __launch_bounds__(256, 4) subset_prep_kernel(SearchArgs a, const double* __restrict__ H, const double* __restrict__ rr,
                                    SubsetPrm* __restrict__ prm, float2* __restrict__ ringv) {
   const int lane = threadIdx.x & 31;
   const long long t = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
@@ -892,7 +892,9 @@ __global__ void __launch_bounds__(TileShape<ST, W1, TI, DBC>::NT, 1)
 }
 
 // FP64 refit + findpeak at the argmax of every valid subset (one warp per subset).
-__global__ void __launch_bounds__(256) subset_refit_kernel(SearchArgs a, const SubsetPrm* __restrict__ prm,
+// Three CTAs per SM (80 registers) and, for subset_prep_kernel, four (64): both warp-per-subset
+// FP64 kernels are latency-bound, and the extra warps measured 0.2 ms off the stereo step.
+__global__ void __launch_bounds__(256, 3) subset_refit_kernel(SearchArgs a, const SubsetPrm* __restrict__ prm,
                                                            const int* __restrict__ best) {
   const long long t = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
   if (t >= (long long)a.nx * a.ny) return;
