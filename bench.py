@@ -24,6 +24,7 @@ import json
 import os
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -122,8 +123,7 @@ def tile_flops(M, N, w, step, s0, s1):
 class ClockSampler:
     def __init__(self, gpu_index):
         self.p = None
-        self.path = os.path.join(ROOT, "gpurun_out" if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else ".",
-                                 f".clocks_{os.getpid()}.csv")
+        self.path = os.path.join(tempfile.gettempdir(), f"aldic_clocks_{os.getpid()}.csv")
         try:
             self.p = subprocess.Popen(
                 ["nvidia-smi", f"--id={gpu_index}",
