@@ -319,9 +319,10 @@ class Context:
         self._check(rc, "aldic_inpaint_nans")
         return (a, tuple(nfo)) if info else a
 
-    def init_u0(self, u, v, out=None):
-        """Init(u, v, Phi, x, y, 0): inpaint the search grids (ny x nx, left unchanged) and
-        return U0 (2 nx ny, mesh order), or fill `out` (a CUDA tensor or host array)."""
+    def init_u0(self, u, v, out=None, index=0):
+        """Init(u, v, Phi, x, y, index): inpaint the search grids (ny x nx, left unchanged;
+        index 1 adds the spring outlier passes) and return U0 (2 nx ny, mesh order), or fill
+        `out` (a CUDA tensor or host array)."""
         k = _Keep()
         if _is_torch(u):
             if u.dim() != 2:
@@ -334,7 +335,7 @@ class Context:
         else:
             U0, op = out, k.dst(out, np.float64, 2 * nx * ny)
         rc = self.lib.aldic_init_u0(self.h, int(ny), int(nx), k.ptr(u, np.float64, numel=nx * ny),
-                                    k.ptr(v, np.float64, numel=nx * ny), op)
+                                    k.ptr(v, np.float64, numel=nx * ny), int(index), op)
         self._check(rc, "aldic_init_u0")
         return U0
 
@@ -406,13 +407,11 @@ def ba_interp2_spline(F, X, Y, method="cubicspline", ctx: Context | None = None)
 
 
 def Init(u, v, Phi=None, x=None, y=None, index=0, ctx: Context | None = None):
-    """Init(u, v, Phi, x, y, index) (func/Init.m).  index 0 (the stereo and temporal
-    drivers' call): inpaint_nans(., 4) of u and v and U0 in mesh order.  The spring outlier
-    passes of index 1 are not built."""
-    if index != 0:
-        raise AldicError("Init index 1 (spring outlier passes) is not built; the drivers call index 0")
+    """Init(u, v, Phi, x, y, index) (func/Init.m): inpaint_nans(., 4) of u and v, with
+    index 1 the three spring outlier passes, and U0 in mesh order.  The stereo and temporal
+    drivers call index 0."""
     ctx = ctx or default_context()
-    return ctx.init_u0(u, v)
+    return ctx.init_u0(u, v, index=index)
 
 
 def funIntegerSearch(f, g, tempSizeOfSearchRegion, gridx, gridy, winsize, winstepsize, tempNoOfInitPt=0,

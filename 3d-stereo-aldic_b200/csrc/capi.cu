@@ -679,8 +679,9 @@ int aldic_inpaint_nans(aldic_ctx* c, int m, int n, double* A, int32_t* info) {
   return finish(c, l);
 }
 
-int aldic_init_u0(aldic_ctx* c, int ny, int nx, const double* u, const double* v, double* U0) {
+int aldic_init_u0(aldic_ctx* c, int ny, int nx, const double* u, const double* v, int index, double* U0) {
   if (!c) return ALDIC_ERR_ARG;
+  if (index != 0 && index != 1) return fail(c, ALDIC_ERR_ARG, "Init index %d (0 or 1)", index);
   if (ny < 0 || nx < 0) return fail(c, ALDIC_ERR_ARG, "grid size %d x %d", ny, nx);
   if ((long long)ny * nx > (1LL << 30)) return fail(c, ALDIC_ERR_ARG, "grid of %d x %d entries too large", ny, nx);
   if (ny == 0 || nx == 0) return ALDIC_OK;
@@ -695,7 +696,7 @@ int aldic_init_u0(aldic_ctx* c, int ny, int nx, const double* u, const double* v
   size_t need = 0;
   for (Arg* a : {&au, &av, &ao})
     if (!is_device_ptr(a->user)) need += ((a->bytes + 255) & ~size_t(255)) + 256;
-  need += 2 * (bytes + 256) + inpaint_scratch_bytes(g) + 512;
+  need += 4 * (bytes + 256) + inpaint_scratch_bytes(g) + 512;
   int rc = arena_reserve(c, need);
   if (rc) return rc;
   for (Arg* a : {&au, &av, &ao}) {
@@ -717,6 +718,17 @@ int aldic_init_u0(aldic_ctx* c, int ny, int nx, const double* u, const double* v
   int* status = (int*)arena_take(c, 64);
   int l = launch_inpaint(wu, ny, nx, scratch, status, c->stream);
   l += launch_inpaint(wv, ny, nx, scratch, status, c->stream);
+  if (index == 1) {  // the three spring outlier passes, each on a copy of the pass's input
+    double* tu = (double*)arena_take(c, bytes);
+    double* tv = (double*)arena_take(c, bytes);
+    for (int mode = 0; mode < 3; ++mode) {
+      CK(cudaMemcpyAsync(tu, wu, bytes, cudaMemcpyDeviceToDevice, c->stream));
+      CK(cudaMemcpyAsync(tv, wv, bytes, cudaMemcpyDeviceToDevice, c->stream));
+      l += launch_spring_pass(tu, tv, wu, wv, ny, nx, mode, c->stream);
+      l += launch_inpaint(wu, ny, nx, scratch, status, c->stream);
+      l += launch_inpaint(wv, ny, nx, scratch, status, c->stream);
+    }
+  }
   l += launch_interleave_u0(wu, wv, ny, nx, (double*)ao.dev, c->stream);
   return finish(c, l);
 }

@@ -177,6 +177,107 @@ __global__ void interleave_u0_kernel(const double* __restrict__ u, const double*
   U0[2 * i + 1] = v[g];
 }
 
+// MATLAB std(x, 'omitnan') of k values in order (mean first, then the squared deviations),
+// every operation rounded on its own as MATLAB's are (no fused multiply-adds).
+__device__ __forceinline__ double std_omitnan(const double* x, int k) {
+  double m = 0.0;
+  int c = 0;
+  for (int t = 0; t < k; ++t)
+    if (!isnan(x[t])) {
+      m = __dadd_rn(m, x[t]);
+      ++c;
+    }
+  if (c < 2) return c == 1 ? 0.0 : (double)NAN;
+  m = __ddiv_rn(m, (double)c);
+  double ss = 0.0;
+  for (int t = 0; t < k; ++t)
+    if (!isnan(x[t])) {
+      const double d = __dsub_rn(x[t], m);
+      ss = __dadd_rn(ss, __dmul_rn(d, d));
+    }
+  return __dsqrt_rn(__ddiv_rn(ss, (double)(c - 1)));
+}
+
+// One spring outlier pass of Init index 1 (func/Init.m:31-62, :76-105, :119-150) over the
+// interior nodes of the m x n grids: ut, vt are the pass's (inpainted) inputs, ui, vi their
+// copies that receive the NaN marks (a node failing the test for u or for v is set NaN in
+// both, with its neighbourhood; overlapping marks write the same NaN).  mode 0: the 8
+// neighbours, average (sum of the 4 edge neighbours / 8 + sum of the 4 corners / 16) / (3/4),
+// 3 standard deviations, 8-neighbourhood marked; mode 1: the 4 edge neighbours, their mean,
+// 2 standard deviations, 4-neighbourhood; mode 2: as mode 0 with 2 standard deviations.
+__global__ void spring_mark_kernel(const double* __restrict__ ut, const double* __restrict__ vt, double* ui,
+                                   double* vi, int m, int n, int mode) {
+  const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (m < 3 || n < 3 || idx >= (long long)(m - 2) * (n - 2)) return;
+  const int i = 1 + (int)(idx % (m - 2)), j = 1 + (int)(idx / (m - 2));
+  const long long g = i + (long long)j * m;
+  // neighbour order of the reference: (i-1,j) (i+1,j) (i,j-1) (i,j+1) (i-1,j-1) (i+1,j-1)
+  // (i+1,j+1) (i-1,j+1)
+  const long long nb[8] = {g - 1, g + 1, g - m, g + m, g - 1 - m, g + 1 - m, g + 1 + m, g - 1 + m};
+  const double kk = mode == 0 ? 3.0 : 2.0;
+  bool bad = false;
+  for (int comp = 0; comp < 2; ++comp) {
+    const double* t = comp ? vt : ut;
+    double x[8];
+    for (int q = 0; q < 8; ++q) x[q] = t[nb[q]];
+    double avg, sd;
+    if (mode == 1) {
+      double acc = 0.0;
+      int c = 0;
+      for (int q = 0; q < 4; ++q)
+        if (!isnan(x[q])) {
+          acc = __dadd_rn(acc, x[q]);
+          ++c;
+        }
+      avg = c ? __ddiv_rn(acc, (double)c) : (double)NAN;
+      sd = std_omitnan(x, 4);
+    } else {
+      const double se = __dadd_rn(__dadd_rn(__dadd_rn(x[0], x[1]), x[2]), x[3]);
+      const double sc = __dadd_rn(__dadd_rn(__dadd_rn(x[4], x[5]), x[6]), x[7]);
+      avg = __ddiv_rn(__dadd_rn(__dmul_rn(0.125, se), __dmul_rn(0.0625, sc)), 0.75);
+      sd = std_omitnan(x, 8);
+    }
+    const double err = __dsub_rn(fabs(__dsub_rn(t[g], avg)), __dmul_rn(kk, sd));
+    if (err > 0.0) bad = true;
+  }
+  if (!bad) return;
+  const int cnt = mode == 1 ? 4 : 8;
+  ui[g] = (double)NAN;
+  vi[g] = (double)NAN;
+  for (int q = 0; q < cnt; ++q) {
+    ui[nb[q]] = (double)NAN;
+    vi[nb[q]] = (double)NAN;
+  }
+}
+
+// The border rows and columns of both grids set NaN (func/Init.m:62-63 and the same lines
+// after each pass).
+__global__ void border_nan_kernel(double* ui, double* vi, int m, int n) {
+  const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long per = 2LL * m + 2LL * n;
+  if (idx >= per) return;
+  long long g;
+  if (idx < m) g = idx;                                          // column 1
+  else if (idx < 2LL * m) g = (idx - m) + (long long)(n - 1) * m;  // column n
+  else if (idx < 2LL * m + n) g = (idx - 2LL * m) * m;            // row 1
+  else g = (m - 1) + (idx - 2LL * m - n) * m;                     // row m
+  ui[g] = (double)NAN;
+  vi[g] = (double)NAN;
+}
+
+int launch_spring_pass(const double* ut, const double* vt, double* ui, double* vi, int m, int n, int mode,
+                       cudaStream_t st) {
+  const long long interior = (m >= 3 && n >= 3) ? (long long)(m - 2) * (n - 2) : 0;
+  int l = 0;
+  if (interior > 0) {
+    spring_mark_kernel<<<(unsigned)((interior + 255) / 256), 256, 0, st>>>(ut, vt, ui, vi, m, n, mode);
+    ++l;
+  }
+  const long long per = 2LL * m + 2LL * n;
+  border_nan_kernel<<<(unsigned)((per + 255) / 256), 256, 0, st>>>(ui, vi, m, n);
+  return l + 1;
+}
+
 size_t inpaint_scratch_bytes(long long mn) { return (size_t)mn * (2 * sizeof(int) + 4 * sizeof(double)) + 1024; }
 
 int launch_inpaint(double* A, int m, int n, void* scratch, int* status, cudaStream_t st) {

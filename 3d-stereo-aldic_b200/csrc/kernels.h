@@ -106,6 +106,8 @@ struct CamPair {
 size_t inpaint_scratch_bytes(long long mn);
 int launch_inpaint(double* A, int m, int n, void* scratch, int* status, cudaStream_t st);
 int launch_interleave_u0(const double* u, const double* v, int ny, int nx, double* U0, cudaStream_t st);
+int launch_spring_pass(const double* ut, const double* vt, double* ui, double* vi, int m, int n, int mode,
+                       cudaStream_t st);
 int launch_triangulate(long long n, const double* pairs, const CamPair& cams, double* xyz, double* err,
                        cudaStream_t st);
 int launch_fp32_probe(int blocks, int threads, int iters, float* out, bool packed, cudaStream_t st);

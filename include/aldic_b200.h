@@ -139,10 +139,14 @@ int aldic_epipolar_icgn(aldic_ctx* ctx, int64_t n, const double* pts, int winsiz
  * 1 when the residual target was met; passing it makes the call wait for the device. */
 int aldic_inpaint_nans(aldic_ctx* ctx, int m, int n, double* A, int32_t* info);
 
-/* Init(u, v, Phi, x, y, 0) (func/Init.m:1-2,85-92): inpaint_nans(., 4) of the search's
- * u and v grids (ny x nx column-major, as aldic_integer_search returns them; left
- * unchanged) and U0 (2 nx ny) interleaved [u1 v1 u2 v2 ...] in mesh order (XList fastest). */
-int aldic_init_u0(aldic_ctx* ctx, int ny, int nx, const double* u, const double* v, double* U0);
+/* Init(u, v, Phi, x, y, index) (func/Init.m): inpaint_nans(., 4) of the search's u and v
+ * grids (ny x nx column-major, as aldic_integer_search returns them; left unchanged) (:13);
+ * index 1 adds the three spring outlier passes (:29-166: nodes whose value departs from
+ * their neighbours' average by more than 3 / 2 / 2 standard deviations are set NaN with
+ * their neighbourhood, the border rows and columns too, and the grids inpainted again);
+ * U0 (2 nx ny) interleaved [u1 v1 u2 v2 ...] in mesh order (XList fastest) (:169-177).
+ * The stereo and temporal drivers call index 0. */
+int aldic_init_u0(aldic_ctx* ctx, int ny, int nx, const double* u, const double* v, int index, double* U0);
 
 /* -------------------------------------------------------- triangulation --------- */
 /* triangulatePoints (func_quadtree/stereoReconstruction_quadtree.m:30-52): per row of

@@ -318,10 +318,83 @@ def inpaint_nans4(A):
     return flat.reshape((m, n), order="F")
 
 
-def init_u0(u, v):
-    """Init(u, v, Phi, x, y, 0) (func/Init.m:1-2 and :85-92): inpaint_nans(., 4) of the
-    search grids u, v (ny x nx) and U0 interleaved over the transposed grids (XList fastest)."""
-    ui, vi = inpaint_nans4(u).T.ravel(order="F"), inpaint_nans4(v).T.ravel(order="F")
+def _std8(vals):
+    """MATLAB std(x, 'omitnan') of the listed values, summed in order (no fused operations)."""
+    xs = [x for x in vals if not np.isnan(x)]
+    k = len(xs)
+    if k < 2:
+        return 0.0 if k == 1 else np.nan
+    m = 0.0
+    for x in xs:
+        m = m + x
+    m = m / k
+    ss = 0.0
+    for x in xs:
+        d = x - m
+        ss = ss + d * d
+    return np.sqrt(ss / (k - 1))
+
+
+def spring_pass(u, v, mode):
+    """One spring outlier pass of Init index 1 (func/Init.m:31-66, :76-109, :119-154): for every
+    interior node of the inpainted grids, compare |value - neighbour average| with a multiple
+    of the neighbours' standard deviation; a node failing the test for u or v is set NaN in
+    both, with its neighbourhood; the border rows and columns are set NaN; both grids are
+    inpainted again.  mode 0: 8 neighbours, weighted average (1/8 edge + 1/16 corner sums)
+    / (3/4), 3 sigma, 8-neighbourhood; mode 1: 4 neighbours, plain mean, 2 sigma,
+    4-neighbourhood; mode 2: as mode 0 with 2 sigma."""
+    ut, vt = np.array(u, dtype=np.float64), np.array(v, dtype=np.float64)
+    ui, vi = ut.copy(), vt.copy()
+    m, n = ut.shape
+    kk = 3.0 if mode == 0 else 2.0
+    edge = ((-1, 0), (1, 0), (0, -1), (0, 1))
+    corner = ((-1, -1), (1, -1), (1, 1), (-1, 1))
+    for i in range(1, m - 1):
+        for j in range(1, n - 1):
+            bad = False
+            for t in (ut, vt):
+                e = [t[i + di, j + dj] for di, dj in edge]
+                if mode == 1:
+                    xs = [x for x in e if not np.isnan(x)]
+                    avg = np.nan
+                    if xs:
+                        acc = 0.0
+                        for x in xs:
+                            acc = acc + x
+                        avg = acc / len(xs)
+                    sd = _std8(e)
+                else:
+                    c = [t[i + di, j + dj] for di, dj in corner]
+                    se = ((e[0] + e[1]) + e[2]) + e[3]
+                    sc = ((c[0] + c[1]) + c[2]) + c[3]
+                    avg = ((1.0 / 8.0) * se + (1.0 / 16.0) * sc) / (3.0 / 4.0)
+                    sd = _std8(e + c)
+                err = abs(t[i, j] - avg) - kk * sd
+                if err > 0:
+                    bad = True
+            if bad:
+                nb = edge if mode == 1 else edge + corner
+                for g in (ui, vi):
+                    g[i, j] = np.nan
+                    for di, dj in nb:
+                        g[i + di, j + dj] = np.nan
+    for g in (ui, vi):
+        g[0, :] = np.nan
+        g[-1, :] = np.nan
+        g[:, 0] = np.nan
+        g[:, -1] = np.nan
+    return inpaint_nans4(ui), inpaint_nans4(vi)
+
+
+def init_u0(u, v, index=0):
+    """Init(u, v, Phi, x, y, index) (func/Init.m): inpaint_nans(., 4) of the search grids u, v
+    (ny x nx) (:13), with index 1 the three spring outlier passes (:29-166), and U0 interleaved
+    over the transposed grids (XList fastest) (:169-177)."""
+    u, v = inpaint_nans4(u), inpaint_nans4(v)
+    if index == 1:
+        for mode in (0, 1, 2):
+            u, v = spring_pass(u, v, mode)
+    ui, vi = u.T.ravel(order="F"), v.T.ravel(order="F")
     U0 = np.empty(2 * ui.size)
     U0[0::2], U0[1::2] = ui, vi
     return U0

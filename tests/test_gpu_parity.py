@@ -508,6 +508,16 @@ def test_inpaint_nans_and_init_parity(A, ctx):
     assert np.abs(U0 - ref).max() <= 1e-10 * np.abs(ref).max()
     assert np.array_equal(u, u_in, equal_nan=True) and np.array_equal(v, v_in, equal_nan=True)
     assert np.array_equal(A.Init(u, v, ctx=ctx), U0)
+    # index 1: the spring outlier passes, with planted outliers (same NaN marks as the oracle,
+    # whose operations are rounded one by one like the device's)
+    uo, vo = r["u"].copy(), r["v"].copy()
+    uo[4, 6] += 9.0
+    vo[10, 3] -= 7.0
+    uo[rng.random(uo.shape) < 0.05] = np.nan
+    U1 = ctx.init_u0(uo, vo, index=1)
+    ref1 = O.init_u0(uo, vo, index=1)
+    assert np.abs(U1 - ref1).max() <= 1e-9 * max(1.0, np.abs(ref1).max())
+    assert abs(U1[0::2].reshape(uo.shape)[4, 6] - r["u"][4, 6]) < 1.0  # the outlier is gone
 
 
 def test_launch_counter_and_errors(A, ctx):

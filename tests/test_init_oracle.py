@@ -55,3 +55,27 @@ def test_inpaint_reproduces_linear_fields_and_init_order():
     assert np.array_equal(U0[0::2], u.T.ravel(order="F"))
     assert np.array_equal(U0[1::2], v.T.ravel(order="F"))
     assert U0[0] == u[0, 0] and U0[2] == u[0, 1]
+
+
+def test_init_index1_removes_outliers_and_index0_keeps_them():
+    rng = np.random.default_rng(1)
+    y, x = np.mgrid[0:20, 0:25]
+    u = 0.02 * x + 0.01 * y + rng.normal(0, 0.01, x.shape)
+    v = -0.03 * x + rng.normal(0, 0.01, x.shape)
+    u[5, 7] += 3.0
+    v[12, 15] -= 2.0
+    u[3, 3] = np.nan
+    U1 = O.init_u0(u, v, index=1)
+    U0 = O.init_u0(u, v, index=0)
+    u1, v1 = U1[0::2].reshape(20, 25), U1[1::2].reshape(20, 25)
+    assert abs(u1[5, 7] - (0.02 * 7 + 0.01 * 5)) < 0.05
+    assert abs(v1[12, 15] - (-0.03 * 15)) < 0.05
+    assert abs(U0[0::2].reshape(20, 25)[5, 7] - u[5, 7]) < 1e-12
+    assert np.isfinite(U1).all()
+
+
+def test_spring_pass_statistics_follow_matlab():
+    # std over the neighbours is the N-1 sample deviation, NaN entries omitted
+    assert abs(O._std8([1.0, 2.0, 3.0, 4.0]) - np.std([1, 2, 3, 4], ddof=1)) < 1e-15
+    assert abs(O._std8([1.0, np.nan, 3.0]) - np.std([1, 3], ddof=1)) < 1e-15
+    assert O._std8([5.0]) == 0.0 and np.isnan(O._std8([np.nan]))
