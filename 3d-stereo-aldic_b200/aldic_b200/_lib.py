@@ -48,6 +48,7 @@ SIGNATURES = {
     "aldic_subpb1": (_i, [_vp, _i, _i64, _vp, _vp, _vp, _vp, _vp, _i, _vp, _d, _d, _vp, _vp]),
     "aldic_epipolar_icgn": (_i, [_vp, _i64, _vp, _i, _d, _vp]),
     "aldic_triangulate": (_i, [_vp, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "aldic_undistort_points": (_i, [_vp, _i64, _vp, _vp, _vp, _i, _vp, _vp]),
     "aldic_inpaint_nans": (_i, [_vp, _i, _i, _vp, _vp]),
     "aldic_init_u0": (_i, [_vp, _i, _i, _vp, _vp, _i, _vp]),
     "aldic_measure_fp32_peak": (_i, [_vp, C.POINTER(_d)]),

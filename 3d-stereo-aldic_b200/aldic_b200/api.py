@@ -23,7 +23,7 @@ from ._lib import AldicError
 __all__ = [
     "Context", "default_context", "funNormalizeImg", "funImgGradient", "ba_interp2_spline", "funIntegerSearch",
     "LocalICGN", "LocalICGNQuadtree", "Subpb1", "Subpb1Quadtree", "epipolar_ICGN1",
-    "stereoReconstruction_quadtree", "bad_points_local", "bad_points_subpb1", "Init",
+    "stereoReconstruction_quadtree", "bad_points_local", "bad_points_subpb1", "Init", "funUndistortPoints",
 ]
 
 
@@ -339,6 +339,20 @@ class Context:
         self._check(rc, "aldic_init_u0")
         return U0
 
+    def undistort_points(self, pts, K, radial, tangential=None):
+        """MATLAB undistortPoints for one camera: pts (n x 2, 1-based pixels) through the
+        inverse of the radial (2 or 3 coefficients) and tangential (p1, p2) lens model of K."""
+        k = _Keep()
+        p = np.asarray(pts, dtype=np.float64).reshape(-1, 2)
+        n = p.shape[0]
+        rad = np.asarray(radial, dtype=np.float64).ravel()
+        out, op = k.out(2 * n, np.float64)
+        tan = None if tangential is None else k.ptr(np.ravel(tangential), np.float64)
+        rc = self.lib.aldic_undistort_points(self.h, n, k.ptr(p, np.float64), k.ptr(np.asarray(K, np.float64), np.float64),
+                                             k.ptr(rad, np.float64), int(rad.size), tan, op)
+        self._check(rc, "aldic_undistort_points")
+        return out.reshape((n, 2), order="F")
+
     def triangulate(self, pairs, KL, KR, R, T, out=None):
         k = _Keep()
         n = _count(pairs, 4)
@@ -569,11 +583,42 @@ def epipolar_ICGN1(pointCandidate, Df, ImgRef, ImgDef, winsize, tol, ICGNmethod=
     return ctx.epipolar_icgn(pts, winsize, tol)
 
 
+def _has_distortion(cameraParams, side):
+    rad = np.ravel(cameraParams.get("radial" + side, [0.0, 0.0]))
+    tan = np.ravel(cameraParams.get("tangential" + side, [0.0, 0.0]))
+    return bool(np.any(rad != 0) or np.any(tan != 0))
+
+
+def funUndistortPoints(matchedPairs, cameraParams, ctx: Context | None = None):
+    """undistortedPoints = funUndistortPoints(matchedPairs, cameraParams)
+    (func/funUndistortPoints.m): every frame's pairs [xL yL xR yR] (n x 4) with the left and
+    right points undistorted by their camera's lens model.  cameraParams: dict with KL, KR
+    (3x3) and radialL / tangentialL / radialR / tangentialR (absent = zero).  Rows with a
+    non-finite entry come back NaN."""
+    ctx = ctx or default_context()
+    out = []
+    for pts in matchedPairs:
+        pts = np.asarray(pts, dtype=np.float64)
+        res = np.full(pts.shape, np.nan)
+        fin = np.all(np.isfinite(pts), axis=1)
+        if fin.any():
+            for side, cols in (("L", slice(0, 2)), ("R", slice(2, 4))):
+                res[fin, cols] = ctx.undistort_points(pts[fin, cols], cameraParams["K" + side],
+                                                      cameraParams.get("radial" + side, [0.0, 0.0]),
+                                                      cameraParams.get("tangential" + side))
+        out.append(res)
+    return out
+
+
 def stereoReconstruction_quadtree(matchedPairs, cameraParams, ctx: Context | None = None):
     """[FinalResult, reprojectionErrors] = stereoReconstruction_quadtree(matchedPairs, cameraParams)
     (func_quadtree/stereoReconstruction_quadtree.m).  matchedPairs: list of n x 4 arrays;
-    cameraParams: dict with KL, KR (3x3), R (3x3), T (3,), zero distortion."""
+    cameraParams: dict with KL, KR (3x3), R (3x3), T (3,) and, optionally, the lens
+    distortion (radialL, tangentialL, radialR, tangentialR): the points are undistorted
+    first (funUndistortPoints) when any coefficient is non-zero."""
     ctx = ctx or default_context()
+    if _has_distortion(cameraParams, "L") or _has_distortion(cameraParams, "R"):
+        matchedPairs = funUndistortPoints(matchedPairs, cameraParams, ctx=ctx)
     coords, errs = [], []
     for pts in matchedPairs:
         xyz, err = ctx.triangulate(np.asarray(pts, dtype=np.float64), cameraParams["KL"], cameraParams["KR"],

@@ -733,6 +733,34 @@ int aldic_init_u0(aldic_ctx* c, int ny, int nx, const double* u, const double* v
   return finish(c, l);
 }
 
+int aldic_undistort_points(aldic_ctx* c, int64_t n, const double* pts, const double* K, const double* radial,
+                           int n_radial, const double* tangential, double* out) {
+  if (!c) return ALDIC_ERR_ARG;
+  if (n < 0) return fail(c, ALDIC_ERR_ARG, "n < 0");
+  if (n_radial != 2 && n_radial != 3) return fail(c, ALDIC_ERR_ARG, "radial distortion needs 2 or 3 coefficients");
+  if (n == 0) return ALDIC_OK;
+  if (!pts || !K || !radial || !out) return fail(c, ALDIC_ERR_ARG, "missing array argument");
+  CK(cudaSetDevice(c->device));
+  // camera parameters (small, read on the host): K 3 x 3 column-major, (k1 k2 [k3]), (p1 p2)
+  double k[9], rad[3] = {0.0, 0.0, 0.0}, tan2[2] = {0.0, 0.0};
+  const double* srcs[3] = {K, radial, tangential};
+  double* dsts[3] = {k, rad, tan2};
+  const int cnts[3] = {9, n_radial, 2};
+  for (int i = 0; i < 3; ++i) {
+    if (!srcs[i]) continue;
+    if (is_device_ptr(srcs[i])) {
+      CK(cudaMemcpy(dsts[i], srcs[i], cnts[i] * 8, cudaMemcpyDeviceToHost));
+    } else {
+      std::memcpy(dsts[i], srcs[i], cnts[i] * 8);
+    }
+  }
+  const double dist[5] = {rad[0], rad[1], rad[2], tan2[0], tan2[1]};
+  Arg ap{pts, (size_t)n * 16, false, nullptr}, ao{out, (size_t)n * 16, true, nullptr};
+  int rc = stage(c, {&ap, &ao});
+  if (rc) return rc;
+  return finish(c, launch_undistort_points(n, (const double*)ap.dev, k, dist, (double*)ao.dev, c->stream));
+}
+
 int aldic_triangulate(aldic_ctx* c, int64_t n, const double* pairs, const double* KL, const double* KR,
                       const double* R, const double* T, double* xyz, double* reproj_err) {
   if (!c) return ALDIC_ERR_ARG;

@@ -108,6 +108,9 @@ int launch_inpaint(double* A, int m, int n, void* scratch, int* status, cudaStre
 int launch_interleave_u0(const double* u, const double* v, int ny, int nx, double* U0, cudaStream_t st);
 int launch_spring_pass(const double* ut, const double* vt, double* ui, double* vi, int m, int n, int mode,
                        cudaStream_t st);
+// dist = (k1, k2, k3, p1, p2); K 3 x 3 column-major (MATLAB)
+int launch_undistort_points(long long n, const double* pts, const double* K, const double* dist, double* out,
+                            cudaStream_t st);
 int launch_triangulate(long long n, const double* pairs, const CamPair& cams, double* xyz, double* err,
                        cudaStream_t st);
 int launch_fp32_probe(int blocks, int threads, int iters, float* out, bool packed, cudaStream_t st);

@@ -101,6 +101,78 @@ int launch_triangulate(long long n, const double* pairs, const CamPair& cams, do
   return 1;
 }
 
+// funUndistortPoints (func/funUndistortPoints.m:8-39, MATLAB undistortPoints per camera):
+// the inverse of the radial / tangential lens model of cameraParameters.  A pixel (u, v)
+// (1-based, as K's principal point) maps to normalised coordinates (xd, yd) = K^-1 (u, v, 1);
+// the undistorted (x, y) solves
+//     xd = x (1 + k1 r^2 + k2 r^4 + k3 r^6) + 2 p1 x y + p2 (r^2 + 2 x^2)
+//     yd = y (1 + k1 r^2 + k2 r^4 + k3 r^6) + p1 (r^2 + 2 y^2) + 2 p2 x y,   r^2 = x^2 + y^2,
+// found by the fixed-point iteration x <- (xd - tangential(x)) / radial(x) from (xd, yd) until
+// the update is below 1e-15 of the point's scale (at most 200 steps); the result goes back
+// through K.  Non-finite input rows give NaN.  FP64 throughout.
+struct Lens {
+  double K[9];     // 3 x 3 row-major
+  double Kinv[9];  // 3 x 3 row-major
+  double k1, k2, k3, p1, p2;
+};
+
+__global__ void undistort_points_kernel(long long n, const double* __restrict__ pts, Lens L, double* __restrict__ out) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double u = pts[i], v = pts[n + i];
+  if (!isfinite(u) || !isfinite(v)) {
+    out[i] = NAN;
+    out[n + i] = NAN;
+    return;
+  }
+  const double* Ki = L.Kinv;
+  const double w = Ki[6] * u + Ki[7] * v + Ki[8];
+  const double xd = (Ki[0] * u + Ki[1] * v + Ki[2]) / w, yd = (Ki[3] * u + Ki[4] * v + Ki[5]) / w;
+  double x = xd, y = yd;
+  for (int it = 0; it < 200; ++it) {
+    const double r2 = x * x + y * y;
+    const double radial = 1.0 + r2 * (L.k1 + r2 * (L.k2 + r2 * L.k3));
+    const double tx = 2.0 * L.p1 * x * y + L.p2 * (r2 + 2.0 * x * x);
+    const double ty = L.p1 * (r2 + 2.0 * y * y) + 2.0 * L.p2 * x * y;
+    const double xn = (xd - tx) / radial, yn = (yd - ty) / radial;
+    const double step = fabs(xn - x) + fabs(yn - y);
+    x = xn;
+    y = yn;
+    if (step <= 1e-15 * (1.0 + fabs(x) + fabs(y))) break;
+  }
+  const double* K = L.K;
+  const double ww = K[6] * x + K[7] * y + K[8];
+  out[i] = (K[0] * x + K[1] * y + K[2]) / ww;
+  out[n + i] = (K[3] * x + K[4] * y + K[5]) / ww;
+}
+
+int launch_undistort_points(long long n, const double* pts, const double* Kcm, const double* dist, double* out,
+                            cudaStream_t st) {
+  if (n <= 0) return 0;
+  Lens L;
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) L.K[r * 3 + c] = Kcm[r + 3 * c];  // MATLAB column-major
+  const double* a = L.K;
+  const double det = a[0] * (a[4] * a[8] - a[5] * a[7]) - a[1] * (a[3] * a[8] - a[5] * a[6]) +
+                     a[2] * (a[3] * a[7] - a[4] * a[6]);
+  L.Kinv[0] = (a[4] * a[8] - a[5] * a[7]) / det;
+  L.Kinv[1] = (a[2] * a[7] - a[1] * a[8]) / det;
+  L.Kinv[2] = (a[1] * a[5] - a[2] * a[4]) / det;
+  L.Kinv[3] = (a[5] * a[6] - a[3] * a[8]) / det;
+  L.Kinv[4] = (a[0] * a[8] - a[2] * a[6]) / det;
+  L.Kinv[5] = (a[2] * a[3] - a[0] * a[5]) / det;
+  L.Kinv[6] = (a[3] * a[7] - a[4] * a[6]) / det;
+  L.Kinv[7] = (a[1] * a[6] - a[0] * a[7]) / det;
+  L.Kinv[8] = (a[0] * a[4] - a[1] * a[3]) / det;
+  L.k1 = dist[0];
+  L.k2 = dist[1];
+  L.k3 = dist[2];
+  L.p1 = dist[3];
+  L.p2 = dist[4];
+  undistort_points_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, pts, L, out);
+  return 1;
+}
+
 // FP32 FMA throughput probe: 8 independent FMA chains per thread, enough blocks to fill
 // every SM; used only to state the measured FP32 roofline beside the kernels.
 __global__ void fp32_probe_kernel(int iters, float seed, float* out) {

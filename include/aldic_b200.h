@@ -148,6 +148,15 @@ int aldic_inpaint_nans(aldic_ctx* ctx, int m, int n, double* A, int32_t* info);
  * The stereo and temporal drivers call index 0. */
 int aldic_init_u0(aldic_ctx* ctx, int ny, int nx, const double* u, const double* v, int index, double* U0);
 
+/* funUndistortPoints (func/funUndistortPoints.m:8-39; MATLAB undistortPoints of one camera):
+ * n points pts (n x 2 column-major, 1-based pixels) through the inverse of the
+ * cameraParameters lens model -- radial (k1, k2 [, k3]: n_radial = 2 or 3) and tangential
+ * (p1, p2; NULL = none) distortion in normalised coordinates K^-1 (u, v, 1) -- solved by
+ * FP64 fixed-point iteration to 1e-15, mapped back through K (3 x 3 column-major) into out
+ * (n x 2).  Non-finite rows give NaN. */
+int aldic_undistort_points(aldic_ctx* ctx, int64_t n, const double* pts, const double* K, const double* radial,
+                           int n_radial, const double* tangential, double* out);
+
 /* -------------------------------------------------------- triangulation --------- */
 /* triangulatePoints (func_quadtree/stereoReconstruction_quadtree.m:30-52): per row of
  * pairs (n x 4 column-major [xL yL xR yR]) the DLT of P_L = K_L [I | 0] and

@@ -398,3 +398,48 @@ def init_u0(u, v, index=0):
     U0 = np.empty(2 * ui.size)
     U0[0::2], U0[1::2] = ui, vi
     return U0
+
+
+def distort_points(pts, K, radial, tangential=None):
+    """The cameraParameters lens model (forward): undistorted pixels -> distorted pixels
+    through normalised coordinates K^-1 (u, v, 1).  Used to check undistort_points."""
+    K = np.asarray(K, dtype=np.float64)
+    rad = list(np.ravel(radial)) + [0.0] * (3 - len(np.ravel(radial)))
+    p1, p2 = (0.0, 0.0) if tangential is None else np.ravel(tangential)[:2]
+    P = np.asarray(pts, dtype=np.float64).reshape(-1, 2)
+    h = np.linalg.solve(K, np.stack([P[:, 0], P[:, 1], np.ones(len(P))]))
+    x, y = h[0] / h[2], h[1] / h[2]
+    r2 = x * x + y * y
+    radial_f = 1.0 + r2 * (rad[0] + r2 * (rad[1] + r2 * rad[2]))
+    xd = x * radial_f + 2 * p1 * x * y + p2 * (r2 + 2 * x * x)
+    yd = y * radial_f + p1 * (r2 + 2 * y * y) + 2 * p2 * x * y
+    q = K @ np.stack([xd, yd, np.ones_like(xd)])
+    return np.stack([q[0] / q[2], q[1] / q[2]], 1)
+
+
+def undistort_points(pts, K, radial, tangential=None):
+    """MATLAB undistortPoints (func/funUndistortPoints.m:24-26) restated: the inverse of
+    distort_points by fixed-point iteration x <- (xd - tangential(x)) / radial(x) in
+    normalised coordinates, to 1e-15 (at most 200 steps).  Non-finite rows give NaN."""
+    K = np.asarray(K, dtype=np.float64)
+    rad = list(np.ravel(radial)) + [0.0] * (3 - len(np.ravel(radial)))
+    p1, p2 = (0.0, 0.0) if tangential is None else np.ravel(tangential)[:2]
+    P = np.asarray(pts, dtype=np.float64).reshape(-1, 2)
+    out = np.full(P.shape, np.nan)
+    fin = np.all(np.isfinite(P), axis=1)
+    h = np.linalg.solve(K, np.stack([P[fin, 0], P[fin, 1], np.ones(int(fin.sum()))]))
+    xd, yd = h[0] / h[2], h[1] / h[2]
+    x, y = xd.copy(), yd.copy()
+    for _ in range(200):
+        r2 = x * x + y * y
+        radial_f = 1.0 + r2 * (rad[0] + r2 * (rad[1] + r2 * rad[2]))
+        tx = 2 * p1 * x * y + p2 * (r2 + 2 * x * x)
+        ty = p1 * (r2 + 2 * y * y) + 2 * p2 * x * y
+        xn, yn = (xd - tx) / radial_f, (yd - ty) / radial_f
+        step = np.abs(xn - x) + np.abs(yn - y)
+        x, y = xn, yn
+        if np.all(step <= 1e-15 * (1.0 + np.abs(x) + np.abs(y))):
+            break
+    q = K @ np.stack([x, y, np.ones_like(x)])
+    out[fin] = np.stack([q[0] / q[2], q[1] / q[2]], 1)
+    return out

@@ -520,6 +520,35 @@ def test_inpaint_nans_and_init_parity(A, ctx):
     assert abs(U1[0::2].reshape(uo.shape)[4, 6] - r["u"][4, 6]) < 1.0  # the outlier is gone
 
 
+def test_undistort_and_reconstruction_parity(A, ctx):
+    """funUndistortPoints against the oracle's restatement and the forward lens model; the
+    reconstruction driver with distortion recovers the points triangulated without it."""
+    K = np.array([[4000.0, 0.5, 1024.5], [0, 4010.0, 1000.2], [0, 0, 1]])
+    rng = np.random.default_rng(2)
+    P = rng.uniform(1, 2048, (3000, 2))
+    P[7] = np.nan
+    for rad, tan in (([-0.12, 0.05, -0.01], [1e-3, -5e-4]), ([0.08, -0.02], None), ([0.0, 0.0], None)):
+        got = ctx.undistort_points(P, K, rad, tan)
+        ref = O.undistort_points(P, K, rad, tan)
+        assert np.array_equal(np.isnan(got), np.isnan(ref))
+        ok = np.isfinite(ref[:, 0])
+        assert np.abs(got[ok] - ref[ok]).max() < 1e-9
+        assert np.abs(O.distort_points(got[ok], K, rad, tan) - P[ok]).max() < 1e-9
+    sc = synth.stereo_pair(seed=3, size=256, f=500.0)
+    xy = rng.uniform(60, 200, (400, 2))
+    tr = synth.stereo_truth(sc, xy)
+    pairs = np.hstack([xy, tr["right0"]])
+    cam = {"KL": sc.KL, "KR": sc.KR, "R": sc.R_rl, "T": sc.T_rl}
+    plain, _ = A.stereoReconstruction_quadtree([pairs], cam, ctx=ctx)
+    lens = dict(cam, radialL=[-0.05, 0.01], tangentialL=[2e-4, 1e-4], radialR=[0.04, 0.0, -0.002])
+    dist_pairs = np.hstack([O.distort_points(pairs[:, :2], sc.KL, lens["radialL"], lens["tangentialL"]),
+                            O.distort_points(pairs[:, 2:], sc.KR, lens["radialR"])])
+    und = A.funUndistortPoints([dist_pairs], lens, ctx=ctx)[0]
+    assert np.abs(und - pairs).max() < 1e-8
+    lensed, _ = A.stereoReconstruction_quadtree([dist_pairs], lens, ctx=ctx)
+    assert np.abs(lensed["Coordinates"][0] - plain["Coordinates"][0]).max() < 1e-6
+
+
 def test_launch_counter_and_errors(A, ctx):
     before = ctx.launches
     ctx.triangulate(np.zeros((4, 4)) + 1.0, np.eye(3), np.eye(3), np.eye(3), [1.0, 0, 0])

@@ -79,3 +79,17 @@ def test_spring_pass_statistics_follow_matlab():
     assert abs(O._std8([1.0, 2.0, 3.0, 4.0]) - np.std([1, 2, 3, 4], ddof=1)) < 1e-15
     assert abs(O._std8([1.0, np.nan, 3.0]) - np.std([1, 3], ddof=1)) < 1e-15
     assert O._std8([5.0]) == 0.0 and np.isnan(O._std8([np.nan]))
+
+
+def test_undistort_is_the_inverse_of_the_lens_model():
+    K = np.array([[4000.0, 0.5, 1024.5], [0, 4010.0, 1000.2], [0, 0, 1]])
+    rng = np.random.default_rng(0)
+    P = rng.uniform(1, 2048, (500, 2))
+    for rad, tan in (([-0.12, 0.05, -0.01], [1e-3, -5e-4]), ([0.08, -0.02], None)):
+        U = O.undistort_points(P, K, rad, tan)
+        assert np.abs(O.distort_points(U, K, rad, tan) - P).max() < 1e-9
+    # zero distortion: the identity (through K and back)
+    assert np.abs(O.undistort_points(P, K, [0.0, 0.0]) - P).max() < 1e-9
+    Q = P.copy()
+    Q[3, 1] = np.nan
+    assert np.isnan(O.undistort_points(Q, K, [0.1, 0.0])[3]).all()
