@@ -24,6 +24,7 @@ __all__ = [
     "Context", "default_context", "funNormalizeImg", "funImgGradient", "ba_interp2_spline", "funIntegerSearch",
     "LocalICGN", "LocalICGNQuadtree", "Subpb1", "Subpb1Quadtree", "epipolar_ICGN1",
     "stereoReconstruction_quadtree", "bad_points_local", "bad_points_subpb1", "Init", "funUndistortPoints",
+    "IntegerSearchQuadtree",
 ]
 
 
@@ -441,6 +442,46 @@ def funIntegerSearch(f, g, tempSizeOfSearchRegion, gridx, gridy, winsize, winste
     st = int(np.ravel(winstepsize)[0])
     r = ctx.integer_search(tempSizeOfSearchRegion, gridx, gridy, w, st)
     return r["x"], r["y"], r["u"], r["v"], {"max": r["phi"], "A": []}
+
+
+def IntegerSearchQuadtree(ImgRef, ImgDef, file_name, DICpara, ImgSeqNum, ctx: Context | None = None):
+    """[DICpara, x0, y0, u, v, cc] = IntegerSearchQuadtree(ImgRef, ImgDef, file_name, DICpara,
+    ImgSeqNum) (func_quadtree/IntegerSearchQuadtree.m), whole-field mode
+    (InitFFTSearchMethod 1).  The search distance follows :48-62 -- stereo (ImgSeqNum -1):
+    StereoSearchDistance, else NewFFTSearchDistance; temporal (ImgSeqNum >= 2):
+    TemporalSearchDistance, else NewFFTSearchDistance -- and a missing one raises instead of
+    prompting.  The whole-field search runs on the device (:93); grid points whose rounded
+    position is outside DICpara['ImgRefMask'] become NaN (:100-111).  The funRemoveOutliers
+    call that follows in the reference (:158-160) prompts for input and is left to the caller
+    (Init's inpaint fills the NaN holes)."""
+    method = DICpara.get("InitFFTSearchMethod", 1)
+    if method != 1:
+        raise AldicError("IntegerSearchQuadtree: only the whole-field mode (InitFFTSearchMethod 1) is implemented")
+    keys = ("StereoSearchDistance", "NewFFTSearchDistance") if ImgSeqNum == -1 else \
+        ("TemporalSearchDistance", "NewFFTSearchDistance") if ImgSeqNum >= 2 else ()
+    s = None
+    for key in keys:
+        if DICpara.get(key) is not None and np.size(DICpara[key]) > 0:
+            s = DICpara[key]
+            break
+    if s is None:
+        raise AldicError("IntegerSearchQuadtree: no search distance in DICpara for this image (the reference prompts)")
+    s = np.ravel(np.asarray(s, dtype=np.int64))
+    s = np.array([s[0], s[0]]) if s.size == 1 else s[:2]
+    roi = DICpara["gridxyROIRange"]
+    x0, y0, u, v, cc = funIntegerSearch(ImgRef, ImgDef, s, roi["gridx"], roi["gridy"], DICpara["winsize"],
+                                        DICpara["winstepsize"], 0, ctx=ctx)
+    mask = DICpara.get("ImgRefMask")
+    if mask is not None:
+        mask = np.asarray(mask)
+        # MATLAB round (half away from zero; the centres are positive)
+        ix = np.clip(np.floor(np.asarray(x0) + 0.5).astype(np.int64) - 1, 0, mask.shape[0] - 1)
+        iy = np.clip(np.floor(np.asarray(y0) + 0.5).astype(np.int64) - 1, 0, mask.shape[1] - 1)
+        hole = ~mask[ix, iy].astype(bool)
+        u = np.where(hole, np.nan, u)
+        v = np.where(hole, np.nan, v)
+    DICpara = dict(DICpara, InitFFTSearchMethod=method, SizeOfFFTSearchRegion=s)
+    return DICpara, x0, y0, u, v, cc
 
 
 def _load_frame(ctx, Df, ImgRef, ImgDef, mask):

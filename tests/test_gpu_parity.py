@@ -549,6 +549,23 @@ def test_undistort_and_reconstruction_parity(A, ctx):
     assert np.abs(lensed["Coordinates"][0] - plain["Coordinates"][0]).max() < 1e-6
 
 
+def test_integer_search_quadtree_driver(A, ctx, affine):
+    """IntegerSearchQuadtree: the distance from DICpara, the device search, mask -> NaN."""
+    sc = affine
+    M, N = sc.ref.shape
+    mask = np.ones((M, N))
+    mask[200:320, 150:260] = 0
+    para = {"gridxyROIRange": {"gridx": [1, M], "gridy": [1, N]}, "winsize": 30, "winstepsize": 16,
+            "TemporalSearchDistance": 10, "ImgRefMask": mask}
+    para2, x0, y0, u, v, cc = A.IntegerSearchQuadtree(sc.ref, sc.deff, None, para, 2, ctx=ctx)
+    xr, yr, ur, vr, _ = A.funIntegerSearch(sc.ref, sc.deff, [10, 10], [1, M], [1, N], 30, 16, ctx=ctx)
+    hole = mask[np.floor(x0 + 0.5).astype(int) - 1, np.floor(y0 + 0.5).astype(int) - 1] == 0
+    assert hole.sum() > 10 and (~hole).sum() > 100
+    assert np.isnan(u[hole]).all() and np.isnan(v[hole]).all()
+    assert np.array_equal(u[~hole], ur[~hole], equal_nan=True)
+    assert list(para2["SizeOfFFTSearchRegion"]) == [10, 10]
+
+
 def test_launch_counter_and_errors(A, ctx):
     before = ctx.launches
     ctx.triangulate(np.zeros((4, 4)) + 1.0, np.eye(3), np.eye(3), np.eye(3), [1.0, 0, 0])

@@ -51,3 +51,19 @@ def test_count_and_shape_validation():
 def test_funintegersearch_rejects_seed_mode():
     with pytest.raises(api.AldicError):
         api.funIntegerSearch(np.zeros((10, 10)), np.zeros((10, 10)), 3, [1, 10], [1, 10], 4, 2, 1)
+
+
+def test_integer_search_quadtree_distance_rules():
+    import pytest
+    import aldic_b200 as A
+
+    roi = {"gridx": [1, 64], "gridy": [1, 64]}
+    base = {"gridxyROIRange": roi, "winsize": 16, "winstepsize": 8, "InitFFTSearchMethod": 1}
+    f = np.zeros((64, 64))
+    # no distance for this image: the reference prompts; here it raises before any device work
+    with pytest.raises(A.AldicError):
+        A.IntegerSearchQuadtree(f, f, None, dict(base, TemporalSearchDistance=5), -1)
+    with pytest.raises(A.AldicError):
+        A.IntegerSearchQuadtree(f, f, None, dict(base, StereoSearchDistance=5), 2)
+    with pytest.raises(A.AldicError):
+        A.IntegerSearchQuadtree(f, f, None, dict(base, InitFFTSearchMethod=0, NewFFTSearchDistance=5), 2)
