@@ -24,7 +24,7 @@ __all__ = [
     "Context", "default_context", "funNormalizeImg", "funImgGradient", "ba_interp2_spline", "funIntegerSearch",
     "LocalICGN", "LocalICGNQuadtree", "Subpb1", "Subpb1Quadtree", "epipolar_ICGN1",
     "stereoReconstruction_quadtree", "bad_points_local", "bad_points_subpb1", "Init", "funUndistortPoints",
-    "IntegerSearchQuadtree",
+    "IntegerSearchQuadtree", "MeshSetUp",
 ]
 
 
@@ -482,6 +482,29 @@ def IntegerSearchQuadtree(ImgRef, ImgDef, file_name, DICpara, ImgSeqNum, ctx: Co
         v = np.where(hole, np.nan, v)
     DICpara = dict(DICpara, InitFFTSearchMethod=method, SizeOfFFTSearchRegion=s)
     return DICpara, x0, y0, u, v, cc
+
+
+def MeshSetUp(x, y, DICpara):
+    """DICmesh = MeshSetUp(x, y, DICpara) (func/MeshSetUp.m), host bookkeeping as in the
+    reference: the search grid x, y (nY x nX, as funIntegerSearch returns them) becomes the
+    FE node list coordinatesFEM (XList fastest), the Q4 elements elementsFEM (1-based) and the
+    world copies (y -> ImgSize(2) + 1 - y, the reference's choice of ImgSize(2)).  The
+    reference also builds a cell-corner mesh that it never stores (func/MeshSetUp.m:44-61,
+    its fields commented out at :82-83); it is left out.  Returns a dict with the
+    reference's field names."""
+    x = np.asarray(x, dtype=np.float64)
+    y = np.asarray(y, dtype=np.float64)
+    img_n = DICpara["ImgSize"][1]          # ImgSize(2), func/MeshSetUp.m:88-89
+    M, N = x.shape[1], x.shape[0]          # M along XList (image x), N along YList
+    xt, yt = x.T, y.T                      # M x N
+    coordinatesFEM = np.stack([xt.ravel(order="F"), yt.ravel(order="F")], 1)
+    j, i = np.meshgrid(np.arange(1, N), np.arange(1, M), indexing="ij")
+    j, i = j.ravel(), i.ravel()            # element order: i (XList) fastest
+    elementsFEM = np.stack([(j - 1) * M + i, (j - 1) * M + i + 1, j * M + i + 1, j * M + i], 1)
+    return {"coordinatesFEM": coordinatesFEM, "elementsFEM": elementsFEM,
+            "dirichlet": [], "neumann": [], "x0": xt, "y0": yt, "M": M, "N": N,
+            "y0World": img_n + 1 - yt,
+            "coordinatesFEMWorld": np.stack([coordinatesFEM[:, 0], img_n + 1 - coordinatesFEM[:, 1]], 1)}
 
 
 def _load_frame(ctx, Df, ImgRef, ImgDef, mask):

@@ -67,3 +67,32 @@ def test_integer_search_quadtree_distance_rules():
         A.IntegerSearchQuadtree(f, f, None, dict(base, StereoSearchDistance=5), 2)
     with pytest.raises(A.AldicError):
         A.IntegerSearchQuadtree(f, f, None, dict(base, InitFFTSearchMethod=0, NewFFTSearchDistance=5), 2)
+
+
+def _mesh_setup_loops(x, y):
+    # the reference's loops (func/MeshSetUp.m), written out one entry at a time
+    M, N = x.shape[1], x.shape[0]
+    xt, yt = x.T, y.T
+    cf = np.zeros((M * N, 2))
+    for i in range(M * N):
+        cf[i] = [xt.ravel(order="F")[i], yt.ravel(order="F")[i]]
+    ef = np.zeros(((M - 1) * (N - 1), 4), dtype=np.int64)
+    for j in range(1, N):
+        for i in range(1, M):
+            ef[(j - 1) * (M - 1) + i - 1] = [(j - 1) * M + i, (j - 1) * M + i + 1, j * M + i + 1, j * M + i]
+    return cf, ef
+
+
+def test_mesh_setup_matches_the_reference_loops():
+    import aldic_b200 as A
+
+    xl = np.arange(1, 120 - 20 - 8 + 1, 8) + 10.0
+    yl = np.arange(1, 90 - 20 - 8 + 1, 8) + 10.0
+    X, Y = np.meshgrid(xl, yl)           # nY x nX, as funIntegerSearch returns them
+    D = A.MeshSetUp(X, Y, {"winstepsize": 8, "ImgSize": [120, 90]})
+    cf, ef = _mesh_setup_loops(X, Y)
+    assert np.array_equal(D["coordinatesFEM"], cf) and np.array_equal(D["elementsFEM"], ef)
+    assert D["M"] == len(xl) and D["N"] == len(yl)
+    assert np.array_equal(D["coordinatesFEMWorld"][:, 1], 91 - cf[:, 1])
+    # the node list is the XList-fastest mesh the pipelines use
+    assert D["coordinatesFEM"][1, 0] - D["coordinatesFEM"][0, 0] == 8
