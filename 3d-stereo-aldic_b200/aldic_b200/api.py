@@ -24,7 +24,7 @@ __all__ = [
     "Context", "default_context", "funNormalizeImg", "funImgGradient", "ba_interp2_spline", "funIntegerSearch",
     "LocalICGN", "LocalICGNQuadtree", "Subpb1", "Subpb1Quadtree", "epipolar_ICGN1",
     "stereoReconstruction_quadtree", "bad_points_local", "bad_points_subpb1", "Init", "funUndistortPoints",
-    "IntegerSearchQuadtree", "MeshSetUp",
+    "IntegerSearchQuadtree", "MeshSetUp", "funRemoveOutliers",
 ]
 
 
@@ -320,6 +320,31 @@ class Context:
         self._check(rc, "aldic_inpaint_nans")
         return (a, tuple(nfo)) if info else a
 
+    def remove_outliers(self, u, v, thr=100.0, maxit=0, info=False):
+        """funRemoveOutliers(u, v, cc, 0, thr): the median test and inpaint of the search grids.
+        Host arrays (m x n) are returned as new arrays (u, v); CUDA tensors (2-D, (n, m)
+        holding the column-major m x n grids) are updated in place.  info=True also returns
+        (removed, NaN holes, method-3 iterations, converged)."""
+        k = _Keep()
+        nfo = (C.c_int32 * 4)()
+        if _is_torch(u):
+            if u.dim() != 2 or tuple(v.shape) != tuple(u.shape):
+                raise AldicError("device grids must be two 2-D tensors (n, m) holding column-major m x n grids")
+            n, m = u.shape
+            rc = self.lib.aldic_remove_outliers(self.h, int(m), int(n), k.ptr(u, np.float64), k.ptr(v, np.float64),
+                                                float(thr), int(maxit), nfo if info else None)
+            self._check(rc, "aldic_remove_outliers")
+            return (u, v, tuple(nfo)) if info else (u, v)
+        a = np.array(u, dtype=np.float64, order="F", copy=True)
+        b = np.array(v, dtype=np.float64, order="F", copy=True)
+        if a.ndim != 2 or a.shape != b.shape:
+            raise AldicError("u and v must be 2-D grids of one shape")
+        m, n = a.shape
+        rc = self.lib.aldic_remove_outliers(self.h, int(m), int(n), C.c_void_p(a.ctypes.data),
+                                            C.c_void_p(b.ctypes.data), float(thr), int(maxit), nfo if info else None)
+        self._check(rc, "aldic_remove_outliers")
+        return (a, b, tuple(nfo)) if info else (a, b)
+
     def init_u0(self, u, v, out=None, index=0):
         """Init(u, v, Phi, x, y, index): inpaint the search grids (ny x nx, left unchanged;
         index 1 adds the spring outlier passes) and return U0 (2 nx ny, mesh order), or fill
@@ -444,6 +469,20 @@ def funIntegerSearch(f, g, tempSizeOfSearchRegion, gridx, gridy, winsize, winste
     return r["x"], r["y"], r["u"], r["v"], {"max": r["phi"], "A": []}
 
 
+def funRemoveOutliers(u, v, cc, qDICOrNot, Thr0, ctx: Context | None = None):
+    """[u, v, cc] = funRemoveOutliers(u, v, cc, qDICOrNot, Thr0) (func/funRemoveOutliers.m) for
+    the form the drivers use, qDICOrNot = 0 and Thr0 > 0 (func_quadtree/IntegerSearchQuadtree.m:
+    158-160): the median test (:44-64) and inpaint (:66-72) on the device.  The q-factor branch
+    (qDICOrNot = 1) and the prompting branches (Thr0 = 0, |qDICOrNot| > 0) raise."""
+    if qDICOrNot != 0:
+        raise AldicError("funRemoveOutliers: only qDICOrNot = 0 is implemented (the q-factor branch prompts)")
+    if Thr0 is None or np.size(Thr0) == 0 or float(np.ravel(Thr0)[0]) == 0.0:
+        raise AldicError("funRemoveOutliers: Thr0 = 0 prompts for a threshold in the reference; pass one")
+    ctx = ctx or default_context()
+    u2, v2 = ctx.remove_outliers(u, v, float(np.ravel(Thr0)[0]))
+    return u2, v2, cc
+
+
 def IntegerSearchQuadtree(ImgRef, ImgDef, file_name, DICpara, ImgSeqNum, ctx: Context | None = None):
     """[DICpara, x0, y0, u, v, cc] = IntegerSearchQuadtree(ImgRef, ImgDef, file_name, DICpara,
     ImgSeqNum) (func_quadtree/IntegerSearchQuadtree.m), whole-field mode
@@ -451,9 +490,9 @@ def IntegerSearchQuadtree(ImgRef, ImgDef, file_name, DICpara, ImgSeqNum, ctx: Co
     StereoSearchDistance, else NewFFTSearchDistance; temporal (ImgSeqNum >= 2):
     TemporalSearchDistance, else NewFFTSearchDistance -- and a missing one raises instead of
     prompting.  The whole-field search runs on the device (:93); grid points whose rounded
-    position is outside DICpara['ImgRefMask'] become NaN (:100-111).  The funRemoveOutliers
-    call that follows in the reference (:158-160) prompts for input and is left to the caller
-    (Init's inpaint fills the NaN holes)."""
+    position is outside DICpara['ImgRefMask'] become NaN (:100-111), then the median-test
+    bad-point removal funRemoveOutliers(u, v, cc, 0, 100) runs on the device (:158-160; the
+    NaN holes stay NaN for Init to fill)."""
     method = DICpara.get("InitFFTSearchMethod", 1)
     if method != 1:
         raise AldicError("IntegerSearchQuadtree: only the whole-field mode (InitFFTSearchMethod 1) is implemented")
@@ -480,6 +519,7 @@ def IntegerSearchQuadtree(ImgRef, ImgDef, file_name, DICpara, ImgSeqNum, ctx: Co
         hole = ~mask[ix, iy].astype(bool)
         u = np.where(hole, np.nan, u)
         v = np.where(hole, np.nan, v)
+    u, v, cc = funRemoveOutliers(u, v, cc, 0, 100, ctx=ctx)
     DICpara = dict(DICpara, InitFFTSearchMethod=method, SizeOfFFTSearchRegion=s)
     return DICpara, x0, y0, u, v, cc
 

@@ -3,6 +3,7 @@
 // include/aldic_b200.h.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -679,6 +680,82 @@ int aldic_inpaint_nans(aldic_ctx* c, int m, int n, double* A, int32_t* info) {
   return finish(c, l);
 }
 
+int aldic_remove_outliers(aldic_ctx* c, int m, int n, double* u, double* v, double thr, int maxit,
+                          int32_t* info) {
+  if (!c) return ALDIC_ERR_ARG;
+  if (m < 0 || n < 0) return fail(c, ALDIC_ERR_ARG, "grid size %d x %d", m, n);
+  if ((long long)m * n > (1LL << 30)) return fail(c, ALDIC_ERR_ARG, "grid of %d x %d entries too large", m, n);
+  if (!(thr > 0.0)) return fail(c, ALDIC_ERR_ARG, "threshold must be > 0 (the reference prompts for 0)");
+  if (info)
+    for (int k = 0; k < 4; ++k) info[k] = k == 3 ? 1 : 0;
+  if (m == 0 || n == 0) return ALDIC_OK;
+  if (!u || !v) return fail(c, ALDIC_ERR_ARG, "missing array argument");
+  CK(cudaSetDevice(c->device));
+  const long long mn = (long long)m * n;
+  const size_t bytes = (size_t)mn * sizeof(double);
+  if (maxit <= 0) maxit = (int)std::min<long long>(8 * mn + 200, 20000);
+  // u and v are both inputs and outputs: staged in, copied back
+  Arg au{u, bytes, false, nullptr}, av{v, bytes, false, nullptr};
+  c->arena.used = 0;
+  c->back.clear();
+  size_t need = 0;
+  for (Arg* a : {&au, &av})
+    if (!is_device_ptr(a->user)) need += bytes + 256;
+  const size_t i2 = 2 * (((inpaint_scratch_bytes(mn) + 255) & ~(size_t)255) + 256);
+  const size_t d2 = 2 * (((del4_scratch_bytes(mn) + 255) & ~(size_t)255) + 256);
+  need += 4 * (bytes + 256) + 2 * ((size_t)mn * sizeof(float) + 256) + (size_t)mn + 256 + i2 + d2 + 128;
+  int rc = arena_reserve(c, need);
+  if (rc) return rc;
+  for (Arg* a : {&au, &av}) {
+    if (is_device_ptr(a->user)) {
+      a->dev = const_cast<void*>(a->user);
+    } else {
+      a->dev = arena_take(c, a->bytes);
+      CK(cudaMemcpyAsync(a->dev, a->user, a->bytes, cudaMemcpyHostToDevice, c->stream));
+      c->back.push_back({const_cast<void*>(a->user), a->dev, a->bytes});
+    }
+  }
+  double* du = (double*)au.dev;
+  double* dv = (double*)av.dev;
+  // the method-4 warm starts and the method-3 fills, written at the NaN entries only
+  double* w4u = (double*)arena_take(c, bytes);
+  double* w4v = (double*)arena_take(c, bytes);
+  double* wfu = (double*)arena_take(c, bytes);
+  double* wfv = (double*)arena_take(c, bytes);
+  float* fu = (float*)arena_take(c, (size_t)mn * sizeof(float));
+  float* fv = (float*)arena_take(c, (size_t)mn * sizeof(float));
+  unsigned char* hole = (unsigned char*)arena_take(c, (size_t)mn);
+  void* iscratch = arena_take(c, i2);
+  void* dscratch = arena_take(c, d2);
+  // status: [0..2] method 3 of u, [3..5] of v, [6] removed, [7..12] the method-4 solves,
+  // [16] #NaN(u), [17] #NaN(v), [18] 0 (the hints' third term before the median test)
+  int* status = (int*)arena_take(c, 128);
+  CK(cudaMemsetAsync(status, 0, 128, c->stream));
+  int* counts = status + 16;
+  int l = launch_nan_count(du, dv, m, n, counts, c->stream);
+  // inpaint_nans(., 3) of u and v, started from inpaint_nans(., 4); skipped without NaN
+  l += launch_inpaint2(du, dv, w4u, w4v, m, n, iscratch, counts, status + 7, c->stream);
+  l += launch_inpaint_del4(du, dv, w4u, w4v, wfu, wfv, m, n, maxit, dscratch, counts, status, c->stream);
+  l += launch_median_fluct(du, dv, wfu, wfv, m, n, fu, fv, c->stream);
+  // the removed count goes to counts[2]: the last fill runs when u, v or the removal has NaN
+  l += launch_outlier_mark(fu, fv, m, n, (float)thr, du, dv, hole, counts + 2, c->stream);
+  l += launch_inpaint2(du, dv, du, dv, m, n, iscratch, counts, status + 7, c->stream);
+  l += launch_restore_holes(hole, m, n, du, dv, c->stream);
+  if (info) {
+    int st[19];
+    CK(cudaMemcpyAsync(st, status, sizeof(st), cudaMemcpyDeviceToHost, c->stream));
+    rc = finish(c, l);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(c->stream));
+    info[0] = st[18];
+    info[1] = st[16];
+    info[2] = std::max(st[1], st[4]);
+    info[3] = (st[2] && st[5]) ? 1 : 0;
+    return ALDIC_OK;
+  }
+  return finish(c, l);
+}
+
 int aldic_init_u0(aldic_ctx* c, int ny, int nx, const double* u, const double* v, int index, double* U0) {
   if (!c) return ALDIC_ERR_ARG;
   if (index != 0 && index != 1) return fail(c, ALDIC_ERR_ARG, "Init index %d (0 or 1)", index);
@@ -696,7 +773,8 @@ int aldic_init_u0(aldic_ctx* c, int ny, int nx, const double* u, const double* v
   size_t need = 0;
   for (Arg* a : {&au, &av, &ao})
     if (!is_device_ptr(a->user)) need += ((a->bytes + 255) & ~size_t(255)) + 256;
-  need += 4 * (bytes + 256) + inpaint_scratch_bytes(g) + 512;
+  const size_t i2 = 2 * (((inpaint_scratch_bytes(g) + 255) & ~(size_t)255) + 256);
+  need += 4 * (bytes + 256) + i2 + 512;
   int rc = arena_reserve(c, need);
   if (rc) return rc;
   for (Arg* a : {&au, &av, &ao}) {
@@ -712,24 +790,32 @@ int aldic_init_u0(aldic_ctx* c, int ny, int nx, const double* u, const double* v
   }
   double* wu = (double*)arena_take(c, bytes);
   double* wv = (double*)arena_take(c, bytes);
-  CK(cudaMemcpyAsync(wu, au.dev, bytes, cudaMemcpyDeviceToDevice, c->stream));
-  CK(cudaMemcpyAsync(wv, av.dev, bytes, cudaMemcpyDeviceToDevice, c->stream));
-  void* scratch = arena_take(c, inpaint_scratch_bytes(g));
-  int* status = (int*)arena_take(c, 64);
-  int l = launch_inpaint(wu, ny, nx, scratch, status, c->stream);
-  l += launch_inpaint(wv, ny, nx, scratch, status, c->stream);
-  if (index == 1) {  // the three spring outlier passes, each on a copy of the pass's input
-    double* tu = (double*)arena_take(c, bytes);
-    double* tv = (double*)arena_take(c, bytes);
-    for (int mode = 0; mode < 3; ++mode) {
-      CK(cudaMemcpyAsync(tu, wu, bytes, cudaMemcpyDeviceToDevice, c->stream));
-      CK(cudaMemcpyAsync(tv, wv, bytes, cudaMemcpyDeviceToDevice, c->stream));
-      l += launch_spring_pass(tu, tv, wu, wv, ny, nx, mode, c->stream);
-      l += launch_inpaint(wu, ny, nx, scratch, status, c->stream);
-      l += launch_inpaint(wv, ny, nx, scratch, status, c->stream);
-    }
+  void* scratch = arena_take(c, i2);
+  int* status = (int*)arena_take(c, 128);
+  const double* du = (const double*)au.dev;
+  const double* dv = (const double*)av.dev;
+  int l = 0;
+  if (index == 0) {  // the NaN entries solved into wu, wv; U0 takes u, v elsewhere
+    CK(cudaMemsetAsync(status, 0, 128, c->stream));
+    l += launch_nan_count(du, dv, ny, nx, status + 16, c->stream);
+    l += launch_inpaint2(du, dv, wu, wv, ny, nx, scratch, status + 16, status, c->stream);
+    l += launch_interleave_u0(du, dv, wu, wv, ny, nx, (double*)ao.dev, c->stream);
+    return finish(c, l);
   }
-  l += launch_interleave_u0(wu, wv, ny, nx, (double*)ao.dev, c->stream);
+  // index 1: working copies, then the three spring outlier passes, each on a copy of the
+  // pass's input
+  CK(cudaMemcpyAsync(wu, du, bytes, cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaMemcpyAsync(wv, dv, bytes, cudaMemcpyDeviceToDevice, c->stream));
+  l += launch_inpaint2(wu, wv, wu, wv, ny, nx, scratch, nullptr, status, c->stream);
+  double* tu = (double*)arena_take(c, bytes);
+  double* tv = (double*)arena_take(c, bytes);
+  for (int mode = 0; mode < 3; ++mode) {
+    CK(cudaMemcpyAsync(tu, wu, bytes, cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaMemcpyAsync(tv, wv, bytes, cudaMemcpyDeviceToDevice, c->stream));
+    l += launch_spring_pass(tu, tv, wu, wv, ny, nx, mode, c->stream);
+    l += launch_inpaint2(wu, wv, wu, wv, ny, nx, scratch, nullptr, status, c->stream);
+  }
+  l += launch_interleave_u0(wu, wv, wu, wv, ny, nx, (double*)ao.dev, c->stream);
   return finish(c, l);
 }
 

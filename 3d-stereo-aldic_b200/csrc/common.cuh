@@ -161,6 +161,20 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
+// Sum of one double per thread over the block, returned to every thread (fixed order: warp
+// shuffles, then the warp totals in warp order).  red holds blockDim.x / 32 doubles; the
+// leading barrier lets the same red serve call after call.
+__device__ __forceinline__ double block_sum_all(double v, double* red) {
+  v = warp_sum(v);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) red[wid] = v;
+  __syncthreads();
+  double s = 0.0;
+  for (int k = 0; k < (int)(blockDim.x >> 5); ++k) s += red[k];
+  return s;
+}
+
 // Block-wide sums of K doubles per thread; result in out[0..K) (shared), visible to all
 // threads after return.  scratch must hold (NT/32)*K doubles.
 template <int K, int NT>

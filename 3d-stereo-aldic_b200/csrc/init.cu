@@ -22,19 +22,6 @@ namespace {
 
 constexpr int kInitThreads = 1024;
 
-// Sum over the block, returned to every thread (fixed order: warp shuffles, then the 32
-// warp totals in warp order).
-__device__ __forceinline__ double block_sum_all(double v, double* red) {
-  v = warp_sum(v);
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  __syncthreads();  // red is reused call after call
-  if (lane == 0) red[wid] = v;
-  __syncthreads();
-  double s = 0.0;
-  for (int k = 0; k < (int)(blockDim.x >> 5); ++k) s += red[k];
-  return s;
-}
-
 // Grid neighbours (row-1, row+1, col-1, col+1) of linear index g in an m x n column-major grid.
 __device__ __forceinline__ int nbr(int g, int k, int m, int n) {
   const int r = g % m, c = g / m;
@@ -48,19 +35,41 @@ __device__ __forceinline__ int nbr(int g, int k, int m, int n) {
 
 }  // namespace
 
-// One CTA per grid: A (m x n, column-major) is overwritten at its NaN entries.  Scratch:
-// map (m n ints), list (m n ints), x, r, p, q (m n doubles each).  status[0] = unknowns,
-// status[1] = CG iterations, status[2] = 1 when the residual target was met.
-__global__ void __launch_bounds__(kInitThreads) inpaint_springs_kernel(double* __restrict__ A, int m, int n,
-                                                                       int* __restrict__ map, int* __restrict__ list,
-                                                                       double* __restrict__ x, double* __restrict__ r,
-                                                                       double* __restrict__ p, double* __restrict__ q,
+// One CTA per grid, blockIdx.x selecting the grid: the NaN entries of A_c (m x n,
+// column-major) are solved and written to the same entries of O_c (O_c may be A_c for an
+// in-place fill; no other entry of O_c is written).  Scratch per grid (stride bytes apart):
+// map (m n ints), list (m n ints), x, r, p, q (m n doubles each).  hint (optional): the
+// grid is skipped when hint[c] + hint[2] == 0, i.e. a caller-side count of its NaN entries
+// is zero.  status[3 c + 0] = unknowns, [3 c + 1] = CG iterations, [3 c + 2] = 1 when the
+// residual target was met.
+__global__ void __launch_bounds__(kInitThreads) inpaint_springs_kernel(const double* A0, const double* A1, double* O0,
+                                                                       double* O1, int m, int n, char* scratch,
+                                                                       size_t stride, const int* __restrict__ hint,
                                                                        int* __restrict__ status) {
   __shared__ double red[32];
   __shared__ int s_count;
   __shared__ int s_warp[32];
+  const int comp = blockIdx.x;
+  const double* A = comp ? A1 : A0;
+  double* O = comp ? O1 : O0;
+  status += 3 * comp;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
+  if (hint && hint[comp] + hint[2] == 0) {  // no NaN entry: nothing to read
+    if (tid == 0) {
+      status[0] = 0;
+      status[1] = 0;
+      status[2] = 1;
+    }
+    return;
+  }
   const int mn = m * n;
+  char* sc = scratch + (size_t)comp * stride;
+  int* map = (int*)sc;
+  int* list = map + mn;
+  double* x = (double*)(((uintptr_t)(list + mn) + 255) & ~(uintptr_t)255);
+  double* r = x + mn;
+  double* p = r + mn;
+  double* q = p + mn;
   // ---- compaction of the NaN entries, in grid order: every thread counts a contiguous
   // range, one block scan gives the offsets, the same ranges are written ----
   const int per = (mn + (int)blockDim.x - 1) / (int)blockDim.x;
@@ -85,7 +94,7 @@ __global__ void __launch_bounds__(kInitThreads) inpaint_springs_kernel(double* _
   }
   __syncthreads();
   const int nu = s_count;
-  if (nu == 0) {  // nothing to fill (the common case): one read of the grid
+  if (nu == 0) {  // nothing to fill: one read of the grid
     if (tid == 0) {
       status[0] = 0;
       status[1] = 0;
@@ -155,8 +164,8 @@ __global__ void __launch_bounds__(kInitThreads) inpaint_springs_kernel(double* _
     rr = rr_new;
     for (int u = tid; u < nu; u += blockDim.x) p[u] = r[u] + beta * p[u];
   }
-  __syncthreads();
-  for (int u = tid; u < nu; u += blockDim.x) A[list[u]] = x[u];
+  __syncthreads();  // every read of A done before an in-place write
+  for (int u = tid; u < nu; u += blockDim.x) O[list[u]] = x[u];
   if (tid == 0) {
     status[0] = nu;
     status[1] = it;
@@ -164,17 +173,20 @@ __global__ void __launch_bounds__(kInitThreads) inpaint_springs_kernel(double* _
   }
 }
 
-// U0 in mesh order from the inpainted grids u, v (ny x nx column-major, the search's
-// output layout): U0(2 i - 1) = u'(i), U0(2 i) = v'(i) with i running over the transposed
-// grid, XList fastest (func/Init.m:86-92).
-__global__ void interleave_u0_kernel(const double* __restrict__ u, const double* __restrict__ v, int ny, int nx,
+// U0 in mesh order from the inpainted grids (ny x nx column-major, the search's output
+// layout): U0(2 i - 1) = u'(i), U0(2 i) = v'(i) with i running over the transposed grid,
+// XList fastest (func/Init.m:86-92); u' is u where finite and the fill fu (written at the
+// NaN entries only) where NaN, v' likewise.
+__global__ void interleave_u0_kernel(const double* __restrict__ u, const double* __restrict__ v,
+                                     const double* __restrict__ fu, const double* __restrict__ fv, int ny, int nx,
                                      double* __restrict__ U0) {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i >= (long long)nx * ny) return;
   const int ix = (int)(i % nx), iy = (int)(i / nx);
   const long long g = iy + (long long)ix * ny;
-  U0[2 * i] = u[g];
-  U0[2 * i + 1] = v[g];
+  const double a = u[g], b = v[g];
+  U0[2 * i] = isnan(a) ? fu[g] : a;
+  U0[2 * i + 1] = isnan(b) ? fv[g] : b;
 }
 
 // MATLAB std(x, 'omitnan') of k values in order (mean first, then the squared deviations),
@@ -281,21 +293,21 @@ int launch_spring_pass(const double* ut, const double* vt, double* ui, double* v
 size_t inpaint_scratch_bytes(long long mn) { return (size_t)mn * (2 * sizeof(int) + 4 * sizeof(double)) + 1024; }
 
 int launch_inpaint(double* A, int m, int n, void* scratch, int* status, cudaStream_t st) {
-  const long long mn = (long long)m * n;
-  char* s = (char*)scratch;
-  int* map = (int*)s;
-  int* list = map + mn;
-  double* x = (double*)(((uintptr_t)(list + mn) + 255) & ~(uintptr_t)255);
-  double* r = x + mn;
-  double* p = r + mn;
-  double* q = p + mn;
-  inpaint_springs_kernel<<<1, kInitThreads, 0, st>>>(A, m, n, map, list, x, r, p, q, status);
+  inpaint_springs_kernel<<<1, kInitThreads, 0, st>>>(A, A, A, A, m, n, (char*)scratch, 0, nullptr, status);
   return 1;
 }
 
-int launch_interleave_u0(const double* u, const double* v, int ny, int nx, double* U0, cudaStream_t st) {
+int launch_inpaint2(const double* A0, const double* A1, double* O0, double* O1, int m, int n, void* scratch,
+                    const int* hint, int* status, cudaStream_t st) {
+  const size_t stride = (inpaint_scratch_bytes((long long)m * n) + 255) & ~(size_t)255;
+  inpaint_springs_kernel<<<2, kInitThreads, 0, st>>>(A0, A1, O0, O1, m, n, (char*)scratch, stride, hint, status);
+  return 1;
+}
+
+int launch_interleave_u0(const double* u, const double* v, const double* fu, const double* fv, int ny, int nx,
+                         double* U0, cudaStream_t st) {
   const long long n = (long long)nx * ny;
-  interleave_u0_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(u, v, ny, nx, U0);
+  interleave_u0_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(u, v, fu, fv, ny, nx, U0);
   return 1;
 }
 

@@ -105,7 +105,22 @@ struct CamPair {
 };
 size_t inpaint_scratch_bytes(long long mn);
 int launch_inpaint(double* A, int m, int n, void* scratch, int* status, cudaStream_t st);
-int launch_interleave_u0(const double* u, const double* v, int ny, int nx, double* U0, cudaStream_t st);
+// Two grids in one launch (one CTA each): NaN entries of A0 / A1 solved into O0 / O1;
+// scratch holds 2 x inpaint_scratch_bytes (each rounded up to 256); hint as the kernel's.
+int launch_inpaint2(const double* A0, const double* A1, double* O0, double* O1, int m, int n, void* scratch,
+                    const int* hint, int* status, cudaStream_t st);
+int launch_interleave_u0(const double* u, const double* v, const double* fu, const double* fv, int ny, int nx,
+                         double* U0, cudaStream_t st);
+size_t del4_scratch_bytes(long long mn);
+int launch_inpaint_del4(const double* A0, const double* A1, const double* X00, const double* X01, double* O0,
+                        double* O1, int m, int n, int maxit, void* scratch, const int* hint, int* status,
+                        cudaStream_t st);
+int launch_nan_count(const double* u, const double* v, int m, int n, int* counts, cudaStream_t st);
+int launch_median_fluct(const double* u, const double* v, const double* uf, const double* vf, int m, int n,
+                        float* fu, float* fv, cudaStream_t st);
+int launch_outlier_mark(const float* fu, const float* fv, int m, int n, float thr, double* u, double* v,
+                        unsigned char* hole, int* count, cudaStream_t st);
+int launch_restore_holes(const unsigned char* hole, int m, int n, double* u, double* v, cudaStream_t st);
 int launch_spring_pass(const double* ut, const double* vt, double* ui, double* vi, int m, int n, int mode,
                        cudaStream_t st);
 // dist = (k1, k2, k3, p1, p2); K 3 x 3 column-major (MATLAB)

@@ -201,7 +201,8 @@ class StereoPipeline:
                            "v": T.empty(g, **f64), "phi": T.empty(g, **f64), "U0": T.empty(2 * n, **f64),
                            "U": T.empty(2 * n, **f64), "F": T.empty(4 * n, **f64),
                            "conv": T.empty(n, dtype=T.int32, device=device),
-                           "mark": T.empty(n, dtype=T.uint8, device=device), "Ug": T.empty(2 * g, **f64)}
+                           "mark": T.empty(n, dtype=T.uint8, device=device), "Ug": T.empty(2 * g, **f64),
+                           "uo": T.empty(g, **f64), "vo": T.empty(g, **f64)}
         self.coordsR = T.empty((2, n), **f64)
         self.pairs = [T.empty((4, n), **f64), T.empty((4, n), **f64)]
         self.xyz = [{"xyz": T.empty(3 * n, **f64), "err": T.empty(n, **f64)} for _ in range(2)]
@@ -211,9 +212,15 @@ class StereoPipeline:
 
 
     def _search_to_U0(self, b, ctx, out=None):
-        """Init(u, v, Phi, x, y, 0): the search grids (nY x nX column-major) inpainted
+        """funRemoveOutliers(u, v, cc, 0, 100) (the end of IntegerSearchQuadtree), then
+        Init(u, v, Phi, x, y, 0): the search grids (nY x nX column-major) inpainted
         (inpaint_nans(., 4)) and interleaved in mesh order, on the device."""
-        ctx.init_u0(b["u"].view(self.nx, self.ny), b["v"].view(self.nx, self.ny), out=b["U0"] if out is None else out)
+        # on copies (uo, vo): the raw search grids stay for the search parity check
+        b["uo"].copy_(b["u"])
+        b["vo"].copy_(b["v"])
+        u, v = b["uo"].view(self.nx, self.ny), b["vo"].view(self.nx, self.ny)
+        ctx.remove_outliers(u, v, 100.0)
+        ctx.init_u0(u, v, out=b["U0"] if out is None else out)
 
     def step(self):
         T, st, ev = self.torch, self.streams, self.ev
@@ -362,10 +369,17 @@ def verify(pipe, scene, P, fr, nthreads=0, search_sample=48, seed=0):
         same = (sub[:, 0] == gu[pj, pi]) & (sub[:, 1] == gv[pj, pi])
         same |= np.isnan(sub[:, 0]) & np.isnan(gu[pj, pi])
         exact = int(same.sum())
+        # the bad-point removal over the whole grid against the oracle's, from the same search
+        uo, vo, bad = O.remove_outliers(gu, gv, 100.0)
+        du = b["uo"].cpu().numpy().reshape(pipe.nx, pipe.ny).T
+        dv = b["vo"].cpu().numpy().reshape(pipe.nx, pipe.ny).T
+        nan_same = np.array_equal(np.isnan(du), np.isnan(uo)) and np.array_equal(np.isnan(dv), np.isnan(vo))
+        out_err = float(max(np.nanmax(np.abs(du - uo)), np.nanmax(np.abs(dv - vo)))) if nan_same else None
         res[name] = {"n": int(n), "converged_gpu": int(fg.sum()), "converged_oracle": int(fo.sum()),
                      "counted": int(ok.sum()), "flag_match": float(np.mean(fg == fo)),
                      "uv_max_err": float(d[both].max()) if both.any() else None,
-                     "search_sample_exact": f"{exact}/{len(pick)}", "oracle_icgn_s": t_icgn}
+                     "search_sample_exact": f"{exact}/{len(pick)}", "outliers_removed": int(bad.size),
+                     "outliers_max_err": out_err, "oracle_icgn_s": t_icgn}
     return res
 
 
@@ -694,7 +708,9 @@ def run_aux(args, P):
                 ctx.set_mask(mask_d)
             ctx.compute_gradients()
             ctx.integer_search([P["s_temp"]] * 2, gx, gy, w, st, out=b)
-            # Init over the search grid, then every mesh node takes its nearest grid node
+            # bad-point removal and Init over the search grid, then every mesh node takes its
+            # nearest grid node
+            ctx.remove_outliers(b["u"].view(nx, ny), b["v"].view(nx, ny), 100.0)
             ctx.init_u0(b["u"].view(nx, ny), b["v"].view(nx, ny), out=b["Ug"])
             i = T.clamp(T.round((cxy[:, 0] - (1 + w / 2.0)) / st), 0, nx - 1).long()
             j = T.clamp(T.round((cxy[:, 1] - (1 + w / 2.0)) / st), 0, ny - 1).long()
@@ -856,8 +872,10 @@ def run_sequence(args, P):
         return {"U": T.empty(2 * n, **f64), "F": T.empty(4 * n, **f64), "conv": T.empty(n, dtype=T.int32, device=dev)}
 
     def grid_to_U0(b, ctx):
-        """Init(u, v, Phi, x, y, 0) on the device: the search grids inpainted, mesh order."""
+        """funRemoveOutliers(u, v, cc, 0, 100), then Init(u, v, Phi, x, y, 0) on the device:
+        the search grids inpainted, mesh order."""
         out = T.empty(2 * g, **f64)
+        ctx.remove_outliers(b["u"].view(nx, ny), b["v"].view(nx, ny), 100.0)
         ctx.init_u0(b["u"].view(nx, ny), b["v"].view(nx, ny), out=out)
         return out
 
@@ -1119,17 +1137,20 @@ def e2e_measure(A, scene, P, steps, local_rank):
     def stereo():
         u, v = search("S", "L0", "R0", P["s_stereo"])
         search_done.set()
+        u, v = ctx["S"].remove_outliers(u, v, 100.0)
         ctx["S"].init_u0(u, v, out=U0["S"])
         ctx["S"].local_icgn(1, crd, U0["S"], w, P["tol_stereo"], out=out["S"])
         stereo_done.set()
 
     def left():
         u, v = search("L", "L0", "L1", P["s_temp"], after=search_done)
+        u, v = ctx["L"].remove_outliers(u, v, 100.0)
         ctx["L"].init_u0(u, v, out=U0["L"])
         ctx["L"].local_icgn(1, crd, U0["L"], w, P["tol_temp"], out=out["L"])
 
     def right():
         u, v = search("R", "R0", "R1", P["s_temp"], after=search_done)
+        u, v = ctx["R"].remove_outliers(u, v, 100.0)
         stereo_done.wait()
         # right-camera mesh = left mesh + stereo match; initial guess: Init over the search
         # grid, then the nearest grid node of each right-image point
@@ -1157,8 +1178,10 @@ def e2e_measure(A, scene, P, steps, local_rank):
         for p, o in zip(pairs, tri):
             ctx["S"].triangulate(p, scene.KL, scene.KR, scene.R_rl, scene.T_rl, out=o)
         conv_total += sum(int(np.sum((out[k]["conv"] > 0) & (out[k]["conv"] < 100))) for k in ("S", "L", "R"))
-        h2d = 6 * imgs["L0"].nbytes + 3 * (2 * n * 8 + U0["S"].nbytes + 2 * g * 8) + 2 * pairs[0].nbytes
-        d2h = 3 * (grid_bytes + icgn_out_bytes + 2 * g * 8) + 2 * (tri[0]["xyz"].nbytes + tri[0]["err"].nbytes)
+        # per pass: the grids staged through the bad-point removal (2 g doubles each way), then
+        # through Init (2 g in, U0 out), the mesh, the IC-GN outputs
+        h2d = 6 * imgs["L0"].nbytes + 3 * (2 * n * 8 + U0["S"].nbytes + 4 * g * 8) + 2 * pairs[0].nbytes
+        d2h = 3 * (grid_bytes + icgn_out_bytes + 4 * g * 8) + 2 * (tri[0]["xyz"].nbytes + tri[0]["err"].nbytes)
         return h2d, d2h
 
     one()  # warm-up

@@ -139,6 +139,21 @@ int aldic_epipolar_icgn(aldic_ctx* ctx, int64_t n, const double* pts, int winsiz
  * 1 when the residual target was met; passing it makes the call wait for the device. */
 int aldic_inpaint_nans(aldic_ctx* ctx, int m, int n, double* A, int32_t* info);
 
+/* funRemoveOutliers(u, v, cc, 0, Thr0) with Thr0 = thr > 0 (func/funRemoveOutliers.m:16,
+ * :44-87; the call of func_quadtree/IntegerSearchQuadtree.m:158-160 uses 100), in place on
+ * the search's m x n column-major u and v grids: the median test of funMedRemoveOutliers
+ * (:374-390; inpaint_nans(., 3) of each grid, medFilt2 [2 2] 'symmetric' skipping the
+ * second neighbour, |u - median| / (median |u - median| + 0.1) in single precision) marks
+ * the entries whose sqrt(nfu^2 + nfv^2) > thr; they are set NaN in both grids, both are
+ * filled with inpaint_nans(., 4), and the entries NaN in u on entry are NaN again.
+ * maxit <= 0 takes the default limit of the method-3 solver (min(8 m n + 200, 20000)
+ * iterations).  info (optional, host, 4 ints): entries removed, NaN holes of u, the
+ * method-3 solver's iterations (larger of u and v), 1 when both met their residual
+ * target; passing it makes the call wait for the device.  The qDIC branch and the manual
+ * (prompting) branches of the reference are not implemented (thr <= 0 is an error). */
+int aldic_remove_outliers(aldic_ctx* ctx, int m, int n, double* u, double* v, double thr, int maxit,
+                          int32_t* info);
+
 /* Init(u, v, Phi, x, y, index) (func/Init.m): inpaint_nans(., 4) of the search's u and v
  * grids (ny x nx column-major, as aldic_integer_search returns them; left unchanged) (:13);
  * index 1 adds the three spring outlier passes (:29-166: nodes whose value departs from

@@ -318,6 +318,117 @@ def inpaint_nans4(A):
     return flat.reshape((m, n), order="F")
 
 
+def _del4_rows(m, n, nodes):
+    """Rows of inpaint_nans method 3's operator (func/inpaint_nans.m:257-321) for the listed
+    linear nodes (0-based, column-major, m rows x n columns): (node, column, coefficient)
+    triples summed over the four stencil sets exactly as the reference's sparse() calls
+    add them -- del^4 (13 points) for rows and columns 3..end-2, the 5-point del^2 on the
+    second / second-last row or column, and [1 -2 1] along the border rows and columns.  The
+    columns are the reference's linear (column-major) offsets, wraps on 2-row grids included."""
+    r = nodes % m + 1
+    c = nodes // m + 1                      # 1-based, as the reference's tests
+    trip = []
+
+    def add(sel, offs, coefs):
+        g = nodes[sel]
+        for o, w in zip(offs, coefs):
+            trip.append((g, g + o, np.full(g.size, float(w))))
+
+    add((r >= 3) & (r <= m - 2) & (c >= 3) & (c <= n - 2),
+        (-2 * m, -m - 1, -m, -m + 1, -2, -1, 0, 1, 2, m - 1, m, m + 1, 2 * m),
+        (1, 2, -8, 2, 1, -8, 20, -8, 1, 2, -8, 2, 1))
+    add((((r == 2) | (r == m - 1)) & (c >= 2) & (c <= n - 1)) | (((c == 2) | (c == n - 1)) & (r >= 2) & (r <= m - 1)),
+        (-m, -1, 0, 1, m), (1, 1, -4, 1, 1))
+    add(((r == 1) | (r == m)) & (c >= 2) & (c <= n - 1), (-m, 0, m), (1, -2, 1))
+    add(((c == 1) | (c == n)) & (r >= 2) & (r <= m - 1), (-1, 0, 1), (1, -2, 1))
+    if not trip:
+        return np.zeros(0, np.int64), np.zeros(0, np.int64), np.zeros(0)
+    return (np.concatenate([t[0] for t in trip]), np.concatenate([t[1] for t in trip]),
+            np.concatenate([t[2] for t in trip]))
+
+
+def inpaint_nans3(A):
+    """inpaint_nans(A, 3) (func/inpaint_nans.m:255-325): the NaN entries and their
+    neighbours under the 12-point del^4 template (identify_neighbors, :633-676) get the rows
+    of _del4_rows; the knowns move to the right-hand side (:323), the rows touching a NaN
+    column are kept (:324) and the NaN entries take the least-squares solution (:328,
+    MATLAB's sparse QR; here a dense SVD least-squares solve of the same system, exact for
+    the full-column-rank grids the tests use).  Restated in numpy / scipy."""
+    import scipy.sparse as sp
+
+    A = np.asarray(A, dtype=np.float64)
+    m, n = A.shape
+    flat = A.ravel(order="F").copy()
+    nan = np.flatnonzero(np.isnan(flat))
+    if nan.size == 0:
+        return A.copy()
+    r, c = nan % m, nan // m
+    talks = ((-2, 0), (-1, -1), (-1, 0), (-1, 1), (0, -2), (0, -1), (0, 1), (0, 2), (1, -1), (1, 0), (1, 1), (2, 0))
+    nb = []
+    for dr, dc in talks:
+        rr, cc = r + dr, c + dc
+        ok = (rr >= 0) & (rr < m) & (cc >= 0) & (cc < n)
+        nb.append((rr + cc * m)[ok])
+    nodes = np.union1d(nan, np.concatenate(nb))
+    i, j, w = _del4_rows(m, n, nodes)
+    if i.size and (j.min() < 0 or j.max() >= m * n):
+        raise IndexError("inpaint_nans3: a stencil index leaves the grid (the reference's sparse() errors)")
+    F = sp.csr_matrix((w, (i, j)), shape=(m * n, m * n))
+    F.sum_duplicates()
+    F.eliminate_zeros()
+    known = np.flatnonzero(~np.isnan(flat))
+    rhs = -(F[:, known] @ flat[known])
+    Fn = F[:, nan].tocsr()
+    k = np.flatnonzero(np.diff(Fn.indptr) > 0)
+    x = np.linalg.lstsq(Fn[k].toarray(), rhs[k], rcond=None)[0]
+    flat[nan] = x
+    return flat.reshape((m, n), order="F")
+
+
+def medfilt2_skip(V):
+    """medFilt2(V, [2 2], 'symmetric', 2) of func/funRemoveOutliers.m:393-441 in MATLAB's
+    single precision (the neighbour stack is single, :413): the median of V(r, c),
+    V(r+1, c), V(r+1, c+1) with the last row and column repeated past the edge (the
+    'post' symmetric pad of one, :403-409; neighbour 2 = V(r, c+1) is skipped, :426-431)."""
+    V = np.asarray(V).astype(np.float32)
+    P = np.pad(V, ((0, 1), (0, 1)), mode="symmetric")
+    st = np.stack([P[:-1, :-1], P[1:, :-1], P[1:, 1:]], 2)
+    return np.sort(st, 2)[:, :, 1]
+
+
+def med_remove_outliers(u, epsilon=0.1):
+    """funMedRemoveOutliers (func/funRemoveOutliers.m:374-390): the normalised median
+    fluctuation |u - median| / (median(|u - median|) + epsilon) of the method-3 inpainted
+    field, in single precision as MATLAB evaluates double op single."""
+    uf = inpaint_nans3(u)
+    med = medfilt2_skip(uf)
+    fl = (uf.astype(np.float32) - med).astype(np.float32)
+    res = medfilt2_skip(np.abs(fl))
+    return med, np.abs(fl / (res + np.float32(epsilon))).astype(np.float32)
+
+
+def remove_outliers(u, v, thr=100.0):
+    """[u, v] = funRemoveOutliers(u, v, cc, 0, Thr0) with Thr0 > 0 (func/funRemoveOutliers.m:
+    16, :44-87), the call IntegerSearchQuadtree makes (func_quadtree/IntegerSearchQuadtree.m:
+    158-160): entries whose |normalised fluctuation| (u and v combined) exceeds Thr0 are
+    set NaN, both grids are inpainted (method 4) and the original NaN holes (of u) are NaN
+    again.  Returns (u, v, list of removed linear indices, 0-based column-major)."""
+    u = np.asarray(u, dtype=np.float64)
+    v = np.asarray(v, dtype=np.float64)
+    hole = np.isnan(u)
+    _, n1 = med_remove_outliers(u)
+    _, n2 = med_remove_outliers(v)
+    mag = np.sqrt((n1 * n1 + n2 * n2).astype(np.float32)).astype(np.float32)
+    bad = mag > thr
+    u2, v2 = u.copy(), v.copy()
+    u2[bad] = np.nan
+    v2[bad] = np.nan
+    u2, v2 = inpaint_nans4(u2), inpaint_nans4(v2)
+    u2[hole] = np.nan
+    v2[hole] = np.nan
+    return u2, v2, np.flatnonzero(bad.ravel(order="F"))
+
+
 def _std8(vals):
     """MATLAB std(x, 'omitnan') of the listed values, summed in order (no fused operations)."""
     xs = [x for x in vals if not np.isnan(x)]

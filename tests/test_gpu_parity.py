@@ -562,8 +562,64 @@ def test_integer_search_quadtree_driver(A, ctx, affine):
     hole = mask[np.floor(x0 + 0.5).astype(int) - 1, np.floor(y0 + 0.5).astype(int) - 1] == 0
     assert hole.sum() > 10 and (~hole).sum() > 100
     assert np.isnan(u[hole]).all() and np.isnan(v[hole]).all()
-    assert np.array_equal(u[~hole], ur[~hole], equal_nan=True)
+    # then funRemoveOutliers(u, v, cc, 0, 100), as the oracle restates it
+    uo, vo, _ = O.remove_outliers(np.where(hole, np.nan, ur), np.where(hole, np.nan, vr), 100.0)
+    assert np.array_equal(np.isnan(u), np.isnan(uo)) and np.array_equal(np.isnan(v), np.isnan(vo))
+    assert np.nanmax(np.abs(u - uo)) < 1e-9 and np.nanmax(np.abs(v - vo)) < 1e-9
     assert list(para2["SizeOfFFTSearchRegion"]) == [10, 10]
+
+
+def _outlier_grids(seed, m=40, n=35):
+    rng = np.random.default_rng(seed)
+    R, C = np.meshgrid(np.arange(m, dtype=float), np.arange(n, dtype=float), indexing="ij")
+    u = np.round(3.37 + 0.02 * R - 0.01 * C + 0.3 * np.sin(R / 6.0), 3)
+    v = np.round(-1.82 + 0.015 * C + 0.2 * np.cos(C / 5.0), 3)
+    bad = rng.random((m, n)) < 0.03
+    u[bad] += rng.choice([-1, 1], bad.sum()) * rng.uniform(15, 60, bad.sum())
+    v[rng.random((m, n)) < 0.02] -= 30.0
+    u[14:19, 9:15] = np.nan  # a mask hole (as IntegerSearchQuadtree leaves it)
+    v[14:19, 9:15] = np.nan
+    u[0, 0] = v[0, 0] = np.nan
+    return u, v
+
+
+@pytest.mark.parametrize("seed", [0, 1])
+def test_remove_outliers_parity(A, ctx, seed):
+    """funRemoveOutliers(u, v, cc, 0, 100): the removed entries bit-exact against the oracle
+    (single-precision median test), the inpainted grids to 1e-9, the holes NaN again."""
+    import torch
+
+    u, v = _outlier_grids(seed)
+    uo, vo, bad = O.remove_outliers(u, v, 100.0)
+    ug, vg, info = ctx.remove_outliers(u, v, 100.0, info=True)
+    assert info[0] == bad.size and bad.size > 5
+    assert info[1] == int(np.isnan(u).sum()) and info[3] == 1
+    assert np.array_equal(np.isnan(ug), np.isnan(uo)) and np.array_equal(np.isnan(vg), np.isnan(vo))
+    assert np.nanmax(np.abs(ug - uo)) < 1e-9 and np.nanmax(np.abs(vg - vo)) < 1e-9
+    # the driver form and the device-tensor form (in place) agree with the host form
+    u2, v2, _ = A.funRemoveOutliers(u, v, {}, 0, 100, ctx=ctx)
+    assert np.array_equal(u2, ug, equal_nan=True) and np.array_equal(v2, vg, equal_nan=True)
+    tu = torch.from_numpy(np.ascontiguousarray(u.T)).cuda()
+    tv = torch.from_numpy(np.ascontiguousarray(v.T)).cuda()
+    ctx.remove_outliers(tu, tv, 100.0)
+    torch.cuda.synchronize()
+    assert np.array_equal(tu.cpu().numpy().T, ug, equal_nan=True)
+    assert np.array_equal(tv.cpu().numpy().T, vg, equal_nan=True)
+
+
+def test_remove_outliers_edges(A, ctx):
+    """No NaN and no outlier: the grids come back unchanged; empty grids are a no-op; a zero
+    threshold (the reference's prompt) is an error."""
+    R, C = np.meshgrid(np.arange(12.0), np.arange(9.0), indexing="ij")
+    u, v = 1.0 + 0.1 * R, 2.0 - 0.05 * C
+    ug, vg, info = ctx.remove_outliers(u, v, 100.0, info=True)
+    assert info == (0, 0, 0, 1) and np.array_equal(ug, u) and np.array_equal(vg, v)
+    e = np.zeros((0, 4))
+    assert ctx.remove_outliers(e, e)[0].shape == (0, 4)
+    with pytest.raises(A.AldicError):
+        ctx.remove_outliers(u, v, 0.0)
+    with pytest.raises(A.AldicError):
+        A.funRemoveOutliers(u, v, {}, 1, 100, ctx=ctx)
 
 
 def test_launch_counter_and_errors(A, ctx):
