@@ -52,6 +52,8 @@ SIGNATURES = {
     "aldic_inpaint_nans": (_i, [_vp, _i, _i, _vp, _vp]),
     "aldic_init_u0": (_i, [_vp, _i, _i, _vp, _vp, _i, _vp]),
     "aldic_remove_outliers": (_i, [_vp, _i, _i, _vp, _vp, _d, _i, _vp]),
+    "aldic_subpb2": (_i, [_vp, _i64, _vp, _i64, _vp, _i, _d, _d, _d, _vp, _vp, _i64, _vp, _d, _i, _vp,
+                          _vp]),
     "aldic_measure_fp32_peak": (_i, [_vp, C.POINTER(_d)]),
     "aldic_set_profiling": (_i, [_vp, _i]),
     "aldic_set_iteration_cap": (_i, [_vp, _i]),

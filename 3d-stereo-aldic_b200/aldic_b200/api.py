@@ -24,7 +24,7 @@ __all__ = [
     "Context", "default_context", "funNormalizeImg", "funImgGradient", "ba_interp2_spline", "funIntegerSearch",
     "LocalICGN", "LocalICGNQuadtree", "Subpb1", "Subpb1Quadtree", "epipolar_ICGN1",
     "stereoReconstruction_quadtree", "bad_points_local", "bad_points_subpb1", "Init", "funUndistortPoints",
-    "IntegerSearchQuadtree", "MeshSetUp", "funRemoveOutliers",
+    "IntegerSearchQuadtree", "MeshSetUp", "funRemoveOutliers", "Subpb2Quadtree",
 ]
 
 
@@ -345,6 +345,40 @@ class Context:
         self._check(rc, "aldic_remove_outliers")
         return (a, b, tuple(nfo)) if info else (a, b)
 
+    def subpb2(self, coords, elements, gauss_order, beta, mu, U, F, alpha=0.0, dirichlet=None, tol=0.0, maxit=0,
+               out=None, info=False):
+        """Subpb2Quadtree's global finite-element step: coords (n x 2), elements (n_el x 8,
+        1-based, 0 = no mid-side node), U (2n), F (4n), dirichlet node numbers (1-based).
+        Returns Uhat (2n), or fills `out`; info=True also returns (iterations, converged)."""
+        k = _Keep()
+        n = _count(coords, 2)
+        if _is_torch(elements):
+            E = elements
+            n_el = _count(elements, 8)  # an (8, n_el) int32 tensor: the column-major n_el x 8 table
+        else:
+            E = np.asarray(elements)
+            if E.ndim != 2 or E.shape[1] != 8:
+                raise AldicError("elements must be an n_el x 8 array (corners 1-4, mid-side nodes 5-8, 0 = none)")
+            n_el = int(E.shape[0])
+        if dirichlet is None:
+            d = np.zeros(0, np.int32)
+        elif _is_torch(dirichlet):
+            d = dirichlet.reshape(-1)
+        else:
+            d = np.ravel(np.asarray(dirichlet)).astype(np.int32)
+        nd = int(d.numel() if _is_torch(d) else d.size)
+        if out is None:
+            Uh, op = k.out(2 * n, np.float64)
+        else:
+            Uh, op = out, k.dst(out, np.float64, 2 * n)
+        nfo = (C.c_int32 * 2)()
+        rc = self.lib.aldic_subpb2(self.h, n, k.ptr(coords, np.float64), n_el, k.ptr(E, np.int32), int(gauss_order),
+                                   float(beta), float(mu), float(alpha), k.ptr(U, np.float64, numel=2 * n),
+                                   k.ptr(F, np.float64, numel=4 * n), nd, k.ptr(d, np.int32) if nd else None,
+                                   float(tol), int(maxit), op, nfo)
+        self._check(rc, "aldic_subpb2")
+        return (Uh, tuple(nfo)) if info else Uh
+
     def init_u0(self, u, v, out=None, index=0):
         """Init(u, v, Phi, x, y, index): inpaint the search grids (ny x nx, left unchanged;
         index 1 adds the spring outlier passes) and return U0 (2 nx ny, mesh order), or fill
@@ -467,6 +501,24 @@ def funIntegerSearch(f, g, tempSizeOfSearchRegion, gridx, gridy, winsize, winste
     st = int(np.ravel(winstepsize)[0])
     r = ctx.integer_search(tempSizeOfSearchRegion, gridx, gridy, w, st)
     return r["x"], r["y"], r["u"], r["v"], {"max": r["phi"], "A": []}
+
+
+def Subpb2Quadtree(DICmesh, GaussPtOrder, beta, mu, U, F, udual=None, vdual=None, alpha=0.0, winstepsize=None,
+                   waitBarDisplayOrNot=0, ctx: Context | None = None):
+    """[Uhat] = Subpb2Quadtree(DICmesh, GaussPtOrder, beta, mu, U, F, udual, vdual, alpha,
+    winstepsize, waitBarDisplayOrNot) (func_quadtree/Subpb2Quadtree.m): ALDIC's global
+    finite-element step on the device.  DICmesh holds coordinatesFEM (n x 2),
+    elementsFEM (n_el x 8) and dirichlet (node numbers, may be empty); a non-empty neumann
+    list raises (the drivers' quadtree meshes carry none).  udual, vdual and winstepsize do
+    not enter the result (the reference multiplies the duals by 0; winstepsize scales only
+    the neumann term)."""
+    neu = DICmesh.get("neumann")
+    if neu is not None and np.size(neu) > 0:
+        raise AldicError("Subpb2Quadtree: neumann boundary terms are not implemented")
+    ctx = ctx or default_context()
+    dirichlet = DICmesh.get("dirichlet")
+    return ctx.subpb2(DICmesh["coordinatesFEM"], DICmesh["elementsFEM"], GaussPtOrder, beta, mu, U, F, alpha=alpha,
+                      dirichlet=None if dirichlet is None or np.size(dirichlet) == 0 else dirichlet)
 
 
 def funRemoveOutliers(u, v, cc, qDICOrNot, Thr0, ctx: Context | None = None):

@@ -756,6 +756,112 @@ int aldic_remove_outliers(aldic_ctx* c, int m, int n, double* u, double* v, doub
   return finish(c, l);
 }
 
+int aldic_subpb2(aldic_ctx* c, int64_t n, const double* coords, int64_t n_el, const int32_t* elements,
+                 int gauss_order, double beta, double mu, double alpha, const double* U, const double* F,
+                 int64_t n_dirichlet, const int32_t* dirichlet, double tol, int maxit, double* Uhat,
+                 int32_t* info) {
+  if (!c) return ALDIC_ERR_ARG;
+  if (info) info[0] = info[1] = 0;
+  if (n <= 0 || n_el <= 0) return fail(c, ALDIC_ERR_ARG, "empty mesh (%lld nodes, %lld elements)", (long long)n,
+                                       (long long)n_el);
+  if (n > (1LL << 28) || n_el > (1LL << 27)) return fail(c, ALDIC_ERR_ARG, "mesh too large");
+  if (gauss_order < 2 || gauss_order > 5) return fail(c, ALDIC_ERR_ARG, "Gauss point order %d (2..5)", gauss_order);
+  if (!(beta + alpha > 0.0) && !(mu > 0.0))
+    return fail(c, ALDIC_ERR_ARG, "beta + alpha and mu are both 0: the system is singular");
+  if (!coords || !elements || !U || !F || !Uhat || (n_dirichlet > 0 && !dirichlet))
+    return fail(c, ALDIC_ERR_ARG, "missing array argument");
+  if (n_dirichlet < 0) return fail(c, ALDIC_ERR_ARG, "n_dirichlet < 0");
+  if (!(tol > 0.0)) tol = 1e-12;
+  if (maxit <= 0) maxit = (int)std::min<int64_t>(20 * n + 1000, 200000);
+  CK(cudaSetDevice(c->device));
+  // the mesh on the host: element table checks, node -> (element, slot) lists, node kinds
+  std::vector<int32_t> E((size_t)n_el * 8), dir((size_t)n_dirichlet);
+  if (is_device_ptr(elements)) {
+    CK(cudaMemcpy(E.data(), elements, E.size() * 4, cudaMemcpyDeviceToHost));
+  } else {
+    std::memcpy(E.data(), elements, E.size() * 4);
+  }
+  if (n_dirichlet > 0) {
+    if (is_device_ptr(dirichlet)) {
+      CK(cudaMemcpy(dir.data(), dirichlet, dir.size() * 4, cudaMemcpyDeviceToHost));
+    } else {
+      std::memcpy(dir.data(), dirichlet, dir.size() * 4);
+    }
+  }
+  std::vector<int> ptr, adj;
+  std::vector<unsigned char> kind;
+  char msg[160];
+  if (subpb2_mesh_tables(n, n_el, E.data(), n_dirichlet, dir.data(), ptr, adj, kind, msg, sizeof(msg)))
+    return fail(c, ALDIC_ERR_ARG, "%s", msg);
+  // device buffers: inputs staged, the mesh tables, K_e / b_e, the CG vectors
+  const size_t nb = (size_t)subpb2_blocks(n);
+  Arg ac{coords, (size_t)n * 16, false, nullptr}, au{U, (size_t)n * 16, false, nullptr},
+      af{F, (size_t)n * 32, false, nullptr}, ao{Uhat, (size_t)n * 16, true, nullptr};
+  c->arena.used = 0;
+  c->back.clear();
+  size_t need = 0;
+  for (Arg* a : {&ac, &au, &af, &ao})
+    if (!is_device_ptr(a->user)) need += ((a->bytes + 255) & ~size_t(255)) + 256;
+  const size_t two_n = (size_t)n * 16;
+  need += E.size() * 4 + ptr.size() * 4 + adj.size() * 4 + kind.size() + (size_t)n_el * (64 + 16) * 8 +
+          6 * two_n + (size_t)n * 8 + nb * 16 + subpb2_scalars_bytes() + 64 + 16 * 256;
+  int rc = arena_reserve(c, need);
+  if (rc) return rc;
+  for (Arg* a : {&ac, &au, &af, &ao}) {
+    if (is_device_ptr(a->user)) {
+      a->dev = const_cast<void*>(a->user);
+    } else {
+      a->dev = arena_take(c, a->bytes);
+      if (a->output)
+        c->back.push_back({const_cast<void*>(a->user), a->dev, a->bytes});
+      else
+        CK(cudaMemcpyAsync(a->dev, a->user, a->bytes, cudaMemcpyHostToDevice, c->stream));
+    }
+  }
+  int* dE = (int*)arena_take(c, E.size() * 4);
+  int* dptr = (int*)arena_take(c, ptr.size() * 4);
+  int* dadj = (int*)arena_take(c, std::max<size_t>(adj.size(), 1) * 4);
+  unsigned char* dkind = (unsigned char*)arena_take(c, kind.size());
+  double* Ke = (double*)arena_take(c, (size_t)n_el * 64 * 8);
+  double* be = (double*)arena_take(c, (size_t)n_el * 16 * 8);
+  double* b = (double*)arena_take(c, two_n);
+  double* r = (double*)arena_take(c, two_n);
+  double* z = (double*)arena_take(c, two_n);
+  double* p = (double*)arena_take(c, two_n);
+  double* q = (double*)arena_take(c, two_n);
+  double* D = (double*)arena_take(c, (size_t)n * 8);
+  double* part = (double*)arena_take(c, nb * 16);
+  Subpb2Scalars* sc = (Subpb2Scalars*)arena_take(c, subpb2_scalars_bytes() + 64);
+  // the tables are copied from pageable host vectors: the copies complete before return
+  CK(cudaMemcpyAsync(dE, E.data(), E.size() * 4, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(dptr, ptr.data(), ptr.size() * 4, cudaMemcpyHostToDevice, c->stream));
+  if (!adj.empty()) CK(cudaMemcpyAsync(dadj, adj.data(), adj.size() * 4, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(dkind, kind.data(), kind.size(), cudaMemcpyHostToDevice, c->stream));
+  double* x = (double*)ao.dev;  // the solution builds in the output
+  int l = launch_subpb2_setup((int)n_el, dE, (const double*)ac.dev, n, (const double*)au.dev, (const double*)af.dev,
+                              gauss_order, beta, mu, alpha, dptr, dadj, dkind, Ke, be, b, D, x, r, z, p, part, sc,
+                              c->stream);
+  // batches of 16 iterations; the scalars are read back between batches (the kernels of a
+  // batch that starts after convergence return at once)
+  std::vector<unsigned char> host_sc(subpb2_scalars_bytes());
+  int it = 0, done = 0, ok = 0;
+  for (int launched = 0; launched < maxit;) {
+    const int k = std::min(16, maxit - launched);
+    l += launch_subpb2_iterations(k, (int)n_el, dE, n, dptr, dadj, Ke, dkind, D, x, r, z, p, q, part, tol * tol,
+                                  maxit, sc, c->stream);
+    launched += k;
+    CK(cudaMemcpyAsync(host_sc.data(), sc, host_sc.size(), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    subpb2_read_status(host_sc.data(), &it, &done, &ok);
+    if (done) break;
+  }
+  if (info) {
+    info[0] = it;
+    info[1] = ok;
+  }
+  return finish(c, l);
+}
+
 int aldic_init_u0(aldic_ctx* c, int ny, int nx, const double* u, const double* v, int index, double* U0) {
   if (!c) return ALDIC_ERR_ARG;
   if (index != 0 && index != 1) return fail(c, ALDIC_ERR_ARG, "Init index %d (0 or 1)", index);

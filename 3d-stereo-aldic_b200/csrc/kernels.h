@@ -1,6 +1,8 @@
 // Internal kernel interfaces of the ALDIC B200 library (not part of the public C ABI).
 #pragma once
 #include <cuda_runtime.h>
+
+#include <vector>
 #include <stddef.h>
 #include <stdint.h>
 
@@ -121,6 +123,28 @@ int launch_median_fluct(const double* u, const double* v, const double* uf, cons
 int launch_outlier_mark(const float* fu, const float* fv, int m, int n, float thr, double* u, double* v,
                         unsigned char* hole, int* count, cudaStream_t st);
 int launch_restore_holes(const unsigned char* hole, int m, int n, double* u, double* v, cudaStream_t st);
+// ALDIC's global step (Subpb2Quadtree), subpb2.cu
+struct Subpb2Scalars;
+size_t subpb2_scalars_bytes();
+int subpb2_blocks(long long n);
+int launch_subpb2_setup(int n_el, const int* elem, const double* coords, long long n, const double* U,
+                        const double* F, int order, double beta, double mu, double alpha, const int* adj_ptr,
+                        const int* adj, const unsigned char* free_, double* Ke, double* be, double* b, double* D,
+                        double* x, double* r, double* z, double* p, double* part, Subpb2Scalars* sc,
+                        cudaStream_t st);
+int launch_subpb2_iterations(int iters, int n_el, const int* elem, long long n, const int* adj_ptr, const int* adj,
+                             const double* Ke, const unsigned char* free_, const double* D, double* x, double* r,
+                             double* z, double* p, double* q, double* part, double tol2, int maxit,
+                             Subpb2Scalars* sc, cudaStream_t st);
+// Host: the mesh tables of a Subpb2 call from the element table E (n_el x 8 column-major,
+// 1-based, 0 = absent mid-side node) and the dirichlet node numbers: ptr / adj, each node's
+// (element * 8 + slot) entries in element order; kind per node, 1 free, 2 dirichlet, 0
+// neither.  Returns non-zero with a message for a bad node number.
+int subpb2_mesh_tables(long long n, long long n_el, const int* E, long long n_dir, const int* dir,
+                       std::vector<int>& ptr, std::vector<int>& adj, std::vector<unsigned char>& kind, char* msg,
+                       size_t msg_len);
+// (iterations, done, converged) of the last solve, from the device scalars (host copy).
+void subpb2_read_status(const void* host_copy, int* it, int* done, int* ok);
 int launch_spring_pass(const double* ut, const double* vt, double* ui, double* vi, int m, int n, int mode,
                        cudaStream_t st);
 // dist = (k1, k2, k3, p1, p2); K 3 x 3 column-major (MATLAB)

@@ -130,6 +130,25 @@ int aldic_subpb1(aldic_ctx* ctx, int variant, int64_t n, const double* coords, c
  * offset Df.DfAxis(1) = 4; znssd = ZNSSD of the final iteration (NaN on failure). */
 int aldic_epipolar_icgn(aldic_ctx* ctx, int64_t n, const double* pts, int winsize, double tol, double* znssd);
 
+/* ---------------------------------------------------- ALDIC global step ------- */
+/* [Uhat] = Subpb2Quadtree(DICmesh, GaussPtOrder, beta, mu, U, F, udual, vdual, alpha,
+ * winstepsize, 0) (func_quadtree/Subpb2Quadtree.m) with an empty neumann list: the global
+ * finite-element step of the augmented Lagrangian on a quadtree mesh of n nodes (coords n x 2
+ * column-major) and n_el elements (elements n_el x 8 column-major, 1-based: corners 1-4,
+ * mid-side hanging nodes 5-8 on the right / top / left / bottom edge, 0 where absent).
+ * Element matrices sum_g |J| w ((beta + alpha) DN' DN + mu N' N) at gauss_order^2 points
+ * (2..5), right-hand side from U (2n interleaved) and F (4n, F11 F21 F12 F22 per node); the
+ * duals do not enter (the reference multiplies them by 0).  Nodes of the elements (but the
+ * first entry of unique(elementsFEM), as the reference) are free, the n_dirichlet
+ * dirichlet nodes (1-based) hold U, all other nodes get 0.  Solved by Jacobi-preconditioned
+ * conjugate gradients in FP64 to |r| <= tol |r0| (tol <= 0: 1e-12) within maxit iterations
+ * (<= 0: min(20 n + 1000, 200000)); the reference solves the free block directly.
+ * Uhat: 2n.  info (optional, host, 2 ints): iterations, 1 when the tolerance was met. */
+int aldic_subpb2(aldic_ctx* ctx, int64_t n, const double* coords, int64_t n_el, const int32_t* elements,
+                 int gauss_order, double beta, double mu, double alpha, const double* U, const double* F,
+                 int64_t n_dirichlet, const int32_t* dirichlet, double tol, int maxit, double* Uhat,
+                 int32_t* info);
+
 /* ------------------------------------------------------ initial guess --------- */
 /* inpaint_nans(A, 4) (func/inpaint_nans.m:369-398, spring analogy), in place on an m x n
  * column-major grid: the NaN entries become the least-squares solution of unit springs

@@ -429,6 +429,139 @@ def remove_outliers(u, v, thr=100.0):
     return u2, v2, np.flatnonzero(bad.ravel(order="F"))
 
 
+def _gauss_rule(order):
+    """Gauss points and weights of func_quadtree/Subpb2Quadtree.m:60-77 (orders 4 and 5 with
+    the file's rounded constants)."""
+    if order == 2:
+        return [-1 / np.sqrt(3), 1 / np.sqrt(3)], [1.0, 1.0]
+    if order == 3:
+        return [0.0, np.sqrt(3 / 5), -np.sqrt(3 / 5)], [8 / 9, 5 / 9, 5 / 9]
+    if order == 4:
+        return [0.339981, -0.339981, 0.861136, -0.861136], [0.652145, 0.652145, 0.347855, 0.347855]
+    if order == 5:
+        return [0.0, 0.538469, -0.538469, 0.90618, -0.90618], [0.568889, 0.478629, 0.478629, 0.236927, 0.236927]
+    raise ValueError("Gauss point order must be 2..5")
+
+
+def quadtree_shape(ksi, eta, present):
+    """The 8-node quadtree element's shape functions and their (ksi, eta) derivatives
+    (func_quadtree/Subpb2Quadtree.m:138-148 and the funDN* functions :343-396): corners 1-4,
+    mid-side (hanging) nodes 5-8 switched on by `present` (4 flags); sign(0) = 0 as MATLAB's."""
+    d5, d6, d7, d8 = (1.0 if f else 0.0 for f in present)
+    sg = np.sign
+    N5 = d5 * 0.5 * (1 + ksi) * (1 - abs(eta))
+    N6 = d6 * 0.5 * (1 + eta) * (1 - abs(ksi))
+    N7 = d7 * 0.5 * (1 - ksi) * (1 - abs(eta))
+    N8 = d8 * 0.5 * (1 - eta) * (1 - abs(ksi))
+    N = np.array([(1 - ksi) * (1 - eta) * 0.25 - 0.5 * (N7 + N8), (1 + ksi) * (1 - eta) * 0.25 - 0.5 * (N8 + N5),
+                  (1 + ksi) * (1 + eta) * 0.25 - 0.5 * (N5 + N6), (1 - ksi) * (1 + eta) * 0.25 - 0.5 * (N6 + N7),
+                  N5, N6, N7, N8])
+    k5, e5 = d5 * 0.5 * (1 - abs(eta)), d5 * 0.5 * (1 + ksi) * sg(-eta)
+    k6, e6 = d6 * 0.5 * (1 + eta) * sg(-ksi), d6 * 0.5 * (1 - abs(ksi))
+    k7, e7 = d7 * 0.5 * (-1) * (1 - abs(eta)), d7 * 0.5 * (1 - ksi) * sg(-eta)
+    k8, e8 = d8 * 0.5 * (1 - eta) * sg(-ksi), d8 * 0.5 * (-1) * (1 - abs(ksi))
+    dk = np.array([-0.25 * (1 - eta) - 0.5 * (k7 + k8), 0.25 * (1 - eta) - 0.5 * (k8 + k5),
+                   0.25 * (1 + eta) - 0.5 * (k5 + k6), -0.25 * (1 + eta) - 0.5 * (k6 + k7), k5, k6, k7, k8])
+    de = np.array([-0.25 * (1 - ksi) - 0.5 * (e7 + e8), -0.25 * (1 + ksi) - 0.5 * (e8 + e5),
+                   0.25 * (1 + ksi) - 0.5 * (e5 + e6), 0.25 * (1 - ksi) - 0.5 * (e6 + e7), e5, e6, e7, e8])
+    return N, dk, de
+
+
+def subpb2_element(xy, present, order, beta, mu, alpha):
+    """Element matrices of Subpb2Quadtree (:149-204) for one element: xy (8 x 2, zeros at absent
+    mid-side nodes, as the reference), returns the 16 x 16 element matrix
+    sum_g |J| w ((beta + alpha) DN' DN + mu N' N) in the reference's dof order
+    [x1 y1 x2 y2 ... x8 y8], and per Gauss point the data the right-hand side needs."""
+    pts, wts = _gauss_rule(order)
+    A = np.zeros((16, 16))
+    gp = []
+    for je, eta in enumerate(pts):          # ndgrid: ksi runs fastest
+        for ik, ksi in enumerate(pts):
+            w = wts[ik] * wts[je]
+            N, dk, de = quadtree_shape(ksi, eta, present)
+            J = np.array([[dk @ xy[:, 0], dk @ xy[:, 1]], [de @ xy[:, 0], de @ xy[:, 1]]])
+            jac = J[0, 0] * J[1, 1] - J[0, 1] * J[1, 0]
+            inv = np.array([[J[1, 1], -J[0, 1]], [-J[1, 0], J[0, 0]]]) / jac
+            dx = inv[0, 0] * dk + inv[0, 1] * de
+            dy = inv[1, 0] * dk + inv[1, 1] * de
+            Nm = np.zeros((2, 16))
+            Nm[0, 0::2], Nm[1, 1::2] = N, N
+            DN = np.zeros((4, 16))
+            DN[0, 0::2], DN[1, 0::2], DN[2, 1::2], DN[3, 1::2] = dx, dy, dx, dy
+            A += jac * w * ((beta + alpha) * DN.T @ DN + mu * Nm.T @ Nm)
+            gp.append((jac * w, Nm, DN))
+    return A, gp
+
+
+def subpb2_element_rhs(gp, beta, mu, alpha, ue, Fr):
+    """Element right-hand side of Subpb2Quadtree (:203): sum_g |J| w (beta diag(DN' Fr') +
+    mu N' N ue + alpha DN' DN ue); Fr holds, per dof row, the reference's F index row
+    (F11, F12, F21, F22 of the dof's node)."""
+    be = np.zeros(16)
+    for jw, Nm, DN in gp:
+        be += jw * (beta * np.einsum("ki,ik->i", DN, Fr) + mu * Nm.T @ Nm @ ue + alpha * DN.T @ DN @ ue)
+    return be
+
+
+def subpb2_quadtree(coords, elements, order, beta, mu, U, F, alpha=0.0, dirichlet=()):
+    """[Uhat] = Subpb2Quadtree(DICmesh, GaussPtOrder, beta, mu, U, F, udual, vdual, alpha, ...)
+    (func_quadtree/Subpb2Quadtree.m) with an empty neumann list: the element matrices and
+    right-hand sides assembled element by element (:94-222; v and W are 0 * the duals,
+    :40-41, so only U and F enter), the involved nodes all nodes of the elements but the
+    first of unique(elementsFEM) (:234-238, the reference's way of dropping the 0 entry),
+    the dirichlet nodes held at U (:271-273) and moved to the right-hand side, the free dofs
+    solved directly (:276).  coords n x 2, elements n_el x 8 (1-based, 0 = no mid-side
+    node), U 2n, F 4n; returns Uhat (2n; 0 at nodes neither free nor dirichlet)."""
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spla
+
+    coords = np.asarray(coords, dtype=np.float64)
+    E = np.asarray(elements, dtype=np.int64)
+    n = coords.shape[0]
+    U = np.asarray(U, dtype=np.float64).ravel()
+    F = np.asarray(F, dtype=np.float64).ravel()
+    rows, cols, vals = [], [], []
+    b = np.zeros(2 * n)
+    for e in range(E.shape[0]):
+        ids = E[e, :8]
+        present = [ids[k] != 0 for k in range(4, 8)]
+        xy = np.zeros((8, 2))
+        for k in range(8):
+            if ids[k] != 0:
+                xy[k] = coords[ids[k] - 1]
+        A, gp = subpb2_element(xy, present, order, beta, mu, alpha)
+        dof = np.full(16, -1)
+        for k in range(8):
+            if ids[k] != 0:
+                dof[2 * k], dof[2 * k + 1] = 2 * (ids[k] - 1), 2 * (ids[k] - 1) + 1
+        ue = np.array([U[d] if d >= 0 else 0.0 for d in dof])
+        # the reference's F index rows: (F11, F12) for an x dof, (F21, F22) for a y dof
+        Fr = np.zeros((16, 4))
+        for k in range(8):
+            if ids[k] != 0:
+                a = ids[k] - 1
+                Fr[2 * k] = Fr[2 * k + 1] = [F[4 * a], F[4 * a + 2], F[4 * a + 1], F[4 * a + 3]]
+        be = subpb2_element_rhs(gp, beta, mu, alpha, ue, Fr)
+        ok = dof >= 0
+        ii, jj = np.meshgrid(dof[ok], dof[ok], indexing="ij")
+        rows.append(ii.ravel())
+        cols.append(jj.ravel())
+        vals.append(A[np.ix_(ok, ok)].ravel())
+        np.add.at(b, dof[ok], be[ok])
+    A = sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=(2 * n, 2 * n))
+    involved = np.unique(E[:, :8])[1:] - 1
+    dnodes = np.unique(np.asarray(dirichlet, dtype=np.int64).ravel()) - 1 if np.size(dirichlet) else \
+        np.zeros(0, np.int64)
+    Uhat = np.zeros(2 * n)
+    Uhat[2 * dnodes] = U[2 * dnodes]
+    Uhat[2 * dnodes + 1] = U[2 * dnodes + 1]
+    b = b - A @ Uhat
+    fn = np.setdiff1d(involved, dnodes)
+    free = np.sort(np.concatenate([2 * fn, 2 * fn + 1]))
+    Uhat[free] = spla.spsolve(A[free][:, free].tocsc(), b[free])
+    return Uhat
+
+
 def _std8(vals):
     """MATLAB std(x, 'omitnan') of the listed values, summed in order (no fused operations)."""
     xs = [x for x in vals if not np.isnan(x)]

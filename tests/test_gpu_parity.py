@@ -628,3 +628,66 @@ def test_launch_counter_and_errors(A, ctx):
     assert ctx.launches > before
     with pytest.raises(A.AldicError):
         ctx.local_icgn(1, np.zeros((3, 2)), np.zeros(6), 1000, 1e-3)
+
+
+@pytest.mark.parametrize("order,dirichlet", [(2, ()), (2, (4, 9, 17, 30)), (3, (2,))])
+def test_subpb2_parity(A, ctx, order, dirichlet):
+    """Subpb2Quadtree: the device's element assembly and preconditioned CG against the
+    oracle's element-by-element assembly and direct solve, on a quadtree mesh with hanging
+    nodes; the driver form with a DICmesh dict gives the same."""
+    from test_subpb2_host import quadtree_mesh
+
+    C, E = quadtree_mesh(7, {(1, 1), (2, 1), (4, 4), (5, 2)})
+    n = C.shape[0]
+    rng = np.random.default_rng(11 + order)
+    U = 3.0 + rng.standard_normal(2 * n)
+    F = 0.01 * rng.standard_normal(4 * n)
+    for beta in (1e-3 * 16 ** 2 * 1e-3, 1e-1 * 16 ** 2 * 1e-3):
+        ref = O.subpb2_quadtree(C, E, order, beta, 1e-3, U, F, dirichlet=dirichlet)
+        got, nfo = ctx.subpb2(C, E, order, beta, 1e-3, U, F, dirichlet=dirichlet or None, info=True)
+        assert nfo[1] == 1 and nfo[0] > 0
+        assert np.abs(got - ref).max() < 1e-9 * max(1.0, np.abs(ref).max())
+    mesh = {"coordinatesFEM": C, "elementsFEM": E, "dirichlet": list(dirichlet), "neumann": []}
+    drv = A.Subpb2Quadtree(mesh, order, beta, 1e-3, U, F, np.zeros(4 * n), np.zeros(2 * n), 0.0, 16, 0, ctx=ctx)
+    assert np.array_equal(drv, got)
+
+
+def test_subpb2_device_tensors_and_errors(A, ctx):
+    """Device-resident inputs and output give the host result; bad tables and parameters
+    are errors, not faults."""
+    import torch
+
+    from test_subpb2_host import quadtree_mesh
+
+    C, E = quadtree_mesh(5, {(1, 2), (3, 3)})
+    n = C.shape[0]
+    rng = np.random.default_rng(3)
+    U = rng.standard_normal(2 * n)
+    F = 0.02 * rng.standard_normal(4 * n)
+    host = ctx.subpb2(C, E, 2, 0.0256, 1e-3, U, F)
+    dev = torch.device("cuda:0")
+    tC = torch.from_numpy(np.ascontiguousarray(C.T)).to(dev)
+    tE = torch.from_numpy(np.ascontiguousarray(E.T.astype(np.int32))).to(dev)
+    tU, tF = torch.from_numpy(U).to(dev), torch.from_numpy(F).to(dev)
+    out = torch.empty(2 * n, dtype=torch.float64, device=dev)
+    ctx.subpb2(tC, tE, 2, 0.0256, 1e-3, tU, tF, out=out)
+    torch.cuda.synchronize()
+    assert np.array_equal(out.cpu().numpy(), host)
+    bad = E.copy()
+    bad[0, 0] = 0
+    with pytest.raises(A.AldicError):
+        ctx.subpb2(C, bad, 2, 0.0256, 1e-3, U, F)
+    bad = E.copy()
+    bad[1, 5] = n + 3
+    with pytest.raises(A.AldicError):
+        ctx.subpb2(C, bad, 2, 0.0256, 1e-3, U, F)
+    with pytest.raises(A.AldicError):
+        ctx.subpb2(C, E, 6, 0.0256, 1e-3, U, F)
+    with pytest.raises(A.AldicError):
+        ctx.subpb2(C, E, 2, 0.0, 0.0, U, F)
+    with pytest.raises(A.AldicError):
+        ctx.subpb2(C, E, 2, 0.0256, 1e-3, U, F, dirichlet=[n + 1])
+    with pytest.raises(A.AldicError):
+        A.Subpb2Quadtree({"coordinatesFEM": C, "elementsFEM": E, "neumann": [[1, 2, 0, 1]]}, 2, 0.1, 1e-3, U, F,
+                         ctx=ctx)
+
