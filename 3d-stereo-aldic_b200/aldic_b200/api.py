@@ -24,7 +24,7 @@ __all__ = [
     "Context", "default_context", "funNormalizeImg", "funImgGradient", "ba_interp2_spline", "funIntegerSearch",
     "LocalICGN", "LocalICGNQuadtree", "Subpb1", "Subpb1Quadtree", "epipolar_ICGN1",
     "stereoReconstruction_quadtree", "bad_points_local", "bad_points_subpb1", "Init", "funUndistortPoints",
-    "IntegerSearchQuadtree", "MeshSetUp", "funRemoveOutliers", "Subpb2Quadtree",
+    "IntegerSearchQuadtree", "MeshSetUp", "funRemoveOutliers", "Subpb2Quadtree", "GenerateQuadtreeMesh",
 ]
 
 
@@ -119,6 +119,7 @@ class Context:
         self.h = h
         self.device = device
         self.M = self.N = None
+        self._sp2_nel = -1  # elements of the resident global-step mesh (none yet)
 
     def close(self):
         if getattr(self, "h", None):
@@ -345,6 +346,27 @@ class Context:
         self._check(rc, "aldic_remove_outliers")
         return (a, b, tuple(nfo)) if info else (a, b)
 
+    @staticmethod
+    def _elements(elements):
+        if _is_torch(elements):
+            return elements, _count(elements, 8)  # an (8, n_el) int32 tensor: the column-major n_el x 8 table
+        E = np.asarray(elements)
+        if E.ndim != 2 or E.shape[1] != 8:
+            raise AldicError("elements must be an n_el x 8 array (corners 1-4, mid-side nodes 5-8, 0 = none)")
+        return E, int(E.shape[0])
+
+    def subpb2_set_mesh(self, n, elements, dirichlet=None):
+        """Keep a global-step mesh (n nodes; elements n_el x 8; dirichlet node numbers)
+        resident for subpb2(..., elements=None, ...)."""
+        k = _Keep()
+        E, n_el = self._elements(elements)
+        d = np.zeros(0, np.int32) if dirichlet is None or np.size(dirichlet) == 0 else \
+            np.ravel(np.asarray(dirichlet)).astype(np.int32)
+        rc = self.lib.aldic_subpb2_set_mesh(self.h, int(n), n_el, k.ptr(E, np.int32), int(d.size),
+                                            k.ptr(d, np.int32) if d.size else None)
+        self._check(rc, "aldic_subpb2_set_mesh")
+        self._sp2_nel = n_el
+
     def subpb2(self, coords, elements, gauss_order, beta, mu, U, F, alpha=0.0, dirichlet=None, tol=0.0, maxit=0,
                out=None, info=False):
         """Subpb2Quadtree's global finite-element step: coords (n x 2), elements (n_el x 8,
@@ -352,14 +374,12 @@ class Context:
         Returns Uhat (2n), or fills `out`; info=True also returns (iterations, converged)."""
         k = _Keep()
         n = _count(coords, 2)
-        if _is_torch(elements):
-            E = elements
-            n_el = _count(elements, 8)  # an (8, n_el) int32 tensor: the column-major n_el x 8 table
+        if elements is None:  # the resident mesh of subpb2_set_mesh
+            E, n_el = None, self._sp2_nel
+            if dirichlet is not None:
+                raise AldicError("the resident mesh carries its dirichlet nodes")
         else:
-            E = np.asarray(elements)
-            if E.ndim != 2 or E.shape[1] != 8:
-                raise AldicError("elements must be an n_el x 8 array (corners 1-4, mid-side nodes 5-8, 0 = none)")
-            n_el = int(E.shape[0])
+            E, n_el = self._elements(elements)
         if dirichlet is None:
             d = np.zeros(0, np.int32)
         elif _is_torch(dirichlet):
@@ -372,7 +392,8 @@ class Context:
         else:
             Uh, op = out, k.dst(out, np.float64, 2 * n)
         nfo = (C.c_int32 * 2)()
-        rc = self.lib.aldic_subpb2(self.h, n, k.ptr(coords, np.float64), n_el, k.ptr(E, np.int32), int(gauss_order),
+        rc = self.lib.aldic_subpb2(self.h, n, k.ptr(coords, np.float64), n_el,
+                                   None if E is None else k.ptr(E, np.int32), int(gauss_order),
                                    float(beta), float(mu), float(alpha), k.ptr(U, np.float64, numel=2 * n),
                                    k.ptr(F, np.float64, numel=4 * n), nd, k.ptr(d, np.int32) if nd else None,
                                    float(tol), int(maxit), op, nfo)
@@ -597,6 +618,179 @@ def MeshSetUp(x, y, DICpara):
             "dirichlet": [], "neumann": [], "x0": xt, "y0": yt, "M": M, "N": N,
             "y0World": img_n + 1 - yt,
             "coordinatesFEMWorld": np.stack([coordinatesFEM[:, 0], img_n + 1 - coordinatesFEM[:, 1]], 1)}
+
+
+def _box_sums(mask):
+    """Inclusive box sums over a 1-based (x, y) pixel box of a mask, from its integral image."""
+    S = np.zeros((mask.shape[0] + 1, mask.shape[1] + 1))
+    S[1:, 1:] = np.cumsum(np.cumsum(np.asarray(mask, dtype=np.float64), 0), 1)
+
+    def box(x0, x1, y0, y1):  # MATLAB mask(x0:x1, y0:y1), 1-based inclusive
+        return S[x1, y1] - S[x0 - 1, y1] - S[x1, y0 - 1] + S[x0 - 1, y0 - 1]
+
+    return box
+
+
+def GenerateQuadtreeMesh(U0, Df, fNormalizedMask, DICmesh, DICpara):
+    """[DICmesh, DICpara, U0] = GenerateQuadtreeMesh(U0, Df, fNormalizedMask, DICmesh, DICpara)
+    (func_quadtree/GenerateQuadtreeMesh.m), host bookkeeping as in the reference:
+      * from the uniform mesh of MeshSetUp, elements whose pixel box meets both values of the
+        mask (funMarkEdge: max - min > 0) and are larger than DICmesh['elementMinSize'] are
+        split in four, pass after pass (:27-36); a split also splits any coarser neighbour of
+        the split element, so that every edge carries at most one hanging node (the
+        1-irregular rule of the red refinement QrefineR applies; QrefineR itself is not
+        vendored with the reference, so its node and element numbering is not restated:
+        existing nodes keep their numbers, new nodes follow in element order);
+      * corners in the reference's order (:40-48: (xmin, ymin), (xmax, ymin), (xmax, ymax),
+        (xmin, ymax)) and hanging nodes in slots 5-8 (right, top, left, bottom edge, :50-67);
+      * elements whose box is less than half mask (funMarkInside, :70-71) are dropped; their
+        nodes stay in coordinatesFEM;
+      * the dirichlet set markCoordHoleEdge (:74-104): nodes of refined elements and of
+        elements within 1.01 winstepsize of the mesh border, grown twice by element
+        adjacency;
+      * U0 carried to the new nodes by linear interpolation over the Delaunay triangulation of
+        the finite old nodes (scatteredInterpolant 'linear', :110-117; outside their hull the
+        nearest old node's value, where the reference extrapolates linearly).
+    Returns (DICmesh, DICpara, U0) with elementsFEM n_el x 8 and irregular (edge ends,
+    midpoint) rows."""
+    from scipy.interpolate import LinearNDInterpolator, NearestNDInterpolator
+
+    C0 = np.asarray(DICmesh["coordinatesFEM"], dtype=np.float64)
+    mask = np.asarray(fNormalizedMask)
+    minsize = float(np.ravel(DICmesh.get("elementMinSize", 0))[0])
+    step = float(np.ravel(DICpara["winstepsize"])[0])
+    xs, ys = np.unique(C0[:, 0]), np.unique(C0[:, 1])
+    M, N = xs.size, ys.size
+    if M * N != C0.shape[0] or M < 2 or N < 2:
+        raise AldicError("GenerateQuadtreeMesh: DICmesh must be the uniform mesh of MeshSetUp")
+    if not (np.allclose(np.diff(xs), xs[1] - xs[0]) and np.allclose(np.diff(ys), ys[1] - ys[0])):
+        raise AldicError("GenerateQuadtreeMesh: the uniform mesh must have one spacing")
+    hx, hy = xs[1] - xs[0], ys[1] - ys[0]
+    binary = np.isin(mask, (0, 1)).all()
+    box = _box_sums(mask != 0) if binary else None
+
+    def cell_box(L, i, j):
+        x0, y0 = xs[0] + i * hx / 2 ** L, ys[0] + j * hy / 2 ** L
+        x1, y1 = x0 + hx / 2 ** L, y0 + hy / 2 ** L
+        if not all(float(v).is_integer() for v in (x0, x1, y0, y1)):
+            raise AldicError("GenerateQuadtreeMesh: a refined element has non-integer corners "
+                             "(the reference indexes the mask with them); raise elementMinSize")
+        return int(x0), int(x1), int(y0), int(y1)
+
+    def mixed(L, i, j):
+        x0, x1, y0, y1 = cell_box(L, i, j)
+        if binary:
+            sm = box(x0, x1, y0, y1)
+            return 0 < sm < (x1 - x0 + 1) * (y1 - y0 + 1)
+        blk = mask[x0 - 1:x1, y0 - 1:y1]
+        return blk.max() - blk.min() > 0
+
+    order = [(0, i, j) for j in range(N - 1) for i in range(M - 1)]  # MeshSetUp's element order
+    leaves = set(order)
+
+    def leaf_at(L, i, j):
+        if i < 0 or j < 0 or i >= (M - 1) << L or j >= (N - 1) << L:
+            return None
+        for lv in range(L, -1, -1):
+            key = (lv, i >> (L - lv), j >> (L - lv))
+            if key in leaves:
+                return key
+        return None
+
+    while True:
+        marked = [c for c in order if min(hx, hy) / 2 ** c[0] > minsize and mixed(*c)]
+        if not marked:
+            break
+        split = set(marked)
+        queue = list(marked)
+        while queue:
+            L, i, j = queue.pop()
+            for di, dj in ((1, 0), (0, 1), (-1, 0), (0, -1)):
+                nb = leaf_at(L, i + di, j + dj)
+                if nb is not None and nb[0] < L and nb not in split:
+                    split.add(nb)
+                    queue.append(nb)
+        new_order = []
+        for c in order:
+            if c in split:
+                L, i, j = c
+                kids = [(L + 1, 2 * i, 2 * j), (L + 1, 2 * i + 1, 2 * j), (L + 1, 2 * i + 1, 2 * j + 1),
+                        (L + 1, 2 * i, 2 * j + 1)]
+                leaves.discard(c)
+                leaves.update(kids)
+                new_order.extend(kids)
+            else:
+                new_order.append(c)
+        order = new_order
+    # nodes: the uniform mesh's first, in its order; new corners in element order
+    node = {(float(x), float(y)): k + 1 for k, (x, y) in enumerate(C0)}
+    coords = [tuple(c) for c in C0]
+    corners = []
+    for L, i, j in order:
+        x0, x1, y0, y1 = cell_box(L, i, j)
+        ids = []
+        for pt in ((x0, y0), (x1, y0), (x1, y1), (x0, y1)):
+            pt = (float(pt[0]), float(pt[1]))
+            if pt not in node:
+                node[pt] = len(coords) + 1
+                coords.append(pt)
+            ids.append(node[pt])
+        corners.append(ids)
+    E = np.zeros((len(order), 8), dtype=np.int64)
+    irregular = []
+    for e, ((L, i, j), ids) in enumerate(zip(order, corners)):
+        x0, x1, y0, y1 = cell_box(L, i, j)
+        E[e, :4] = ids
+        mids = (((x1, (y0 + y1) / 2), (ids[1], ids[2])), (((x0 + x1) / 2, y1), (ids[2], ids[3])),
+                ((x0, (y0 + y1) / 2), (ids[3], ids[0])), (((x0 + x1) / 2, y0), (ids[0], ids[1])))
+        for slot, (pt, ends) in enumerate(mids):
+            k = node.get((float(pt[0]), float(pt[1])))
+            if k is not None:
+                E[e, 4 + slot] = k
+                irregular.append((ends[0], ends[1], k))
+    C = np.array(coords, dtype=np.float64)
+    # funMarkInside: drop the elements whose box is less than half mask
+    keep = []
+    for e, (L, i, j) in enumerate(order):
+        x0, x1, y0, y1 = cell_box(L, i, j)
+        sm = box(x0, x1, y0, y1) if binary else float(mask[x0 - 1:x1, y0 - 1:y1].sum())
+        keep.append(not sm < 0.5 * (x1 - x0) * (y1 - y0))
+    E = E[np.array(keep, dtype=bool)]
+    # the dirichlet set
+    size = np.hypot(C[E[:, 0] - 1, 0] - C[E[:, 2] - 1, 0], C[E[:, 0] - 1, 1] - C[E[:, 2] - 1, 1])
+    wsz = float(np.ravel(DICpara.get("winsize", 0))[0])
+    mark = size < 0.99 * np.sqrt(2) * max(step, 0 * wsz)
+    xMin, xMax, yMin, yMax = C0[:, 0].min(), C0[:, 0].max(), C0[:, 1].min(), C0[:, 1].max()
+    mark |= C[E[:, 0] - 1, 0] < xMin + 1.01 * step
+    mark |= C[E[:, 2] - 1, 0] > xMax - 1.01 * step
+    mark |= C[E[:, 0] - 1, 1] < yMin + 1.01 * step
+    mark |= C[E[:, 2] - 1, 1] > yMax - 1.01 * step
+
+    def nodes_of(rows):
+        u = np.unique(E[rows])
+        return u[1:] if u.size and u[0] == 0 else u
+
+    hole_edge = nodes_of(mark)
+    for _ in range(2):
+        rows = np.isin(E, hole_edge).any(1)
+        hole_edge = nodes_of(rows)
+    # U0 on the new nodes
+    U0 = np.asarray(U0, dtype=np.float64).ravel()
+    ok = np.flatnonzero(np.isfinite(U0[0::2]))
+    Unew = np.zeros(2 * C.shape[0])
+    if ok.size >= 3:
+        for comp in (0, 1):
+            vals = U0[2 * ok + comp]
+            lin = LinearNDInterpolator(C0[ok], vals)(C)
+            bad = ~np.isfinite(lin)
+            if bad.any():
+                lin[bad] = NearestNDInterpolator(C0[ok], vals)(C[bad])
+            Unew[comp::2] = lin
+    out = dict(DICmesh)
+    out.update(coordinatesFEM=C, elementsFEM=E, irregular=np.array(irregular, dtype=np.int64).reshape(-1, 3),
+               markCoordHoleEdge=hole_edge, dirichlet=hole_edge,
+               coordinatesFEMWorld=np.stack([C[:, 0], mask.shape[1] + 1 - C[:, 1]], 1))
+    return out, DICpara, Unew
 
 
 def _load_frame(ctx, Df, ImgRef, ImgDef, mask):

@@ -56,6 +56,12 @@ struct aldic_ctx {
   void* tscratch = nullptr;  // shared-product search scratch
   size_t tscratch_cap = 0;
   int warp_cap = kDefaultWarpCap;  // aldic_set_iteration_cap
+  // aldic_subpb2_set_mesh: the resident global-step mesh tables (element table, node ->
+  // element lists, node kinds) in one device buffer
+  char* sp2 = nullptr;
+  size_t sp2_cap = 0;
+  int64_t sp2_n = 0, sp2_nel = 0;
+  size_t sp2_nadj = 0;
   // profiling: event pairs around the correlation kernel of each integer search
   bool prof = false;
   std::vector<cudaEvent_t> prof_ev;  // 2 per record
@@ -251,7 +257,7 @@ void aldic_destroy(aldic_ctx* c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   void* bufs[] = {c->img[0], c->img[1], c->mask, c->gx, c->gy, c->stats, c->partials, c->counter, c->qcount,
-                  c->I1, c->I2, c->iitot, c->tscratch, c->arena.base};
+                  c->I1, c->I2, c->iitot, c->tscratch, c->arena.base, c->sp2};
   for (void* b : bufs)
     if (b) cudaFree(b);
   for (cudaEvent_t e : c->prof_ev) cudaEventDestroy(e);
@@ -756,26 +762,36 @@ int aldic_remove_outliers(aldic_ctx* c, int m, int n, double* u, double* v, doub
   return finish(c, l);
 }
 
-int aldic_subpb2(aldic_ctx* c, int64_t n, const double* coords, int64_t n_el, const int32_t* elements,
-                 int gauss_order, double beta, double mu, double alpha, const double* U, const double* F,
-                 int64_t n_dirichlet, const int32_t* dirichlet, double tol, int maxit, double* Uhat,
-                 int32_t* info) {
-  if (!c) return ALDIC_ERR_ARG;
-  if (info) info[0] = info[1] = 0;
-  if (n <= 0 || n_el <= 0) return fail(c, ALDIC_ERR_ARG, "empty mesh (%lld nodes, %lld elements)", (long long)n,
-                                       (long long)n_el);
+namespace {
+
+// Device layout of one mesh's tables: element table (8 n_el ints), node pointers (n + 1),
+// node -> element entries (nadj), node kinds (n bytes); each part 256-byte aligned.
+size_t sp2_bytes(int64_t n, int64_t n_el, size_t nadj) {
+  auto up = [](size_t b) { return (b + 255) & ~size_t(255); };
+  return up((size_t)n_el * 32) + up(((size_t)n + 1) * 4) + up(std::max<size_t>(nadj, 1) * 4) + up((size_t)n);
+}
+
+void sp2_parts(char* base, int64_t n, int64_t n_el, size_t nadj, int** E, int** ptr, int** adj,
+               unsigned char** kind) {
+  auto up = [](size_t b) { return (b + 255) & ~size_t(255); };
+  *E = (int*)base;
+  *ptr = (int*)(base + up((size_t)n_el * 32));
+  *adj = (int*)((char*)*ptr + up(((size_t)n + 1) * 4));
+  *kind = (unsigned char*)((char*)*adj + up(std::max<size_t>(nadj, 1) * 4));
+}
+
+// The mesh tables on the host from a caller's element table and dirichlet list (host or
+// device pointers).
+int sp2_tables(aldic_ctx* c, int64_t n, int64_t n_el, const int32_t* elements, int64_t n_dirichlet,
+               const int32_t* dirichlet, std::vector<int32_t>& E, std::vector<int>& ptr, std::vector<int>& adj,
+               std::vector<unsigned char>& kind) {
+  if (n <= 0 || n_el <= 0)
+    return fail(c, ALDIC_ERR_ARG, "empty mesh (%lld nodes, %lld elements)", (long long)n, (long long)n_el);
   if (n > (1LL << 28) || n_el > (1LL << 27)) return fail(c, ALDIC_ERR_ARG, "mesh too large");
-  if (gauss_order < 2 || gauss_order > 5) return fail(c, ALDIC_ERR_ARG, "Gauss point order %d (2..5)", gauss_order);
-  if (!(beta + alpha > 0.0) && !(mu > 0.0))
-    return fail(c, ALDIC_ERR_ARG, "beta + alpha and mu are both 0: the system is singular");
-  if (!coords || !elements || !U || !F || !Uhat || (n_dirichlet > 0 && !dirichlet))
-    return fail(c, ALDIC_ERR_ARG, "missing array argument");
+  if (!elements || (n_dirichlet > 0 && !dirichlet)) return fail(c, ALDIC_ERR_ARG, "missing mesh array");
   if (n_dirichlet < 0) return fail(c, ALDIC_ERR_ARG, "n_dirichlet < 0");
-  if (!(tol > 0.0)) tol = 1e-12;
-  if (maxit <= 0) maxit = (int)std::min<int64_t>(20 * n + 1000, 200000);
-  CK(cudaSetDevice(c->device));
-  // the mesh on the host: element table checks, node -> (element, slot) lists, node kinds
-  std::vector<int32_t> E((size_t)n_el * 8), dir((size_t)n_dirichlet);
+  E.resize((size_t)n_el * 8);
+  std::vector<int32_t> dir((size_t)std::max<int64_t>(n_dirichlet, 1));
   if (is_device_ptr(elements)) {
     CK(cudaMemcpy(E.data(), elements, E.size() * 4, cudaMemcpyDeviceToHost));
   } else {
@@ -783,17 +799,78 @@ int aldic_subpb2(aldic_ctx* c, int64_t n, const double* coords, int64_t n_el, co
   }
   if (n_dirichlet > 0) {
     if (is_device_ptr(dirichlet)) {
-      CK(cudaMemcpy(dir.data(), dirichlet, dir.size() * 4, cudaMemcpyDeviceToHost));
+      CK(cudaMemcpy(dir.data(), dirichlet, (size_t)n_dirichlet * 4, cudaMemcpyDeviceToHost));
     } else {
-      std::memcpy(dir.data(), dirichlet, dir.size() * 4);
+      std::memcpy(dir.data(), dirichlet, (size_t)n_dirichlet * 4);
     }
   }
-  std::vector<int> ptr, adj;
-  std::vector<unsigned char> kind;
   char msg[160];
   if (subpb2_mesh_tables(n, n_el, E.data(), n_dirichlet, dir.data(), ptr, adj, kind, msg, sizeof(msg)))
     return fail(c, ALDIC_ERR_ARG, "%s", msg);
-  // device buffers: inputs staged, the mesh tables, K_e / b_e, the CG vectors
+  return ALDIC_OK;
+}
+
+}  // namespace
+
+int aldic_subpb2_set_mesh(aldic_ctx* c, int64_t n, int64_t n_el, const int32_t* elements, int64_t n_dirichlet,
+                          const int32_t* dirichlet) {
+  if (!c) return ALDIC_ERR_ARG;
+  CK(cudaSetDevice(c->device));
+  std::vector<int32_t> E;
+  std::vector<int> ptr, adj;
+  std::vector<unsigned char> kind;
+  int rc = sp2_tables(c, n, n_el, elements, n_dirichlet, dirichlet, E, ptr, adj, kind);
+  if (rc) return rc;
+  const size_t bytes = sp2_bytes(n, n_el, adj.size());
+  CK(cudaStreamSynchronize(c->stream));  // the previous tables may still be in use
+  if (c->sp2_cap < bytes) {
+    if (c->sp2) CK(cudaFree(c->sp2));
+    c->sp2 = nullptr;
+    c->sp2_cap = 0;
+    CK(cudaMalloc(&c->sp2, bytes));
+    c->sp2_cap = bytes;
+  }
+  int *dE, *dptr, *dadj;
+  unsigned char* dkind;
+  sp2_parts(c->sp2, n, n_el, adj.size(), &dE, &dptr, &dadj, &dkind);
+  CK(cudaMemcpyAsync(dE, E.data(), E.size() * 4, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(dptr, ptr.data(), ptr.size() * 4, cudaMemcpyHostToDevice, c->stream));
+  if (!adj.empty()) CK(cudaMemcpyAsync(dadj, adj.data(), adj.size() * 4, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(dkind, kind.data(), kind.size(), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->sp2_n = n;
+  c->sp2_nel = n_el;
+  c->sp2_nadj = adj.size();
+  return ALDIC_OK;
+}
+
+int aldic_subpb2(aldic_ctx* c, int64_t n, const double* coords, int64_t n_el, const int32_t* elements,
+                 int gauss_order, double beta, double mu, double alpha, const double* U, const double* F,
+                 int64_t n_dirichlet, const int32_t* dirichlet, double tol, int maxit, double* Uhat,
+                 int32_t* info) {
+  if (!c) return ALDIC_ERR_ARG;
+  if (info) info[0] = info[1] = 0;
+  if (gauss_order < 2 || gauss_order > 5) return fail(c, ALDIC_ERR_ARG, "Gauss point order %d (2..5)", gauss_order);
+  if (!(beta + alpha > 0.0) && !(mu > 0.0))
+    return fail(c, ALDIC_ERR_ARG, "beta + alpha and mu are both 0: the system is singular");
+  if (!coords || !U || !F || !Uhat) return fail(c, ALDIC_ERR_ARG, "missing array argument");
+  if (!(tol > 0.0)) tol = 1e-12;
+  if (maxit <= 0) maxit = (int)std::min<int64_t>(20 * n + 1000, 200000);
+  CK(cudaSetDevice(c->device));
+  const bool resident = elements == nullptr;
+  std::vector<int32_t> E;
+  std::vector<int> ptr, adj;
+  std::vector<unsigned char> kind;
+  if (resident) {  // the tables of aldic_subpb2_set_mesh
+    if (!c->sp2 || c->sp2_n != n || c->sp2_nel != n_el)
+      return fail(c, ALDIC_ERR_ARG, "no resident mesh of %lld nodes / %lld elements (aldic_subpb2_set_mesh)",
+                  (long long)n, (long long)n_el);
+    if (n_dirichlet != 0) return fail(c, ALDIC_ERR_ARG, "the resident mesh carries its dirichlet nodes");
+  } else {
+    int rc = sp2_tables(c, n, n_el, elements, n_dirichlet, dirichlet, E, ptr, adj, kind);
+    if (rc) return rc;
+  }
+  // device buffers: inputs staged, the mesh tables (unless resident), K_e / b_e, the CG vectors
   const size_t nb = (size_t)subpb2_blocks(n);
   Arg ac{coords, (size_t)n * 16, false, nullptr}, au{U, (size_t)n * 16, false, nullptr},
       af{F, (size_t)n * 32, false, nullptr}, ao{Uhat, (size_t)n * 16, true, nullptr};
@@ -803,8 +880,9 @@ int aldic_subpb2(aldic_ctx* c, int64_t n, const double* coords, int64_t n_el, co
   for (Arg* a : {&ac, &au, &af, &ao})
     if (!is_device_ptr(a->user)) need += ((a->bytes + 255) & ~size_t(255)) + 256;
   const size_t two_n = (size_t)n * 16;
-  need += E.size() * 4 + ptr.size() * 4 + adj.size() * 4 + kind.size() + (size_t)n_el * (64 + 16) * 8 +
-          6 * two_n + (size_t)n * 8 + nb * 16 + subpb2_scalars_bytes() + 64 + 16 * 256;
+  if (!resident) need += sp2_bytes(n, n_el, adj.size()) + 256;
+  need += (size_t)n_el * (64 + 16) * 8 + 6 * two_n + (size_t)n * 8 + nb * 16 + subpb2_scalars_bytes() + 64 +
+          16 * 256;
   int rc = arena_reserve(c, need);
   if (rc) return rc;
   for (Arg* a : {&ac, &au, &af, &ao}) {
@@ -818,10 +896,19 @@ int aldic_subpb2(aldic_ctx* c, int64_t n, const double* coords, int64_t n_el, co
         CK(cudaMemcpyAsync(a->dev, a->user, a->bytes, cudaMemcpyHostToDevice, c->stream));
     }
   }
-  int* dE = (int*)arena_take(c, E.size() * 4);
-  int* dptr = (int*)arena_take(c, ptr.size() * 4);
-  int* dadj = (int*)arena_take(c, std::max<size_t>(adj.size(), 1) * 4);
-  unsigned char* dkind = (unsigned char*)arena_take(c, kind.size());
+  int *dE, *dptr, *dadj;
+  unsigned char* dkind;
+  if (resident) {
+    sp2_parts(c->sp2, n, n_el, c->sp2_nadj, &dE, &dptr, &dadj, &dkind);
+  } else {
+    char* tb = (char*)arena_take(c, sp2_bytes(n, n_el, adj.size()));
+    sp2_parts(tb, n, n_el, adj.size(), &dE, &dptr, &dadj, &dkind);
+    // copied from pageable host vectors: each copy has completed when the call returns
+    CK(cudaMemcpyAsync(dE, E.data(), E.size() * 4, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(dptr, ptr.data(), ptr.size() * 4, cudaMemcpyHostToDevice, c->stream));
+    if (!adj.empty()) CK(cudaMemcpyAsync(dadj, adj.data(), adj.size() * 4, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(dkind, kind.data(), kind.size(), cudaMemcpyHostToDevice, c->stream));
+  }
   double* Ke = (double*)arena_take(c, (size_t)n_el * 64 * 8);
   double* be = (double*)arena_take(c, (size_t)n_el * 16 * 8);
   double* b = (double*)arena_take(c, two_n);
@@ -832,11 +919,6 @@ int aldic_subpb2(aldic_ctx* c, int64_t n, const double* coords, int64_t n_el, co
   double* D = (double*)arena_take(c, (size_t)n * 8);
   double* part = (double*)arena_take(c, nb * 16);
   Subpb2Scalars* sc = (Subpb2Scalars*)arena_take(c, subpb2_scalars_bytes() + 64);
-  // the tables are copied from pageable host vectors: the copies complete before return
-  CK(cudaMemcpyAsync(dE, E.data(), E.size() * 4, cudaMemcpyHostToDevice, c->stream));
-  CK(cudaMemcpyAsync(dptr, ptr.data(), ptr.size() * 4, cudaMemcpyHostToDevice, c->stream));
-  if (!adj.empty()) CK(cudaMemcpyAsync(dadj, adj.data(), adj.size() * 4, cudaMemcpyHostToDevice, c->stream));
-  CK(cudaMemcpyAsync(dkind, kind.data(), kind.size(), cudaMemcpyHostToDevice, c->stream));
   double* x = (double*)ao.dev;  // the solution builds in the output
   int l = launch_subpb2_setup((int)n_el, dE, (const double*)ac.dev, n, (const double*)au.dev, (const double*)af.dev,
                               gauss_order, beta, mu, alpha, dptr, dadj, dkind, Ke, be, b, D, x, r, z, p, part, sc,

@@ -143,11 +143,20 @@ int aldic_epipolar_icgn(aldic_ctx* ctx, int64_t n, const double* pts, int winsiz
  * dirichlet nodes (1-based) hold U, all other nodes get 0.  Solved by Jacobi-preconditioned
  * conjugate gradients in FP64 to |r| <= tol |r0| (tol <= 0: 1e-12) within maxit iterations
  * (<= 0: min(20 n + 1000, 200000)); the reference solves the free block directly.
- * Uhat: 2n.  info (optional, host, 2 ints): iterations, 1 when the tolerance was met. */
+ * Uhat: 2n.  info (optional, host, 2 ints): iterations, 1 when the tolerance was met.
+ * elements = NULL solves on the mesh of the last aldic_subpb2_set_mesh (same n and n_el;
+ * n_dirichlet 0: the resident mesh carries its dirichlet nodes). */
 int aldic_subpb2(aldic_ctx* ctx, int64_t n, const double* coords, int64_t n_el, const int32_t* elements,
                  int gauss_order, double beta, double mu, double alpha, const double* U, const double* F,
                  int64_t n_dirichlet, const int32_t* dirichlet, double tol, int maxit, double* Uhat,
                  int32_t* info);
+
+/* Keeps a global-step mesh resident in the context (no reference counterpart: the drivers
+ * call Subpb2Quadtree four to six times per frame on one mesh): the element table's checks,
+ * the node -> element lists and the free / dirichlet kinds are built once, on the host, and
+ * held on the device until the next call or aldic_destroy. */
+int aldic_subpb2_set_mesh(aldic_ctx* ctx, int64_t n, int64_t n_el, const int32_t* elements, int64_t n_dirichlet,
+                          const int32_t* dirichlet);
 
 /* ------------------------------------------------------ initial guess --------- */
 /* inpaint_nans(A, 4) (func/inpaint_nans.m:369-398, spring analogy), in place on an m x n

@@ -179,3 +179,69 @@ def test_patch_test_through_the_library_steps(harness, tmp_path):
     U, F = _linear_case(C)
     _, _, x, _, ok, _ = _run(harness, tmp_path, C, E, 2, 0.256, 1e-3, 0.0, U, F)
     assert ok == 1 and np.abs(x - U).max() < 1e-9
+
+
+def _plate_mesh(min_size=4):
+    import aldic_b200 as A
+    from aldic_b200 import synth
+
+    sc = synth.plate_with_hole(size=384, hole_r=60.0, peak=2.0, sin_amp=0.3, sin_wl=120.0)
+    w, st = 32, 16
+    xl = np.arange(1 + w // 2, 384 - w // 2 + 1, st, dtype=float)
+    X, Y = np.meshgrid(xl, xl)
+    mesh = A.MeshSetUp(X, Y, {"winstepsize": st, "ImgSize": [384, 384]})
+    mesh["elementMinSize"] = min_size
+    C0 = mesh["coordinatesFEM"]
+    U0 = np.stack([0.5 + 0.01 * C0[:, 0] - 0.002 * C0[:, 1], -1.0 + 0.003 * C0[:, 1]], 1).ravel()
+    m2, _, U = A.GenerateQuadtreeMesh(U0, None, sc.mask, mesh, {"winstepsize": st, "winsize": w})
+    return sc.mask, mesh, m2, U
+
+
+def test_quadtree_mesh_structure():
+    mask, mesh0, m, U = _plate_mesh()
+    C, E = m["coordinatesFEM"], m["elementsFEM"]
+    n0 = mesh0["coordinatesFEM"].shape[0]
+    assert np.array_equal(C[:n0], mesh0["coordinatesFEM"])  # old nodes keep their numbers
+    x1, y1 = C[E[:, 0] - 1].T
+    x2, y2 = C[E[:, 1] - 1].T
+    x3, y3 = C[E[:, 2] - 1].T
+    x4, y4 = C[E[:, 3] - 1].T
+    s = x2 - x1
+    # squares, corners (xmin, ymin), (xmax, ymin), (xmax, ymax), (xmin, ymax)
+    assert (s > 0).all() and np.array_equal(y2, y1) and np.array_equal(x3, x2) and np.array_equal(y3 - y2, s)
+    assert np.array_equal(x4, x1) and np.array_equal(y4, y3)
+    assert set(np.unique(s)) == {4.0, 8.0, 16.0}
+    # hanging nodes sit at the midpoints of their edges; no other node lies inside any edge
+    mids = {4: ((x2 + x3) / 2, (y2 + y3) / 2), 5: ((x3 + x4) / 2, (y3 + y4) / 2), 6: ((x4 + x1) / 2, (y4 + y1) / 2),
+            7: ((x1 + x2) / 2, (y1 + y2) / 2)}
+    for slot, (mx, my) in mids.items():
+        h = E[:, slot] > 0
+        assert np.array_equal(C[E[h, slot] - 1, 0], mx[h]) and np.array_equal(C[E[h, slot] - 1, 1], my[h])
+    pts = {tuple(p) for p in C}
+    for e in range(E.shape[0]):
+        q = s[e] / 4  # a 2-irregular edge would have nodes at the quarter points
+        for (ax, ay), (bx, by) in (((x1[e], y1[e]), (x2[e], y2[e])), ((x2[e], y2[e]), (x3[e], y3[e])),
+                                   ((x3[e], y3[e]), (x4[e], y4[e])), ((x4[e], y4[e]), (x1[e], y1[e]))):
+            for t in (0.25, 0.75):
+                assert (ax + t * (bx - ax), ay + t * (by - ay)) not in pts, (e, q)
+    # refinement finished: no kept element larger than the minimum still meets both mask values
+    for e in range(E.shape[0]):
+        blk = mask[int(x1[e]) - 1:int(x2[e]), int(y1[e]) - 1:int(y4[e])]
+        assert not (s[e] > 4 and blk.max() > blk.min())
+        assert blk.sum() >= 0.5 * s[e] * s[e]  # funMarkInside kept it
+    # the dirichlet set holds the nodes of every refined element
+    fine = E[s < 16][:, :4].ravel()
+    assert np.isin(fine, m["dirichlet"]).all()
+    # U0 (linear in x, y) carried exactly to the new nodes
+    want = np.stack([0.5 + 0.01 * C[:, 0] - 0.002 * C[:, 1], -1.0 + 0.003 * C[:, 1]], 1).ravel()
+    assert np.abs(U - want).max() < 1e-12
+
+
+def test_generated_mesh_passes_the_global_step_patch_test():
+    _, _, m, _ = _plate_mesh()
+    C, E = m["coordinatesFEM"], m["elementsFEM"]
+    U, F = _linear_case(C)
+    Uh = O.subpb2_quadtree(C, E, 2, 0.0256, 1e-3, U, F, dirichlet=m["dirichlet"])
+    used = np.unique(E[E > 0]) - 1
+    d = np.abs(Uh - U).reshape(-1, 2)[used]
+    assert d.max() < 1e-10
