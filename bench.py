@@ -47,7 +47,7 @@ UNIT = "subsets/s"
 # ----------------------------------------------------------------------------------
 def workload_params(name):
     if name == "quadtree2048":
-        return dict(size=2048, w=32, step=16, s_temp=10, tol_temp=1e-3, mu=1e-3, admm=3)
+        return dict(size=2048, w=32, step=16, s_temp=10, tol_temp=1e-3, mu=1e-3, admm=2, min_elem=4)
     if name == "stereo2048":
         return dict(size=2048, w=40, step=10, s_stereo=70, s_temp=10, tol_stereo=1e-3, tol_temp=1e-2)
     if name == "stereo1024":  # same geometry at half the resolution (profiling case)
@@ -629,32 +629,12 @@ def main():
 # ----------------------------------------------------------------------------------
 # the 2D temporal (512^2) and quadtree ALDIC (2048^2, hole + notch, Subpb1) workloads
 # ----------------------------------------------------------------------------------
-def quadtree_nodes(M, N, mask, margin):
-    """A quadtree-like node set: spacing 8 px within 640 px of the mask edge (hole and notch),
-    16 px within 960 px, 32 px elsewhere (mesh generation is host work in the reference; this stands in
-    for GenerateQuadtreeMesh).  Returns coords (n x 2, 1-based) and the local spacing."""
-    from scipy import ndimage
-
-    edge_dist = np.where(mask > 0, ndimage.distance_transform_edt(mask > 0), ndimage.distance_transform_edt(mask == 0))
-    pts, sp = [], []
-    for s, lo, hi in ((8, 0, 640), (16, 640, 960), (32, 960, 1e9)):
-        xs = np.arange(margin, M - margin + 1, s, dtype=np.float64)
-        ys = np.arange(margin, N - margin + 1, s, dtype=np.float64)
-        X, Y = np.meshgrid(xs, ys, indexing="ij")
-        d = edge_dist[X.astype(int) - 1, Y.astype(int) - 1]
-        inside = mask[X.astype(int) - 1, Y.astype(int) - 1] > 0
-        keep = (d >= lo) & (d < hi) & (inside | (d < 8))
-        pts.append(np.stack([X[keep], Y[keep]], 1))
-        sp.append(np.full(int(keep.sum()), s))
-    coords = np.concatenate(pts)
-    coords, idx = np.unique(coords, axis=0, return_index=True)
-    return coords, np.concatenate(sp)[idx]
-
-
 def run_aux(args, P):
     """temporal512: LocalICGN on a 512^2 affine pair, FFT-search init.
-    quadtree2048 (config 2): masked quadtree LocalICGNQuadtree + 3 Subpb1Quadtree steps on a
-    2048^2 plate with a hole and an edge notch.  Device-resident; verified on the oracle."""
+    quadtree2048 (config 2): one ALDIC frame on a 2048^2 plate with a hole and an edge notch:
+    search, bad-point removal, Init, LocalICGNQuadtree on the quadtree mesh of
+    GenerateQuadtreeMesh, the global step with the first frame's beta tuning, and two ADMM
+    rounds of Subpb1Quadtree + Subpb2Quadtree.  Device-resident; verified on the oracle."""
     import torch
 
     import aldic_b200 as A
@@ -676,10 +656,29 @@ def run_aux(args, P):
     gx, gy = [1, M], [1, N]
     # search grid (XList rule) and the solve mesh
     gcoords, nx, ny = grid_coords(M, N, w, st)
+    g = nx * ny
     if quad:
-        coords_np, spacing = quadtree_nodes(M, N, mask, margin=w // 2 + P["s_temp"] + 8)
-        wl_np = np.clip(2 * spacing, 16, 64).astype(np.int32)
+        # MeshSetUp on the search grid, refined at the mask's edges by GenerateQuadtreeMesh
+        # (elements down to min_elem px): host set-up, as the reference builds its mesh once
+        mesh0 = A.MeshSetUp(gcoords[:, 0].reshape(ny, nx), gcoords[:, 1].reshape(ny, nx),
+                            {"winstepsize": st, "ImgSize": [M, N]})
+        mesh0["elementMinSize"] = P["min_elem"]
+        qmesh, _, _ = A.GenerateQuadtreeMesh(np.zeros(2 * g), None, mask, mesh0, {"winstepsize": st, "winsize": w})
+        coords_np, E_np, dir_np = qmesh["coordinatesFEM"], qmesh["elementsFEM"], qmesh["dirichlet"]
+        # the ADMM loop's uniform winsize_List
+        wl_np = np.full(coords_np.shape[0], w, dtype=np.int32)
         wl = T.from_numpy(np.concatenate([wl_np, wl_np])).to(dev)  # n x 2 column-major (wx, wy)
+        # U0 carried from the grid to the mesh nodes by bilinear weights (GenerateQuadtreeMesh
+        # carries it by linear interpolation; the two agree on the grid's edges)
+        fx = (coords_np[:, 0] - gcoords[0, 0]) / st
+        fy = (coords_np[:, 1] - gcoords[0, 1]) / st
+        i0 = np.clip(np.floor(fx), 0, nx - 2).astype(np.int64)
+        j0 = np.clip(np.floor(fy), 0, ny - 2).astype(np.int64)
+        tx, ty = fx - i0, fy - j0
+        k00 = i0 + j0 * nx
+        tr_idx = T.from_numpy(np.stack([k00, k00 + 1, k00 + nx, k00 + nx + 1])).to(dev)
+        tr_w = T.from_numpy(np.stack([(1 - tx) * (1 - ty), tx * (1 - ty), (1 - tx) * ty, tx * ty])).to(dev)
+        betas = [c * float(st) ** 2 * P["mu"] for c in (1e-3, 1e-2, 1e-1)]
     else:
         coords_np = gcoords
     n = coords_np.shape[0]
@@ -690,15 +689,62 @@ def run_aux(args, P):
     ctx = A.Context(0)
     stream = T.cuda.Stream(dev)
     ctx.set_stream(stream.cuda_stream)
-    g = nx * ny
+    if quad:
+        ctx.subpb2_set_mesh(n, E_np, dir_np)
     b = {"x": T.empty(g, **f64), "y": T.empty(g, **f64), "u": T.empty(g, **f64), "v": T.empty(g, **f64),
          "phi": T.empty(g, **f64), "U0": T.empty(2 * n, **f64), "U": T.empty(2 * n, **f64),
          "F": T.empty(4 * n, **f64), "H": T.empty(21 * n, **f64), "conv": T.empty(n, dtype=T.int32, device=dev),
          "mark": T.empty(n, dtype=T.uint8, device=dev), "Ug": T.empty(2 * g, **f64)}
     sub = [{"U": T.empty(2 * n, **f64), "conv": T.empty(n, dtype=T.int32, device=dev)} for _ in range(P.get("admm", 0))]
-    vdual = T.zeros(2 * n, **f64)
     cxy = coords.t()
     shp = (M, N)
+    glob = {"U2": [T.empty(2 * n, **f64) for _ in range(3)], "out": T.empty(2 * n, **f64), "beta": None,
+            "sub_in": None, "last": None}
+
+    def select_beta(errs):
+        """The reference's beta for the first frame (func/TemporalMatch_quadtree_ST1.m:274-294):
+        normalised |U1 - U2| over the beta list, a parabola in log10(beta) through the
+        minimum and its neighbours, the list's beta when the minimum is at an end."""
+        e = np.asarray(errs, dtype=np.float64)
+        z = (e - e.mean()) / e.std(ddof=1)
+        if not np.isfinite(z).all():
+            return betas[0]
+        k = int(np.argmin(z))
+        if k != 1:
+            return betas[k]
+        p = np.polyfit(np.log10(betas), z, 2)
+        return 10 ** (-p[1] / 2 / p[0])
+
+    def aldic_frame():
+        """ALDIC after the local step (func/TemporalMatch_quadtree_ST1.m:248-380): the global
+        step with the first frame's beta tuning, then admm x (Subpb1, Subpb2, dual update),
+        hole-edge nodes (markCoordHoleStrain) keeping the local result.  Bad local results
+        take the initial guess (U) or 0 (F) where the reference fills them by
+        natural-neighbour interpolation."""
+        U1 = T.where(T.isnan(b["U"]), b["U0"], b["U"])
+        F1 = T.nan_to_num(b["F"], nan=0.0)
+        hole = b["mark"].bool().repeat_interleave(2)
+        errs = []
+        for k, bt in enumerate(betas):
+            ctx.subpb2(coords, None, 2, bt, P["mu"], U1, F1, out=glob["U2"][k])
+            errs.append(T.linalg.vector_norm(U1 - glob["U2"][k]))
+        beta = select_beta(T.stack(errs).cpu().numpy())
+        U2 = glob["U2"][2]
+        if abs(beta - betas[2]) > np.finfo(float).eps:
+            ctx.subpb2(coords, None, 2, beta, P["mu"], U1, F1, out=glob["out"])
+            U2 = glob["out"]
+        glob["beta"] = beta
+        U2 = T.where(hole, U1, U2)
+        vdual = U2 - U1
+        for k in range(P["admm"]):
+            if k == 0:
+                glob["sub_in"] = (U2, vdual)
+            ctx.subpb1(1, coords, U2, F1, vdual, P["mu"], P["tol_temp"], winsize=w, winsize_list=wl, out=sub[k])
+            U1 = T.where(T.isnan(sub[k]["U"]), U2, sub[k]["U"])
+            ctx.subpb2(coords, None, 2, beta, P["mu"], U1, F1, out=glob["out"])
+            glob["last"] = (U1, F1, glob["out"].clone())
+            U2 = T.where(hole, U1, glob["out"])
+            vdual = U2 - U1
 
     def step():
         with T.cuda.stream(stream):
@@ -708,19 +754,16 @@ def run_aux(args, P):
                 ctx.set_mask(mask_d)
             ctx.compute_gradients()
             ctx.integer_search([P["s_temp"]] * 2, gx, gy, w, st, out=b)
-            # bad-point removal and Init over the search grid, then every mesh node takes its
-            # nearest grid node
+            # bad-point removal and Init over the search grid, then U0 on the mesh nodes
             ctx.remove_outliers(b["u"].view(nx, ny), b["v"].view(nx, ny), 100.0)
             ctx.init_u0(b["u"].view(nx, ny), b["v"].view(nx, ny), out=b["Ug"])
-            i = T.clamp(T.round((cxy[:, 0] - (1 + w / 2.0)) / st), 0, nx - 1).long()
-            j = T.clamp(T.round((cxy[:, 1] - (1 + w / 2.0)) / st), 0, ny - 1).long()
-            b["U0"].view(n, 2).copy_(b["Ug"].view(-1, 2)[i + j * nx])
+            if quad:
+                b["U0"].view(n, 2).copy_((b["Ug"].view(-1, 2)[tr_idx] * tr_w[..., None]).sum(0))
+            else:
+                b["U0"].copy_(b["Ug"])
             ctx.local_icgn(1 if quad else 0, coords, b["U0"], w, P["tol_temp"], out=b)
-            Uold = b["U"]
-            for k in range(P.get("admm", 0)):
-                ctx.subpb1(1, coords, T.nan_to_num(Uold, nan=0.0), T.nan_to_num(b["F"], nan=0.0), vdual, P["mu"],
-                           P["tol_temp"], winsize=w, winsize_list=wl, out=sub[k])
-                Uold = sub[k]["U"]
+            if quad:
+                aldic_frame()
 
     for _ in range(max(args.warmup, 3)):
         step()
@@ -737,6 +780,7 @@ def run_aux(args, P):
     ms_step = ev0.elapsed_time(ev1) / args.steps
     launches = ctx.launches - l0
     solves = n * (1 + P.get("admm", 0))
+    n_global = (3 + (abs(glob["beta"] - betas[2]) > np.finfo(float).eps) + P["admm"]) if quad else 0
     ver = None
     counted = None
     if not args.no_verify:
@@ -766,10 +810,12 @@ def run_aux(args, P):
                "icgn_counted_fraction": float(ok.mean()), "oracle_icgn_s": t_icgn}
         counted = ok.mean() * n
         if quad:
-            # first ADMM step from the device's own IC-GN results
-            Uin = np.nan_to_num(b["U"].view(n, 2).cpu().numpy()[pick]).ravel()
+            # the first ADMM round's Subpb1 from the device's own inputs
+            U2_in, vd_in = glob["sub_in"]
+            Uin = U2_in.view(n, 2).cpu().numpy()[pick].ravel()
+            vin = vd_in.view(n, 2).cpu().numpy()[pick].ravel()
             Fin = np.nan_to_num(b["F"].view(n, 4).cpu().numpy()[pick]).ravel()
-            s1 = O.subpb1(frame, coords_np[pick], Uin, Fin, np.zeros(2 * len(pick)), P["mu"], P["tol_temp"],
+            s1 = O.subpb1(frame, coords_np[pick], Uin, Fin, vin, P["mu"], P["tol_temp"],
                           winsize=w, winsize_list=np.stack([wl_np[pick], wl_np[pick]], 1), nthreads=host_threads())
             Us = sub[0]["U"].view(n, 2).cpu().numpy()[pick]
             cs = sub[0]["conv"].cpu().numpy()[pick]
@@ -778,6 +824,14 @@ def run_aux(args, P):
             ds = np.abs(Us - s1["U"].reshape(-1, 2))
             ver.update({"subpb1_flag_match": float(np.mean(fgs == fos)),
                         "subpb1_uv_max_err": float(ds[fgs & fos].max()) if (fgs & fos).any() else None})
+            # the last global step, whole mesh, from the device's own inputs
+            U1l, F1l, outl = (t.cpu().numpy() for t in glob["last"])
+            t0 = time.perf_counter()
+            ref2 = O.subpb2_quadtree(coords_np, E_np, 2, glob["beta"], P["mu"], U1l, F1l, dirichlet=dir_np)
+            t_sp2 = time.perf_counter() - t0
+            ver.update({"subpb2_max_err": float(np.abs(outl - ref2).max()),
+                        "subpb2_field_max": float(np.abs(ref2).max()), "oracle_subpb2_s": t_sp2,
+                        "beta": glob["beta"], "global_solves_per_step": int(n_global)})
     cpu = None
     if not args.no_cpu:
         import oracle as O
@@ -792,6 +846,7 @@ def run_aux(args, P):
         Fh = np.nan_to_num(b["F"].view(n, 4).cpu().numpy())
         rng = np.random.default_rng(args.seed + 7)
         cpu = {"kind": "port", "unit": "subsets/s" if not quad else "subset solves/s"}
+        t_sp2_cpu = None
         for threads in (host_threads(), 1):
             ns = min(n, 900 if threads > 1 else 150)
             pk = np.sort(rng.choice(n, ns, replace=False))
@@ -804,26 +859,37 @@ def run_aux(args, P):
             O.local_icgn(frame, coords_np[pk], U0h[pk].ravel(), w, P["tol_temp"], variant=1 if quad else 0,
                          nthreads=threads)
             t_solve = time.perf_counter() - t0
+            t_global = 0.0
             if quad:
                 for _ in range(P["admm"]):
                     O.subpb1(frame, coords_np[pk], Uh[pk].ravel(), Fh[pk].ravel(), np.zeros(2 * ns), P["mu"],
                              P["tol_temp"], winsize=w, winsize_list=np.stack([wl_np[pk], wl_np[pk]], 1),
                              nthreads=threads)
                 t_solve = time.perf_counter() - t0
-            t_step = t_search + t_solve * n / ns
+                if t_sp2_cpu is None:  # one global step on the whole mesh (single-threaded either way)
+                    t1 = time.perf_counter()
+                    O.subpb2_quadtree(coords_np, E_np, 2, betas[1], P["mu"], Uh.ravel(), Fh.ravel(), dirichlet=dir_np)
+                    t_sp2_cpu = time.perf_counter() - t1
+                t_global = t_sp2_cpu * n_global
+            t_step = t_search + t_solve * n / ns + t_global
             per = (solves if quad else (counted if counted is not None else n)) / t_step
             key = "value" if threads > 1 else "value_1core"
             cpu[key] = per
             if threads > 1:
                 cpu["cores"] = threads
         cpu["sample"] = ("whole-field search timed on a sample of grid subsets and scaled to the grid; "
-                         "solves timed on 900 (150 on one core) mesh nodes and scaled to the mesh")
-    line = {"metric": METRIC if not quad else "subset solves/s (1 LocalICGNQuadtree + 3 Subpb1Quadtree per node)",
+                         "solves timed on 900 (150 on one core) mesh nodes and scaled to the mesh"
+                         + ("; one global step on the whole mesh (element loop + sparse direct solve), times "
+                            "the frame's global solves" if quad else ""))
+    line = {"metric": METRIC if not quad else ("subset solves/s (1 LocalICGNQuadtree + 2 Subpb1Quadtree per node, "
+                                               "with the frame's Subpb2Quadtree global solves)"),
             "value": (counted if (counted is not None and not quad) else solves) / (ms_step * 1e-3),
             "unit": UNIT if not quad else "subset solves/s", "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 (FP64 solve)", "data": "synthetic (seeded analytic speckle rendering)",
-            "config": {"workload": args.workload, "subsets": int(n), "image": [int(M), int(N)], **P},
+            "config": {"workload": args.workload, "subsets": int(n), "image": [int(M), int(N)], **P,
+                       **({"elements": int(E_np.shape[0]), "hanging_nodes": int((E_np[:, 4:] > 0).sum()),
+                           "dirichlet_nodes": int(np.size(dir_np)), "global_solves": int(n_global)} if quad else {})},
             "gpu_launches": int(launches), "clocks": clk, "verification": ver, "cpu_baseline": cpu}
     print(json.dumps(line), flush=True)
     ctx.close()

@@ -673,6 +673,11 @@ def test_subpb2_device_tensors_and_errors(A, ctx):
     ctx.subpb2(tC, tE, 2, 0.0256, 1e-3, tU, tF, out=out)
     torch.cuda.synchronize()
     assert np.array_equal(out.cpu().numpy(), host)
+    # the resident mesh gives the same; a node count that does not match it is an error
+    ctx.subpb2_set_mesh(n, E)
+    assert np.array_equal(ctx.subpb2(C, None, 2, 0.0256, 1e-3, U, F), host)
+    with pytest.raises(A.AldicError):
+        ctx.subpb2(C[:-1], None, 2, 0.0256, 1e-3, U[:-2], F[:-4])
     bad = E.copy()
     bad[0, 0] = 0
     with pytest.raises(A.AldicError):
