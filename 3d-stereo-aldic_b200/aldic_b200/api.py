@@ -17,6 +17,7 @@ import time
 
 import numpy as np
 
+from . import fill as _fill
 from . import _lib
 from ._lib import AldicError
 
@@ -793,6 +794,11 @@ def GenerateQuadtreeMesh(U0, Df, fNormalizedMask, DICmesh, DICpara):
     return out, DICpara, Unew
 
 
+def _fill_mask(Df, ImgRef):
+    m = Df.get("ImgRefMask") if isinstance(Df, dict) else None
+    return np.ones(np.shape(ImgRef)) if m is None else np.asarray(m)
+
+
 def _load_frame(ctx, Df, ImgRef, ImgDef, mask):
     ctx.load_image(_lib.SLOT_REF, np.asarray(ImgRef, dtype=np.float64))
     ctx.load_image(_lib.SLOT_DEF, np.asarray(ImgDef, dtype=np.float64))
@@ -840,11 +846,12 @@ def bad_points_subpb1(conv):
 
 
 def LocalICGN(U0, coordinatesFEM, Df, ImgRef, ImgDef, DICpara, ICGNmethod="GaussNewton", tol=1e-3,
-              shapeFunctionOrder=1, ctx: Context | None = None):
+              shapeFunctionOrder=1, ctx: Context | None = None, fill=True):
     """[U, F, HtempPar, LocalTime, ConvItPerEle, LocalICGNBadPtNum] = LocalICGN(...)
     (func/LocalICGN.m).  The device runs the loop body (:64-164); the bad-point marking
-    (:166-189) follows; bad points are returned as NaN (the natural-neighbour fill of
-    :198-220 is left to the caller)."""
+    (:166-189) follows; bad points are filled by natural-neighbour interpolation of the good
+    ones (:198-220; outside their hull the nearest value, where MATLAB extrapolates
+    linearly), or returned as NaN with fill=False."""
     if shapeFunctionOrder != 1:
         raise AldicError("only the first-order shape function is implemented (as in the reference)")
     ctx = ctx or default_context()
@@ -858,15 +865,24 @@ def LocalICGN(U0, coordinatesFEM, Df, ImgRef, ImgDef, DICpara, ICGNmethod="Gauss
     U[2 * bad + 1] = np.nan
     for k in range(4):
         F[4 * bad + k] = np.nan
+    if fill:
+        crd = np.asarray(coordinatesFEM, dtype=np.float64)
+        nan_u = np.isnan(U[0::2])
+        U = _fill.fill_nans_natural(crd, U.reshape(-1, 2), "nearest").ravel()
+        F4 = F.reshape(-1, 4).copy()
+        F4[nan_u] = np.nan  # F is filled over the same good nodes as U (:199-218)
+        F = _fill.fill_nans_natural(crd, F4, "nearest").ravel()
     return U, F, r["H"], local_time, conv, num
 
 
 def LocalICGNQuadtree(U0, coordinatesFEM, Df, ImgRef, ImgDef, DICpara, ICGNmethod="GaussNewton", tol=1e-3,
-                      shapeFunctionOrder=1, ctx: Context | None = None):
+                      shapeFunctionOrder=1, ctx: Context | None = None, fill=True):
     """[U, F, HtempPar, LocalTime, ConvItPerEle, LocalICGNBadPtNum, markCoordHoleStrain]
     = LocalICGNQuadtree(...) (func_quadtree/LocalICGNQuadtree.m).  Device loop body
-    (:67-164), then the bad-point rules (:167-202); bad points are NaN (the region-wise
-    fill of :208-325 is left to the caller)."""
+    (:67-164), then the bad-point rules (:167-202), then the fill of the bad displacements
+    per connected region of Df['ImgRefMask'] and over the whole mesh (:208-325, natural
+    neighbour with 'nearest' outside the hull; F keeps its NaN, as the reference's F fill is
+    commented out); fill=False returns the bad points as NaN."""
     if shapeFunctionOrder != 1:
         raise AldicError("only the first-order shape function is implemented (as in the reference)")
     ctx = ctx or default_context()
@@ -879,14 +895,17 @@ def LocalICGNQuadtree(U0, coordinatesFEM, Df, ImgRef, ImgDef, DICpara, ICGNmetho
     U[2 * bad] = np.nan
     U[2 * bad + 1] = np.nan
     mark = np.nonzero(r["markHole"] == 1)[0]
+    if fill:
+        U = _fill.fill_quadtree(U, np.asarray(coordinatesFEM, dtype=np.float64), _fill_mask(Df, ImgRef))
     return U, F, r["H"], local_time, conv, num, mark
 
 
 def Subpb1Quadtree(UOld, FOld, udual, vdual, coordinatesFEM, Df, ImgRef, ImgDef, mu, beta, HPar, ALSolveStep,
-                   DICpara, ICGNmethod="GaussNewton", tol=1e-2, ctx: Context | None = None):
+                   DICpara, ICGNmethod="GaussNewton", tol=1e-2, ctx: Context | None = None, fill=True):
     """[U, HPar, ALSub1Time, ConvItPerEle, LocalICGNBadPtNum] = Subpb1Quadtree(...)
     (func_quadtree/Subpb1Quadtree.m).  Device loop body (:71-126), then the bad-point rules
-    (:130-149); bad points are NaN."""
+    (:130-149), then the region-wise and whole-mesh fill of the bad points (:188-254, the
+    mask of DICpara['ImgRefMask']); fill=False returns them as NaN."""
     ctx = ctx or default_context()
     _load_frame(ctx, Df, ImgRef, ImgDef, Df.get("ImgRefMask"))
     n = np.asarray(coordinatesFEM).shape[0]
@@ -901,6 +920,10 @@ def Subpb1Quadtree(UOld, FOld, udual, vdual, coordinatesFEM, Df, ImgRef, ImgDef,
     bad, num = bad_points_subpb1(conv)
     U[2 * bad] = np.nan
     U[2 * bad + 1] = np.nan
+    if fill:
+        mask = DICpara.get("ImgRefMask")
+        U = _fill.fill_quadtree(U, np.asarray(coordinatesFEM, dtype=np.float64),
+                                np.ones(np.shape(ImgRef)) if mask is None else np.asarray(mask))
     return U, HPar, t, conv, num
 
 

@@ -1,0 +1,199 @@
+"""The drivers' fill of bad points after the local steps: MATLAB's scatteredInterpolant with
+the 'natural' method (Sibson's natural-neighbour interpolation), host work in the reference
+as here.
+
+Callers in the reference: func/LocalICGN.m:199-220 (U, F over the whole mesh),
+func_quadtree/LocalICGNQuadtree.m:212-247 (per connected region of the mask, 'natural' +
+'nearest') and :300-325 (the whole mesh, 'natural' + 'nearest'),
+func_quadtree/Subpb1Quadtree.m:193-254, func/TemporalMatch_quadtree_ST1.m:216-235 (F,
+'natural' + 'none').
+
+Sibson coordinates of a query q with respect to the source points P are the shares of q's
+Voronoi cell (in the diagram of P + {q}) that each old cell loses.  They are computed
+exactly by half-plane clipping: the natural neighbours of q are the vertices of the Delaunay
+triangles of P whose circumcircle holds q (the Bowyer-Watson cavity; a tolerance admits
+circles through q, whose share is 0); q's cell is a box clipped by the bisectors of q and its
+natural neighbours; each neighbour's share is that cell clipped by the bisectors of the
+neighbour and its own Delaunay neighbours (which bound its old Voronoi cell).  A query whose
+cell is unbounded lies on or outside the convex hull of P: on a hull edge it takes the
+edge's linear interpolation (the limit of the Sibson coordinates there); outside, the value
+of the nearest source ('nearest') or NaN ('none').  MATLAB's default 'linear'
+extrapolation is not implemented (parity for queries outside the hull is unpinned)."""
+from __future__ import annotations
+
+import numpy as np
+
+
+class FillError(ValueError):
+    pass
+
+
+def _clip(poly, a, b):
+    """Convex polygon (k x 2) clipped to a . x <= b."""
+    if len(poly) == 0:
+        return poly
+    f = poly @ a - b
+    out = []
+    k = len(poly)
+    for i in range(k):
+        j = (i + 1) % k
+        if f[i] <= 0:
+            out.append(poly[i])
+        if (f[i] < 0 < f[j]) or (f[j] < 0 < f[i]):
+            t = f[i] / (f[i] - f[j])
+            out.append(poly[i] + t * (poly[j] - poly[i]))
+    return np.array(out) if out else np.zeros((0, 2))
+
+
+def _area(poly):
+    if len(poly) < 3:
+        return 0.0
+    x, y = poly[:, 0], poly[:, 1]
+    return 0.5 * abs(float(np.dot(x, np.roll(y, -1)) - np.dot(y, np.roll(x, -1))))
+
+
+class NaturalNeighbor:
+    """scatteredInterpolant(x, y, v, 'natural', extrap) over the source points P (k x 2)."""
+
+    def __init__(self, P, extrapolation="nearest"):
+        from scipy.spatial import Delaunay, cKDTree
+
+        self.P = np.asarray(P, dtype=np.float64)
+        if self.P.ndim != 2 or self.P.shape[1] != 2 or self.P.shape[0] < 3:
+            raise FillError("natural-neighbour interpolation needs at least 3 source points (k x 2)")
+        if extrapolation not in ("nearest", "none"):
+            raise FillError("extrapolation must be 'nearest' or 'none'")
+        self.extrap = extrapolation
+        self.tri = Delaunay(self.P)
+        self.kd = cKDTree(self.P)
+        S = self.tri.simplices
+        A, B, C = self.P[S[:, 0]], self.P[S[:, 1]], self.P[S[:, 2]]
+        d = 2.0 * (A[:, 0] * (B[:, 1] - C[:, 1]) + B[:, 0] * (C[:, 1] - A[:, 1]) + C[:, 0] * (A[:, 1] - B[:, 1]))
+        a2, b2, c2 = (A ** 2).sum(1), (B ** 2).sum(1), (C ** 2).sum(1)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            ux = (a2 * (B[:, 1] - C[:, 1]) + b2 * (C[:, 1] - A[:, 1]) + c2 * (A[:, 1] - B[:, 1])) / d
+            uy = (a2 * (C[:, 0] - B[:, 0]) + b2 * (A[:, 0] - C[:, 0]) + c2 * (B[:, 0] - A[:, 0])) / d
+        self.cc = np.stack([ux, uy], 1)
+        self.r2 = ((A - self.cc) ** 2).sum(1)
+        self.nbr_ptr, self.nbr = self.tri.vertex_neighbor_vertices
+        self.scale = float(np.ptp(self.P, axis=0).max()) or 1.0
+
+    def weights(self, q):
+        """(indices, Sibson weights) of the query q, or (None, None) when q's cell is unbounded."""
+        q = np.asarray(q, dtype=np.float64)
+        s = int(self.tri.find_simplex(q))
+        if s < 0:
+            return None, None
+        tol = 1e-10
+        cav, seen, stack = [], {s}, [s]
+        while stack:
+            t = stack.pop()
+            if ((q - self.cc[t]) ** 2).sum() <= self.r2[t] * (1 + tol) + (tol * self.scale) ** 2:
+                cav.append(t)
+                for u in self.tri.neighbors[t]:
+                    if u >= 0 and u not in seen:
+                        seen.add(u)
+                        stack.append(u)
+        nat = np.unique(self.tri.simplices[cav].ravel())
+        # q's cell: a box clipped by the bisectors; a bounded cell stops touching the box as the
+        # box grows (near the hull it can reach far past the neighbours), an unbounded one
+        # never does
+        R0 = 4.0 * (np.abs(self.P[nat] - q).max() + self.scale * 1e-6)
+        V = None
+        for R in (R0, R0 * 64, R0 * 4096, R0 * 262144):
+            W = q + R * np.array([[-1, -1], [1, -1], [1, 1], [-1, 1]], dtype=np.float64)
+            for i in nat:
+                p = self.P[i]
+                W = _clip(W, p - q, 0.5 * (p @ p - q @ q))
+            if len(W) >= 3 and np.abs(W - q).max() < 0.999 * R:
+                V = W
+                break
+        if V is None:
+            return None, None  # on the hull or outside it
+        w = np.zeros(len(nat))
+        for k, i in enumerate(nat):
+            pi = self.P[i]
+            Sx = V
+            for j in self.nbr[self.nbr_ptr[i]:self.nbr_ptr[i + 1]]:
+                pj = self.P[j]
+                Sx = _clip(Sx, pj - pi, 0.5 * (pj @ pj - pi @ pi))
+                if len(Sx) == 0:
+                    break
+            w[k] = _area(Sx)
+        tot = w.sum()
+        if not tot > 0:
+            return None, None
+        return nat, w / tot
+
+    def _on_hull_edge(self, q):
+        """Linear interpolation weights along the hull edge that holds q, if one does."""
+        tol = 1e-9 * self.scale
+        for a, b in self.tri.convex_hull:
+            pa, pb = self.P[a], self.P[b]
+            e = pb - pa
+            L2 = float(e @ e)
+            t = float((q - pa) @ e) / L2
+            if -1e-12 <= t <= 1 + 1e-12 and np.linalg.norm(pa + t * e - q) <= tol:
+                return np.array([a, b]), np.array([1.0 - t, t])
+        return None, None
+
+    def __call__(self, Q, V):
+        """Values at the queries Q (m x 2) of the data V (k or k x c)."""
+        Q = np.atleast_2d(np.asarray(Q, dtype=np.float64))
+        V = np.asarray(V, dtype=np.float64)
+        vec = V.ndim == 1
+        V2 = V[:, None] if vec else V
+        out = np.full((Q.shape[0], V2.shape[1]), np.nan)
+        for m, q in enumerate(Q):
+            idx, w = self.weights(q)
+            if idx is None:
+                idx, w = self._on_hull_edge(q)
+            if idx is not None:
+                out[m] = w @ V2[idx]
+            elif self.extrap == "nearest":
+                out[m] = V2[int(self.kd.query(q)[1])]
+        return out[:, 0] if vec else out
+
+
+def fill_nans_natural(coords, values, extrapolation="nearest"):
+    """The reference's fill of one field over the mesh (func/LocalICGN.m:199-220, with
+    'nearest' outside the hull): the rows of values (n x c) whose first column is NaN take
+    the natural-neighbour interpolation of the finite rows.  Returns a filled copy."""
+    coords = np.asarray(coords, dtype=np.float64)
+    V = np.array(values, dtype=np.float64)
+    bad = np.isnan(V[:, 0] if V.ndim > 1 else V)
+    if not bad.any() or (~bad).sum() < 3:
+        return V
+    nn = NaturalNeighbor(coords[~bad], extrapolation)
+    V[bad] = nn(coords[bad], V[~bad])
+    return V
+
+
+def fill_quadtree(U, coords, mask):
+    """LocalICGNQuadtree's fill of NaN displacements (func_quadtree/LocalICGNQuadtree.m:
+    212-247, then :300-325): per 8-connected region of the mask (bwconncomp), the region's NaN
+    nodes from its finite nodes (a region with fewer than 3 skipped), by natural-neighbour
+    interpolation with 'nearest' outside their hull; then whatever is still NaN from all
+    finite nodes.  A node belongs to the region of its rounded pixel.  U: 2n interleaved (F is
+    not filled there: the reference's F lines are commented out).  Returns a filled copy."""
+    from scipy import ndimage
+
+    coords = np.asarray(coords, dtype=np.float64)
+    U2 = np.array(U, dtype=np.float64).reshape(-1, 2)
+    mask = np.asarray(mask)
+    bad = np.isnan(U2[:, 0])
+    if bad.any():
+        lab, nlab = ndimage.label(mask != 0, structure=np.ones((3, 3), dtype=int))
+        ix = np.clip(np.floor(coords[:, 0] + 0.5).astype(np.int64) - 1, 0, mask.shape[0] - 1)
+        iy = np.clip(np.floor(coords[:, 1] + 0.5).astype(np.int64) - 1, 0, mask.shape[1] - 1)
+        node_lab = lab[ix, iy]
+        for r in range(1, nlab + 1):
+            inr = node_lab == r
+            src = inr & ~bad
+            qry = inr & bad
+            if src.sum() < 3 or not qry.any():
+                continue
+            nn = NaturalNeighbor(coords[src], "nearest")
+            U2[qry] = nn(coords[qry], U2[src])
+        U2 = fill_nans_natural(coords, U2, "nearest")
+    return U2.ravel()

@@ -562,6 +562,55 @@ def subpb2_quadtree(coords, elements, order, beta, mu, U, F, alpha=0.0, dirichle
     return Uhat
 
 
+def _clip(poly, a, b):
+    """Convex polygon (k x 2) clipped to the half-plane a . x <= b (Sutherland-Hodgman)."""
+    out = []
+    k = len(poly)
+    for i in range(k):
+        P, Q = poly[i], poly[(i + 1) % k]
+        fp, fq = a @ P - b, a @ Q - b
+        if fp <= 0:
+            out.append(P)
+        if (fp < 0 < fq) or (fq < 0 < fp):
+            t = fp / (fp - fq)
+            out.append(P + t * (Q - P))
+    return np.array(out) if out else np.zeros((0, 2))
+
+
+def _area(poly):
+    if len(poly) < 3:
+        return 0.0
+    x, y = poly[:, 0], poly[:, 1]
+    return 0.5 * abs(np.dot(x, np.roll(y, -1)) - np.dot(y, np.roll(x, -1)))
+
+
+def sibson_bruteforce(P, q):
+    """Sibson (natural-neighbour) coordinates of q with respect to the points P (k x 2) by the
+    definition, every point against every other: the Voronoi cell of q in P + {q}, and the
+    part of it each old point's cell loses.  Returns (weights, bounded); bounded is False when
+    q's cell is unbounded (q on or outside the convex hull).  For small tests only."""
+    P = np.asarray(P, dtype=np.float64)
+    q = np.asarray(q, dtype=np.float64)
+    R0 = 4.0 * (np.abs(P - q).max() + 1.0)
+    bounded = False
+    for R in (R0, R0 * 64, R0 * 4096, R0 * 262144):  # a bounded cell stops touching a growing box
+        V = q + R * np.array([[-1, -1], [1, -1], [1, 1], [-1, 1]], dtype=np.float64)
+        for p in P:
+            V = _clip(V, p - q, 0.5 * (p @ p - q @ q))
+        if len(V) > 0 and np.abs(V - q).max() < 0.999 * R:
+            bounded = True
+            break
+    w = np.zeros(len(P))
+    for i, pi in enumerate(P):
+        S = V
+        for j, pj in enumerate(P):
+            if j != i and len(S):
+                S = _clip(S, pj - pi, 0.5 * (pj @ pj - pi @ pi))
+        w[i] = _area(S)
+    tot = w.sum()
+    return (w / tot if tot > 0 else w), bounded
+
+
 def _std8(vals):
     """MATLAB std(x, 'omitnan') of the listed values, summed in order (no fused operations)."""
     xs = [x for x in vals if not np.isnan(x)]

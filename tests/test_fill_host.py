@@ -1,0 +1,75 @@
+"""CPU checks of the natural-neighbour fill (MATLAB scatteredInterpolant 'natural').
+
+The library's Sibson coordinates (Delaunay-cavity candidates, exact half-plane clipping)
+are compared with the oracle's brute-force restatement of the definition (every point clips
+every cell), and with Sibson's properties: partition of unity, linear precision inside the
+hull, the centroid property, the edge-linear limit on hull edges, 'nearest' / 'none'
+outside.  Then the drivers' fills on meshes with NaN holes.  No GPU is involved.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from aldic_b200.fill import NaturalNeighbor, fill_nans_natural, fill_quadtree
+
+
+def _lin(X):
+    return 2.0 + 0.3 * X[..., 0] - 0.7 * X[..., 1]
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_sibson_matches_the_bruteforce_definition(seed):
+    rng = np.random.default_rng(seed)
+    P = rng.random((60, 2)) * 10
+    nn = NaturalNeighbor(P)
+    for q in rng.random((25, 2)) * 8 + 1:
+        idx, w = nn.weights(q)
+        wb, bounded = O.sibson_bruteforce(P, q)
+        if idx is None:
+            assert not bounded
+            continue
+        full = np.zeros(len(P))
+        full[idx] = w
+        assert bounded and np.abs(full - wb).max() < 1e-10
+        assert abs(w.sum() - 1) < 1e-12 and np.abs(w @ P[idx] - q).max() < 1e-9
+
+
+def test_grid_with_holes_linear_precision_and_hull():
+    pts = np.array([(x, y) for x in range(12) for y in range(10)], dtype=float) * 8 + 10
+    hole = ((pts[:, 0] - 50) ** 2 + (pts[:, 1] - 46) ** 2) < 20 ** 2
+    hole |= (pts[:, 0] == 10) & (pts[:, 1] == 42)   # a border node (on the hull edge)
+    P, Q = pts[~hole], pts[hole]
+    nn = NaturalNeighbor(P, "nearest")
+    got = nn(Q, _lin(P))
+    assert np.abs(got - _lin(Q)).max() < 1e-9      # interior and hull-edge queries alike
+    for q in Q[:6]:
+        idx, w = nn.weights(q)
+        if idx is not None:
+            wb, _ = O.sibson_bruteforce(P, q)
+            full = np.zeros(len(P))
+            full[idx] = w
+            assert np.abs(full - wb).max() < 1e-10
+    far = np.array([[500.0, 500.0]])
+    assert np.array_equal(nn(far, _lin(P)), _lin(P[[np.argmin(((P - far) ** 2).sum(1))]]))
+    assert np.isnan(NaturalNeighbor(P, "none")(far, _lin(P))).all()
+
+
+def test_fill_nans_natural_and_quadtree_regions():
+    pts = np.array([(x, y) for x in range(14) for y in range(14)], dtype=float) * 8 + 10
+    n = len(pts)
+    U = np.stack([_lin(pts), 0.5 * _lin(pts)], 1)
+    bad = np.zeros(n, bool)
+    bad[[20, 21, 35, 100, 101, 150]] = True
+    Ub = U.copy()
+    Ub[bad] = np.nan
+    assert np.abs(fill_nans_natural(pts, Ub) - U).max() < 1e-9
+    # two mask regions split by a vertical gap: each region's NaN nodes come from its own nodes
+    mask = np.ones((140, 140))
+    mask[59:63, :] = 0  # pixels 60-63: between the node columns at 58 and 66
+    left = pts[:, 0] < 60
+    Uq = U.copy()
+    Uq[left, 0] += 100.0                      # the left region lives on another level
+    Uqb = Uq.copy()
+    Uqb[bad] = np.nan
+    out = fill_quadtree(Uqb.ravel(), pts, mask).reshape(-1, 2)
+    assert np.abs(out - Uq).max() < 1e-9      # no blending across the gap

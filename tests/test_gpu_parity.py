@@ -696,3 +696,31 @@ def test_subpb2_device_tensors_and_errors(A, ctx):
         A.Subpb2Quadtree({"coordinatesFEM": C, "elementsFEM": E, "neumann": [[1, 2, 0, 1]]}, 2, 0.1, 1e-3, U, F,
                          ctx=ctx)
 
+
+
+def test_local_icgn_quadtree_driver_fill(A, ctx, hole):
+    """LocalICGNQuadtree as the reference returns it: the device loop, the bad-point rules,
+    then the natural-neighbour fill per mask region and over the mesh; bad nodes (inside
+    the hole, failed subsets) filled, good nodes untouched."""
+    from aldic_b200.fill import fill_quadtree
+
+    sc = hole
+    ctx.load_image_raw(0, sc.ref, [1, sc.ref.shape[0]], [1, sc.ref.shape[1]], mask=sc.mask)
+    ctx.load_image_raw(1, sc.deff, [1, sc.ref.shape[0]], [1, sc.ref.shape[1]])
+    ctx.set_mask(sc.mask)
+    ctx.compute_gradients()
+    f, g = ctx.get_state(0), ctx.get_state(1)
+    Df = {"DfDx": ctx.get_state(2), "DfDy": ctx.get_state(3), "ImgRefMask": sc.mask}
+    xs = np.arange(24, 366, 12.0)
+    X, Y = np.meshgrid(xs, xs, indexing="ij")
+    coords = np.stack([X.ravel(), Y.ravel()], 1)
+    tu, tv = sc.disp(coords[:, 0], coords[:, 1])
+    U0 = np.stack([np.round(tu), np.round(tv)], 1).ravel()
+    U, F, H, t, conv, num, mark = A.LocalICGNQuadtree(U0, coords, Df, f, g, {"winsize": 24}, tol=1e-3, ctx=ctx)
+    Un, _, _, _, conv2, num2, _ = A.LocalICGNQuadtree(U0, coords, Df, f, g, {"winsize": 24}, tol=1e-3, ctx=ctx,
+                                                      fill=False)
+    bad = np.isnan(Un[0::2])
+    assert num == num2 and bad.sum() > 10 and np.array_equal(conv, conv2)
+    assert np.isfinite(U).all()
+    assert np.array_equal(U.reshape(-1, 2)[~bad], Un.reshape(-1, 2)[~bad])
+    assert np.array_equal(U, fill_quadtree(Un, coords, sc.mask))
