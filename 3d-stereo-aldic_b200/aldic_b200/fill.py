@@ -45,6 +45,13 @@ def _clip(poly, a, b):
     return np.array(out) if out else np.zeros((0, 2))
 
 
+def _circumcentre(a, b, c):
+    d = 2.0 * (a[0] * (b[1] - c[1]) + b[0] * (c[1] - a[1]) + c[0] * (a[1] - b[1]))
+    a2, b2, c2 = a @ a, b @ b, c @ c
+    return np.array([(a2 * (b[1] - c[1]) + b2 * (c[1] - a[1]) + c2 * (a[1] - b[1])) / d,
+                     (a2 * (c[0] - b[0]) + b2 * (a[0] - c[0]) + c2 * (b[0] - a[0])) / d])
+
+
 def _area(poly):
     if len(poly) < 3:
         return 0.0
@@ -78,12 +85,12 @@ class NaturalNeighbor:
         self.nbr_ptr, self.nbr = self.tri.vertex_neighbor_vertices
         self.scale = float(np.ptp(self.P, axis=0).max()) or 1.0
 
-    def weights(self, q):
-        """(indices, Sibson weights) of the query q, or (None, None) when q's cell is unbounded."""
-        q = np.asarray(q, dtype=np.float64)
+    def _cavity(self, q):
+        """Delaunay triangles whose circumcircle holds q (the query's simplex first), or None
+        outside the hull."""
         s = int(self.tri.find_simplex(q))
         if s < 0:
-            return None, None
+            return None
         tol = 1e-10
         cav, seen, stack = [], {s}, [s]
         while stack:
@@ -94,6 +101,84 @@ class NaturalNeighbor:
                     if u >= 0 and u not in seen:
                         seen.add(u)
                         stack.append(u)
+        return cav
+
+    def weights(self, q):
+        """(indices, Sibson weights) of the query q, or (None, None) when q's cell is unbounded.
+        Watson's construction: walking the cavity's boundary around q, q's new Voronoi
+        vertices are the circumcentres of (q, b_i, b_i+1); the area q takes from b_i is the
+        polygon of the two new vertices at b_i and the circumcentres of the cavity triangles
+        at b_i, in fan order.  Falls back to half-plane clipping when the cavity is not a
+        simple ring (near-degenerate ties)."""
+        q = np.asarray(q, dtype=np.float64)
+        cav = self._cavity(q)
+        if cav is None:
+            return None, None
+        S, NB = self.tri.simplices, self.tri.neighbors
+        incav = set(cav)
+        nxt, tri_of = {}, {}
+        for t in cav:  # boundary edges, oriented counter-clockwise as the triangles are
+            a, b, c = S[t]
+            ccw = ((self.P[b] - self.P[a])[0] * (self.P[c] - self.P[a])[1]
+                   - (self.P[b] - self.P[a])[1] * (self.P[c] - self.P[a])[0]) > 0
+            for k in range(3):
+                if NB[t][k] in incav:
+                    continue
+                if NB[t][k] < 0:
+                    return self._weights_clip(q, cav)  # cavity reaches the hull
+                u, v = S[t][(k + 1) % 3], S[t][(k + 2) % 3]
+                if not ccw:
+                    u, v = v, u
+                if u in nxt:
+                    return self._weights_clip(q, cav)
+                nxt[u] = v
+                tri_of[(u, v)] = t
+        ring = [next(iter(nxt))]
+        while True:
+            w_ = nxt.get(ring[-1])
+            if w_ is None:
+                return self._weights_clip(q, cav)
+            if w_ == ring[0]:
+                break
+            ring.append(w_)
+            if len(ring) > len(nxt):
+                return self._weights_clip(q, cav)
+        if len(ring) != len(nxt):
+            return self._weights_clip(q, cav)
+        m = len(ring)
+        B = self.P[ring]
+        newv = np.array([_circumcentre(q, B[i], B[(i + 1) % m]) for i in range(m)])
+        w = np.zeros(m)
+        for i in range(m):
+            bi = ring[i]
+            prev, nx = ring[i - 1], ring[(i + 1) % m]
+            t, came, end = tri_of[(prev, bi)], -1, tri_of[(bi, nx)]
+            pts = [newv[i - 1]]
+            for _ in range(len(cav) + 1):  # the fan of cavity triangles at bi
+                pts.append(self.cc[t])
+                if t == end:
+                    break
+                k_bi = int(np.nonzero(S[t] == bi)[0][0])
+                step = -1
+                for k in range(3):  # across an edge at bi, into the cavity, not back
+                    u = NB[t][k]
+                    if k != k_bi and u >= 0 and u in incav and u != came:
+                        step = u
+                        break
+                if step < 0:
+                    return self._weights_clip(q, cav)
+                came, t = t, step
+            else:
+                return self._weights_clip(q, cav)
+            pts.append(newv[i])
+            w[i] = _area(np.array(pts))
+        tot = w.sum()
+        if not tot > 0:
+            return None, None
+        return np.array(ring), w / tot
+
+    def _weights_clip(self, q, cav):
+        """Sibson weights by clipping (see the module note); (None, None) for an unbounded cell."""
         nat = np.unique(self.tri.simplices[cav].ravel())
         # q's cell: a box clipped by the bisectors; a bounded cell stops touching the box as the
         # box grows (near the hull it can reach far past the neighbours), an unbounded one
