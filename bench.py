@@ -629,6 +629,24 @@ def main():
 # ----------------------------------------------------------------------------------
 # the 2D temporal (512^2) and quadtree ALDIC (2048^2, hole + notch, Subpb1) workloads
 # ----------------------------------------------------------------------------------
+def admm_beta(betas, errs):
+    """The reference's beta for the first frame (func/TemporalMatch_quadtree_ST1.m:274-294):
+    |U1 - U2| over the three-entry beta list normalised by its mean and standard deviation,
+    the minimum's beta, or, with the minimum in the middle, the vertex of the parabola in
+    log10(beta) through the three points (MATLAB's fit(..., 'poly2') there, whose try falls
+    to the list's beta at an end)."""
+    e = np.asarray(errs, dtype=np.float64)
+    sd = e.std(ddof=1)
+    if not (np.isfinite(sd) and sd > 0):  # MATLAB's min over NaN picks the first entry
+        return betas[0]
+    z = (e - e.mean()) / sd
+    k = int(np.argmin(z))
+    if k != 1:
+        return betas[k]
+    p = np.polyfit(np.log10(betas), z, 2)
+    return 10 ** (-p[1] / 2 / p[0])
+
+
 def run_aux(args, P):
     """temporal512: LocalICGN on a 512^2 affine pair, FFT-search init.
     quadtree2048 (config 2): one ALDIC frame on a 2048^2 plate with a hole and an edge notch:
@@ -701,20 +719,6 @@ def run_aux(args, P):
     glob = {"U2": [T.empty(2 * n, **f64) for _ in range(3)], "out": T.empty(2 * n, **f64), "beta": None,
             "sub_in": None, "last": None}
 
-    def select_beta(errs):
-        """The reference's beta for the first frame (func/TemporalMatch_quadtree_ST1.m:274-294):
-        normalised |U1 - U2| over the beta list, a parabola in log10(beta) through the
-        minimum and its neighbours, the list's beta when the minimum is at an end."""
-        e = np.asarray(errs, dtype=np.float64)
-        z = (e - e.mean()) / e.std(ddof=1)
-        if not np.isfinite(z).all():
-            return betas[0]
-        k = int(np.argmin(z))
-        if k != 1:
-            return betas[k]
-        p = np.polyfit(np.log10(betas), z, 2)
-        return 10 ** (-p[1] / 2 / p[0])
-
     def aldic_frame():
         """ALDIC after the local step (func/TemporalMatch_quadtree_ST1.m:248-380): the global
         step with the first frame's beta tuning, then admm x (Subpb1, Subpb2, dual update),
@@ -728,7 +732,7 @@ def run_aux(args, P):
         for k, bt in enumerate(betas):
             ctx.subpb2(coords, None, 2, bt, P["mu"], U1, F1, out=glob["U2"][k])
             errs.append(T.linalg.vector_norm(U1 - glob["U2"][k]))
-        beta = select_beta(T.stack(errs).cpu().numpy())
+        beta = admm_beta(betas, T.stack(errs).cpu().numpy())
         U2 = glob["U2"][2]
         if abs(beta - betas[2]) > np.finfo(float).eps:
             ctx.subpb2(coords, None, 2, beta, P["mu"], U1, F1, out=glob["out"])

@@ -42,3 +42,19 @@ def test_workloads_are_defined():
         P = bench.workload_params(name)
         assert P["w"] % 2 == 0 and P["step"] > 0
     assert set(bench.TILE_TRAFFIC) == {"stereo2048", "stereo1024"}
+
+
+def test_admm_beta_follows_the_reference_rule():
+    import bench
+
+    betas = [c * 16.0 ** 2 * 1e-3 for c in (1e-3, 1e-2, 1e-1)]
+    assert bench.admm_beta(betas, [1.0, 2.0, 3.0]) == betas[0]
+    assert bench.admm_beta(betas, [3.0, 2.0, 1.0]) == betas[2]
+    # minimum in the middle: the vertex of the parabola through the normalised errors
+    errs = [2.0, 1.0, 1.5]
+    b = bench.admm_beta(betas, errs)
+    x = np.log10(betas)
+    z = (np.array(errs) - np.mean(errs)) / np.std(errs, ddof=1)
+    p = np.polyfit(x, z, 2)
+    assert abs(np.log10(b) - (-p[1] / (2 * p[0]))) < 1e-12 and x[0] < np.log10(b) < x[2]
+    assert bench.admm_beta(betas, [1.0, 1.0, 1.0]) == betas[0]  # no spread: MATLAB's min of NaN
