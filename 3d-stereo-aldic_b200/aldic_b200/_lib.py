@@ -53,6 +53,7 @@ SIGNATURES = {
     "aldic_init_u0": (_i, [_vp, _i, _i, _vp, _vp, _i, _vp]),
     "aldic_remove_outliers": (_i, [_vp, _i, _i, _vp, _vp, _d, _i, _vp]),
     "aldic_subpb2_set_mesh": (_i, [_vp, _i64, _i64, _vp, _i64, _vp]),
+    "aldic_sibson_weights": (_i, [_i64, _vp, _i64, _vp, _vp, _vp, _vp, _d, _i64, _vp, _vp, _i, _vp, _vp, _vp]),
     "aldic_subpb2": (_i, [_vp, _i64, _vp, _i64, _vp, _i, _d, _d, _d, _vp, _vp, _i64, _vp, _d, _i, _vp,
                           _vp]),
     "aldic_measure_fp32_peak": (_i, [_vp, C.POINTER(_d)]),

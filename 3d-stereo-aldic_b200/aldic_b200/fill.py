@@ -8,6 +8,10 @@ func_quadtree/LocalICGNQuadtree.m:212-247 (per connected region of the mask, 'na
 func_quadtree/Subpb1Quadtree.m:193-254, func/TemporalMatch_quadtree_ST1.m:216-235 (F,
 'natural' + 'none').
 
+The per-query construction runs in the library's host code (aldic_sibson_weights); the
+rare queries it hands back (cavities that reach the hull, ties that break the ring) take
+the Python path below, and queries outside the hull the extrapolation.
+
 Sibson coordinates of a query q with respect to the source points P are the shares of q's
 Voronoi cell (in the diagram of P + {q}) that each old cell loses.  They are computed
 exactly by half-plane clipping: the natural neighbours of q are the vertices of the Delaunay
@@ -222,6 +226,33 @@ class NaturalNeighbor:
                 return np.array([a, b]), np.array([1.0 - t, t])
         return None, None
 
+    def native_weights(self, Q, cap=512):
+        """Watson's construction for all queries at once in the library's host code
+        (aldic_sibson_weights): (idx, w, count) with count -2 outside the hull and -1 where
+        the construction needs the Python path."""
+        import ctypes as C
+
+        from . import _lib
+
+        lib = _lib.load()
+        Q = np.ascontiguousarray(np.atleast_2d(np.asarray(Q, dtype=np.float64)))
+        m = Q.shape[0]
+        P = np.ascontiguousarray(self.P)
+        S = np.ascontiguousarray(self.tri.simplices, dtype=np.int32)
+        NB = np.ascontiguousarray(self.tri.neighbors, dtype=np.int32)
+        cc = np.ascontiguousarray(self.cc)
+        r2 = np.ascontiguousarray(self.r2)
+        qs = np.ascontiguousarray(self.tri.find_simplex(Q), dtype=np.int32)
+        idx = np.zeros((m, cap), dtype=np.int32)
+        w = np.zeros((m, cap))
+        cnt = np.zeros(m, dtype=np.int32)
+        vp = lambda a: C.c_void_p(a.ctypes.data)  # noqa: E731
+        rc = lib.aldic_sibson_weights(P.shape[0], vp(P), S.shape[0], vp(S), vp(NB), vp(cc), vp(r2), self.scale, m,
+                                      vp(Q), vp(qs), cap, vp(idx), vp(w), vp(cnt))
+        if rc != 0:
+            raise FillError(f"aldic_sibson_weights failed with code {rc}")
+        return idx, w, cnt
+
     def __call__(self, Q, V):
         """Values at the queries Q (m x 2) of the data V (k or k x c)."""
         Q = np.atleast_2d(np.asarray(Q, dtype=np.float64))
@@ -229,12 +260,17 @@ class NaturalNeighbor:
         vec = V.ndim == 1
         V2 = V[:, None] if vec else V
         out = np.full((Q.shape[0], V2.shape[1]), np.nan)
+        idx, w, cnt = self.native_weights(Q)
         for m, q in enumerate(Q):
-            idx, w = self.weights(q)
-            if idx is None:
-                idx, w = self._on_hull_edge(q)
-            if idx is not None:
-                out[m] = w @ V2[idx]
+            c = int(cnt[m])
+            if c > 0:
+                out[m] = w[m, :c] @ V2[idx[m, :c]]
+                continue
+            ii, ww = self.weights(q) if c == -1 else (None, None)
+            if ii is None:
+                ii, ww = self._on_hull_edge(q)
+            if ii is not None:
+                out[m] = ww @ V2[ii]
             elif self.extrap == "nearest":
                 out[m] = V2[int(self.kd.query(q)[1])]
         return out[:, 0] if vec else out

@@ -158,6 +158,22 @@ int aldic_subpb2(aldic_ctx* ctx, int64_t n, const double* coords, int64_t n_el, 
 int aldic_subpb2_set_mesh(aldic_ctx* ctx, int64_t n, int64_t n_el, const int32_t* elements, int64_t n_dirichlet,
                           const int32_t* dirichlet);
 
+/* ------------------------------------------------- bad-point fill (host) ------- */
+/* Sibson (natural-neighbour) weights of m queries Q (m x 2, row-major (x, y) pairs) with
+ * respect to k source points P (k x 2, row-major), for MATLAB's scatteredInterpolant
+ * 'natural' in the drivers' fill of bad points (func/LocalICGN.m:199-220,
+ * func_quadtree/LocalICGNQuadtree.m:212-325).  Host code; no context, no device.  The
+ * caller supplies a Delaunay triangulation of P: simplices and neighbors (ntri x 3,
+ * row-major; neighbour e lies opposite vertex e, -1 on the hull), circumcentres cc (ntri x 2)
+ * and squared circumradii r2, the containing triangle of each query (qsimplex, -1 outside)
+ * and the point set's extent (scale, for the in-circle tolerance).  Per query: idx / w
+ * (cap entries each) receive the natural neighbours and their weights, count the number
+ * used, or -2 outside the hull, -1 where the cavity reaches the hull, is not a simple ring
+ * or has more than cap vertices (the caller computes those another way). */
+int aldic_sibson_weights(int64_t k, const double* P, int64_t ntri, const int32_t* simplices, const int32_t* neighbors,
+                         const double* cc, const double* r2, double scale, int64_t m, const double* Q,
+                         const int32_t* qsimplex, int32_t cap, int32_t* idx, double* w, int32_t* count);
+
 /* ------------------------------------------------------ initial guess --------- */
 /* inpaint_nans(A, 4) (func/inpaint_nans.m:369-398, spring analogy), in place on an m x n
  * column-major grid: the NaN entries become the least-squares solution of unit springs

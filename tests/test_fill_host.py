@@ -73,3 +73,33 @@ def test_fill_nans_natural_and_quadtree_regions():
     Uqb[bad] = np.nan
     out = fill_quadtree(Uqb.ravel(), pts, mask).reshape(-1, 2)
     assert np.abs(out - Uq).max() < 1e-9      # no blending across the gap
+
+
+def test_native_weights_match_the_python_construction():
+    """The library's host code (aldic_sibson_weights) against the Python construction and
+    the brute-force definition, on random points and on a grid with a large hole."""
+    rng = np.random.default_rng(9)
+    cases = [rng.random((120, 2)) * 10]
+    pts = np.array([(x, y) for x in range(30) for y in range(30)], dtype=float) * 8 + 10
+    hole = ((pts[:, 0] - 130) ** 2 + (pts[:, 1] - 120) ** 2) < 60 ** 2
+    cases.append(pts[~hole])
+    queries = [rng.random((60, 2)) * 9 + 0.5, pts[hole]]
+    for P, Q in zip(cases, queries):
+        nn = NaturalNeighbor(P)
+        idx, w, cnt = nn.native_weights(Q)
+        assert (cnt > 0).mean() > 0.8
+        for m, q in enumerate(Q):
+            if cnt[m] <= 0:
+                continue
+            a = np.zeros(len(P))
+            a[idx[m, :cnt[m]]] = w[m, :cnt[m]]
+            i2, w2 = nn.weights(q)
+            b = np.zeros(len(P))
+            b[i2] = w2
+            assert np.abs(a - b).max() < 1e-12
+        for m in range(0, len(Q), 20):
+            if cnt[m] > 0 and len(P) <= 150:  # the definition by brute force: small sets only
+                a = np.zeros(len(P))
+                a[idx[m, :cnt[m]]] = w[m, :cnt[m]]
+                wb, _ = O.sibson_bruteforce(P, Q[m])
+                assert np.abs(a - wb).max() < 1e-10
