@@ -649,8 +649,8 @@ def admm_beta(betas, errs):
 
 
 def run_aux(args, P):
-    """temporal512 (BASELINE config 0): LocalICGN on a 512^2 affine pair, FFT-search init.
-    quadtree2048 (config 2): one ALDIC frame on a 2048^2 plate with a hole and an edge notch:
+    """temporal512: LocalICGN on a 512^2 affine pair, FFT-search init.
+    quadtree2048: one ALDIC frame on a 2048^2 plate with a hole and an edge notch:
     search, bad-point removal, Init, LocalICGNQuadtree on the quadtree mesh of
     GenerateQuadtreeMesh, the global step with the first frame's beta tuning, and two ADMM
     rounds of Subpb1Quadtree + Subpb2Quadtree.  Device-resident; verified on the oracle."""
@@ -901,8 +901,8 @@ def run_aux(args, P):
 
 
 def run_sequence(args, P):
-    """sequence4096 (BASELINE config 4, without the learned initial guess): 50 stereo frame
-    pairs at 4096 x 3000 uint16 with the stereo rig of config 1 aimed at a plane stretched
+    """sequence4096 (without the learned initial guess): 50 stereo frame
+    pairs at 4096 x 3000 uint16 with the stereo rig of the stereo2048 workload aimed at a plane stretched
     progressively (8 % in x at the last frame) with a growing local bulge, rendered on the GPU.
     Frame 0: stereo L0 -> R0 whole-field search + IC-GN (set-up, timed separately).  Frames
     1..49, each timed alone: temporal L0 -> Lk and R0 -> Rk IC-GN on the left mesh and the
