@@ -560,7 +560,7 @@ def funRemoveOutliers(u, v, cc, qDICOrNot, Thr0, ctx: Context | None = None):
 def IntegerSearchQuadtree(ImgRef, ImgDef, file_name, DICpara, ImgSeqNum, ctx: Context | None = None):
     """[DICpara, x0, y0, u, v, cc] = IntegerSearchQuadtree(ImgRef, ImgDef, file_name, DICpara,
     ImgSeqNum) (func_quadtree/IntegerSearchQuadtree.m), whole-field mode
-    (InitFFTSearchMethod 1).  The search distance follows :48-62 -- stereo (ImgSeqNum -1):
+    (InitFFTSearchMethod 1) or all-zero initial guesses (3).  The search distance follows :48-62 -- stereo (ImgSeqNum -1):
     StereoSearchDistance, else NewFFTSearchDistance; temporal (ImgSeqNum >= 2):
     TemporalSearchDistance, else NewFFTSearchDistance -- and a missing one raises instead of
     prompting.  The whole-field search runs on the device (:93); grid points whose rounded
@@ -568,8 +568,19 @@ def IntegerSearchQuadtree(ImgRef, ImgDef, file_name, DICpara, ImgSeqNum, ctx: Co
     bad-point removal funRemoveOutliers(u, v, cc, 0, 100) runs on the device (:158-160; the
     NaN holes stay NaN for Init to fill)."""
     method = DICpara.get("InitFFTSearchMethod", 1)
+    if method == 3:  # all initial guesses zero (:213-222): the ROI grid at winstepsize, no search
+        roi = DICpara["gridxyROIRange"]
+        st = int(np.ravel(DICpara["winstepsize"])[0])
+        xs = np.arange(roi["gridx"][0], roi["gridx"][1] + 1, st, dtype=np.float64)
+        ys = np.arange(roi["gridy"][0], roi["gridy"][1] + 1, st, dtype=np.float64)
+        x0 = np.tile(xs, (ys.size, 1))
+        y0 = np.tile(ys[:, None], (1, xs.size))
+        z = np.zeros(x0.shape)
+        return (dict(DICpara, InitFFTSearchMethod=3, SizeOfFFTSearchRegion=np.array([0, 0])), x0, y0, z, z.copy(),
+                {"max": np.ones(x0.shape)})
     if method != 1:
-        raise AldicError("IntegerSearchQuadtree: only the whole-field mode (InitFFTSearchMethod 1) is implemented")
+        raise AldicError("IntegerSearchQuadtree: the whole-field (1) and zero (3) initial guesses are implemented; "
+                         "modes 0 and 2 need interactive input in the reference")
     keys = ("StereoSearchDistance", "NewFFTSearchDistance") if ImgSeqNum == -1 else \
         ("TemporalSearchDistance", "NewFFTSearchDistance") if ImgSeqNum >= 2 else ()
     s = None

@@ -96,3 +96,16 @@ def test_mesh_setup_matches_the_reference_loops():
     assert np.array_equal(D["coordinatesFEMWorld"][:, 1], 91 - cf[:, 1])
     # the node list is the XList-fastest mesh the pipelines use
     assert D["coordinatesFEM"][1, 0] - D["coordinatesFEM"][0, 0] == 8
+
+
+def test_integer_search_quadtree_zero_initial_guess():
+    import aldic_b200 as A
+
+    para = {"InitFFTSearchMethod": 3, "gridxyROIRange": {"gridx": [11, 60], "gridy": [5, 40]}, "winstepsize": 8}
+    p2, x0, y0, u, v, cc = A.IntegerSearchQuadtree(None, None, None, para, 2)
+    xs, ys = np.arange(11, 61, 8), np.arange(5, 41, 8)   # MATLAB gridx(1):step:gridx(2)
+    assert x0.shape == (ys.size, xs.size) and np.array_equal(x0[0], xs) and np.array_equal(y0[:, 0], ys)
+    assert not u.any() and not v.any() and (cc["max"] == 1).all()
+    assert list(p2["SizeOfFFTSearchRegion"]) == [0, 0] and p2["InitFFTSearchMethod"] == 3
+    with pytest.raises(A.AldicError):
+        A.IntegerSearchQuadtree(None, None, None, dict(para, InitFFTSearchMethod=2), 2)
