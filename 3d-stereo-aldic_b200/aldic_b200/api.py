@@ -26,6 +26,7 @@ __all__ = [
     "LocalICGN", "LocalICGNQuadtree", "Subpb1", "Subpb1Quadtree", "epipolar_ICGN1",
     "stereoReconstruction_quadtree", "bad_points_local", "bad_points_subpb1", "Init", "funUndistortPoints",
     "IntegerSearchQuadtree", "MeshSetUp", "funRemoveOutliers", "Subpb2Quadtree", "GenerateQuadtreeMesh",
+    "StereoMatch_STAQ",
 ]
 
 
@@ -965,6 +966,52 @@ def epipolar_ICGN1(pointCandidate, Df, ImgRef, ImgDef, winsize, tol, ICGNmethod=
     _load_frame(ctx, Df, ImgRef, ImgDef, None)
     pts = np.atleast_2d(np.asarray(pointCandidate, dtype=np.float64))
     return ctx.epipolar_icgn(pts, winsize, tol)
+
+
+def StereoMatch_STAQ(RD_L, RD_R, Normalized_L, Normalized_R, file_name_L, NormalizedMask_L, NormalizedMask_R,
+                     DICpara, StereoInfo, stereoMatchShapeOrder=1, ctx: Context | None = None):
+    """[StereoInfo, RD_L, RD_R] = StereoMatch_STAQ(...) (func/StereoMatch_STAQ.m), the stereo
+    match of the first frame pair, step for step: gradients of the left image (:22), the
+    whole-field search with its bad-point removal (IntegerSearchQuadtree, stereo distance,
+    :25), the uniform mesh (MeshSetUp, :28) and Init (:33), nodes outside the left mask NaN
+    (:36-41), the quadtree mesh (GenerateQuadtreeMesh with elementMinSize =
+    DICpara['winsizeMin'], :63-64) and LocalICGNQuadtree with tol 1e-3 (:86-93), then
+    ResultFEMesh_corr = coordinates + U (:105-117).  The search, Init and IC-GN run on the
+    device; meshing and the fills on the host, as in the reference.  Only the first-order
+    shape function exists (stereoMatchShapeOrder 1)."""
+    if stereoMatchShapeOrder != 1:
+        raise AldicError("StereoMatch_STAQ: only the first-order shape function is implemented")
+    ctx = ctx or default_context()
+    StereoInfo = dict(StereoInfo or {})
+    RD_R = dict(RD_R or {})
+    maskL = np.asarray(NormalizedMask_L, dtype=np.float64)
+    Df = funImgGradient(Normalized_L, Normalized_L, maskL, ctx=ctx)
+    DICpara, x0, y0, u, v, cc = IntegerSearchQuadtree(Normalized_L, Normalized_R, file_name_L, DICpara, -1, ctx=ctx)
+    mesh = MeshSetUp(x0, y0, DICpara)
+    U0 = Init(u, v, cc["max"], mesh["x0"], mesh["y0"], 0, ctx=ctx)
+    C = mesh["coordinatesFEM"]
+    ix = np.floor(C[:, 0] + 0.5).astype(np.int64) - 1
+    iy = np.floor(C[:, 1] + 0.5).astype(np.int64) - 1
+    out = maskL[ix, iy] < 1
+    U0 = np.array(U0, dtype=np.float64)
+    U0[2 * np.flatnonzero(out)] = np.nan
+    U0[2 * np.flatnonzero(out) + 1] = np.nan
+    StereoInfo["ResultFEMesh"] = {"coordinatesFEM": C, "elementsFEM": mesh["elementsFEM"],
+                                  "winsize": DICpara["winsize"], "winstepsize": DICpara["winstepsize"],
+                                  "gridxyROIRange": DICpara["gridxyROIRange"]}
+    mesh["elementMinSize"] = DICpara["winsizeMin"]
+    mesh, DICpara, U0 = GenerateQuadtreeMesh(U0, Df, maskL, mesh, DICpara)
+    StereoInfo["ResultFEMeshEachFrame"] = {"coordinatesFEM": mesh["coordinatesFEM"],
+                                           "elementsFEM": mesh["elementsFEM"],
+                                           "markCoordHoleEdge": mesh["markCoordHoleEdge"]}
+    U, *_ = LocalICGNQuadtree(U0, mesh["coordinatesFEM"], Df, Normalized_L, Normalized_R, DICpara, "GaussNewton",
+                              1e-3, 1, ctx=ctx)
+    StereoInfo["U"] = U
+    Cq = mesh["coordinatesFEM"]
+    StereoInfo["ResultFEMesh_corr"] = Cq + (U.reshape(-1, 2) if U.size == Cq.size else 0.0)
+    RD_R["Coordinates_corr"] = StereoInfo["ResultFEMesh_corr"]
+    StereoInfo["CalPointsNum"] = np.shape(u)
+    return StereoInfo, RD_L, RD_R
 
 
 def _has_distortion(cameraParams, side):

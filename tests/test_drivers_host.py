@@ -1,0 +1,81 @@
+"""CPU check of the stereo match driver's glue (StereoMatch_STAQ).
+
+The driver composes the library's calls (gradients, whole-field search, bad-point removal,
+Init, IC-GN) with the host steps (MeshSetUp, GenerateQuadtreeMesh, the fills).  Here it runs
+on a stand-in context whose device calls are the oracle's restatements, so the test checks
+the order of the steps, the arguments passed between them and the outputs' layout, without
+a GPU; the device calls themselves are checked against the oracle by the GPU tests.
+"""
+import numpy as np
+
+import oracle as O
+from aldic_b200 import synth
+
+
+class OracleContext:
+    """The Context methods the MATLAB-named drivers call, restated by the oracle."""
+
+    def __init__(self):
+        self.img = [None, None]
+        self.mask = None
+        self.g = (None, None)
+
+    def load_image(self, slot, img):
+        self.img[slot] = np.asarray(img, dtype=np.float64)
+
+    def set_mask(self, mask):
+        self.mask = None if mask is None else np.asarray(mask, dtype=np.float64)
+
+    def compute_gradients(self):
+        self.g = O.gradient(self.img[0], self.mask)
+
+    def set_gradients(self, dfdx, dfdy):
+        self.g = (np.asarray(dfdx, dtype=np.float64), np.asarray(dfdy, dtype=np.float64))
+
+    def get_state(self, what):
+        return [self.img[0], self.img[1], self.g[0], self.g[1]][what]
+
+    def integer_search(self, search, gridx, gridy, winsize, step):
+        return O.integer_search(self.img[0], self.img[1], list(np.ravel(search)), gridx, gridy, winsize, step)
+
+    def remove_outliers(self, u, v, thr=100.0, maxit=0, info=False):
+        u2, v2, _ = O.remove_outliers(u, v, thr)
+        return u2, v2
+
+    def init_u0(self, u, v, out=None, index=0):
+        return O.init_u0(u, v, index)
+
+    def local_icgn(self, variant, coords, U0, winsize, tol, **kw):
+        frame = O.Frame(self.img[0], self.img[1], self.mask, self.g[0], self.g[1])
+        return O.local_icgn(frame, np.asarray(coords, dtype=np.float64), np.asarray(U0, dtype=np.float64), winsize,
+                            tol, variant=variant)
+
+
+def test_stereo_match_driver_on_the_oracle():
+    import aldic_b200 as A
+
+    O.build()
+    sc = synth.temporal_affine(seed=3, M=192, N=176, n_speckles=1200, u=2.6, v=-1.4)
+    M, N = sc.ref.shape
+    mask = np.ones((M, N))
+    X, Y = np.meshgrid(np.arange(1, M + 1), np.arange(1, N + 1), indexing="ij")
+    mask[(X - 96) ** 2 + (Y - 90) ** 2 < 24 ** 2] = 0
+    para = {"winsize": 20, "winstepsize": 16, "winsizeMin": 4, "StereoSearchDistance": 6, "ImgSize": [M, N],
+            "gridxyROIRange": {"gridx": [1, M], "gridy": [1, N]}, "ImgRefMask": mask}
+    info, RD_L, RD_R = A.StereoMatch_STAQ({}, {}, sc.ref.astype(float), sc.deff.astype(float), None, mask, mask,
+                                          para, {}, 1, ctx=OracleContext())
+    C = info["ResultFEMeshEachFrame"]["coordinatesFEM"]
+    E = info["ResultFEMeshEachFrame"]["elementsFEM"]
+    assert E.shape[1] == 8 and (E[:, 4:] > 0).any()               # a quadtree with hanging nodes
+    assert info["U"].shape == (2 * C.shape[0],) and np.isfinite(info["U"]).all()   # filled
+    assert np.array_equal(RD_R["Coordinates_corr"], C + info["U"].reshape(-1, 2))
+    # away from the hole and the border, the match is the true displacement
+    tu, tv = sc.disp(C[:, 0], C[:, 1])
+    ix = np.floor(C[:, 0] + 0.5).astype(int) - 1
+    iy = np.floor(C[:, 1] + 0.5).astype(int) - 1
+    far = (np.hypot(C[:, 0] - 96, C[:, 1] - 90) > 40) & (C[:, 0] > 20) & (C[:, 0] < M - 20) & \
+          (C[:, 1] > 20) & (C[:, 1] < N - 20) & (mask[ix, iy] > 0)
+    err = np.hypot(info["U"][0::2] - tu, info["U"][1::2] - tv)[far]
+    assert far.sum() > 20 and np.median(err) < 0.02
+    # CalPointsNum is the search grid's shape, the uniform mesh's node count
+    assert int(np.prod(info["CalPointsNum"])) == info["ResultFEMesh"]["coordinatesFEM"].shape[0]
