@@ -26,7 +26,7 @@ __all__ = [
     "LocalICGN", "LocalICGNQuadtree", "Subpb1", "Subpb1Quadtree", "epipolar_ICGN1",
     "stereoReconstruction_quadtree", "bad_points_local", "bad_points_subpb1", "Init", "funUndistortPoints",
     "IntegerSearchQuadtree", "MeshSetUp", "funRemoveOutliers", "Subpb2Quadtree", "GenerateQuadtreeMesh",
-    "StereoMatch_STAQ",
+    "StereoMatch_STAQ", "ALDICFrameQuadtree", "subpb2_beta",
 ]
 
 
@@ -542,6 +542,98 @@ def Subpb2Quadtree(DICmesh, GaussPtOrder, beta, mu, U, F, udual=None, vdual=None
     dirichlet = DICmesh.get("dirichlet")
     return ctx.subpb2(DICmesh["coordinatesFEM"], DICmesh["elementsFEM"], GaussPtOrder, beta, mu, U, F, alpha=alpha,
                       dirichlet=None if dirichlet is None or np.size(dirichlet) == 0 else dirichlet)
+
+
+def subpb2_beta(betaList, errs):
+    """The reference's beta for the first frame (func/TemporalMatch_quadtree_ST1.m:274-294):
+    |U1 - U2| over the three-entry beta list normalised by its mean and standard deviation,
+    the minimum's beta, or, with the minimum in the middle, the vertex of the parabola in
+    log10(beta) through the three points (MATLAB's fit(..., 'poly2') there, whose try falls
+    to the list's beta at an end)."""
+    e = np.asarray(errs, dtype=np.float64)
+    sd = e.std(ddof=1)
+    if not (np.isfinite(sd) and sd > 0):  # MATLAB's min over NaN picks the first entry
+        return betaList[0]
+    z = (e - e.mean()) / sd
+    k = int(np.argmin(z))
+    if k != 1:
+        return betaList[k]
+    p = np.polyfit(np.log10(betaList), z, 2)
+    return 10 ** (-p[1] / 2 / p[0])
+
+
+def ALDICFrameQuadtree(fNormalized, gNormalized, fNormalizedMask, DICpara, ImgSeqNum=2, file_name=None,
+                       shapeFuncOrder=1, ctx: Context | None = None):
+    """One frame of func/TemporalMatch_quadtree_ST1.m (:41-390, sections 3 to 6) in its
+    default form (accumulative, whole-field search initial guess, UseGlobal): gradients of
+    the reference frame; IntegerSearchQuadtree (search and bad-point removal), MeshSetUp, Init
+    and the nodes outside the mask set NaN (:108-160); GenerateQuadtreeMesh with
+    elementMinSize = DICpara['winsizeMin'] (:163-169); LocalICGNQuadtree with tol 1e-2 and
+    its fills, then the section-4 fills of U and F ('natural', 'none', :200-240); the global
+    step with mu = 1e-3, alpha = 0, Gauss order 2, beta tuned over [1e-3 1e-2 1e-1]
+    mean(winstepsize)^2 mu at frame 2 (DICpara['beta'] or the list's first entry later,
+    :266-306), the hole-strain nodes held at the local result, the duals (:313-323); two ADMM
+    rounds of Subpb1Quadtree + Subpb2Quadtree (:333-389).  Returns a dict: DICmesh, U
+    (USubpb2), USubpb1, FSubpb1, beta, markCoordHoleStrain, DICpara.  The displacement
+    smoothing options (DispSmoothness, Smooth2DTimes) are not implemented and must be 0."""
+    if DICpara.get("DispSmoothness", 0) > 1e-6 or DICpara.get("Smooth2DTimes", 0):
+        raise AldicError("ALDICFrameQuadtree: displacement smoothing (funSmoothDispQuadtree) is not implemented")
+    ctx = ctx or default_context()
+    fN = np.asarray(fNormalized, dtype=np.float64)
+    gN = np.asarray(gNormalized, dtype=np.float64)
+    fMask = np.asarray(fNormalizedMask, dtype=np.float64)
+    Df = funImgGradient(fN, fN, fMask, ctx=ctx)
+    DICpara, x0, y0, u, v, cc = IntegerSearchQuadtree(fN, gN, file_name, DICpara, ImgSeqNum, ctx=ctx)
+    mesh0 = MeshSetUp(x0, y0, DICpara)
+    U0 = np.array(Init(u, v, cc["max"], mesh0["x0"], mesh0["y0"], 0, ctx=ctx), dtype=np.float64)
+    C0 = mesh0["coordinatesFEM"]
+    off = np.flatnonzero(fMask[np.floor(C0[:, 0] + 0.5).astype(np.int64) - 1,
+                               np.floor(C0[:, 1] + 0.5).astype(np.int64) - 1] < 1)
+    U0[2 * off] = np.nan
+    U0[2 * off + 1] = np.nan
+    mesh0["elementMinSize"] = DICpara["winsizeMin"]
+    mesh, DICpara, U0 = GenerateQuadtreeMesh(U0, Df, fMask, mesh0, DICpara)
+    C = mesh["coordinatesFEM"]
+    # section 4: the local step and its fills
+    U1, F1, _, _, _, _, hole = LocalICGNQuadtree(U0, C, Df, fN, gN, DICpara, "GaussNewton", 1e-2, shapeFuncOrder,
+                                                 ctx=ctx)
+    U1 = U1.reshape(-1, 2)
+    if np.isnan(U1[:, 0]).any() and (~np.isnan(U1[:, 0])).sum() > 10:
+        U1 = _fill.fill_nans_natural(C, U1, "none")
+    F1 = F1.reshape(-1, 4)
+    if np.isnan(F1[:, 0]).any() and (~np.isnan(F1[:, 0])).sum() > 10:
+        F1 = _fill.fill_nans_natural(C, F1, "none")
+    U1, F1 = U1.ravel(), F1.ravel()
+    # section 5: the global step
+    mu, alpha, order = 1e-3, 0.0, 2
+    step = float(np.mean(np.ravel(DICpara["winstepsize"])))
+    betaList = [c * step ** 2 * mu for c in (1e-3, 1e-2, 1e-1)]
+    hdof = np.concatenate([2 * np.asarray(hole, dtype=np.int64), 2 * np.asarray(hole, dtype=np.int64) + 1])
+    U2 = None
+    if ImgSeqNum == 2:
+        errs = []
+        for bt in betaList:
+            U2 = Subpb2Quadtree(mesh, order, bt, mu, U1, F1, None, None, alpha, step, 0, ctx=ctx)
+            errs.append(np.linalg.norm(U1 - U2))
+        beta = subpb2_beta(betaList, errs)
+    else:
+        beta = DICpara.get("beta", 1e-3 * step ** 2 * mu)
+    if U2 is None or abs(beta - betaList[-1]) > np.finfo(float).eps:
+        U2 = Subpb2Quadtree(mesh, order, beta, mu, U1, F1, None, None, alpha, step, 0, ctx=ctx)
+    U2 = np.array(U2)
+    U2[hdof] = U1[hdof]
+    F2 = F1
+    vdual = U2 - U1
+    # section 6: two ADMM rounds
+    para = dict(DICpara, winsize_List=np.full((C.shape[0], 2), int(np.ravel(DICpara["winsize"])[0]), np.int32))
+    for ALSolveStep in (2, 3):
+        U1, _, _, _, _ = Subpb1Quadtree(U2, F2, np.zeros(4 * C.shape[0]), vdual, C, Df, fN, gN, mu, beta, None,
+                                        ALSolveStep, para, "GaussNewton", 1e-2, ctx=ctx)
+        U2 = np.array(Subpb2Quadtree(mesh, order, beta, mu, U1, F1, None, None, alpha, step, 0, ctx=ctx))
+        U2[hdof] = U1[hdof]
+        vdual = U2 - U1
+    return {"DICmesh": mesh, "U": U2, "USubpb1": U1, "FSubpb1": F1, "beta": beta, "markCoordHoleStrain": hole,
+            "DICpara": DICpara}
 
 
 def funRemoveOutliers(u, v, cc, qDICOrNot, Thr0, ctx: Context | None = None):

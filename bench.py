@@ -631,21 +631,10 @@ def main():
 # the 2D temporal (512^2) and quadtree ALDIC (2048^2, hole + notch, Subpb1) workloads
 # ----------------------------------------------------------------------------------
 def admm_beta(betas, errs):
-    """The reference's beta for the first frame (func/TemporalMatch_quadtree_ST1.m:274-294):
-    |U1 - U2| over the three-entry beta list normalised by its mean and standard deviation,
-    the minimum's beta, or, with the minimum in the middle, the vertex of the parabola in
-    log10(beta) through the three points (MATLAB's fit(..., 'poly2') there, whose try falls
-    to the list's beta at an end)."""
-    e = np.asarray(errs, dtype=np.float64)
-    sd = e.std(ddof=1)
-    if not (np.isfinite(sd) and sd > 0):  # MATLAB's min over NaN picks the first entry
-        return betas[0]
-    z = (e - e.mean()) / sd
-    k = int(np.argmin(z))
-    if k != 1:
-        return betas[k]
-    p = np.polyfit(np.log10(betas), z, 2)
-    return 10 ** (-p[1] / 2 / p[0])
+    """The reference's beta for the first frame (aldic_b200.api.subpb2_beta)."""
+    from aldic_b200.api import subpb2_beta
+
+    return subpb2_beta(betas, errs)
 
 
 def run_aux(args, P):

@@ -45,6 +45,17 @@ class OracleContext:
     def init_u0(self, u, v, out=None, index=0):
         return O.init_u0(u, v, index)
 
+    def subpb1(self, variant, coords, UOld, FOld, vdual, mu, tol, winsize=0, winsize_list=None, HPar=None, out=None):
+        frame = O.Frame(self.img[0], self.img[1], self.mask, self.g[0], self.g[1])
+        wl = None if winsize_list is None else np.asarray(winsize_list).reshape(-1, 2)
+        return O.subpb1(frame, np.asarray(coords, dtype=np.float64), np.asarray(UOld, dtype=np.float64),
+                        np.asarray(FOld, dtype=np.float64), np.asarray(vdual, dtype=np.float64), mu, tol,
+                        winsize=winsize, winsize_list=wl, HPar=HPar, variant=variant)
+
+    def subpb2(self, coords, elements, order, beta, mu, U, F, alpha=0.0, dirichlet=None, **kw):
+        return O.subpb2_quadtree(coords, elements, order, beta, mu, U, F, alpha=alpha,
+                                 dirichlet=() if dirichlet is None else dirichlet)
+
     def local_icgn(self, variant, coords, U0, winsize, tol, **kw):
         frame = O.Frame(self.img[0], self.img[1], self.mask, self.g[0], self.g[1])
         return O.local_icgn(frame, np.asarray(coords, dtype=np.float64), np.asarray(U0, dtype=np.float64), winsize,
@@ -79,3 +90,34 @@ def test_stereo_match_driver_on_the_oracle():
     assert far.sum() > 20 and np.median(err) < 0.02
     # CalPointsNum is the search grid's shape, the uniform mesh's node count
     assert int(np.prod(info["CalPointsNum"])) == info["ResultFEMesh"]["coordinatesFEM"].shape[0]
+
+
+def test_aldic_frame_on_the_oracle():
+    """One ALDIC frame (TemporalMatch_quadtree_ST1 sections 3-6) on a masked plate, the
+    device calls restated by the oracle: every step runs, the global step's beta comes from
+    the tuning rule, and the final displacements match the plate's known field."""
+    import aldic_b200 as A
+
+    O.build()
+    sc = synth.plate_with_hole(size=256, hole_r=40.0, peak=1.5, sin_amp=0.2, sin_wl=100.0)
+    M, N = sc.ref.shape
+    para = {"winsize": 24, "winstepsize": 16, "winsizeMin": 8, "TemporalSearchDistance": 6, "ImgSize": [M, N],
+            "gridxyROIRange": {"gridx": [1, M], "gridy": [1, N]}, "ImgRefMask": sc.mask}
+    ctx = OracleContext()
+    r = A.ALDICFrameQuadtree(sc.ref.astype(float) * sc.mask, sc.deff.astype(float), sc.mask, para, 2, ctx=ctx)
+    mesh = r["DICmesh"]
+    C = mesh["coordinatesFEM"]
+    assert r["U"].shape == (2 * C.shape[0],) and mesh["elementsFEM"].shape[1] == 8
+    step = 16.0
+    betas = [c * step ** 2 * 1e-3 for c in (1e-3, 1e-2, 1e-1)]
+    assert betas[0] <= r["beta"] <= betas[2]
+    used = np.unique(mesh["elementsFEM"][mesh["elementsFEM"] > 0]) - 1
+    tu, tv = sc.disp(C[:, 0], C[:, 1])
+    ix = np.floor(C[:, 0] + 0.5).astype(int) - 1
+    iy = np.floor(C[:, 1] + 0.5).astype(int) - 1
+    inside = np.zeros(C.shape[0], bool)
+    inside[used] = True
+    inside &= (sc.mask[ix, iy] > 0) & (C[:, 0] > 24) & (C[:, 0] < M - 24) & (C[:, 1] > 24) & (C[:, 1] < N - 24)
+    err = np.hypot(r["U"][0::2] - tu, r["U"][1::2] - tv)[inside]
+    assert inside.sum() > 30 and np.isfinite(err).all() and np.median(err) < 0.05
+
