@@ -26,7 +26,7 @@ __all__ = [
     "LocalICGN", "LocalICGNQuadtree", "Subpb1", "Subpb1Quadtree", "epipolar_ICGN1",
     "stereoReconstruction_quadtree", "bad_points_local", "bad_points_subpb1", "Init", "funUndistortPoints",
     "IntegerSearchQuadtree", "MeshSetUp", "funRemoveOutliers", "Subpb2Quadtree", "GenerateQuadtreeMesh",
-    "StereoMatch_STAQ", "ALDICFrameQuadtree", "subpb2_beta",
+    "StereoMatch_STAQ", "ALDICFrameQuadtree", "subpb2_beta", "organizeMatchedPairds_quadtree_ST1",
 ]
 
 
@@ -1104,6 +1104,23 @@ def StereoMatch_STAQ(RD_L, RD_R, Normalized_L, Normalized_R, file_name_L, Normal
     RD_R["Coordinates_corr"] = StereoInfo["ResultFEMesh_corr"]
     StereoInfo["CalPointsNum"] = np.shape(u)
     return StereoInfo, RD_L, RD_R
+
+
+def organizeMatchedPairds_quadtree_ST1(RD_L, RD_R, DICpara=None):
+    """matchedPairs = organizeMatchedPairds_quadtree_ST1(RD_L, RD_R, DICpara)
+    (func_quadtree/organizeMatchedPairds_quadtree_ST1.m:8-14): per frame the n x 4 pairs
+    [xL yL xR yR], frame 1 the left mesh and its stereo match (RD_R['Coordinates_corr']),
+    frame i + 1 both moved by their temporal displacements.  RD_L / RD_R hold
+    ResultFEMeshEachFrame (a list whose first entry has coordinatesFEM), Coordinates_corr
+    (right) and ResultDisp (a list of dicts with U, n x 2 or 2n interleaved)."""
+    C = np.asarray(RD_L["ResultFEMeshEachFrame"][0]["coordinatesFEM"], dtype=np.float64)
+    Cr = np.asarray(RD_R["Coordinates_corr"], dtype=np.float64)
+    pairs = [np.concatenate([C, Cr], 1)]
+    for dl, dr in zip(RD_L.get("ResultDisp", []), RD_R.get("ResultDisp", [])):
+        ul = np.asarray(dl["U"], dtype=np.float64).reshape(-1, 2)
+        ur = np.asarray(dr["U"], dtype=np.float64).reshape(-1, 2)
+        pairs.append(np.concatenate([C + ul, Cr + ur], 1))
+    return pairs
 
 
 def _has_distortion(cameraParams, side):

@@ -109,3 +109,18 @@ def test_integer_search_quadtree_zero_initial_guess():
     assert list(p2["SizeOfFFTSearchRegion"]) == [0, 0] and p2["InitFFTSearchMethod"] == 3
     with pytest.raises(A.AldicError):
         A.IntegerSearchQuadtree(None, None, None, dict(para, InitFFTSearchMethod=2), 2)
+
+
+def test_organize_matched_pairs():
+    import aldic_b200 as A
+
+    C = np.array([[10.0, 20.0], [30.0, 40.0], [50.0, 60.0]])
+    Cr = C + [[5.0, 1.0]]
+    RD_L = {"ResultFEMeshEachFrame": [{"coordinatesFEM": C}],
+            "ResultDisp": [{"U": np.array([[1.0, 2.0]] * 3)}, {"U": np.array([1.5, 2.5] * 3)}]}
+    RD_R = {"Coordinates_corr": Cr, "ResultDisp": [{"U": np.array([[0.5, -1.0]] * 3)}, {"U": np.zeros(6)}]}
+    P = A.organizeMatchedPairds_quadtree_ST1(RD_L, RD_R, {})
+    assert len(P) == 3 and all(p.shape == (3, 4) for p in P)
+    assert np.array_equal(P[0], np.concatenate([C, Cr], 1))
+    assert np.array_equal(P[1][:, :2], C + [1.0, 2.0]) and np.array_equal(P[1][:, 2:], Cr + [0.5, -1.0])
+    assert np.array_equal(P[2][:, :2], C + [1.5, 2.5]) and np.array_equal(P[2][:, 2:], Cr)
