@@ -27,9 +27,11 @@ from __future__ import annotations
 
 import numpy as np
 
+from ._lib import AldicError
 
-class FillError(ValueError):
-    pass
+
+class FillError(AldicError):
+    """A bad argument to the natural-neighbour fill."""
 
 
 def _clip(poly, a, b):
