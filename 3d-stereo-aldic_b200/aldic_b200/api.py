@@ -27,6 +27,7 @@ __all__ = [
     "stereoReconstruction_quadtree", "bad_points_local", "bad_points_subpb1", "Init", "funUndistortPoints",
     "IntegerSearchQuadtree", "MeshSetUp", "funRemoveOutliers", "Subpb2Quadtree", "GenerateQuadtreeMesh",
     "StereoMatch_STAQ", "ALDICFrameQuadtree", "subpb2_beta", "organizeMatchedPairds_quadtree_ST1",
+    "TemporalMatch_quadtree_ST1",
 ]
 
 
@@ -563,7 +564,7 @@ def subpb2_beta(betaList, errs):
 
 
 def ALDICFrameQuadtree(fNormalized, gNormalized, fNormalizedMask, DICpara, ImgSeqNum=2, file_name=None,
-                       shapeFuncOrder=1, ctx: Context | None = None):
+                       shapeFuncOrder=1, ctx: Context | None = None, seed=None):
     """One frame of func/TemporalMatch_quadtree_ST1.m (:41-390, sections 3 to 6) in its
     default form (accumulative, whole-field search initial guess, UseGlobal): gradients of
     the reference frame; IntegerSearchQuadtree (search and bad-point removal), MeshSetUp, Init
@@ -573,9 +574,12 @@ def ALDICFrameQuadtree(fNormalized, gNormalized, fNormalizedMask, DICpara, ImgSe
     step with mu = 1e-3, alpha = 0, Gauss order 2, beta tuned over [1e-3 1e-2 1e-1]
     mean(winstepsize)^2 mu at frame 2 (DICpara['beta'] or the list's first entry later,
     :266-306), the hole-strain nodes held at the local result, the duals (:313-323); two ADMM
-    rounds of Subpb1Quadtree + Subpb2Quadtree (:333-389).  Returns a dict: DICmesh, U
-    (USubpb2), USubpb1, FSubpb1, beta, markCoordHoleStrain, DICpara.  The displacement
-    smoothing options (DispSmoothness, Smooth2DTimes) are not implemented and must be 0."""
+    rounds of Subpb1Quadtree + Subpb2Quadtree (:333-389).  seed = (coords, U n x 2) replaces
+    the search by the natural-neighbour interpolation of an earlier result onto the search
+    grid ('natural', 'none', NaN -> 0, cc.max = 1; the 'reuseLast' initial guess, :112-128).
+    Returns a dict: DICmesh, DICmesh_nonQuadtree, U (USubpb2), USubpb1, FSubpb1, beta,
+    markCoordHoleStrain, DICpara.  The displacement smoothing options (DispSmoothness,
+    Smooth2DTimes) are not implemented and must be 0."""
     if DICpara.get("DispSmoothness", 0) > 1e-6 or DICpara.get("Smooth2DTimes", 0):
         raise AldicError("ALDICFrameQuadtree: displacement smoothing (funSmoothDispQuadtree) is not implemented")
     ctx = ctx or default_context()
@@ -583,7 +587,23 @@ def ALDICFrameQuadtree(fNormalized, gNormalized, fNormalizedMask, DICpara, ImgSe
     gN = np.asarray(gNormalized, dtype=np.float64)
     fMask = np.asarray(fNormalizedMask, dtype=np.float64)
     Df = funImgGradient(fN, fN, fMask, ctx=ctx)
-    DICpara, x0, y0, u, v, cc = IntegerSearchQuadtree(fN, gN, file_name, DICpara, ImgSeqNum, ctx=ctx)
+    if seed is None:
+        DICpara, x0, y0, u, v, cc = IntegerSearchQuadtree(fN, gN, file_name, DICpara, ImgSeqNum, ctx=ctx)
+    else:  # the grid of funIntegerSearch (XList / YList, :114-118) from the earlier result
+        w = int(np.ravel(DICpara["winsize"])[0])
+        st = int(np.ravel(DICpara["winstepsize"])[0])
+        roi = DICpara["gridxyROIRange"]
+        xl = np.arange(roi["gridx"][0], roi["gridx"][1] - w - st + 1, st, dtype=np.float64)
+        yl = np.arange(roi["gridy"][0], roi["gridy"][1] - w - st + 1, st, dtype=np.float64)
+        X, Y = np.meshgrid(xl, yl, indexing="ij")
+        pc, pu = np.asarray(seed[0], dtype=np.float64), np.asarray(seed[1], dtype=np.float64).reshape(-1, 2)
+        ok = ~np.isnan(pu[:, 0])
+        nn = _fill.NaturalNeighbor(pc[ok], "none")
+        uv = nn(np.stack([X.ravel(), Y.ravel()], 1), pu[ok])
+        uv[np.isnan(uv)] = 0.0
+        x0, y0 = X.T, Y.T  # nY x nX, as funIntegerSearch returns them
+        u, v = uv[:, 0].reshape(X.shape).T, uv[:, 1].reshape(X.shape).T
+        cc = {"max": np.ones(u.shape)}
     mesh0 = MeshSetUp(x0, y0, DICpara)
     U0 = np.array(Init(u, v, cc["max"], mesh0["x0"], mesh0["y0"], 0, ctx=ctx), dtype=np.float64)
     C0 = mesh0["coordinatesFEM"]
@@ -632,8 +652,65 @@ def ALDICFrameQuadtree(fNormalized, gNormalized, fNormalizedMask, DICpara, ImgSe
         U2 = np.array(Subpb2Quadtree(mesh, order, beta, mu, U1, F1, None, None, alpha, step, 0, ctx=ctx))
         U2[hdof] = U1[hdof]
         vdual = U2 - U1
-    return {"DICmesh": mesh, "U": U2, "USubpb1": U1, "FSubpb1": F1, "beta": beta, "markCoordHoleStrain": hole,
-            "DICpara": DICpara}
+    return {"DICmesh": mesh, "DICmesh_nonQuadtree": mesh0, "U": U2, "USubpb1": U1, "FSubpb1": F1, "beta": beta,
+            "markCoordHoleStrain": hole, "DICpara": DICpara}
+
+
+def TemporalMatch_quadtree_ST1(DICpara, file_name, ImgMask, ImgNormalized, RD=None, StereoInfo=None,
+                               camera0OrNot="camera0", shapeFuncOrder=1, ctx: Context | None = None):
+    """[RD] = TemporalMatch_quadtree_ST1(DICpara, file_name, ImgMask, ImgNormalized, RD,
+    StereoInfo, camera0OrNot, shapeFuncOrder) (func/TemporalMatch_quadtree_ST1.m) in the
+    accumulative mode (DICIncOrNot 0) with the global step: every frame k >= 2 is matched
+    against frame 1 (masked by ImgMask[0]; the deformed frame unmasked, :43-53) by
+    ALDICFrameQuadtree; for 'notCamera0' the search ROI is the mask's bounding box
+    (localizeDICparaForFrame, :513-531) and the field is carried to RD['Coordinates_corr'] by
+    natural-neighbour interpolation over the first frame's mesh ('natural', 'none',
+    :409-426).  DICpara['TemporalInitGuess'] = 'reuseLast' seeds frames 3+ from the previous
+    result when more than half of it is valid (:62-81).  RD gains ResultFEMesh and
+    ResultFEMeshEachFrame (first frame), ResultDisp_acc (2n per frame), ResultDisp (n x 2
+    per frame) and, for 'notCamera0', ResultDisp_corr.  The incremental mode raises."""
+    if DICpara.get("DICIncOrNot", 0) != 0:
+        raise AldicError("TemporalMatch_quadtree_ST1: only the accumulative mode (DICIncOrNot 0) is implemented")
+    if camera0OrNot not in ("camera0", "notCamera0"):
+        raise AldicError("camera0OrNot must be 'camera0' or 'notCamera0'")
+    RD = dict(RD or {})
+    for key in ("ResultDisp_acc", "ResultDisp", "ResultDisp_corr"):
+        RD[key] = list(RD.get(key, []))
+    fMask = np.asarray(ImgMask[0], dtype=np.float64)
+    fN = np.asarray(ImgNormalized[0], dtype=np.float64) * fMask
+    para = dict(DICpara, ImgRefMask=fMask)
+    if camera0OrNot == "notCamera0":
+        rows, cols = np.nonzero(fMask)
+        para["gridxyROIRange"] = {"gridx": [int(rows.min()) + 1, int(rows.max()) + 1],
+                                  "gridy": [int(cols.min()) + 1, int(cols.max()) + 1]}
+    for k in range(2, len(ImgNormalized) + 1):
+        seed = None
+        if para.get("TemporalInitGuess") == "reuseLast" and k >= 3:
+            prev = np.asarray(RD["ResultDisp"][k - 3]["U"], dtype=np.float64).reshape(-1, 2)
+            pc = np.asarray(RD["ResultFEMeshEachFrame"][0]["coordinatesFEM"], dtype=np.float64)
+            if prev.shape[0] == pc.shape[0] and 1 - np.isnan(prev[:, 0]).mean() > 0.5:
+                seed = (pc, prev)
+        r = ALDICFrameQuadtree(fN, np.asarray(ImgNormalized[k - 1], dtype=np.float64), fMask, para, k, file_name,
+                               shapeFuncOrder, ctx=ctx, seed=seed)
+        para = dict(r["DICpara"], ImgRefMask=fMask, gridxyROIRange=para["gridxyROIRange"])
+        if k == 2:
+            m0, mq = r["DICmesh_nonQuadtree"], r["DICmesh"]
+            RD["ResultFEMesh"] = [{"coordinatesFEM": m0["coordinatesFEM"], "elementsFEM": m0["elementsFEM"],
+                                   "winsize": para["winsize"], "winstepsize": para["winstepsize"],
+                                   "gridxyROIRange": para["gridxyROIRange"]}]
+            RD["ResultFEMeshEachFrame"] = [{"coordinatesFEM": mq["coordinatesFEM"], "elementsFEM": mq["elementsFEM"]}]
+        U = np.asarray(r["U"], dtype=np.float64)
+        RD["ResultDisp_acc"].append({"U": U})
+        if camera0OrNot == "camera0":
+            RD["ResultDisp"].append({"U": U.reshape(-1, 2)})
+        else:
+            src = np.asarray(RD["ResultFEMeshEachFrame"][0]["coordinatesFEM"], dtype=np.float64)
+            Uq = U.reshape(-1, 2)
+            ok = ~np.isnan(Uq[:, 0])
+            nn = _fill.NaturalNeighbor(src[ok], "none")
+            RD["ResultDisp"].append({"U": nn(np.asarray(RD["Coordinates_corr"], dtype=np.float64), Uq[ok])})
+            RD["ResultDisp_corr"].append({"U": Uq})
+    return RD
 
 
 def funRemoveOutliers(u, v, cc, qDICOrNot, Thr0, ctx: Context | None = None):

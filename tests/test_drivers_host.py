@@ -121,3 +121,43 @@ def test_aldic_frame_on_the_oracle():
     err = np.hypot(r["U"][0::2] - tu, r["U"][1::2] - tv)[inside]
     assert inside.sum() > 30 and np.isfinite(err).all() and np.median(err) < 0.05
 
+
+
+def test_temporal_match_driver_on_the_oracle():
+    """TemporalMatch_quadtree_ST1 (accumulative) over three frames with one reference
+    speckle pattern, both camera forms and the 'reuseLast' seed: the device calls restated
+    by the oracle, the fields recovered at the first frame's mesh (camera0) and at given
+    matched points (notCamera0)."""
+    import aldic_b200 as A
+
+    O.build()
+    M = N = 176
+    frames = [synth.temporal_affine(seed=5, M=M, N=N, n_speckles=1100, u=u, v=v, dudx=0.001, dvdy=-0.001)
+              for u, v in ((1.6, -0.8), (2.9, -1.7))]
+    imgs = [frames[0].ref.astype(float)] + [f.deff.astype(float) for f in frames]
+    mask = np.ones((M, N))
+    X, Y = np.meshgrid(np.arange(1, M + 1), np.arange(1, N + 1), indexing="ij")
+    mask[(X - 90) ** 2 + (Y - 84) ** 2 < 22 ** 2] = 0
+    para = {"winsize": 20, "winstepsize": 16, "winsizeMin": 8, "TemporalSearchDistance": 6, "ImgSize": [M, N],
+            "gridxyROIRange": {"gridx": [1, M], "gridy": [1, N]}, "TemporalInitGuess": "reuseLast"}
+    ctx = OracleContext()
+    RD = A.TemporalMatch_quadtree_ST1(para, None, [mask] * 3, imgs, {}, None, "camera0", 1, ctx=ctx)
+    C = RD["ResultFEMeshEachFrame"][0]["coordinatesFEM"]
+    assert len(RD["ResultDisp"]) == 2 and RD["ResultDisp"][1]["U"].shape == (C.shape[0], 2)
+    ix = np.floor(C[:, 0] + 0.5).astype(int) - 1
+    iy = np.floor(C[:, 1] + 0.5).astype(int) - 1
+    good = (mask[ix, iy] > 0) & (np.hypot(C[:, 0] - 90, C[:, 1] - 84) > 36) & (C[:, 0] > 20) & (C[:, 0] < M - 20) \
+        & (C[:, 1] > 20) & (C[:, 1] < N - 20)
+    for k, f in enumerate(frames):
+        tu, tv = f.disp(C[:, 0], C[:, 1])
+        U = RD["ResultDisp"][k]["U"]
+        assert np.median(np.hypot(U[good, 0] - tu[good], U[good, 1] - tv[good])) < 0.03, k
+    # the second camera's form: the field carried to matched points inside the mesh
+    inner = good & (C[:, 0] < C[:, 0].max() - 1) & (C[:, 1] < C[:, 1].max() - 1)
+    pts = C[inner][:20] + [0.5, 0.25]  # inside the mesh's hull
+    RDr = A.TemporalMatch_quadtree_ST1(para, None, [mask] * 3, imgs, {"Coordinates_corr": pts}, None, "notCamera0", 1,
+                                       ctx=ctx)
+    Ur = RDr["ResultDisp"][1]["U"]
+    tu, tv = frames[1].disp(pts[:, 0], pts[:, 1])
+    assert Ur.shape == (20, 2) and np.median(np.hypot(Ur[:, 0] - tu, Ur[:, 1] - tv)) < 0.03
+    assert len(RDr["ResultDisp_corr"]) == 2
