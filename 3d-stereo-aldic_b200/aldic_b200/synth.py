@@ -155,8 +155,8 @@ class StereoScene:
     Z: float
 
     def plane_point_left(self, x, y, frame=0):
-        """World point (left-camera frame, mm) seen at left pixel (x, y) (1-based image x/y)
-        on the plane of `frame`."""
+        """World point (mm; to_left_camera_frame gives the left camera's coordinates) seen at
+        left pixel (x, y) (1-based image x/y) on the plane of `frame`."""
         return _ray_plane(self.camL, np.asarray(x, float), np.asarray(y, float), self.Z,
                           None if frame == 0 else (self.plane_R, self.plane_t))
 
@@ -236,7 +236,8 @@ def stereo_pair(seed=1, size=2048, f=4000.0, baseline=300.0, Z=1000.0, yaw_deg=N
 
 def stereo_truth(scene: StereoScene, coords_left, frame=0):
     """True matches of left pixels `coords_left` (n x 2, 1-based x/y): the right-image
-    point of frame 0, the left/right points of `frame`, and the 3D point (left camera frame)."""
+    point of frame 0, the left/right points of `frame`, and the 3D points xyz0 / xyz1 in world
+    coordinates (to_left_camera_frame gives the left camera's, those of the triangulation)."""
     x = coords_left[:, 0]
     y = coords_left[:, 1]
     W0 = _ray_plane(scene.camL, x, y, scene.Z)

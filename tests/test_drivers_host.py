@@ -56,6 +56,9 @@ class OracleContext:
         return O.subpb2_quadtree(coords, elements, order, beta, mu, U, F, alpha=alpha,
                                  dirichlet=() if dirichlet is None else dirichlet)
 
+    def triangulate(self, pairs, KL, KR, R, T, out=None):
+        return O.triangulate(pairs, KL, KR, R, T)
+
     def local_icgn(self, variant, coords, U0, winsize, tol, **kw):
         frame = O.Frame(self.img[0], self.img[1], self.mask, self.g[0], self.g[1])
         return O.local_icgn(frame, np.asarray(coords, dtype=np.float64), np.asarray(U0, dtype=np.float64), winsize,
@@ -161,3 +164,51 @@ def test_temporal_match_driver_on_the_oracle():
     tu, tv = frames[1].disp(pts[:, 0], pts[:, 1])
     assert Ur.shape == (20, 2) and np.median(np.hypot(Ur[:, 0] - tu, Ur[:, 1] - tv)) < 0.03
     assert len(RDr["ResultDisp_corr"]) == 2
+
+
+def test_stereo_pipeline_end_to_end_on_the_oracle():
+    """The reference's stereo sequence, driver by driver: StereoMatch_STAQ on the first pair,
+    TemporalMatch_quadtree_ST1 for the left camera and for the right one (its field at the
+    stereo-matched points), organizeMatchedPairds_quadtree_ST1 and
+    stereoReconstruction_quadtree; the plane's rigid 3-D motion comes back."""
+    import aldic_b200 as A
+
+    O.build()
+    sc = synth.stereo_pair(seed=2, size=224, f=500.0, plane_half=320.0, motion_t=(1.0, -0.6, 3.0),
+                           motion_rot=2e-3)
+    L = [im.astype(float) for im in sc.L]
+    R = [im.astype(float) for im in sc.R]
+    M, N = L[0].shape
+    ones = np.ones((M, N))
+    para = {"winsize": 20, "winstepsize": 16, "winsizeMin": 8, "StereoSearchDistance": 14,
+            "TemporalSearchDistance": 6, "ImgSize": [M, N], "gridxyROIRange": {"gridx": [1, M], "gridy": [1, N]},
+            "ImgRefMask": ones}
+    ctx = OracleContext()
+    info, RD_L, RD_R = A.StereoMatch_STAQ({}, {}, L[0], R[0], None, ones, ones, para, {}, 1, ctx=ctx)
+    RD_L = A.TemporalMatch_quadtree_ST1(para, None, [ones, ones], L, RD_L, info, "camera0", 1, ctx=ctx)
+    RD_R = A.TemporalMatch_quadtree_ST1(para, None, [ones, ones], R, RD_R, info, "notCamera0", 1, ctx=ctx)
+    assert np.array_equal(RD_L["ResultFEMeshEachFrame"][0]["coordinatesFEM"],
+                          info["ResultFEMeshEachFrame"]["coordinatesFEM"])  # one mesh for both drivers
+    pairs = A.organizeMatchedPairds_quadtree_ST1(RD_L, RD_R, para)
+    cam = {"KL": sc.KL, "KR": sc.KR, "R": sc.R_rl, "T": sc.T_rl}
+    final, errs = A.stereoReconstruction_quadtree(pairs, cam, ctx=ctx)
+    C = RD_L["ResultFEMeshEachFrame"][0]["coordinatesFEM"]
+    t = synth.stereo_truth(sc, C, 1)
+    inner = (C[:, 0] > 30) & (C[:, 0] < M - 30) & (C[:, 1] > 30) & (C[:, 1] < N - 30)
+
+    def med(e):
+        return float(np.nanmedian(np.linalg.norm(e, axis=1)[inner]))
+
+    # each stage in pixels: the stereo match, the left and the right temporal fields
+    Cr = RD_R["Coordinates_corr"]
+    assert med(Cr - t["right0"]) < 0.06
+    assert med(C + RD_L["ResultDisp"][0]["U"] - t["left1"]) < 0.06
+    assert med(Cr + RD_R["ResultDisp"][0]["U"] - t["right1"]) < 0.06
+    # in 3-D, left camera frame (P_L = K [I | 0]): ~6.7 mm of depth per pixel of disparity here
+    X0 = synth.to_left_camera_frame(sc, t["xyz0"])
+    X1 = synth.to_left_camera_frame(sc, t["xyz1"])
+    ok = inner & np.isfinite(final["Displacement"][1]).all(1)
+    assert ok.sum() > 20
+    assert np.median(np.linalg.norm(final["Coordinates"][0][ok] - X0[ok], axis=1)) < 1.0      # mm at ~1 m
+    d = np.linalg.norm(final["Displacement"][1][ok] - (X1 - X0)[ok], axis=1)
+    assert np.median(d) < 0.25                                                                 # mm of ~3.2 mm
