@@ -212,3 +212,32 @@ def test_stereo_pipeline_end_to_end_on_the_oracle():
     assert np.median(np.linalg.norm(final["Coordinates"][0][ok] - X0[ok], axis=1)) < 1.0      # mm at ~1 m
     d = np.linalg.norm(final["Displacement"][1][ok] - (X1 - X0)[ok], axis=1)
     assert np.median(d) < 0.25                                                                 # mm of ~3.2 mm
+
+
+def test_local_icgn_uniform_driver_fills_u_and_f():
+    """LocalICGN (uniform mesh) as the reference returns it: bad points (here subsets whose
+    window leaves the image) filled in U and in F from the good ones."""
+    import aldic_b200 as A
+
+    O.build()
+    sc = synth.temporal_affine(seed=7, M=160, N=160, n_speckles=900, u=2.2, v=-1.1)
+    M, N = sc.ref.shape
+    ctx = OracleContext()
+    Df = A.funImgGradient(sc.ref.astype(float), ctx=ctx)
+    xs = np.arange(8.0, 156.0, 12.0)
+    X, Y = np.meshgrid(xs, xs, indexing="ij")
+    C = np.stack([X.ravel(), Y.ravel()], 1)
+    tu, tv = sc.disp(C[:, 0], C[:, 1])
+    U0 = np.stack([np.round(tu), np.round(tv)], 1).ravel()
+    U, F, H, t, conv, nbad = A.LocalICGN(U0, C, Df, sc.ref.astype(float), sc.deff.astype(float), {"winsize": 20},
+                                         ctx=ctx)
+    Un, Fn, *_ = A.LocalICGN(U0, C, Df, sc.ref.astype(float), sc.deff.astype(float), {"winsize": 20}, ctx=ctx,
+                             fill=False)
+    bad = np.isnan(Un[0::2])
+    # failed subsets (code -1 at the border) and, by the uniform rule, iteration-count outliers
+    assert bad.sum() >= nbad >= 5
+    assert np.isfinite(U).all() and np.isfinite(F).all()
+    assert np.array_equal(U.reshape(-1, 2)[~bad], Un.reshape(-1, 2)[~bad])
+    # the filled border values continue the affine field
+    err = np.hypot(U[0::2] - tu, U[1::2] - tv)[bad]
+    assert np.median(err) < 0.05
