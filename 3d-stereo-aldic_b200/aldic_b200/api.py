@@ -659,57 +659,90 @@ def ALDICFrameQuadtree(fNormalized, gNormalized, fNormalizedMask, DICpara, ImgSe
 def TemporalMatch_quadtree_ST1(DICpara, file_name, ImgMask, ImgNormalized, RD=None, StereoInfo=None,
                                camera0OrNot="camera0", shapeFuncOrder=1, ctx: Context | None = None):
     """[RD] = TemporalMatch_quadtree_ST1(DICpara, file_name, ImgMask, ImgNormalized, RD,
-    StereoInfo, camera0OrNot, shapeFuncOrder) (func/TemporalMatch_quadtree_ST1.m) in the
-    accumulative mode (DICIncOrNot 0) with the global step: every frame k >= 2 is matched
-    against frame 1 (masked by ImgMask[0]; the deformed frame unmasked, :43-53) by
-    ALDICFrameQuadtree; for 'notCamera0' the search ROI is the mask's bounding box
-    (localizeDICparaForFrame, :513-531) and the field is carried to RD['Coordinates_corr'] by
-    natural-neighbour interpolation over the first frame's mesh ('natural', 'none',
-    :409-426).  DICpara['TemporalInitGuess'] = 'reuseLast' seeds frames 3+ from the previous
-    result when more than half of it is valid (:62-81).  RD gains ResultFEMesh and
-    ResultFEMeshEachFrame (first frame), ResultDisp_acc (2n per frame), ResultDisp (n x 2
-    per frame) and, for 'notCamera0', ResultDisp_corr.  The incremental mode raises."""
-    if DICpara.get("DICIncOrNot", 0) != 0:
-        raise AldicError("TemporalMatch_quadtree_ST1: only the accumulative mode (DICIncOrNot 0) is implemented")
+    StereoInfo, camera0OrNot, shapeFuncOrder) (func/TemporalMatch_quadtree_ST1.m) with the
+    global step, frame by frame through ALDICFrameQuadtree.
+    * Accumulative mode (DICIncOrNot 0): frame k >= 2 against frame 1 (masked by ImgMask[0],
+      the deformed frame unmasked, :48-53); ResultDisp_acc holds USubpb2; ResultDisp the field
+      at the first frame's mesh ('camera0') or carried to RD['Coordinates_corr'] by
+      natural-neighbour interpolation ('notCamera0', 'natural', 'none', :401-426);
+      DICpara['TemporalInitGuess'] = 'reuseLast' seeds frames 3+ from the previous result when
+      more than half of it is valid (:62-81).
+    * Incremental mode (DICIncOrNot 1): frame k against frame k - 1, both masked by their own
+      masks (:43-47), a mesh per frame; ResultDisp_inc holds USubpb2, and ResultDisp
+      accumulates it at the tracked points (the first frame's mesh, or the matched points,
+      moved by the displacement so far; 'natural', 'none', :434-479).
+    For 'notCamera0' the search ROI is the reference frame mask's bounding box
+    (localizeDICparaForFrame, :513-531).  RD gains ResultFEMesh, ResultFEMeshEachFrame,
+    ResultDisp and ResultDisp_acc / ResultDisp_inc (and ResultDisp_corr for 'notCamera0' in
+    the accumulative mode)."""
+    inc = int(DICpara.get("DICIncOrNot", 0))
+    if inc not in (0, 1):
+        raise AldicError("DICIncOrNot must be 0 (accumulative) or 1 (incremental)")
     if camera0OrNot not in ("camera0", "notCamera0"):
         raise AldicError("camera0OrNot must be 'camera0' or 'notCamera0'")
     RD = dict(RD or {})
-    for key in ("ResultDisp_acc", "ResultDisp", "ResultDisp_corr"):
+    for key in ("ResultDisp_acc", "ResultDisp_inc", "ResultDisp", "ResultDisp_corr", "ResultFEMesh",
+                "ResultFEMeshEachFrame"):
         RD[key] = list(RD.get(key, []))
-    fMask = np.asarray(ImgMask[0], dtype=np.float64)
-    fN = np.asarray(ImgNormalized[0], dtype=np.float64) * fMask
-    para = dict(DICpara, ImgRefMask=fMask)
-    if camera0OrNot == "notCamera0":
-        rows, cols = np.nonzero(fMask)
-        para["gridxyROIRange"] = {"gridx": [int(rows.min()) + 1, int(rows.max()) + 1],
-                                  "gridy": [int(cols.min()) + 1, int(cols.max()) + 1]}
+
+    def localize(para, mask):
+        para = dict(para, ImgRefMask=mask)
+        if camera0OrNot == "notCamera0":
+            rows, cols = np.nonzero(mask)
+            para["gridxyROIRange"] = {"gridx": [int(rows.min()) + 1, int(rows.max()) + 1],
+                                      "gridy": [int(cols.min()) + 1, int(cols.max()) + 1]}
+        return para
+
+    def carry(src, Uq, pts):
+        ok = ~np.isnan(Uq[:, 0])
+        return _fill.NaturalNeighbor(src[ok], "none")(np.asarray(pts, dtype=np.float64), Uq[ok])
+
+    para = dict(DICpara)
     for k in range(2, len(ImgNormalized) + 1):
+        if inc:
+            fMask = np.asarray(ImgMask[k - 2], dtype=np.float64)
+            gMask = np.asarray(ImgMask[k - 1], dtype=np.float64)
+            fN = np.asarray(ImgNormalized[k - 2], dtype=np.float64) * fMask
+            gN = np.asarray(ImgNormalized[k - 1], dtype=np.float64) * gMask
+        else:
+            fMask = np.asarray(ImgMask[0], dtype=np.float64)
+            fN = np.asarray(ImgNormalized[0], dtype=np.float64) * fMask
+            gN = np.asarray(ImgNormalized[k - 1], dtype=np.float64)
+        para = localize(para, fMask)
         seed = None
-        if para.get("TemporalInitGuess") == "reuseLast" and k >= 3:
+        if not inc and para.get("TemporalInitGuess") == "reuseLast" and k >= 3:
             prev = np.asarray(RD["ResultDisp"][k - 3]["U"], dtype=np.float64).reshape(-1, 2)
             pc = np.asarray(RD["ResultFEMeshEachFrame"][0]["coordinatesFEM"], dtype=np.float64)
             if prev.shape[0] == pc.shape[0] and 1 - np.isnan(prev[:, 0]).mean() > 0.5:
                 seed = (pc, prev)
-        r = ALDICFrameQuadtree(fN, np.asarray(ImgNormalized[k - 1], dtype=np.float64), fMask, para, k, file_name,
-                               shapeFuncOrder, ctx=ctx, seed=seed)
-        para = dict(r["DICpara"], ImgRefMask=fMask, gridxyROIRange=para["gridxyROIRange"])
-        if k == 2:
+        r = ALDICFrameQuadtree(fN, gN, fMask, para, k, file_name, shapeFuncOrder, ctx=ctx, seed=seed)
+        para = dict(r["DICpara"], gridxyROIRange=para["gridxyROIRange"])
+        if k == 2 or inc:
             m0, mq = r["DICmesh_nonQuadtree"], r["DICmesh"]
-            RD["ResultFEMesh"] = [{"coordinatesFEM": m0["coordinatesFEM"], "elementsFEM": m0["elementsFEM"],
-                                   "winsize": para["winsize"], "winstepsize": para["winstepsize"],
-                                   "gridxyROIRange": para["gridxyROIRange"]}]
-            RD["ResultFEMeshEachFrame"] = [{"coordinatesFEM": mq["coordinatesFEM"], "elementsFEM": mq["elementsFEM"]}]
+            RD["ResultFEMesh"].append({"coordinatesFEM": m0["coordinatesFEM"], "elementsFEM": m0["elementsFEM"],
+                                       "winsize": para["winsize"], "winstepsize": para["winstepsize"],
+                                       "gridxyROIRange": para["gridxyROIRange"]})
+            RD["ResultFEMeshEachFrame"].append({"coordinatesFEM": mq["coordinatesFEM"],
+                                                "elementsFEM": mq["elementsFEM"]})
         U = np.asarray(r["U"], dtype=np.float64)
-        RD["ResultDisp_acc"].append({"U": U})
-        if camera0OrNot == "camera0":
-            RD["ResultDisp"].append({"U": U.reshape(-1, 2)})
+        Uq = U.reshape(-1, 2)
+        first = np.asarray(RD["ResultFEMeshEachFrame"][0]["coordinatesFEM"], dtype=np.float64)
+        if not inc:
+            RD["ResultDisp_acc"].append({"U": U})
+            if camera0OrNot == "camera0":
+                RD["ResultDisp"].append({"U": Uq})
+            else:
+                RD["ResultDisp"].append({"U": carry(first, Uq, RD["Coordinates_corr"])})
+                RD["ResultDisp_corr"].append({"U": Uq})
+            continue
+        RD["ResultDisp_inc"].append({"U": U})
+        src = np.asarray(RD["ResultFEMeshEachFrame"][k - 2]["coordinatesFEM"], dtype=np.float64)
+        base = first if camera0OrNot == "camera0" else np.asarray(RD["Coordinates_corr"], dtype=np.float64)
+        if k == 2:
+            RD["ResultDisp"].append({"U": Uq if camera0OrNot == "camera0" else carry(src, Uq, base)})
         else:
-            src = np.asarray(RD["ResultFEMeshEachFrame"][0]["coordinatesFEM"], dtype=np.float64)
-            Uq = U.reshape(-1, 2)
-            ok = ~np.isnan(Uq[:, 0])
-            nn = _fill.NaturalNeighbor(src[ok], "none")
-            RD["ResultDisp"].append({"U": nn(np.asarray(RD["Coordinates_corr"], dtype=np.float64), Uq[ok])})
-            RD["ResultDisp_corr"].append({"U": Uq})
+            prev = np.asarray(RD["ResultDisp"][k - 3]["U"], dtype=np.float64)
+            RD["ResultDisp"].append({"U": prev + carry(src, Uq, base + prev)})
     return RD
 
 

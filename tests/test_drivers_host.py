@@ -241,3 +241,27 @@ def test_local_icgn_uniform_driver_fills_u_and_f():
     # the filled border values continue the affine field
     err = np.hypot(U[0::2] - tu, U[1::2] - tv)[bad]
     assert np.median(err) < 0.05
+
+
+def test_temporal_match_incremental_mode_accumulates():
+    """The incremental mode: each frame against the previous one, the increments carried to
+    the tracked points and summed; frame 3's accumulated field is the total displacement."""
+    import aldic_b200 as A
+
+    O.build()
+    M = N = 176
+    frames = [synth.temporal_affine(seed=5, M=M, N=N, n_speckles=1100, u=u, v=v, dudx=0.001, dvdy=-0.001)
+              for u, v in ((1.6, -0.8), (2.9, -1.7))]
+    imgs = [frames[0].ref.astype(float)] + [f.deff.astype(float) for f in frames]
+    ones = np.ones((M, N))
+    para = {"winsize": 20, "winstepsize": 16, "winsizeMin": 8, "TemporalSearchDistance": 6, "ImgSize": [M, N],
+            "gridxyROIRange": {"gridx": [1, M], "gridy": [1, N]}, "DICIncOrNot": 1}
+    RD = A.TemporalMatch_quadtree_ST1(para, None, [ones] * 3, imgs, {}, None, "camera0", 1, ctx=OracleContext())
+    assert len(RD["ResultDisp_inc"]) == 2 and len(RD["ResultFEMeshEachFrame"]) == 2
+    C = RD["ResultFEMeshEachFrame"][0]["coordinatesFEM"]
+    inner = (C[:, 0] > 24) & (C[:, 0] < M - 40) & (C[:, 1] > 24) & (C[:, 1] < N - 40)
+    for k, f in enumerate(frames):
+        tu, tv = f.disp(C[:, 0], C[:, 1])
+        U = RD["ResultDisp"][k]["U"]
+        e = np.hypot(U[:, 0] - tu, U[:, 1] - tv)[inner]
+        assert np.isfinite(e).sum() > 20 and np.nanmedian(e) < 0.05, k
