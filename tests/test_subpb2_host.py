@@ -129,7 +129,7 @@ def _run(exe, tmp_path, C, E, order, beta, mu, alpha, U, F, dirichlet=(), tol=1e
     return Ke, be, x, int(it), int(ok), kind
 
 
-@pytest.mark.parametrize("order", [2, 3])
+@pytest.mark.parametrize("order", [2, 3, 4, 5])
 def test_element_rows_match_the_oracle(harness, tmp_path, order):
     C, E = quadtree_mesh(4, {(1, 1), (2, 1), (0, 3)})
     n = C.shape[0]
