@@ -1142,9 +1142,11 @@ def Subpb1Quadtree(UOld, FOld, udual, vdual, coordinatesFEM, Df, ImgRef, ImgDef,
 
 
 def Subpb1(UOld, FOld, udual, vdual, coordinatesFEM, Df, ImgRef, ImgDef, mu, beta, HPar, ALSolveStep, DICpara,
-           ICGNmethod="GaussNewton", tol=1e-2, ctx: Context | None = None):
+           ICGNmethod="GaussNewton", tol=1e-2, ctx: Context | None = None, fill=True):
     """Uniform-mesh Subpb1 (func/Subpb1.m with func/funICGN_Subpb1.m); HPar is the n x 21
-    Hessian array of LocalICGN (zeros at ALSolveStep 1, as the reference passes)."""
+    Hessian array of LocalICGN (zeros at ALSolveStep 1, as the reference passes).  The bad
+    points are marked NaN (:166-183) and, as the reference ends (:186-199), every node takes
+    the gridfit 'springs' surface of the good ones (fill=False returns the marked field)."""
     ctx = ctx or default_context()
     _load_frame(ctx, Df, ImgRef, ImgDef, None)
     n = np.asarray(coordinatesFEM).shape[0]
@@ -1157,6 +1159,13 @@ def Subpb1(UOld, FOld, udual, vdual, coordinatesFEM, Df, ImgRef, ImgDef, mu, bet
     bad, num = bad_points_subpb1(conv)
     U[2 * bad] = np.nan
     U[2 * bad + 1] = np.nan
+    if fill:
+        crd = np.asarray(coordinatesFEM, dtype=np.float64)
+        xn, yn = np.unique(crd[:, 0]), np.unique(crd[:, 1])
+        ii, jj = np.searchsorted(xn, crd[:, 0]), np.searchsorted(yn, crd[:, 1])
+        for comp in (0, 1):
+            zg = _fill.gridfit_springs(crd[:, 0], crd[:, 1], U[comp::2], xn, yn)
+            U[comp::2] = zg[jj, ii]
     return U, HPar, t, conv, num
 
 

@@ -320,3 +320,70 @@ def fill_quadtree(U, coords, mask):
             U2[qry] = nn(coords[qry], U2[src])
         U2 = fill_nans_natural(coords, U2, "nearest")
     return U2.ravel()
+
+
+def gridfit_springs(x, y, z, xnodes, ynodes, smoothness=1.0):
+    """zgrid = gridfit(x, y, z, xnodes, ynodes, 'regularizer', 'springs') (func/gridfit.m,
+    D'Errico's surface fit, vendored with the reference), the form func/Subpb1.m:189-190 calls:
+    data points with a NaN dropped; each point's value tied to the grid by the 'triangle'
+    interpolation of its cell (the diagonal from the cell's lower-left to its upper-right
+    node); zero-rest-length springs between every node and its right, upper and two diagonal
+    neighbours, stiffness 1 / (spacing / mean spacing) (autoscale); the spring rows scaled by
+    smoothness * norm(A, 1) / norm(Areg, 1) under the data rows, and the stacked system
+    solved in the least-squares sense (MATLAB's backslash; here its normal equations, which
+    have the same solution for this full-rank system).  Returns zgrid (len(ynodes) x
+    len(xnodes)), zgrid[j, i] at (xnodes[i], ynodes[j]).  The data must lie inside the node
+    range (the reference's 'extend' case is not taken)."""
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spla
+
+    x, y, z = (np.asarray(a, dtype=np.float64).ravel() for a in (x, y, z))
+    keep = ~(np.isnan(x) | np.isnan(y) | np.isnan(z))
+    x, y, z = x[keep], y[keep], z[keep]
+    xn = np.asarray(xnodes, dtype=np.float64).ravel()
+    yn = np.asarray(ynodes, dtype=np.float64).ravel()
+    if x.min() < xn[0] or x.max() > xn[-1] or y.min() < yn[0] or y.max() > yn[-1]:
+        raise FillError("gridfit: data outside the node range")
+    nx, ny, n = xn.size, yn.size, x.size
+    dx, dy = np.diff(xn), np.diff(yn)
+    xscale, yscale = dx.mean(), dy.mean()
+    # histc bins (0-based here), the last node folded into the last cell
+    ix = np.clip(np.searchsorted(xn, x, side="right") - 1, 0, nx - 2)
+    iy = np.clip(np.searchsorted(yn, y, side="right") - 1, 0, ny - 2)
+    ind = iy + ny * ix  # column-major node index of the cell's lower-left node
+    tx = np.clip((x - xn[ix]) / dx[ix], 0, 1)
+    ty = np.clip((y - yn[iy]) / dy[iy], 0, 1)
+    above = tx > ty
+    L = np.where(above, ny, 1)
+    t1, t2 = np.minimum(tx, ty), np.maximum(tx, ty)
+    rows = np.repeat(np.arange(n), 3)
+    cols = np.stack([ind, ind + ny + 1, ind + L], 1).ravel()
+    vals = np.stack([1 - t2, t1, t2 - t1], 1).ravel()
+    A = sp.csr_matrix((vals, (rows, cols)), shape=(n, nx * ny))
+    blocks = []
+    i, j = np.meshgrid(np.arange(nx), np.arange(ny - 1))          # springs along y
+    k = (j + ny * i).ravel()
+    st = 1.0 / (dy[j.ravel()] / yscale)
+    blocks.append((k, k + 1, st))
+    i, j = np.meshgrid(np.arange(nx - 1), np.arange(ny))          # along x
+    k = (j + ny * i).ravel()
+    st = 1.0 / (dx[i.ravel()] / xscale)
+    blocks.append((k, k + ny, st))
+    i, j = np.meshgrid(np.arange(nx - 1), np.arange(ny - 1))      # the two diagonals
+    k = (j + ny * i).ravel()
+    st = 1.0 / np.sqrt((dx[i.ravel()] / xscale) ** 2 + (dy[j.ravel()] / yscale) ** 2)
+    blocks.append((k, k + ny + 1, st))
+    blocks.append((k + 1, k + ny, st))
+    regs = []
+    for a_, b_, st in blocks:
+        m = a_.size
+        regs.append(sp.csr_matrix((np.concatenate([-st, st]), (np.tile(np.arange(m), 2), np.concatenate([a_, b_]))),
+                                  shape=(m, nx * ny)))
+    Areg = sp.vstack(regs).tocsr()
+    NA = abs(A).sum(0).max()
+    NR = abs(Areg).sum(0).max()
+    S = sp.vstack([A, Areg * (smoothness * NA / NR)]).tocsc()
+    rhs = np.concatenate([z, np.zeros(Areg.shape[0])])
+    zflat = spla.spsolve((S.T @ S).tocsc(), S.T @ rhs)
+    return zflat.reshape((nx, ny)).T
+

@@ -265,3 +265,29 @@ def test_temporal_match_incremental_mode_accumulates():
         U = RD["ResultDisp"][k]["U"]
         e = np.hypot(U[:, 0] - tu, U[:, 1] - tv)[inner]
         assert np.isfinite(e).sum() > 20 and np.nanmedian(e) < 0.05, k
+
+
+def test_uniform_subpb1_driver_ends_with_the_gridfit_surface():
+    """Subpb1 (uniform) as the reference returns it: every node on the gridfit 'springs'
+    surface of the good nodes (func/Subpb1.m:186-199)."""
+    import aldic_b200 as A
+    from aldic_b200.fill import gridfit_springs
+
+    O.build()
+    sc = synth.temporal_affine(seed=8, M=160, N=160, n_speckles=900, u=1.7, v=-0.9)
+    ctx = OracleContext()
+    Df = A.funImgGradient(sc.ref.astype(float), ctx=ctx)
+    xs = np.arange(20.0, 141.0, 12.0)
+    X, Y = np.meshgrid(xs, xs, indexing="ij")
+    C = np.stack([X.ravel(), Y.ravel()], 1)
+    tu, tv = sc.disp(C[:, 0], C[:, 1])
+    U0 = np.stack([tu, tv], 1).ravel()
+    F0 = np.tile([sc.dudx, 0.0, 0.0, sc.dvdy], len(C))
+    args = (U0, F0, np.zeros(4 * len(C)), np.zeros(2 * len(C)), C, Df, sc.ref.astype(float), sc.deff.astype(float),
+            1e-3, 0.0, None, 1, {"winsize": 20})
+    U, *_ = A.Subpb1(*args, ctx=ctx)
+    Un, *_ = A.Subpb1(*args, ctx=ctx, fill=False)
+    assert np.isfinite(U).all()
+    zg = gridfit_springs(C[:, 0], C[:, 1], Un[0::2], xs, xs)
+    assert np.abs(U[0::2] - zg[np.searchsorted(xs, C[:, 1]), np.searchsorted(xs, C[:, 0])]).max() < 1e-12
+    assert np.median(np.hypot(U[0::2] - tu, U[1::2] - tv)) < 0.02

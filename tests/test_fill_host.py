@@ -103,3 +103,59 @@ def test_native_weights_match_the_python_construction():
                 a[idx[m, :cnt[m]]] = w[m, :cnt[m]]
                 wb, _ = O.sibson_bruteforce(P, Q[m])
                 assert np.abs(a - wb).max() < 1e-10
+
+
+def _gridfit_dense(xn, yn, data, smoothness=1.0):
+    """The springs fit by a separate construction: one row per finite node value, one per
+    spring between grid neighbours (right, up, both diagonals), dense least squares."""
+    nx, ny = len(xn), len(yn)
+    idx = lambda i, j: j + ny * i  # noqa: E731  (column-major node number, as MATLAB's grid)
+    A, z = [], []
+    for i in range(nx):
+        for j in range(ny):
+            if np.isfinite(data[j, i]):
+                r = np.zeros(nx * ny)
+                r[idx(i, j)] = 1.0
+                A.append(r)
+                z.append(data[j, i])
+    A = np.array(A)
+    sx, sy = np.mean(np.diff(xn)), np.mean(np.diff(yn))
+    reg = []
+    for i in range(nx):
+        for j in range(ny):
+            for di, dj in ((0, 1), (1, 0), (1, 1), (1, -1)):
+                i2, j2 = i + di, j + dj
+                if not (0 <= i2 < nx and 0 <= j2 < ny):
+                    continue
+                h = np.hypot((xn[i2] - xn[i]) / sx * (di != 0), (yn[j2] - yn[j]) / sy * (dj != 0))
+                r = np.zeros(nx * ny)
+                r[idx(i, j)], r[idx(i2, j2)] = -1.0 / h, 1.0 / h
+                reg.append(r)
+    R = np.array(reg)
+    lam = smoothness * np.abs(A).sum(0).max() / np.abs(R).sum(0).max()
+    S = np.vstack([A, lam * R])
+    sol = np.linalg.lstsq(S, np.concatenate([z, np.zeros(len(R))]), rcond=None)[0]
+    return sol.reshape((nx, ny)).T
+
+
+def test_gridfit_springs_matches_a_separate_construction():
+    from aldic_b200.fill import gridfit_springs
+
+    rng = np.random.default_rng(4)
+    xn = np.array([10.0, 18.0, 26.0, 34.0, 42.0, 50.0])
+    yn = np.array([5.0, 13.0, 21.0, 29.0, 37.0])
+    X, Y = np.meshgrid(xn, yn)                     # ny x nx
+    data = 0.3 * X - 0.1 * Y + np.sin(X / 7.0) + 0.05 * rng.standard_normal(X.shape)
+    data[2, 3] = data[0, 0] = data[4, 5] = np.nan  # the fit covers them
+    got = gridfit_springs(X.ravel(), Y.ravel(), data.ravel(), xn, yn)
+    want = _gridfit_dense(xn, yn, data)
+    assert got.shape == (5, 6) and np.abs(got - want).max() < 1e-10
+    # the 'triangle' rule off the nodes: a cell centre is the mean of the cell's diagonal
+    # corners, so a plane sampled there, with vanishing smoothing, comes back exactly
+    cx = (X[:-1, :-1] + X[1:, 1:]).ravel() / 2
+    cy = (Y[:-1, :-1] + Y[1:, 1:]).ravel() / 2
+    plane = lambda a, b: 1.0 + 0.2 * a - 0.3 * b  # noqa: E731
+    pts_x = np.concatenate([X.ravel(), cx])
+    pts_y = np.concatenate([Y.ravel(), cy])
+    zg = gridfit_springs(pts_x, pts_y, plane(pts_x, pts_y), xn, yn, smoothness=1e-9)
+    assert np.abs(zg - plane(X, Y)).max() < 1e-6
