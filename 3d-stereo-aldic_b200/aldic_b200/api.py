@@ -18,6 +18,7 @@ import time
 import numpy as np
 
 from . import fill as _fill
+from . import smooth as _smooth
 from . import _lib
 from ._lib import AldicError
 
@@ -578,11 +579,13 @@ def ALDICFrameQuadtree(fNormalized, gNormalized, fNormalizedMask, DICpara, ImgSe
     the search by the natural-neighbour interpolation of an earlier result onto the search
     grid ('natural', 'none', NaN -> 0, cc.max = 1; the 'reuseLast' initial guess, :112-128).
     Returns a dict: DICmesh, DICmesh_nonQuadtree, U (USubpb2), USubpb1, FSubpb1, beta,
-    markCoordHoleStrain, DICpara.  The displacement smoothing options (DispSmoothness,
-    Smooth2DTimes) are not implemented and must be 0."""
-    if DICpara.get("DispSmoothness", 0) > 1e-6 or DICpara.get("Smooth2DTimes", 0):
-        raise AldicError("ALDICFrameQuadtree: displacement smoothing (funSmoothDispQuadtree) is not implemented")
+    markCoordHoleStrain, DICpara.  DICpara['Smooth2DTimes'] (default 0) smooths USubpb1
+    before the global step and USubpb2 in each ADMM round that many times, and
+    DICpara['DispSmoothness'] > 1e-6 smooths the first global result once
+    (funSmoothDispQuadtree, :257-263, :310, :355-357)."""
     ctx = ctx or default_context()
+    n_smooth = int(DICpara.get("Smooth2DTimes", 0) or 0)
+    disp_smooth = float(DICpara.get("DispSmoothness", 0) or 0) > 1e-6
     fN = np.asarray(fNormalized, dtype=np.float64)
     gN = np.asarray(gNormalized, dtype=np.float64)
     fMask = np.asarray(fNormalizedMask, dtype=np.float64)
@@ -624,6 +627,8 @@ def ALDICFrameQuadtree(fNormalized, gNormalized, fNormalizedMask, DICpara, ImgSe
     if np.isnan(F1[:, 0]).any() and (~np.isnan(F1[:, 0])).sum() > 10:
         F1 = _fill.fill_nans_natural(C, F1, "none")
     U1, F1 = U1.ravel(), F1.ravel()
+    for _ in range(n_smooth):
+        U1 = _smooth.funSmoothDispQuadtree(U1, mesh, DICpara)
     # section 5: the global step
     mu, alpha, order = 1e-3, 0.0, 2
     step = float(np.mean(np.ravel(DICpara["winstepsize"])))
@@ -641,6 +646,8 @@ def ALDICFrameQuadtree(fNormalized, gNormalized, fNormalizedMask, DICpara, ImgSe
     if U2 is None or abs(beta - betaList[-1]) > np.finfo(float).eps:
         U2 = Subpb2Quadtree(mesh, order, beta, mu, U1, F1, None, None, alpha, step, 0, ctx=ctx)
     U2 = np.array(U2)
+    if disp_smooth:
+        U2 = _smooth.funSmoothDispQuadtree(U2, mesh, DICpara)
     U2[hdof] = U1[hdof]
     F2 = F1
     vdual = U2 - U1
@@ -650,6 +657,8 @@ def ALDICFrameQuadtree(fNormalized, gNormalized, fNormalizedMask, DICpara, ImgSe
         U1, _, _, _, _ = Subpb1Quadtree(U2, F2, np.zeros(4 * C.shape[0]), vdual, C, Df, fN, gN, mu, beta, None,
                                         ALSolveStep, para, "GaussNewton", 1e-2, ctx=ctx)
         U2 = np.array(Subpb2Quadtree(mesh, order, beta, mu, U1, F1, None, None, alpha, step, 0, ctx=ctx))
+        for _ in range(n_smooth):
+            U2 = _smooth.funSmoothDispQuadtree(U2, mesh, DICpara)
         U2[hdof] = U1[hdof]
         vdual = U2 - U1
     return {"DICmesh": mesh, "DICmesh_nonQuadtree": mesh0, "U": U2, "USubpb1": U1, "FSubpb1": F1, "beta": beta,

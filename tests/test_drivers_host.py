@@ -291,3 +291,25 @@ def test_uniform_subpb1_driver_ends_with_the_gridfit_surface():
     zg = gridfit_springs(C[:, 0], C[:, 1], Un[0::2], xs, xs)
     assert np.abs(U[0::2] - zg[np.searchsorted(xs, C[:, 1]), np.searchsorted(xs, C[:, 0])]).max() < 1e-12
     assert np.median(np.hypot(U[0::2] - tu, U[1::2] - tv)) < 0.02
+
+
+def test_aldic_frame_with_displacement_smoothing():
+    """The ALDIC frame with the optional smoothing switched on (Smooth2DTimes 1,
+    DispSmoothness 5e-4): every step runs and the field still matches the plate's."""
+    import aldic_b200 as A
+
+    O.build()
+    sc = synth.plate_with_hole(size=256, hole_r=40.0, peak=1.5, sin_amp=0.2, sin_wl=100.0)
+    M, N = sc.ref.shape
+    para = {"winsize": 24, "winstepsize": 16, "winsizeMin": 8, "TemporalSearchDistance": 6, "ImgSize": [M, N],
+            "gridxyROIRange": {"gridx": [1, M], "gridy": [1, N]}, "ImgRefMask": sc.mask, "Smooth2DTimes": 1,
+            "DispSmoothness": 5e-4, "DispFilterStd": 0, "DispFilterSize": 0}
+    r = A.ALDICFrameQuadtree(sc.ref.astype(float) * sc.mask, sc.deff.astype(float), sc.mask, para, 2,
+                             ctx=OracleContext())
+    C = r["DICmesh"]["coordinatesFEM"]
+    tu, tv = sc.disp(C[:, 0], C[:, 1])
+    ix = np.floor(C[:, 0] + 0.5).astype(int) - 1
+    iy = np.floor(C[:, 1] + 0.5).astype(int) - 1
+    inside = (sc.mask[ix, iy] > 0) & (C[:, 0] > 24) & (C[:, 0] < M - 24) & (C[:, 1] > 24) & (C[:, 1] < N - 24)
+    err = np.hypot(r["U"][0::2] - tu, r["U"][1::2] - tv)[inside]
+    assert np.isfinite(err).all() and np.median(err) < 0.08
