@@ -59,6 +59,9 @@ class OracleContext:
     def triangulate(self, pairs, KL, KR, R, T, out=None):
         return O.triangulate(pairs, KL, KR, R, T)
 
+    def undistort_points(self, pts, K, radial, tangential=None):
+        return O.undistort_points(pts, K, radial, tangential)
+
     def local_icgn(self, variant, coords, U0, winsize, tol, **kw):
         frame = O.Frame(self.img[0], self.img[1], self.mask, self.g[0], self.g[1])
         return O.local_icgn(frame, np.asarray(coords, dtype=np.float64), np.asarray(U0, dtype=np.float64), winsize,
@@ -313,3 +316,27 @@ def test_aldic_frame_with_displacement_smoothing():
     inside = (sc.mask[ix, iy] > 0) & (C[:, 0] > 24) & (C[:, 0] < M - 24) & (C[:, 1] > 24) & (C[:, 1] < N - 24)
     err = np.hypot(r["U"][0::2] - tu, r["U"][1::2] - tv)[inside]
     assert np.isfinite(err).all() and np.median(err) < 0.08
+
+
+def test_reconstruction_undistorts_first():
+    """stereoReconstruction_quadtree with lens distortion: pairs pushed through each camera's
+    lens model and reconstructed with its coefficients give the same 3-D points as the
+    undistorted pairs without them (funUndistortPoints, then triangulate)."""
+    import aldic_b200 as A
+
+    sc = synth.stereo_pair(seed=2, size=224, f=500.0, plane_half=320.0)
+    xs = np.arange(40.0, 190.0, 25.0)
+    X, Y = np.meshgrid(xs, xs, indexing="ij")
+    C = np.stack([X.ravel(), Y.ravel()], 1)
+    t = synth.stereo_truth(sc, C)
+    pairs = [np.concatenate([C, t["right0"]], 1)]
+    cam = {"KL": sc.KL, "KR": sc.KR, "R": sc.R_rl, "T": sc.T_rl}
+    ref, _ = A.stereoReconstruction_quadtree(pairs, cam, ctx=OracleContext())
+    lens = dict(cam, radialL=[-0.08, 0.01], tangentialL=[1e-3, -5e-4], radialR=[0.05, -0.02, 0.003],
+                tangentialR=[-8e-4, 2e-4])
+    dpairs = [np.concatenate([O.distort_points(C, sc.KL, lens["radialL"], lens["tangentialL"]),
+                              O.distort_points(t["right0"], sc.KR, lens["radialR"], lens["tangentialR"])], 1)]
+    got, _ = A.stereoReconstruction_quadtree(dpairs, lens, ctx=OracleContext())
+    assert np.abs(got["Coordinates"][0] - ref["Coordinates"][0]).max() < 1e-6
+    assert np.abs(dpairs[0] - pairs[0]).max() > 0.1   # the lens model moved the points
+
