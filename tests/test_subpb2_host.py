@@ -245,3 +245,36 @@ def test_generated_mesh_passes_the_global_step_patch_test():
     used = np.unique(E[E > 0]) - 1
     d = np.abs(Uh - U).reshape(-1, 2)[used]
     assert d.max() < 1e-10
+
+
+def test_quadtree_mesh_nonbinary_mask_and_integer_corners():
+    import aldic_b200 as A
+    from aldic_b200 import synth
+
+    sc = synth.plate_with_hole(size=256, hole_r=40.0, peak=1.0, sin_amp=0.1, sin_wl=100.0)
+    w, st = 32, 16
+    xl = np.arange(1 + w // 2, 256 - w // 2 + 1, st, dtype=float)
+    X, Y = np.meshgrid(xl, xl)
+    mesh = A.MeshSetUp(X, Y, {"winstepsize": st, "ImgSize": [256, 256]})
+    mesh["elementMinSize"] = 4
+    para = {"winstepsize": st, "winsize": w}
+    U0 = np.zeros(2 * mesh["coordinatesFEM"].shape[0])
+    mask = sc.mask * 0.7 + 0.2  # two levels, not 0 / 1: the min / max and sum rules on values
+    m, _, _ = A.GenerateQuadtreeMesh(U0, None, mask, mesh, para)
+    C, E = m["coordinatesFEM"], m["elementsFEM"]
+    for e in range(E.shape[0]):
+        x0, y0 = C[E[e, 0] - 1].astype(int)
+        x1, y1 = C[E[e, 2] - 1].astype(int)
+        blk = mask[x0 - 1:x1, y0 - 1:y1]
+        assert not (x1 - x0 > 4 and blk.max() > blk.min())          # nothing left to refine
+        assert blk.sum() >= 0.5 * (x1 - x0) * (y1 - y0)              # funMarkInside kept it
+    assert (E[:, 4:] > 0).any()
+    # a minimum size that halves 16-px elements into 2-px ones reaches 1-px corners only
+    # through non-integer boxes for odd sizes: step 10 -> 5 -> 2.5 must raise
+    xl10 = np.arange(1 + w // 2, 256 - w // 2 + 1, 10, dtype=float)
+    X10, Y10 = np.meshgrid(xl10, xl10)
+    mesh10 = A.MeshSetUp(X10, Y10, {"winstepsize": 10, "ImgSize": [256, 256]})
+    mesh10["elementMinSize"] = 2
+    with pytest.raises(A.AldicError):
+        A.GenerateQuadtreeMesh(np.zeros(2 * mesh10["coordinatesFEM"].shape[0]), None, sc.mask, mesh10,
+                               {"winstepsize": 10, "winsize": w})
