@@ -5,6 +5,6 @@ include/aldic_b200.h); this package is its host-side mirror of the reference's M
 interface (funIntegerSearch, LocalICGN, LocalICGNQuadtree, Subpb1, Subpb1Quadtree,
 epipolar_ICGN1, stereoReconstruction_quadtree, ...).
 """
-from ._lib import DEFAULT_ITERATION_CAP, QUADTREE, UNIFORM, AldicError, load as load_library  # noqa: F401
+from ._lib import DEFAULT_FP64_BAND, DEFAULT_ITERATION_CAP, QUADTREE, UNIFORM, AldicError, load as load_library  # noqa: F401,E501
 from .api import *  # noqa: F401,F403
 from . import api, synth  # noqa: F401

@@ -21,6 +21,9 @@ UNIFORM, QUADTREE = 0, 1
 # iterations the one-warp solver pass gives a subset before the multi-warp pass restarts it, when
 # aldic_set_iteration_cap has not been called (kDefaultWarpCap in csrc/kernels.h)
 DEFAULT_ITERATION_CAP = 8
+# relative band around tol in which an FP32 convergence test is re-decided in FP64, when
+# aldic_set_fp64_band has not been called (kDefaultFp64Band in csrc/kernels.h)
+DEFAULT_FP64_BAND = 1e-2
 
 # Every symbol the header declares, with (restype, argtypes).
 _vp = C.c_void_p
@@ -59,6 +62,7 @@ SIGNATURES = {
     "aldic_measure_fp32_peak": (_i, [_vp, C.POINTER(_d)]),
     "aldic_set_profiling": (_i, [_vp, _i]),
     "aldic_set_iteration_cap": (_i, [_vp, _i]),
+    "aldic_set_fp64_band": (_i, [_vp, _d]),
     "aldic_profile_read": (_i, [_vp, C.POINTER(_d), C.POINTER(_i)]),
     "aldic_local_icgn_noalloc": (_i, [_i, _vp, _vp, _vp, _vp, _vp, _i, _i, _i64, _vp, _vp, _i, _d, _vp, _vp, _vp,
                                       _vp, _vp, _vp]),

@@ -162,6 +162,11 @@ class Context:
         restarts it (default 8)."""
         self._check(self.lib.aldic_set_iteration_cap(self.h, int(cap)), "aldic_set_iteration_cap")
 
+    def set_fp64_band(self, band):
+        """Relative band around tol in which local_icgn re-decides a convergence test by an
+        FP64 re-solve of the subset (0 disables; a huge value re-solves every subset)."""
+        self._check(self.lib.aldic_set_fp64_band(self.h, float(band)), "aldic_set_fp64_band")
+
     def set_profiling(self, on=True):
         """Record the device time of the correlation kernel of each integer_search call."""
         self._check(self.lib.aldic_set_profiling(self.h, 1 if on else 0), "aldic_set_profiling")

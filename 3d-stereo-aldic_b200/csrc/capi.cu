@@ -56,6 +56,7 @@ struct aldic_ctx {
   void* tscratch = nullptr;  // shared-product search scratch
   size_t tscratch_cap = 0;
   int warp_cap = kDefaultWarpCap;  // aldic_set_iteration_cap
+  double fp64_band = kDefaultFp64Band;  // aldic_set_fp64_band
   // aldic_subpb2_set_mesh: the resident global-step mesh tables (element table, node ->
   // element lists, node kinds) in one device buffer
   char* sp2 = nullptr;
@@ -515,7 +516,7 @@ static int icgn_common(aldic_ctx* c, int variant, int64_t n, const double* coord
   }
   if (wmax < winsize) wmax = winsize;
   if (icgn_smem_bytes(wmax) > 200 * 1024) return fail(c, ALDIC_ERR_ARG, "winsize %d too large for shared memory", winsize);
-  const size_t qbytes = (size_t)2 * n * 3 * sizeof(int);
+  const size_t qbytes = (size_t)kIcgnQueueBuckets * n * 3 * sizeof(int);
   Arg ac{coords, (size_t)n * 2 * 8, false, nullptr}, au0{epi ? nullptr : U0, epi ? 0 : (size_t)n * 2 * 8, false, nullptr};
   Arg au{U, epi ? 0 : (size_t)n * 2 * 8, true, nullptr}, af{F, epi ? 0 : (size_t)n * 4 * 8, true, nullptr};
   Arg ah{H, H ? (size_t)n * 21 * 8 : 0, true, nullptr};
@@ -548,6 +549,8 @@ static int icgn_common(aldic_ctx* c, int variant, int64_t n, const double* coord
   a.queue = (int*)arena_take(c, qbytes);
   a.qcount = c->qcount;
   a.carry = (double*)arena_take(c, (size_t)n * 8 * sizeof(double));
+  // the FP64 re-solve needs its (larger) shared-memory window; beyond that, FP32 decides alone
+  a.band = icgn_smem_bytes_f64(wmax) <= 200 * 1024 ? c->fp64_band : 0.0;
   return finish(c, launch_icgn(a, wmax, c->stream));
 }
 
@@ -1108,6 +1111,13 @@ int aldic_set_iteration_cap(aldic_ctx* c, int cap) {
   if (!c) return ALDIC_ERR_ARG;
   if (cap < 1 || cap > 1000) return fail(c, ALDIC_ERR_ARG, "iteration cap %d outside 1..1000", cap);
   c->warp_cap = cap;
+  return ALDIC_OK;
+}
+
+int aldic_set_fp64_band(aldic_ctx* c, double band) {
+  if (!c) return ALDIC_ERR_ARG;
+  if (!(band >= 0.0) || !(band <= 1e300)) return fail(c, ALDIC_ERR_ARG, "band %g must be >= 0 and finite", band);
+  c->fp64_band = band;
   return ALDIC_OK;
 }
 

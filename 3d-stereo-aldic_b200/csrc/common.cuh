@@ -45,6 +45,48 @@ __device__ __forceinline__ float stencil16(const float* __restrict__ img, int M,
   return acc;
 }
 
+// The same stencil in FP64 arranged as the reference's double path computes it
+// (ba_interp2_spline.cpp:235-331): per row i of the integer matrix K = 56 BC (up to sign and
+// scale), T_ij = K_j . (K_i . Q), and the value sum_ij s_ij T_ij tr^i tc^j, where each
+// scale s_ij is a float-literal constant of the reference rounded to float before it is
+// promoted (3/56, 1/7, 9/3136, 3/392, 1/49; ba_interp2_spline.cpp:310-325).  It tracks the
+// reference MEX to ~1e-13 and serves the FP64 re-solve of subsets whose FP32 convergence
+// decision was too close to call.  All 16 taps in bounds.
+__device__ __forceinline__ double stencil16_ref64(const float* __restrict__ img, int M, int r0, int c0, double tr,
+                                                  double tc) {
+  constexpr int K[4][4] = {{0, 1, 0, 0}, {11, 1, -15, 3}, {19, -39, 25, -5}, {-3, 8, -8, 3}};
+  constexpr double sgn[4] = {1.0, -1.0, 1.0, 1.0};
+  const double s356 = (double)(3.0f / 56.0f), s17 = (double)(1.0f / 7.0f);
+  const double s9 = (double)((1.0f / 3136.0f) * 9.0f), s3392 = (double)(3.0f / 392.0f);
+  const double s149 = (double)(1.0f / 49.0f);
+  const double one[4] = {1.0, s356, s356, s17};
+  const float* p = img + (size_t)r0 + (size_t)c0 * M;
+  double rowc[4][4];  // rowc[i][c] = sum_r K_i[r] Q[r][c]
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    const double q0 = __ldg(p + (size_t)c * M), q1 = __ldg(p + (size_t)c * M + 1);
+    const double q2 = __ldg(p + (size_t)c * M + 2), q3 = __ldg(p + (size_t)c * M + 3);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) rowc[i][c] = ((K[i][0] * q0 + K[i][1] * q1) + K[i][2] * q2) + K[i][3] * q3;
+  }
+  const double pr[4] = {1.0, tr, tr * tr, tr * tr * tr};
+  const double pc[4] = {1.0, tc, tc * tc, tc * tc * tc};
+  double val = 0.0;
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const double t = ((K[j][0] * rowc[i][0] + K[j][1] * rowc[i][1]) + K[j][2] * rowc[i][2]) + K[j][3] * rowc[i][3];
+      double s;
+      if (i == 0 || j == 0) s = (i == 0) ? one[j] : one[i];
+      else if (i == 3 && j == 3) s = s149;
+      else if (i == 3 || j == 3) s = s3392;
+      else s = s9;
+      val += sgn[i] * sgn[j] * s * t * pr[i] * pc[j];
+    }
+  return val;
+}
+
 // Clamped version for arbitrary points (the MEX clamps taps to the image edge,
 // ba_interp2_spline.cpp:60-66).
 __device__ __forceinline__ float stencil16_clamped(const float* __restrict__ img, int M, int N, int r0, int c0, float tr,
@@ -113,6 +155,39 @@ __host__ __device__ __forceinline__ float2 fadd2(float2 a, float2 b) {
       : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
   return d;
 #endif
+}
+
+__host__ __device__ __forceinline__ float2 fsub2(float2 a, float2 b) {
+#ifndef __CUDA_ARCH__
+  return make_float2(a.x - b.x, a.y - b.y);
+#else
+  float2 d;
+  asm("{\n\t.reg .b64 ra, rb, rd;\n\t"
+      "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+      "sub.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+      : "=f"(d.x), "=f"(d.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return d;
+#endif
+}
+
+// Kahan-compensated accumulation (Kahan 1965), the compensation kept with the opposite sign:
+// the running total is s + k.  The caller forms y = x + k, fused into the term's own
+// operation (y = fma(a, b, k) for a product term), then
+//   t = s + y;  k = (s - t) + y;  s = t
+// (each operation rounded on its own: packed instructions or _rn intrinsics, never
+// contracted or reassociated).  The error of the total is bounded by ~2 ulp of sum |x|,
+// independent of the number of terms.
+__host__ __device__ __forceinline__ void kahan2(float2& s, float2& k, float2 y) {
+  const float2 t = fadd2(s, y);
+  k = fadd2(fsub2(s, t), y);
+  s = t;
+}
+
+__device__ __forceinline__ void kahan1(float& s, float& k, float y) {
+  const float t = __fadd_rn(s, y);
+  k = __fadd_rn(__fsub_rn(s, t), y);
+  s = t;
 }
 
 // Two stencils at once with packed FP32 pairs (.x: point a, .y: point b); each lane's

@@ -20,13 +20,17 @@
 // equals bf * (A_k - (C_k - mean_g * B_k) / bg) with A_k = sum J_k fn, B_k = sum J_k
 // (constant per subset) and C_k = sum J_k g (per iteration); mean_g and bg come from
 // sum g, sum g^2 over the same pass.
+#include <type_traits>
+
 #include "common.cuh"
 #include "kernels.h"
 
 namespace aldic {
 
 constexpr int kNT = 128;  // threads per solve CTA
-constexpr int kSlowSubset = 2;  // queue-1 flag of a subset restarted by the multi-warp pass
+constexpr int kSlowSubset = 2;   // queue-1 flag of a subset continued by the multi-warp pass
+constexpr int kMovedSubset = 4;  // queue-1 flag of a subset moved to the FP64 re-solve queue
+constexpr int kToFp64 = 5;       // hand-off code of the warp passes: re-solve in FP64
 
 struct SolveCtl {
   double P[6];
@@ -37,9 +41,10 @@ struct SolveCtl {
   double normNew, normAbs, normInit;
   double gsum_prev;
   double znssd;
+  double d5, d6;  // P5 - round(P5), P6 - round(P6) (FP64 interpolation)
   float pf[4], f5, f6;
   int base_r, base_c;  // 0-based tap-0 row/col offsets: x0 + n5 - 2, y0 + n6 - 2
-  int step, go, status, need_mask, fbw8_ready, done_error;
+  int step, go, status, need_mask, fbw8_ready, done_error, to_fp64;
 };
 
 __device__ __forceinline__ bool is_intd(double v) { return floor(v) == v && fabs(v) < 1e9; }
@@ -81,8 +86,10 @@ __device__ __forceinline__ void prep_coeffs(SolveCtl& c, double x0, double y0) {
   c.pf[1] = (float)c.P[1];
   c.pf[2] = (float)c.P[2];
   c.pf[3] = (float)c.P[3];
-  c.f5 = (float)(c.P[4] - n5);
-  c.f6 = (float)(c.P[5] - n6);
+  c.d5 = c.P[4] - n5;
+  c.d6 = c.P[5] - n6;
+  c.f5 = (float)c.d5;
+  c.f6 = (float)c.d6;
   c.base_r = (int)(x0 + n5) - 2;
   c.base_c = (int)(y0 + n6) - 2;
 }
@@ -230,26 +237,32 @@ __global__ void icgn_classify_kernel(IcgnArgs a) {
 }
 
 // ================================================================================
-// 6-DOF solve kernel
+// 6-DOF solve kernel (general: masks, enlarged windows; FP32, or FP64 for re-solves)
 // ================================================================================
+// Shared-memory arrays of one subset: g (the interpolated deformed window, FP32 or FP64),
+// f, f_x, f_y (FP32 image data), and the u8 masks of the flood fills.
+template <bool F64>
 struct SolveSmem {
+  using G = typename std::conditional<F64, double, float>::type;
+  G* g;
   float* f;
   float* gx;
   float* gy;
-  float* g;
   uint8_t* on;    // f-mask pixel on (quadtree)
   uint8_t* lab;   // flood-fill output (bw4, then per-iteration g region)
   uint8_t* tmp;   // flood-fill input
   uint8_t* fbw8;  // 8-connected f-mask region (g-mask fallback)
 };
 
-__device__ __forceinline__ SolveSmem carve(unsigned char* base, int npx) {
-  SolveSmem s;
-  s.f = reinterpret_cast<float*>(base);
+template <bool F64>
+__device__ __forceinline__ SolveSmem<F64> carve(unsigned char* base, int npx) {
+  using G = typename SolveSmem<F64>::G;
+  SolveSmem<F64> s;
+  s.g = reinterpret_cast<G*>(base);  // first: 8-byte aligned for the FP64 form
+  s.f = reinterpret_cast<float*>(s.g + npx);
   s.gx = s.f + npx;
   s.gy = s.gx + npx;
-  s.g = s.gy + npx;
-  uint8_t* u = reinterpret_cast<uint8_t*>(s.g + npx);
+  uint8_t* u = reinterpret_cast<uint8_t*>(s.gy + npx);
   s.on = u;
   s.lab = u + npx;
   s.tmp = u + 2 * npx;
@@ -257,7 +270,34 @@ __device__ __forceinline__ SolveSmem carve(unsigned char* base, int npx) {
   return s;
 }
 
+// Queue 2 receives a subset for the FP64 re-solve (from its initial guess): its entry keeps
+// the window and the masked flag of the entry it came from.
+__device__ __forceinline__ void push_fp64(const IcgnArgs& a, long long t, int w, int masked) {
+  const int pos = atomicAdd(&a.qcount[4], 1);
+  int* q2 = a.queue + 3 * (2 * a.n + pos);
+  q2[0] = (int)t;
+  q2[1] = w;
+  q2[2] = masked;
+}
+
+// Whether a convergence test (funICGN.m:268-282: |b|/|b_1| < tol or |b| < tol) lies within
+// the relative band of tol where FP32 arithmetic cannot be trusted to decide as the FP64
+// reference does; such subsets are re-solved in FP64.
+__device__ __forceinline__ bool too_close_to_call(double normRel, double normAbs, double normInit, double tol,
+                                                  double band) {
+  if (!(band > 0)) return false;
+  const double lim = band * tol;
+  if (fabs(normAbs - tol) <= lim) return true;
+  return normInit > tol && fabs(normRel - tol) <= lim;
+}
+
+// The FP32 form solves queue 1 (enlarged or masked subsets and those handed over by the warp
+// passes) and moves subsets whose convergence test is too close to call to queue 2; the FP64
+// form (interpolation in the reference's own double arithmetic, FP64 sums) re-solves queue 2
+// from the initial guesses, so its decisions are the FP64 reference's.
+template <bool F64>
 __global__ void __launch_bounds__(kNT) icgn_solve_kernel(IcgnArgs a, int bucket) {
+  using G = typename SolveSmem<F64>::G;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ SolveCtl c;
   __shared__ double red[(kNT / 32) * 40];
@@ -266,14 +306,14 @@ __global__ void __launch_bounds__(kNT) icgn_solve_kernel(IcgnArgs a, int bucket)
   const FrameDev& fr = a.fr;
   const bool quad = (a.variant == 1);
   const bool epi = (a.variant == 2);
-  const int count = a.qcount[bucket];
+  const int count = a.qcount[bucket == 2 ? 4 : bucket];
   const int gM = fr.M - 6;
   for (int qi = blockIdx.x; qi < count; qi += gridDim.x) {
     const int* q = a.queue + 3 * ((long long)bucket * a.n + qi);
     const long long t = q[0];
     const int w = q[1];
-    if (q[2] == kSlowSubset) continue;  // restarted by the multi-warp pass
-    const bool masked = q[2] != 0;
+    if (q[2] == kSlowSubset || q[2] == kMovedSubset) continue;  // solved by another pass
+    const bool masked = q[2] == 1;
     const int W1 = w + 1, npx = W1 * W1;
     const int half = w / 2;
     double x0 = a.coords[t], y0 = a.coords[a.n + t];
@@ -282,7 +322,7 @@ __global__ void __launch_bounds__(kNT) icgn_solve_kernel(IcgnArgs a, int bucket)
       y0 = mround(y0);
     }
     const int seed = (int)floor((w + 1) / 2.0) - 1;
-    SolveSmem s = carve(smem_raw, npx);
+    SolveSmem<F64> s = carve<F64>(smem_raw, npx);
     // ---- load the subset window ----
     {
       const int r0 = (int)x0 - half - 1, c0 = (int)y0 - half - 1;
@@ -314,50 +354,36 @@ __global__ void __launch_bounds__(kNT) icgn_solve_kernel(IcgnArgs a, int bucket)
         }
       __syncthreads();
     }
-    // ---- setup sums: H (21), sum J f (6), sum J (6), f stats (3), sum |f| (1) ----
+    // ---- setup sums: H (21), sum J f (6), sum J (6), f stats (3), sum |f| (1); FP64 per thread
+    //      (J = gradient x integer offset is exact in FP64) ----
     {
-      float h[21], jf[6], jb[6], fs = 0.f, fs2 = 0.f, fn = 0.f, fab = 0.f;
+      double v[37];
 #pragma unroll
-      for (int k = 0; k < 21; ++k) h[k] = 0.f;
-#pragma unroll
-      for (int k = 0; k < 6; ++k) {
-        jf[k] = 0.f;
-        jb[k] = 0.f;
-      }
+      for (int k = 0; k < 37; ++k) v[k] = 0.0;
       for (int p = tid; p < npx; p += kNT) {
-        const float dx = (float)(p % W1 - half), dy = (float)(p / W1 - half);
-        const float gxv = s.gx[p], gyv = s.gy[p], f = s.f[p];
-        const float J[6] = {gxv * dx, gyv * dx, gxv * dy, gyv * dy, gxv, gyv};
-        int k = 0;
+        const double dx = (double)(p % W1 - half), dy = (double)(p / W1 - half);
+        const double gxv = s.gx[p], gyv = s.gy[p], f = s.f[p];
+        const double J[6] = {gxv * dx, gyv * dx, gxv * dy, gyv * dy, gxv, gyv};
 #pragma unroll
         for (int i = 0; i < 6; ++i)
 #pragma unroll
-          for (int j = i; j < 6; ++j) h[k++] = fmaf(J[i], J[j], h[k]);
+          for (int j = i; j < 6; ++j) {
+            const int m = i * 6 - i * (i - 1) / 2 + (j - i);  // packed upper triangle by rows
+            v[m] = fma(J[i], J[j], v[m]);
+          }
 #pragma unroll
         for (int i = 0; i < 6; ++i) {
-          jf[i] = fmaf(J[i], f, jf[i]);
-          jb[i] += J[i];
+          v[21 + i] = fma(J[i], f, v[21 + i]);
+          v[27 + i] += J[i];
         }
-        const bool sel = quad ? (fabsf(f) > 1e-10f) : true;
+        const bool sel = quad ? (fabs(f) > 1e-10) : true;
         if (sel) {
-          fs += f;
-          fs2 = fmaf(f, f, fs2);
-          fn += 1.f;
+          v[33] += f;
+          v[34] = fma(f, f, v[34]);
+          v[35] += 1.0;
         }
-        fab += fabsf(f);
+        v[36] += fabs(f);
       }
-      double v[37];
-#pragma unroll
-      for (int k = 0; k < 21; ++k) v[k] = h[k];
-#pragma unroll
-      for (int k = 0; k < 6; ++k) {
-        v[21 + k] = jf[k];
-        v[27 + k] = jb[k];
-      }
-      v[33] = fs;
-      v[34] = fs2;
-      v[35] = fn;
-      v[36] = fab;
       block_sum<37, kNT>(v, red, sums);
     }
     if (tid == 0) {
@@ -402,6 +428,7 @@ __global__ void __launch_bounds__(kNT) icgn_solve_kernel(IcgnArgs a, int bucket)
       c.status = 0;
       c.fbw8_ready = 0;
       c.done_error = 0;
+      c.to_fp64 = 0;
       c.gsum_prev = 0.0;
       c.znssd = ALDIC_NAN;
     }
@@ -410,7 +437,7 @@ __global__ void __launch_bounds__(kNT) icgn_solve_kernel(IcgnArgs a, int bucket)
     const int q_nt = kNT / W1, r_nt = kNT % W1;
     while (true) {
       if (tid == 0) {
-        int go = (c.step <= a.max_iter && c.normNew > a.tol && c.normAbs > a.tol) ? 1 : 0;
+        int go = (!c.to_fp64 && c.step <= a.max_iter && c.normNew > a.tol && c.normAbs > a.tol) ? 1 : 0;
         if (go) {
           c.step += 1;
           if (quad && masked && c.step > 1) {
@@ -438,29 +465,41 @@ __global__ void __launch_bounds__(kNT) icgn_solve_kernel(IcgnArgs a, int bucket)
       }
       __syncthreads();
       if (!c.go) break;
-      // pass 1: interpolate, single-pass sums
-      float C[6] = {0, 0, 0, 0, 0, 0}, S1 = 0.f, S2 = 0.f, ns = 0.f, nz = 0.f, fg = 0.f;
+      // pass 1: interpolate, single-pass sums (FP64 across the threads' partials)
+      double v[11];
       {
+        G C[6] = {0, 0, 0, 0, 0, 0}, S1 = 0, S2 = 0, fg = 0;
+        float ns = 0.f, nz = 0.f;
         int aa = tid % W1, bb = tid / W1;
         for (int p = tid; p < npx; p += kNT) {
-          const float dx = (float)(aa - half), dy = (float)(bb - half);
-          const float g = warp_g(fr, c, dx, dy);
+          G g;
+          if constexpr (F64) {
+            // u22 - (x0 + n5) in FP64, the reference's own interpolation arithmetic
+            const double dx = (double)(aa - half), dy = (double)(bb - half);
+            const double lx = dx + (c.P[0] * dx + (c.P[2] * dy + c.d5));
+            const double ly = dy + (c.P[3] * dy + (c.P[1] * dx + c.d6));
+            const double ix = floor(lx), iy = floor(ly);
+            g = stencil16_ref64(fr.def, fr.M, c.base_r + (int)ix, c.base_c + (int)iy, lx - ix, ly - iy);
+          } else {
+            g = warp_g(fr, c, (float)(aa - half), (float)(bb - half));
+          }
           s.g[p] = g;
-          const float ag = s.gx[p] * g, bg = s.gy[p] * g;
-          C[0] = fmaf(ag, dx, C[0]);
-          C[1] = fmaf(bg, dx, C[1]);
-          C[2] = fmaf(ag, dy, C[2]);
-          C[3] = fmaf(bg, dy, C[3]);
+          const G dx = (G)(aa - half), dy = (G)(bb - half);
+          const G ag = (G)s.gx[p] * g, bg = (G)s.gy[p] * g;
+          C[0] = fma(ag, dx, C[0]);
+          C[1] = fma(bg, dx, C[1]);
+          C[2] = fma(ag, dy, C[2]);
+          C[3] = fma(bg, dy, C[3]);
           C[4] += ag;
           C[5] += bg;
-          const bool sel = quad ? (fabsf(g) > 1e-10f) : true;
+          const bool sel = quad ? (fabs(g) > (G)1e-10) : true;
           if (sel) {
             S1 += g;
-            S2 = fmaf(g, g, S2);
+            S2 = fma(g, g, S2);
             ns += 1.f;
           }
-          nz += (g == 0.f) ? 1.f : 0.f;
-          if (epi) fg = fmaf(s.f[p], g, fg);
+          nz += (g == (G)0) ? 1.f : 0.f;
+          if (epi) fg = fma((G)s.f[p], g, fg);
           aa += r_nt;
           bb += q_nt;
           if (aa >= W1) {
@@ -468,14 +507,20 @@ __global__ void __launch_bounds__(kNT) icgn_solve_kernel(IcgnArgs a, int bucket)
             bb += 1;
           }
         }
+#pragma unroll
+        for (int k = 0; k < 6; ++k) v[k] = C[k];
+        v[6] = S1;
+        v[7] = S2;
+        v[8] = ns;
+        v[9] = nz;
+        v[10] = fg;
       }
-      double v[11] = {C[0], C[1], C[2], C[3], C[4], C[5], S1, S2, ns, nz, fg};
       block_sum<11, kNT>(v, red, sums);
       const bool run_mask = quad && (masked || sums[9] > 0);
       if (run_mask) {
         // g region: bwselect(logical(g), seed, seed, 8); if it covers the window, the
         // 8-connected f-mask region instead (funICGNQuadtree.m:170-182)
-        for (int p = tid; p < npx; p += kNT) s.tmp[p] = (s.g[p] != 0.f);
+        for (int p = tid; p < npx; p += kNT) s.tmp[p] = (s.g[p] != (G)0);
         __syncthreads();
         flood_select(s.tmp, s.lab, W1, W1, seed, seed, 8, nullptr);
         int allon = 1;
@@ -490,20 +535,21 @@ __global__ void __launch_bounds__(kNT) icgn_solve_kernel(IcgnArgs a, int bucket)
           gm = s.fbw8;
         }
         __syncthreads();
-        float C2[6] = {0, 0, 0, 0, 0, 0}, T1 = 0.f, T2 = 0.f, tn = 0.f, gs = 0.f;
+        G C2[6] = {0, 0, 0, 0, 0, 0}, T1 = 0, T2 = 0;
+        float tn = 0.f, gs = 0.f;
         for (int p = tid; p < npx; p += kNT) {
-          const float dx = (float)(p % W1 - half), dy = (float)(p / W1 - half);
-          const float g = gm[p] ? s.g[p] : 0.f;
-          const float ag = s.gx[p] * g, bg = s.gy[p] * g;
-          C2[0] = fmaf(ag, dx, C2[0]);
-          C2[1] = fmaf(bg, dx, C2[1]);
-          C2[2] = fmaf(ag, dy, C2[2]);
-          C2[3] = fmaf(bg, dy, C2[3]);
+          const G dx = (G)(p % W1 - half), dy = (G)(p / W1 - half);
+          const G g = gm[p] ? s.g[p] : (G)0;
+          const G ag = (G)s.gx[p] * g, bg = (G)s.gy[p] * g;
+          C2[0] = fma(ag, dx, C2[0]);
+          C2[1] = fma(bg, dx, C2[1]);
+          C2[2] = fma(ag, dy, C2[2]);
+          C2[3] = fma(bg, dy, C2[3]);
           C2[4] += ag;
           C2[5] += bg;
-          if (fabsf(g) > 1e-10f) {
+          if (fabs(g) > (G)1e-10) {
             T1 += g;
-            T2 = fmaf(g, g, T2);
+            T2 = fma(g, g, T2);
             tn += 1.f;
           }
           gs += gm[p] ? 1.f : 0.f;
@@ -532,7 +578,9 @@ __global__ void __launch_bounds__(kNT) icgn_solve_kernel(IcgnArgs a, int bucket)
         if (c.step == 1) c.normInit = c.normNew;
         if (c.normInit > a.tol) c.normNew = c.normNew / c.normInit;
         else c.normNew = 0.0;
-        if (!(c.normNew < a.tol || c.normAbs < a.tol)) {
+        if (!F64 && !epi && too_close_to_call(c.normNew, c.normAbs, c.normInit, a.tol, a.band)) {
+          c.to_fp64 = 1;  // leave the loop; the FP64 pass re-solves this subset
+        } else if (!(c.normNew < a.tol || c.normAbs < a.tol)) {
           double dP[6];
           for (int i = 0; i < 6; ++i) {
             double acc = 0;
@@ -557,7 +605,9 @@ __global__ void __launch_bounds__(kNT) icgn_solve_kernel(IcgnArgs a, int bucket)
       if (!(c.normNew < a.tol || c.normAbs < a.tol)) step = a.max_iter + 1;
       if (isnan(c.normNew)) step = a.max_iter + 1;
       if (quad && c.sabsf < 1e-6) step = a.max_iter + 3;
-      if (epi) {
+      if (c.to_fp64) {
+        push_fp64(a, t, w, masked ? 1 : 0);
+      } else if (epi) {
         a.znssd[t] = c.done_error ? ALDIC_NAN : c.znssd;
         if (a.conv) a.conv[t] = c.done_error ? -1 : step;
       } else if (c.done_error) {
@@ -691,41 +741,36 @@ __global__ void __launch_bounds__(kWT, NW == 1 ? 3 : 2) icgn_group_kernel(IcgnAr
     }
     const int r0 = (int)x0 - half - 1, c0 = (int)y0 - half - 1;
     const int q_nt = GT / W1, r_nt = GT % W1;
-    // ---- set-up sums in one pass over the window ----
+    // ---- set-up sums, FP64 per lane (J = gradient x integer offset is exact in FP64), in two
+    //      passes over the window to bound the live accumulators ----
     double meanf, bf, sabsf;
     {
-      float h[21], jf[6], jb[6], fs = 0.f, fs2 = 0.f, fn = 0.f, fab = 0.f;
-#pragma unroll
-      for (int k = 0; k < 21; ++k) h[k] = 0.f;
+      double jf[6], jb[6], fs = 0.0, fs2 = 0.0, fab = 0.0;
+      float fn = 0.f;
 #pragma unroll
       for (int k = 0; k < 6; ++k) {
-        jf[k] = 0.f;
-        jb[k] = 0.f;
+        jf[k] = 0.0;
+        jb[k] = 0.0;
       }
       int aa = gt % W1, bb = gt / W1;
       for (int p = gt; p < npx; p += GT) {
         const int k = (r0 + aa) + (c0 + bb) * fr.M;
         const int kg = (r0 + aa - a.crop) + (c0 + bb - a.crop) * gM;
-        const float f = fr.ref[k];  // a quadtree subset here has no masked pixel
-        const float gxv = fr.gx[kg], gyv = fr.gy[kg];
-        const float dx = (float)(aa - half), dy = (float)(bb - half);
-        const float J[6] = {gxv * dx, gyv * dx, gxv * dy, gyv * dy, gxv, gyv};
-        int m = 0;
-#pragma unroll
-        for (int i = 0; i < 6; ++i)
-#pragma unroll
-          for (int j = i; j < 6; ++j) h[m++] = fmaf(J[i], J[j], h[m]);
+        const float ff = fr.ref[k];  // a quadtree subset here has no masked pixel
+        const double f = ff, gxv = fr.gx[kg], gyv = fr.gy[kg];
+        const double dx = (double)(aa - half), dy = (double)(bb - half);
+        const double J[6] = {gxv * dx, gyv * dx, gxv * dy, gyv * dy, gxv, gyv};
 #pragma unroll
         for (int i = 0; i < 6; ++i) {
-          jf[i] = fmaf(J[i], f, jf[i]);
+          jf[i] = fma(J[i], f, jf[i]);
           jb[i] += J[i];
         }
-        if (!quad || fabsf(f) > 1e-10f) {
+        if (!quad || fabsf(ff) > 1e-10f) {
           fs += f;
-          fs2 = fmaf(f, f, fs2);
+          fs2 = fma(f, f, fs2);
           fn += 1.f;
         }
-        fab += fabsf(f);
+        fab += fabs(f);
         aa += r_nt;
         bb += q_nt;
         if (aa >= W1) {
@@ -734,7 +779,7 @@ __global__ void __launch_bounds__(kWT, NW == 1 ? 3 : 2) icgn_group_kernel(IcgnAr
         }
       }
       {
-        double v[4] = {fs, fs2, fn, fab};
+        double v[4] = {fs, fs2, (double)fn, fab};
         group_sum<NW, 4>(v, red, gw, lane, bar);
         sabsf = v[3];
         if (v[2] > 0) {
@@ -762,16 +807,36 @@ __global__ void __launch_bounds__(kWT, NW == 1 ? 3 : 2) icgn_group_kernel(IcgnAr
             }
         }
       }
-      {
-        double v[21];
+    }
+    {
+      double h[21];
 #pragma unroll
-        for (int k = 0; k < 21; ++k) v[k] = h[k];
-        group_sum<NW, 21>(v, red, gw, lane, bar);
-        if (gt < 21) {
+      for (int k = 0; k < 21; ++k) h[k] = 0.0;
+      int aa = gt % W1, bb = gt / W1;
+      for (int p = gt; p < npx; p += GT) {
+        const int kg = (r0 + aa - a.crop) + (c0 + bb - a.crop) * gM;
+        const double gxv = fr.gx[kg], gyv = fr.gy[kg];
+        const double dx = (double)(aa - half), dy = (double)(bb - half);
+        const double J[6] = {gxv * dx, gyv * dx, gxv * dy, gyv * dy, gxv, gyv};
 #pragma unroll
-          for (int k = 0; k < 21; ++k)
-            if (gt == k) s_h[grp][k] = v[k];
+        for (int i = 0; i < 6; ++i)
+#pragma unroll
+          for (int j = i; j < 6; ++j) {
+            const int m = i * 6 - i * (i - 1) / 2 + (j - i);  // packed upper triangle by rows
+            h[m] = fma(J[i], J[j], h[m]);
+          }
+        aa += r_nt;
+        bb += q_nt;
+        if (aa >= W1) {
+          aa -= W1;
+          bb += 1;
         }
+      }
+      group_sum<NW, 21>(h, red, gw, lane, bar);
+      if (gt < 21) {
+#pragma unroll
+        for (int k = 0; k < 21; ++k)
+          if (gt == k) s_h[grp][k] = h[k];
       }
     }
     group_bar<NW>(bar);
@@ -789,10 +854,30 @@ __global__ void __launch_bounds__(kWT, NW == 1 ? 3 : 2) icgn_group_kernel(IcgnAr
       }
       __syncwarp();
       for (int k = 0; k < 6; ++k) {
-        if (lane < 6) s_fac[grp][lane] = aug[lane * 12 + k];
-        const double piv = aug[k * 12 + k];
+        // partial pivoting: the row (>= k) with the largest |entry| in column k, first one on
+        // ties (the mldivide of funICGN.m:288 pivots as well)
+        double best = lane >= k && lane < 6 ? fabs(aug[lane * 12 + k]) : -1.0;
+        int piv = lane;
+#pragma unroll
+        for (int o = 4; o > 0; o >>= 1) {
+          const double ob = __shfl_down_sync(0xffffffffu, best, o);
+          const int op = __shfl_down_sync(0xffffffffu, piv, o);
+          if (lane + o < 8 && (ob > best || (ob == best && op < piv))) {
+            best = ob;
+            piv = op;
+          }
+        }
+        piv = __shfl_sync(0xffffffffu, piv, 0);
+        if (piv != k && lane < 12) {
+          const double tk = aug[k * 12 + lane];
+          aug[k * 12 + lane] = aug[piv * 12 + lane];
+          aug[piv * 12 + lane] = tk;
+        }
         __syncwarp();
-        if (lane < 12) aug[k * 12 + lane] /= piv;
+        if (lane < 6) s_fac[grp][lane] = aug[lane * 12 + k];
+        const double pv = aug[k * 12 + k];
+        __syncwarp();
+        if (lane < 12) aug[k * 12 + lane] /= pv;
         __syncwarp();
         for (int e = lane; e < 72; e += 32) {
           const int i = e / 12, j = e % 12;
@@ -827,12 +912,19 @@ __global__ void __launch_bounds__(kWT, NW == 1 ? 3 : 2) icgn_group_kernel(IcgnAr
       const float p0 = (float)P[0], p1 = (float)P[1], p2 = (float)P[2], p3 = (float)P[3];
       const float f5 = (float)(P[4] - n5), f6 = (float)(P[5] - n6);
       const int br = (int)(x0 + n5) - 2, bc = (int)(y0 + n6) - 2;
-      float C[6] = {0, 0, 0, 0, 0, 0}, S1 = 0.f, S2 = 0.f, ns = 0.f, nz = 0.f, fg = 0.f;
+      // per-lane sums of the pixel pairs (p, p + GT) in packed FP32 with Kahan compensation
+      // (s + k is the compensated total; 3 extra packed operations per term), a last unpaired
+      // pixel alone; the lane totals go to FP64 before the cross-lane sums
+      double v[11];
       {
-        // pixels in pairs (p, p + GT) with packed FP32 pairs; a last unpaired pixel alone
-        float2 C2[6], S12 = make_float2(0.f, 0.f), S22 = make_float2(0.f, 0.f), fg2 = make_float2(0.f, 0.f);
+        float2 C2[6], K2[6], S12 = make_float2(0.f, 0.f), KS1 = make_float2(0.f, 0.f);
+        float2 S22 = make_float2(0.f, 0.f), KS2 = make_float2(0.f, 0.f), fg2 = make_float2(0.f, 0.f);
+        float S1 = 0.f, kS1 = 0.f, S2 = 0.f, kS2 = 0.f, ns = 0.f, nz = 0.f;
 #pragma unroll
-        for (int k = 0; k < 6; ++k) C2[k] = make_float2(0.f, 0.f);
+        for (int k = 0; k < 6; ++k) {
+          C2[k] = make_float2(0.f, 0.f);
+          K2[k] = make_float2(0.f, 0.f);
+        }
         const float2 pp0 = make_float2(p0, p0), pp1 = make_float2(p1, p1), pp2 = make_float2(p2, p2);
         const float2 pp3 = make_float2(p3, p3), ff5 = make_float2(f5, f5), ff6 = make_float2(f6, f6);
         int aa = gt % W1, bb = gt / W1;
@@ -855,24 +947,24 @@ __global__ void __launch_bounds__(kWT, NW == 1 ? 3 : 2) icgn_group_kernel(IcgnAr
           const int kb = (r0 + ab - a.crop) + (c0 + bbb - a.crop) * gM;
           const float2 ag = fmul2(make_float2(fr.gx[ka], fr.gx[kb]), g);
           const float2 bg = fmul2(make_float2(fr.gy[ka], fr.gy[kb]), g);
-          C2[0] = ffma2(ag, dx, C2[0]);
-          C2[1] = ffma2(bg, dx, C2[1]);
-          C2[2] = ffma2(ag, dy, C2[2]);
-          C2[3] = ffma2(bg, dy, C2[3]);
-          C2[4] = fadd2(C2[4], ag);
-          C2[5] = fadd2(C2[5], bg);
+          kahan2(C2[0], K2[0], ffma2(ag, dx, K2[0]));
+          kahan2(C2[1], K2[1], ffma2(bg, dx, K2[1]));
+          kahan2(C2[2], K2[2], ffma2(ag, dy, K2[2]));
+          kahan2(C2[3], K2[3], ffma2(bg, dy, K2[3]));
+          kahan2(C2[4], K2[4], fadd2(ag, K2[4]));
+          kahan2(C2[5], K2[5], fadd2(bg, K2[5]));
           if (!quad) {
-            S12 = fadd2(S12, g);
-            S22 = ffma2(g, g, S22);
+            kahan2(S12, KS1, fadd2(g, KS1));
+            kahan2(S22, KS2, ffma2(g, g, KS2));
           } else {
             if (fabsf(g.x) > 1e-10f) {
-              S1 += g.x;
-              S2 = fmaf(g.x, g.x, S2);
+              kahan1(S1, kS1, g.x + kS1);
+              kahan1(S2, kS2, fmaf(g.x, g.x, kS2));
               ns += 1.f;
             }
             if (fabsf(g.y) > 1e-10f) {
-              S1 += g.y;
-              S2 = fmaf(g.y, g.y, S2);
+              kahan1(S1, kS1, g.y + kS1);
+              kahan1(S2, kS2, fmaf(g.y, g.y, kS2));
               ns += 1.f;
             }
             nz += (g.x == 0.f ? 1.f : 0.f) + (g.y == 0.f ? 1.f : 0.f);
@@ -887,6 +979,18 @@ __global__ void __launch_bounds__(kWT, NW == 1 ? 3 : 2) icgn_group_kernel(IcgnAr
             bb += 1;
           }
         }
+#pragma unroll
+        for (int k = 0; k < 6; ++k)
+          v[k] = ((double)C2[k].x + (double)K2[k].x) + ((double)C2[k].y + (double)K2[k].y);
+        if (!quad) {
+          v[6] = ((double)S12.x + (double)KS1.x) + ((double)S12.y + (double)KS1.y);
+          v[7] = ((double)S22.x + (double)KS2.x) + ((double)S22.y + (double)KS2.y);
+          ns = (float)((npx - gt + GT - 1) / GT);  // pixels of this thread
+        } else {
+          v[6] = (double)S1 + (double)kS1;
+          v[7] = (double)S2 + (double)kS2;
+        }
+        v[10] = (double)fg2.x + (double)fg2.y;
         if (p < npx) {  // the last, unpaired pixel
           const float dx = (float)(aa - half), dy = (float)(bb - half);
           const float lx = dx + fmaf(p0, dx, fmaf(p2, dy, f5));
@@ -895,30 +999,28 @@ __global__ void __launch_bounds__(kWT, NW == 1 ? 3 : 2) icgn_group_kernel(IcgnAr
           const float g = stencil16(fr.def, fr.M, br + (int)ix, bc + (int)iy, lx - ix, ly - iy);
           const int kg = (r0 + aa - a.crop) + (c0 + bb - a.crop) * gM;
           const float ag = fr.gx[kg] * g, bg = fr.gy[kg] * g;
-          C[0] = fmaf(ag, dx, C[0]);
-          C[1] = fmaf(bg, dx, C[1]);
-          C[2] = fmaf(ag, dy, C[2]);
-          C[3] = fmaf(bg, dy, C[3]);
-          C[4] += ag;
-          C[5] += bg;
-          if (!quad || fabsf(g) > 1e-10f) {
-            S1 += g;
-            S2 = fmaf(g, g, S2);
-            ns += 1.f;
+          v[0] += (double)(ag * dx);
+          v[1] += (double)(bg * dx);
+          v[2] += (double)(ag * dy);
+          v[3] += (double)(bg * dy);
+          v[4] += (double)ag;
+          v[5] += (double)bg;
+          if (quad) {
+            if (fabsf(g) > 1e-10f) {
+              v[6] += (double)g;
+              v[7] += (double)g * (double)g;
+              ns += 1.f;
+            }
+            if (g == 0.f) nz += 1.f;
+          } else {
+            v[6] += (double)g;
+            v[7] += (double)g * (double)g;
           }
-          if (quad && g == 0.f) nz += 1.f;
-          if (epi) fg = fmaf(fr.ref[(r0 + aa) + (c0 + bb) * fr.M], g, fg);
+          if (epi) v[10] += (double)fr.ref[(r0 + aa) + (c0 + bb) * fr.M] * (double)g;
         }
-#pragma unroll
-        for (int k = 0; k < 6; ++k) C[k] += C2[k].x + C2[k].y;
-        if (!quad) {
-          S1 += S12.x + S12.y;
-          S2 += S22.x + S22.y;
-          ns = (float)((npx - gt + GT - 1) / GT);  // pixels of this thread
-        }
-        if (epi) fg += fg2.x + fg2.y;
+        v[8] = ns;
+        v[9] = nz;
       }
-      double v[11] = {C[0], C[1], C[2], C[3], C[4], C[5], S1, S2, ns, nz, fg};
       group_sum<NW, 11>(v, red, gw, lane, bar);
       if (v[9] > 0) {  // exact zero in g: the g-region flood fill is needed
         requeue = 0;
@@ -953,6 +1055,10 @@ __global__ void __launch_bounds__(kWT, NW == 1 ? 3 : 2) icgn_group_kernel(IcgnAr
       if (step == 1) normInit = normNew;
       if (normInit > a.tol) normNew = normNew / normInit;
       else normNew = 0.0;
+      if (!epi && too_close_to_call(normNew, normAbs, normInit, a.tol, a.band)) {
+        requeue = kToFp64;  // the FP64 pass re-solves this subset from its initial guess
+        break;
+      }
       if (!(normNew < a.tol || normAbs < a.tol)) {
         if (!compose_inverse(P, dP)) {
           step = a.max_iter + 1000;
@@ -964,6 +1070,11 @@ __global__ void __launch_bounds__(kWT, NW == 1 ? 3 : 2) icgn_group_kernel(IcgnAr
       }
     }
     if (gt == 0) {
+      if (requeue == kToFp64) {
+        push_fp64(a, t, w, 0);  // unmasked, at the window this pass solved
+        if (SLOW) const_cast<int*>(q)[2] = kMovedSubset;
+        requeue = -2;
+      }
       if (requeue == kSlowSubset && a.carry) {
         double* cs = a.carry + 8 * t;
 #pragma unroll
@@ -984,7 +1095,7 @@ __global__ void __launch_bounds__(kWT, NW == 1 ? 3 : 2) icgn_group_kernel(IcgnAr
           q1[1] = w;
           q1[2] = requeue;
         }
-      } else {
+      } else if (requeue == -1) {
         if (status == 1) step -= 1000;
         if (!(normNew < a.tol || normAbs < a.tol)) step = a.max_iter + 1;
         if (isnan(normNew)) step = a.max_iter + 1;
@@ -1412,6 +1523,7 @@ static int occupancy_grid(const void* fn, size_t smem) {
 }
 
 size_t icgn_smem_bytes(int w) { return (size_t)(w + 1) * (w + 1) * (4 * sizeof(float) + 4); }
+size_t icgn_smem_bytes_f64(int w) { return (size_t)(w + 1) * (w + 1) * (sizeof(double) + 3 * sizeof(float) + 4); }
 size_t sub1_smem_bytes(int wx, int wy) { return (size_t)(wx + 1) * (wy + 1) * (4 * sizeof(float) + 5); }
 
 
@@ -1630,7 +1742,8 @@ __global__ void __launch_bounds__(kWT, 2) subpb1_group_kernel(Sub1Args a) {
 
 int launch_icgn(const IcgnArgs& a, int wmax_enlarged, cudaStream_t st) {
   int launches = 0;
-  cudaMemsetAsync(a.qcount, 0, 4 * sizeof(int), st);  // 2 queue counts, 2 work counters
+  // counts of buckets 0 and 1, the 2 work counters, the count of bucket 2
+  cudaMemsetAsync(a.qcount, 0, 8 * sizeof(int), st);
   const long long threads = a.n * 32;
   const int cb = 256;
   icgn_classify_kernel<<<(unsigned)((threads + cb - 1) / cb), cb, 0, st>>>(a);
@@ -1655,12 +1768,22 @@ int launch_icgn(const IcgnArgs& a, int wmax_enlarged, cudaStream_t st) {
   }
   {  // enlarged / masked subsets, and those handed over by the fast kernel
     const size_t smem = icgn_smem_bytes(wmax_enlarged);
-    cudaFuncSetAttribute(icgn_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    int grid = occupancy_grid((const void*)icgn_solve_kernel, smem);
+    cudaFuncSetAttribute(icgn_solve_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int grid = occupancy_grid((const void*)icgn_solve_kernel<false>, smem);
     grid = grid < 296 ? grid : 296;
     if ((long long)grid > a.n) grid = (int)a.n;
     if (grid < 1) grid = 1;
-    icgn_solve_kernel<<<grid, kNT, smem, st>>>(a, 1);
+    icgn_solve_kernel<false><<<grid, kNT, smem, st>>>(a, 1);
+    ++launches;
+  }
+  if (a.band > 0 && a.variant != 2) {  // FP64 re-solves of the subsets too close to call in FP32
+    const size_t smem = icgn_smem_bytes_f64(wmax_enlarged);
+    cudaFuncSetAttribute(icgn_solve_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int grid = occupancy_grid((const void*)icgn_solve_kernel<true>, smem);
+    grid = grid < 296 ? grid : 296;
+    if ((long long)grid > a.n) grid = (int)a.n;
+    if (grid < 1) grid = 1;
+    icgn_solve_kernel<true><<<grid, kNT, smem, st>>>(a, 2);
     ++launches;
   }
   return launches;

@@ -36,10 +36,14 @@ struct IcgnArgs {
   int* conv;     // n
   uint8_t* mark; // n or null
   double* znssd; // n (epipolar)
-  int* queue;    // 2 buckets x n x 3 ints
-  int* qcount;   // 4: queue counts of the 2 buckets, work counters of the 2 warp-group passes
+  int* queue;    // 3 buckets x n x 3 ints: nominal window; enlarged / masked / handed over; FP64 re-solve
+  int* qcount;   // 5 (8 cleared): counts of buckets 0 and 1, work counters of the 2 warp-group passes,
+                 // count of bucket 2
   double* carry; // n x 8 or null: where the warp pass left a subset it hands to the multi-warp pass
+  double band;   // relative band around tol in which an FP32 convergence test is re-decided by an
+                 // FP64 re-solve of the subset (0: never)
 };
+constexpr double kDefaultFp64Band = 1e-2;  // default IcgnArgs::band
 
 struct Sub1Args {
   FrameDev fr;
@@ -90,7 +94,9 @@ int launch_mask_binarize(const double* in, long long n, uint8_t* out, cudaStream
 int launch_gradient(const float* img, const uint8_t* mask, int M, int N, float* gx, float* gy, cudaStream_t st);
 int launch_interp_points(const float* img, int M, int N, long long n, const double* X, const double* Y, double* Z,
                          cudaStream_t st);
-size_t icgn_smem_bytes(int w);
+size_t icgn_smem_bytes(int w);       // FP32 general solve kernel, window w
+size_t icgn_smem_bytes_f64(int w);   // FP64 re-solve kernel
+constexpr int kIcgnQueueBuckets = 3;
 size_t sub1_smem_bytes(int wx, int wy);
 int launch_icgn(const IcgnArgs& a, int wmax_enlarged, cudaStream_t st);
 int launch_subpb1(const Sub1Args& a, int wmax_x, int wmax_y, cudaStream_t st);

@@ -11,11 +11,16 @@
 // Limits and sharing:
 //   * at most ALDIC_NOALLOC_MAX_SUBSETS subsets per call (larger n is rejected with
 //     ALDIC_ERR_ARG before any work is queued);
-//   * the array (2 buckets x ALDIC_NOALLOC_MAX_SUBSETS x 3 ints + 2 counters, ~1.5 MB) is
-//     held by every GPU that loads the library until the process exits;
+//   * the array (3 buckets x ALDIC_NOALLOC_MAX_SUBSETS x 3 ints, then the counters: the
+//     three bucket counts and the two work counters of the solver passes; ~2.4 MB) is held
+//     by every GPU that loads the library until the process exits;
 //   * all calls share the one array: calls that overlap on the GPU (different streams, or
 //     different host threads) race on it and must be serialised by the caller.  Each call
-//     clears the two bucket counters before use; the queue entries are rewritten.
+//     clears the counters before use; the queue entries are rewritten.
+//   * every array must be device (or managed) memory of the current device; a pointer to
+//     another GPU's memory is refused with ALDIC_ERR_ARG.
+//   * a CUDA error already pending from the caller's earlier work is reported as
+//     ALDIC_ERR_CUDA before anything is queued, and left pending for the caller.
 //   * the first call on a device looks up the array's device address
 //     (cudaGetSymbolAddress) once for that device; make that first call before any stream
 //     capture.
@@ -33,8 +38,12 @@ namespace {
 constexpr long long kMaxSubsets = ALDIC_NOALLOC_MAX_SUBSETS;
 constexpr int kMaxDevices = 64;
 
-// queue (2 x kMaxSubsets x 3 ints) followed by the two bucket counters
-__device__ __align__(256) int g_noalloc_scratch[2 * kMaxSubsets * 3 + 64];
+// queue (3 buckets x kMaxSubsets x 3 ints) followed by the counters: the counts of the three
+// buckets and the two work counters (launch_icgn clears eight ints), padded to 64 ints
+constexpr int kCounterInts = 64;
+static_assert(kCounterInts >= 8, "launch_icgn clears eight counters after the queue");
+constexpr long long kQueueInts = (long long)aldic::kIcgnQueueBuckets * kMaxSubsets * 3;
+__device__ __align__(256) int g_noalloc_scratch[kQueueInts + kCounterInts];
 
 std::mutex g_setup_mutex;
 int* g_scratch_addr[kMaxDevices] = {nullptr};
@@ -57,14 +66,17 @@ int scratch_address(int** out) {
   return ALDIC_OK;
 }
 
-bool on_device(const void* p) {
+// Device or managed memory that belongs to device `dev` (the current device).
+bool on_device(const void* p, int dev) {
   if (!p) return false;
   cudaPointerAttributes at;
   if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
     cudaGetLastError();
     return false;
   }
-  return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+  if (at.type == cudaMemoryTypeDevice) return at.device == dev;
+  if (at.type == cudaMemoryTypeManaged) return true;  // reachable from every device
+  return false;
 }
 
 }  // namespace
@@ -84,10 +96,15 @@ extern "C" int aldic_local_icgn_noalloc(int variant, const float* ref, const flo
     return ALDIC_ERR_ARG;
   }
   if (n == 0) return ALDIC_OK;
+  // an error left pending by the caller's earlier work: report it, queue nothing, and leave
+  // it pending (cudaPeekAtLastError does not clear it)
+  if (cudaPeekAtLastError() != cudaSuccess) return ALDIC_ERR_CUDA;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return ALDIC_ERR_CUDA;
   const void* need[] = {ref, def, dfdx, dfdy, coords, U0, U, F, conv};
   for (const void* p : need)
-    if (!on_device(p)) return ALDIC_ERR_ARG;  // every array must already be device memory
-  if ((mask && !on_device(mask)) || (H && !on_device(H)) || (markHole && !on_device(markHole)))
+    if (!on_device(p, dev)) return ALDIC_ERR_ARG;  // every array must be memory of the current device
+  if ((mask && !on_device(mask, dev)) || (H && !on_device(H, dev)) || (markHole && !on_device(markHole, dev)))
     return ALDIC_ERR_ARG;
   const double w = winsize;
   int wmax = variant == ALDIC_QUADTREE ? (int)(2 * std::ceil(std::sqrt(1.0 / 0.6) * w / 2)) + 2
@@ -121,8 +138,9 @@ extern "C" int aldic_local_icgn_noalloc(int variant, const float* ref, const flo
   a.mark = variant == ALDIC_QUADTREE ? markHole : nullptr;
   a.znssd = nullptr;
   a.queue = scratch;
-  a.qcount = scratch + 2 * kMaxSubsets * 3;  // cleared by launch_icgn before the classify kernel
+  a.qcount = scratch + kQueueInts;  // cleared by launch_icgn before the classify kernel
   a.carry = nullptr;  // slow subsets restart from their initial guess (no state buffer here)
+  a.band = aldic::icgn_smem_bytes_f64(wmax) <= 200 * 1024 ? aldic::kDefaultFp64Band : 0.0;
   aldic::launch_icgn(a, wmax, static_cast<cudaStream_t>(stream));
   return cudaGetLastError() == cudaSuccess ? ALDIC_OK : ALDIC_ERR_CUDA;
 }

@@ -111,7 +111,12 @@ int aldic_integer_search(aldic_ctx* ctx, const int* search, const int* gridx, co
  * func/funICGN.m) or LocalICGNQuadtree (ALDIC_QUADTREE;
  * func_quadtree/LocalICGNQuadtree.m:67-164 with func_quadtree/funICGNQuadtree.m):
  * first-order IC-GN, Gauss-Newton, maxIter 100, on the REF/DEF slots, gradients and
- * mask of the context.  H (n x 21) and markHole (n, quadtree only) may be NULL. */
+ * mask of the context.  H (n x 21) and markHole (n, quadtree only) may be NULL.
+ * Interpolation and sums run in FP32 (Kahan-compensated per thread, FP64 across threads);
+ * a subset whose convergence test |b|/|b_1| < tol or |b| < tol (func/funICGN.m:268-282)
+ * falls within a relative band of tol (aldic_set_fp64_band) is re-solved from its initial
+ * guess in FP64 with the reference's own interpolation arithmetic, so that its iteration
+ * count, and with it U, is the FP64 reference's. */
 int aldic_local_icgn(aldic_ctx* ctx, int variant, int64_t n, const double* coords, const double* U0, int winsize,
                      double tol, double* U, double* F, double* H, int32_t* conv, uint8_t* markHole);
 
@@ -230,7 +235,7 @@ int aldic_triangulate(aldic_ctx* ctx, int64_t n, const double* pairs, const doub
  * device memory (a host that owns every allocation: gpuArray buffers handed over by a
  * MEX, a fixed memory budget or pool).  No context and no cudaMalloc/cudaFree: the work
  * queue lives in a fixed file-scope device array sized for ALDIC_NOALLOC_MAX_SUBSETS
- * subsets (~1.5 MB, held by every GPU that loads the library until exit).  Every array
+ * subsets (~2.4 MB, held by every GPU that loads the library until exit).  Every array
  * must be device memory on the current device: ref/def are the normalised FP32 images
  * (M x N), mask is u8 (may be NULL), dfdx/dfdy are FP32 (M-6) x (N-6); the rest as
  * aldic_local_icgn.  Work is queued on `stream` (NULL = legacy default stream) and not
@@ -249,6 +254,10 @@ int aldic_local_icgn_noalloc(int variant, const float* ref, const float* def, co
  * FFMA loop and a packed FFMA2 (fma.rn.f32x2) loop, the denominator the library's
  * compute-bound kernels are reported against.  Not part of the reference. */
 int aldic_measure_fp32_peak(aldic_ctx* ctx, double* tflops);
+/* Relative band around tol within which aldic_local_icgn re-decides an FP32 convergence
+ * test by an FP64 re-solve of the subset (default 1e-2; 0 = never; a huge value re-solves
+ * every subset in FP64).  A precision setting; not part of the reference. */
+int aldic_set_fp64_band(aldic_ctx* ctx, double band);
 /* Iterations the one-warp-per-subset solver pass of aldic_local_icgn / aldic_subpb1 spends
  * on a subset before a multi-warp pass restarts it from its initial guess (default 8, 1..1000).
  * Results do not depend on it beyond FP32 summation order; it trades the tail of slow

@@ -171,6 +171,74 @@ def test_local_icgn_parity_affine(ctx, affine, variant):
     assert np.all(np.isnan(res["U"].reshape(-1, 2)[res["conv"] == -1]))
 
 
+@pytest.mark.parametrize("variant", [0, 1])
+def test_local_icgn_fp64_resolve_band(A, ctx, affine, variant):
+    # band 0: every convergence test decided in FP32 (Kahan-compensated sums), the old bar;
+    # a huge band: every subset re-solved from its initial guess by the FP64 kernel with the
+    # reference's interpolation arithmetic on the same FP32 images as the oracle sees, so
+    # codes are identical and U, F, H agree to FP64 rounding; the default band: codes equal
+    sc = affine
+    _load_raw(ctx, sc, mask=np.ones(sc.ref.shape) if variant == 1 else None)
+    M, N = sc.ref.shape
+    f, g = ctx.get_state(0), ctx.get_state(1)
+    gx, gy = ctx.get_state(2), ctx.get_state(3)
+    r = ctx.integer_search([10, 10], [1, M], [1, N], 30, 16)
+    coords = np.stack([r["x"].T.ravel(order="F"), r["y"].T.ravel(order="F")], 1)
+    U0 = np.nan_to_num(np.stack([r["u"].T.ravel(order="F"), r["v"].T.ravel(order="F")], 1)).ravel()
+    ref = O.local_icgn(O.Frame(f, g, None if variant == 0 else np.ones_like(f), gx, gy), coords, U0, 30, 1e-3,
+                       variant=variant)
+    ok = _flag(ref["conv"])
+    try:
+        ctx.set_fp64_band(0.0)
+        r32 = ctx.local_icgn(variant, coords, U0, 30, 1e-3)
+        ctx.set_fp64_band(1e300)
+        r64 = ctx.local_icgn(variant, coords, U0, 30, 1e-3)
+    finally:
+        ctx.set_fp64_band(A.DEFAULT_FP64_BAND)
+    rd = ctx.local_icgn(variant, coords, U0, 30, 1e-3)
+    both = _flag(r32["conv"]) & ok
+    assert np.mean(_flag(r32["conv"]) == ok) >= FLAG_RATE
+    assert np.abs(r32["U"] - ref["U"]).reshape(-1, 2)[both].max() < UV_TOL
+    assert np.array_equal(r64["conv"], ref["conv"])
+    assert np.array_equal(np.isnan(r64["U"]), np.isnan(ref["U"]))
+    assert np.abs(r64["U"] - ref["U"]).reshape(-1, 2)[ok].max() < 1e-8
+    assert np.abs(r64["F"] - ref["F"]).reshape(-1, 4)[ok].max() < 1e-9
+    Hr = ref["H"][ok]
+    assert np.max(np.abs(r64["H"][ok] - Hr) / np.abs(Hr).max(axis=1, keepdims=True)) < 1e-11
+    assert np.array_equal(rd["conv"], ref["conv"])
+    assert np.abs(rd["U"] - ref["U"]).reshape(-1, 2)[ok].max() < 1e-5
+    with pytest.raises(Exception):
+        ctx.set_fp64_band(-1.0)
+
+
+def test_local_icgn_fp64_resolve_masked(A, ctx, hole):
+    # the FP64 re-solve of masked subsets: bwselect regions, enlarged windows, the regrowth
+    # rule and codes -1 / 102 / 103 all decided in FP64
+    sc = hole
+    M, N = sc.ref.shape
+    ctx.load_image_raw(0, sc.ref, [1, M], [1, N], mask=sc.mask)
+    ctx.load_image_raw(1, sc.deff, [1, M], [1, N])
+    ctx.set_mask(sc.mask)
+    ctx.compute_gradients()
+    f, g = ctx.get_state(0), ctx.get_state(1)
+    gx, gy = ctx.get_state(2), ctx.get_state(3)
+    xs = np.arange(20, 370, 8.0)
+    X, Y = np.meshgrid(xs, xs, indexing="ij")
+    coords = np.stack([X.ravel(), Y.ravel()], 1)
+    tu, tv = sc.disp(coords[:, 0], coords[:, 1])
+    U0 = np.stack([np.round(tu), np.round(tv)], 1).ravel()
+    ref = O.local_icgn(O.Frame(f, g, sc.mask, gx, gy), coords, U0, 24, 1e-3, variant=1)
+    try:
+        ctx.set_fp64_band(1e300)
+        r64 = ctx.local_icgn(1, coords, U0, 24, 1e-3)
+    finally:
+        ctx.set_fp64_band(A.DEFAULT_FP64_BAND)
+    assert np.array_equal(r64["conv"], ref["conv"])
+    assert np.array_equal(r64["markHole"], ref["markHole"])
+    ok = _flag(ref["conv"])
+    assert np.abs(r64["U"] - ref["U"]).reshape(-1, 2)[ok].max() < 1e-8
+
+
 @pytest.fixture(scope="module")
 def hole():
     return synth.plate_with_hole(size=384, hole_r=60.0, peak=2.0, sin_amp=0.3, sin_wl=120.0)
