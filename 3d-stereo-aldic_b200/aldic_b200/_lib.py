@@ -18,12 +18,15 @@ ALDIC_ERR_STATE = 4
 U8, U16, F32, F64 = 0, 1, 2, 3
 SLOT_REF, SLOT_DEF = 0, 1
 UNIFORM, QUADTREE = 0, 1
+OPT_ITERATION_CAP, OPT_STAGING, OPT_SLOW_WARPS, OPT_SEARCH_IMPL, OPT_SEARCH_CHUNK, OPT_AUTOTUNE = 0, 1, 2, 3, 4, 5
+OPT_SLOW_FP64, OPT_FP64_THREADS = 6, 7
+STAT_FP64_RESOLVES, STAT_STAGING_TIMEOUT = 100, 101
 # iterations the one-warp solver pass gives a subset before the multi-warp pass restarts it, when
 # aldic_set_iteration_cap has not been called (kDefaultWarpCap in csrc/kernels.h)
 DEFAULT_ITERATION_CAP = 8
 # relative band around tol in which an FP32 convergence test is re-decided in FP64, when
 # aldic_set_fp64_band has not been called (kDefaultFp64Band in csrc/kernels.h)
-DEFAULT_FP64_BAND = 1e-2
+DEFAULT_FP64_BAND = 1e-3
 
 # Every symbol the header declares, with (restype, argtypes).
 _vp = C.c_void_p
@@ -63,6 +66,9 @@ SIGNATURES = {
     "aldic_set_profiling": (_i, [_vp, _i]),
     "aldic_set_iteration_cap": (_i, [_vp, _i]),
     "aldic_set_fp64_band": (_i, [_vp, _d]),
+    "aldic_set_option": (_i, [_vp, _i, _i]),
+    "aldic_get_option": (_i, [_vp, _i, C.POINTER(_i)]),
+    "aldic_tuning_report": (_i, [_vp, C.c_char_p, _i64]),
     "aldic_profile_read": (_i, [_vp, C.POINTER(_d), C.POINTER(_i)]),
     "aldic_local_icgn_noalloc": (_i, [_i, _vp, _vp, _vp, _vp, _vp, _i, _i, _i64, _vp, _vp, _i, _d, _vp, _vp, _vp,
                                       _vp, _vp, _vp]),

@@ -162,6 +162,24 @@ class Context:
         restarts it (default 8)."""
         self._check(self.lib.aldic_set_iteration_cap(self.h, int(cap)), "aldic_set_iteration_cap")
 
+    def set_option(self, option, value):
+        """A tuning option (aldic_set_option): OPT_ITERATION_CAP, OPT_STAGING, OPT_SLOW_WARPS,
+        OPT_SEARCH_IMPL, OPT_SEARCH_CHUNK, OPT_AUTOTUNE."""
+        self._check(self.lib.aldic_set_option(self.h, int(option), int(value)), "aldic_set_option")
+
+    def get_option(self, option):
+        v = C.c_int()
+        self._check(self.lib.aldic_get_option(self.h, int(option), C.byref(v)), "aldic_get_option")
+        return v.value
+
+    def tuning_report(self):
+        """The autotuner's choices (ALDIC_OPT_AUTOTUNE) as a dict."""
+        import json
+
+        buf = C.create_string_buffer(1 << 16)
+        self._check(self.lib.aldic_tuning_report(self.h, buf, len(buf)), "aldic_tuning_report")
+        return json.loads(buf.value.decode())
+
     def set_fp64_band(self, band):
         """Relative band around tol in which local_icgn re-decides a convergence test by an
         FP64 re-solve of the subset (0 disables; a huge value re-solves every subset)."""

@@ -8,6 +8,8 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <functional>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -57,6 +59,21 @@ struct aldic_ctx {
   size_t tscratch_cap = 0;
   int warp_cap = kDefaultWarpCap;  // aldic_set_iteration_cap
   double fp64_band = kDefaultFp64Band;  // aldic_set_fp64_band
+  // tuning options (aldic_set_option); with autotune on, each call shape takes the winner of
+  // its first call's candidate runs instead (tuned below)
+  int staging = 0;      // ALDIC_OPT_STAGING
+  int slow_nw = 2;      // ALDIC_OPT_SLOW_WARPS (FP32 slow pass, with ALDIC_OPT_SLOW_FP64 0)
+  int slow_fp64 = 0;    // ALDIC_OPT_SLOW_FP64
+  int fp64_threads = 128;  // ALDIC_OPT_FP64_THREADS
+  int search_impl = 0;  // ALDIC_OPT_SEARCH_IMPL
+  int search_chunk = 0; // ALDIC_OPT_SEARCH_CHUNK
+  int autotune = 0;     // ALDIC_OPT_AUTOTUNE
+  struct Tuned {
+    std::string choice;                    // the winner, as JSON
+    std::vector<std::pair<std::string, double>> ms;  // every candidate's time (ms; < 0: results differed)
+    int a = 0, b = 0, c = 0, d = 0;        // the winner's settings
+  };
+  std::map<std::string, Tuned> tuned;  // call-shape key -> winner
   // aldic_subpb2_set_mesh: the resident global-step mesh tables (element table, node ->
   // element lists, node kinds) in one device buffer
   char* sp2 = nullptr;
@@ -420,6 +437,8 @@ int aldic_search_grid(const int* gridx, const int* gridy, int winsize, int step,
   return ALDIC_OK;
 }
 
+static int tune_search(aldic_ctx* c, SearchArgs& a);  // the autotuner (below)
+
 int aldic_integer_search(aldic_ctx* c, const int* search, const int* gridx, const int* gridy, int winsize, int step,
                          double* x, double* y, double* u, double* v, double* phi) {
   if (!c) return ALDIC_ERR_ARG;
@@ -447,7 +466,8 @@ int aldic_integer_search(aldic_ctx* c, const int* search, const int* gridx, cons
     CK(cudaMalloc(&c->iitot, search_tot_bytes(c->M, c->N)));
     c->ii_cap = iin;
   }
-  const size_t tbytes = search_tile_bytes(c->M, c->N, winsize, step, nx, ny, search[0], search[1]);
+  // scratch for the tile kernel whenever one exists (the autotuner may choose either chunk)
+  const size_t tbytes = search_tile_bytes(c->M, c->N, winsize, step, nx, ny, search[0], search[1], 0);
   if (tbytes > c->tscratch_cap) {
     CK(cudaStreamSynchronize(c->stream));
     if (c->tscratch) CK(cudaFree(c->tscratch));
@@ -485,12 +505,173 @@ int aldic_integer_search(aldic_ctx* c, const int* search, const int* gridx, cons
   a.tot = c->iitot;
   a.tile_scratch = tbytes ? c->tscratch : nullptr;
   a.ev_start = a.ev_stop = nullptr;
+  a.impl = c->search_impl;
+  a.chunk = c->search_chunk;
+  if (c->autotune) {
+    rc = tune_search(c, a);
+    if (rc) return rc;
+  }
   if (c->prof && 2 * (c->prof_n + 1) <= (int)c->prof_ev.size()) {
     a.ev_start = c->prof_ev[2 * c->prof_n];
     a.ev_stop = c->prof_ev[2 * c->prof_n + 1];
     ++c->prof_n;
   }
   return finish(c, launch_search(a, c->stream));
+}
+
+// ------------------------------------------------------------------------ autotuner
+// The first call of each call shape (with ALDIC_OPT_AUTOTUNE on) runs every candidate
+// configuration on its own inputs, each twice (the second run timed with CUDA events on the
+// context's stream), checks that every candidate's results agree with the first's, and keeps
+// the fastest agreeing one for that shape; later calls of the shape take it without timing.
+// The call itself then runs (returns) the winner's results.  Keys bucket n by powers of two.
+static std::string shape_key(const char* kind, std::initializer_list<long long> v) {
+  std::string k = kind;
+  for (long long x : v) k += ":" + std::to_string(x);
+  return k;
+}
+
+static int log2_bucket(long long n) {
+  int b = 0;
+  while ((1LL << (b + 1)) <= n) ++b;
+  return b;
+}
+
+static int time_on_stream(aldic_ctx* c, const std::function<int()>& run, double* ms) {
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  c->launches += run();  // warm-up run (first-use attribute set-up, caches)
+  CK(cudaEventRecord(e0, c->stream));
+  c->launches += run();
+  CK(cudaEventRecord(e1, c->stream));
+  CK(cudaEventSynchronize(e1));
+  float t = 0.f;
+  CK(cudaEventElapsedTime(&t, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  CK(cudaGetLastError());
+  *ms = t;
+  return ALDIC_OK;
+}
+
+static int tune_icgn(aldic_ctx* c, IcgnArgs& a, int wmax) {
+  const std::string key = shape_key("icgn", {a.variant, a.winsize, log2_bucket(a.n)});
+  auto it = c->tuned.find(key);
+  if (it == c->tuned.end()) {
+    aldic_ctx::Tuned tn;
+    std::vector<int32_t> conv0((size_t)a.n), conv1((size_t)a.n);
+    std::vector<double> U0v((size_t)a.n * 2), U1v((size_t)a.n * 2);
+    double best = 1e300;
+    bool first = true;
+    // staging x warps per subset of the FP32 slow pass x threads per subset of the FP64
+    // re-solve x the warp pass's iteration cap
+    for (int staging = 0; staging <= 1; ++staging)
+      for (int snw : {2, 4})
+        for (int f64t : {128, 512})
+          for (int cap : {8, 16}) {
+            IcgnArgs b = a;
+            b.staging = staging;
+            b.slow_nw = snw;
+            b.fp64_threads = f64t;
+            b.warp_cap = cap;
+          double ms = 0;
+          int rc = time_on_stream(c, [&] { return launch_icgn(b, wmax, c->stream); }, &ms);
+          if (rc) return rc;
+          // results of this candidate against the first: the codes exactly (the FP64 re-solve of
+          // near-threshold tests makes them independent of summation order), U to 1e-5 px where
+          // the subset converged (a non-converged subset's U is whatever its 100 iterations left)
+          std::vector<int32_t>& cv = first ? conv0 : conv1;
+          std::vector<double>& uv = first ? U0v : U1v;
+          CK(cudaMemcpyAsync(cv.data(), b.conv, cv.size() * 4, cudaMemcpyDeviceToHost, c->stream));
+          CK(cudaMemcpyAsync(uv.data(), b.U, uv.size() * 8, cudaMemcpyDeviceToHost, c->stream));
+          CK(cudaStreamSynchronize(c->stream));
+          bool agree = true;
+          if (!first) {
+            for (size_t i = 0; i < conv0.size() && agree; ++i) agree = conv0[i] == conv1[i];
+            for (size_t i = 0; i < U0v.size() && agree; ++i) {
+              const int cd = conv0[i / 2];
+              if (cd < 1 || cd > 100) continue;
+              agree = (std::isnan(U0v[i]) && std::isnan(U1v[i])) || std::fabs(U0v[i] - U1v[i]) <= 1e-5;
+            }
+          }
+          first = false;
+          char name[80];
+          std::snprintf(name, sizeof(name), "staging%d_slow%d_fp64threads%d_cap%d", staging, snw, f64t, cap);
+          tn.ms.push_back({name, agree ? ms : -ms});
+          if (agree && ms < best) {
+            best = ms;
+            tn.a = staging;
+            tn.b = snw;
+            tn.c = cap;
+            tn.d = f64t;
+          }
+        }
+    char ch[200];
+    std::snprintf(ch, sizeof(ch),
+                  "{\"staging\": %d, \"slow_warps\": %d, \"fp64_threads\": %d, \"iteration_cap\": %d}", tn.a, tn.b,
+                  tn.d, tn.c);
+    tn.choice = ch;
+    it = c->tuned.emplace(key, tn).first;
+  }
+  a.staging = it->second.a;
+  a.slow_nw = it->second.b;
+  a.fp64_threads = it->second.d;
+  a.warp_cap = it->second.c;
+  return ALDIC_OK;
+}
+
+static int tune_search(aldic_ctx* c, SearchArgs& a) {
+  const std::string key = shape_key("search", {a.M, a.N, a.winsize, a.step, a.s0, a.s1, a.nx, a.ny});
+  auto it = c->tuned.find(key);
+  if (it == c->tuned.end()) {
+    aldic_ctx::Tuned tn;
+    const size_t n = (size_t)a.nx * a.ny;
+    std::vector<double> u0(n), v0(n), p0(n), u1(n), v1(n), p1(n);
+    double best = 1e300;
+    bool first = true;
+    struct Cand {
+      int impl, chunk;
+      const char* name;
+    };
+    const Cand cands[] = {{1, 24, "tile24"}, {1, 16, "tile16"}, {2, 0, "direct"}};
+    for (const Cand& cd : cands) {
+      if (cd.impl == 1 && (!a.tile_scratch || !search_tile_available(a.step, a.winsize, cd.chunk))) continue;
+      SearchArgs b = a;
+      b.impl = cd.impl;
+      b.chunk = cd.chunk;
+      b.ev_start = b.ev_stop = nullptr;
+      double ms = 0;
+      int rc = time_on_stream(c, [&] { return launch_search(b, c->stream); }, &ms);
+      if (rc) return rc;
+      CK(cudaMemcpyAsync((first ? u0 : u1).data(), b.u, n * 8, cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaMemcpyAsync((first ? v0 : v1).data(), b.v, n * 8, cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaMemcpyAsync((first ? p0 : p1).data(), b.phi, n * 8, cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+      bool agree = true;
+      if (!first)  // u, v identical (both implementations match the FP64 search exactly), phi to 1e-5
+        for (size_t i = 0; i < n && agree; ++i) {
+          const bool un = std::isnan(u0[i]) && std::isnan(u1[i]), vn = std::isnan(v0[i]) && std::isnan(v1[i]);
+          const bool pn = std::isnan(p0[i]) && std::isnan(p1[i]);
+          agree = (un || u0[i] == u1[i]) && (vn || v0[i] == v1[i]) && (pn || std::fabs(p0[i] - p1[i]) <= 1e-5);
+        }
+      first = false;
+      tn.ms.push_back({cd.name, agree ? ms : -ms});
+      if (agree && ms < best) {
+        best = ms;
+        tn.a = cd.impl;
+        tn.b = cd.chunk;
+      }
+    }
+    char ch[160];
+    std::snprintf(ch, sizeof(ch), "{\"search\": \"%s\"}",
+                  tn.a == 2 ? "direct" : (tn.b == 16 ? "tile16" : "tile24"));
+    tn.choice = ch;
+    it = c->tuned.emplace(key, tn).first;
+  }
+  a.impl = it->second.a;
+  a.chunk = it->second.b;
+  return ALDIC_OK;
 }
 
 static int icgn_common(aldic_ctx* c, int variant, int64_t n, const double* coords, const double* U0, int winsize,
@@ -551,6 +732,14 @@ static int icgn_common(aldic_ctx* c, int variant, int64_t n, const double* coord
   a.carry = (double*)arena_take(c, (size_t)n * 8 * sizeof(double));
   // the FP64 re-solve needs its (larger) shared-memory window; beyond that, FP32 decides alone
   a.band = icgn_smem_bytes_f64(wmax) <= 200 * 1024 ? c->fp64_band : 0.0;
+  a.staging = c->staging;
+  a.slow_nw = c->slow_nw;
+  a.slow_fp64 = c->slow_fp64;
+  a.fp64_threads = c->fp64_threads;
+  if (c->autotune && !epi) {
+    rc = tune_icgn(c, a, wmax);
+    if (rc) return rc;
+  }
   return finish(c, launch_icgn(a, wmax, c->stream));
 }
 
@@ -1111,6 +1300,110 @@ int aldic_set_iteration_cap(aldic_ctx* c, int cap) {
   if (!c) return ALDIC_ERR_ARG;
   if (cap < 1 || cap > 1000) return fail(c, ALDIC_ERR_ARG, "iteration cap %d outside 1..1000", cap);
   c->warp_cap = cap;
+  return ALDIC_OK;
+}
+
+int aldic_set_option(aldic_ctx* c, int option, int value) {
+  if (!c) return ALDIC_ERR_ARG;
+  switch (option) {
+    case ALDIC_OPT_ITERATION_CAP:
+      return aldic_set_iteration_cap(c, value);
+    case ALDIC_OPT_STAGING:
+      if (value != 0 && value != 1) return fail(c, ALDIC_ERR_ARG, "staging must be 0 or 1, not %d", value);
+      c->staging = value;
+      return ALDIC_OK;
+    case ALDIC_OPT_SLOW_WARPS:
+      if (value != 2 && value != 4) return fail(c, ALDIC_ERR_ARG, "slow-pass warps must be 2 or 4, not %d", value);
+      c->slow_nw = value;
+      return ALDIC_OK;
+    case ALDIC_OPT_SEARCH_IMPL:
+      if (value < 0 || value > 2) return fail(c, ALDIC_ERR_ARG, "search implementation must be 0, 1 or 2");
+      c->search_impl = value;
+      return ALDIC_OK;
+    case ALDIC_OPT_SEARCH_CHUNK:
+      if (value != 0 && value != 16 && value != 24) return fail(c, ALDIC_ERR_ARG, "chunk must be 0, 16 or 24");
+      c->search_chunk = value;
+      return ALDIC_OK;
+    case ALDIC_OPT_AUTOTUNE:
+      if (value != 0 && value != 1) return fail(c, ALDIC_ERR_ARG, "autotune must be 0 or 1");
+      c->autotune = value;
+      return ALDIC_OK;
+    case ALDIC_OPT_SLOW_FP64:
+      if (value != 0 && value != 1) return fail(c, ALDIC_ERR_ARG, "slow_fp64 must be 0 or 1");
+      c->slow_fp64 = value;
+      return ALDIC_OK;
+    case ALDIC_OPT_FP64_THREADS:
+      if (value != 128 && value != 256 && value != 512)
+        return fail(c, ALDIC_ERR_ARG, "FP64 threads must be 128, 256 or 512");
+      c->fp64_threads = value;
+      return ALDIC_OK;
+    default:
+      return fail(c, ALDIC_ERR_ARG, "unknown option %d", option);
+  }
+}
+
+int aldic_get_option(aldic_ctx* c, int option, int* value) {
+  if (!c || !value) return ALDIC_ERR_ARG;
+  switch (option) {
+    case ALDIC_OPT_ITERATION_CAP:
+      *value = c->warp_cap;
+      return ALDIC_OK;
+    case ALDIC_OPT_STAGING:
+      *value = c->staging;
+      return ALDIC_OK;
+    case ALDIC_OPT_SLOW_WARPS:
+      *value = c->slow_nw;
+      return ALDIC_OK;
+    case ALDIC_OPT_SEARCH_IMPL:
+      *value = c->search_impl;
+      return ALDIC_OK;
+    case ALDIC_OPT_SEARCH_CHUNK:
+      *value = c->search_chunk;
+      return ALDIC_OK;
+    case ALDIC_OPT_AUTOTUNE:
+      *value = c->autotune;
+      return ALDIC_OK;
+    case ALDIC_OPT_SLOW_FP64:
+      *value = c->slow_fp64;
+      return ALDIC_OK;
+    case ALDIC_OPT_FP64_THREADS:
+      *value = c->fp64_threads;
+      return ALDIC_OK;
+    case ALDIC_STAT_FP64_RESOLVES:
+    case ALDIC_STAT_STAGING_TIMEOUT: {
+      // counters the last aldic_local_icgn left in the context's queue block (waits for it)
+      CK(cudaSetDevice(c->device));
+      int q[16];
+      CK(cudaMemcpyAsync(q, c->qcount, sizeof(q), cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+      *value = option == ALDIC_STAT_FP64_RESOLVES ? q[4] : q[8];
+      return ALDIC_OK;
+    }
+    default:
+      return fail(c, ALDIC_ERR_ARG, "unknown option %d", option);
+  }
+}
+
+int aldic_tuning_report(aldic_ctx* c, char* buf, int64_t len) {
+  if (!c || !buf || len < 3) return ALDIC_ERR_ARG;
+  std::string r = "{";
+  bool firstk = true;
+  for (const auto& kv : c->tuned) {
+    if (!firstk) r += ", ";
+    firstk = false;
+    r += "\"" + kv.first + "\": {\"choice\": " + kv.second.choice + ", \"ms\": {";
+    bool f = true;
+    for (const auto& m : kv.second.ms) {
+      char t[96];
+      std::snprintf(t, sizeof(t), "%s\"%s\": %.4f", f ? "" : ", ", m.first.c_str(), m.second);
+      r += t;
+      f = false;
+    }
+    r += "}}";
+  }
+  r += "}";
+  if ((int64_t)r.size() + 1 > len) return fail(c, ALDIC_ERR_ARG, "report needs %zu bytes", r.size() + 1);
+  std::memcpy(buf, r.c_str(), r.size() + 1);
   return ALDIC_OK;
 }
 

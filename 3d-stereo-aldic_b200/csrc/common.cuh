@@ -227,6 +227,49 @@ __device__ __forceinline__ float2 stencil16_x2(const float* __restrict__ img, in
   return acc;
 }
 
+// The two stencils of stencil16_x2 read from a staged shared-memory tile (column-major,
+// `pitch` rows); oa, ob are the tile offsets of tap 0.  Same operations in the same order,
+// so each lane's value is bit-identical to stencil16_x2 on the image.
+__device__ __forceinline__ float2 stencil16_x2_tile(const float* tile, int pitch, int oa, int ob, float2 tr,
+                                                    float2 tc) {
+  float2 wr[4], wc[4];
+  bspline_weights_x2(tr, wr);
+  bspline_weights_x2(tc, wc);
+  const float* pa = tile + oa;
+  const float* pb = tile + ob;
+  float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    const float* qa = pa + c * pitch;
+    const float* qb = pb + c * pitch;
+    float2 col = fmul2(wr[0], make_float2(qa[0], qb[0]));
+    col = ffma2(wr[1], make_float2(qa[1], qb[1]), col);
+    col = ffma2(wr[2], make_float2(qa[2], qb[2]), col);
+    col = ffma2(wr[3], make_float2(qa[3], qb[3]), col);
+    acc = ffma2(wc[c], col, acc);
+  }
+  return acc;
+}
+
+// stencil16 on a staged tile (see stencil16_x2_tile); bit-identical to stencil16.
+__device__ __forceinline__ float stencil16_tile(const float* tile, int pitch, int o, float tr, float tc) {
+  float wr[4], wc[4];
+  bspline_weights(tr, wr);
+  bspline_weights(tc, wc);
+  const float* p = tile + o;
+  float acc = 0.f;
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    const float* q = p + c * pitch;
+    float col = wr[0] * q[0];
+    col = fmaf(wr[1], q[1], col);
+    col = fmaf(wr[2], q[2], col);
+    col = fmaf(wr[3], q[3], col);
+    acc = fmaf(wc[c], col, acc);
+  }
+  return acc;
+}
+
 // ---------------------------------------------------------------------------------
 // Reductions
 // ---------------------------------------------------------------------------------

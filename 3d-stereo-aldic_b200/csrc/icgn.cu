@@ -20,10 +20,13 @@
 // equals bf * (A_k - (C_k - mean_g * B_k) / bg) with A_k = sum J_k fn, B_k = sum J_k
 // (constant per subset) and C_k = sum J_k g (per iteration); mean_g and bg come from
 // sum g, sum g^2 over the same pass.
+#include <cstring>
+#include <mutex>
 #include <type_traits>
 
 #include "common.cuh"
 #include "kernels.h"
+#include "tma.cuh"
 
 namespace aldic {
 
@@ -280,27 +283,36 @@ __device__ __forceinline__ void push_fp64(const IcgnArgs& a, long long t, int w,
   q2[2] = masked;
 }
 
-// Whether a convergence test (funICGN.m:268-282: |b|/|b_1| < tol or |b| < tol) lies within
-// the relative band of tol where FP32 arithmetic cannot be trusted to decide as the FP64
-// reference does; such subsets are re-solved in FP64.
+// Whether a convergence test (funICGN.m:268-282: |b|/|b_1| < tol or |b| < tol) lies too close
+// to tol for FP32 arithmetic to decide it as the FP64 reference does; such subsets are
+// re-solved in FP64.  Two margins: a relative one, band * tol, and the FP32 noise of |b| at
+// this iteration, sig = step * kNoise * eps32 * (bf / bg) * sqrt(tr(H) * sum(g^2) / n) (the
+// rounding of the products J_k g and of the interpolated g, about sqrt(n) terms of size
+// |J| |g|; it grows with the iterations behind it), which dominates when |b| itself is
+// near tol.  The relative test |b| / |b_1| carries sig / |b_1|.
+constexpr double kNoise = 16.0 * 5.9604644775390625e-08;  // safety factor x 2^-24
+
 __device__ __forceinline__ bool too_close_to_call(double normRel, double normAbs, double normInit, double tol,
-                                                  double band) {
+                                                  double band, double sig) {
   if (!(band > 0)) return false;
-  const double lim = band * tol;
-  if (fabs(normAbs - tol) <= lim) return true;
-  return normInit > tol && fabs(normRel - tol) <= lim;
+  if (!(fabs(normAbs - tol) > band * tol + sig)) return true;  // NaN also goes to FP64
+  return normInit > tol && !(fabs(normRel - tol) > band * tol + sig / normInit);
+}
+
+__device__ __forceinline__ double fp32_noise(int step, double bf, double bg, double trH, double sum_g2, double n) {
+  return step * kNoise * (bf / bg) * sqrt(fmax(trH * sum_g2 / n, 0.0));
 }
 
 // The FP32 form solves queue 1 (enlarged or masked subsets and those handed over by the warp
 // passes) and moves subsets whose convergence test is too close to call to queue 2; the FP64
 // form (interpolation in the reference's own double arithmetic, FP64 sums) re-solves queue 2
 // from the initial guesses, so its decisions are the FP64 reference's.
-template <bool F64>
-__global__ void __launch_bounds__(kNT) icgn_solve_kernel(IcgnArgs a, int bucket) {
+template <bool F64, int NT>
+__global__ void __launch_bounds__(NT) icgn_solve_kernel(IcgnArgs a, int bucket) {
   using G = typename SolveSmem<F64>::G;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ SolveCtl c;
-  __shared__ double red[(kNT / 32) * 40];
+  __shared__ double red[(NT / 32) * 40];
   __shared__ double sums[40];
   const int tid = threadIdx.x;
   const FrameDev& fr = a.fr;
@@ -326,7 +338,7 @@ __global__ void __launch_bounds__(kNT) icgn_solve_kernel(IcgnArgs a, int bucket)
     // ---- load the subset window ----
     {
       const int r0 = (int)x0 - half - 1, c0 = (int)y0 - half - 1;
-      for (int p = tid; p < npx; p += kNT) {
+      for (int p = tid; p < npx; p += NT) {
         const int aa = p % W1, bb = p / W1;
         const size_t k = (size_t)(r0 + aa) + (size_t)(c0 + bb) * fr.M;
         const size_t kg = (size_t)(r0 + aa - a.crop) + (size_t)(c0 + bb - a.crop) * gM;
@@ -346,7 +358,7 @@ __global__ void __launch_bounds__(kNT) icgn_solve_kernel(IcgnArgs a, int bucket)
     if (masked) {
       // bwselect(logical(mask), seed, seed, 4) restricts f, fx, fy (funICGNQuadtree.m:83-88)
       flood_select(s.on, s.lab, W1, W1, seed, seed, 4, nullptr);
-      for (int p = tid; p < npx; p += kNT)
+      for (int p = tid; p < npx; p += NT)
         if (!s.lab[p]) {
           s.f[p] = 0.f;
           s.gx[p] = 0.f;
@@ -360,7 +372,7 @@ __global__ void __launch_bounds__(kNT) icgn_solve_kernel(IcgnArgs a, int bucket)
       double v[37];
 #pragma unroll
       for (int k = 0; k < 37; ++k) v[k] = 0.0;
-      for (int p = tid; p < npx; p += kNT) {
+      for (int p = tid; p < npx; p += NT) {
         const double dx = (double)(p % W1 - half), dy = (double)(p / W1 - half);
         const double gxv = s.gx[p], gyv = s.gy[p], f = s.f[p];
         const double J[6] = {gxv * dx, gyv * dx, gxv * dy, gyv * dy, gxv, gyv};
@@ -384,7 +396,7 @@ __global__ void __launch_bounds__(kNT) icgn_solve_kernel(IcgnArgs a, int bucket)
         }
         v[36] += fabs(f);
       }
-      block_sum<37, kNT>(v, red, sums);
+      block_sum<37, NT>(v, red, sums);
     }
     if (tid == 0) {
       double H[36];
@@ -434,10 +446,14 @@ __global__ void __launch_bounds__(kNT) icgn_solve_kernel(IcgnArgs a, int bucket)
     }
     __syncthreads();
     // ---- Gauss-Newton iterations ----
-    const int q_nt = kNT / W1, r_nt = kNT % W1;
+    const int q_nt = NT / W1, r_nt = NT % W1;
     while (true) {
       if (tid == 0) {
         int go = (!c.to_fp64 && c.step <= a.max_iter && c.normNew > a.tol && c.normAbs > a.tol) ? 1 : 0;
+        if (go && !F64 && !epi && a.slow_fp64 && c.step >= a.warp_cap) {
+          c.to_fp64 = 1;  // a long trajectory: the FP64 pass re-solves it from its initial guess
+          go = 0;
+        }
         if (go) {
           c.step += 1;
           if (quad && masked && c.step > 1) {
@@ -471,7 +487,7 @@ __global__ void __launch_bounds__(kNT) icgn_solve_kernel(IcgnArgs a, int bucket)
         G C[6] = {0, 0, 0, 0, 0, 0}, S1 = 0, S2 = 0, fg = 0;
         float ns = 0.f, nz = 0.f;
         int aa = tid % W1, bb = tid / W1;
-        for (int p = tid; p < npx; p += kNT) {
+        for (int p = tid; p < npx; p += NT) {
           G g;
           if constexpr (F64) {
             // u22 - (x0 + n5) in FP64, the reference's own interpolation arithmetic
@@ -515,16 +531,16 @@ __global__ void __launch_bounds__(kNT) icgn_solve_kernel(IcgnArgs a, int bucket)
         v[9] = nz;
         v[10] = fg;
       }
-      block_sum<11, kNT>(v, red, sums);
+      block_sum<11, NT>(v, red, sums);
       const bool run_mask = quad && (masked || sums[9] > 0);
       if (run_mask) {
         // g region: bwselect(logical(g), seed, seed, 8); if it covers the window, the
         // 8-connected f-mask region instead (funICGNQuadtree.m:170-182)
-        for (int p = tid; p < npx; p += kNT) s.tmp[p] = (s.g[p] != (G)0);
+        for (int p = tid; p < npx; p += NT) s.tmp[p] = (s.g[p] != (G)0);
         __syncthreads();
         flood_select(s.tmp, s.lab, W1, W1, seed, seed, 8, nullptr);
         int allon = 1;
-        for (int p = tid; p < npx; p += kNT) allon &= s.lab[p];
+        for (int p = tid; p < npx; p += NT) allon &= s.lab[p];
         allon = __syncthreads_and(allon);
         const uint8_t* gm = s.lab;
         if (allon) {
@@ -537,7 +553,7 @@ __global__ void __launch_bounds__(kNT) icgn_solve_kernel(IcgnArgs a, int bucket)
         __syncthreads();
         G C2[6] = {0, 0, 0, 0, 0, 0}, T1 = 0, T2 = 0;
         float tn = 0.f, gs = 0.f;
-        for (int p = tid; p < npx; p += kNT) {
+        for (int p = tid; p < npx; p += NT) {
           const G dx = (G)(p % W1 - half), dy = (G)(p / W1 - half);
           const G g = gm[p] ? s.g[p] : (G)0;
           const G ag = (G)s.gx[p] * g, bg = (G)s.gy[p] * g;
@@ -555,7 +571,7 @@ __global__ void __launch_bounds__(kNT) icgn_solve_kernel(IcgnArgs a, int bucket)
           gs += gm[p] ? 1.f : 0.f;
         }
         double v2[10] = {C2[0], C2[1], C2[2], C2[3], C2[4], C2[5], T1, T2, tn, gs};
-        block_sum<10, kNT>(v2, red, sums);
+        block_sum<10, NT>(v2, red, sums);
         if (tid == 0) c.gsum_prev = sums[9];
       }
       if (tid == 0) {
@@ -578,7 +594,10 @@ __global__ void __launch_bounds__(kNT) icgn_solve_kernel(IcgnArgs a, int bucket)
         if (c.step == 1) c.normInit = c.normNew;
         if (c.normInit > a.tol) c.normNew = c.normNew / c.normInit;
         else c.normNew = 0.0;
-        if (!F64 && !epi && too_close_to_call(c.normNew, c.normAbs, c.normInit, a.tol, a.band)) {
+        const double trH = c.H[0] + c.H[6] + c.H[11] + c.H[15] + c.H[18] + c.H[20];
+        if (!F64 && !epi &&
+            too_close_to_call(c.normNew, c.normAbs, c.normInit, a.tol, a.band,
+                              fp32_noise(c.step, c.bf, bg, trH, sums[7], n))) {
           c.to_fp64 = 1;  // leave the loop; the FP64 pass re-solves this subset
         } else if (!(c.normNew < a.tol || c.normAbs < a.tol)) {
           double dP[6];
@@ -693,10 +712,102 @@ __device__ __forceinline__ void group_sum(double (&v)[K], double* red, int gw, i
 // The one-warp pass is latency-bound on its image reads: three CTAs per SM (24 warps, 80
 // registers with a few spills) measured 12 % faster than two (128 registers, no spills);
 // four (64 registers) spill too much.
-template <int NW, bool SLOW>
-__global__ void __launch_bounds__(kWT, NW == 1 ? 3 : 2) icgn_group_kernel(IcgnArgs a) {
+// Staging (STAGED): every group owns a shared-memory buffer of box_r x box_c floats (the
+// box of a TMA tensor map over the deformed image, column-major) and an mbarrier.  Before an
+// iteration it computes the tap footprint of the warped window (0-based image rows / columns
+// from the window's corners in the pixel loop's own FP32 arithmetic, one row / column of
+// margin) and, when that leaves the staged box, loads a new box whose first row is rounded
+// down to a 16-byte boundary (the TMA rule for the innermost coordinate).  The stencil then
+// reads shared memory with the same operations as the gather path, so values are
+// bit-identical.  An iteration whose footprint exceeds the box (a large deformation) gathers
+// from the image.  A wait that outlasts kTmaWaitCycles sets qcount[8] and the group gathers
+// from the image from then on.
+constexpr long long kTmaWaitCycles = 2000000000LL;  // ~1 s at the B200 clock
+constexpr size_t kStageBytesMax = 100 * 1024;       // staging buffers of one block: two blocks per SM
+
+struct StageGeom {
+  int box_r, box_c;  // tensor-map box: rows (a multiple of 4) x columns
+  int buf_floats;    // floats per group buffer (a multiple of 32: 128-byte aligned buffers)
+};
+
+// Tap footprint (0-based image rows rlo..rhi, columns clo..chi) of the warped window of an
+// iteration: the window's corners in the pixel loop's own FP32 arithmetic, one row / column
+// of margin on each side (an interior pixel's floor() may differ from a corner's by one).
+__device__ __forceinline__ void tap_footprint(float p0, float p1, float p2, float p3, float f5, float f6, int half,
+                                              int br, int bc, int& rlo, int& rhi, int& clo, int& chi) {
+  float lxmin = 3.0e38f, lxmax = -3.0e38f, lymin = 3.0e38f, lymax = -3.0e38f;
+#pragma unroll
+  for (int cx = -1; cx <= 1; cx += 2)
+#pragma unroll
+    for (int cy = -1; cy <= 1; cy += 2) {
+      const float dxc = (float)(cx * half), dyc = (float)(cy * half);
+      const float lx = dxc + fmaf(p0, dxc, fmaf(p2, dyc, f5));
+      const float ly = dyc + fmaf(p3, dyc, fmaf(p1, dxc, f6));
+      lxmin = fminf(lxmin, lx);
+      lxmax = fmaxf(lxmax, lx);
+      lymin = fminf(lymin, ly);
+      lymax = fmaxf(lymax, ly);
+    }
+  rlo = br + (int)floorf(lxmin) - 1;
+  rhi = br + (int)floorf(lxmax) + 4;
+  clo = bc + (int)floorf(lymin) - 1;
+  chi = bc + (int)floorf(lymax) + 4;
+}
+
+// Issue the TMA load of the box that covers a footprint (its first row rounded down to a
+// 16-byte boundary) into the group's buffer; false when the footprint does not fit a box.  The
+// caller has no load in flight into this buffer.  Every thread of the group calls it.
+template <int NW>
+__device__ __forceinline__ bool stage_issue(const CUtensorMap& tmap, float* tile, int BR, int BC, int rlo, int rhi,
+                                            int clo, int chi, uint64_t& bar_mem, int bar, int gt, int& tr0,
+                                            int& tc0) {
+  const int nr0 = rlo - (((rlo % 4) + 4) % 4);
+  if (!(rhi - nr0 < BR && chi - clo < BC)) return false;
+  fence_proxy_async_shared();  // this thread's reads of the old box before the copy writes
+  group_bar<NW>(bar);
+  if (gt == 0) {
+    mbar_arrive_expect_tx(&bar_mem, (uint32_t)(BR * BC * 4));
+    tma_load_2d(tile, &tmap, nr0, clo, &bar_mem);
+  }
+  tr0 = nr0;
+  tc0 = clo;
+  return true;
+}
+
+// Wait for the group's load in flight (every thread polls; the outcome is agreed by the group).
+// On time-out the group gathers from the image from then on and flags qcount[8].
+template <int NW>
+__device__ __forceinline__ void stage_wait(bool& pending, bool& tile_ok, bool& broken, uint32_t& phase,
+                                           uint64_t& bar_mem, int& ok_mem, int bar, int gt, int* qcount) {
+  bool ok = mbar_wait(&bar_mem, phase, kTmaWaitCycles);
+  if (NW == 1) {
+    ok = __all_sync(0xffffffffu, ok);
+  } else {
+    if (gt == 0) ok_mem = 1;
+    group_bar<NW>(bar);
+    if (!ok) ok_mem = 0;
+    group_bar<NW>(bar);
+    ok = ok_mem != 0;
+  }
+  if (ok) {
+    phase ^= 1;
+    pending = false;
+    tile_ok = true;
+  } else {
+    broken = true;  // the copy may still land: the buffer is never reused
+    tile_ok = false;
+    if (gt == 0) atomicOr(qcount + 8, 1);
+  }
+}
+
+template <int NW, bool SLOW, bool STAGED>
+__global__ void __launch_bounds__(kWT, STAGED ? 2 : (NW == 1 ? 3 : 2))
+    icgn_group_kernel(IcgnArgs a, const __grid_constant__ CUtensorMap tmap, StageGeom geo) {
   constexpr int NG = kWT / (32 * NW);  // subset groups per CTA
   constexpr int GT = 32 * NW;          // threads per group
+  extern __shared__ __align__(128) float s_tiles[];
+  __shared__ __align__(8) uint64_t s_bar[NG];
+  __shared__ int s_ok[NG];
   __shared__ double s_aug[NG][72];     // 6 x 12 row-major [H | I] -> [I | H^-1]
   __shared__ double s_ab[NG][12];      // A (0..5), B (6..11)
   __shared__ double s_h[NG][21];       // packed upper triangle by rows
@@ -714,6 +825,22 @@ __global__ void __launch_bounds__(kWT, NW == 1 ? 3 : 2) icgn_group_kernel(IcgnAr
   const int count = a.qcount[SLOW ? 1 : 0];
   const int gM = fr.M - 6;
   int* next = a.qcount + (SLOW ? 3 : 2);  // work counter of this pass (zeroed with the queues)
+  // staging state of the group (replicated in its threads)
+  // the buffers start at the first 128-byte boundary of the dynamic shared memory (the launch
+  // allocates 128 bytes more than the buffers need)
+  float* tile = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(s_tiles) + 127) & ~uintptr_t(127)) +
+                (STAGED ? grp * geo.buf_floats : 0);
+  const int BR = geo.box_r, BC = geo.box_c;
+  int tr0 = 0, tc0 = 0;
+  bool tile_ok = false, pending = false, broken = false;
+  uint32_t phase = 0;
+  if (STAGED) {
+    if (gt == 0) {
+      mbar_init(&s_bar[grp], 1);
+      fence_barrier_init();
+    }
+    group_bar<NW>(bar);
+  }
   while (true) {
     // the group's next queue entry (dynamic: slow subsets do not pile up on one group)
     int qi = 0;
@@ -725,7 +852,12 @@ __global__ void __launch_bounds__(kWT, NW == 1 ? 3 : 2) icgn_group_kernel(IcgnAr
       group_bar<NW>(bar);
       qi = s_qi[grp];
     }
-    if (qi >= count) break;
+    if (qi >= count) {
+      // a copy in flight (a prefetch never used, or one that outlasted its wait) must land
+      // before the block's shared memory is released
+      if (STAGED && (pending || broken)) mbar_wait(&s_bar[grp], phase, kTmaWaitCycles);
+      break;
+    }
     const int* q = a.queue + 3 * ((SLOW ? a.n : 0) + qi);
     if (SLOW && q[2] != kSlowSubset) {
       group_bar<NW>(bar);
@@ -741,6 +873,26 @@ __global__ void __launch_bounds__(kWT, NW == 1 ? 3 : 2) icgn_group_kernel(IcgnAr
     }
     const int r0 = (int)x0 - half - 1, c0 = (int)y0 - half - 1;
     const int q_nt = GT / W1, r_nt = GT % W1;
+    if constexpr (STAGED) {
+      // prefetch the first iteration's box (P = [0 0 0 0 U0], or the carried state) so the
+      // load overlaps the set-up sums
+      if (!broken && !pending) {
+        double Pp[6] = {0.0, 0.0, 0.0, 0.0, epi ? 0.0 : a.U0[2 * t], epi ? 0.0 : a.U0[2 * t + 1]};
+        if (SLOW && a.carry)
+          for (int k = 0; k < 6; ++k) Pp[k] = a.carry[8 * t + k];
+        const double m5 = mround(Pp[4]), m6 = mround(Pp[5]);
+        if (isfinite(m5) && isfinite(m6) && fabs(m5) < 1e6 && fabs(m6) < 1e6) {
+          int rlo, rhi, clo, chi;
+          tap_footprint((float)Pp[0], (float)Pp[1], (float)Pp[2], (float)Pp[3], (float)(Pp[4] - m5),
+                        (float)(Pp[5] - m6), half, (int)(x0 + m5) - 2, (int)(y0 + m6) - 2, rlo, rhi, clo, chi);
+          const bool covered = tile_ok && rlo >= tr0 && rhi < tr0 + BR && clo >= tc0 && chi < tc0 + BC;
+          if (!covered && stage_issue<NW>(tmap, tile, BR, BC, rlo, rhi, clo, chi, s_bar[grp], bar, gt, tr0, tc0)) {
+            pending = true;
+            tile_ok = false;
+          }
+        }
+      }
+    }
     // ---- set-up sums, FP64 per lane (J = gradient x integer offset is exact in FP64), in two
     //      passes over the window to bound the live accumulators ----
     double meanf, bf, sabsf;
@@ -888,6 +1040,7 @@ __global__ void __launch_bounds__(kWT, NW == 1 ? 3 : 2) icgn_group_kernel(IcgnAr
     }
     group_bar<NW>(bar);
     // ---- Gauss-Newton iterations (control replicated in every thread) ----
+    const double trH = s_h[grp][0] + s_h[grp][6] + s_h[grp][11] + s_h[grp][15] + s_h[grp][18] + s_h[grp][20];
     double P[6] = {0.0, 0.0, 0.0, 0.0, epi ? 0.0 : a.U0[2 * t], epi ? 0.0 : a.U0[2 * t + 1]};
     double normNew = 1.0, normAbs = 1.0, normInit = 0.0, znssd = ALDIC_NAN;
     int step = 0, status = 0, requeue = -1;
@@ -899,8 +1052,10 @@ __global__ void __launch_bounds__(kWT, NW == 1 ? 3 : 2) icgn_group_kernel(IcgnAr
       step = (int)cs[7];
     }
     while (step <= a.max_iter && normNew > a.tol && normAbs > a.tol) {
-      if (!SLOW && step >= a.warp_cap) {  // a slow subset: continued by the multi-warp pass
-        requeue = kSlowSubset;
+      if (!SLOW && step >= a.warp_cap) {
+        // a long trajectory: FP32 rounding accumulates along it, so it is re-solved in FP64
+        // from its initial guess (or, for the epipolar score, continued by the multi-warp pass)
+        requeue = (a.slow_fp64 && !epi) ? kToFp64 : kSlowSubset;
         break;
       }
       step += 1;
@@ -912,6 +1067,23 @@ __global__ void __launch_bounds__(kWT, NW == 1 ? 3 : 2) icgn_group_kernel(IcgnAr
       const float p0 = (float)P[0], p1 = (float)P[1], p2 = (float)P[2], p3 = (float)P[3];
       const float f5 = (float)(P[4] - n5), f6 = (float)(P[5] - n6);
       const int br = (int)(x0 + n5) - 2, bc = (int)(y0 + n6) - 2;
+      bool use_tile = false;
+      if constexpr (STAGED) {
+        if (!broken) {
+          int rlo, rhi, clo, chi;
+          tap_footprint(p0, p1, p2, p3, f5, f6, half, br, bc, rlo, rhi, clo, chi);
+          const bool covered = rlo >= tr0 && rhi < tr0 + BR && clo >= tc0 && chi < tc0 + BC;
+          if (!(covered && (tile_ok || pending))) {
+            // the staged (or prefetched) box misses this footprint: load the one that covers it
+            if (pending) stage_wait<NW>(pending, tile_ok, broken, phase, s_bar[grp], s_ok[grp], bar, gt, a.qcount);
+            tile_ok = false;
+            if (!broken && stage_issue<NW>(tmap, tile, BR, BC, rlo, rhi, clo, chi, s_bar[grp], bar, gt, tr0, tc0))
+              pending = true;
+          }
+          if (pending) stage_wait<NW>(pending, tile_ok, broken, phase, s_bar[grp], s_ok[grp], bar, gt, a.qcount);
+          use_tile = tile_ok && !broken;
+        }
+      }
       // per-lane sums of the pixel pairs (p, p + GT) in packed FP32 with Kahan compensation
       // (s + k is the compensated total; 3 extra packed operations per term), a last unpaired
       // pixel alone; the lane totals go to FP64 before the cross-lane sums
@@ -941,8 +1113,15 @@ __global__ void __launch_bounds__(kWT, NW == 1 ? 3 : 2) icgn_group_kernel(IcgnAr
           const float2 ly = fadd2(dy, ffma2(pp3, dy, ffma2(pp1, dx, ff6)));
           const float ixa = floorf(lx.x), ixb = floorf(lx.y), iya = floorf(ly.x), iyb = floorf(ly.y);
           const float2 tr = make_float2(lx.x - ixa, lx.y - ixb), tc = make_float2(ly.x - iya, ly.y - iyb);
-          const int ia = (br + (int)ixa) + (bc + (int)iya) * fr.M, ib = (br + (int)ixb) + (bc + (int)iyb) * fr.M;
-          const float2 g = stencil16_x2(fr.def, fr.M, ia, ib, tr, tc);
+          float2 g;
+          if (STAGED && use_tile) {
+            const int oa = (br + (int)ixa - tr0) + (bc + (int)iya - tc0) * BR;
+            const int ob = (br + (int)ixb - tr0) + (bc + (int)iyb - tc0) * BR;
+            g = stencil16_x2_tile(tile, BR, oa, ob, tr, tc);
+          } else {
+            const int ia = (br + (int)ixa) + (bc + (int)iya) * fr.M, ib = (br + (int)ixb) + (bc + (int)iyb) * fr.M;
+            g = stencil16_x2(fr.def, fr.M, ia, ib, tr, tc);
+          }
           const int ka = (r0 + aa - a.crop) + (c0 + bb - a.crop) * gM;
           const int kb = (r0 + ab - a.crop) + (c0 + bbb - a.crop) * gM;
           const float2 ag = fmul2(make_float2(fr.gx[ka], fr.gx[kb]), g);
@@ -996,7 +1175,10 @@ __global__ void __launch_bounds__(kWT, NW == 1 ? 3 : 2) icgn_group_kernel(IcgnAr
           const float lx = dx + fmaf(p0, dx, fmaf(p2, dy, f5));
           const float ly = dy + fmaf(p3, dy, fmaf(p1, dx, f6));
           const float ix = floorf(lx), iy = floorf(ly);
-          const float g = stencil16(fr.def, fr.M, br + (int)ix, bc + (int)iy, lx - ix, ly - iy);
+          const float g = (STAGED && use_tile)
+                              ? stencil16_tile(tile, BR, (br + (int)ix - tr0) + (bc + (int)iy - tc0) * BR, lx - ix,
+                                               ly - iy)
+                              : stencil16(fr.def, fr.M, br + (int)ix, bc + (int)iy, lx - ix, ly - iy);
           const int kg = (r0 + aa - a.crop) + (c0 + bb - a.crop) * gM;
           const float ag = fr.gx[kg] * g, bg = fr.gy[kg] * g;
           v[0] += (double)(ag * dx);
@@ -1055,7 +1237,8 @@ __global__ void __launch_bounds__(kWT, NW == 1 ? 3 : 2) icgn_group_kernel(IcgnAr
       if (step == 1) normInit = normNew;
       if (normInit > a.tol) normNew = normNew / normInit;
       else normNew = 0.0;
-      if (!epi && too_close_to_call(normNew, normAbs, normInit, a.tol, a.band)) {
+      if (!epi && too_close_to_call(normNew, normAbs, normInit, a.tol, a.band,
+                                    fp32_noise(step, bf, bgn, trH, v[7], v[8]))) {
         requeue = kToFp64;  // the FP64 pass re-solves this subset from its initial guess
         break;
       }
@@ -1513,11 +1696,11 @@ __global__ void __launch_bounds__(kNT) subpb1_solve_kernel(Sub1Args a, int bucke
 // ================================================================================
 // host launchers
 // ================================================================================
-static int occupancy_grid(const void* fn, size_t smem) {
+static int occupancy_grid(const void* fn, size_t smem, int threads = kNT) {
   int dev = 0, sms = 148, per_sm = 1;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kNT, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem);
   if (per_sm < 1) per_sm = 1;
   return sms * per_sm;
 }
@@ -1740,10 +1923,39 @@ __global__ void __launch_bounds__(kWT, 2) subpb1_group_kernel(Sub1Args a) {
   }
 }
 
+// Tensor map of a column-major FP32 image for the staging boxes (see tma.cuh).
+bool make_tmap_2d_f32(CUtensorMap* map, const float* base, int M, int N, int box_r, int box_c) {
+  using EncodeFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+  static EncodeFn encode = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess && fn)
+      encode = reinterpret_cast<EncodeFn>(fn);
+    else
+      cudaGetLastError();
+  });
+  if (!encode || !base || M < 1 || N < 1) return false;
+  if ((reinterpret_cast<uintptr_t>(base) & 15) != 0 || ((size_t)M * sizeof(float)) % 16 != 0) return false;
+  if (box_r < 4 || box_r > 256 || box_r % 4 != 0 || box_c < 1 || box_c > 256) return false;
+  const cuuint64_t dims[2] = {(cuuint64_t)M, (cuuint64_t)N};
+  const cuuint64_t strides[1] = {(cuuint64_t)M * sizeof(float)};  // bytes between columns
+  const cuuint32_t box[2] = {(cuuint32_t)box_r, (cuuint32_t)box_c};
+  const cuuint32_t estride[2] = {1, 1};
+  const CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(base), dims, strides, box,
+                            estride, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
 int launch_icgn(const IcgnArgs& a, int wmax_enlarged, cudaStream_t st) {
   int launches = 0;
-  // counts of buckets 0 and 1, the 2 work counters, the count of bucket 2
-  cudaMemsetAsync(a.qcount, 0, 8 * sizeof(int), st);
+  // counts of buckets 0 and 1, the 2 work counters, the count of bucket 2, the staging flag
+  cudaMemsetAsync(a.qcount, 0, 16 * sizeof(int), st);
   const long long threads = a.n * 32;
   const int cb = 256;
   icgn_classify_kernel<<<(unsigned)((threads + cb - 1) / cb), cb, 0, st>>>(a);
@@ -1752,38 +1964,71 @@ int launch_icgn(const IcgnArgs& a, int wmax_enlarged, cudaStream_t st) {
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   {  // nominal-window subsets without a mask region: one warp per subset, then the slow ones
+    // TMA staging of the deformed window when the tensor map can describe the image and the
+    // per-group boxes fit two blocks per SM; the gather path otherwise
+    StageGeom geo{0, 0, 0};
+    CUtensorMap tmap;
+    std::memset(&tmap, 0, sizeof(tmap));
+    bool staged = false;
+    if (a.staging) {
+      const int W1 = a.winsize + 1;
+      geo.box_r = (W1 + 14 + 3) / 4 * 4;  // footprint W1 + 5, alignment 3, 6 rows of deformation
+      geo.box_c = W1 + 11;                // footprint W1 + 5, 6 columns of deformation
+      geo.buf_floats = (geo.box_r * geo.box_c + 31) / 32 * 32;
+      const size_t bytes = (size_t)(kWT / 32) * geo.buf_floats * sizeof(float) + 128;
+      staged = geo.box_r <= 256 && geo.box_c <= 256 && bytes <= kStageBytesMax &&
+               make_tmap_2d_f32(&tmap, a.fr.def, a.fr.M, a.fr.N, geo.box_r, geo.box_c);
+    }
+    const int snw = a.slow_nw == 4 ? 4 : kSlowNW;
+    const size_t smem1 = staged ? (size_t)(kWT / 32) * geo.buf_floats * sizeof(float) + 128 : 0;
+    const size_t smem2 = staged ? (size_t)(kWT / (32 * snw)) * geo.buf_floats * sizeof(float) + 128 : 0;
+    auto k1 = staged ? icgn_group_kernel<1, false, true> : icgn_group_kernel<1, false, false>;
+    auto k2 = snw == 4 ? (staged ? icgn_group_kernel<4, true, true> : icgn_group_kernel<4, true, false>)
+                       : (staged ? icgn_group_kernel<kSlowNW, true, true> : icgn_group_kernel<kSlowNW, true, false>);
+    if (staged) {
+      cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem1);
+      cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2);
+    }
     int per_sm = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, icgn_group_kernel<1, false>, kWT, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k1, kWT, smem1);
     long long grid = (long long)sms * (per_sm < 1 ? 1 : per_sm);
     const long long need = (a.n + 7) / 8;
     if (grid > need) grid = need;
-    icgn_group_kernel<1, false><<<(unsigned)grid, kWT, 0, st>>>(a);
-    per_sm = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, icgn_group_kernel<kSlowNW, true>, kWT, 0);
-    grid = (long long)sms * (per_sm < 1 ? 1 : per_sm);
-    const long long need_slow = (a.n + kWT / (32 * kSlowNW) - 1) / (kWT / (32 * kSlowNW));
-    if (grid > need_slow) grid = need_slow;
-    icgn_group_kernel<kSlowNW, true><<<(unsigned)grid, kWT, 0, st>>>(a);
-    launches += 2;
+    k1<<<(unsigned)grid, kWT, smem1, st>>>(a, tmap, geo);
+    ++launches;
+    if (!a.slow_fp64 || a.variant == 2) {  // the FP32 multi-warp pass continues the slow subsets
+      per_sm = 1;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k2, kWT, smem2);
+      grid = (long long)sms * (per_sm < 1 ? 1 : per_sm);
+      const long long need_slow = (a.n + kWT / (32 * snw) - 1) / (kWT / (32 * snw));
+      if (grid > need_slow) grid = need_slow;
+      k2<<<(unsigned)grid, kWT, smem2, st>>>(a, tmap, geo);
+      ++launches;
+    }
   }
   {  // enlarged / masked subsets, and those handed over by the fast kernel
     const size_t smem = icgn_smem_bytes(wmax_enlarged);
-    cudaFuncSetAttribute(icgn_solve_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    int grid = occupancy_grid((const void*)icgn_solve_kernel<false>, smem);
+    cudaFuncSetAttribute(icgn_solve_kernel<false, kNT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int grid = occupancy_grid((const void*)icgn_solve_kernel<false, kNT>, smem, kNT);
     grid = grid < 296 ? grid : 296;
     if ((long long)grid > a.n) grid = (int)a.n;
     if (grid < 1) grid = 1;
-    icgn_solve_kernel<false><<<grid, kNT, smem, st>>>(a, 1);
+    icgn_solve_kernel<false, kNT><<<grid, kNT, smem, st>>>(a, 1);
     ++launches;
   }
-  if (a.band > 0 && a.variant != 2) {  // FP64 re-solves of the subsets too close to call in FP32
+  if ((a.band > 0 || a.slow_fp64) && a.variant != 2) {
+    // FP64 re-solves: the subsets too close to call in FP32 and the long trajectories
     const size_t smem = icgn_smem_bytes_f64(wmax_enlarged);
-    cudaFuncSetAttribute(icgn_solve_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    int grid = occupancy_grid((const void*)icgn_solve_kernel<true>, smem);
-    grid = grid < 296 ? grid : 296;
+    auto kf = a.fp64_threads == 512   ? icgn_solve_kernel<true, 512>
+              : a.fp64_threads == 256 ? icgn_solve_kernel<true, 256>
+                                      : icgn_solve_kernel<true, 128>;
+    const int nt = a.fp64_threads == 512 ? 512 : (a.fp64_threads == 256 ? 256 : 128);
+    cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int grid = occupancy_grid((const void*)kf, smem, nt);
+    grid = grid < 4 * sms ? grid : 4 * sms;
     if ((long long)grid > a.n) grid = (int)a.n;
     if (grid < 1) grid = 1;
-    icgn_solve_kernel<true><<<grid, kNT, smem, st>>>(a, 2);
+    kf<<<grid, nt, smem, st>>>(a, 2);
     ++launches;
   }
   return launches;

@@ -37,13 +37,18 @@ struct IcgnArgs {
   uint8_t* mark; // n or null
   double* znssd; // n (epipolar)
   int* queue;    // 3 buckets x n x 3 ints: nominal window; enlarged / masked / handed over; FP64 re-solve
-  int* qcount;   // 5 (8 cleared): counts of buckets 0 and 1, work counters of the 2 warp-group passes,
-                 // count of bucket 2
+  int* qcount;   // 16 ints (cleared per call): counts of buckets 0 and 1, work counters of the 2
+                 // warp-group passes, count of bucket 2; [8] set when a staging wait timed out
   double* carry; // n x 8 or null: where the warp pass left a subset it hands to the multi-warp pass
-  double band;   // relative band around tol in which an FP32 convergence test is re-decided by an
-                 // FP64 re-solve of the subset (0: never)
+  double band;   // relative margin around tol, added to the FP32 noise of |b|, within which an
+                 // FP32 convergence test is re-decided by an FP64 re-solve of the subset (0: never)
+  int staging;   // 1: the warp passes stage the deformed window by TMA when they can; 0: gathers
+  int slow_nw;   // warps per subset of the FP32 pass that continues the slow subsets: 2 or 4
+  int slow_fp64; // 1: subsets still iterating after warp_cap are re-solved in FP64 (not the epipolar
+                 // variant, whose slow subsets always take the FP32 multi-warp pass)
+  int fp64_threads;  // threads per subset of the FP64 re-solve kernel: 128 or 256
 };
-constexpr double kDefaultFp64Band = 1e-2;  // default IcgnArgs::band
+constexpr double kDefaultFp64Band = 1e-3;  // default IcgnArgs::band (plus the FP32 noise of |b|)
 
 struct Sub1Args {
   FrameDev fr;
@@ -82,7 +87,12 @@ struct SearchArgs {
   double* tot;  // row-pass chunk totals (scratch, search_tot_bytes)
   void* tile_scratch;  // shared-product search scratch (search_tile_bytes bytes), or null
   cudaEvent_t ev_start, ev_stop;  // recorded around the correlation kernel when non-null
+  int impl;   // 0: the shared-product tile kernel where one exists for (step, w + 1), else direct;
+              // 1: the tile kernel (falls back to direct without one); 2: the direct kernel
+  int chunk;  // tile kernel shift columns per pass: 16 or 24 (0: the shape's default)
 };
+// Whether a shared-product tile kernel exists for (step, w + 1) and fits this device.
+bool search_tile_available(int step, int winsize, int chunk);
 
 // launchers return the number of kernels they enqueued (or < 0 on argument errors)
 int launch_normalize(const void* img, int dtype, int M, int N, int gx0, int gx1, int gy0, int gy1,
@@ -106,7 +116,7 @@ int launch_search(const SearchArgs& a, cudaStream_t st);
 // Shared-product search (search_tile.cu): scratch size (0 when the step / window pair has
 // no tile kernel), and the launcher (returns the launch count, or -1 when not available).
 constexpr int kDefaultWarpCap = 8;   // default IcgnArgs / Sub1Args warp_cap
-size_t search_tile_bytes(int M, int N, int winsize, int step, int nx, int ny, int s0, int s1);
+size_t search_tile_bytes(int M, int N, int winsize, int step, int nx, int ny, int s0, int s1, int chunk = 0);
 int launch_search_tile(const SearchArgs& a, cudaStream_t st);
 struct CamPair {
   double P[24];  // P_L = K_L [I | 0] then P_R = K_R [R | T], each 3x4 row-major

@@ -971,32 +971,42 @@ TileEntry entry() {
   return TileEntry{TileFor<ST, W1, DBC>::TI, launch_tile<ST, W1, DBC>, tile_fits<ST, W1, DBC>};
 }
 
-// The step / window pairs with a tile kernel (others use the per-subset kernel).
-bool tile_entry(int step, int W1, TileEntry* e) {
+// The step / window pairs with a tile kernel (others use the per-subset kernel), each with
+// 16 or 24 shift columns per pass (chunk); chunk 0 takes the shape's measured default (24 for
+// the stereo shape (10, 41), 16 for the others).
+bool tile_entry(int step, int W1, int chunk, TileEntry* e) {
+  if (chunk != 0 && chunk != 16 && chunk != 24) return false;
+  const bool c24 = chunk == 24 || (chunk == 0 && step == 10 && W1 == 41);
   switch (step * 1000 + W1) {
-    case 10 * 1000 + 41: *e = entry<10, 41, 24>(); return true;
-    case 16 * 1000 + 31: *e = entry<16, 31>(); return true;
-    case 16 * 1000 + 33: *e = entry<16, 33>(); return true;
-    case 12 * 1000 + 21: *e = entry<12, 21>(); return true;
-    case 9 * 1000 + 17: *e = entry<9, 17>(); return true;
-    case 8 * 1000 + 33: *e = entry<8, 33>(); return true;
+    case 10 * 1000 + 41: *e = c24 ? entry<10, 41, 24>() : entry<10, 41, 16>(); return true;
+    case 16 * 1000 + 31: *e = c24 ? entry<16, 31, 24>() : entry<16, 31>(); return true;
+    case 16 * 1000 + 33: *e = c24 ? entry<16, 33, 24>() : entry<16, 33>(); return true;
+    case 12 * 1000 + 21: *e = c24 ? entry<12, 21, 24>() : entry<12, 21>(); return true;
+    case 9 * 1000 + 17: *e = c24 ? entry<9, 17, 24>() : entry<9, 17>(); return true;
+    case 8 * 1000 + 33: *e = c24 ? entry<8, 33, 24>() : entry<8, 33>(); return true;
     default: return false;
   }
 }
 
 }  // namespace
 
-size_t search_tile_bytes(int M, int N, int winsize, int step, int nx, int ny, int s0, int s1) {
+bool search_tile_available(int step, int winsize, int chunk) {
+  TileEntry e;
+  return tile_entry(step, winsize + 1, chunk, &e) && e.fits();
+}
+
+size_t search_tile_bytes(int M, int N, int winsize, int step, int nx, int ny, int s0, int s1, int chunk) {
   const int W1 = winsize + 1;
   TileEntry e;
-  if (!tile_entry(step, W1, &e) || M < W1 || N < W1 || nx <= 0 || ny <= 0) return 0;
+  if (!tile_entry(step, W1, chunk, &e) || M < W1 || N < W1 || nx <= 0 || ny <= 0) return 0;
   return scratch_layout(M, N, W1, nx, ny, s0 + s1 + 3, nullptr, nullptr);
 }
 
 int launch_search_tile(const SearchArgs& a, cudaStream_t st) {
   const int W1 = a.winsize + 1;
   TileEntry e;
-  if (!tile_entry(a.step, W1, &e) || !a.tile_scratch || a.M < W1 || a.N < W1 || !e.fits()) return -1;
+  if (a.impl == 2 || !tile_entry(a.step, W1, a.chunk, &e) || !a.tile_scratch || a.M < W1 || a.N < W1 || !e.fits())
+    return -1;
   const int nda = a.s0 + a.s1 + 3;
   TileScratch sc;
   scratch_layout(a.M, a.N, W1, a.nx, a.ny, nda, (char*)a.tile_scratch, &sc);

@@ -112,11 +112,12 @@ int aldic_integer_search(aldic_ctx* ctx, const int* search, const int* gridx, co
  * func_quadtree/LocalICGNQuadtree.m:67-164 with func_quadtree/funICGNQuadtree.m):
  * first-order IC-GN, Gauss-Newton, maxIter 100, on the REF/DEF slots, gradients and
  * mask of the context.  H (n x 21) and markHole (n, quadtree only) may be NULL.
- * Interpolation and sums run in FP32 (Kahan-compensated per thread, FP64 across threads);
- * a subset whose convergence test |b|/|b_1| < tol or |b| < tol (func/funICGN.m:268-282)
- * falls within a relative band of tol (aldic_set_fp64_band) is re-solved from its initial
- * guess in FP64 with the reference's own interpolation arithmetic, so that its iteration
- * count, and with it U, is the FP64 reference's. */
+ * Interpolation and sums run in FP32 (Kahan-compensated per thread, FP64 across threads)
+ * for up to the iteration cap; a subset whose convergence test |b|/|b_1| < tol or |b| < tol
+ * (func/funICGN.m:268-282) falls within the FP32 noise of |b| plus a relative margin of tol
+ * (aldic_set_fp64_band) is re-solved from its initial guess in FP64 with the reference's own
+ * interpolation arithmetic, so that its iteration count, and with it U, is the FP64
+ * reference's (ALDIC_OPT_SLOW_FP64 sends every long trajectory there too). */
 int aldic_local_icgn(aldic_ctx* ctx, int variant, int64_t n, const double* coords, const double* U0, int winsize,
                      double tol, double* U, double* F, double* H, int32_t* conv, uint8_t* markHole);
 
@@ -254,9 +255,57 @@ int aldic_local_icgn_noalloc(int variant, const float* ref, const float* def, co
  * FFMA loop and a packed FFMA2 (fma.rn.f32x2) loop, the denominator the library's
  * compute-bound kernels are reported against.  Not part of the reference. */
 int aldic_measure_fp32_peak(aldic_ctx* ctx, double* tflops);
-/* Relative band around tol within which aldic_local_icgn re-decides an FP32 convergence
- * test by an FP64 re-solve of the subset (default 1e-2; 0 = never; a huge value re-solves
- * every subset in FP64).  A precision setting; not part of the reference. */
+/* Tuning options of a context (no reference counterpart; results do not depend on them
+ * beyond FP32 summation order, and with the FP64 re-solve not at all in the codes):
+ *   ALDIC_OPT_ITERATION_CAP  as aldic_set_iteration_cap (1..1000, default 8);
+ *   ALDIC_OPT_STAGING        1: the IC-GN warp passes stage each subset's deformed window in
+ *                            shared memory by TMA 2-D tile loads when the image layout allows
+ *                            (rows a multiple of 4, 16-byte aligned) and the window is small
+ *                            enough; 0 (default): they gather from the image through L1;
+ *   ALDIC_OPT_SLOW_WARPS     warps per subset of the pass that continues the subsets still
+ *                            iterating after the iteration cap: 2 (default) or 4;
+ *   ALDIC_OPT_SEARCH_IMPL    aldic_integer_search: 0 (default) the shared-product tile kernel
+ *                            where one is compiled for (step, winsize + 1), else the direct
+ *                            per-subset correlation; 1 the tile kernel; 2 the direct kernel;
+ *   ALDIC_OPT_SEARCH_CHUNK   shift columns per pass of the tile kernel: 16, 24 or 0 (the
+ *                            shape's default);
+ *   ALDIC_OPT_AUTOTUNE       1: the first call of every call shape (IC-GN: variant, winsize, n
+ *                            to a power of two; search: image, winsize, step, search region,
+ *                            grid) times every candidate of the options above on its own
+ *                            inputs, checks that all candidates' results agree, and keeps the
+ *                            fastest for that shape (that call waits for the device);
+ *                            aldic_tuning_report gives the choices and timings as JSON. */
+#define ALDIC_OPT_ITERATION_CAP 0
+#define ALDIC_OPT_STAGING 1
+#define ALDIC_OPT_SLOW_WARPS 2
+#define ALDIC_OPT_SEARCH_IMPL 3
+#define ALDIC_OPT_SEARCH_CHUNK 4
+#define ALDIC_OPT_AUTOTUNE 5
+/*   ALDIC_OPT_SLOW_FP64      1: aldic_local_icgn re-solves every subset still iterating after
+ *                            the iteration cap from its initial guess in FP64; 0 (default): an
+ *                            FP32 multi-warp pass continues them (ALDIC_OPT_SLOW_WARPS warps
+ *                            each), its convergence tests checked against the band like the
+ *                            first pass's;
+ *   ALDIC_OPT_FP64_THREADS   threads per subset of the FP64 re-solve: 128 (default), 256 or
+ *                            512. */
+#define ALDIC_OPT_SLOW_FP64 6
+#define ALDIC_OPT_FP64_THREADS 7
+/* Read-only statistics of the last aldic_local_icgn (aldic_get_option; waits for the call):
+ * subsets re-solved in FP64, and 1 if a staging load outlasted its wait (the warp group then
+ * gathered from the image). */
+#define ALDIC_STAT_FP64_RESOLVES 100
+#define ALDIC_STAT_STAGING_TIMEOUT 101
+int aldic_set_option(aldic_ctx* ctx, int option, int value);
+int aldic_get_option(aldic_ctx* ctx, int option, int* value);
+/* The autotuner's choices so far as a JSON object {shape key: {"choice": {...}, "ms":
+ * {candidate: time, ...}}} (a negative time marks a candidate whose results differed) into
+ * buf (len bytes, NUL-terminated). */
+int aldic_tuning_report(aldic_ctx* ctx, char* buf, int64_t len);
+/* Relative margin around tol within which aldic_local_icgn re-decides an FP32 convergence
+ * test by an FP64 re-solve of the subset (default 1e-3; 0 = never; a huge value re-solves
+ * every subset in FP64).  The library adds to it an estimate of the FP32 noise of |b| at that
+ * iteration (2^-24 x 16 x (bf / bg) x sqrt(tr(H) sum(g^2) / n), times the iteration number),
+ * which decides when |b| itself is near tol.  A precision setting; not part of the reference. */
 int aldic_set_fp64_band(aldic_ctx* ctx, double band);
 /* Iterations the one-warp-per-subset solver pass of aldic_local_icgn / aldic_subpb1 spends
  * on a subset before a multi-warp pass restarts it from its initial guess (default 8, 1..1000).

@@ -1164,6 +1164,146 @@ static void search_one(const double* f, const double* g, int M, int N, const int
   out5[2] = mf;
 }
 
+// The same subset as search_one for whole-grid checks, computed only where the result needs
+// it: normxcorr2's numerator and local sums over the crop (func/funIntegerSearch.m:166) in
+// the same summation order as normxcorr2() above (template column outer, row inner; zero
+// padding adds exact zeros where the overlap is partial), so u, v and phi are bit-identical
+// to search_one's; the zero threshold takes the largest denominator of the full output from
+// box sums (it enters only through eps(dmax), a power of two).  Eight consecutive shifts of
+// a crop column are independent accumulators held together (no sum is reordered).
+// out4 = [u v phi margin], margin = the crop's largest NCC minus its second largest.
+namespace {
+// num / sa / saa of crop rows d0 .. d0 + 7 of one crop column: per shift the sums over the
+// template in normxcorr2()'s order; the 8 shifts are independent accumulators.
+__attribute__((target_clones("avx2", "default"))) void crop_block8(const double* P, int Pm, const double* T, int m,
+                                                                  int row0, int col0, double* num, double* sa,
+                                                                  double* saa) {
+  double na[8] = {0, 0, 0, 0, 0, 0, 0, 0}, s1[8] = {0, 0, 0, 0, 0, 0, 0, 0}, s2[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  for (int j = 0; j < m; ++j)
+    for (int i = 0; i < m; ++i) {
+      const double t = T[i + (size_t)j * m];
+      const double* a = P + (row0 + i) + (size_t)(col0 + j) * Pm;
+      for (int k = 0; k < 8; ++k) {
+        const double v = a[k];
+        na[k] += t * v;
+        s1[k] += v;
+        s2[k] += v * v;
+      }
+    }
+  for (int k = 0; k < 8; ++k) {
+    num[k] = na[k];
+    sa[k] = s1[k];
+    saa[k] = s2[k];
+  }
+}
+}  // namespace
+
+static void search_fast_one(const double* f, const double* g, int M, int N, const int* search, int gridx_end,
+                            int gridy_end, int ii, int jj, int w, double* out4) {
+  int L = search[0], R = search[1], Uu = search[0], D = search[1];
+  if (ii - L < 1) L = ii - 1;
+  if (jj - Uu < 1) Uu = jj - 1;
+  if (ii + w + R > M) R = gridx_end - ii - w - 1;
+  if (jj + w + D > N) D = gridy_end - jj - w - 1;
+  L = std::max(L, 0);
+  R = std::max(R, 0);
+  Uu = std::max(Uu, 0);
+  D = std::max(D, 0);
+  out4[0] = out4[1] = out4[2] = out4[3] = kNaN;
+  const int m = w + 1;
+  const int ar0 = ii - L, ar1 = ii + w + R, ac0 = jj - Uu, ac1 = jj + w + D;
+  if (!(ii >= 1 && ii + w <= M && jj >= 1 && jj + w <= N && ar0 >= 1 && ar1 <= M && ac0 >= 1 && ac1 <= N)) return;
+  const int ma = ar1 - ar0 + 1, na = ac1 - ac0 + 1;
+  if (m > ma || m > na) return;
+  std::vector<double> T((size_t)m * m);
+  for (int b = 0; b < m; ++b)
+    for (int a = 0; a < m; ++a) T[a + (size_t)b * m] = f[(ii - 1 + a) + (size_t)(jj - 1 + b) * M];
+  const double mn = (double)m * m;
+  double sT = 0;
+  for (int k = 0; k < m * m; ++k) sT += T[k];
+  const double Tbar = sT / mn;
+  double ssT = 0;
+  for (int k = 0; k < m * m; ++k) ssT += (T[k] - Tbar) * (T[k] - Tbar);
+  const double denomT = std::sqrt(ssT);
+  if (!(denomT != 0)) return;
+  // window zero-padded by m - 1 on every side: full-output position (r, c) has its template
+  // top-left at padded (r, c)
+  const int R2 = ma + m - 1, C2 = na + m - 1;
+  const int Pm = ma + 2 * (m - 1), Pn = na + 2 * (m - 1);
+  std::vector<double> Pd((size_t)Pm * Pn + 8, 0.0);  // + 8: the last block of 8 shifts reads past the end
+  for (int b = 0; b < na; ++b)
+    for (int a = 0; a < ma; ++a)
+      Pd[(m - 1 + a) + (size_t)(m - 1 + b) * Pm] = g[(ar0 - 1 + a) + (size_t)(ac0 - 1 + b) * M];
+  // largest denominator over the full output (box sums: column sums, then across columns)
+  double dmax = 0;
+  {
+    std::vector<double> cs((size_t)R2 * Pn), cs2((size_t)R2 * Pn);
+    for (int c = 0; c < Pn; ++c)
+      for (int r = 0; r < R2; ++r) {
+        double s1 = 0, s2 = 0;
+        for (int i = 0; i < m; ++i) {
+          const double v = Pd[(r + i) + (size_t)c * Pm];
+          s1 += v;
+          s2 += v * v;
+        }
+        cs[r + (size_t)c * R2] = s1;
+        cs2[r + (size_t)c * R2] = s2;
+      }
+    for (int c = 0; c < C2; ++c)
+      for (int r = 0; r < R2; ++r) {
+        double s1 = 0, s2 = 0;
+        for (int j = 0; j < m; ++j) {
+          s1 += cs[r + (size_t)(c + j) * R2];
+          s2 += cs2[r + (size_t)(c + j) * R2];
+        }
+        dmax = std::max(dmax, std::fabs(denomT * std::sqrt(std::max(s2 - s1 * s1 / mn, 0.0))));
+      }
+  }
+  const double tolz = std::sqrt(matlab_eps(dmax));
+  const double one_tol = std::sqrt(matlab_eps(1.0));
+  // the crop: full-output rows / columns w-1 .. (its first and last are partial overlaps)
+  const int cr = R2 - 2 * w + 2, ccn = C2 - 2 * w + 2;
+  const int crp = (cr + 7) / 8 * 8;
+  std::vector<double> crop((size_t)cr * ccn), num(crp), sa(crp), saa(crp);
+  for (int b = 0; b < ccn; ++b) {
+    for (int d0 = 0; d0 < cr; d0 += 8)
+      crop_block8(Pd.data(), Pm, T.data(), m, w - 1 + d0, w - 1 + b, &num[d0], &sa[d0], &saa[d0]);
+    for (int a = 0; a < cr; ++a) {
+      const double nm = num[a] - sa[a] * sT / mn;
+      const double den = denomT * std::sqrt(std::max(saa[a] - sa[a] * sa[a] / mn, 0.0));
+      double c = 0;
+      if (den > tolz) c = nm / den;
+      if (std::fabs(c) - 1 > one_tol) c = 0;
+      crop[a + (size_t)b * cr] = c;
+    }
+  }
+  double xp, yp, mf;
+  findpeak(crop.data(), cr, ccn, &xp, &yp, &mf);
+  // margin: the largest crop value minus the second largest
+  double b1 = -INFINITY, b2 = -INFINITY;
+  for (double v : crop) {
+    if (v > b1) {
+      b2 = b1;
+      b1 = v;
+    } else if (v > b2) {
+      b2 = v;
+    }
+  }
+  out4[0] = yp - 2 - L;
+  out4[1] = xp - 2 - Uu;
+  out4[2] = mf;
+  out4[3] = b1 - b2;
+}
+
+void orc_search_check(const double* f, const double* g, int M, int N, const int* search, int gridx_end, int gridy_end,
+                      long n, const int* ii, const int* jj, int w, double* out, int nthreads) {
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#endif
+#pragma omp parallel for schedule(dynamic, 2)
+  for (long k = 0; k < n; ++k) search_fast_one(f, g, M, N, search, gridx_end, gridy_end, ii[k], jj[k], w, out + 4 * k);
+}
+
 // A list of grid subsets (template top-lefts ii[k], jj[k]) searched in parallel, for
 // sampled checks and CPU timing; out is n x 5 row-major [u v phi pce ppe].
 void orc_search_list(const double* f, const double* g, int M, int N, const int* search, int gridx_end,

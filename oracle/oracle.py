@@ -55,6 +55,8 @@ def lib():
                                          _dp, _dp, _dp, C.c_void_p, C.c_int]
         L.orc_search_list.argtypes = [_dp, _dp, C.c_int, C.c_int, _ip, C.c_int, C.c_int, C.c_long, _ip, _ip,
                                       C.c_int, _dp, C.c_int]
+        L.orc_search_check.argtypes = [_dp, _dp, C.c_int, C.c_int, _ip, C.c_int, C.c_int, C.c_long, _ip, _ip,
+                                       C.c_int, _dp, C.c_int]
         L.orc_findpeak.argtypes = [_dp, C.c_int, C.c_int, _dp]
         L.orc_normxcorr2.argtypes = [_dp, C.c_int, C.c_int, _dp, C.c_int, C.c_int, _dp]
         L.orc_normxcorr2.restype = C.c_int
@@ -228,6 +230,23 @@ def search_list(f, g, search, gridx_end, gridy_end, ii, jj, winsize, nthreads=0)
     lib().orc_search_list(_f64(f), _f64(g), M, N, _flat(s, np.int32), int(gridx_end), int(gridy_end), ii.size,
                           ii, jj, int(winsize), out, nthreads)
     return out.reshape(-1, 5)
+
+
+def search_check(f, g, search, gridx_end, gridy_end, ii, jj, winsize, nthreads=0):
+    """The subsets of search_list computed over the crop only (bit-identical u, v, phi; no
+    q-factors), for whole-grid checks.  Returns n x 4 [u v phi margin], margin = the crop's
+    largest NCC minus its second largest."""
+    f = np.asarray(f, dtype=np.float64)
+    M, N = f.shape
+    ii = _flat(ii, np.int32)
+    jj = _flat(jj, np.int32)
+    s = np.asarray(search, dtype=np.int32).ravel()
+    if s.size == 1:
+        s = np.array([s[0], s[0]], dtype=np.int32)
+    out = np.empty(4 * ii.size)
+    lib().orc_search_check(_f64(f), _f64(g), M, N, _flat(s, np.int32), int(gridx_end), int(gridy_end), ii.size,
+                           ii, jj, int(winsize), out, nthreads)
+    return out.reshape(-1, 4)
 
 
 def findpeak(f):

@@ -239,6 +239,112 @@ def test_local_icgn_fp64_resolve_masked(A, ctx, hole):
     assert np.abs(r64["U"] - ref["U"]).reshape(-1, 2)[ok].max() < 1e-8
 
 
+@pytest.mark.parametrize("variant", [0, 1])
+def test_local_icgn_tma_staging_matches_gathers(A, ctx, affine, variant):
+    # the warp passes' TMA-staged deformed windows give bit-identical results to the gather
+    # path (same stencil operations, shared memory instead of the image); an iteration cap of
+    # 2 also drives the multi-warp pass through its staged form
+    sc = affine
+    _load_raw(ctx, sc, mask=np.ones(sc.ref.shape) if variant == 1 else None)
+    M, N = sc.ref.shape
+    r = ctx.integer_search([10, 10], [1, M], [1, N], 30, 16)
+    coords = np.stack([r["x"].T.ravel(order="F"), r["y"].T.ravel(order="F")], 1)
+    U0 = np.nan_to_num(np.stack([r["u"].T.ravel(order="F"), r["v"].T.ravel(order="F")], 1)).ravel()
+    staging0 = ctx.get_option(A.OPT_STAGING)
+    try:
+        out = {}
+        for cap in (8, 2):
+            ctx.set_option(A.OPT_ITERATION_CAP, cap)
+            for staging in (1, 0):
+                ctx.set_option(A.OPT_STAGING, staging)
+                out[cap, staging] = ctx.local_icgn(variant, coords, U0, 30, 1e-3)
+    finally:
+        ctx.set_option(A.OPT_STAGING, staging0)
+        ctx.set_option(A.OPT_ITERATION_CAP, A.DEFAULT_ITERATION_CAP)
+    for cap in (8, 2):
+        a, b = out[cap, 1], out[cap, 0]
+        assert np.array_equal(a["conv"], b["conv"]), cap
+        assert np.array_equal(a["U"], b["U"], equal_nan=True), cap
+        assert np.array_equal(a["F"], b["F"], equal_nan=True), cap
+    with pytest.raises(Exception):
+        ctx.set_option(A.OPT_STAGING, 2)
+
+
+def test_local_icgn_tma_staging_large_deformation(A, ctx):
+    # a 6 % stretch and a 4 % contraction: boxes reload as the warp grows, and iterations whose
+    # footprint outgrows the box gather from the image; still bit-identical to the gather path
+    # and within the parity bar of the oracle
+    sc = synth.temporal_affine(M=384, N=384, n_speckles=2400, u=2.3, v=-1.4, dudx=0.06, dvdy=-0.04)
+    _load_raw(ctx, sc)
+    f, g = ctx.get_state(0), ctx.get_state(1)
+    gx, gy = ctx.get_state(2), ctx.get_state(3)
+    xs = np.arange(40, 345, 9.0)
+    X, Y = np.meshgrid(xs, xs, indexing="ij")
+    coords = np.stack([X.ravel(), Y.ravel()], 1)
+    tu, tv = sc.disp(coords[:, 0], coords[:, 1])
+    U0 = np.stack([np.round(tu), np.round(tv)], 1).ravel()
+    try:
+        ctx.set_option(A.OPT_STAGING, 0)
+        b = ctx.local_icgn(0, coords, U0, 40, 1e-3)
+        ctx.set_option(A.OPT_STAGING, 1)
+        a = ctx.local_icgn(0, coords, U0, 40, 1e-3)
+    finally:
+        ctx.set_option(A.OPT_STAGING, 0)
+    assert np.array_equal(a["conv"], b["conv"])
+    assert np.array_equal(a["U"], b["U"], equal_nan=True)
+    ref = O.local_icgn(O.Frame(f, g, None, gx, gy), coords, U0, 40, 1e-3, variant=0)
+    ok = _flag(ref["conv"])
+    assert ok.sum() > 0.9 * len(ok)
+    assert np.array_equal(a["conv"], ref["conv"])
+    assert np.abs(a["U"] - ref["U"]).reshape(-1, 2)[ok].max() < UV_TOL
+
+
+def test_autotuner_candidates_agree(A, affine):
+    # the autotuner runs every candidate (IC-GN: staging x slow-pass warps x FP64 re-solve
+    # threads x iteration cap;
+    # search: tile kernel with 24 / 16 shift columns, direct kernel) on the call's inputs and
+    # keeps the fastest of those whose results agree with the first; every candidate must
+    # agree, and the tuned call's results equal an untuned call's
+    c = A.Context(0)
+    try:
+        sc = affine
+        _load_raw(c, sc)
+        M, N = sc.ref.shape
+        r0 = c.integer_search([10, 10], [1, M], [1, N], 30, 16)
+        coords = np.stack([r0["x"].T.ravel(order="F"), r0["y"].T.ravel(order="F")], 1)
+        U0 = np.nan_to_num(np.stack([r0["u"].T.ravel(order="F"), r0["v"].T.ravel(order="F")], 1)).ravel()
+        w0 = c.local_icgn(0, coords, U0, 30, 1e-3)
+        c.set_option(A.OPT_AUTOTUNE, 1)
+        r1 = c.integer_search([10, 10], [1, M], [1, N], 30, 16)
+        w1 = c.local_icgn(0, coords, U0, 30, 1e-3)
+        w2 = c.local_icgn(0, coords, U0, 30, 1e-3)  # the cached choice, no timing
+        rep = c.tuning_report()
+        ks = [k for k in rep if k.startswith("search")]
+        ki = [k for k in rep if k.startswith("icgn")]
+        assert len(ks) == 1 and len(ki) == 1
+        assert set(rep[ks[0]]["ms"]) == {"tile24", "tile16", "direct"}
+        assert all(t > 0 for t in rep[ks[0]]["ms"].values())
+        assert len(rep[ki[0]]["ms"]) == 16 and all(t > 0 for t in rep[ki[0]]["ms"].values())
+        for k in ("u", "v"):
+            assert np.array_equal(r0[k], r1[k], equal_nan=True)
+        ok = _flag(w0["conv"])
+        for w in (w1, w2):
+            assert np.array_equal(w["conv"], w0["conv"])
+            assert np.abs(w["U"] - w0["U"]).reshape(-1, 2)[ok].max() <= 1e-5
+        # each search candidate set explicitly gives the same integer peaks
+        c.set_option(A.OPT_AUTOTUNE, 0)
+        for impl, chunk in ((1, 16), (1, 24), (2, 0)):
+            c.set_option(A.OPT_SEARCH_IMPL, impl)
+            c.set_option(A.OPT_SEARCH_CHUNK, chunk)
+            rr = c.integer_search([10, 10], [1, M], [1, N], 30, 16)
+            assert np.array_equal(rr["u"], r0["u"], equal_nan=True), (impl, chunk)
+            assert np.array_equal(rr["v"], r0["v"], equal_nan=True), (impl, chunk)
+        with pytest.raises(Exception):
+            c.set_option(A.OPT_SLOW_WARPS, 3)
+    finally:
+        c.close()
+
+
 @pytest.fixture(scope="module")
 def hole():
     return synth.plate_with_hole(size=384, hole_r=60.0, peak=2.0, sin_amp=0.3, sin_wl=120.0)
@@ -382,13 +488,23 @@ def test_local_icgn_slow_subsets_restart(A, ctx, affine):
     assert np.sum(ref["conv"] > 1) > len(coords) // 2
     try:
         ctx.set_iteration_cap(1)
-        res = ctx.local_icgn(0, coords, U0, 30, 1e-3)
+        ctx.set_option(A.OPT_SLOW_FP64, 1)
+        res = ctx.local_icgn(0, coords, U0, 30, 1e-3)  # long trajectories re-solved in FP64
+        ctx.set_option(A.OPT_SLOW_FP64, 0)
+        for nw in (2, 4):  # the FP32 multi-warp pass instead
+            ctx.set_option(A.OPT_SLOW_WARPS, nw)
+            r32 = ctx.local_icgn(0, coords, U0, 30, 1e-3)
+            assert np.mean(r32["conv"] == ref["conv"]) >= 0.98, nw
+            assert np.mean(_flag(r32["conv"]) == _flag(ref["conv"])) >= FLAG_RATE, nw
+            b32 = _flag(r32["conv"]) & _flag(ref["conv"])
+            assert np.abs(r32["U"] - ref["U"]).reshape(-1, 2)[b32].max() < UV_TOL, nw
     finally:
         ctx.set_iteration_cap(A.DEFAULT_ITERATION_CAP)
-    assert np.mean(res["conv"] == ref["conv"]) >= 0.98
-    assert np.mean(_flag(res["conv"]) == _flag(ref["conv"])) >= FLAG_RATE
-    both = _flag(res["conv"]) & _flag(ref["conv"])
-    assert np.abs(res["U"] - ref["U"]).reshape(-1, 2)[both].max() < UV_TOL
+        ctx.set_option(A.OPT_SLOW_FP64, 0)
+        ctx.set_option(A.OPT_SLOW_WARPS, 2)
+    assert np.array_equal(res["conv"], ref["conv"])
+    ok = _flag(ref["conv"])
+    assert np.abs(res["U"] - ref["U"]).reshape(-1, 2)[ok].max() < 1e-6
     with pytest.raises(Exception):
         ctx.set_iteration_cap(0)
 
