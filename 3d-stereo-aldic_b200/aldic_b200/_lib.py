@@ -27,6 +27,7 @@ DEFAULT_ITERATION_CAP = 8
 # relative band around tol in which an FP32 convergence test is re-decided in FP64, when
 # aldic_set_fp64_band has not been called (kDefaultFp64Band in csrc/kernels.h)
 DEFAULT_FP64_BAND = 1e-3
+DEFAULT_FP64_NOISE = 4.0
 
 # Every symbol the header declares, with (restype, argtypes).
 _vp = C.c_void_p
@@ -65,7 +66,7 @@ SIGNATURES = {
     "aldic_measure_fp32_peak": (_i, [_vp, C.POINTER(_d)]),
     "aldic_set_profiling": (_i, [_vp, _i]),
     "aldic_set_iteration_cap": (_i, [_vp, _i]),
-    "aldic_set_fp64_band": (_i, [_vp, _d]),
+    "aldic_set_fp64_band": (_i, [_vp, _d, _d]),
     "aldic_set_option": (_i, [_vp, _i, _i]),
     "aldic_get_option": (_i, [_vp, _i, C.POINTER(_i)]),
     "aldic_tuning_report": (_i, [_vp, C.c_char_p, _i64]),

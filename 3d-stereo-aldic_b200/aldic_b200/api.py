@@ -180,10 +180,11 @@ class Context:
         self._check(self.lib.aldic_tuning_report(self.h, buf, len(buf)), "aldic_tuning_report")
         return json.loads(buf.value.decode())
 
-    def set_fp64_band(self, band):
-        """Relative band around tol in which local_icgn re-decides a convergence test by an
-        FP64 re-solve of the subset (0 disables; a huge value re-solves every subset)."""
-        self._check(self.lib.aldic_set_fp64_band(self.h, float(band)), "aldic_set_fp64_band")
+    def set_fp64_band(self, band, noise=_lib.DEFAULT_FP64_NOISE):
+        """Margin around tol in which local_icgn re-decides a convergence test by an FP64
+        re-solve of the subset: band x tol plus noise x the FP32 noise estimate of |b| (band 0
+        disables; a huge band re-solves every subset)."""
+        self._check(self.lib.aldic_set_fp64_band(self.h, float(band), float(noise)), "aldic_set_fp64_band")
 
     def set_profiling(self, on=True):
         """Record the device time of the correlation kernel of each integer_search call."""

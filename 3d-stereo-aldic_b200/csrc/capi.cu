@@ -59,6 +59,7 @@ struct aldic_ctx {
   size_t tscratch_cap = 0;
   int warp_cap = kDefaultWarpCap;  // aldic_set_iteration_cap
   double fp64_band = kDefaultFp64Band;  // aldic_set_fp64_band
+  double fp64_noise = kDefaultFp64Noise;  // aldic_set_fp64_band
   // tuning options (aldic_set_option); with autotune on, each call shape takes the winner of
   // its first call's candidate runs instead (tuned below)
   int staging = 0;      // ALDIC_OPT_STAGING
@@ -732,6 +733,7 @@ static int icgn_common(aldic_ctx* c, int variant, int64_t n, const double* coord
   a.carry = (double*)arena_take(c, (size_t)n * 8 * sizeof(double));
   // the FP64 re-solve needs its (larger) shared-memory window; beyond that, FP32 decides alone
   a.band = icgn_smem_bytes_f64(wmax) <= 200 * 1024 ? c->fp64_band : 0.0;
+  a.noise = c->fp64_noise;
   a.staging = c->staging;
   a.slow_nw = c->slow_nw;
   a.slow_fp64 = c->slow_fp64;
@@ -1407,10 +1409,12 @@ int aldic_tuning_report(aldic_ctx* c, char* buf, int64_t len) {
   return ALDIC_OK;
 }
 
-int aldic_set_fp64_band(aldic_ctx* c, double band) {
+int aldic_set_fp64_band(aldic_ctx* c, double band, double noise) {
   if (!c) return ALDIC_ERR_ARG;
   if (!(band >= 0.0) || !(band <= 1e300)) return fail(c, ALDIC_ERR_ARG, "band %g must be >= 0 and finite", band);
+  if (!(noise >= 0.0) || !(noise <= 1e300)) return fail(c, ALDIC_ERR_ARG, "noise %g must be >= 0 and finite", noise);
   c->fp64_band = band;
+  c->fp64_noise = noise;
   return ALDIC_OK;
 }
 

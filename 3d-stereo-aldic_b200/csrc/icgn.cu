@@ -286,12 +286,10 @@ __device__ __forceinline__ void push_fp64(const IcgnArgs& a, long long t, int w,
 // Whether a convergence test (funICGN.m:268-282: |b|/|b_1| < tol or |b| < tol) lies too close
 // to tol for FP32 arithmetic to decide it as the FP64 reference does; such subsets are
 // re-solved in FP64.  Two margins: a relative one, band * tol, and the FP32 noise of |b| at
-// this iteration, sig = step * kNoise * eps32 * (bf / bg) * sqrt(tr(H) * sum(g^2) / n) (the
+// this iteration, sig = step * noise * 2^-24 * (bf / bg) * sqrt(tr(H) * sum(g^2) / n) (the
 // rounding of the products J_k g and of the interpolated g, about sqrt(n) terms of size
 // |J| |g|; it grows with the iterations behind it), which dominates when |b| itself is
 // near tol.  The relative test |b| / |b_1| carries sig / |b_1|.
-constexpr double kNoise = 16.0 * 5.9604644775390625e-08;  // safety factor x 2^-24
-
 __device__ __forceinline__ bool too_close_to_call(double normRel, double normAbs, double normInit, double tol,
                                                   double band, double sig) {
   if (!(band > 0)) return false;
@@ -299,8 +297,9 @@ __device__ __forceinline__ bool too_close_to_call(double normRel, double normAbs
   return normInit > tol && !(fabs(normRel - tol) > band * tol + sig / normInit);
 }
 
-__device__ __forceinline__ double fp32_noise(int step, double bf, double bg, double trH, double sum_g2, double n) {
-  return step * kNoise * (bf / bg) * sqrt(fmax(trH * sum_g2 / n, 0.0));
+__device__ __forceinline__ double fp32_noise(double factor, int step, double bf, double bg, double trH, double sum_g2,
+                                             double n) {
+  return step * factor * 5.9604644775390625e-08 * (bf / bg) * sqrt(fmax(trH * sum_g2 / n, 0.0));
 }
 
 // The FP32 form solves queue 1 (enlarged or masked subsets and those handed over by the warp
@@ -597,7 +596,7 @@ __global__ void __launch_bounds__(NT) icgn_solve_kernel(IcgnArgs a, int bucket) 
         const double trH = c.H[0] + c.H[6] + c.H[11] + c.H[15] + c.H[18] + c.H[20];
         if (!F64 && !epi &&
             too_close_to_call(c.normNew, c.normAbs, c.normInit, a.tol, a.band,
-                              fp32_noise(c.step, c.bf, bg, trH, sums[7], n))) {
+                              fp32_noise(a.noise, c.step, c.bf, bg, trH, sums[7], n))) {
           c.to_fp64 = 1;  // leave the loop; the FP64 pass re-solves this subset
         } else if (!(c.normNew < a.tol || c.normAbs < a.tol)) {
           double dP[6];
@@ -1238,7 +1237,7 @@ __global__ void __launch_bounds__(kWT, STAGED ? 2 : (NW == 1 ? 3 : 2))
       if (normInit > a.tol) normNew = normNew / normInit;
       else normNew = 0.0;
       if (!epi && too_close_to_call(normNew, normAbs, normInit, a.tol, a.band,
-                                    fp32_noise(step, bf, bgn, trH, v[7], v[8]))) {
+                                    fp32_noise(a.noise, step, bf, bgn, trH, v[7], v[8]))) {
         requeue = kToFp64;  // the FP64 pass re-solves this subset from its initial guess
         break;
       }

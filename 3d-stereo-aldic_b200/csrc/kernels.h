@@ -42,6 +42,7 @@ struct IcgnArgs {
   double* carry; // n x 8 or null: where the warp pass left a subset it hands to the multi-warp pass
   double band;   // relative margin around tol, added to the FP32 noise of |b|, within which an
                  // FP32 convergence test is re-decided by an FP64 re-solve of the subset (0: never)
+  double noise;  // factor of the FP32 noise estimate of |b| added to the band
   int staging;   // 1: the warp passes stage the deformed window by TMA when they can; 0: gathers
   int slow_nw;   // warps per subset of the FP32 pass that continues the slow subsets: 2 or 4
   int slow_fp64; // 1: subsets still iterating after warp_cap are re-solved in FP64 (not the epipolar
@@ -49,6 +50,7 @@ struct IcgnArgs {
   int fp64_threads;  // threads per subset of the FP64 re-solve kernel: 128 or 256
 };
 constexpr double kDefaultFp64Band = 1e-3;  // default IcgnArgs::band (plus the FP32 noise of |b|)
+constexpr double kDefaultFp64Noise = 4.0;  // default IcgnArgs::noise (2x the calibrated need)
 
 struct Sub1Args {
   FrameDev fr;

@@ -687,6 +687,7 @@ def main():
                                                "code 101) + 50 (w+1)^2 per subset solved",
                               "peak_source": "the measured FP32 peak above"},
             "tuning": pipe.tuning(),
+            "fp64_resolves": {k: c.get_option(A.STAT_FP64_RESOLVES) for k, c in pipe.ctx.items()},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_conv_all / (e2e_ms_all * 1e-3), "unit": UNIT,
                     "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"]},

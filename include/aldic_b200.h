@@ -301,12 +301,13 @@ int aldic_get_option(aldic_ctx* ctx, int option, int* value);
  * {candidate: time, ...}}} (a negative time marks a candidate whose results differed) into
  * buf (len bytes, NUL-terminated). */
 int aldic_tuning_report(aldic_ctx* ctx, char* buf, int64_t len);
-/* Relative margin around tol within which aldic_local_icgn re-decides an FP32 convergence
- * test by an FP64 re-solve of the subset (default 1e-3; 0 = never; a huge value re-solves
- * every subset in FP64).  The library adds to it an estimate of the FP32 noise of |b| at that
- * iteration (2^-24 x 16 x (bf / bg) x sqrt(tr(H) sum(g^2) / n), times the iteration number),
- * which decides when |b| itself is near tol.  A precision setting; not part of the reference. */
-int aldic_set_fp64_band(aldic_ctx* ctx, double band);
+/* Margin around tol within which aldic_local_icgn re-decides an FP32 convergence test by an
+ * FP64 re-solve of the subset: band x tol (default band 1e-3; a huge value re-solves every
+ * subset in FP64) plus noise x 2^-24 x (bf / bg) x sqrt(tr(H) sum(g^2) / n) x the iteration
+ * number, an estimate of the FP32 rounding noise of |b| (default noise 4), which decides
+ * when |b| itself is near tol.  band = 0 turns the re-solve off.  A precision setting; not
+ * part of the reference. */
+int aldic_set_fp64_band(aldic_ctx* ctx, double band, double noise);
 /* Iterations the one-warp-per-subset solver pass of aldic_local_icgn / aldic_subpb1 spends
  * on a subset before a multi-warp pass restarts it from its initial guess (default 8, 1..1000).
  * Results do not depend on it beyond FP32 summation order; it trades the tail of slow

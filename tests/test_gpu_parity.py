@@ -194,7 +194,7 @@ def test_local_icgn_fp64_resolve_band(A, ctx, affine, variant):
         ctx.set_fp64_band(1e300)
         r64 = ctx.local_icgn(variant, coords, U0, 30, 1e-3)
     finally:
-        ctx.set_fp64_band(A.DEFAULT_FP64_BAND)
+        ctx.set_fp64_band(A.DEFAULT_FP64_BAND, A.DEFAULT_FP64_NOISE)
     rd = ctx.local_icgn(variant, coords, U0, 30, 1e-3)
     both = _flag(r32["conv"]) & ok
     assert np.mean(_flag(r32["conv"]) == ok) >= FLAG_RATE
@@ -232,7 +232,7 @@ def test_local_icgn_fp64_resolve_masked(A, ctx, hole):
         ctx.set_fp64_band(1e300)
         r64 = ctx.local_icgn(1, coords, U0, 24, 1e-3)
     finally:
-        ctx.set_fp64_band(A.DEFAULT_FP64_BAND)
+        ctx.set_fp64_band(A.DEFAULT_FP64_BAND, A.DEFAULT_FP64_NOISE)
     assert np.array_equal(r64["conv"], ref["conv"])
     assert np.array_equal(r64["markHole"], ref["markHole"])
     ok = _flag(ref["conv"])
