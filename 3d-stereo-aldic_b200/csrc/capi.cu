@@ -439,9 +439,24 @@ int aldic_search_grid(const int* gridx, const int* gridy, int winsize, int step,
 }
 
 static int tune_search(aldic_ctx* c, SearchArgs& a);  // the autotuner (below)
+static int search_common(aldic_ctx* c, const int* search, const int* gridx, const int* gridy, int winsize, int step,
+                         int64_t nlist, const int32_t* list, double* x, double* y, double* u, double* v, double* phi);
 
 int aldic_integer_search(aldic_ctx* c, const int* search, const int* gridx, const int* gridy, int winsize, int step,
                          double* x, double* y, double* u, double* v, double* phi) {
+  return search_common(c, search, gridx, gridy, winsize, step, -1, nullptr, x, y, u, v, phi);
+}
+
+int aldic_integer_search_list(aldic_ctx* c, const int* search, const int* gridx, const int* gridy, int winsize,
+                              int step, int64_t n, const int32_t* list, double* x, double* y, double* u, double* v,
+                              double* phi) {
+  if (!c) return ALDIC_ERR_ARG;
+  if (n < 0 || (n > 0 && !list)) return fail(c, ALDIC_ERR_ARG, "a list of n >= 0 grid subsets is required");
+  return search_common(c, search, gridx, gridy, winsize, step, n, list, x, y, u, v, phi);
+}
+
+static int search_common(aldic_ctx* c, const int* search, const int* gridx, const int* gridy, int winsize, int step,
+                         int64_t nlist, const int32_t* list, double* x, double* y, double* u, double* v, double* phi) {
   if (!c) return ALDIC_ERR_ARG;
   int rc = need_frame(c, false);
   if (rc) return rc;
@@ -452,8 +467,9 @@ int aldic_integer_search(aldic_ctx* c, const int* search, const int* gridx, cons
   if (search[0] + search[1] > 2000) return fail(c, ALDIC_ERR_ARG, "search region too large");
   int nx, ny;
   aldic_search_grid(gridx, gridy, winsize, step, &nx, &ny);
-  const size_t n = (size_t)nx * ny;
-  if (n == 0) return ALDIC_OK;
+  const size_t ngrid = (size_t)nx * ny;
+  const size_t n = nlist >= 0 ? (size_t)nlist : ngrid;  // output slots
+  if (n == 0 || ngrid == 0) return ALDIC_OK;
   if (!x || !y || !u || !v || !phi) return fail(c, ALDIC_ERR_ARG, "output arrays required");
   const size_t iin = (size_t)(c->M + 1) * (c->N + 1);
   if (c->ii_cap < iin) {
@@ -468,7 +484,7 @@ int aldic_integer_search(aldic_ctx* c, const int* search, const int* gridx, cons
     c->ii_cap = iin;
   }
   // scratch for the tile kernel whenever one exists (the autotuner may choose either chunk)
-  const size_t tbytes = search_tile_bytes(c->M, c->N, winsize, step, nx, ny, search[0], search[1], 0);
+  const size_t tbytes = list ? 0 : search_tile_bytes(c->M, c->N, winsize, step, nx, ny, search[0], search[1], 0);
   if (tbytes > c->tscratch_cap) {
     CK(cudaStreamSynchronize(c->stream));
     if (c->tscratch) CK(cudaFree(c->tscratch));
@@ -479,8 +495,20 @@ int aldic_integer_search(aldic_ctx* c, const int* search, const int* gridx, cons
   }
   Arg ox{x, n * 8, true, nullptr}, oy{y, n * 8, true, nullptr}, ou{u, n * 8, true, nullptr};
   Arg ov{v, n * 8, true, nullptr}, op{phi, n * 8, true, nullptr};
-  rc = stage(c, {&ox, &oy, &ou, &ov, &op});
+  Arg al{list, list ? n * 4 : 0, false, nullptr};
+  rc = stage(c, {&ox, &oy, &ou, &ov, &op, &al});
   if (rc) return rc;
+  if (list) {  // every entry a grid subset
+    std::vector<int32_t> hl(n);
+    if (is_device_ptr(list)) {
+      CK(cudaMemcpyAsync(hl.data(), list, n * 4, cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+    } else {
+      std::memcpy(hl.data(), list, n * 4);
+    }
+    for (int32_t t : hl)
+      if (t < 0 || (size_t)t >= ngrid) return fail(c, ALDIC_ERR_ARG, "list entry %d outside the grid of %zu", (int)t, ngrid);
+  }
   SearchArgs a;
   a.f = c->img[0];
   a.g = c->img[1];
@@ -508,7 +536,9 @@ int aldic_integer_search(aldic_ctx* c, const int* search, const int* gridx, cons
   a.ev_start = a.ev_stop = nullptr;
   a.impl = c->search_impl;
   a.chunk = c->search_chunk;
-  if (c->autotune) {
+  a.list = (const int*)al.dev;
+  a.nlist = list ? (long long)n : 0;
+  if (c->autotune && !list) {
     rc = tune_search(c, a);
     if (rc) return rc;
   }
@@ -676,7 +706,8 @@ static int tune_search(aldic_ctx* c, SearchArgs& a) {
 }
 
 static int icgn_common(aldic_ctx* c, int variant, int64_t n, const double* coords, const double* U0, int winsize,
-                       double tol, double* U, double* F, double* H, int32_t* conv, uint8_t* mark, double* znssd) {
+                       double tol, double* U, double* F, double* H, int32_t* conv, uint8_t* mark, double* znssd,
+                       const double* F0 = nullptr) {
   int rc = need_frame(c, true);
   if (rc) return rc;
   if (n < 0) return fail(c, ALDIC_ERR_ARG, "n < 0");
@@ -705,11 +736,12 @@ static int icgn_common(aldic_ctx* c, int variant, int64_t n, const double* coord
   Arg acv{conv, conv ? (size_t)n * 4 : 0, true, nullptr};
   Arg am{mark, mark ? (size_t)n : 0, true, nullptr};
   Arg az{znssd, znssd ? (size_t)n * 8 : 0, true, nullptr};
+  Arg af0{F0, F0 ? (size_t)n * 4 * 8 : 0, false, nullptr};
   // the work queue comes from the arena too: reserve room for it with the staged arguments
   c->arena.used = 0;
-  rc = arena_reserve(c, qbytes + 4096 + (size_t)n * (2 + 2 + 2 + 4 + 21 + 1 + 1 + 8) * 8 + 8192);
+  rc = arena_reserve(c, qbytes + 4096 + (size_t)n * (2 + 2 + 2 + 4 + 4 + 21 + 1 + 1 + 8) * 8 + 8192);
   if (rc) return rc;
-  rc = stage(c, {&ac, &au0, &au, &af, &ah, &acv, &am, &az});
+  rc = stage(c, {&ac, &au0, &au, &af, &ah, &acv, &am, &az, &af0});
   if (rc) return rc;
   IcgnArgs a;
   a.fr = frame_of(c);
@@ -734,6 +766,7 @@ static int icgn_common(aldic_ctx* c, int variant, int64_t n, const double* coord
   // the FP64 re-solve needs its (larger) shared-memory window; beyond that, FP32 decides alone
   a.band = icgn_smem_bytes_f64(wmax) <= 200 * 1024 ? c->fp64_band : 0.0;
   a.noise = c->fp64_noise;
+  a.F0 = (const double*)af0.dev;
   a.staging = c->staging;
   a.slow_nw = c->slow_nw;
   a.slow_fp64 = c->slow_fp64;
@@ -751,6 +784,51 @@ int aldic_local_icgn(aldic_ctx* c, int variant, int64_t n, const double* coords,
   if (variant != ALDIC_UNIFORM && variant != ALDIC_QUADTREE) return fail(c, ALDIC_ERR_ARG, "bad variant %d", variant);
   return icgn_common(c, variant, n, coords, U0, winsize, tol, U, F, H, conv,
                      variant == ALDIC_QUADTREE ? markHole : nullptr, nullptr);
+}
+
+int aldic_local_icgn_guess(aldic_ctx* c, int variant, int64_t n, const double* coords, const double* U0,
+                           const double* F0, int winsize, double tol, double* U, double* F, double* H, int32_t* conv,
+                           uint8_t* markHole) {
+  if (!c) return ALDIC_ERR_ARG;
+  if (variant != ALDIC_UNIFORM && variant != ALDIC_QUADTREE) return fail(c, ALDIC_ERR_ARG, "bad variant %d", variant);
+  if (!F0) return fail(c, ALDIC_ERR_ARG, "F0 required (aldic_local_icgn starts from F = 0)");
+  return icgn_common(c, variant, n, coords, U0, winsize, tol, U, F, H, conv,
+                     variant == ALDIC_QUADTREE ? markHole : nullptr, nullptr, F0);
+}
+
+int aldic_subset_zncc(aldic_ctx* c, int64_t n, const double* coords, const double* U, const double* F, int winsize,
+                      double* zncc) {
+  if (!c) return ALDIC_ERR_ARG;
+  int rc = need_frame(c, false);
+  if (rc) return rc;
+  if (n < 0 || winsize < 2 || winsize > 200) return fail(c, ALDIC_ERR_ARG, "bad n or winsize");
+  if (n == 0) return ALDIC_OK;
+  if (!coords || !U || !F || !zncc) return fail(c, ALDIC_ERR_ARG, "coords, U, F and zncc are required");
+  Arg ac{coords, (size_t)n * 16, false, nullptr}, au{U, (size_t)n * 16, false, nullptr};
+  Arg af{F, (size_t)n * 32, false, nullptr}, az{zncc, (size_t)n * 8, true, nullptr};
+  rc = stage(c, {&ac, &au, &af, &az});
+  if (rc) return rc;
+  return finish(c, launch_subset_zncc(frame_of(c), n, (const double*)ac.dev, (const double*)au.dev,
+                                      (const double*)af.dev, winsize, (double*)az.dev, c->stream));
+}
+
+int aldic_net_predict(aldic_net* net, aldic_ctx* c, int64_t n, const double* coords, double* U0, double* F0) {
+  if (!c || !net) return ALDIC_ERR_ARG;
+  int rc = need_frame(c, false);
+  if (rc) return rc;
+  if (n < 0) return fail(c, ALDIC_ERR_ARG, "n < 0");
+  if (n == 0) return ALDIC_OK;
+  if (!coords || !U0 || !F0) return fail(c, ALDIC_ERR_ARG, "coords, U0 and F0 are required");
+  Arg ac{coords, (size_t)n * 16, false, nullptr}, au{U0, (size_t)n * 16, true, nullptr};
+  Arg af{F0, (size_t)n * 32, true, nullptr};
+  rc = stage(c, {&ac, &au, &af});
+  if (rc) return rc;
+  // the network runs on the context's stream so that the frame and the results are ordered
+  aldic_net_set_stream(net, c->stream);
+  rc = net_predict(net, frame_of(c), (const double*)ac.dev, n, (double*)au.dev, (double*)af.dev);
+  if (rc) return fail(c, rc, "proposal network: %s", aldic_net_last_error(net));
+  c->launches += 3 * ((n + 255) / 256);
+  return finish(c, 0);
 }
 
 int aldic_epipolar_icgn(aldic_ctx* c, int64_t n, const double* pts, int winsize, double tol, double* znssd) {

@@ -425,6 +425,8 @@ __global__ void __launch_bounds__(NT) icgn_solve_kernel(IcgnArgs a, int bucket) 
       }
       c.sabsf = sums[36];
       c.P[0] = c.P[1] = c.P[2] = c.P[3] = 0.0;
+      if (a.F0 && !epi)
+        for (int k = 0; k < 4; ++k) c.P[k] = a.F0[4 * t + k];  // a gradient initial guess (learned)
       if (epi) {
         c.P[4] = 0.0;
         c.P[5] = 0.0;
@@ -877,6 +879,8 @@ __global__ void __launch_bounds__(kWT, STAGED ? 2 : (NW == 1 ? 3 : 2))
       // load overlaps the set-up sums
       if (!broken && !pending) {
         double Pp[6] = {0.0, 0.0, 0.0, 0.0, epi ? 0.0 : a.U0[2 * t], epi ? 0.0 : a.U0[2 * t + 1]};
+        if (a.F0 && !epi)
+          for (int k = 0; k < 4; ++k) Pp[k] = a.F0[4 * t + k];
         if (SLOW && a.carry)
           for (int k = 0; k < 6; ++k) Pp[k] = a.carry[8 * t + k];
         const double m5 = mround(Pp[4]), m6 = mround(Pp[5]);
@@ -1041,6 +1045,8 @@ __global__ void __launch_bounds__(kWT, STAGED ? 2 : (NW == 1 ? 3 : 2))
     // ---- Gauss-Newton iterations (control replicated in every thread) ----
     const double trH = s_h[grp][0] + s_h[grp][6] + s_h[grp][11] + s_h[grp][15] + s_h[grp][18] + s_h[grp][20];
     double P[6] = {0.0, 0.0, 0.0, 0.0, epi ? 0.0 : a.U0[2 * t], epi ? 0.0 : a.U0[2 * t + 1]};
+    if (a.F0 && !epi)
+      for (int k = 0; k < 4; ++k) P[k] = a.F0[4 * t + k];  // a gradient initial guess (learned)
     double normNew = 1.0, normAbs = 1.0, normInit = 0.0, znssd = ALDIC_NAN;
     int step = 0, status = 0, requeue = -1;
     if (SLOW && a.carry) {  // continue from where the warp pass stopped: P, the first norm, the step
@@ -2031,6 +2037,62 @@ int launch_icgn(const IcgnArgs& a, int wmax_enlarged, cudaStream_t st) {
     ++launches;
   }
   return launches;
+}
+
+// ZNCC of a subset under the warp P = [F U]: one warp per subset, FP32 interpolation (the
+// IC-GN stencil), FP64 sums of f, f^2, g, g^2, f g over the (w+1)^2 window.
+__global__ void subset_zncc_kernel(FrameDev fr, long long n, const double* __restrict__ coords,
+                                   const double* __restrict__ U, const double* __restrict__ F, int w,
+                                   double* __restrict__ zncc) {
+  const long long t = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (t >= n) return;
+  const double x0 = mround(coords[t]), y0 = mround(coords[n + t]);
+  const double P[6] = {F[4 * t], F[4 * t + 1], F[4 * t + 2], F[4 * t + 3], U[2 * t], U[2 * t + 1]};
+  const int half = w / 2, W1 = w + 1;
+  const bool finite = isfinite(P[0]) && isfinite(P[1]) && isfinite(P[2]) && isfinite(P[3]) && isfinite(P[4]) &&
+                      isfinite(P[5]);
+  if (!finite || !window_ok(fr, x0, y0, w, w, false, 3) || warped_oob(fr, P, x0, y0, half, half)) {
+    if (lane == 0) zncc[t] = ALDIC_NAN;
+    return;
+  }
+  const double n5 = mround(P[4]), n6 = mround(P[5]);
+  const float p0 = (float)P[0], p1 = (float)P[1], p2 = (float)P[2], p3 = (float)P[3];
+  const float f5 = (float)(P[4] - n5), f6 = (float)(P[5] - n6);
+  const int br = (int)(x0 + n5) - 2, bc = (int)(y0 + n6) - 2;
+  const int r0 = (int)x0 - half - 1, c0 = (int)y0 - half - 1;
+  double sf = 0, sf2 = 0, sg = 0, sg2 = 0, sfg = 0;
+  for (int p = lane; p < W1 * W1; p += 32) {
+    const int aa = p % W1, bb = p / W1;
+    const float dx = (float)(aa - half), dy = (float)(bb - half);
+    const float lx = dx + fmaf(p0, dx, fmaf(p2, dy, f5));
+    const float ly = dy + fmaf(p3, dy, fmaf(p1, dx, f6));
+    const float ix = floorf(lx), iy = floorf(ly);
+    const double g = stencil16(fr.def, fr.M, br + (int)ix, bc + (int)iy, lx - ix, ly - iy);
+    const double f = fr.ref[(size_t)(r0 + aa) + (size_t)(c0 + bb) * fr.M];
+    sf += f;
+    sf2 += f * f;
+    sg += g;
+    sg2 += g * g;
+    sfg += f * g;
+  }
+  sf = warp_sum(sf);
+  sf2 = warp_sum(sf2);
+  sg = warp_sum(sg);
+  sg2 = warp_sum(sg2);
+  sfg = warp_sum(sfg);
+  if (lane == 0) {
+    const double m = (double)W1 * W1;
+    const double den = sqrt(fmax(sf2 - sf * sf / m, 0.0) * fmax(sg2 - sg * sg / m, 0.0));
+    zncc[t] = den > 0 ? (sfg - sf * sg / m) / den : ALDIC_NAN;
+  }
+}
+
+int launch_subset_zncc(const FrameDev& fr, long long n, const double* coords, const double* U, const double* F,
+                       int winsize, double* zncc, cudaStream_t st) {
+  if (n <= 0) return 0;
+  subset_zncc_kernel<<<(unsigned)((n * 32 + 255) / 256), 256, 0, st>>>(fr, n, coords, U, F, winsize, zncc);
+  return 1;
 }
 
 int launch_subpb1(const Sub1Args& a, int wmax_x, int wmax_y, cudaStream_t st) {

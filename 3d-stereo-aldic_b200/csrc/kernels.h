@@ -6,6 +6,8 @@
 #include <stddef.h>
 #include <stdint.h>
 
+struct aldic_net;
+
 namespace aldic {
 
 // Device-resident frame: normalised images (FP32, column-major M x N), binary mask
@@ -45,6 +47,7 @@ struct IcgnArgs {
   double noise;  // factor of the FP32 noise estimate of |b| added to the band
   int staging;   // 1: the warp passes stage the deformed window by TMA when they can; 0: gathers
   int slow_nw;   // warps per subset of the FP32 pass that continues the slow subsets: 2 or 4
+  const double* F0;  // 4n initial displacement gradients [F11 F21 F12 F22] or null (the reference's 0)
   int slow_fp64; // 1: subsets still iterating after warp_cap are re-solved in FP64 (not the epipolar
                  // variant, whose slow subsets always take the FP32 multi-warp pass)
   int fp64_threads;  // threads per subset of the FP64 re-solve kernel: 128 or 256
@@ -92,6 +95,9 @@ struct SearchArgs {
   int impl;   // 0: the shared-product tile kernel where one exists for (step, w + 1), else direct;
               // 1: the tile kernel (falls back to direct without one); 2: the direct kernel
   int chunk;  // tile kernel shift columns per pass: 16 or 24 (0: the shape's default)
+  const int* list;  // grid subsets (i + j nx) to search, or null for the whole grid; with a list
+                    // the direct kernel runs and writes the outputs compactly (slot k = list[k])
+  long long nlist;
 };
 // Whether a shared-product tile kernel exists for (step, w + 1) and fits this device.
 bool search_tile_available(int step, int winsize, int chunk);
@@ -111,6 +117,13 @@ size_t icgn_smem_bytes_f64(int w);   // FP64 re-solve kernel
 constexpr int kIcgnQueueBuckets = 3;
 size_t sub1_smem_bytes(int wx, int wy);
 int launch_icgn(const IcgnArgs& a, int wmax_enlarged, cudaStream_t st);
+// ZNCC of each subset's (w+1)^2 window of REF against DEF warped by P = [F U] (NaN where the
+// warped window leaves [3, M-2] x [3, N-2]); FP32 interpolation, FP64 sums.
+int launch_subset_zncc(const FrameDev& fr, long long n, const double* coords, const double* U, const double* F,
+                       int winsize, double* zncc, cudaStream_t st);
+// Proposal network (cnn.cu): initial guesses of n subsets on frame fr.
+int net_predict(struct ::aldic_net* net, const FrameDev& fr, const double* coords_dev, long long n, double* U0,
+                double* F0);
 int launch_subpb1(const Sub1Args& a, int wmax_x, int wmax_y, cudaStream_t st);
 size_t search_smem_bytes(int winsize, int s0, int s1);
 size_t search_tot_bytes(int M, int N);

@@ -142,6 +142,7 @@ extern "C" int aldic_local_icgn_noalloc(int variant, const float* ref, const flo
   a.carry = nullptr;  // slow subsets restart from their initial guess (no state buffer here)
   a.band = aldic::icgn_smem_bytes_f64(wmax) <= 200 * 1024 ? aldic::kDefaultFp64Band : 0.0;
   a.noise = aldic::kDefaultFp64Noise;
+  a.F0 = nullptr;
   a.staging = 0;
   a.slow_nw = 2;
   a.slow_fp64 = 0;

@@ -156,10 +156,11 @@ __global__ void __launch_bounds__(512, 1) ncc_search_kernel(SearchArgs a, int st
   const size_t ld = (size_t)a.M + 1;
   float* Tp = reinterpret_cast<float*>(smem_raw);
   float* Dt = Tp + TR * W1;
-  const long long n = (long long)a.nx * a.ny;
-  for (long long t = blockIdx.x; t < n; t += gridDim.x) {
+  const long long n = a.list ? a.nlist : (long long)a.nx * a.ny;
+  for (long long q = blockIdx.x; q < n; q += gridDim.x) {
+    const long long t = a.list ? (long long)a.list[q] : q;
     const SubsetGeom s = subset_geom(a, t);
-    const long long o = subset_out(a, t);
+    const long long o = a.list ? q : subset_out(a, t);
     if (tid == 0) {
       a.x[o] = (s.ii + s.ii + w) / 2.0;
       a.y[o] = (s.jj + s.jj + w) / 2.0;
@@ -381,15 +382,16 @@ size_t search_tot_bytes(int M, int N) {
 }
 
 int launch_search(const SearchArgs& a, cudaStream_t st) {
-  const long long n = (long long)a.nx * a.ny;
+  const long long n = a.list ? a.nlist : (long long)a.nx * a.ny;
   if (n <= 0) return 0;
   integral_cols_kernel<<<(unsigned)(((long long)(a.N + 1) * 32 + 255) / 256), 256, 0, st>>>(a.g, a.M, a.N, a.I1,
                                                                                           a.I2);
   const long long rt = (long long)(a.M + 1) * ((a.N + kRowChunk - 1) / kRowChunk);
   integral_rows_local_kernel<<<(unsigned)((rt + 255) / 256), 256, 0, st>>>(a.M, a.N, a.I1, a.I2, a.tot);
   integral_rows_fix_kernel<<<(unsigned)((rt + 255) / 256), 256, 0, st>>>(a.M, a.N, a.I1, a.I2, a.tot);
-  // shared products over tiles of subsets where a tile kernel exists for (step, w + 1)
-  const int tl = launch_search_tile(a, st);
+  // shared products over tiles of subsets where a tile kernel exists for (step, w + 1) (a
+  // subset list takes the direct kernel)
+  const int tl = a.list ? -1 : launch_search_tile(a, st);
   if (tl >= 0) return 3 + tl;
   const int na = crop_max(a.s0, a.s1);
   const int sb = strip_columns(a.winsize, na, na, 200 * 1024);

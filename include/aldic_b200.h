@@ -55,6 +55,7 @@ extern "C" {
 #define ALDIC_QUADTREE 1 /* LocalICGNQuadtree / Subpb1Quadtree (masked solvers) */
 
 typedef struct aldic_ctx aldic_ctx;
+typedef struct aldic_net aldic_net;
 
 /* Create a context on CUDA device `device`; it owns a stream and device buffers. */
 int aldic_create(aldic_ctx** ctx, int device);
@@ -249,6 +250,63 @@ int aldic_local_icgn_noalloc(int variant, const float* ref, const float* def, co
                              const float* dfdy, int M, int N, int64_t n, const double* coords, const double* U0,
                              int winsize, double tol, double* U, double* F, double* H, int32_t* conv,
                              uint8_t* markHole, void* stream);
+
+/* ------------------------------------------------- learned initial guess ------- */
+/* No counterpart in the reference, whose initial guess is the integer search
+ * (func/funIntegerSearch.m:132-180); that search stays the fallback and the judge.
+ *
+ * A proposal network: a 32 x 32 reference subset and the 64 x 64 deformed window around it
+ * (each normalised to zero mean, unit deviation) -> the subset's (u, v, du/dx, dv/dx, du/dy,
+ * dv/dy).  Four 3 x 3 stride-2 convolutions (2 -> 32 -> 32 -> 64 -> 64 channels, 64 -> 4
+ * pixels) and two fully connected layers (1024 -> 128 -> 6), ReLU between, 197 254 FP32
+ * parameters with BF16 copies; every layer, gradient and weight gradient is a BF16 x BF16 ->
+ * FP32 tensor-core GEMM (tcgen05, TMA-staged operands).  Outputs are scaled (u / 8, v / 8,
+ * gradients x 20).  Inputs x: batch x 64 x 64 x 2 BF16 (NHWC, channel 0 the reference subset
+ * in the centre of a zero canvas, channel 1 the window), device memory; targets t: batch x 6
+ * FP32 (device), scaled as the outputs.  batch a multiple of 8, at most max_batch. */
+int aldic_net_create(aldic_net** net, int device, int max_batch);
+void aldic_net_destroy(aldic_net* net);
+const char* aldic_net_last_error(const aldic_net* net);
+int aldic_net_set_stream(aldic_net* net, void* stream);
+int64_t aldic_net_launch_count(const aldic_net* net);
+/* Number of FP32 parameters and their flat layout: per layer W (rows x cols, row-major) then
+ * b: conv 32 x 24 (K = 3 x 3 x 2 taps, padded to 24 with zeros), 32 x 288, 64 x 288, 64 x 576
+ * (K ordered (ky, kx, channel)); FC 128 x 1024 (input ordered (y, x, channel) of the 4 x 4 x 64
+ * map), 16 x 128 (rows 6..15 zero, as biases 6..15). */
+int64_t aldic_net_param_count(void);
+/* Parameters in (host or device FP32); resets the Adam moments. */
+int aldic_net_set_params(aldic_net* net, const float* params);
+int aldic_net_get_params(aldic_net* net, float* params);
+/* y (device, batch x 6 FP32) = the network's scaled outputs for x. */
+int aldic_net_forward(aldic_net* net, int batch, const void* x, float* y);
+/* Gradients of the mean squared error of the outputs against t (grads: param_count FP32,
+ * host or device) and the loss (host or device, 1 FP32); waits for the device. */
+int aldic_net_gradients(aldic_net* net, int batch, const void* x, const float* t, float* grads, float* loss);
+/* One Adam step (beta 0.9 / 0.999, eps 1e-8) at learning rate lr on the batch; loss (host,
+ * optional) receives the batch's loss before the step (then the call waits). */
+int aldic_net_train_step(aldic_net* net, int batch, const void* x, const float* t, float lr, float* loss);
+/* ALDIC_OK, or ALDIC_ERR_TIMEOUT if a GEMM's bounded wait timed out since creation. */
+int aldic_net_status(aldic_net* net);
+/* Initial guesses of n subsets (coords n x 2, 1-based, rounded) on the frame of ctx (REF and
+ * DEF slots): U0 (2n interleaved) and F0 (4n, [F11 F21 F12 F22] = [du/dx dv/dx du/dy dv/dy])
+ * for aldic_local_icgn_guess.  Runs on the context's stream. */
+int aldic_net_predict(aldic_net* net, aldic_ctx* ctx, int64_t n, const double* coords, double* U0, double* F0);
+/* aldic_local_icgn from the initial guess P = [F0 U0] instead of [0 U0] (the reference starts
+ * from F = 0, func/funICGN.m:46); everything else as aldic_local_icgn. */
+int aldic_local_icgn_guess(aldic_ctx* ctx, int variant, int64_t n, const double* coords, const double* U0,
+                           const double* F0, int winsize, double tol, double* U, double* F, double* H, int32_t* conv,
+                           uint8_t* markHole);
+/* Zero-normalised cross-correlation of each subset's (winsize+1)^2 window of REF with DEF under
+ * the warp [F U] (the acceptance test of a learned initial guess); NaN where the warped window
+ * leaves the image. */
+int aldic_subset_zncc(aldic_ctx* ctx, int64_t n, const double* coords, const double* U, const double* F, int winsize,
+                      double* zncc);
+/* aldic_integer_search on the n grid subsets list[k] = i + j nX (0-based grid column i, row j)
+ * only, with the direct correlation kernel; outputs n entries each, in list order (the
+ * fallback search of the subsets a learned initial guess fails). */
+int aldic_integer_search_list(aldic_ctx* ctx, const int* search, const int* gridx, const int* gridy, int winsize,
+                              int step, int64_t n, const int32_t* list, double* x, double* y, double* u, double* v,
+                              double* phi);
 
 /* ------------------------------------------------------------- diagnostics ------- */
 /* Measured FP32 FMA throughput of the current device (TFLOP/s): the faster of a scalar

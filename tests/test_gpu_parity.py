@@ -908,3 +908,58 @@ def test_local_icgn_quadtree_driver_fill(A, ctx, hole):
     assert np.isfinite(U).all()
     assert np.array_equal(U.reshape(-1, 2)[~bad], Un.reshape(-1, 2)[~bad])
     assert np.array_equal(U, fill_quadtree(Un, coords, sc.mask))
+
+
+def test_quadtree_aldic_frame_parity(A, ctx):
+    """A reduced form of the quadtree ALDIC frame: a plate with a hole and an edge notch, the
+    GenerateQuadtreeMesh mesh refined at the mask edges, LocalICGNQuadtree, then two ADMM
+    rounds of Subpb2Quadtree + Subpb1Quadtree (func/TemporalMatch_quadtree_ST1.m:248-380);
+    every device step against the oracle on the same inputs (the device's results of the
+    step before): codes, flags and u/v within the bar, the global steps to 1e-8 px."""
+    sc = synth.plate_with_hole(seed=5, size=512, hole_r=75.0, peak=2.0, sin_amp=0.3, sin_wl=100.0)
+    M, N = sc.ref.shape
+    w, st, mu, tol = 24, 8, 1e-3, 1e-3
+    ctx.load_image_raw(0, sc.ref, [1, M], [1, N], mask=sc.mask)
+    ctx.load_image_raw(1, sc.deff, [1, M], [1, N])
+    ctx.set_mask(sc.mask)
+    ctx.compute_gradients()
+    f, g = ctx.get_state(0), ctx.get_state(1)
+    gx, gy = ctx.get_state(2), ctx.get_state(3)
+    frame = O.Frame(f, g, sc.mask, gx, gy)
+    xl = np.arange(1, M - w - st + 1, st) + w / 2.0
+    yl = np.arange(1, N - w - st + 1, st) + w / 2.0
+    X, Y = np.meshgrid(xl, yl, indexing="ij")
+    mesh0 = A.MeshSetUp(X.T, Y.T, {"winstepsize": st, "ImgSize": [M, N]})
+    mesh0["elementMinSize"] = 4
+    qmesh, _, _ = A.GenerateQuadtreeMesh(np.zeros(2 * X.size), None, sc.mask, mesh0, {"winstepsize": st, "winsize": w})
+    coords, E, dirichlet = qmesh["coordinatesFEM"], qmesh["elementsFEM"], list(qmesh["dirichlet"])
+    n = coords.shape[0]
+    assert n > X.size and E.shape[1] == 8 and np.any(E[:, 4:] > 0)  # refined, with hanging nodes
+    tu, tv = sc.disp(coords[:, 0], coords[:, 1])
+    U0 = np.stack([np.round(tu), np.round(tv)], 1).ravel()
+
+    def agree(got, ref):
+        fl = _flag(got["conv"]) & _flag(ref["conv"])
+        assert np.mean(_flag(got["conv"]) == _flag(ref["conv"])) >= FLAG_RATE
+        assert np.mean(got["conv"] == ref["conv"]) >= 0.99
+        assert fl.sum() > 0.5 * n
+        assert np.abs(got["U"] - ref["U"]).reshape(-1, 2)[fl].max() < UV_TOL
+
+    loc = ctx.local_icgn(1, coords, U0, w, tol)
+    lref = O.local_icgn(frame, coords, U0, w, tol, variant=1, nthreads=8)
+    agree(loc, lref)
+    assert np.array_equal(loc["markHole"], lref["markHole"])
+    U1 = np.where(np.isnan(loc["U"]), U0, loc["U"])
+    F1 = np.nan_to_num(loc["F"])
+    hole = np.repeat(loc["markHole"].astype(bool), 2)
+    wl = np.full((n, 2), w, dtype=np.int32)
+    beta = 1e-2 * st ** 2 * mu
+    for _ in range(2):
+        U2 = ctx.subpb2(coords, E, 2, beta, mu, U1, F1, dirichlet=dirichlet)
+        ref2 = O.subpb2_quadtree(coords, E, 2, beta, mu, U1, F1, dirichlet=dirichlet)
+        assert np.abs(U2 - ref2).max() < 1e-8
+        U2 = np.where(hole, U1, U2)
+        vdual = U2 - U1
+        s1 = ctx.subpb1(1, coords, U2, F1, vdual, mu, tol, winsize=w, winsize_list=wl)
+        agree(s1, O.subpb1(frame, coords, U2, F1, vdual, mu, tol, winsize_list=wl, variant=1, nthreads=8))
+        U1 = np.where(np.isnan(s1["U"]), U2, s1["U"])
