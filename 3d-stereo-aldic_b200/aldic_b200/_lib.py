@@ -71,6 +71,23 @@ SIGNATURES = {
     "aldic_get_option": (_i, [_vp, _i, C.POINTER(_i)]),
     "aldic_tuning_report": (_i, [_vp, C.c_char_p, _i64]),
     "aldic_profile_read": (_i, [_vp, C.POINTER(_d), C.POINTER(_i)]),
+    "aldic_net_create": (_i, [C.POINTER(_vp), _i, _i]),
+    "aldic_net_destroy": (None, [_vp]),
+    "aldic_net_last_error": (C.c_char_p, [_vp]),
+    "aldic_net_set_stream": (_i, [_vp, _vp]),
+    "aldic_net_launch_count": (_i64, [_vp]),
+    "aldic_net_param_count": (_i64, []),
+    "aldic_net_set_params": (_i, [_vp, _vp]),
+    "aldic_net_get_params": (_i, [_vp, _vp]),
+    "aldic_net_forward": (_i, [_vp, _i, _vp, _vp]),
+    "aldic_net_gradients": (_i, [_vp, _i, _vp, _vp, _vp, _vp]),
+    "aldic_net_train_step": (_i, [_vp, _i, _vp, _vp, C.c_float, _vp]),
+    "aldic_net_status": (_i, [_vp]),
+    "aldic_net_predict": (_i, [_vp, _vp, _i64, _vp, _vp, _vp]),
+    "aldic_local_icgn_guess": (_i, [_vp, _i, _i64, _vp, _vp, _vp, _i, _d, _vp, _vp, _vp, _vp, _vp]),
+    "aldic_subset_zncc": (_i, [_vp, _i64, _vp, _vp, _vp, _i, _vp]),
+    "aldic_integer_search_list": (_i, [_vp, _vp, _vp, _vp, _i, _i, _i64, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "aldic_gemm_bf16": (_i, [_vp, _i64, _vp, _i64, _i64, _i64, _i64, _vp, _i64, _i, _vp]),
     "aldic_local_icgn_noalloc": (_i, [_i, _vp, _vp, _vp, _vp, _vp, _i, _i, _i64, _vp, _vp, _i, _d, _vp, _vp, _vp,
                                       _vp, _vp, _vp]),
 }

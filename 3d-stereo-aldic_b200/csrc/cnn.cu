@@ -593,6 +593,31 @@ int aldic_net_train_step(aldic_net* net, int batch, const void* x, const float* 
   return ALDIC_OK;
 }
 
+int aldic_gemm_bf16(const void* A, int64_t lda, const void* B, int64_t ldb, int64_t M, int64_t N, int64_t K, float* C,
+                    int64_t ldc, int splits, void* stream) {
+  if (!A || !B || !C || M < 0 || N < 0 || K < 0 || lda < K || ldb < K || ldc < N || splits < 1) return ALDIC_ERR_ARG;
+  if (M == 0 || N == 0 || K == 0) return ALDIC_OK;
+  GemmArgs g;
+  g.A = A;
+  g.lda = lda;
+  g.B = B;
+  g.ldb = ldb;
+  g.M = M;
+  g.N = N;
+  g.K = K;
+  g.splits = splits;
+  g.epi.mode = splits > 1 ? kEpiAtomic : kEpiStore;
+  g.epi.c32 = C;
+  g.epi.c16 = nullptr;
+  g.epi.bias = nullptr;
+  g.epi.ldc = ldc;
+  static int* errflag = nullptr;  // the GEMM time-out flag of this entry (one per process)
+  if (!errflag && cudaMalloc(&errflag, sizeof(int)) != cudaSuccess) return ALDIC_ERR_CUDA;
+  g.epi.err = errflag;
+  if (launch_umma_gemm(g, static_cast<cudaStream_t>(stream)) < 0) return ALDIC_ERR_ARG;
+  return cudaGetLastError() == cudaSuccess ? ALDIC_OK : ALDIC_ERR_CUDA;
+}
+
 int aldic_net_status(aldic_net* net) {
   if (!net) return ALDIC_ERR_ARG;
   NK(cudaSetDevice(net->device));

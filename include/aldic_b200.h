@@ -308,6 +308,14 @@ int aldic_integer_search_list(aldic_ctx* ctx, const int* search, const int* grid
                               int step, int64_t n, const int32_t* list, double* x, double* y, double* u, double* v,
                               double* phi);
 
+/* C (M x N FP32, row pitch ldc) = A (M x K) * B (N x K)^T on the tensor cores (tcgen05, the
+ * proposal network's GEMM): A and B device BF16, row-major with pitches lda / ldb (multiples
+ * of 8), 16-byte aligned; splits > 1 adds split-K partial sums into C (which the caller
+ * zeroes).  Queued on stream (a cudaStream_t; NULL = legacy default).  A test and tuning
+ * entry; not part of the reference. */
+int aldic_gemm_bf16(const void* A, int64_t lda, const void* B, int64_t ldb, int64_t M, int64_t N, int64_t K, float* C,
+                    int64_t ldc, int splits, void* stream);
+
 /* ------------------------------------------------------------- diagnostics ------- */
 /* Measured FP32 FMA throughput of the current device (TFLOP/s): the faster of a scalar
  * FFMA loop and a packed FFMA2 (fma.rn.f32x2) loop, the denominator the library's
