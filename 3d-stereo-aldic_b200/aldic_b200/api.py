@@ -278,7 +278,9 @@ class Context:
             return out
         return {nm: bufs[nm][0].reshape((ny, nx), order="F") for nm in ("x", "y", "u", "v", "phi")}
 
-    def local_icgn(self, variant, coords, U0, winsize, tol, want_H=True, want_mark=True, out=None):
+    def local_icgn(self, variant, coords, U0, winsize, tol, want_H=True, want_mark=True, out=None, F0=None):
+        """LocalICGN / LocalICGNQuadtree loop body; F0 (4n) starts IC-GN from [F0 U0] (the
+        learned initial guess) instead of the reference's [0 U0]."""
         k = _Keep()
         n = _count(coords, 2)
         if out is None:
@@ -293,13 +295,62 @@ class Context:
             hp = k.dst(out.get("H"), np.float64, 21 * n)
             cp = k.dst(out["conv"], np.int32, n)
             mp = k.dst(out.get("mark"), np.uint8, n)
-        rc = self.lib.aldic_local_icgn(self.h, int(variant), n, k.ptr(coords, np.float64, numel=2 * n),
-                                       k.ptr(U0, np.float64, "C", numel=2 * n), int(winsize), float(tol), up, fp, hp,
-                                       cp, mp)
+        if F0 is None:
+            rc = self.lib.aldic_local_icgn(self.h, int(variant), n, k.ptr(coords, np.float64, numel=2 * n),
+                                           k.ptr(U0, np.float64, "C", numel=2 * n), int(winsize), float(tol), up, fp,
+                                           hp, cp, mp)
+        else:
+            rc = self.lib.aldic_local_icgn_guess(self.h, int(variant), n, k.ptr(coords, np.float64, numel=2 * n),
+                                                 k.ptr(U0, np.float64, "C", numel=2 * n),
+                                                 k.ptr(F0, np.float64, "C", numel=4 * n), int(winsize), float(tol), up,
+                                                 fp, hp, cp, mp)
         self._check(rc, "aldic_local_icgn")
         if out is not None:
             return out
         return dict(U=U, F=F, H=None if H is None else H.reshape((n, 21), order="F"), conv=conv, markHole=mark)
+
+    def subset_zncc(self, coords, U, F, winsize, out=None):
+        """ZNCC of each subset's window under the warp [F U] (NaN where it leaves the image)."""
+        k = _Keep()
+        n = _count(coords, 2)
+        if out is None:
+            z, zp = k.out(n, np.float64)
+        else:
+            z, zp = out, k.dst(out, np.float64, n)
+        self._check(self.lib.aldic_subset_zncc(self.h, n, k.ptr(coords, np.float64, numel=2 * n),
+                                               k.ptr(U, np.float64, "C", numel=2 * n),
+                                               k.ptr(F, np.float64, "C", numel=4 * n), int(winsize), zp),
+                    "aldic_subset_zncc")
+        return z
+
+    def integer_search_list(self, search, gridx, gridy, winsize, step, grid_idx, out=None):
+        """The integer search on the grid subsets grid_idx (i + j nX) only: dict of n-entry
+        arrays x, y, u, v, phi in list order (or the CUDA tensors of `out`)."""
+        k = _Keep()
+        s = np.asarray(search, dtype=np.int32).ravel()
+        if s.size == 1:
+            s = np.array([s[0], s[0]], dtype=np.int32)
+        n = int(grid_idx.numel() if _is_torch(grid_idx) else np.asarray(grid_idx).size)
+        names = ("x", "y", "u", "v", "phi")
+        if out is None:
+            bufs = [k.out(n, np.float64) for _ in names]
+            res, ptrs = {nm: b[0] for nm, b in zip(names, bufs)}, [b[1] for b in bufs]
+        else:
+            res, ptrs = out, [k.dst(out[nm], np.float64, n) for nm in names]
+        rc = self.lib.aldic_integer_search_list(self.h, k.ptr(s, np.int32), k.ptr(np.asarray(gridx), np.int32),
+                                                k.ptr(np.asarray(gridy), np.int32), int(winsize), int(step), n,
+                                                k.ptr(grid_idx, np.int32), *ptrs)
+        self._check(rc, "aldic_integer_search_list")
+        return res
+
+    def net_extract(self, coords, X):
+        """The proposal network's inputs of the subsets at coords into X, a CUDA bf16 tensor
+        (n, 64, 64, 2)."""
+        k = _Keep()
+        n = _count(coords, 2)
+        self._check(self.lib.aldic_net_extract(self.h, n, k.ptr(coords, np.float64, numel=2 * n),
+                                               C.c_void_p(X.data_ptr())), "aldic_net_extract")
+        return X
 
     def subpb1(self, variant, coords, UOld, FOld, vdual, mu, tol, winsize=0, winsize_list=None, HPar=None, out=None):
         """Subpb1 / Subpb1Quadtree local step.  With `out` (dict of CUDA tensors U (2n), conv (n))

@@ -19,15 +19,42 @@ from ._lib import AldicError
 SCALE = np.array([1 / 8.0, 1 / 8.0, 20.0, 20.0, 20.0, 20.0], dtype=np.float32)  # network output units
 
 
+# weight matrices (rows x cols, row-major, then rows biases) of the four 3 x 3 stride-2
+# convolutions (cols = 9 x input channels, the first padded 18 -> 24) and the two fully
+# connected layers (1024 -> 128 -> 6, the output padded to 16 rows)
+_ROWS = (32, 32, 64, 64, 128, 16)
+_COLS = (24, 288, 288, 576, 1024, 128)
+_FAN_IN = (18, 288, 288, 576, 1024, 128)
+
+
 def param_count():
     return int(_lib.load().aldic_net_param_count())
 
 
-class ProposalNet:
-    """The network on one device: FP32 parameters with BF16 copies, Adam moments and the
-    activation buffers of batches up to max_batch (a multiple of 8)."""
+def init_params(seed=0):
+    """He-normal weights (std sqrt(2 / fan-in)) and zero biases, with the padding columns of
+    the first layer and the padding rows of the output layer zero: the flat FP32 vector
+    aldic_net_set_params takes."""
+    rng = np.random.default_rng(seed)
+    parts = []
+    for l, (r, c) in enumerate(zip(_ROWS, _COLS)):
+        W = rng.normal(0.0, np.sqrt(2.0 / _FAN_IN[l]), (r, c)).astype(np.float32)
+        if l == 0:
+            W[:, _FAN_IN[0]:] = 0.0
+        if l == len(_ROWS) - 1:
+            W[6:, :] = 0.0
+        parts += [W.ravel(), np.zeros(r, dtype=np.float32)]
+    p = np.concatenate(parts)
+    if p.size != param_count():
+        raise AldicError(f"parameter layout mismatch: {p.size} vs {param_count()}")
+    return p
 
-    def __init__(self, device=0, max_batch=256):
+
+class ProposalNet:
+    """The network on one device: FP32 parameters (He-normal from `seed`) with BF16 copies,
+    Adam moments and the activation buffers of batches up to max_batch (a multiple of 8)."""
+
+    def __init__(self, device=0, max_batch=256, seed=0):
         self.lib = _lib.load()
         h = C.c_void_p()
         rc = self.lib.aldic_net_create(C.byref(h), int(device), int(max_batch))
@@ -36,6 +63,7 @@ class ProposalNet:
         self.h = h
         self.max_batch = max_batch
         self.n_params = param_count()
+        self.set_params(init_params(seed))
 
     def close(self):
         if self.h:
@@ -125,3 +153,149 @@ def gemm_bf16(A, B, C_out, splits=1, stream=0):
     if rc != _lib.ALDIC_OK:
         raise AldicError(f"aldic_gemm_bf16 failed ({rc})")
     return C_out
+
+
+# ------------------------------------------------------------------------ training
+def grid_nodes(M, N, w, step, margin=None):
+    """Subset centres (1-based) of a uniform grid whose 64 x 64 network windows stay inside the
+    image: a (2, n) float64 array, x fastest."""
+    m = 33 if margin is None else margin
+    lo = max(m, w // 2 + 4)
+    xs = np.arange(lo, M - lo + 1, step, dtype=np.float64)
+    ys = np.arange(lo, N - lo + 1, step, dtype=np.float64)
+    X, Y = np.meshgrid(xs, ys, indexing="ij")
+    return np.stack([X.ravel(order="F"), Y.ravel(order="F")], 0)
+
+
+def label_pair(ctx, pair, w=32, step=12, tol=1e-3, variant=_lib.QUADTREE, stream=None):
+    """Training samples of one speckle pair (synth_gpu.FieldPair): the network inputs of a grid
+    of subsets whose 64 x 64 windows lie inside the image and, as labels, the method's own
+    converged IC-GN results (LocalICGN's loop body started from the field's analytic
+    displacement and gradient); unconverged subsets are dropped.  Returns CUDA tensors X bf16
+    (n, 64, 64, 2) and T float32 (n, 6) (scaled outputs), made on `stream` (a torch stream;
+    a new one if None) which the current stream then waits for."""
+    import torch as T
+
+    st = stream or T.cuda.Stream()
+    ctx.set_stream(st.cuda_stream)
+    M, N = pair.M, pair.N
+    with T.cuda.stream(st):
+        ctx.load_image_raw(0, pair.ref, [1, M], [1, N], want_stats=False, shape=(M, N))
+        ctx.load_image_raw(1, pair.deff, [1, M], [1, N], want_stats=False, shape=(M, N))
+        ctx.compute_gradients()
+        nodes = grid_nodes(M, N, w, step)
+        u, v = pair.field.disp(nodes[0], nodes[1])
+        U0 = np.stack([u, v], 1).ravel()
+        F0 = pair.field.grad(nodes[0], nodes[1]).ravel()
+        r = ctx.local_icgn(variant, nodes.T, U0, w, tol, F0=F0, want_H=False, want_mark=False)
+        ok = (r["conv"] > 0) & (r["conv"] < 100)
+        crd = T.from_numpy(np.ascontiguousarray(nodes[:, ok])).to(pair.ref.device, non_blocking=False)
+        X = T.empty((int(ok.sum()), 64, 64, 2), dtype=T.bfloat16, device=pair.ref.device)
+        ctx.net_extract(crd, X)
+        lab = np.concatenate([r["U"].reshape(-1, 2)[ok], r["F"].reshape(-1, 4)[ok]], 1) * SCALE
+        Tg = T.from_numpy(lab.astype(np.float32)).to(pair.ref.device)
+    T.cuda.current_stream().wait_stream(st)
+    return X, Tg
+
+
+def train(net, X, Tgt, steps, batch=256, lr=1e-3, lr_end=1e-5, seed=0, log_every=100):
+    """Adam steps on random minibatches of (X, Tgt) with a cosine learning-rate decay from lr to
+    lr_end, on a stream of their own; returns the logged (step, loss) pairs."""
+    import torch as T
+
+    st = T.cuda.Stream(X.device)
+    st.wait_stream(T.cuda.current_stream())
+    net.set_stream(st.cuda_stream)
+    gen = T.Generator(device=X.device)
+    gen.manual_seed(seed)
+    n = X.shape[0]
+    log = []
+    with T.cuda.stream(st):
+        for k in range(steps):
+            idx = T.randint(0, n, (batch,), device=X.device, generator=gen)
+            rate = lr_end + 0.5 * (lr - lr_end) * (1 + np.cos(np.pi * k / max(steps - 1, 1)))
+            want = (k % log_every == 0) or k == steps - 1
+            loss = net.train_step(X.index_select(0, idx), Tgt.index_select(0, idx), float(rate), want_loss=want)
+            if want:
+                log.append((k, loss))
+    st.synchronize()
+    net.set_stream(None)
+    net.status()
+    return log
+
+
+# ------------------------------------------------------------------------ inference
+def search_nodes(gridx, gridy, winsize, step):
+    """Centres (1-based) of the integer-search grid subsets of funIntegerSearchWholeField
+    (func/funIntegerSearch.m:132-180): x = gridx[0] + i step + winsize / 2 and y alike, in grid
+    order t = i + j nX (MeshSetUp's coordinatesFEM order).  Returns ((2, n) float64, nX, nY)."""
+    ex, ey = gridx[1] - winsize - step, gridy[1] - winsize - step
+    nx = (ex - gridx[0]) // step + 1 if ex >= gridx[0] else 0
+    ny = (ey - gridy[0]) // step + 1 if ey >= gridy[0] else 0
+    xs = gridx[0] + step * np.arange(nx) + winsize / 2.0
+    ys = gridy[0] + step * np.arange(ny) + winsize / 2.0
+    X, Y = np.meshgrid(xs, ys, indexing="ij")
+    return np.stack([X.ravel(order="F"), Y.ravel(order="F")], 0), nx, ny
+
+
+class LearnedInit:
+    """IC-GN with the network's initial guess on the subsets of an integer-search grid, the
+    integer search as the fallback and the judge.
+
+    run() on the frame resident in ctx: the network predicts [F0 U0] for every grid subset,
+    IC-GN (LocalICGN's loop body) runs from it, and a subset whose IC-GN did not converge or
+    whose final ZNCC is below zncc_min is searched (funIntegerSearchWholeField restricted to
+    those grid subsets) and solved again from the search's [0 U0], as the reference's
+    search-initialised path would.  Everything stays on ctx's stream; the host waits once, for
+    the number of fallback subsets."""
+
+    def __init__(self, net, ctx, search, gridx, gridy, winsize, step, tol, zncc_min=0.9, variant=_lib.QUADTREE):
+        import torch as T
+
+        self.T, self.net, self.ctx = T, net, ctx
+        self.search = [int(search)] * 2 if np.ndim(search) == 0 else [int(s) for s in search]
+        self.gx, self.gy = [int(g) for g in gridx], [int(g) for g in gridy]
+        self.w, self.step, self.tol, self.zncc_min, self.variant = int(winsize), int(step), tol, zncc_min, variant
+        nodes, self.nx, self.ny = search_nodes(self.gx, self.gy, self.w, self.step)
+        self.n = n = nodes.shape[1]
+        dev = T.device("cuda", ctx.device if hasattr(ctx, "device") else T.cuda.current_device())
+        self.stream = T.cuda.Stream(dev)
+        ctx.set_stream(self.stream.cuda_stream)
+        f64 = dict(dtype=T.float64, device=dev)
+        self.coords = T.from_numpy(np.ascontiguousarray(nodes)).to(dev)
+        self.buf = {"U0": T.empty(2 * n, **f64), "F0": T.empty(4 * n, **f64), "U": T.empty(2 * n, **f64),
+                    "F": T.empty(4 * n, **f64), "conv": T.empty(n, dtype=T.int32, device=dev),
+                    "zncc": T.empty(n, **f64), "fallback": T.zeros(n, dtype=T.bool, device=dev)}
+        self.n_fallback = 0
+
+    def run(self):
+        """One frame; returns the number of fallback subsets."""
+        T, ctx, b, n = self.T, self.ctx, self.buf, self.n
+        with T.cuda.stream(self.stream):
+            self.net.predict(ctx, self.coords, b)
+            ctx.local_icgn(self.variant, self.coords, b["U0"], self.w, self.tol, want_H=False, want_mark=False,
+                           out=b, F0=b["F0"])
+            ctx.subset_zncc(self.coords, b["U"], b["F"], self.w, out=b["zncc"])
+            c = b["conv"]
+            bad = (c < 1) | (c > 100) | ~(b["zncc"] >= self.zncc_min)
+            b["fallback"].copy_(bad)
+            idx = T.nonzero(bad).flatten()
+            nf = int(idx.numel())  # the host's one wait
+            if nf:
+                dev = self.coords.device
+                f64 = dict(dtype=T.float64, device=dev)
+                il = idx.to(T.int32)
+                r = {k: T.empty(nf, **f64) for k in ("x", "y", "u", "v", "phi")}
+                ctx.integer_search_list(self.search, self.gx, self.gy, self.w, self.step, il, out=r)
+                U0f = T.nan_to_num(T.stack([r["u"], r["v"]], 1), nan=0.0).reshape(-1).contiguous()
+                crd = self.coords.index_select(1, idx).contiguous()
+                o = {"U": T.empty(2 * nf, **f64), "F": T.empty(4 * nf, **f64),
+                     "conv": T.empty(nf, dtype=T.int32, device=dev)}
+                ctx.local_icgn(self.variant, crd, U0f, self.w, self.tol, want_H=False, want_mark=False, out=o)
+                b["U"].view(n, 2)[idx] = o["U"].view(nf, 2)
+                b["F"].view(n, 4)[idx] = o["F"].view(nf, 4)
+                b["conv"][idx] = o["conv"]
+                b["U0"].view(n, 2)[idx] = U0f.view(nf, 2)
+                b["F0"].view(n, 4)[idx] = 0.0
+        self.n_fallback = nf
+        return nf

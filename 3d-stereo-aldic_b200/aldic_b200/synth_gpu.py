@@ -121,3 +121,107 @@ def stereo_sequence(frames=50, M=4096, N=3000, seed=4, f=4000.0, baseline=300.0,
     K1 = np.array([[f, 0, (M + 1) / 2.0], [0, f, (N + 1) / 2.0], [0, 0, 1.0]])
     return SequenceScene(L=Ls, R=Rs, M=M, N=N, camL=camL, camR=camR, KL=K1, KR=K1, R_rl=R_rl, T_rl=T_rl, Z=Z,
                          params=params)
+
+
+@dataclass
+class FieldPair:
+    ref: object        # flat uint8 CUDA tensor, M * N, x fastest
+    deff: object
+    M: int
+    N: int
+    field: "SmoothField"
+
+
+class SmoothField:
+    """u(x, y) = u0 + sum_k a_k sin(2 pi (kx_k x + ky_k y) + phi_k) (and v alike): a random offset
+    plus low-frequency sinusoids, scaled so that |u|, |v| <= umax and every displacement
+    gradient <= gmax everywhere (the bounds hold term by term)."""
+
+    def __init__(self, rng, umax=12.0, gmax=0.05, waves=3, wl=(300.0, 1200.0)):
+        self.terms = []
+        budget_u, budget_g = umax, gmax
+        off = rng.uniform(-0.5, 0.5, 2) * umax
+        self.off = off
+        for comp in range(2):
+            ts = []
+            ru = umax - abs(off[comp])
+            for _ in range(waves):
+                lam = rng.uniform(*wl)
+                ang = rng.uniform(0, 2 * np.pi)
+                kx, ky = np.cos(ang) / lam, np.sin(ang) / lam
+                a = rng.uniform(0.3, 1.0) * min(ru / waves, gmax / waves / (2 * np.pi / lam))
+                ts.append((a, kx, ky, rng.uniform(0, 2 * np.pi)))
+            self.terms.append(ts)
+        del budget_u, budget_g
+
+    def disp(self, x, y, xp=np):
+        """(u, v) at (x, y) (1-based pixel coordinates; numpy or torch arrays via xp)."""
+        out = []
+        for comp in range(2):
+            s = self.off[comp] + 0.0 * x
+            for a, kx, ky, ph in self.terms[comp]:
+                s = s + a * xp.sin(2 * np.pi * (kx * x + ky * y) + ph)
+            out.append(s)
+        return out[0], out[1]
+
+    def grad(self, x, y):
+        """[du/dx, dv/dx, du/dy, dv/dy] at (x, y) (numpy): the IC-GN gradient order."""
+        g = {}
+        for comp in range(2):
+            gx = 0.0 * x
+            gy = 0.0 * x
+            for a, kx, ky, ph in self.terms[comp]:
+                c = a * 2 * np.pi * np.cos(2 * np.pi * (kx * x + ky * y) + ph)
+                gx = gx + c * kx
+                gy = gy + c * ky
+            g[comp] = (gx, gy)
+        return np.stack([g[0][0], g[1][0], g[0][1], g[1][1]], -1)
+
+
+def field_pair(seed, M=2048, N=2048, umax=12.0, gmax=0.05, density=0.0153, noise=2.0, device="cuda") -> FieldPair:
+    """A reference speckle image (Gaussian speckles r ~ U(2, 4) px, amplitude U(60, 200), as the
+    other scenes) and the same speckle field carried by a SmoothField, rendered analytically
+    (every pixel evaluated at its own material coordinates, the inverse map by fixed point),
+    uint8 with N(0, noise) noise."""
+    import torch
+
+    dev = torch.device(device)
+    rng = np.random.default_rng(seed)
+    field = SmoothField(rng, umax, gmax)
+    n_sp = int(round(density * (M + 32) * (N + 32)))
+    sp = synth.make_speckles(rng, n_sp, -16, M + 16, -16, N + 16, 2.0, 4.0, 60.0, 200.0)
+    f64 = dict(dtype=torch.float64, device=dev)
+    cx, cy = torch.tensor(sp.cx, **f64), torch.tensor(sp.cy, **f64)
+    ir2 = torch.tensor(1.0 / sp.r ** 2, **f64)
+    aa = torch.tensor(sp.a, **f64)
+    Yg, Xg = torch.meshgrid(torch.arange(1, N + 1, **f64), torch.arange(1, M + 1, **f64), indexing="ij")
+    Xg, Yg = Xg.reshape(-1), Yg.reshape(-1)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(seed)
+
+    def render(px, py, qx, qy):
+        img = torch.zeros(M * N, **f64)
+        ipx, ipy = torch.round(px).long(), torch.round(py).long()
+        keep = (ipx > -12) & (ipx <= M + 12) & (ipy > -12) & (ipy <= N + 12)
+        ipx, ipy, kcx, kcy, kir2, ka = ipx[keep], ipy[keep], cx[keep], cy[keep], ir2[keep], aa[keep]
+        offs = torch.arange(-12, 13, device=dev)
+        Xp = ipx[:, None] + offs[None, :]
+        okx = (Xp >= 1) & (Xp <= M)
+        for dy in range(-12, 13):
+            Yp = ipy + dy
+            ok = okx & ((Yp >= 1) & (Yp <= N))[:, None]
+            lin = ((Xp - 1) + ((Yp - 1) * M)[:, None])[ok]
+            sel = ok.nonzero()[:, 0]
+            d2 = (qx[lin] - kcx[sel]) ** 2 + (qy[lin] - kcy[sel]) ** 2
+            img.index_add_(0, lin, ka[sel] * torch.exp(-d2 * kir2[sel]))
+        img += torch.randn(M * N, generator=gen, **f64) * noise
+        return torch.clamp(torch.round(img), 0, 255).to(torch.uint8)
+
+    ref = render(cx, cy, Xg, Yg)
+    fu, fv = field.disp(cx, cy, xp=torch)
+    qx, qy = Xg.clone(), Yg.clone()
+    for _ in range(30):  # material point of every deformed-image pixel: q = x - u(q)
+        u, v = field.disp(qx, qy, xp=torch)
+        qx, qy = Xg - u, Yg - v
+    deff = render(cx + fu, cy + fv, qx, qy)
+    return FieldPair(ref=ref, deff=deff, M=M, N=N, field=field)

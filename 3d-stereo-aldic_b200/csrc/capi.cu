@@ -825,10 +825,24 @@ int aldic_net_predict(aldic_net* net, aldic_ctx* c, int64_t n, const double* coo
   if (rc) return rc;
   // the network runs on the context's stream so that the frame and the results are ordered
   aldic_net_set_stream(net, c->stream);
+  const long long before = aldic_net_launch_count(net);
   rc = net_predict(net, frame_of(c), (const double*)ac.dev, n, (double*)au.dev, (double*)af.dev);
   if (rc) return fail(c, rc, "proposal network: %s", aldic_net_last_error(net));
-  c->launches += 3 * ((n + 255) / 256);
+  c->launches += aldic_net_launch_count(net) - before;
   return finish(c, 0);
+}
+
+int aldic_net_extract(aldic_ctx* c, int64_t n, const double* coords, void* X) {
+  if (!c) return ALDIC_ERR_ARG;
+  int rc = need_frame(c, false);
+  if (rc) return rc;
+  if (n < 0) return fail(c, ALDIC_ERR_ARG, "n < 0");
+  if (n == 0) return ALDIC_OK;
+  if (!coords || !X || !is_device_ptr(X)) return fail(c, ALDIC_ERR_ARG, "coords and a device array X are required");
+  Arg ac{coords, (size_t)n * 16, false, nullptr};
+  rc = stage(c, {&ac});
+  if (rc) return rc;
+  return finish(c, launch_net_patches(frame_of(c), (const double*)ac.dev, n, X, c->stream));
 }
 
 int aldic_epipolar_icgn(aldic_ctx* c, int64_t n, const double* pts, int winsize, double tol, double* znssd) {

@@ -635,15 +635,9 @@ int net_predict(aldic_net* net, const FrameDev& fr, const double* coords_dev, lo
   for (long long s = 0; s < n; s += B) {
     const long long nb = std::min<long long>(B, n - s);
     const int bpad = (int)((nb + 7) / 8 * 8);
-    // coords of this batch: the kernel reads coords[t] and coords[n + t] of its own slice
-    // (a strided view: x at coords_dev + s, y at coords_dev + n + s)
-    std::vector<double> dummy;
-    (void)dummy;
-    // patches for nb subsets (pad subsets repeat the last one)
-    FrameDev f = fr;
-    // build a contiguous (2 x nb) coordinate view in the loss buffer area is not needed: the
-    // patch kernel takes the full arrays and an offset through coords_dev + s with stride n
-    patch_kernel<<<(unsigned)nb, 256, 0, net->stream>>>(f, coords_dev + s, n, net->Xbuf);
+    // the patch kernel reads x at coords[t] and y at coords[n + t]: the batch's slice is the
+    // same arrays offset by s
+    patch_kernel<<<(unsigned)nb, 256, 0, net->stream>>>(fr, coords_dev + s, n, net->Xbuf);
     ++net->launches;
     if (bpad > nb) NK(cudaMemsetAsync(net->Xbuf + nb * 64 * 64 * 2, 0, (size_t)(bpad - nb) * 64 * 64 * 2 * 2, net->stream));
     int rc = forward(net, bpad, net->Xbuf);

@@ -121,6 +121,8 @@ int launch_icgn(const IcgnArgs& a, int wmax_enlarged, cudaStream_t st);
 // warped window leaves [3, M-2] x [3, N-2]); FP32 interpolation, FP64 sums.
 int launch_subset_zncc(const FrameDev& fr, long long n, const double* coords, const double* U, const double* F,
                        int winsize, double* zncc, cudaStream_t st);
+// Proposal network (cnn.cu): the network input of n subsets (n x 64 x 64 x 2 BF16) from frame fr.
+int launch_net_patches(const FrameDev& fr, const double* coords, long long n, void* X, cudaStream_t st);
 // Proposal network (cnn.cu): initial guesses of n subsets on frame fr.
 int net_predict(struct ::aldic_net* net, const FrameDev& fr, const double* coords_dev, long long n, double* U0,
                 double* F0);

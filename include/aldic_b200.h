@@ -291,6 +291,12 @@ int aldic_net_status(aldic_net* net);
  * DEF slots): U0 (2n interleaved) and F0 (4n, [F11 F21 F12 F22] = [du/dx dv/dx du/dy dv/dy])
  * for aldic_local_icgn_guess.  Runs on the context's stream. */
 int aldic_net_predict(aldic_net* net, aldic_ctx* ctx, int64_t n, const double* coords, double* U0, double* F0);
+/* The network input of n subsets (coords n x 2, 1-based, rounded) on the frame of ctx: X
+ * (device, n x 64 x 64 x 2 BF16), channel 0 the reference subset (rows x0-16 .. x0+15, columns
+ * y0-16 .. y0+15) in the centre of a zero canvas, channel 1 the deformed window (x0-32 ..
+ * x0+31, y0-32 .. y0+31), each normalised to zero mean and unit deviation (taps clamped to
+ * the image).  For training sets; aldic_net_predict builds the same inputs itself. */
+int aldic_net_extract(aldic_ctx* ctx, int64_t n, const double* coords, void* X);
 /* aldic_local_icgn from the initial guess P = [F0 U0] instead of [0 U0] (the reference starts
  * from F = 0, func/funICGN.m:46); everything else as aldic_local_icgn. */
 int aldic_local_icgn_guess(aldic_ctx* ctx, int variant, int64_t n, const double* coords, const double* U0,

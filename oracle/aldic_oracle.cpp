@@ -365,11 +365,15 @@ inline double norm6(const double* b, int n) {
 
 // funICGN (func/funICGN.m:1-347): uniform-mesh 6-DOF IC-GN, Gauss-Newton.
 // `zero_fix_p56` and `max_iter` give epipolar_ICGN1 (func/epipolar_ICGN1.m:49,134-135).
+// F0 (optional): an initial displacement gradient [F11 F21 F12 F22] in place of the reference's
+// zero start (the learned initial guess; not part of the reference).
 void fun_icgn(const Frame& fr, const double U0[2], double x0, double y0, int winsize, double tol, int max_iter,
-              bool zero_fix_p56, IcgnOut* out, std::vector<double>* znssd_out = nullptr) {
+              bool zero_fix_p56, IcgnOut* out, std::vector<double>* znssd_out = nullptr, const double* F0 = nullptr) {
   out->error = false;
   std::memset(out->H, 0, sizeof(out->H));
   double P[6] = {0, 0, 0, 0, U0[0], U0[1]};
+  if (F0)
+    for (int k = 0; k < 4; ++k) P[k] = F0[k];
   std::memcpy(out->P, P, sizeof(P));
   double w = winsize;
   Window W;
@@ -440,11 +444,13 @@ void fun_icgn(const Frame& fr, const double U0[2], double x0, double y0, int win
 
 // funICGNQuadtree (func_quadtree/funICGNQuadtree.m:1-454): masked 6-DOF IC-GN.
 void fun_icgn_quadtree(const Frame& fr, const double U0[2], double x0, double y0, int winsize, double tol,
-                       IcgnOut* out) {
+                       IcgnOut* out, const double* F0 = nullptr) {
   const int maxIter = 100;
   out->error = false;
   std::memset(out->H, 0, sizeof(out->H));
   double P[6] = {0, 0, 0, 0, U0[0], U0[1]};
+  if (F0)
+    for (int k = 0; k < 4; ++k) P[k] = F0[k];
   std::memcpy(out->P, P, sizeof(P));
   const double w0 = winsize;
   double w = winsize;
@@ -998,9 +1004,23 @@ void orc_gradient(const double* img, const double* mask, int M, int N, double* d
 // coords: n x 2 column-major; U0/U: 2n interleaved; F: 4n interleaved; H: n x 21
 // column-major; conv: n; markHole (variant 1 only, may be null): n.
 // A solver error gives conv = -1 and U = F = NaN, as the drivers' catch blocks do.
+void orc_local_icgn_guess(int variant, const double* ref, const double* def, const double* mask, const double* dfdx,
+                          const double* dfdy, int M, int N, long n, const double* coords, const double* U0,
+                          const double* F0, int winsize, double tol, double* U, double* F, double* H, int* conv,
+                          uint8_t* markHole, int nthreads);
+
 void orc_local_icgn(int variant, const double* ref, const double* def, const double* mask, const double* dfdx,
                     const double* dfdy, int M, int N, long n, const double* coords, const double* U0, int winsize,
                     double tol, double* U, double* F, double* H, int* conv, uint8_t* markHole, int nthreads) {
+  orc_local_icgn_guess(variant, ref, def, mask, dfdx, dfdy, M, N, n, coords, U0, nullptr, winsize, tol, U, F, H, conv,
+                       markHole, nthreads);
+}
+
+// orc_local_icgn from the initial guesses [F0 U0] (F0 4n, or null for the reference's zero).
+void orc_local_icgn_guess(int variant, const double* ref, const double* def, const double* mask, const double* dfdx,
+                          const double* dfdy, int M, int N, long n, const double* coords, const double* U0,
+                          const double* F0, int winsize, double tol, double* U, double* F, double* H, int* conv,
+                          uint8_t* markHole, int nthreads) {
   Frame fr{ref, def, mask, dfdx, dfdy, M, N, 3};
 #ifdef _OPENMP
   if (nthreads > 0) omp_set_num_threads(nthreads);
@@ -1027,8 +1047,9 @@ void orc_local_icgn(int variant, const double* ref, const double* def, const dou
     }
     IcgnOut o;
     const double u0[2] = {U0[2 * t], U0[2 * t + 1]};
-    if (variant == 1) fun_icgn_quadtree(fr, u0, x0, y0, winsize, tol, &o);
-    else fun_icgn(fr, u0, x0, y0, winsize, tol, 100, false, &o);
+    const double* f0 = F0 ? F0 + 4 * t : nullptr;
+    if (variant == 1) fun_icgn_quadtree(fr, u0, x0, y0, winsize, tol, &o, f0);
+    else fun_icgn(fr, u0, x0, y0, winsize, tol, 100, false, &o, nullptr, f0);
     if (o.error) {
       conv[t] = -1;
       U[2 * t] = U[2 * t + 1] = kNaN;

@@ -45,6 +45,9 @@ def lib():
         L.orc_gradient.argtypes = [_dp, C.c_void_p, C.c_int, C.c_int, _dp, _dp]
         L.orc_local_icgn.argtypes = [C.c_int, _dp, _dp, C.c_void_p, _dp, _dp, C.c_int, C.c_int, C.c_long, _dp,
                                      _dp, C.c_int, C.c_double, _dp, _dp, _dp, _ip, C.c_void_p, C.c_int]
+        L.orc_local_icgn_guess.argtypes = [C.c_int, _dp, _dp, C.c_void_p, _dp, _dp, C.c_int, C.c_int, C.c_long, _dp,
+                                           _dp, C.c_void_p, C.c_int, C.c_double, _dp, _dp, _dp, _ip, C.c_void_p,
+                                           C.c_int]
         L.orc_subpb1.argtypes = [C.c_int, _dp, _dp, C.c_void_p, _dp, _dp, C.c_int, C.c_int, C.c_long, _dp, _dp,
                                  _dp, _dp, C.c_void_p, C.c_int, C.c_void_p, C.c_double, C.c_double, _dp, _ip,
                                  C.c_int]
@@ -148,8 +151,9 @@ class Frame:
         return None if self.mask is None else self.mask.ctypes.data
 
 
-def local_icgn(frame: Frame, coords, U0, winsize, tol, variant=1, nthreads=0):
-    """Loop body of LocalICGN (variant 0) / LocalICGNQuadtree (variant 1)."""
+def local_icgn(frame: Frame, coords, U0, winsize, tol, variant=1, nthreads=0, F0=None):
+    """Loop body of LocalICGN (variant 0) / LocalICGNQuadtree (variant 1); F0 (4n) starts
+    from [F0 U0] instead of the reference's [0 U0] (the learned initial guess)."""
     coords = np.asarray(coords, dtype=np.float64)
     n = coords.shape[0]
     U = np.empty(2 * n)
@@ -157,9 +161,11 @@ def local_icgn(frame: Frame, coords, U0, winsize, tol, variant=1, nthreads=0):
     H = np.empty(21 * n)
     conv = np.empty(n, dtype=np.int32)
     mark = np.zeros(n, dtype=np.uint8)
-    lib().orc_local_icgn(variant, frame.ref, frame.deff, frame._mask_ptr(), frame.dfdx, frame.dfdy, frame.M, frame.N,
-                         n, _f64(coords), _flat(U0), int(winsize), float(tol), U, F, H, conv,
-                         mark.ctypes.data if variant == 1 else None, nthreads)
+    f0 = None if F0 is None else _flat(F0)
+    lib().orc_local_icgn_guess(variant, frame.ref, frame.deff, frame._mask_ptr(), frame.dfdx, frame.dfdy, frame.M,
+                               frame.N, n, _f64(coords), _flat(U0), None if f0 is None else f0.ctypes.data,
+                               int(winsize), float(tol), U, F, H, conv, mark.ctypes.data if variant == 1 else None,
+                               nthreads)
     return dict(U=U, F=F, H=H.reshape((n, 21), order="F"), conv=conv, markHole=mark)
 
 
