@@ -167,11 +167,12 @@ def grid_nodes(M, N, w, step, margin=None):
     return np.stack([X.ravel(order="F"), Y.ravel(order="F")], 0)
 
 
-def label_pair(ctx, pair, w=32, step=12, tol=1e-3, variant=_lib.QUADTREE, stream=None):
+def label_pair(ctx, pair, w=32, step=12, tol=1e-3, variant=_lib.QUADTREE, stream=None, umax=12.0):
     """Training samples of one speckle pair (synth_gpu.FieldPair): the network inputs of a grid
-    of subsets whose 64 x 64 windows lie inside the image and, as labels, the method's own
-    converged IC-GN results (LocalICGN's loop body started from the field's analytic
-    displacement and gradient); unconverged subsets are dropped.  Returns CUDA tensors X bf16
+    of subsets whose 64 x 64 windows lie inside the image and whose displacement is within
+    umax, and, as labels, the method's own converged IC-GN results (LocalICGN's loop body
+    started from the field's analytic displacement and gradient); unconverged subsets are
+    dropped.  Returns CUDA tensors X bf16
     (n, 64, 64, 2) and T float32 (n, 6) (scaled outputs), made on `stream` (a torch stream;
     a new one if None) which the current stream then waits for."""
     import torch as T
@@ -185,6 +186,8 @@ def label_pair(ctx, pair, w=32, step=12, tol=1e-3, variant=_lib.QUADTREE, stream
         ctx.compute_gradients()
         nodes = grid_nodes(M, N, w, step)
         u, v = pair.field.disp(nodes[0], nodes[1])
+        keep = (np.abs(u) <= umax) & (np.abs(v) <= umax)
+        nodes, u, v = nodes[:, keep], u[keep], v[keep]
         U0 = np.stack([u, v], 1).ravel()
         F0 = pair.field.grad(nodes[0], nodes[1]).ravel()
         r = ctx.local_icgn(variant, nodes.T, U0, w, tol, F0=F0, want_H=False, want_mark=False)

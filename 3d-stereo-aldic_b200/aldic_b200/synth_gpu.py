@@ -133,32 +133,36 @@ class FieldPair:
 
 
 class SmoothField:
-    """u(x, y) = u0 + sum_k a_k sin(2 pi (kx_k x + ky_k y) + phi_k) (and v alike): a random offset
-    plus low-frequency sinusoids, scaled so that |u|, |v| <= umax and every displacement
-    gradient <= gmax everywhere (the bounds hold term by term)."""
+    """u(x, y) = u0 + g_ux (x - xc) + g_uy (y - yc) + sum_k a_k sin(2 pi (kx_k x + ky_k y) + phi_k)
+    (and v alike): a random offset, an optional random affine part (gradients up to `affine`
+    about the centre (xc, yc)) and low-frequency sinusoids, scaled so that every displacement
+    gradient stays <= gmax everywhere and, without the affine part, |u|, |v| <= umax (the
+    bounds hold term by term)."""
 
-    def __init__(self, rng, umax=12.0, gmax=0.05, waves=3, wl=(300.0, 1200.0)):
-        self.terms = []
-        budget_u, budget_g = umax, gmax
+    def __init__(self, rng, umax=12.0, gmax=0.05, waves=3, wl=(300.0, 1200.0), affine=0.0, centre=(0.0, 0.0)):
         off = rng.uniform(-0.5, 0.5, 2) * umax
         self.off = off
+        self.centre = (float(centre[0]), float(centre[1]))
+        self.lin = rng.uniform(-affine, affine, (2, 2)) if affine > 0 else np.zeros((2, 2))
+        self.terms = []
         for comp in range(2):
             ts = []
             ru = umax - abs(off[comp])
+            rg = gmax - np.abs(self.lin[comp]).max()
             for _ in range(waves):
                 lam = rng.uniform(*wl)
                 ang = rng.uniform(0, 2 * np.pi)
                 kx, ky = np.cos(ang) / lam, np.sin(ang) / lam
-                a = rng.uniform(0.3, 1.0) * min(ru / waves, gmax / waves / (2 * np.pi / lam))
+                a = rng.uniform(0.3, 1.0) * min(ru / waves, rg / waves / (2 * np.pi / lam))
                 ts.append((a, kx, ky, rng.uniform(0, 2 * np.pi)))
             self.terms.append(ts)
-        del budget_u, budget_g
 
     def disp(self, x, y, xp=np):
         """(u, v) at (x, y) (1-based pixel coordinates; numpy or torch arrays via xp)."""
         out = []
+        dx, dy = x - self.centre[0], y - self.centre[1]
         for comp in range(2):
-            s = self.off[comp] + 0.0 * x
+            s = self.off[comp] + self.lin[comp, 0] * dx + self.lin[comp, 1] * dy
             for a, kx, ky, ph in self.terms[comp]:
                 s = s + a * xp.sin(2 * np.pi * (kx * x + ky * y) + ph)
             out.append(s)
@@ -168,8 +172,8 @@ class SmoothField:
         """[du/dx, dv/dx, du/dy, dv/dy] at (x, y) (numpy): the IC-GN gradient order."""
         g = {}
         for comp in range(2):
-            gx = 0.0 * x
-            gy = 0.0 * x
+            gx = self.lin[comp, 0] + 0.0 * x
+            gy = self.lin[comp, 1] + 0.0 * x
             for a, kx, ky, ph in self.terms[comp]:
                 c = a * 2 * np.pi * np.cos(2 * np.pi * (kx * x + ky * y) + ph)
                 gx = gx + c * kx
@@ -178,16 +182,17 @@ class SmoothField:
         return np.stack([g[0][0], g[1][0], g[0][1], g[1][1]], -1)
 
 
-def field_pair(seed, M=2048, N=2048, umax=12.0, gmax=0.05, density=0.0153, noise=2.0, device="cuda") -> FieldPair:
+def field_pair(seed, M=2048, N=2048, umax=12.0, gmax=0.05, density=0.0153, noise=2.0, device="cuda",
+               affine=0.0) -> FieldPair:
     """A reference speckle image (Gaussian speckles r ~ U(2, 4) px, amplitude U(60, 200), as the
-    other scenes) and the same speckle field carried by a SmoothField, rendered analytically
-    (every pixel evaluated at its own material coordinates, the inverse map by fixed point),
-    uint8 with N(0, noise) noise."""
+    other scenes) and the same speckle field carried by a SmoothField (affine part about the
+    image centre), rendered analytically (every pixel evaluated at its own material
+    coordinates, the inverse map by fixed point), uint8 with N(0, noise) noise."""
     import torch
 
     dev = torch.device(device)
     rng = np.random.default_rng(seed)
-    field = SmoothField(rng, umax, gmax)
+    field = SmoothField(rng, umax, gmax, affine=affine, centre=((M + 1) / 2.0, (N + 1) / 2.0))
     n_sp = int(round(density * (M + 32) * (N + 32)))
     sp = synth.make_speckles(rng, n_sp, -16, M + 16, -16, N + 16, 2.0, 4.0, 60.0, 200.0)
     f64 = dict(dtype=torch.float64, device=dev)

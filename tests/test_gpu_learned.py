@@ -113,7 +113,7 @@ def test_list_search_matches_the_whole_grid(env):
     idx = rng.choice(nx * ny, size=min(37, nx * ny), replace=False).astype(np.int32)
     lst = ctx.integer_search_list([8, 8], gx, gy, w, st, idx)
     for k in ("x", "y", "u", "v", "phi"):
-        want = full[k].ravel(order="F")[idx]
+        want = full[k].ravel()[idx]  # the (nY, nX) grid in list order i + j nX
         assert np.array_equal(lst[k], want, equal_nan=True), k
     # device list and outputs
     dev = torch.device("cuda:0")
@@ -127,8 +127,8 @@ def test_list_search_matches_the_whole_grid(env):
 
     nodes, nx2, ny2 = search_nodes(gx, gy, w, st)
     assert (nx2, ny2) == (nx, ny)
-    assert np.array_equal(nodes[0], full["x"].ravel(order="F"))
-    assert np.array_equal(nodes[1], full["y"].ravel(order="F"))
+    assert np.array_equal(nodes[0], full["x"].ravel())
+    assert np.array_equal(nodes[1], full["y"].ravel())
 
 
 def _patches_numpy(f, g, crd):
