@@ -1,7 +1,7 @@
 """The learned initial guess: host side of the proposal network (csrc/cnn.cu).
 
-The network reads a 32 x 32 reference subset and the 64 x 64 deformed window around it and
-predicts (u, v, du/dx, dv/dx, du/dy, dv/dy) as IC-GN's initial guess [F0 U0], in place of the
+The network reads a 32 x 32 reference subset and the 64 x 64 deformed window around it (with
+4 px of context each side: a 72 x 72 x 2 input) and predicts (u, v, du/dx, dv/dx, du/dy, dv/dy) as IC-GN's initial guess [F0 U0], in place of the
 integer search (func/funIntegerSearch.m:132-180), which stays the fallback and the judge.  It
 has no counterpart in the reference.  Everything here drives the library's C ABI: device
 memory comes from torch, every layer, gradient and optimiser step is the library's own
@@ -19,12 +19,12 @@ from ._lib import AldicError
 SCALE = np.array([1 / 8.0, 1 / 8.0, 20.0, 20.0, 20.0, 20.0], dtype=np.float32)  # network output units
 
 
-# weight matrices (rows x cols, row-major, then rows biases) of the four 3 x 3 stride-2
-# convolutions (cols = 9 x input channels, the first padded 18 -> 24) and the two fully
-# connected layers (1024 -> 128 -> 6, the output padded to 16 rows)
+# weight matrices (rows x cols, row-major, then rows biases) of the four 3 x 3 convolutions
+# (cols = 9 x input channels, padded to a multiple of 8: conv1 9 -> 16, conv3 729 -> 736) and
+# the two fully connected layers (1024 -> 128 -> 6, the output padded to 16 rows)
 _ROWS = (32, 32, 64, 64, 128, 16)
-_COLS = (24, 288, 288, 576, 1024, 128)
-_FAN_IN = (18, 288, 288, 576, 1024, 128)
+_COLS = (16, 288, 736, 576, 1024, 128)
+_FAN_IN = (9, 288, 729, 576, 1024, 128)
 
 
 def param_count():
@@ -33,14 +33,13 @@ def param_count():
 
 def init_params(seed=0):
     """He-normal weights (std sqrt(2 / fan-in)) and zero biases, with the padding columns of
-    the first layer and the padding rows of the output layer zero: the flat FP32 vector
+    the convolutions and the padding rows of the output layer zero: the flat FP32 vector
     aldic_net_set_params takes."""
     rng = np.random.default_rng(seed)
     parts = []
     for l, (r, c) in enumerate(zip(_ROWS, _COLS)):
         W = rng.normal(0.0, np.sqrt(2.0 / _FAN_IN[l]), (r, c)).astype(np.float32)
-        if l == 0:
-            W[:, _FAN_IN[0]:] = 0.0
+        W[:, _FAN_IN[l]:] = 0.0
         if l == len(_ROWS) - 1:
             W[6:, :] = 0.0
         parts += [W.ravel(), np.zeros(r, dtype=np.float32)]
@@ -107,9 +106,9 @@ class ProposalNet:
         return C.c_void_p(t.data_ptr())
 
     def forward(self, x, out):
-        """out (batch, 6) float32 CUDA tensor <- the scaled outputs for x (batch, 64, 64, 2) bf16."""
+        """out (batch, 6) float32 CUDA tensor <- the scaled outputs for x (batch, 72, 72, 2) bf16."""
         b = int(x.shape[0])
-        self._check(self.lib.aldic_net_forward(self.h, b, self._dev(x, "torch.bfloat16", (64, 64, 2)),
+        self._check(self.lib.aldic_net_forward(self.h, b, self._dev(x, "torch.bfloat16", (72, 72, 2)),
                                                self._dev(out, "torch.float32", (6,))), "aldic_net_forward")
         return out
 
@@ -117,14 +116,14 @@ class ProposalNet:
         """(loss, flat FP32 gradients) of the mean squared error against t (batch, 6)."""
         g = np.empty(self.n_params, dtype=np.float32)
         loss = np.zeros(1, dtype=np.float32)
-        self._check(self.lib.aldic_net_gradients(self.h, int(x.shape[0]), self._dev(x, "torch.bfloat16", (64, 64, 2)),
+        self._check(self.lib.aldic_net_gradients(self.h, int(x.shape[0]), self._dev(x, "torch.bfloat16", (72, 72, 2)),
                                                  self._dev(t, "torch.float32", (6,)), C.c_void_p(g.ctypes.data),
                                                  C.c_void_p(loss.ctypes.data)), "aldic_net_gradients")
         return float(loss[0]), g
 
     def train_step(self, x, t, lr, want_loss=False):
         loss = np.zeros(1, dtype=np.float32)
-        self._check(self.lib.aldic_net_train_step(self.h, int(x.shape[0]), self._dev(x, "torch.bfloat16", (64, 64, 2)),
+        self._check(self.lib.aldic_net_train_step(self.h, int(x.shape[0]), self._dev(x, "torch.bfloat16", (72, 72, 2)),
                                                   self._dev(t, "torch.float32", (6,)), C.c_float(lr),
                                                   C.c_void_p(loss.ctypes.data) if want_loss else None),
                     "aldic_net_train_step")
@@ -157,9 +156,9 @@ def gemm_bf16(A, B, C_out, splits=1, stream=0):
 
 # ------------------------------------------------------------------------ training
 def grid_nodes(M, N, w, step, margin=None):
-    """Subset centres (1-based) of a uniform grid whose 64 x 64 network windows stay inside the
+    """Subset centres (1-based) of a uniform grid whose 72 x 72 network windows stay inside the
     image: a (2, n) float64 array, x fastest."""
-    m = 33 if margin is None else margin
+    m = 37 if margin is None else margin
     lo = max(m, w // 2 + 4)
     xs = np.arange(lo, M - lo + 1, step, dtype=np.float64)
     ys = np.arange(lo, N - lo + 1, step, dtype=np.float64)
@@ -168,12 +167,12 @@ def grid_nodes(M, N, w, step, margin=None):
 
 
 def label_pair(ctx, pair, w=32, step=12, tol=1e-3, variant=_lib.QUADTREE, stream=None, umax=12.0):
-    """Training samples of one speckle pair (synth_gpu.FieldPair): the network inputs of a grid
-    of subsets whose 64 x 64 windows lie inside the image and whose displacement is within
-    umax, and, as labels, the method's own converged IC-GN results (LocalICGN's loop body
+    """Training samples of one speckle pair (synth_gpu.FieldPair): the network inputs of the
+    pair's own nodes (a tile mosaic's tile centres) or of a grid of subsets whose 72 x 72
+    windows lie inside the image, whose displacement is within umax, and, as labels, the method's own converged IC-GN results (LocalICGN's loop body
     started from the field's analytic displacement and gradient); unconverged subsets are
     dropped.  Returns CUDA tensors X bf16
-    (n, 64, 64, 2) and T float32 (n, 6) (scaled outputs), made on `stream` (a torch stream;
+    (n, 72, 72, 2) and T float32 (n, 6) (scaled outputs), made on `stream` (a torch stream;
     a new one if None) which the current stream then waits for."""
     import torch as T
 
@@ -184,7 +183,9 @@ def label_pair(ctx, pair, w=32, step=12, tol=1e-3, variant=_lib.QUADTREE, stream
         ctx.load_image_raw(0, pair.ref, [1, M], [1, N], want_stats=False, shape=(M, N))
         ctx.load_image_raw(1, pair.deff, [1, M], [1, N], want_stats=False, shape=(M, N))
         ctx.compute_gradients()
-        nodes = grid_nodes(M, N, w, step)
+        nodes = getattr(pair, "nodes", None)
+        if nodes is None:
+            nodes = grid_nodes(M, N, w, step)
         u, v = pair.field.disp(nodes[0], nodes[1])
         keep = (np.abs(u) <= umax) & (np.abs(v) <= umax)
         nodes, u, v = nodes[:, keep], u[keep], v[keep]
@@ -193,7 +194,7 @@ def label_pair(ctx, pair, w=32, step=12, tol=1e-3, variant=_lib.QUADTREE, stream
         r = ctx.local_icgn(variant, nodes.T, U0, w, tol, F0=F0, want_H=False, want_mark=False)
         ok = (r["conv"] > 0) & (r["conv"] < 100)
         crd = T.from_numpy(np.ascontiguousarray(nodes[:, ok])).to(pair.ref.device, non_blocking=False)
-        X = T.empty((int(ok.sum()), 64, 64, 2), dtype=T.bfloat16, device=pair.ref.device)
+        X = T.empty((int(ok.sum()), 72, 72, 2), dtype=T.bfloat16, device=pair.ref.device)
         ctx.net_extract(crd, X)
         lab = np.concatenate([r["U"].reshape(-1, 2)[ok], r["F"].reshape(-1, 4)[ok]], 1) * SCALE
         Tg = T.from_numpy(lab.astype(np.float32)).to(pair.ref.device)

@@ -230,3 +230,106 @@ def field_pair(seed, M=2048, N=2048, umax=12.0, gmax=0.05, density=0.0153, noise
         qx, qy = Xg - u, Yg - v
     deff = render(cx + fu, cy + fv, qx, qy)
     return FieldPair(ref=ref, deff=deff, M=M, N=N, field=field)
+
+
+class TileField:
+    """A mosaic of independent affine warps: tile (i, j) (tile x tile pixels, 1-based rows
+    i tile + 1 .. (i + 1) tile, columns alike) carries u(x) = U_ij + F_ij (x - c_ij) about its
+    centre c_ij = (i tile + tile / 2 + 1, j tile + tile / 2 + 1)."""
+
+    def __init__(self, U, F, tile):
+        self.U, self.F, self.tile = U, F, tile  # (ti, tj, 2), (ti, tj, 4) [du/dx dv/dx du/dy dv/dy]
+
+    def centres(self):
+        """The tile centres, (2, n) float64 in tile order (i fastest)."""
+        ti, tj = self.U.shape[:2]
+        h = self.tile // 2 + 1
+        X, Y = np.meshgrid(self.tile * np.arange(ti) + h, self.tile * np.arange(tj) + h, indexing="ij")
+        return np.stack([X.ravel(order="F"), Y.ravel(order="F")], 0).astype(np.float64)
+
+    def _at(self, x, y):
+        i = ((np.asarray(x) - 1) // self.tile).astype(np.int64)
+        j = ((np.asarray(y) - 1) // self.tile).astype(np.int64)
+        h = self.tile // 2 + 1
+        return i, j, x - (self.tile * i + h), y - (self.tile * j + h)
+
+    def disp(self, x, y):
+        i, j, dx, dy = self._at(x, y)
+        U, F = self.U[i, j], self.F[i, j]
+        return U[..., 0] + F[..., 0] * dx + F[..., 2] * dy, U[..., 1] + F[..., 1] * dx + F[..., 3] * dy
+
+    def grad(self, x, y):
+        i, j, _, _ = self._at(x, y)
+        return self.F[i, j]
+
+
+def tile_pair(seed, tiles=28, tile=72, umax=12.0, gmax=0.05, density=0.0153, noise=2.0, device="cuda") -> FieldPair:
+    """Training pairs with an independent speckle pattern and affine warp per tile: a tiles x
+    tiles mosaic of tile x tile pixels, tile (i, j) showing its own Gaussian speckles
+    (r ~ U(2, 4) px, amplitude U(60, 200)) in the reference image and the same speckles under
+    u = U + F (x - c) in the deformed image, U ~ U(-umax, umax)^2, F ~ U(-gmax, gmax)^4,
+    rendered analytically (the exact inverse of the affine map per pixel), uint8 with
+    N(0, noise) noise.  The tile x tile window about each tile centre (1-based tile start +
+    tile / 2) is the tile itself."""
+    import torch
+
+    dev = torch.device(device)
+    rng = np.random.default_rng(seed)
+    M = N = tiles * tile
+    U = rng.uniform(-umax, umax, (tiles, tiles, 2))
+    F = rng.uniform(-gmax, gmax, (tiles, tiles, 4))
+    field = TileField(U, F, tile)
+    h = tile // 2 + 1
+    box = tile // 2 + 32  # material half-box covering the tile and its warped preimage
+    n_t = int(round(density * (2 * box) ** 2))
+    f64 = dict(dtype=torch.float64, device=dev)
+    ti = np.repeat(np.arange(tiles), tiles)
+    tj = np.tile(np.arange(tiles), tiles)
+    x0 = torch.tensor(np.repeat(tile * ti + h, n_t), **f64)
+    y0 = torch.tensor(np.repeat(tile * tj + h, n_t), **f64)
+    cx = x0 + torch.tensor(rng.uniform(-box, box, x0.numel()), **f64)
+    cy = y0 + torch.tensor(rng.uniform(-box, box, x0.numel()), **f64)
+    ir2 = torch.tensor(1.0 / rng.uniform(2.0, 4.0, x0.numel()) ** 2, **f64)
+    aa = torch.tensor(rng.uniform(60.0, 200.0, x0.numel()), **f64)
+    Ut = torch.tensor(np.repeat(U[ti, tj], n_t, axis=0), **f64)
+    Ft = torch.tensor(np.repeat(F[ti, tj], n_t, axis=0), **f64)
+    # A = I + F (rows: u, v; columns: d/dx, d/dy) and its inverse, per speckle
+    a11, a21, a12, a22 = 1 + Ft[:, 0], Ft[:, 1], Ft[:, 2], 1 + Ft[:, 3]
+    det = a11 * a22 - a12 * a21
+    i11, i12, i21, i22 = a22 / det, -a12 / det, -a21 / det, a11 / det
+    lo_x, lo_y = x0 - (h - 1), y0 - (h - 1)  # the speckle's tile, 1-based inclusive
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(seed)
+    offs = torch.arange(-12, 13, device=dev)
+
+    def render(deformed):
+        img = torch.zeros(M * N, **f64)
+        if deformed:
+            px = x0 + Ut[:, 0] + a11 * (cx - x0) + a12 * (cy - y0)
+            py = y0 + Ut[:, 1] + a21 * (cx - x0) + a22 * (cy - y0)
+        else:
+            px, py = cx, cy
+        ipx, ipy = torch.round(px).long(), torch.round(py).long()
+        Xp = ipx[:, None] + offs[None, :]
+        okx = (Xp >= lo_x[:, None]) & (Xp < lo_x[:, None] + tile)
+        for dy in range(-12, 13):
+            Yp = ipy + dy
+            ok = okx & ((Yp >= lo_y) & (Yp < lo_y + tile))[:, None]
+            sel = ok.nonzero()[:, 0]
+            X = Xp[ok].double()
+            Y = Yp[sel].double()
+            if deformed:
+                rx, ry = X - x0[sel] - Ut[sel, 0], Y - y0[sel] - Ut[sel, 1]
+                qx = x0[sel] + i11[sel] * rx + i12[sel] * ry
+                qy = y0[sel] + i21[sel] * rx + i22[sel] * ry
+            else:
+                qx, qy = X, Y
+            lin = (Xp[ok] - 1) + (Yp[sel] - 1) * M
+            d2 = (qx - cx[sel]) ** 2 + (qy - cy[sel]) ** 2
+            img.index_add_(0, lin, aa[sel] * torch.exp(-d2 * ir2[sel]))
+        img += torch.randn(M * N, generator=gen, **f64) * noise
+        return torch.clamp(torch.round(img), 0, 255).to(torch.uint8)
+
+    pair = FieldPair(ref=render(False), deff=render(True), M=M, N=N, field=field)
+    pair.nodes = field.centres()
+    return pair

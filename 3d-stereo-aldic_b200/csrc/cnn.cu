@@ -5,17 +5,28 @@
 // reference (its initial guess is the integer search, func/funIntegerSearch.m:132-180, which
 // stays the fallback here).
 //
-// Architecture (NHWC BF16 activations, FP32 accumulation, ReLU after every layer but the last):
-//   input 64 x 64 x 2 (channel 0: the normalised reference subset in the centre 32 x 32 of a
-//   zero canvas; channel 1: the normalised deformed window)
-//   conv 3x3 stride 2 pad 1:  2 -> 32 (32 x 32),  32 -> 32 (16 x 16),  32 -> 64 (8 x 8),
-//                             64 -> 64 (4 x 4)
+// Architecture (NHWC BF16 activations, FP32 accumulation, ReLU after every convolution and the
+// hidden fully connected layer; 3 x 3 convolutions with padding 1):
+//   input 72 x 72 x 2 centred on the subset: channel 1 the frame's normalised deformed image,
+//   channel 0 the normalised reference image in the centre 40 x 40 (zero elsewhere); zero
+//   outside the image
+//   the reference part R and the deformed window D through the same two convolutions:
+//       conv1 1 -> 32 stride 2, conv2 32 -> 32 stride 2 (R: 10 x 10 x 32, D: 18 x 18 x 32), of
+//       which the inner 8 x 8 (R, the 32 x 32 subset) and 16 x 16 (D, the 64 x 64 window) are
+//       kept: the outer ring is the only part that sees the window's own zero padding, so the
+//       kept features equal those of the two convolutions run over the whole image
+//   correlation volume C[i, j, d] = sum_c fR[i, j, c] fD[i + 4 + di, j + 4 + dj, c] / 32 for
+//       the 81 offsets d = (di + 4) 9 + (dj + 4), di, dj in -4..4 (+-16 px at stride 4)
+//   conv3 81 -> 64 stride 2 (4 x 4), conv4 64 -> 64 stride 1 (4 x 4)
 //   fully connected: 1024 -> 128 -> 6
-// 197 254 trained parameters.  Every convolution, data gradient, weight gradient and fully
-// connected layer is one tcgen05 GEMM (cnn_gemm.cu) over im2col rows; the rest are the small
-// kernels below (im2col, col2im, transposes, ReLU gradient, loss, bias gradient, Adam, patch
-// extraction).  Training: mean squared error on the scaled outputs (u / 8, v / 8, F x 20),
-// Adam.
+// 227 152 parameters.  Training runs the network per subset window; prediction runs conv1 and
+// conv2 once over each whole image and the correlation and the rest per subset, on feature
+// crops at the subset's position (subset centres x = 1 mod 4 in both coordinates align the
+// two).  Every convolution, data gradient, weight gradient and fully connected layer is one
+// tcgen05 GEMM (cnn_gemm.cu) over im2col rows; the correlation and the rest are the small
+// kernels below (im2col, col2im, correlation and its gradient, transposes, ReLU gradient, loss,
+// bias gradient, Adam, patch extraction).  Training: mean squared error on the scaled outputs
+// (u / 8, v / 8, F x 20), Adam.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -34,25 +45,45 @@ namespace {
 
 typedef __nv_bfloat16 bf16;
 
-struct ConvL {
-  int Hin, Win, Cin, Hout, Wout, Cout, K, Kp;
+// One convolution applied to one input: parameter layer, input Hin x Win x Cin, output
+// Hout x Wout x Cout, K = 9 Cin im2col columns padded to Kp (a multiple of 8).
+struct ConvI {
+  int layer, Hin, Win, Cin, Hout, Wout, Cout, K, Kp, stride;
 };
-constexpr ConvL kConv[4] = {{64, 64, 2, 32, 32, 32, 18, 24},
-                            {32, 32, 32, 16, 16, 32, 288, 288},
-                            {16, 16, 32, 8, 8, 64, 288, 288},
-                            {8, 8, 64, 4, 4, 64, 576, 576}};
-constexpr int kFcIn = 1024, kFcHid = 128, kOut = 6, kOutP = 16;
+constexpr int kConvR1 = 0, kConvD1 = 1, kConvR2 = 2, kConvD2 = 3, kConv3 = 4, kConv4 = 5, kNumConv = 6;
+constexpr ConvI kConv[kNumConv] = {{0, 40, 40, 1, 20, 20, 32, 9, 16, 2},      {0, 72, 72, 1, 36, 36, 32, 9, 16, 2},
+                                   {1, 20, 20, 32, 10, 10, 32, 288, 288, 2},  {1, 36, 36, 32, 18, 18, 32, 288, 288, 2},
+                                   {2, 8, 8, 81, 4, 4, 64, 729, 736, 2},      {3, 4, 4, 64, 4, 4, 64, 576, 576, 1}};
+constexpr int kWin = 72, kRefWin = 40, kRefOff = 16;  // input window, reference part and its offset
+constexpr int kDisp = 81, kFcIn = 1024, kFcHid = 128, kOut = 6, kOutP = 16;
 
-// flat FP32 parameter layout: per conv layer W [Cout x Kp] then b [Cout]; FC1 W [128 x 1024],
-// b [128]; FC2 W [16 x 128] (rows 6..15 zero), b [16] (entries 6..15 zero)
+// Where an input of a convolution sits: element (b, y, x, c) at base + off + b sb + y sy + x sx + c.
+struct View {
+  long long off, sb, sy, sx;
+};
+View nhwc(int H, int W, int C) { return View{0, (long long)H * W * C, (long long)W * C, C}; }
+// the two image channels of the 72 x 72 x 2 input
+constexpr View kViewRef{(kRefOff * kWin + kRefOff) * 2, kWin * kWin * 2, kWin * 2, 2};
+constexpr View kViewDef{1, kWin * kWin * 2, kWin * 2, 2};
+
+// Where the kept 8 x 8 (reference) and 16 x 16 (deformed) feature crops of sample b sit:
+// element (i, j, c) at base + b sb + off + i row + j 32 + c.
+struct Crop {
+  long long sb, off, row;
+};
+
+// flat FP32 parameter layout: per layer W [rows x cols] then b [rows]: conv1 32 x 16 (9 used),
+// conv2 32 x 288, conv3 64 x 736 (729 used), conv4 64 x 576, FC1 128 x 1024, FC2 16 x 128
+// (rows 6..15 and bias entries 6..15 zero)
 struct Layout {
   long long w[6], b[6], n;
   long long rows[6], cols[6];
   Layout() {
+    const long long r[6] = {32, 32, 64, 64, kFcHid, kOutP}, c[6] = {16, 288, 736, 576, kFcIn, kFcHid};
     long long o = 0;
     for (int l = 0; l < 6; ++l) {
-      rows[l] = l < 4 ? kConv[l].Cout : (l == 4 ? kFcHid : kOutP);
-      cols[l] = l < 4 ? kConv[l].Kp : (l == 4 ? kFcIn : kFcHid);
+      rows[l] = r[l];
+      cols[l] = c[l];
       w[l] = o;
       o += rows[l] * cols[l];
       b[l] = o;
@@ -66,49 +97,173 @@ const Layout kL;
 __device__ __forceinline__ long long ceil_div_ll(long long a, long long b) { return (a + b - 1) / b; }
 
 // ------------------------------------------------------------------------- kernels
-// im2col of a stride-2, pad-1, 3 x 3 convolution: row p = (b, oy, ox), column k = (ky, kx, ci),
-// zero outside the input and in the K padding.
-__global__ void im2col_kernel(const bf16* __restrict__ H, bf16* __restrict__ A, int batch, ConvL L) {
-  const long long P = (long long)batch * L.Hout * L.Wout;
-  const long long total = P * L.Kp;
+// im2col of a 3 x 3, pad-1 convolution: row p = (b, oy, ox), column k = (ky, kx, ci), zero
+// outside the input and in the K padding.  Each thread writes 8 columns (one 16-byte store).
+__global__ void im2col_kernel(const bf16* __restrict__ in, View v, bf16* __restrict__ A, long long P, ConvI L) {
+  const int groups = L.Kp / 8;
+  const long long total = P * groups;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
-    const long long p = i / L.Kp;
-    const int k = (int)(i % L.Kp);
-    bf16 v = __float2bfloat16_rn(0.f);
-    if (k < L.K) {
-      const int tap = k / L.Cin, ci = k % L.Cin, ky = tap / 3, kx = tap % 3;
-      const int ox = (int)(p % L.Wout), oy = (int)((p / L.Wout) % L.Hout);
-      const long long b = p / ((long long)L.Wout * L.Hout);
-      const int iy = 2 * oy - 1 + ky, ix = 2 * ox - 1 + kx;
-      if (iy >= 0 && iy < L.Hin && ix >= 0 && ix < L.Win) v = H[((b * L.Hin + iy) * L.Win + ix) * L.Cin + ci];
+    const long long p = i / groups;
+    const int k0 = (int)(i % groups) * 8;
+    const int ox = (int)(p % L.Wout), oy = (int)((p / L.Wout) % L.Hout);
+    const long long b = p / ((long long)L.Wout * L.Hout);
+    const bf16* base = in + v.off + b * v.sb;
+    __align__(16) bf16 vals[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int k = k0 + j;
+      bf16 x = __float2bfloat16_rn(0.f);
+      if (k < L.K) {
+        const int tap = k / L.Cin, ci = k % L.Cin, ky = tap / 3, kx = tap % 3;
+        const int iy = L.stride * oy - 1 + ky, ix = L.stride * ox - 1 + kx;
+        if (iy >= 0 && iy < L.Hin && ix >= 0 && ix < L.Win) x = base[iy * v.sy + ix * v.sx + ci];
+      }
+      vals[j] = x;
     }
-    A[i] = v;
+    *reinterpret_cast<uint4*>(A + p * L.Kp + k0) = *reinterpret_cast<const uint4*>(vals);
   }
 }
 
 // col2im (gather form, no atomics): the gradient of input pixel (b, iy, ix, ci) sums the
 // im2col gradient entries that read it.
-__global__ void col2im_kernel(const float* __restrict__ dA, float* __restrict__ dH, int batch, ConvL L) {
+__global__ void col2im_kernel(const float* __restrict__ dA, float* __restrict__ dH, int batch, ConvI L) {
   const long long total = (long long)batch * L.Hin * L.Win * L.Cin;
+  const int s = L.stride;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
     const int ci = (int)(i % L.Cin);
     const int ix = (int)((i / L.Cin) % L.Win);
     const int iy = (int)((i / ((long long)L.Cin * L.Win)) % L.Hin);
     const long long b = i / ((long long)L.Cin * L.Win * L.Hin);
-    float s = 0.f;
+    float acc = 0.f;
 #pragma unroll
     for (int ky = 0; ky < 3; ++ky) {
       const int ty = iy + 1 - ky;
-      if (ty < 0 || (ty & 1) || (ty >> 1) >= L.Hout) continue;
+      if (ty < 0 || ty % s || ty / s >= L.Hout) continue;
 #pragma unroll
       for (int kx = 0; kx < 3; ++kx) {
         const int tx = ix + 1 - kx;
-        if (tx < 0 || (tx & 1) || (tx >> 1) >= L.Wout) continue;
-        const long long p = (b * L.Hout + (ty >> 1)) * L.Wout + (tx >> 1);
-        s += dA[p * L.Kp + (ky * 3 + kx) * L.Cin + ci];
+        if (tx < 0 || tx % s || tx / s >= L.Wout) continue;
+        const long long p = (b * L.Hout + ty / s) * L.Wout + tx / s;
+        acc += dA[p * L.Kp + (ky * 3 + kx) * L.Cin + ci];
       }
     }
-    dH[i] = s;
+    dH[i] = acc;
+  }
+}
+
+// 8 BF16 -> 8 floats
+__device__ __forceinline__ void load8(const bf16* p, float (&f)[8]) {
+  const uint4 u = *reinterpret_cast<const uint4*>(p);
+  const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&u);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const float2 t = __bfloat1622float2(h[k]);
+    f[2 * k] = t.x;
+    f[2 * k + 1] = t.y;
+  }
+}
+
+// one correlation entry: reference feature r (32 channels) against deformed feature q
+__device__ __forceinline__ float dot32(const bf16* r, const bf16* q) {
+  float s = 0.f;
+#pragma unroll
+  for (int c = 0; c < 32; c += 8) {
+    float a[8], e[8];
+    load8(r + c, a);
+    load8(q + c, e);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) s = fmaf(a[k], e[k], s);
+  }
+  return s;
+}
+
+// correlation volume C (B, 8, 8, 81) of the reference crops against the deformed crops, BF16
+__global__ void corr_kernel(const bf16* __restrict__ fR, Crop cr, const bf16* __restrict__ fD, Crop cd,
+                            bf16* __restrict__ C, long long total) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+    const int d = (int)(i % kDisp);
+    const long long pos = i / kDisp;
+    const int j = (int)(pos % 8), ii = (int)((pos / 8) % 8);
+    const long long b = pos / 64;
+    const int di = d / 9 - 4, dj = d % 9 - 4;
+    const bf16* r = fR + b * cr.sb + cr.off + ii * cr.row + j * 32;
+    const bf16* q = fD + b * cd.sb + cd.off + (ii + 4 + di) * cd.row + (j + 4 + dj) * 32;
+    C[i] = __float2bfloat16_rn(dot32(r, q) * (1.f / 32.f));
+  }
+}
+
+// The same volume for subsets t0 .. t0 + nb - 1 of coords (n x 2) from the feature maps of the
+// whole reference and deformed images (Hf x Wf x 32 each, element (i, j) the features centred
+// on image pixel (4 i + 1, 4 j + 1)): the reference crop starts at ((x - 17) / 4, (y - 17) / 4),
+// the deformed crop at ((x - 33) / 4, (y - 33) / 4), x, y the subset centre moved to the
+// nearest centre = 1 mod 4.  ok[t - t0] = 0 where a crop leaves the maps (volume zero).
+__global__ void corr_image_kernel(const bf16* __restrict__ FR, const bf16* __restrict__ FD, int Hf, int Wf,
+                                  const double* __restrict__ coords, long long n, long long t0, int nb,
+                                  bf16* __restrict__ C, uint8_t* __restrict__ ok) {
+  const long long total = (long long)nb * 64 * kDisp;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+    const int d = (int)(i % kDisp);
+    const long long pos = i / kDisp;
+    const int j = (int)(pos % 8), ii = (int)((pos / 8) % 8);
+    const long long b = pos / 64;
+    const long long x = 4 * llround((coords[t0 + b] - 1.0) / 4.0) + 1, y = 4 * llround((coords[n + t0 + b] - 1.0) / 4.0) + 1;
+    const long long rx = (x - 17) / 4, ry = (y - 17) / 4, dx = (x - 33) / 4, dy = (y - 33) / 4;
+    const bool inside = x >= 33 && y >= 33 && rx + 7 < Hf && ry + 7 < Wf && dx + 15 < Hf && dy + 15 < Wf;
+    float v = 0.f;
+    if (inside) {
+      const int di = d / 9 - 4, dj = d % 9 - 4;
+      const bf16* r = FR + ((rx + ii) * Wf + ry + j) * 32;
+      const bf16* q = FD + ((dx + ii + 4 + di) * Wf + dy + j + 4 + dj) * 32;
+      v = dot32(r, q) * (1.f / 32.f);
+    }
+    C[i] = __float2bfloat16_rn(v);
+    if (ii == 0 && j == 0 && d == 0) ok[b] = inside ? 1 : 0;
+  }
+}
+
+// Gradients of the correlation with the ReLU of its inputs folded in, over the whole conv2
+// output maps (zero on the ring outside the crops): dZR = dC fD / 32 where fR > 0 (B, 10, 10,
+// 32), dZD = dC^T fR / 32 where fD > 0 (B, 18, 18, 32), BF16; dC (B, 8, 8, 81) FP32.
+__global__ void corr_grad_ref_kernel(const float* __restrict__ dC, const bf16* __restrict__ fR,
+                                     const bf16* __restrict__ fD, bf16* __restrict__ dZR, long long total) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(i % 32);
+    const long long pix = i / 32;
+    const int x = (int)(pix % 10) - 1, y = (int)((pix / 10) % 10) - 1;  // crop coordinates
+    const long long b = pix / 100;
+    float s = 0.f;
+    if (x >= 0 && x < 8 && y >= 0 && y < 8 && __bfloat162float(fR[i]) > 0.f) {
+      const long long pos = (b * 8 + y) * 8 + x;
+      for (int d = 0; d < kDisp; ++d) {
+        const int di = d / 9 - 4, dj = d % 9 - 4;
+        s = fmaf(dC[pos * kDisp + d], __bfloat162float(fD[((b * 18 + y + 5 + di) * 18 + x + 5 + dj) * 32 + c]), s);
+      }
+    }
+    dZR[i] = __float2bfloat16_rn(s * (1.f / 32.f));
+  }
+}
+
+__global__ void corr_grad_def_kernel(const float* __restrict__ dC, const bf16* __restrict__ fR,
+                                     const bf16* __restrict__ fD, bf16* __restrict__ dZD, long long total) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(i % 32);
+    const long long pix = i / 32;
+    const int q = (int)(pix % 18) - 1, p = (int)((pix / 18) % 18) - 1;  // crop coordinates
+    const long long b = pix / 324;
+    float s = 0.f;
+    if (p >= 0 && p < 16 && q >= 0 && q < 16 && __bfloat162float(fD[i]) > 0.f) {
+      for (int di = -4; di <= 4; ++di) {
+        const int ii = p - 4 - di;
+        if (ii < 0 || ii >= 8) continue;
+        for (int dj = -4; dj <= 4; ++dj) {
+          const int j = q - 4 - dj;
+          if (j < 0 || j >= 8) continue;
+          const long long rp = (b * 8 + ii) * 8 + j;
+          s = fmaf(dC[rp * kDisp + (di + 4) * 9 + (dj + 4)], __bfloat162float(fR[((b * 10 + ii + 1) * 10 + j + 1) * 32 + c]), s);
+        }
+      }
+    }
+    dZD[i] = __float2bfloat16_rn(s * (1.f / 32.f));
   }
 }
 
@@ -191,66 +346,63 @@ __global__ void to_bf16_kernel(const float* __restrict__ x, bf16* __restrict__ y
     y[i] = __float2bfloat16_rn(x[i]);
 }
 
-// The network input of subset t: the reference subset (rows x0-16 .. x0+15, columns
-// y0-16 .. y0+15, 1-based) in the centre of channel 0 and the deformed window (x0-32 ..
-// x0+31, y0-32 .. y0+31) in channel 1, each normalised to zero mean and unit deviation over
-// its own pixels (taps clamped to the image).  One block of 256 threads per subset.
+// The network input of subset t (centre rounded to whole pixels): the frame's normalised
+// deformed image over rows x0-36 .. x0+35 and columns y0-36 .. y0+35 (1-based) in channel 1,
+// its normalised reference image over the centre 40 x 40 of that window (rows x0-20 .. x0+19)
+// in channel 0, zero outside the image.  One block of 256 threads per subset.
 __global__ void patch_kernel(FrameDev fr, const double* __restrict__ coords, long long n, bf16* __restrict__ X) {
-  __shared__ double red[2][256];
   const long long t = blockIdx.x;
   if (t >= n) return;
-  const int tid = threadIdx.x;
   const int x0 = (int)llround(coords[t]), y0 = (int)llround(coords[n + t]);
-  auto at = [&](const float* img, int r1, int c1) {  // 1-based, clamped
-    r1 = r1 < 1 ? 1 : (r1 > fr.M ? fr.M : r1);
-    c1 = c1 < 1 ? 1 : (c1 > fr.N ? fr.N : c1);
-    return img[(size_t)(r1 - 1) + (size_t)(c1 - 1) * fr.M];
-  };
-  double sr = 0, sr2 = 0, sd = 0, sd2 = 0;
-  for (int p = tid; p < 4096; p += 256) {
-    const int i = p >> 6, j = p & 63;  // canvas row, column
-    const double d = at(fr.def, x0 - 32 + i, y0 - 32 + j);
-    sd += d;
-    sd2 += d * d;
-    if (p < 1024) {
-      const double r = at(fr.ref, x0 - 16 + (p >> 5), y0 - 16 + (p & 31));
-      sr += r;
-      sr2 += r * r;
-    }
-  }
-  double st[4] = {sr, sr2, sd, sd2};
-  double out[4];
-  for (int k = 0; k < 4; ++k) {
-    red[0][tid] = st[k];
-    __syncthreads();
-    for (int o = 128; o > 0; o >>= 1) {
-      if (tid < o) red[0][tid] += red[0][tid + o];
-      __syncthreads();
-    }
-    out[k] = red[0][0];
-    __syncthreads();
-  }
-  const double mr = out[0] / 1024.0, md = out[2] / 4096.0;
-  const double ir = 1.0 / sqrt(fmax(out[1] / 1024.0 - mr * mr, 1e-12));
-  const double id = 1.0 / sqrt(fmax(out[3] / 4096.0 - md * md, 1e-12));
-  bf16* x = X + t * 64 * 64 * 2;
-  for (int p = tid; p < 4096; p += 256) {
-    const int i = p >> 6, j = p & 63;
-    const bool in_ref = i >= 16 && i < 48 && j >= 16 && j < 48;
-    const float r = in_ref ? (float)((at(fr.ref, x0 - 32 + i, y0 - 32 + j) - mr) * ir) : 0.f;
-    const float d = (float)((at(fr.def, x0 - 32 + i, y0 - 32 + j) - md) * id);
-    x[(size_t)p * 2] = __float2bfloat16_rn(r);
-    x[(size_t)p * 2 + 1] = __float2bfloat16_rn(d);
+  bf16* x = X + t * kWin * kWin * 2;
+  for (int p = threadIdx.x; p < kWin * kWin; p += blockDim.x) {
+    const int i = p / kWin, j = p % kWin;
+    const int r1 = x0 - kWin / 2 + i, c1 = y0 - kWin / 2 + j;  // 1-based image pixel
+    const bool in_img = r1 >= 1 && r1 <= fr.M && c1 >= 1 && c1 <= fr.N;
+    const bool in_ref = i >= kRefOff && i < kRefOff + kRefWin && j >= kRefOff && j < kRefOff + kRefWin;
+    const size_t o = (size_t)(r1 - 1) + (size_t)(c1 - 1) * fr.M;
+    x[(size_t)p * 2] = __float2bfloat16_rn(in_img && in_ref ? fr.ref[o] : 0.f);
+    x[(size_t)p * 2 + 1] = __float2bfloat16_rn(in_img ? fr.def[o] : 0.f);
   }
 }
 
-// Network outputs (scaled) -> IC-GN initial guess: U0 = (u, v), F0 = (du/dx, dv/dx, du/dy, dv/dy)
-__global__ void unscale_kernel(const float* __restrict__ Y, long long n, double* __restrict__ U0, double* __restrict__ F0) {
+// A frame image (column-major M x N FP32) as a BF16 M x N row-major map (element (i, j) at
+// i N + j: image x along the map's rows), through 32 x 32 shared-memory tiles.
+__global__ void image_bf16_kernel(const float* __restrict__ img, int M, int N, bf16* __restrict__ out) {
+  __shared__ float t[32][33];
+  const int i0 = blockIdx.x * 32, j0 = blockIdx.y * 32;
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    const int i = i0 + threadIdx.x, j = j0 + k;
+    t[k][threadIdx.x] = (i < M && j < N) ? img[(size_t)i + (size_t)j * M] : 0.f;
+  }
+  __syncthreads();
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    const int i = i0 + k, j = j0 + threadIdx.x;
+    if (i < M && j < N) out[(size_t)i * N + j] = __float2bfloat16_rn(t[threadIdx.x][k]);
+  }
+}
+
+// Network outputs (scaled) -> IC-GN initial guess: U0 = (u, v), F0 = (du/dx, dv/dx, du/dy,
+// dv/dy).  With coords, the prediction belongs to the aligned centre (x = 1 mod 4) nearest the
+// subset's: U0 moves to the subset's own centre along F0; ok[t] = 0 gives NaN (no guess).
+__global__ void unscale_kernel(const float* __restrict__ Y, long long n, double* __restrict__ U0,
+                               double* __restrict__ F0, const double* __restrict__ coords, long long ncoords,
+                               const uint8_t* __restrict__ ok) {
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
     const float* y = Y + t * kOutP;
-    U0[2 * t] = 8.0 * y[0];
-    U0[2 * t + 1] = 8.0 * y[1];
-    for (int k = 0; k < 4; ++k) F0[4 * t + k] = y[2 + k] / 20.0;
+    double f[4];
+    for (int k = 0; k < 4; ++k) f[k] = y[2 + k] / 20.0;
+    double u = 8.0 * y[0], v = 8.0 * y[1];
+    if (coords) {
+      const double x = coords[t], yy = coords[ncoords + t];
+      const double ex = x - (4.0 * llround((x - 1.0) / 4.0) + 1.0), ey = yy - (4.0 * llround((yy - 1.0) / 4.0) + 1.0);
+      u += f[0] * ex + f[2] * ey;
+      v += f[1] * ex + f[3] * ey;
+    }
+    if (ok && !ok[t]) u = v = __longlong_as_double(0x7ff8000000000000LL);
+    U0[2 * t] = u;
+    U0[2 * t + 1] = v;
+    for (int k = 0; k < 4; ++k) F0[4 * t + k] = f[k];
   }
 }
 
@@ -271,10 +423,19 @@ struct ProposalNet {
   bf16* wb = nullptr;
   bf16* wt[6] = {};  // transposed weights [cols x rows] for the data gradients
   int step_count = 0;
-  // activations and their gradients (max_batch)
-  bf16 *A[4] = {}, *At[4] = {}, *H[5] = {}, *Ht[5] = {}, *dZ[5] = {}, *dZt[5] = {}, *dY = nullptr, *dYt = nullptr;
+  // activations and their gradients (max_batch): per convolution its im2col rows A and their
+  // transpose At, output H (NHWC) and output gradient dZ with its transpose dZt; the
+  // correlation volume Cv; FC1's input transposed (Ht5), output H6 (Ht6) and output gradient
+  // dZ6 (dZt6); the output gradient dY (dYt)
+  bf16 *A[kNumConv] = {}, *At[kNumConv] = {}, *H[kNumConv] = {}, *dZ[kNumConv] = {}, *dZt[kNumConv] = {};
+  bf16 *Cv = nullptr, *Ht5 = nullptr, *H6 = nullptr, *Ht6 = nullptr, *dZ6 = nullptr, *dZt6 = nullptr;
+  bf16 *dY = nullptr, *dYt = nullptr;
   float *dAf = nullptr, *dHf = nullptr, *Y = nullptr, *loss = nullptr;
-  bf16* Xbuf = nullptr;  // patch batch for predict
+  uint8_t* ok = nullptr;  // per predicted subset: its feature crops lie inside the maps
+  // whole-image features for prediction (sized for the last frame size): the BF16 image,
+  // conv1's im2col rows and output, conv2's im2col rows, the reference and deformed maps
+  int fM = 0, fN = 0;
+  bf16 *imgb = nullptr, *A1i = nullptr, *H1i = nullptr, *A2i = nullptr, *FR = nullptr, *FD = nullptr;
   int* errflag = nullptr;
 };
 
@@ -295,7 +456,7 @@ namespace {
     }                                                                             \
   } while (0)
 
-long long P_of(int l, int batch) { return (long long)batch * kConv[l].Hout * kConv[l].Wout; }
+long long P_of(int i, int batch) { return (long long)batch * kConv[i].Hout * kConv[i].Hout; }
 
 int gemm(ProposalNet* net, const void* A, long long lda, const void* B, long long ldb, long long M, long long N,
          long long K, int mode, float* c32, bf16* c16, const float* bias, long long ldc, int splits) {
@@ -338,80 +499,127 @@ int wsplit(long long M, long long N, long long K) {
   return (int)(s < 1 ? 1 : s);
 }
 
-int forward(ProposalNet* net, int batch, const bf16* X) {
-  const bf16* in = X;
-  for (int l = 0; l < 4; ++l) {
-    const ConvL& L = kConv[l];
-    const long long P = P_of(l, batch);
-    im2col_kernel<<<blocks_for(P * L.Kp), 256, 0, net->stream>>>(in, net->A[l], batch, L);
-    ++net->launches;
-    int rc = gemm(net, net->A[l], L.Kp, net->wb + kL.w[l], L.Kp, P, L.Cout, L.Kp, kEpiBiasReluBf16, nullptr,
-                  net->H[l], net->w + kL.b[l], L.Cout, 1);
-    if (rc) return rc;
-    in = net->H[l];
-  }
-  int rc = gemm(net, net->H[3], kFcIn, net->wb + kL.w[4], kFcIn, batch, kFcHid, kFcIn, kEpiBiasReluBf16, nullptr,
-                net->H[4], net->w + kL.b[4], kFcHid, 1);
+// im2col of convolution i's input (at `in` seen through v) and its GEMM with bias + ReLU
+int conv_forward(ProposalNet* net, int i, int batch, const bf16* in, View v) {
+  const ConvI& L = kConv[i];
+  const long long P = P_of(i, batch);
+  im2col_kernel<<<blocks_for(P * (L.Kp / 8)), 256, 0, net->stream>>>(in, v, net->A[i], P, L);
+  ++net->launches;
+  return gemm(net, net->A[i], L.Kp, net->wb + kL.w[L.layer], L.Kp, P, L.Cout, L.Kp, kEpiBiasReluBf16, nullptr,
+              net->H[i], net->w + kL.b[L.layer], L.Cout, 1);
+}
+
+// the layers after the correlation volume net->Cv: conv3, conv4, FC1, FC2 (into net->Y)
+int head(ProposalNet* net, int batch) {
+  int rc = conv_forward(net, kConv3, batch, net->Cv, nhwc(8, 8, kDisp));
+  if (!rc) rc = conv_forward(net, kConv4, batch, net->H[kConv3], nhwc(4, 4, 64));
+  if (!rc)
+    rc = gemm(net, net->H[kConv4], kFcIn, net->wb + kL.w[4], kFcIn, batch, kFcHid, kFcIn, kEpiBiasReluBf16, nullptr,
+              net->H6, net->w + kL.b[4], kFcHid, 1);
   if (rc) return rc;
-  return gemm(net, net->H[4], kFcHid, net->wb + kL.w[5], kFcHid, batch, kOutP, kFcHid, kEpiStore, net->Y, nullptr,
+  return gemm(net, net->H6, kFcHid, net->wb + kL.w[5], kFcHid, batch, kOutP, kFcHid, kEpiStore, net->Y, nullptr,
               net->w + kL.b[5], kOutP, 1);
+}
+
+// crops of the kept features in the per-window conv2 outputs (B, 10, 10, 32) and (B, 18, 18, 32)
+constexpr Crop kCropR{10 * 10 * 32, (10 + 1) * 32, 10 * 32};
+constexpr Crop kCropD{18 * 18 * 32, (18 + 1) * 32, 18 * 32};
+
+int forward(ProposalNet* net, int batch, const bf16* X) {
+  int rc = conv_forward(net, kConvR1, batch, X, kViewRef);
+  if (!rc) rc = conv_forward(net, kConvD1, batch, X, kViewDef);
+  if (!rc) rc = conv_forward(net, kConvR2, batch, net->H[kConvR1], nhwc(20, 20, 32));
+  if (!rc) rc = conv_forward(net, kConvD2, batch, net->H[kConvD1], nhwc(36, 36, 32));
+  if (rc) return rc;
+  const long long nc = (long long)batch * 64 * kDisp;
+  corr_kernel<<<blocks_for(nc), 256, 0, net->stream>>>(net->H[kConvR2], kCropR, net->H[kConvD2], kCropD, net->Cv, nc);
+  ++net->launches;
+  return head(net, batch);
+}
+
+// weight and bias gradients of convolution i from its output gradient dZ[i] (added to net->g)
+int conv_wgrad(ProposalNet* net, int i, int batch) {
+  const ConvI& L = kConv[i];
+  const long long P = P_of(i, batch);
+  transpose(net, net->dZ[i], net->dZt[i], P, L.Cout);
+  transpose(net, net->A[i], net->At[i], P, L.Kp);
+  int rc = gemm(net, net->dZt[i], P, net->At[i], P, L.Cout, L.Kp, P, kEpiAtomic, net->g + kL.w[L.layer], nullptr,
+                nullptr, L.Kp, wsplit(L.Cout, L.Kp, P));
+  if (rc) return rc;
+  bias_grad_kernel<<<148, L.Cout, 0, net->stream>>>(net->dZ[i], P, L.Cout, net->g + kL.b[L.layer]);
+  ++net->launches;
+  return ALDIC_OK;
+}
+
+// gradient of convolution i's input: dA = dZ W, then col2im into net->dHf (FP32, the input's
+// NHWC layout)
+int conv_dgrad(ProposalNet* net, int i, int batch) {
+  const ConvI& L = kConv[i];
+  const long long P = P_of(i, batch);
+  int rc = gemm(net, net->dZ[i], L.Cout, net->wt[L.layer], L.Cout, P, L.Kp, L.Cout, kEpiStore, net->dAf, nullptr,
+                nullptr, L.Kp, 1);
+  if (rc) return rc;
+  const long long nin = (long long)batch * L.Hin * L.Hin * L.Cin;
+  col2im_kernel<<<blocks_for(nin), 256, 0, net->stream>>>(net->dAf, net->dHf, batch, L);
+  ++net->launches;
+  return ALDIC_OK;
+}
+
+void relu_grad(ProposalNet* net, const bf16* H, bf16* dZ, long long n) {
+  relu_grad_kernel<<<blocks_for(n), 256, 0, net->stream>>>(net->dHf, H, dZ, n);
+  ++net->launches;
 }
 
 // gradients of the mean squared error into net->g (zeroed here)
 int backward(ProposalNet* net, int batch, const float* T) {
   cudaStream_t st = net->stream;
+  const long long B = batch;
   NK(cudaMemsetAsync(net->g, 0, sizeof(float) * kL.n, st));
   NK(cudaMemsetAsync(net->loss, 0, sizeof(float), st));
   mse_kernel<<<1, 256, 0, st>>>(net->Y, T, batch, net->dY, net->loss);
   ++net->launches;
-  // transposed weights for the data gradients
+  // transposed weights for the data gradients (conv1's input needs none)
   for (int l = 1; l < 6; ++l) transpose(net, net->wb + kL.w[l], net->wt[l], kL.rows[l], kL.cols[l]);
-  // FC2: dW = dY^T H4, db = sum dY, dH4 = dY W
-  transpose(net, net->dY, net->dYt, batch, kOutP);
-  transpose(net, net->H[4], net->Ht[4], batch, kFcHid);
-  int rc = gemm(net, net->dYt, batch, net->Ht[4], batch, kOutP, kFcHid, batch, kEpiAtomic, net->g + kL.w[5], nullptr,
-                nullptr, kFcHid, wsplit(kOutP, kFcHid, batch));
+  // FC2: dW = dY^T H6, db = sum dY, dH6 = dY W
+  transpose(net, net->dY, net->dYt, B, kOutP);
+  transpose(net, net->H6, net->Ht6, B, kFcHid);
+  int rc = gemm(net, net->dYt, B, net->Ht6, B, kOutP, kFcHid, B, kEpiAtomic, net->g + kL.w[5], nullptr, nullptr,
+                kFcHid, wsplit(kOutP, kFcHid, B));
   if (rc) return rc;
-  bias_grad_kernel<<<64, kOutP, 0, st>>>(net->dY, batch, kOutP, net->g + kL.b[5]);
-  rc = gemm(net, net->dY, kOutP, net->wt[5], kOutP, batch, kFcHid, kOutP, kEpiStore, net->dHf, nullptr, nullptr,
-            kFcHid, 1);
+  bias_grad_kernel<<<64, kOutP, 0, st>>>(net->dY, B, kOutP, net->g + kL.b[5]);
+  ++net->launches;
+  rc = gemm(net, net->dY, kOutP, net->wt[5], kOutP, B, kFcHid, kOutP, kEpiStore, net->dHf, nullptr, nullptr, kFcHid, 1);
   if (rc) return rc;
-  relu_grad_kernel<<<blocks_for((long long)batch * kFcHid), 256, 0, st>>>(net->dHf, net->H[4], net->dZ[4],
-                                                                         (long long)batch * kFcHid);
-  // FC1: dW = dZ^T H3flat, db, dH3 = dZ W
-  transpose(net, net->dZ[4], net->dZt[4], batch, kFcHid);
-  transpose(net, net->H[3], net->Ht[3], batch, kFcIn);
-  rc = gemm(net, net->dZt[4], batch, net->Ht[3], batch, kFcHid, kFcIn, batch, kEpiAtomic, net->g + kL.w[4], nullptr,
-            nullptr, kFcIn, wsplit(kFcHid, kFcIn, batch));
+  relu_grad(net, net->H6, net->dZ6, B * kFcHid);
+  // FC1: dW = dZ6^T F, db, dF = dZ6 W (F = conv4's output, flattened)
+  transpose(net, net->dZ6, net->dZt6, B, kFcHid);
+  transpose(net, net->H[kConv4], net->Ht5, B, kFcIn);
+  rc = gemm(net, net->dZt6, B, net->Ht5, B, kFcHid, kFcIn, B, kEpiAtomic, net->g + kL.w[4], nullptr, nullptr, kFcIn,
+            wsplit(kFcHid, kFcIn, B));
   if (rc) return rc;
-  bias_grad_kernel<<<64, kFcHid, 0, st>>>(net->dZ[4], batch, kFcHid, net->g + kL.b[4]);
-  rc = gemm(net, net->dZ[4], kFcHid, net->wt[4], kFcHid, batch, kFcIn, kFcHid, kEpiStore, net->dHf, nullptr, nullptr,
-            kFcIn, 1);
+  bias_grad_kernel<<<64, kFcHid, 0, st>>>(net->dZ6, B, kFcHid, net->g + kL.b[4]);
+  ++net->launches;
+  rc = gemm(net, net->dZ6, kFcHid, net->wt[4], kFcHid, B, kFcIn, kFcHid, kEpiStore, net->dHf, nullptr, nullptr, kFcIn,
+            1);
   if (rc) return rc;
-  relu_grad_kernel<<<blocks_for((long long)batch * kFcIn), 256, 0, st>>>(net->dHf, net->H[3], net->dZ[3],
-                                                                        (long long)batch * kFcIn);
-  net->launches += 4;
-  // conv layers 4 .. 1: dW = dZ^T A, db, dA = dZ W -> col2im -> ReLU gradient of the input
-  for (int l = 3; l >= 0; --l) {
-    const ConvL& L = kConv[l];
-    const long long P = P_of(l, batch);
-    transpose(net, net->dZ[l], net->dZt[l], P, L.Cout);
-    transpose(net, net->A[l], net->At[l], P, L.Kp);
-    rc = gemm(net, net->dZt[l], P, net->At[l], P, L.Cout, L.Kp, P, kEpiAtomic, net->g + kL.w[l], nullptr, nullptr,
-              L.Kp, wsplit(L.Cout, L.Kp, P));
-    if (rc) return rc;
-    bias_grad_kernel<<<148, L.Cout, 0, st>>>(net->dZ[l], P, L.Cout, net->g + kL.b[l]);
-    ++net->launches;
-    if (l == 0) break;
-    rc = gemm(net, net->dZ[l], L.Cout, net->wt[l], L.Cout, P, L.Kp, L.Cout, kEpiStore, net->dAf, nullptr, nullptr,
-              L.Kp, 1);
-    if (rc) return rc;
-    const long long nin = (long long)batch * L.Hin * L.Win * L.Cin;
-    col2im_kernel<<<blocks_for(nin), 256, 0, st>>>(net->dAf, net->dHf, batch, L);
-    relu_grad_kernel<<<blocks_for(nin), 256, 0, st>>>(net->dHf, net->H[l - 1], net->dZ[l - 1], nin);
-    net->launches += 2;
-  }
-  return ALDIC_OK;
+  relu_grad(net, net->H[kConv4], net->dZ[kConv4], B * kFcIn);
+  // conv4, conv3
+  if ((rc = conv_wgrad(net, kConv4, batch)) || (rc = conv_dgrad(net, kConv4, batch))) return rc;
+  relu_grad(net, net->H[kConv3], net->dZ[kConv3], B * 16 * 64);
+  if ((rc = conv_wgrad(net, kConv3, batch)) || (rc = conv_dgrad(net, kConv3, batch))) return rc;
+  // correlation: dHf holds dC (B, 8, 8, 81); the ReLUs of conv2's outputs folded in
+  corr_grad_ref_kernel<<<blocks_for(B * 100 * 32), 256, 0, st>>>(net->dHf, net->H[kConvR2], net->H[kConvD2],
+                                                                  net->dZ[kConvR2], B * 100 * 32);
+  corr_grad_def_kernel<<<blocks_for(B * 324 * 32), 256, 0, st>>>(net->dHf, net->H[kConvR2], net->H[kConvD2],
+                                                                  net->dZ[kConvD2], B * 324 * 32);
+  net->launches += 2;
+  // conv2 and conv1 on the reference subset, then on the deformed window (shared weights)
+  if ((rc = conv_wgrad(net, kConvR2, batch)) || (rc = conv_dgrad(net, kConvR2, batch))) return rc;
+  relu_grad(net, net->H[kConvR1], net->dZ[kConvR1], B * 400 * 32);
+  if ((rc = conv_wgrad(net, kConvR1, batch))) return rc;
+  if ((rc = conv_wgrad(net, kConvD2, batch)) || (rc = conv_dgrad(net, kConvD2, batch))) return rc;
+  relu_grad(net, net->H[kConvD1], net->dZ[kConvD1], B * 1296 * 32);
+  return conv_wgrad(net, kConvD1, batch);
 }
 
 int check_errflag(ProposalNet* net) {
@@ -462,29 +670,31 @@ int aldic_net_create(aldic_net** out, int device, int max_batch) {
   if (e == cudaSuccess) e = cudaMalloc(&net->v, n * 4);
   if (e == cudaSuccess) e = cudaMalloc(&net->wb, n * 2);
   for (int l = 0; l < 6 && e == cudaSuccess; ++l) e = cudaMalloc(&net->wt[l], kL.rows[l] * kL.cols[l] * 2);
-  long long maxA = 0, maxH = 0;
-  for (int l = 0; l < 4 && e == cudaSuccess; ++l) {
-    const long long P = P_of(l, (int)B);
-    maxA = std::max(maxA, P * kConv[l].Kp);
-    maxH = std::max(maxH, (long long)B * kConv[l].Hin * kConv[l].Win * kConv[l].Cin);
-    e = cudaMalloc(&net->A[l], P * kConv[l].Kp * 2);
-    if (e == cudaSuccess) e = cudaMalloc(&net->At[l], P * kConv[l].Kp * 2);
-    if (e == cudaSuccess) e = cudaMalloc(&net->H[l], P * kConv[l].Cout * 2);
-    if (e == cudaSuccess) e = cudaMalloc(&net->Ht[l], P * kConv[l].Cout * 2);
-    if (e == cudaSuccess) e = cudaMalloc(&net->dZ[l], P * kConv[l].Cout * 2);
-    if (e == cudaSuccess) e = cudaMalloc(&net->dZt[l], P * kConv[l].Cout * 2);
+  long long maxA = 0, maxH = B * kFcIn;
+  for (int i = 0; i < kNumConv && e == cudaSuccess; ++i) {
+    const ConvI& L = kConv[i];
+    const long long P = P_of(i, (int)B);
+    maxA = std::max(maxA, P * L.Kp);
+    maxH = std::max(maxH, B * L.Hin * L.Hin * L.Cin);
+    e = cudaMalloc(&net->A[i], P * L.Kp * 2);
+    if (e == cudaSuccess) e = cudaMalloc(&net->At[i], P * L.Kp * 2);
+    if (e == cudaSuccess) e = cudaMalloc(&net->H[i], P * L.Cout * 2);
+    if (e == cudaSuccess) e = cudaMalloc(&net->dZ[i], P * L.Cout * 2);
+    if (e == cudaSuccess) e = cudaMalloc(&net->dZt[i], P * L.Cout * 2);
   }
-  if (e == cudaSuccess) e = cudaMalloc(&net->H[4], B * kFcHid * 2);
-  if (e == cudaSuccess) e = cudaMalloc(&net->Ht[4], B * kFcHid * 2);
-  if (e == cudaSuccess) e = cudaMalloc(&net->dZ[4], B * kFcHid * 2);
-  if (e == cudaSuccess) e = cudaMalloc(&net->dZt[4], B * kFcHid * 2);
+  if (e == cudaSuccess) e = cudaMalloc(&net->Cv, B * 64 * kDisp * 2);
+  if (e == cudaSuccess) e = cudaMalloc(&net->Ht5, B * kFcIn * 2);
+  if (e == cudaSuccess) e = cudaMalloc(&net->H6, B * kFcHid * 2);
+  if (e == cudaSuccess) e = cudaMalloc(&net->Ht6, B * kFcHid * 2);
+  if (e == cudaSuccess) e = cudaMalloc(&net->dZ6, B * kFcHid * 2);
+  if (e == cudaSuccess) e = cudaMalloc(&net->dZt6, B * kFcHid * 2);
   if (e == cudaSuccess) e = cudaMalloc(&net->dY, B * kOutP * 2);
   if (e == cudaSuccess) e = cudaMalloc(&net->dYt, B * kOutP * 2);
   if (e == cudaSuccess) e = cudaMalloc(&net->Y, B * kOutP * 4);
   if (e == cudaSuccess) e = cudaMalloc(&net->dAf, maxA * 4);
-  if (e == cudaSuccess) e = cudaMalloc(&net->dHf, std::max(maxH, B * kFcIn) * 4);
+  if (e == cudaSuccess) e = cudaMalloc(&net->dHf, maxH * 4);
   if (e == cudaSuccess) e = cudaMalloc(&net->loss, 4);
-  if (e == cudaSuccess) e = cudaMalloc(&net->Xbuf, B * 64 * 64 * 2 * 2);
+  if (e == cudaSuccess) e = cudaMalloc(&net->ok, B);
   if (e == cudaSuccess) e = cudaMalloc(&net->errflag, 4);
   if (e != cudaSuccess) return fail(e);
   cudaMemset(net->m, 0, n * 4);
@@ -500,21 +710,17 @@ void aldic_net_destroy(aldic_net* net) {
   if (!net) return;
   cudaSetDevice(net->device);
   if (net->stream) cudaStreamSynchronize(net->stream);
-  void* bufs[] = {net->w,  net->g,  net->m,    net->v,    net->wb, net->dY, net->dYt,   net->Y,
-                  net->dAf, net->dHf, net->loss, net->Xbuf, net->errflag};
+  void* bufs[] = {net->w,  net->g,   net->m,   net->v,   net->wb,  net->Cv,   net->Ht5, net->H6,     net->Ht6,
+                  net->dZ6, net->dZt6, net->dY, net->dYt, net->Y, net->dAf, net->dHf, net->loss, net->ok,  net->errflag,
+                  net->imgb, net->A1i, net->H1i, net->A2i, net->FR, net->FD};
   for (void* p : bufs)
     if (p) cudaFree(p);
   for (int l = 0; l < 6; ++l)
     if (net->wt[l]) cudaFree(net->wt[l]);
-  for (int l = 0; l < 5; ++l) {
-    if (l < 4) {
-      if (net->A[l]) cudaFree(net->A[l]);
-      if (net->At[l]) cudaFree(net->At[l]);
-    }
-    if (net->H[l]) cudaFree(net->H[l]);
-    if (net->Ht[l]) cudaFree(net->Ht[l]);
-    if (net->dZ[l]) cudaFree(net->dZ[l]);
-    if (net->dZt[l]) cudaFree(net->dZt[l]);
+  for (int i = 0; i < kNumConv; ++i) {
+    bf16* per[] = {net->A[i], net->At[i], net->H[i], net->dZ[i], net->dZt[i]};
+    for (bf16* p : per)
+      if (p) cudaFree(p);
   }
   if (net->own) cudaStreamDestroy(net->own);
   delete net;
@@ -627,22 +833,69 @@ int aldic_net_status(aldic_net* net) {
 }  // extern "C"
 
 namespace aldic {
-// Predict the initial guesses of n subsets (coords device n x 2) on the frame fr, in batches of
-// the network's max_batch; U0 (2n) and F0 (4n) device arrays.
+// conv1 and conv2 over the whole reference and deformed images of frame fr into net->FR and
+// net->FD: (M + 3) / 4 x (N + 3) / 4 x 32 maps whose pixel (i, j) is centred on image pixel
+// (4 i + 1, 4 j + 1) (1-based)
+int image_features(ProposalNet* net, const FrameDev& fr) {
+  const int M = fr.M, N = fr.N, M1 = (M + 1) / 2, N1 = (N + 1) / 2, M2 = (M1 + 1) / 2, N2 = (N1 + 1) / 2;
+  const long long P1 = (long long)M1 * N1, P2 = (long long)M2 * N2;
+  if (net->fM != M || net->fN != N) {
+    NK(cudaStreamSynchronize(net->stream));
+    bf16** bufs[] = {&net->imgb, &net->A1i, &net->H1i, &net->A2i, &net->FR, &net->FD};
+    for (bf16** b : bufs) {
+      if (*b) NK(cudaFree(*b));
+      *b = nullptr;
+    }
+    net->fM = net->fN = 0;
+    NK(cudaMalloc(&net->imgb, (size_t)M * N * 2));
+    NK(cudaMalloc(&net->A1i, (size_t)P1 * 16 * 2));
+    NK(cudaMalloc(&net->H1i, (size_t)P1 * 32 * 2));
+    NK(cudaMalloc(&net->A2i, (size_t)P2 * 288 * 2));
+    NK(cudaMalloc(&net->FR, (size_t)P2 * 32 * 2));
+    NK(cudaMalloc(&net->FD, (size_t)P2 * 32 * 2));
+    net->fM = M;
+    net->fN = N;
+  }
+  const ConvI c1{0, M, N, 1, M1, N1, 32, 9, 16, 2}, c2{1, M1, N1, 32, M2, N2, 32, 288, 288, 2};
+  for (int side = 0; side < 2; ++side) {
+    const dim3 tg((unsigned)((M + 31) / 32), (unsigned)((N + 31) / 32));
+    image_bf16_kernel<<<tg, dim3(32, 8), 0, net->stream>>>(side ? fr.def : fr.ref, M, N, net->imgb);
+    im2col_kernel<<<blocks_for(P1 * 2), 256, 0, net->stream>>>(net->imgb, View{0, 0, N, 1}, net->A1i, P1, c1);
+    net->launches += 2;
+    int rc = gemm(net, net->A1i, 16, net->wb + kL.w[0], 16, P1, 32, 16, kEpiBiasReluBf16, nullptr, net->H1i,
+                  net->w + kL.b[0], 32, 1);
+    if (rc) return rc;
+    im2col_kernel<<<blocks_for(P2 * 36), 256, 0, net->stream>>>(net->H1i, nhwc(M1, N1, 32), net->A2i, P2, c2);
+    ++net->launches;
+    rc = gemm(net, net->A2i, 288, net->wb + kL.w[1], 288, P2, 32, 288, kEpiBiasReluBf16, nullptr,
+              side ? net->FD : net->FR, net->w + kL.b[1], 32, 1);
+    if (rc) return rc;
+  }
+  return ALDIC_OK;
+}
+
+// Predict the initial guesses of n subsets (coords device n x 2) on the frame fr: the feature
+// maps of both images once, then the correlation volumes and the rest in batches of the
+// network's max_batch; U0 (2n) and F0 (4n) device arrays (U0 NaN where a subset's crops
+// leave the maps: no guess).
 int net_predict(aldic_net* net, const FrameDev& fr, const double* coords_dev, long long n, double* U0, double* F0) {
   NK(cudaSetDevice(net->device));
+  int rc = image_features(net, fr);
+  if (rc) return rc;
+  const int Hf = (fr.M + 3) / 4, Wf = (fr.N + 3) / 4;
   const int B = net->max_batch;
   for (long long s = 0; s < n; s += B) {
-    const long long nb = std::min<long long>(B, n - s);
-    const int bpad = (int)((nb + 7) / 8 * 8);
-    // the patch kernel reads x at coords[t] and y at coords[n + t]: the batch's slice is the
-    // same arrays offset by s
-    patch_kernel<<<(unsigned)nb, 256, 0, net->stream>>>(fr, coords_dev + s, n, net->Xbuf);
+    const int nb = (int)std::min<long long>(B, n - s);
+    const int bpad = (nb + 7) / 8 * 8;
+    corr_image_kernel<<<blocks_for((long long)nb * 64 * kDisp), 256, 0, net->stream>>>(
+        net->FR, net->FD, Hf, Wf, coords_dev, n, s, nb, net->Cv, net->ok);
     ++net->launches;
-    if (bpad > nb) NK(cudaMemsetAsync(net->Xbuf + nb * 64 * 64 * 2, 0, (size_t)(bpad - nb) * 64 * 64 * 2 * 2, net->stream));
-    int rc = forward(net, bpad, net->Xbuf);
+    if (bpad > nb)
+      NK(cudaMemsetAsync(net->Cv + (size_t)nb * 64 * kDisp, 0, (size_t)(bpad - nb) * 64 * kDisp * 2, net->stream));
+    rc = head(net, bpad);
     if (rc) return rc;
-    unscale_kernel<<<blocks_for(nb), 256, 0, net->stream>>>(net->Y, nb, U0 + 2 * s, F0 + 4 * s);
+    unscale_kernel<<<blocks_for(nb), 256, 0, net->stream>>>(net->Y, nb, U0 + 2 * s, F0 + 4 * s, coords_dev + s, n,
+                                                           net->ok);
     ++net->launches;
   }
   NK(cudaGetLastError());

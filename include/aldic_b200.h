@@ -256,23 +256,26 @@ int aldic_local_icgn_noalloc(int variant, const float* ref, const float* def, co
  * (func/funIntegerSearch.m:132-180); that search stays the fallback and the judge.
  *
  * A proposal network: a 32 x 32 reference subset and the 64 x 64 deformed window around it
- * (each normalised to zero mean, unit deviation) -> the subset's (u, v, du/dx, dv/dx, du/dy,
- * dv/dy).  Four 3 x 3 stride-2 convolutions (2 -> 32 -> 32 -> 64 -> 64 channels, 64 -> 4
- * pixels) and two fully connected layers (1024 -> 128 -> 6), ReLU between, 197 254 FP32
- * parameters with BF16 copies; every layer, gradient and weight gradient is a BF16 x BF16 ->
- * FP32 tensor-core GEMM (tcgen05, TMA-staged operands).  Outputs are scaled (u / 8, v / 8,
- * gradients x 20).  Inputs x: batch x 64 x 64 x 2 BF16 (NHWC, channel 0 the reference subset
- * in the centre of a zero canvas, channel 1 the window), device memory; targets t: batch x 6
- * FP32 (device), scaled as the outputs.  batch a multiple of 8, at most max_batch. */
+ * -> the subset's (u, v, du/dx, dv/dx, du/dy, dv/dy).  The same two 3 x 3 stride-2
+ * convolutions (1 -> 32 -> 32 channels) turn the subset into 8 x 8 and the window into
+ * 16 x 16 feature maps, their correlation over 9 x 9 offsets (+-16 px) gives an 8 x 8 x 81
+ * volume, then a 3 x 3 stride-2 and a 3 x 3 stride-1 convolution (81 -> 64 -> 64 channels,
+ * 4 x 4) and two fully connected layers (1024 -> 128 -> 6), ReLU between: 227 152 FP32
+ * parameters with BF16 copies; every layer, data gradient and weight gradient is a BF16 x
+ * BF16 -> FP32 tensor-core GEMM (tcgen05, TMA-staged operands).  Outputs are scaled (u / 8,
+ * v / 8, gradients x 20).  Inputs x: batch x 72 x 72 x 2 BF16 (NHWC; the window with 4 px of
+ * context each side in channel 1, the subset with 4 px of context, 40 x 40, in the centre of
+ * channel 0, zero elsewhere), device memory; targets t: batch x 6 FP32 (device), scaled as the
+ * outputs.  batch a multiple of 8, at most max_batch. */
 int aldic_net_create(aldic_net** net, int device, int max_batch);
 void aldic_net_destroy(aldic_net* net);
 const char* aldic_net_last_error(const aldic_net* net);
 int aldic_net_set_stream(aldic_net* net, void* stream);
 int64_t aldic_net_launch_count(const aldic_net* net);
 /* Number of FP32 parameters and their flat layout: per layer W (rows x cols, row-major) then
- * b: conv 32 x 24 (K = 3 x 3 x 2 taps, padded to 24 with zeros), 32 x 288, 64 x 288, 64 x 576
- * (K ordered (ky, kx, channel)); FC 128 x 1024 (input ordered (y, x, channel) of the 4 x 4 x 64
- * map), 16 x 128 (rows 6..15 zero, as biases 6..15). */
+ * b: conv 32 x 16 (K = 9 taps, padded to 16 with zeros), 32 x 288, 64 x 736 (K = 729 padded),
+ * 64 x 576 (K ordered (ky, kx, channel)); FC 128 x 1024 (input ordered (y, x, channel) of the
+ * 4 x 4 x 64 map), 16 x 128 (rows 6..15 zero, as biases 6..15). */
 int64_t aldic_net_param_count(void);
 /* Parameters in (host or device FP32); resets the Adam moments. */
 int aldic_net_set_params(aldic_net* net, const float* params);
@@ -287,15 +290,19 @@ int aldic_net_gradients(aldic_net* net, int batch, const void* x, const float* t
 int aldic_net_train_step(aldic_net* net, int batch, const void* x, const float* t, float lr, float* loss);
 /* ALDIC_OK, or ALDIC_ERR_TIMEOUT if a GEMM's bounded wait timed out since creation. */
 int aldic_net_status(aldic_net* net);
-/* Initial guesses of n subsets (coords n x 2, 1-based, rounded) on the frame of ctx (REF and
- * DEF slots): U0 (2n interleaved) and F0 (4n, [F11 F21 F12 F22] = [du/dx dv/dx du/dy dv/dy])
- * for aldic_local_icgn_guess.  Runs on the context's stream. */
+/* Initial guesses of n subsets (coords n x 2, 1-based) on the frame of ctx (REF and DEF
+ * slots): U0 (2n interleaved) and F0 (4n, [F11 F21 F12 F22] = [du/dx dv/dx du/dy dv/dy]) for
+ * aldic_local_icgn_guess.  The two shared convolutions run once over each whole image; each
+ * subset reads its feature crops at the nearest centre with x, y = 1 (mod 4) (equal to the
+ * per-window network there) and its U0 is moved to its own centre along F0.  U0 is NaN where
+ * the crops leave the feature maps (centres nearer than 32 px to the first row or column, or
+ * than about 26 px to the last).  Runs on the context's stream. */
 int aldic_net_predict(aldic_net* net, aldic_ctx* ctx, int64_t n, const double* coords, double* U0, double* F0);
 /* The network input of n subsets (coords n x 2, 1-based, rounded) on the frame of ctx: X
- * (device, n x 64 x 64 x 2 BF16), channel 0 the reference subset (rows x0-16 .. x0+15, columns
- * y0-16 .. y0+15) in the centre of a zero canvas, channel 1 the deformed window (x0-32 ..
- * x0+31, y0-32 .. y0+31), each normalised to zero mean and unit deviation (taps clamped to
- * the image).  For training sets; aldic_net_predict builds the same inputs itself. */
+ * (device, n x 72 x 72 x 2 BF16), channel 1 the normalised deformed image over rows x0-36 ..
+ * x0+35 and columns y0-36 .. y0+35, channel 0 the normalised reference image over the centre
+ * 40 x 40 (x0-20 .. x0+19, y0-20 .. y0+19), zero elsewhere and outside the image.  For
+ * training sets and checks of aldic_net_predict. */
 int aldic_net_extract(aldic_ctx* ctx, int64_t n, const double* coords, void* X);
 /* aldic_local_icgn from the initial guess P = [F0 U0] instead of [0 U0] (the reference starts
  * from F = 0, func/funICGN.m:46); everything else as aldic_local_icgn. */

@@ -38,9 +38,9 @@ def test_tensor_core_gemm_matches_numpy(M, N, K, splits):
 
 def _batch(seed, B):
     rng = np.random.default_rng(seed)
-    X = rng.normal(size=(B, 64, 64, 2)).astype(np.float32)
+    X = rng.normal(size=(B, 72, 72, 2)).astype(np.float32)
     X[:, :, :, 0] = 0.0
-    X[:, 16:48, 16:48, 0] = rng.normal(size=(B, 32, 32))
+    X[:, 16:56, 16:56, 0] = rng.normal(size=(B, 40, 40))
     T = rng.normal(scale=0.5, size=(B, 6)).astype(np.float32)
     return CO.bf16(X), T
 

@@ -112,9 +112,12 @@ def test_list_search_matches_the_whole_grid(env):
     rng = np.random.default_rng(3)
     idx = rng.choice(nx * ny, size=min(37, nx * ny), replace=False).astype(np.int32)
     lst = ctx.integer_search_list([8, 8], gx, gy, w, st, idx)
-    for k in ("x", "y", "u", "v", "phi"):
+    for k in ("x", "y", "u", "v"):
         want = full[k].ravel()[idx]  # the (nY, nX) grid in list order i + j nX
         assert np.array_equal(lst[k], want, equal_nan=True), k
+    # the peak ZNCC: the list runs the direct correlation, the whole grid the shared-product
+    # kernel, whose sums round differently
+    assert np.abs(lst["phi"] - full["phi"].ravel()[idx]).max() < 1e-6
     # device list and outputs
     dev = torch.device("cuda:0")
     out = {k: torch.empty(idx.size, dtype=torch.float64, device=dev) for k in ("x", "y", "u", "v", "phi")}
@@ -133,15 +136,15 @@ def test_list_search_matches_the_whole_grid(env):
 
 def _patches_numpy(f, g, crd):
     M, N = f.shape
-    out = np.zeros((crd.shape[0], 64, 64, 2))
+    out = np.zeros((crd.shape[0], 72, 72, 2))
     for t, (x, y) in enumerate(crd):
         x0, y0 = int(round(x)), int(round(y))
-        ri = np.clip(np.arange(x0 - 32, x0 + 32), 1, M) - 1
-        ci = np.clip(np.arange(y0 - 32, y0 + 32), 1, N) - 1
-        d = g[np.ix_(ri, ci)]
-        r = f[np.ix_(ri[16:48], ci[16:48])]
-        out[t, :, :, 1] = (d - d.mean()) / np.sqrt(max(d.var(), 1e-12))
-        out[t, 16:48, 16:48, 0] = (r - r.mean()) / np.sqrt(max(r.var(), 1e-12))
+        r1, c1 = np.arange(x0 - 36, x0 + 36), np.arange(y0 - 36, y0 + 36)
+        inr, inc = (r1 >= 1) & (r1 <= M), (c1 >= 1) & (c1 <= N)
+        ri, ci = np.clip(r1, 1, M) - 1, np.clip(c1, 1, N) - 1
+        keep = np.outer(inr, inc)
+        out[t, :, :, 1] = np.where(keep, g[np.ix_(ri, ci)], 0.0)
+        out[t, 16:56, 16:56, 0] = np.where(keep, f[np.ix_(ri, ci)], 0.0)[16:56, 16:56]
     return out
 
 
@@ -150,23 +153,35 @@ def test_network_patches_and_prediction(env):
     from aldic_b200.learned import ProposalNet
 
     dev = torch.device("cuda:0")
-    crd = _nodes(pair.M, pair.N, step=10)[:150]
-    crd[-1] = [3.0, 250.0]  # a window clamped at the image border
+    # centres = 1 (mod 4) far enough from the border that every crop is the whole-image one,
+    # one off the 4-grid (moved to its aligned neighbour), one at the border (no guess)
+    g = np.arange(41, 216, 8, dtype=np.float64)
+    X_, Y_ = np.meshgrid(g, g, indexing="ij")
+    crd = np.stack([X_.ravel(), Y_.ravel()], 1)[:150].copy()
+    crd[-2] = [102.0, 130.0]
+    crd[-1] = [9.0, 120.0]
     n = crd.shape[0]
     ct = torch.from_numpy(np.ascontiguousarray(crd.T)).to(dev)
-    X = torch.empty((n, 64, 64, 2), dtype=torch.bfloat16, device=dev)
+    X = torch.empty((n, 72, 72, 2), dtype=torch.bfloat16, device=dev)
     ctx.net_extract(ct, X)
     ctx.synchronize()
     got = X.float().cpu().numpy()
+    # the device's normalised images are FP32 copies of the oracle's FP64 ones: BF16 values
+    # agree up to the rare tie
     want = CO.bf16(_patches_numpy(env["f"], env["g"], crd).astype(np.float32))
-    same = got == want
-    assert same.mean() > 0.999
+    assert (got == want).mean() > 0.999
     assert np.abs(got - want).max() <= 2.0 ** -7 * max(1.0, np.abs(want).max())
     net = ProposalNet(0, max_batch=64, seed=5)
     try:
         b = {"U0": torch.empty(2 * n, dtype=torch.float64, device=dev),
              "F0": torch.empty(4 * n, dtype=torch.float64, device=dev)}
         net.predict(ctx, ct, b)
+        ctx.synchronize()
+        # the per-window network on the same windows (the off-grid one at its aligned centre)
+        crd_al = crd.copy()
+        crd_al[-2] = [101.0, 129.0]
+        ca = torch.from_numpy(np.ascontiguousarray(crd_al.T)).to(dev)
+        ctx.net_extract(ca, X)
         ctx.synchronize()
         Y = torch.empty((n + 2, 6), dtype=torch.float32, device=dev)
         Xp = torch.cat([X, X[:2]])  # a multiple of 8 rows
@@ -175,59 +190,92 @@ def test_network_patches_and_prediction(env):
             net.forward(Xp[s:e].contiguous(), Y[s:e])
         torch.cuda.synchronize()
         y = Y[:n].cpu().numpy().astype(np.float64)
-        assert np.array_equal(b["U0"].cpu().numpy().reshape(n, 2), 8.0 * y[:, :2].astype(np.float32))
+        U0 = b["U0"].cpu().numpy().reshape(n, 2)
         F0 = b["F0"].cpu().numpy().reshape(n, 4)
-        assert np.abs(F0 - y[:, 2:] / 20.0).max() <= 1e-7 * max(1.0, np.abs(y).max())
+        m = n - 2
+        assert np.array_equal(U0[:m], 8.0 * y[:m, :2])
+        assert np.abs(F0[:m] - y[:m, 2:] / 20.0).max() <= 1e-7 * max(1.0, np.abs(y).max())
+        # the off-grid centre: the aligned prediction moved along F0 by (1, 1) px
+        f = F0[-2]
+        want_u = 8.0 * y[-2, :2] + np.array([f[0] + f[2], f[1] + f[3]])
+        assert np.abs(U0[-2] - want_u).max() < 1e-6
+        assert np.all(np.isnan(U0[-1]))
     finally:
         net.close()
 
 
-def test_trained_network_beats_the_search_guess():
-    """Train on six 512 x 512 speckle pairs (labels: converged IC-GN from the analytic guess),
-    then on a held-out pair: IC-GN from the network's guess converges on at least as many
-    subsets as from the integer search's guess, in fewer iterations, with few fallbacks."""
-    import torch
+def test_training_lowers_the_held_out_error():
+    """A short training run on tile mosaics (every tile its own speckles and affine warp,
+    labelled by IC-GN): the held-out displacement error falls well below the untrained one."""
+    import aldic_b200 as A
+    from aldic_b200 import train_net
+    from aldic_b200.learned import ProposalNet
+
+    net, summary = train_net.train_network(frames=12, steps=1500, batch=256, lr=2e-3, eval_frames=1)
+    fresh = ProposalNet(0, max_batch=4096, seed=0)
+    ctx = A.Context(0)
+    try:
+        Xe, Te = train_net.build_dataset(ctx, 1, 900000)
+        before = train_net.evaluate(fresh, Xe, Te)
+        after = summary["held_out"]
+        assert after["u_px_p50"] < 0.5 * before["u_px_p50"], (before, after)
+        assert summary["loss"][-1][1] < 0.3 * summary["loss"][0][1]
+    finally:
+        ctx.close()
+        fresh.close()
+        net.close()
+
+
+def test_trained_network_gains_over_the_search_guess():
+    """The shipped trained network on a held-out smooth-field pair (512 x 512): IC-GN from its
+    guess converges where IC-GN from the integer search's guess does, to the same solution,
+    with few fallbacks; its gradient guess is far closer to the converged gradient than the
+    search's F = 0; an untrained network's guesses mostly fall back."""
+    import os
 
     import aldic_b200 as A
     from aldic_b200 import learned as L
-    from aldic_b200 import synth_gpu
+    from aldic_b200 import synth_gpu, train_net
 
+    if not os.path.exists(train_net.DEFAULT_WEIGHTS):
+        pytest.skip("no trained weights shipped")
     ctx = A.Context(0)
-    net = L.ProposalNet(0, max_batch=512, seed=0)
+    net = L.ProposalNet(0, max_batch=4096)
     try:
-        Xs, Ts = [], []
-        for s in range(6):
-            X, T = L.label_pair(ctx, synth_gpu.field_pair(100 + s, M=512, N=512), w=32, step=6)
-            Xs.append(X)
-            Ts.append(T)
-        X, T = torch.cat(Xs), torch.cat(Ts)
-        log = L.train(net, X, T, steps=1500, batch=256, lr=2e-3, lr_end=2e-5)
-        assert log[-1][1] < 0.2 * log[0][1]
         pair = synth_gpu.field_pair(999, M=512, N=512)
         M, N = pair.M, pair.N
-        gx, gy, w, st, s = [17, M - 16], [17, N - 16], 32, 16, 16
+        gx, gy, w, st, s = [21, M - 20], [21, N - 20], 32, 16, 16
         ctx.load_image_raw(0, pair.ref, gx, gy, want_stats=False, shape=(M, N))
         ctx.load_image_raw(1, pair.deff, gx, gy, want_stats=False, shape=(M, N))
         ctx.compute_gradients()
-        li = L.LearnedInit(net, ctx, s, gx, gy, w, st, 1e-3)
-        nf = li.run()
-        li.stream.synchronize()
-        conv_l = li.buf["conv"].cpu().numpy()
         # the reference's start: the integer search, outliers removed, inpainted, F = 0
         r = ctx.integer_search([s, s], gx, gy, w, st)
         u, v, _ = O.remove_outliers(r["u"], r["v"], 100.0)
         U0 = O.init_u0(u, v)
+        li = L.LearnedInit(net, ctx, s, gx, gy, w, st, 1e-3)
         crd = li.coords.cpu().numpy().T.copy()
         f = ctx.local_icgn(A.QUADTREE, crd, U0, w, 1e-3, want_H=False)
-        ok_l = (conv_l > 0) & (conv_l < 100)
         ok_f = (f["conv"] > 0) & (f["conv"] < 100)
-        assert ok_l.sum() >= ok_f.sum()
+
+        net.set_params(L.init_params(0))  # untrained
+        nf0 = li.run()
+        li.stream.synchronize()
+        net.set_params(np.load(train_net.DEFAULT_WEIGHTS))
+        nf = li.run()
+        li.stream.synchronize()
+        b = {k: v.cpu().numpy() for k, v in li.buf.items()}
+        ok_l = (b["conv"] > 0) & (b["conv"] < 100)
+        assert nf0 > 0.5 * li.n and nf <= 0.02 * li.n, (nf0, nf, li.n)
+        assert ok_l[ok_f].all()
         both = ok_l & ok_f
-        it_l, it_f = conv_l[both].mean(), f["conv"][both].mean()
-        assert it_l < it_f, (it_l, it_f)
-        assert nf <= 0.1 * li.n
-        d = np.abs(li.buf["U"].cpu().numpy() - f["U"]).reshape(-1, 2)[both]
-        assert np.median(d) < 1e-3
+        assert np.abs(b["U"] - f["U"]).reshape(-1, 2)[both].max() < 1e-2
+        keep = ~b["fallback"]
+        Fc = b["F"].reshape(-1, 4)[keep & both]
+        err_net = np.median(np.abs(b["F0"].reshape(-1, 4)[keep & both] - Fc))
+        err_zero = np.median(np.abs(Fc))
+        assert err_net < 0.5 * err_zero, (err_net, err_zero)
+        du = np.hypot(*(b["U0"].reshape(-1, 2)[keep] - b["U"].reshape(-1, 2)[keep]).T)
+        assert np.median(du) < 0.5
     finally:
         net.close()
         ctx.close()
