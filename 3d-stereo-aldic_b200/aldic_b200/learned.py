@@ -271,14 +271,30 @@ class LearnedInit:
                     "F": T.empty(4 * n, **f64), "conv": T.empty(n, dtype=T.int32, device=dev),
                     "zncc": T.empty(n, **f64), "fallback": T.zeros(n, dtype=T.bool, device=dev)}
         self.n_fallback = 0
+        # (start, stop) CUDA event pairs recorded around the prediction and the main IC-GN call
+        # when these are lists (timing hooks)
+        self.predict_events = None
+        self.icgn_events = None
+
+    def _timed(self, events, fn):
+        if events is None:
+            return fn()
+        T = self.T
+        e = (T.cuda.Event(enable_timing=True), T.cuda.Event(enable_timing=True))
+        e[0].record(self.stream)
+        r = fn()
+        e[1].record(self.stream)
+        events.append(e)
+        return r
 
     def run(self):
         """One frame; returns the number of fallback subsets."""
         T, ctx, b, n = self.T, self.ctx, self.buf, self.n
         with T.cuda.stream(self.stream):
-            self.net.predict(ctx, self.coords, b)
-            ctx.local_icgn(self.variant, self.coords, b["U0"], self.w, self.tol, want_H=False, want_mark=False,
-                           out=b, F0=b["F0"])
+            self._timed(self.predict_events, lambda: self.net.predict(ctx, self.coords, b))
+            self._timed(self.icgn_events,
+                        lambda: ctx.local_icgn(self.variant, self.coords, b["U0"], self.w, self.tol, want_H=False,
+                                               want_mark=False, out=b, F0=b["F0"]))
             ctx.subset_zncc(self.coords, b["U"], b["F"], self.w, out=b["zncc"])
             c = b["conv"]
             bad = (c < 1) | (c > 100) | ~(b["zncc"] >= self.zncc_min)

@@ -39,6 +39,7 @@
 #include "../../include/aldic_b200.h"
 #include "cnn.h"
 #include "kernels.h"
+#include "umma.cuh"
 
 namespace aldic {
 namespace {
@@ -98,7 +99,8 @@ __device__ __forceinline__ long long ceil_div_ll(long long a, long long b) { ret
 
 // ------------------------------------------------------------------------- kernels
 // im2col of a 3 x 3, pad-1 convolution: row p = (b, oy, ox), column k = (ky, kx, ci), zero
-// outside the input and in the K padding.  Each thread writes 8 columns (one 16-byte store).
+// outside the input and in the K padding.  Each thread writes 8 columns (one 16-byte store);
+// with Cin a multiple of 8 (16-byte aligned channel runs) it also reads them in one load.
 __global__ void im2col_kernel(const bf16* __restrict__ in, View v, bf16* __restrict__ A, long long P, ConvI L) {
   const int groups = L.Kp / 8;
   const long long total = P * groups;
@@ -108,6 +110,17 @@ __global__ void im2col_kernel(const bf16* __restrict__ in, View v, bf16* __restr
     const int ox = (int)(p % L.Wout), oy = (int)((p / L.Wout) % L.Hout);
     const long long b = p / ((long long)L.Wout * L.Hout);
     const bf16* base = in + v.off + b * v.sb;
+    if (L.Cin % 8 == 0) {  // the 8 columns are 8 channels of one tap: one 16-byte load
+      uint4 val = make_uint4(0u, 0u, 0u, 0u);
+      if (k0 < L.K) {
+        const int tap = k0 / L.Cin, ci = k0 % L.Cin, ky = tap / 3, kx = tap % 3;
+        const int iy = L.stride * oy - 1 + ky, ix = L.stride * ox - 1 + kx;
+        if (iy >= 0 && iy < L.Hin && ix >= 0 && ix < L.Win)
+          val = *reinterpret_cast<const uint4*>(base + iy * v.sy + ix * v.sx + ci);
+      }
+      *reinterpret_cast<uint4*>(A + p * L.Kp + k0) = val;
+      continue;
+    }
     __align__(16) bf16 vals[8];
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
@@ -148,76 +161,6 @@ __global__ void col2im_kernel(const float* __restrict__ dA, float* __restrict__ 
       }
     }
     dH[i] = acc;
-  }
-}
-
-// 8 BF16 -> 8 floats
-__device__ __forceinline__ void load8(const bf16* p, float (&f)[8]) {
-  const uint4 u = *reinterpret_cast<const uint4*>(p);
-  const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&u);
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    const float2 t = __bfloat1622float2(h[k]);
-    f[2 * k] = t.x;
-    f[2 * k + 1] = t.y;
-  }
-}
-
-// one correlation entry: reference feature r (32 channels) against deformed feature q
-__device__ __forceinline__ float dot32(const bf16* r, const bf16* q) {
-  float s = 0.f;
-#pragma unroll
-  for (int c = 0; c < 32; c += 8) {
-    float a[8], e[8];
-    load8(r + c, a);
-    load8(q + c, e);
-#pragma unroll
-    for (int k = 0; k < 8; ++k) s = fmaf(a[k], e[k], s);
-  }
-  return s;
-}
-
-// correlation volume C (B, 8, 8, 81) of the reference crops against the deformed crops, BF16
-__global__ void corr_kernel(const bf16* __restrict__ fR, Crop cr, const bf16* __restrict__ fD, Crop cd,
-                            bf16* __restrict__ C, long long total) {
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
-    const int d = (int)(i % kDisp);
-    const long long pos = i / kDisp;
-    const int j = (int)(pos % 8), ii = (int)((pos / 8) % 8);
-    const long long b = pos / 64;
-    const int di = d / 9 - 4, dj = d % 9 - 4;
-    const bf16* r = fR + b * cr.sb + cr.off + ii * cr.row + j * 32;
-    const bf16* q = fD + b * cd.sb + cd.off + (ii + 4 + di) * cd.row + (j + 4 + dj) * 32;
-    C[i] = __float2bfloat16_rn(dot32(r, q) * (1.f / 32.f));
-  }
-}
-
-// The same volume for subsets t0 .. t0 + nb - 1 of coords (n x 2) from the feature maps of the
-// whole reference and deformed images (Hf x Wf x 32 each, element (i, j) the features centred
-// on image pixel (4 i + 1, 4 j + 1)): the reference crop starts at ((x - 17) / 4, (y - 17) / 4),
-// the deformed crop at ((x - 33) / 4, (y - 33) / 4), x, y the subset centre moved to the
-// nearest centre = 1 mod 4.  ok[t - t0] = 0 where a crop leaves the maps (volume zero).
-__global__ void corr_image_kernel(const bf16* __restrict__ FR, const bf16* __restrict__ FD, int Hf, int Wf,
-                                  const double* __restrict__ coords, long long n, long long t0, int nb,
-                                  bf16* __restrict__ C, uint8_t* __restrict__ ok) {
-  const long long total = (long long)nb * 64 * kDisp;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
-    const int d = (int)(i % kDisp);
-    const long long pos = i / kDisp;
-    const int j = (int)(pos % 8), ii = (int)((pos / 8) % 8);
-    const long long b = pos / 64;
-    const long long x = 4 * llround((coords[t0 + b] - 1.0) / 4.0) + 1, y = 4 * llround((coords[n + t0 + b] - 1.0) / 4.0) + 1;
-    const long long rx = (x - 17) / 4, ry = (y - 17) / 4, dx = (x - 33) / 4, dy = (y - 33) / 4;
-    const bool inside = x >= 33 && y >= 33 && rx + 7 < Hf && ry + 7 < Wf && dx + 15 < Hf && dy + 15 < Wf;
-    float v = 0.f;
-    if (inside) {
-      const int di = d / 9 - 4, dj = d % 9 - 4;
-      const bf16* r = FR + ((rx + ii) * Wf + ry + j) * 32;
-      const bf16* q = FD + ((dx + ii + 4 + di) * Wf + dy + j + 4 + dj) * 32;
-      v = dot32(r, q) * (1.f / 32.f);
-    }
-    C[i] = __float2bfloat16_rn(v);
-    if (ii == 0 && j == 0 && d == 0) ok[b] = inside ? 1 : 0;
   }
 }
 
@@ -265,6 +208,200 @@ __global__ void corr_grad_def_kernel(const float* __restrict__ dC, const bf16* _
     }
     dZD[i] = __float2bfloat16_rn(s * (1.f / 32.f));
   }
+}
+
+// conv1 (1 -> 32 channels, 3 x 3, stride 2, pad 1) + bias + ReLU computed directly (9 taps per
+// output, FP32 sums in tap order): one thread per output pixel p = (b, oy, ox) of the input
+// seen through v, 32 BF16 outputs (four 16-byte stores).  Weights W (32 x 16 BF16, 9 used).
+__global__ void conv1_kernel(const bf16* __restrict__ in, View v, ConvI L, long long P, const bf16* __restrict__ W,
+                             const float* __restrict__ bias, bf16* __restrict__ H) {
+  __shared__ float w[32][9], bs[32];
+  for (int i = threadIdx.x; i < 32 * 9; i += blockDim.x) w[i / 9][i % 9] = __bfloat162float(W[(i / 9) * 16 + i % 9]);
+  for (int i = threadIdx.x; i < 32; i += blockDim.x) bs[i] = bias[i];
+  __syncthreads();
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < P; p += (long long)gridDim.x * blockDim.x) {
+    const int ox = (int)(p % L.Wout), oy = (int)((p / L.Wout) % L.Hout);
+    const long long b = p / ((long long)L.Wout * L.Hout);
+    const bf16* base = in + v.off + b * v.sb;
+    float x[9];
+#pragma unroll
+    for (int t = 0; t < 9; ++t) {
+      const int iy = 2 * oy - 1 + t / 3, ix = 2 * ox - 1 + t % 3;
+      x[t] = (iy >= 0 && iy < L.Hin && ix >= 0 && ix < L.Win) ? __bfloat162float(base[iy * v.sy + ix * v.sx]) : 0.f;
+    }
+    uint4* out = reinterpret_cast<uint4*>(H + p * 32);
+#pragma unroll 1
+    for (int g = 0; g < 4; ++g) {
+      __align__(16) bf16 o[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const int c = g * 8 + k;
+        float acc = 0.f;
+#pragma unroll
+        for (int t = 0; t < 9; ++t) acc = fmaf(w[c][t], x[t], acc);
+        o[k] = __float2bfloat16_rn(fmaxf(acc + bs[c], 0.f));
+      }
+      out[g] = *reinterpret_cast<const uint4*>(o);
+    }
+  }
+}
+
+// Where the feature crops of sample t sit: per-window conv2 outputs (coords null; crops at
+// offsets cr / cd of the (B, 10, 10, 32) and (B, 18, 18, 32) maps) or the whole-image maps
+// FR, FD (Hf x Wf x 32) at the positions of subset t0 + t of coords (n x 2).
+struct CorrSrc {
+  const bf16 *R, *D;
+  Crop cr, cd;
+  const double* coords;
+  long long n, t0;
+  int Hf, Wf;
+};
+
+// crop bases and row pitches of sample t; false where a whole-image crop leaves the maps
+__device__ __forceinline__ bool corr_crops(const CorrSrc& s, long long t, const bf16*& r, long long& rrow,
+                                           const bf16*& d, long long& drow) {
+  if (!s.coords) {
+    r = s.R + t * s.cr.sb + s.cr.off;
+    d = s.D + t * s.cd.sb + s.cd.off;
+    rrow = s.cr.row;
+    drow = s.cd.row;
+    return true;
+  }
+  const long long x = 4 * llround((s.coords[s.t0 + t] - 1.0) / 4.0) + 1;
+  const long long y = 4 * llround((s.coords[s.n + s.t0 + t] - 1.0) / 4.0) + 1;
+  const long long rx = (x - 17) / 4, ry = (y - 17) / 4, dx = (x - 33) / 4, dy = (y - 33) / 4;
+  if (x < 33 || y < 33 || rx + 7 >= s.Hf || ry + 7 >= s.Wf || dx + 15 >= s.Hf || dy + 15 >= s.Wf) return false;
+  r = s.R + (rx * s.Wf + ry) * 32;
+  d = s.D + (dx * s.Wf + dy) * 32;
+  rrow = drow = (long long)s.Wf * 32;
+  return true;
+}
+
+// The correlation volume of sample t (blockIdx.x) on the tensor cores and, from it, conv3's
+// im2col rows.  The 8 x 8 reference feature crop (64 rows of 32 BF16 channels) and the
+// 16 x 16 deformed crop (256 rows) are written to shared memory in the 128-byte-swizzled
+// K-major layout (only the first 64 bytes of each 128-byte row, the 32 channels the two
+// K = 16 steps read, are written; A rows 64..127 are not read back); one thread issues two
+// tcgen05.mma (M 128, N 256) into 256 TMEM columns: D[p, q] = fR[p] . fD[q] for every
+// reference / deformed position pair.  Warps 0 and 1 (TMEM lanes 0..63, the reference
+// positions p = 8 ii + j) then read the 12 deformed rows their 32 lanes touch (tcgen05.ld, 16
+// columns each) and keep, for their own row ii, the 9 offsets of each of deformed rows ii ..
+// ii + 8 (columns j .. j + 8, picked by a 3-stage rotation by j): the volume entries / 32,
+// rounded to BF16, each written straight to the (at most 4) places conv3's im2col rows use it,
+// in a shared-memory copy of the sample's 16 rows x 736 columns (zero elsewhere).  All 128
+// threads then copy those rows out with 16-byte stores.  ok[t] = 0 (whole-image crops
+// leaving the maps) gives a zero volume.  The MMA wait is bounded (err bit 2 on time-out,
+// the volume then undefined).
+constexpr int kCorrThreads = 128;
+constexpr int kCorrA = 128 * 128, kCorrB = 256 * 128;  // operand tiles (bytes)
+constexpr int kCorrRows = 16 * 736 * 2;                // conv3's im2col rows of the sample
+constexpr int kCorrSmem = 1024 + kCorrA + kCorrB + kCorrRows;  // + alignment slack
+constexpr long long kCorrWaitCycles = 2000000000LL;
+
+__device__ __forceinline__ void put_chunk(unsigned char* tile, int row, int chunk, uint4 v) {
+  *reinterpret_cast<uint4*>(tile + row * 128 + ((chunk ^ (row & 7)) << 4)) = v;
+}
+
+__global__ void __launch_bounds__(kCorrThreads) corr_im2col_kernel(CorrSrc src, bf16* __restrict__ A3,
+                                                                   uint8_t* __restrict__ ok, int* __restrict__ err) {
+  extern __shared__ unsigned char corr_raw[];
+  __shared__ __align__(8) uint64_t done;
+  __shared__ uint32_t s_tmem;
+  unsigned char* smem =
+      reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(corr_raw) + 1023) & ~uintptr_t(1023));
+  unsigned char* tA = smem;
+  unsigned char* tB = smem + kCorrA;
+  bf16* rows = reinterpret_cast<bf16*>(smem + kCorrA + kCorrB);
+  const long long t = blockIdx.x;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const bf16 *r, *d;
+  long long rrow, drow;
+  const bool inside = corr_crops(src, t, r, rrow, d, drow);
+  if (ok && tid == 0) ok[t] = inside ? 1 : 0;
+  const uint4 zero = make_uint4(0u, 0u, 0u, 0u);
+  // A: reference rows 0..63 (crop row ii = p / 8, column j = p % 8); B: deformed rows
+  // q = 16 dr + dc; 4 chunks of 16 bytes per row, 256 + 1024 chunks: each thread issues its
+  // 10 loads before storing any (their latencies overlapped)
+  {
+    uint4 v[10];
+#pragma unroll
+    for (int i = 0; i < 10; ++i) {
+      const int q = tid + i * kCorrThreads, row = i < 2 ? q / 4 : (q - 256) / 4, ch = q % 4;
+      const bf16* src_row = i < 2 ? r + (row / 8) * rrow + (row % 8) * 32 : d + (row / 16) * drow + (row % 16) * 32;
+      v[i] = inside ? *reinterpret_cast<const uint4*>(src_row + ch * 8) : zero;
+    }
+#pragma unroll
+    for (int i = 0; i < 10; ++i) {
+      const int q = tid + i * kCorrThreads;
+      if (i < 2)
+        put_chunk(tA, q / 4, q % 4, v[i]);
+      else
+        put_chunk(tB, (q - 256) / 4, q % 4, v[i]);
+    }
+  }
+  // the im2col rows start at zero (padding taps and the 7 padding columns)
+  for (int q = tid; q < kCorrRows / 16; q += kCorrThreads) reinterpret_cast<uint4*>(rows)[q] = zero;
+  if (tid == 0) {
+    mbar_init(&done, 1);
+    fence_barrier_init();
+  }
+  if (warp == 0) tmem_alloc(&s_tmem, 256);
+  fence_proxy_async_shared();  // the generic-proxy tile writes, visible to the tensor cores
+  tcgen05_before_sync();
+  __syncthreads();
+  tcgen05_after_sync();
+  const uint32_t tmem = s_tmem;
+  if (tid == 0) {
+    constexpr uint32_t idesc = bf16_idesc(128, 256);
+    const uint32_t a = smem_u32(tA), b = smem_u32(tB);
+    umma_bf16(tmem, sw128_desc(a), sw128_desc(b), idesc, false);
+    umma_bf16(tmem, sw128_desc(a + 32), sw128_desc(b + 32), idesc, true);
+    umma_commit(&done);
+  }
+  __syncwarp();
+  const bool ready = mbar_wait(&done, 0, kCorrWaitCycles);
+  if (!ready && lane == 0) atomicOr(err, 4);
+  tcgen05_after_sync();
+  if (warp < 2) {
+    const int p = warp * 32 + lane, ii = p / 8, j = p % 8, ii0 = warp * 4;
+    // the im2col places of volume position (ii, j): output (oy, ox) with 2 oy - 1 + ky = ii and
+    // 2 ox - 1 + kx = j, tap (ky, kx); at most 2 per axis
+    int base[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int oy = ((ii + 1) >> 1) - (k >> 1), ox = ((j + 1) >> 1) - (k & 1);
+      const int ky = ii + 1 - 2 * oy, kx = j + 1 - 2 * ox;
+      base[k] = (oy >= 0 && oy < 4 && ox >= 0 && ox < 4 && ky >= 0 && ky <= 2 && kx >= 0 && kx <= 2)
+                    ? (oy * 4 + ox) * 736 + (ky * 3 + kx) * kDisp
+                    : -1;
+    }
+#pragma unroll 1
+    for (int rr = 0; rr < 12; ++rr) {
+      float v[16];
+      tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)((ii0 + rr) * 16), v);
+      const int di = ii0 + rr - ii;  // deformed row ii0 + rr = ii + di
+      if (di < 0 || di > 8) continue;
+      // rotate left by j (bits 4, 2, 1) so that v[0..8] = columns j .. j + 8
+#pragma unroll
+      for (int k = 0; k < 12; ++k) v[k] = (j & 4) ? v[k + 4] : v[k];
+#pragma unroll
+      for (int k = 0; k < 10; ++k) v[k] = (j & 2) ? v[k + 2] : v[k];
+#pragma unroll
+      for (int k = 0; k < 9; ++k) v[k] = (j & 1) ? v[k + 1] : v[k];
+#pragma unroll
+      for (int b = 0; b < 9; ++b) {
+        const bf16 x = __float2bfloat16_rn(inside ? v[b] * (1.f / 32.f) : 0.f);
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+          if (base[k] >= 0) rows[base[k] + di * 9 + b] = x;
+      }
+    }
+  }
+  tcgen05_before_sync();
+  __syncthreads();
+  if (warp == 0) tmem_free(tmem, 256);
+  uint4* outA = reinterpret_cast<uint4*>(A3 + t * 16 * 736);
+  for (int q = tid; q < kCorrRows / 16; q += kCorrThreads) outA[q] = reinterpret_cast<const uint4*>(rows)[q];
 }
 
 // out[c, r] = in[r, c] (BF16, 32 x 32 tiles through shared memory)
@@ -425,17 +562,17 @@ struct ProposalNet {
   int step_count = 0;
   // activations and their gradients (max_batch): per convolution its im2col rows A and their
   // transpose At, output H (NHWC) and output gradient dZ with its transpose dZt; the
-  // correlation volume Cv; FC1's input transposed (Ht5), output H6 (Ht6) and output gradient
-  // dZ6 (dZt6); the output gradient dY (dYt)
+  // FC1's input transposed (Ht5), output H6 (Ht6) and output gradient dZ6 (dZt6); the output
+  // gradient dY (dYt).  conv3's im2col rows A[kConv3] come straight from the correlation.
   bf16 *A[kNumConv] = {}, *At[kNumConv] = {}, *H[kNumConv] = {}, *dZ[kNumConv] = {}, *dZt[kNumConv] = {};
-  bf16 *Cv = nullptr, *Ht5 = nullptr, *H6 = nullptr, *Ht6 = nullptr, *dZ6 = nullptr, *dZt6 = nullptr;
+  bf16 *Ht5 = nullptr, *H6 = nullptr, *Ht6 = nullptr, *dZ6 = nullptr, *dZt6 = nullptr;
   bf16 *dY = nullptr, *dYt = nullptr;
   float *dAf = nullptr, *dHf = nullptr, *Y = nullptr, *loss = nullptr;
   uint8_t* ok = nullptr;  // per predicted subset: its feature crops lie inside the maps
   // whole-image features for prediction (sized for the last frame size): the BF16 image,
-  // conv1's im2col rows and output, conv2's im2col rows, the reference and deformed maps
+  // conv1's output, conv2's im2col rows, the reference and deformed maps
   int fM = 0, fN = 0;
-  bf16 *imgb = nullptr, *A1i = nullptr, *H1i = nullptr, *A2i = nullptr, *FR = nullptr, *FD = nullptr;
+  bf16 *imgb = nullptr, *H1i = nullptr, *A2i = nullptr, *FR = nullptr, *FD = nullptr;
   int* errflag = nullptr;
 };
 
@@ -499,19 +636,29 @@ int wsplit(long long M, long long N, long long K) {
   return (int)(s < 1 ? 1 : s);
 }
 
-// im2col of convolution i's input (at `in` seen through v) and its GEMM with bias + ReLU
-int conv_forward(ProposalNet* net, int i, int batch, const bf16* in, View v) {
+// im2col rows of convolution i's input (at `in` seen through v) into net->A[i]
+void im2col(ProposalNet* net, int i, int batch, const bf16* in, View v) {
   const ConvI& L = kConv[i];
   const long long P = P_of(i, batch);
   im2col_kernel<<<blocks_for(P * (L.Kp / 8)), 256, 0, net->stream>>>(in, v, net->A[i], P, L);
   ++net->launches;
+}
+
+// im2col of convolution i's input and its GEMM with bias + ReLU
+int conv_forward(ProposalNet* net, int i, int batch, const bf16* in, View v) {
+  const ConvI& L = kConv[i];
+  const long long P = P_of(i, batch);
+  im2col(net, i, batch, in, v);
   return gemm(net, net->A[i], L.Kp, net->wb + kL.w[L.layer], L.Kp, P, L.Cout, L.Kp, kEpiBiasReluBf16, nullptr,
               net->H[i], net->w + kL.b[L.layer], L.Cout, 1);
 }
 
-// the layers after the correlation volume net->Cv: conv3, conv4, FC1, FC2 (into net->Y)
+// the layers after the correlation: conv3 (its im2col rows A[kConv3] written by the
+// correlation kernel), conv4, FC1, FC2 (into net->Y)
 int head(ProposalNet* net, int batch) {
-  int rc = conv_forward(net, kConv3, batch, net->Cv, nhwc(8, 8, kDisp));
+  const ConvI& L3 = kConv[kConv3];
+  int rc = gemm(net, net->A[kConv3], L3.Kp, net->wb + kL.w[L3.layer], L3.Kp, P_of(kConv3, batch), L3.Cout, L3.Kp,
+                kEpiBiasReluBf16, nullptr, net->H[kConv3], net->w + kL.b[L3.layer], L3.Cout, 1);
   if (!rc) rc = conv_forward(net, kConv4, batch, net->H[kConv3], nhwc(4, 4, 64));
   if (!rc)
     rc = gemm(net, net->H[kConv4], kFcIn, net->wb + kL.w[4], kFcIn, batch, kFcHid, kFcIn, kEpiBiasReluBf16, nullptr,
@@ -525,16 +672,27 @@ int head(ProposalNet* net, int batch) {
 constexpr Crop kCropR{10 * 10 * 32, (10 + 1) * 32, 10 * 32};
 constexpr Crop kCropD{18 * 18 * 32, (18 + 1) * 32, 18 * 32};
 
-int forward(ProposalNet* net, int batch, const bf16* X) {
-  int rc = conv_forward(net, kConvR1, batch, X, kViewRef);
-  if (!rc) rc = conv_forward(net, kConvD1, batch, X, kViewDef);
-  if (!rc) rc = conv_forward(net, kConvR2, batch, net->H[kConvR1], nhwc(20, 20, 32));
-  if (!rc) rc = conv_forward(net, kConvD2, batch, net->H[kConvD1], nhwc(36, 36, 32));
-  if (rc) return rc;
-  const long long nc = (long long)batch * 64 * kDisp;
-  corr_kernel<<<blocks_for(nc), 256, 0, net->stream>>>(net->H[kConvR2], kCropR, net->H[kConvD2], kCropD, net->Cv, nc);
+void conv1(ProposalNet* net, const bf16* in, View v, const ConvI& L, long long P, bf16* H) {
+  conv1_kernel<<<blocks_for(P), 256, 0, net->stream>>>(in, v, L, P, net->wb + kL.w[0], net->w + kL.b[0], H);
   ++net->launches;
-  return head(net, batch);
+}
+
+int corr_im2col(ProposalNet* net, const CorrSrc& src, int nb) {
+  cudaFuncSetAttribute(corr_im2col_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kCorrSmem);
+  corr_im2col_kernel<<<(unsigned)nb, kCorrThreads, kCorrSmem, net->stream>>>(src, net->A[kConv3],
+                                                                             src.coords ? net->ok : nullptr,
+                                                                             net->errflag);
+  ++net->launches;
+  return ALDIC_OK;
+}
+
+int forward(ProposalNet* net, int batch, const bf16* X) {
+  conv1(net, X, kViewRef, kConv[kConvR1], P_of(kConvR1, batch), net->H[kConvR1]);
+  conv1(net, X, kViewDef, kConv[kConvD1], P_of(kConvD1, batch), net->H[kConvD1]);
+  int rc = conv_forward(net, kConvR2, batch, net->H[kConvR1], nhwc(20, 20, 32));
+  if (!rc) rc = conv_forward(net, kConvD2, batch, net->H[kConvD1], nhwc(36, 36, 32));
+  if (!rc) rc = corr_im2col(net, CorrSrc{net->H[kConvR2], net->H[kConvD2], kCropR, kCropD, nullptr, 0, 0, 0, 0}, batch);
+  return rc ? rc : head(net, batch);
 }
 
 // weight and bias gradients of convolution i from its output gradient dZ[i] (added to net->g)
@@ -571,7 +729,7 @@ void relu_grad(ProposalNet* net, const bf16* H, bf16* dZ, long long n) {
 }
 
 // gradients of the mean squared error into net->g (zeroed here)
-int backward(ProposalNet* net, int batch, const float* T) {
+int backward(ProposalNet* net, int batch, const bf16* X, const float* T) {
   cudaStream_t st = net->stream;
   const long long B = batch;
   NK(cudaMemsetAsync(net->g, 0, sizeof(float) * kL.n, st));
@@ -616,9 +774,11 @@ int backward(ProposalNet* net, int batch, const float* T) {
   // conv2 and conv1 on the reference subset, then on the deformed window (shared weights)
   if ((rc = conv_wgrad(net, kConvR2, batch)) || (rc = conv_dgrad(net, kConvR2, batch))) return rc;
   relu_grad(net, net->H[kConvR1], net->dZ[kConvR1], B * 400 * 32);
+  im2col(net, kConvR1, batch, X, kViewRef);  // conv1 ran directly: its im2col rows for dW
   if ((rc = conv_wgrad(net, kConvR1, batch))) return rc;
   if ((rc = conv_wgrad(net, kConvD2, batch)) || (rc = conv_dgrad(net, kConvD2, batch))) return rc;
   relu_grad(net, net->H[kConvD1], net->dZ[kConvD1], B * 1296 * 32);
+  im2col(net, kConvD1, batch, X, kViewDef);
   return conv_wgrad(net, kConvD1, batch);
 }
 
@@ -682,7 +842,6 @@ int aldic_net_create(aldic_net** out, int device, int max_batch) {
     if (e == cudaSuccess) e = cudaMalloc(&net->dZ[i], P * L.Cout * 2);
     if (e == cudaSuccess) e = cudaMalloc(&net->dZt[i], P * L.Cout * 2);
   }
-  if (e == cudaSuccess) e = cudaMalloc(&net->Cv, B * 64 * kDisp * 2);
   if (e == cudaSuccess) e = cudaMalloc(&net->Ht5, B * kFcIn * 2);
   if (e == cudaSuccess) e = cudaMalloc(&net->H6, B * kFcHid * 2);
   if (e == cudaSuccess) e = cudaMalloc(&net->Ht6, B * kFcHid * 2);
@@ -710,9 +869,9 @@ void aldic_net_destroy(aldic_net* net) {
   if (!net) return;
   cudaSetDevice(net->device);
   if (net->stream) cudaStreamSynchronize(net->stream);
-  void* bufs[] = {net->w,  net->g,   net->m,   net->v,   net->wb,  net->Cv,   net->Ht5, net->H6,     net->Ht6,
+  void* bufs[] = {net->w,  net->g,   net->m,   net->v,   net->wb,  net->Ht5, net->H6,     net->Ht6,
                   net->dZ6, net->dZt6, net->dY, net->dYt, net->Y, net->dAf, net->dHf, net->loss, net->ok,  net->errflag,
-                  net->imgb, net->A1i, net->H1i, net->A2i, net->FR, net->FD};
+                  net->imgb, net->H1i, net->A2i, net->FR, net->FD};
   for (void* p : bufs)
     if (p) cudaFree(p);
   for (int l = 0; l < 6; ++l)
@@ -771,7 +930,7 @@ int aldic_net_gradients(aldic_net* net, int batch, const void* x, const float* t
   if (!net || !x || !t || batch < 8 || batch % 8 != 0 || batch > net->max_batch) return ALDIC_ERR_ARG;
   NK(cudaSetDevice(net->device));
   int rc = forward(net, batch, reinterpret_cast<const bf16*>(x));
-  if (!rc) rc = backward(net, batch, t);
+  if (!rc) rc = backward(net, batch, reinterpret_cast<const bf16*>(x), t);
   if (rc) return rc;
   if (grads) NK(cudaMemcpyAsync(grads, net->g, sizeof(float) * kL.n, cudaMemcpyDefault, net->stream));
   if (loss) NK(cudaMemcpyAsync(loss, net->loss, sizeof(float), cudaMemcpyDefault, net->stream));
@@ -783,7 +942,7 @@ int aldic_net_train_step(aldic_net* net, int batch, const void* x, const float* 
   if (!net || !x || !t || batch < 8 || batch % 8 != 0 || batch > net->max_batch || !(lr > 0)) return ALDIC_ERR_ARG;
   NK(cudaSetDevice(net->device));
   int rc = forward(net, batch, reinterpret_cast<const bf16*>(x));
-  if (!rc) rc = backward(net, batch, t);
+  if (!rc) rc = backward(net, batch, reinterpret_cast<const bf16*>(x), t);
   if (rc) return rc;
   net->step_count += 1;
   const float b1 = 0.9f, b2 = 0.999f;
@@ -841,14 +1000,13 @@ int image_features(ProposalNet* net, const FrameDev& fr) {
   const long long P1 = (long long)M1 * N1, P2 = (long long)M2 * N2;
   if (net->fM != M || net->fN != N) {
     NK(cudaStreamSynchronize(net->stream));
-    bf16** bufs[] = {&net->imgb, &net->A1i, &net->H1i, &net->A2i, &net->FR, &net->FD};
+    bf16** bufs[] = {&net->imgb, &net->H1i, &net->A2i, &net->FR, &net->FD};
     for (bf16** b : bufs) {
       if (*b) NK(cudaFree(*b));
       *b = nullptr;
     }
     net->fM = net->fN = 0;
     NK(cudaMalloc(&net->imgb, (size_t)M * N * 2));
-    NK(cudaMalloc(&net->A1i, (size_t)P1 * 16 * 2));
     NK(cudaMalloc(&net->H1i, (size_t)P1 * 32 * 2));
     NK(cudaMalloc(&net->A2i, (size_t)P2 * 288 * 2));
     NK(cudaMalloc(&net->FR, (size_t)P2 * 32 * 2));
@@ -860,15 +1018,12 @@ int image_features(ProposalNet* net, const FrameDev& fr) {
   for (int side = 0; side < 2; ++side) {
     const dim3 tg((unsigned)((M + 31) / 32), (unsigned)((N + 31) / 32));
     image_bf16_kernel<<<tg, dim3(32, 8), 0, net->stream>>>(side ? fr.def : fr.ref, M, N, net->imgb);
-    im2col_kernel<<<blocks_for(P1 * 2), 256, 0, net->stream>>>(net->imgb, View{0, 0, N, 1}, net->A1i, P1, c1);
-    net->launches += 2;
-    int rc = gemm(net, net->A1i, 16, net->wb + kL.w[0], 16, P1, 32, 16, kEpiBiasReluBf16, nullptr, net->H1i,
-                  net->w + kL.b[0], 32, 1);
-    if (rc) return rc;
+    ++net->launches;
+    conv1(net, net->imgb, View{0, 0, N, 1}, c1, P1, net->H1i);
     im2col_kernel<<<blocks_for(P2 * 36), 256, 0, net->stream>>>(net->H1i, nhwc(M1, N1, 32), net->A2i, P2, c2);
     ++net->launches;
-    rc = gemm(net, net->A2i, 288, net->wb + kL.w[1], 288, P2, 32, 288, kEpiBiasReluBf16, nullptr,
-              side ? net->FD : net->FR, net->w + kL.b[1], 32, 1);
+    const int rc = gemm(net, net->A2i, 288, net->wb + kL.w[1], 288, P2, 32, 288, kEpiBiasReluBf16, nullptr,
+                        side ? net->FD : net->FR, net->w + kL.b[1], 32, 1);
     if (rc) return rc;
   }
   return ALDIC_OK;
@@ -887,11 +1042,9 @@ int net_predict(aldic_net* net, const FrameDev& fr, const double* coords_dev, lo
   for (long long s = 0; s < n; s += B) {
     const int nb = (int)std::min<long long>(B, n - s);
     const int bpad = (nb + 7) / 8 * 8;
-    corr_image_kernel<<<blocks_for((long long)nb * 64 * kDisp), 256, 0, net->stream>>>(
-        net->FR, net->FD, Hf, Wf, coords_dev, n, s, nb, net->Cv, net->ok);
-    ++net->launches;
+    corr_im2col(net, CorrSrc{net->FR, net->FD, Crop{}, Crop{}, coords_dev, n, s, Hf, Wf}, nb);
     if (bpad > nb)
-      NK(cudaMemsetAsync(net->Cv + (size_t)nb * 64 * kDisp, 0, (size_t)(bpad - nb) * 64 * kDisp * 2, net->stream));
+      NK(cudaMemsetAsync(net->A[kConv3] + (size_t)nb * 16 * 736, 0, (size_t)(bpad - nb) * 16 * 736 * 2, net->stream));
     rc = head(net, bpad);
     if (rc) return rc;
     unscale_kernel<<<blocks_for(nb), 256, 0, net->stream>>>(net->Y, nb, U0 + 2 * s, F0 + 4 * s, coords_dev + s, n,

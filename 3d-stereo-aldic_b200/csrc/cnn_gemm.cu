@@ -9,7 +9,8 @@
 //     instructions (M 128, N BN, K 16 each) into an FP32 accumulator of BN TMEM columns;
 //     tcgen05.commit on a per-stage mbarrier frees a stage for the next load;
 //   * the 4 warps then read their 32 accumulator rows back (tcgen05.ld 32x32b) and apply the
-//     epilogue: store (+ bias), atomic add (split-K), or bias + ReLU to BF16.
+//     epilogue: store (+ bias), atomic add (split-K), or bias + ReLU to BF16 (16-byte vector
+//     stores for whole 16-column runs at 16-byte aligned addresses).
 // Every wait is bounded; a time-out sets *err, stops issuing, drains and frees TMEM.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -122,6 +123,37 @@ __global__ void __launch_bounds__(128, 1)
     for (int c = 0; c < BN; c += 16) {
       float v[16];
       tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, v);
+      const int col0 = n0 + c;
+      if (row < M && col0 + 16 <= N && epi.mode != kEpiAtomic) {  // 16 whole columns: vector stores
+        const size_t o = (size_t)row * epi.ldc + col0;
+        if (epi.mode == kEpiBiasReluBf16 && ((reinterpret_cast<uintptr_t>(epi.c16 + o) & 15) == 0)) {
+          __align__(16) __nv_bfloat16 h[16];
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            const float x = v[j] + (epi.bias ? epi.bias[col0 + j] : 0.f);
+            h[j] = __float2bfloat16_rn(x > 0.f ? x : 0.f);
+          }
+          uint4* dst = reinterpret_cast<uint4*>(epi.c16 + o);
+          dst[0] = reinterpret_cast<const uint4*>(h)[0];
+          dst[1] = reinterpret_cast<const uint4*>(h)[1];
+          continue;
+        }
+        if (epi.mode == kEpiStore && ((reinterpret_cast<uintptr_t>(epi.c32 + o) & 15) == 0)) {
+          float4* dst = reinterpret_cast<float4*>(epi.c32 + o);
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            float4 q = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+            if (epi.bias) {
+              q.x += epi.bias[col0 + 4 * j];
+              q.y += epi.bias[col0 + 4 * j + 1];
+              q.z += epi.bias[col0 + 4 * j + 2];
+              q.w += epi.bias[col0 + 4 * j + 3];
+            }
+            dst[j] = q;
+          }
+          continue;
+        }
+      }
       if (row < M) {
 #pragma unroll
         for (int j = 0; j < 16; ++j) {

@@ -3,21 +3,29 @@
 
 Metric: converged IC-GN subsets per second at <= 0.01 px from the FP64 oracle.
 
-Workload (default ``stereo2048``): the calibrated stereo pair + temporal match +
-triangulation case -- two synthetic pinhole cameras (f = 4000 px, principal point at the
-image centre, 300 mm baseline, optical axes aimed at a speckled plane 1 m away),
-2048 x 2048 uint16 frames 0 and 1 (plane moved by (0.1, -0.05, 0.3) mm and a 1e-3 rad
-rotation), subset 41 (winsize 40), step 10 (~40k subsets per camera).  One step is one
-pass of the hot path over the frame set:
-  prep (normalise 4 frames, gradients) -> stereo L0->R0 integer search (search 70) +
-  IC-GN (tol 1e-3) -> temporal L0->L1 and R0->R1 integer search (search 10) + IC-GN
-  (tol 1e-2) -> FP64 triangulation of frames 0 and 1.
+Workload (default ``learned2048``): the learned initial guess against the FFT integer search
+on held-out 2048 x 2048 uint8 speckle frames (Gaussian speckles, a smooth random displacement
+field with |u|, |v| <= 12 px and gradients <= 0.05, N(0, 2) noise), subset 33 (winsize 32),
+step 16 (15 129 subsets per frame), tolerance 1e-3.  One step is one frame pair through one
+path: load + normalise + gradients, then
+  learned: network prediction -> IC-GN from [F0 U0] -> ZNCC check -> integer search (radius
+           16) + IC-GN from [0 U0] on the subsets that failed (the fallback);
+  fft:     whole-field integer search (radius 16) -> outlier removal -> Init -> IC-GN.
+``value`` is the learned path, ``fft_init`` the FFT path on the same frames.
+
+``stereo2048``: the calibrated stereo pair + temporal match + triangulation case -- two
+synthetic pinhole cameras (f = 4000 px, principal point at the image centre, 300 mm baseline,
+optical axes aimed at a speckled plane 1 m away), 2048 x 2048 uint16 frames 0 and 1 (plane
+moved by (0.1, -0.05, 0.3) mm and a 1e-3 rad rotation), subset 41 (winsize 40), step 10 (~40k
+subsets per camera); one step: prep (normalise 4 frames, gradients) -> stereo L0->R0 integer
+search (search 70) + IC-GN (tol 1e-3) -> temporal L0->L1 and R0->R1 integer search (search 10)
++ IC-GN (tol 1e-2) -> FP64 triangulation of frames 0 and 1.
 ``temporal512`` is the single-camera 512 x 512 uint8 affine case (900 subsets).
 
 A subset counts when the device flags it converged and its u, v are within 0.01 px of
 the FP64 oracle run from the same initial guess on the same frames.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload W]
 """
 import argparse
 import json
@@ -46,6 +54,8 @@ UNIT = "subsets/s"
 # workload description
 # ----------------------------------------------------------------------------------
 def workload_params(name):
+    if name == "learned2048":  # learned vs FFT initial guess, held-out 2048 x 2048 smooth-field frames
+        return dict(size=2048, w=32, step=16, search=16, tol=1e-3, roi=20, umax=12.0, gmax=0.05, frames=8)
     if name == "quadtree2048":
         return dict(size=2048, w=32, step=16, s_temp=10, tol_temp=1e-3, mu=1e-3, admm=2, min_elem=4)
     if name == "stereo2048":
@@ -519,15 +529,428 @@ def run_reference(args, P):
 
 
 # ----------------------------------------------------------------------------------
+# learned vs FFT initial guess (learned2048)
+# ----------------------------------------------------------------------------------
+LEARNED_METRIC = "converged IC-GN subsets/s at <=0.01 px vs FP64 oracle; learned vs FFT init, 1 B200"
+
+
+class LearnedBench:
+    """The two initial-guess paths on one device, each a pass over one frame pair (uint8
+    2048 x 2048, resident): load + normalise + gradients, then
+      learned: network prediction -> IC-GN from [F0 U0] -> ZNCC check -> integer search + IC-GN
+               on the failed subsets (the fallback);
+      fft:     whole-field integer search -> outlier removal -> Init (inpaint) -> IC-GN from
+               [0 U0] (LocalICGN's reference path).
+    Both on the same integer-search grid (ROI [roi+1, size-roi], winsize w, step), all work on
+    one stream."""
+
+    def __init__(self, A, torch, P, device):
+        from aldic_b200 import learned as L
+        from aldic_b200 import train_net
+
+        self.A, self.T, self.P = A, torch, P
+        M = N = P["size"]
+        self.M, self.N = M, N
+        self.gx, self.gy = [P["roi"] + 1, M - P["roi"]], [P["roi"] + 1, N - P["roi"]]
+        di = device.index or 0
+        self.net = L.ProposalNet(di, max_batch=16384)
+        self.net.set_params(np.load(train_net.DEFAULT_WEIGHTS))
+        self.ctx = A.Context(di)
+        self.ctx.set_option(A.OPT_AUTOTUNE, 1)
+        self.li = L.LearnedInit(self.net, self.ctx, P["search"], self.gx, self.gy, P["w"], P["step"], P["tol"])
+        self.stream = self.li.stream
+        self.n, self.nx, self.ny = self.li.n, self.li.nx, self.li.ny
+        f64 = dict(dtype=torch.float64, device=device)
+        g, n = self.nx * self.ny, self.n
+        self.fb = {k: torch.empty(g, **f64) for k in ("x", "y", "u", "v", "phi")}
+        self.fb.update({"U0": torch.empty(2 * n, **f64), "U": torch.empty(2 * n, **f64),
+                        "F": torch.empty(4 * n, **f64), "conv": torch.empty(n, dtype=torch.int32, device=device)})
+        self.fft_icgn_events = None
+
+    def load(self, ref, deff):
+        c = self.ctx
+        c.load_image_raw(0, ref, self.gx, self.gy, want_stats=False, shape=(self.M, self.N))
+        c.load_image_raw(1, deff, self.gx, self.gy, want_stats=False, shape=(self.M, self.N))
+        c.compute_gradients()
+
+    def learned(self, ref, deff):
+        with self.T.cuda.stream(self.stream):
+            self.load(ref, deff)
+        return self.li.run()
+
+    def fft(self, ref, deff):
+        P, c, b = self.P, self.ctx, self.fb
+        with self.T.cuda.stream(self.stream):
+            self.load(ref, deff)
+            c.integer_search([P["search"]] * 2, self.gx, self.gy, P["w"], P["step"], out=b)
+            u, v = b["u"].view(self.nx, self.ny), b["v"].view(self.nx, self.ny)
+            c.remove_outliers(u, v, 100.0)
+            c.init_u0(u, v, out=b["U0"])
+            self.li._timed(self.fft_icgn_events, lambda: c.local_icgn(
+                self.A.QUADTREE, self.li.coords, b["U0"], P["w"], P["tol"], want_H=False, want_mark=False, out=b))
+
+    def snapshot(self, which):
+        """Host copies of the last pass's results (waits for the stream)."""
+        self.stream.synchronize()
+        b = self.li.buf if which == "learned" else self.fb
+        keys = ("U0", "F0", "U", "F", "conv", "fallback") if which == "learned" else ("U0", "U", "F", "conv")
+        return {k: b[k].cpu().numpy() for k in keys}
+
+    def launches(self):
+        return self.ctx.launches + self.net.launches
+
+    def close(self):
+        self.net.close()
+        self.ctx.close()
+
+
+def learned_frames(P, seeds, device):
+    from aldic_b200 import synth_gpu
+
+    return [synth_gpu.field_pair(s, P["size"], P["size"], umax=P["umax"], gmax=P["gmax"], device=device)
+            for s in seeds]
+
+
+def learned_verify(bench, pair, res_l, res_f, nthreads):
+    """Both paths' results on one frame against the FP64 oracle run from the same initial
+    guesses (the learned path's [F0 U0], the search's fallback guesses included; the FFT
+    path's [0 U0]) on the same normalised frames."""
+    import oracle as O
+
+    M, N = bench.M, bench.N
+    P = bench.P
+    ref = pair.ref.cpu().numpy().reshape((M, N), order="F").astype(np.float64)
+    deff = pair.deff.cpu().numpy().reshape((M, N), order="F").astype(np.float64)
+    f, _ = O.normalize(ref, bench.gx, bench.gy)
+    g, _ = O.normalize(deff, bench.gx, bench.gy)
+    gx, gy = O.gradient(f)
+    frame = O.Frame(f, g, None, gx, gy)
+    crd = bench.li.coords.cpu().numpy().T.copy()
+    out = {}
+    for name, r in (("learned", res_l), ("fft", res_f)):
+        F0 = r["F0"] if name == "learned" else None
+        t0 = time.perf_counter()
+        o = O.local_icgn(frame, crd, r["U0"], P["w"], P["tol"], variant=1, nthreads=nthreads, F0=F0)
+        t_o = time.perf_counter() - t0
+        fg = (r["conv"] > 0) & (r["conv"] < 100)
+        fo = (o["conv"] > 0) & (o["conv"] < 100)
+        d = np.abs(r["U"] - o["U"]).reshape(-1, 2)
+        dF = np.abs(r["F"] - o["F"]).reshape(-1, 4)
+        ok = fg & fo & np.all(d <= 0.01, axis=1)
+        both = fg & fo
+        out[name] = {"n": int(fg.size), "converged_gpu": int(fg.sum()), "converged_oracle": int(fo.sum()),
+                     "counted": int(ok.sum()), "flag_match": float(np.mean(fg == fo)),
+                     "iterations_match": float(np.mean(r["conv"] == o["conv"])),
+                     "mean_iterations": float(r["conv"][fg].mean()) if fg.any() else None,
+                     "uv_max_err": float(d[both].max()) if both.any() else None,
+                     "F_max_err": float(dF[both].max()) if both.any() else None, "oracle_s": t_o}
+    # the network's guesses against the converged solutions (non-fallback subsets)
+    keep = ~res_l["fallback"] & (res_l["conv"] > 0) & (res_l["conv"] < 100)
+    du = np.hypot(*(res_l["U0"] - res_l["U"]).reshape(-1, 2)[keep].T)
+    dF0 = np.abs(res_l["F0"] - res_l["F"]).reshape(-1, 4)[keep]
+    okf = (res_f["conv"] > 0) & (res_f["conv"] < 100)
+    dus = np.hypot(*(res_f["U0"] - res_f["U"]).reshape(-1, 2)[okf].T)
+    both = keep & okf
+    out["guess"] = {"net_u_err_px_p50": float(np.median(du)), "net_u_err_px_p99": float(np.percentile(du, 99)),
+                    "net_F_err_p50": float(np.median(dF0)),
+                    "zero_F_err_p50": float(np.median(np.abs(res_l["F"].reshape(-1, 4)[keep]))),
+                    "search_u_err_px_p50": float(np.median(dus)),
+                    "learned_vs_fft_uv_max": float(np.abs(res_l["U"] - res_f["U"]).reshape(-1, 2)[both].max())
+                    if both.any() else None,
+                    "fallback": int(res_l["fallback"].sum())}
+    return out
+
+
+def net_flops(M, N, n):
+    """Algorithmic FLOPs of one prediction: conv1 (9 taps x 32) and conv2 (288 x 32) over the
+    two whole images' output pixels, then per subset the 64 x 81 correlation entries (32
+    channels), conv3 (16 x 64 x 729), conv4 (16 x 64 x 576), FC1 (1024 x 128), FC2 (128 x 6);
+    2 per multiply-add."""
+    M1, N1 = (M + 1) // 2, (N + 1) // 2
+    M2, N2 = (M1 + 1) // 2, (N1 + 1) // 2
+    per_image = M1 * N1 * 32 * 9 + M2 * N2 * 32 * 288
+    per_subset = 64 * 81 * 32 + 16 * 64 * 729 + 16 * 64 * 576 + 1024 * 128 + 128 * 6
+    return 2.0 * (2 * per_image + n * per_subset)
+
+
+def learned_cpu_sample(P, pair, gx, gy, per, nthreads, seed=0):
+    """The FP64 CPU restatement of the reference's path on this workload (integer search +
+    IC-GN from [0 U0], LocalICGN), timed on `per` grid subsets of one frame, the frame's
+    normalisation and gradients scaled to the sample."""
+    import oracle as O
+
+    M = N = P["size"]
+    w, st, s = P["w"], P["step"], P["search"]
+    ref = pair.ref.cpu().numpy().reshape((M, N), order="F").astype(np.float64)
+    deff = pair.deff.cpu().numpy().reshape((M, N), order="F").astype(np.float64)
+    t0 = time.perf_counter()
+    f, _ = O.normalize(ref, gx, gy)
+    g, _ = O.normalize(deff, gx, gy)
+    dfx, dfy = O.gradient(f)
+    t_prep = time.perf_counter() - t0
+    nx, ny = O.search_grid(gx, gy, w, st)
+    rng = np.random.default_rng(seed)
+    pick = rng.choice(nx * ny, size=min(per, nx * ny), replace=False)
+    ii = gx[0] + (pick % nx) * st
+    jj = gy[0] + (pick // nx) * st
+    t1 = time.perf_counter()
+    sub = O.search_list(f, g, [s, s], gx[1], gy[1], ii, jj, w, nthreads=nthreads)
+    U0 = np.nan_to_num(sub[:, :2]).ravel()
+    crd = np.stack([ii + w / 2.0, jj + w / 2.0], 1).astype(np.float64)
+    r = O.local_icgn(O.Frame(f, g, None, dfx, dfy), crd, U0, w, P["tol"], variant=1, nthreads=nthreads)
+    t = time.perf_counter() - t1 + t_prep * pick.size / (nx * ny)
+    conv = int(np.sum((r["conv"] > 0) & (r["conv"] < 100)))
+    return conv / t, t, int(pick.size), conv
+
+
+def run_learned(args, P):
+    import torch
+
+    import aldic_b200 as A
+    from aldic_b200 import train_net
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    dev = torch.device(f"cuda:{local_rank}")
+    torch.cuda.set_device(dev)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    # weak scaling: every rank its own held-out frames, no data-path collective
+    F = P["frames"]
+    base = 50000 + 1000 * (args.seed + rank)
+    pairs = learned_frames(P, [base + k for k in range(F)], dev)
+    warm = learned_frames(P, [base + 900 + k for k in range(max(args.warmup, 3))], dev)
+    bench = LearnedBench(A, torch, P, dev)
+    st = bench.stream
+    for p in warm:  # warm-up: the autotuner's first calls, page-in
+        bench.fft(p.ref, p.deff)
+        bench.learned(p.ref, p.deff)
+    torch.cuda.synchronize(dev)
+    if dist:
+        dist.barrier()
+
+    def timed(fn, icgn_list):
+        clocks = ClockSampler(local_rank)
+        l0 = bench.launches()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(dev)
+        ev0.record(st)
+        extra = [fn(pairs[k % F].ref, pairs[k % F].deff) for k in range(args.steps)]
+        ev1.record(st)
+        torch.cuda.synchronize(dev)
+        return ev0.elapsed_time(ev1), clocks.stop(), bench.launches() - l0, extra
+
+    bench.li.predict_events, bench.li.icgn_events = [], []
+    ms_l, clk_l, launches_l, fallbacks = timed(bench.learned, None)
+    pred_ev, icgn_ev = bench.li.predict_events, bench.li.icgn_events
+    bench.li.predict_events = bench.li.icgn_events = None
+    if dist:
+        dist.barrier()
+    bench.fft_icgn_events = []
+    ms_f, clk_f, launches_f, _ = timed(bench.fft, None)
+    fft_icgn_ev, bench.fft_icgn_events = bench.fft_icgn_events, None
+    predict_ms = float(np.mean([a.elapsed_time(b) for a, b in pred_ev]))
+    icgn_ms = float(np.mean([a.elapsed_time(b) for a, b in icgn_ev]))
+    fft_icgn_ms = float(np.mean([a.elapsed_time(b) for a, b in fft_icgn_ev]))
+
+    # per frame: both paths' results (deterministic: the timed passes produced the same) and
+    # their verification against the FP64 oracle
+    import oracle as O
+
+    O.build()
+    nthr = host_threads()
+    counted_l, counted_f, ver, conv_frames = [], [], [], []
+    for k, p in enumerate(pairs[:min(F, args.steps)]):
+        bench.learned(p.ref, p.deff)
+        rl = bench.snapshot("learned")
+        conv_frames.append(rl["conv"])
+        bench.fft(p.ref, p.deff)
+        rf = bench.snapshot("fft")
+        v = learned_verify(bench, p, rl, rf, nthr) if not args.no_verify else None
+        ver.append(v)
+        counted_l.append(v["learned"]["counted"] if v else int(((rl["conv"] > 0) & (rl["conv"] < 100)).sum()))
+        counted_f.append(v["fft"]["counted"] if v else int(((rf["conv"] > 0) & (rf["conv"] < 100)).sum()))
+    nF = len(counted_l)
+    tot_l = float(sum(counted_l[k % nF] for k in range(args.steps)))
+    tot_f = float(sum(counted_f[k % nF] for k in range(args.steps)))
+    # end to end through the public API: frames from pinned host memory, results back to it
+    e2e_steps = max(1, args.e2e_steps)
+    M, N, n = bench.M, bench.N, bench.n
+    host = []
+    for p in pairs[:min(nF, e2e_steps)]:
+        hr = torch.empty(M * N, dtype=torch.uint8, pin_memory=True)
+        hd = torch.empty(M * N, dtype=torch.uint8, pin_memory=True)
+        hr.copy_(p.ref)
+        hd.copy_(p.deff)
+        host.append((hr.numpy().reshape((M, N), order="F"), hd.numpy().reshape((M, N), order="F")))
+    hU = torch.empty(2 * n, dtype=torch.float64, pin_memory=True)
+    hc = torch.empty(n, dtype=torch.int32, pin_memory=True)
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for k in range(e2e_steps):
+        hr, hd = host[k % len(host)]
+        bench.learned(hr, hd)
+        with torch.cuda.stream(st):
+            hU.copy_(bench.li.buf["U"], non_blocking=True)
+            hc.copy_(bench.li.buf["conv"], non_blocking=True)
+    e1.record(st)
+    torch.cuda.synchronize(dev)
+    e2e_ms = e0.elapsed_time(e1) / e2e_steps
+    e2e_conv = float(np.mean([counted_l[k % len(host)] for k in range(e2e_steps)]))
+    h2d, d2h = 2 * M * N, hU.numel() * 8 + hc.numel() * 4
+
+    if dist:
+        t = torch.tensor([ms_l, ms_f, e2e_ms], dtype=torch.float64, device=dev)
+        tot = torch.tensor([tot_l, tot_f, e2e_conv], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(tot, op=dist.ReduceOp.SUM)
+        ms_l, ms_f, e2e_ms = float(t[0]), float(t[1]), float(t[2])
+        tot_l, tot_f, e2e_conv = float(tot[0]), float(tot[1]), float(tot[2])
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        v, tcpu, done, conv = learned_cpu_sample(P, pairs[0], bench.gx, bench.gy, args.cpu_per_pass, nthr)
+        cpu = {"value": v, "unit": UNIT, "cores": nthr, "kind": "port",
+               "sample": f"{done} grid subsets of one 2048 x 2048 frame: integer search + IC-GN from [0 U0] "
+                         f"(the reference's path; it has no learned guess), normalisation and gradients scaled "
+                         f"to the sample; {tcpu:.1f} s of CPU wall time, FP64 C++ restatement, OpenMP"}
+
+    if rank == 0:
+        peaks = {}
+        try:
+            peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        except Exception:
+            pass
+        fp32_peak = measure_fp32_peak(torch, dev)
+        icgn_work = float(np.mean([icgn_flops(c, P["w"]) for c in conv_frames])) if conv_frames else None
+        nf = net_flops(M, N, n)
+        bf16_peak = peaks.get("bf16_tflops")
+        summary = {}
+        try:
+            summary = json.load(open(os.path.splitext(train_net.DEFAULT_WEIGHTS)[0] + ".json"))
+        except Exception:
+            pass
+
+        def agg(key):
+            vs = [v[key] for v in ver if v]
+            if not vs:
+                return None
+            return {"counted": int(sum(x["counted"] for x in vs)), "n": int(sum(x["n"] for x in vs)),
+                    "converged_gpu": int(sum(x["converged_gpu"] for x in vs)),
+                    "flag_match_min": min(x["flag_match"] for x in vs),
+                    "iterations_match_min": min(x["iterations_match"] for x in vs),
+                    "mean_iterations": float(np.mean([x["mean_iterations"] for x in vs])),
+                    "uv_max_err": max(x["uv_max_err"] for x in vs), "F_max_err": max(x["F_max_err"] for x in vs)}
+
+        guess = None
+        if ver and ver[0]:
+            gk = ver[0]["guess"].keys()
+            guess = {k: (float(np.mean([v["guess"][k] for v in ver])) if k != "fallback"
+                         else int(sum(v["guess"][k] for v in ver))) for k in gk}
+        value, fft_value = tot_l / (ms_l * 1e-3), tot_f / (ms_f * 1e-3)
+        line = {
+            "metric": LEARNED_METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_l / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 (BF16 network, FP64 solve and re-decisions)",
+            "data": "synthetic (seeded analytic speckle rendering; held-out frames, not in the training set)",
+            "config": {"workload": "learned2048", "subsets_per_frame": n, "frames_cycled": nF, **P,
+                       "l2_flush": "each step a different frame; a step's working set (two 16 MiB FP32 images "
+                                   "and gradients, 2 x 16 MiB feature maps, 356 MiB of conv3 input rows) "
+                                   "exceeds the 126 MB L2"},
+            "fft_init": {"value": fft_value, "unit": UNIT, "ms_per_step": ms_f / args.steps,
+                         "gpu_launches": int(launches_f), "clocks": clk_f},
+            "learned_over_fft": value / fft_value,
+            "gpu_launches": int(launches_l),
+            "stage_ms": {"predict": predict_ms, "icgn_from_net_guess": icgn_ms, "icgn_from_search_guess": fft_icgn_ms},
+            "fallback_rate": float(sum(fallbacks)) / (args.steps * n),
+            "roofline": {"bound": "fp32", "kernel": "IC-GN call from the network's guess (classify, one-warp pass, "
+                                                 "slow-subset pass, general and FP64 re-solve kernels)",
+                         "achieved": icgn_work / (icgn_ms * 1e-3) / 1e12 if icgn_work else None,
+                         "peak": fp32_peak, "unit": "TFLOP/s",
+                         "frac": icgn_work / (icgn_ms * 1e-3) / 1e12 / fp32_peak if icgn_work and fp32_peak else None,
+                         "traffic": None, "algorithmic_flops_per_call": icgn_work, "call_ms": icgn_ms,
+                         "calls_timed": len(icgn_ev),
+                         "flops_counted": "92 (w+1)^2 per subset-iteration + 50 (w+1)^2 per subset solved",
+                         "peak_source": "measured on this GPU: the faster of a scalar FFMA and a packed FFMA2 loop"},
+            "roofline_net": {"bound": "tensor", "kernel": "network prediction (whole-image conv1/conv2, tcgen05 "
+                                                          "correlation, conv3/conv4/FC GEMMs)",
+                             "achieved": nf / (predict_ms * 1e-3) / 1e12, "peak": bf16_peak, "unit": "TFLOP/s",
+                             "frac": nf / (predict_ms * 1e-3) / 1e12 / bf16_peak if bf16_peak else None,
+                             "algorithmic_flops_per_call": nf, "call_ms": predict_ms,
+                             "peak_source": "MEASURED_PEAKS.json bf16_tflops (cuBLAS burst)"},
+            "network": {k: summary.get(k) for k in ("samples", "steps", "batch", "train_s", "data_s", "held_out")},
+            "tuning": bench.ctx.tuning_report(),
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_conv / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "clocks": clk_l,
+            "verification": {"frames": nF, "learned": agg("learned"), "fft": agg("fft"), "guess": guess},
+            "hbm_peak_gbs": peaks.get("hbm_gbs"),
+        }
+        print(json.dumps(line), flush=True)
+    bench.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_reference_learned(args, P):
+    """--impl reference on learned2048: the reference's own path for it (integer search +
+    IC-GN from [0 U0]; it has no learned guess) in the FP64 CPU restatement, all host threads,
+    each step a bounded sample of one held-out frame's grid subsets."""
+    import oracle as O
+
+    O.build()
+    try:
+        import torch
+
+        device = "cuda" if torch.cuda.is_available() else "cpu"
+    except Exception:
+        device = "cpu"
+    nthr = host_threads()
+    frames = learned_frames(P, [50000 + 1000 * args.seed + k for k in range(min(args.steps, P["frames"]))], device)
+    M = P["size"]
+    gx = [P["roi"] + 1, M - P["roi"]]
+    per = 3 * args.ref_per_pass
+    learned_cpu_sample(P, frames[0], gx, gx, max(8, per // 8), nthr, seed=99)  # warm-up
+    times, conv_tot = [], 0
+    for k in range(args.steps):
+        _, t, _, conv = learned_cpu_sample(P, frames[k % len(frames)], gx, gx, per, nthr, seed=k)
+        times.append(t)
+        conv_tot += conv
+    value = conv_tot / sum(times)
+    line = {"impl": "reference", "metric": LEARNED_METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * float(np.mean(times)),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded analytic speckle rendering; held-out frames)",
+            "config": {"workload": args.workload, **P},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthr, "kind": "port",
+                             "sample": f"{per} grid subsets per step: integer search + IC-GN from [0 U0] (the "
+                                       f"reference's path), normalisation and gradients scaled to the sample; "
+                                       f"FP64 C++ restatement, OpenMP"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------------
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="stereo2048",
-                    choices=["stereo2048", "stereo1024", "temporal512", "quadtree2048", "sequence4096"],
-                    help="stereo2048: the headline stereo + temporal + triangulation step; temporal512 and "
+    ap.add_argument("--workload", default="learned2048",
+                    choices=["learned2048", "stereo2048", "stereo1024", "temporal512", "quadtree2048",
+                             "sequence4096"],
+                    help="learned2048: learned vs FFT initial guess on held-out 2048 x 2048 frames (the "
+                         "headline); stereo2048: the stereo + temporal + triangulation step; temporal512 and "
                          "quadtree2048: the 2D and quadtree/Subpb1 configurations; sequence4096: the 50-frame "
                          "4096 x 3000 stereo sequence with per-frame latency (separate JSON lines)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
@@ -545,12 +968,17 @@ def main():
 
     if args.impl == "reference":
         if rank == 0:
-            if args.workload in ("sequence4096", "temporal512", "quadtree2048"):
+            if args.workload == "learned2048":
+                run_reference_learned(args, P)
+            elif args.workload in ("sequence4096", "temporal512", "quadtree2048"):
                 print(json.dumps({"impl": "reference", "unavailable": f"{args.workload} times the FP64 CPU oracle "
                                   "on its own sample of the workload, from the device run's inputs (cpu_baseline "
                                   "of the ours line)"}), flush=True)
             else:
                 run_reference(args, P)
+        return
+    if args.workload == "learned2048":
+        run_learned(args, P)
         return
     if args.workload == "sequence4096":
         if rank == 0:
