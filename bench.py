@@ -894,11 +894,25 @@ def run_learned(args, P):
             "verification": {"frames": nF, "learned": agg("learned"), "fft": agg("fft"), "guess": guess},
             "hbm_peak_gbs": peaks.get("hbm_gbs"),
         }
-        print(json.dumps(line), flush=True)
     bench.close()
+    del pairs, warm
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+    if rank == 0:
+        if world == 1 and not args.no_stereo:
+            # the 1-GPU line also carries the stereo + temporal + triangulation step (its own
+            # frames, timing and whole-grid oracle verification), run after the learned one
+            sargs = argparse.Namespace(**vars(args))
+            sargs.workload, sargs.no_cpu = "stereo2048", True
+            try:
+                sl = run_stereo(sargs, workload_params("stereo2048"), emit=False)
+                line["stereo2048"] = {k: sl.get(k) for k in ("value", "unit", "ms_per_step", "gpu_launches", "config",
+                                                             "roofline", "roofline_icgn", "e2e", "clocks",
+                                                             "verification", "fp64_resolves")}
+            except Exception as e:  # recorded, not fatal to the headline line
+                line["stereo2048"] = {"error": f"{type(e).__name__}: {e}"}
+        print(json.dumps(line), flush=True)
 
 
 def run_reference_learned(args, P):
@@ -940,55 +954,12 @@ def run_reference_learned(args, P):
 
 
 # ----------------------------------------------------------------------------------
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="learned2048",
-                    choices=["learned2048", "stereo2048", "stereo1024", "temporal512", "quadtree2048",
-                             "sequence4096"],
-                    help="learned2048: learned vs FFT initial guess on held-out 2048 x 2048 frames (the "
-                         "headline); stereo2048: the stereo + temporal + triangulation step; temporal512 and "
-                         "quadtree2048: the 2D and quadtree/Subpb1 configurations; sequence4096: the 50-frame "
-                         "4096 x 3000 stereo sequence with per-frame latency (separate JSON lines)")
-    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
-    ap.add_argument("--seed", type=int, default=1)
-    ap.add_argument("--ref-per-pass", type=int, default=200)
-    ap.add_argument("--cpu-per-pass", type=int, default=1200)
-    ap.add_argument("--e2e-steps", type=int, default=2)
-    ap.add_argument("--no-verify", action="store_true")
-    args = ap.parse_args()
-    P = workload_params(args.workload)
-
+def run_stereo(args, P, emit=True):
+    """The stereo2048 / stereo1024 step (see the module docstring); rank 0 returns its JSON
+    line (and prints it when emit)."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
-
-    if args.impl == "reference":
-        if rank == 0:
-            if args.workload == "learned2048":
-                run_reference_learned(args, P)
-            elif args.workload in ("sequence4096", "temporal512", "quadtree2048"):
-                print(json.dumps({"impl": "reference", "unavailable": f"{args.workload} times the FP64 CPU oracle "
-                                  "on its own sample of the workload, from the device run's inputs (cpu_baseline "
-                                  "of the ours line)"}), flush=True)
-            else:
-                run_reference(args, P)
-        return
-    if args.workload == "learned2048":
-        run_learned(args, P)
-        return
-    if args.workload == "sequence4096":
-        if rank == 0:
-            run_sequence(args, P)
-        return
-    if args.workload in ("temporal512", "quadtree2048"):
-        if rank == 0:
-            run_aux(args, P)
-        return
-
     import torch
 
     import aldic_b200 as A
@@ -1123,11 +1094,67 @@ def main():
             "verification": ver,
             "hbm_peak_gbs": peaks.get("hbm_gbs"),
         }
-        print(json.dumps(line), flush=True)
+        if emit:
+            print(json.dumps(line), flush=True)
     pipe.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+    return line if rank == 0 else None
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="learned2048",
+                    choices=["learned2048", "stereo2048", "stereo1024", "temporal512", "quadtree2048",
+                             "sequence4096"],
+                    help="learned2048: learned vs FFT initial guess on held-out 2048 x 2048 frames (the "
+                         "headline); stereo2048: the stereo + temporal + triangulation step; temporal512 and "
+                         "quadtree2048: the 2D and quadtree/Subpb1 configurations; sequence4096: the 50-frame "
+                         "4096 x 3000 stereo sequence with per-frame latency (separate JSON lines)")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--ref-per-pass", type=int, default=200)
+    ap.add_argument("--cpu-per-pass", type=int, default=1200)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-verify", action="store_true")
+    ap.add_argument("--no-stereo", action="store_true",
+                    help="learned2048: skip the stereo2048 step that the 1-GPU line carries as a sub-object")
+    args = ap.parse_args()
+    P = workload_params(args.workload)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank == 0:
+            if args.workload == "learned2048":
+                run_reference_learned(args, P)
+            elif args.workload in ("sequence4096", "temporal512", "quadtree2048"):
+                print(json.dumps({"impl": "reference", "unavailable": f"{args.workload} times the FP64 CPU oracle "
+                                  "on its own sample of the workload, from the device run's inputs (cpu_baseline "
+                                  "of the ours line)"}), flush=True)
+            else:
+                run_reference(args, P)
+        return
+    if args.workload == "learned2048":
+        run_learned(args, P)
+        return
+    if args.workload == "sequence4096":
+        if rank == 0:
+            run_sequence(args, P)
+        return
+    if args.workload in ("temporal512", "quadtree2048"):
+        if rank == 0:
+            run_aux(args, P)
+        return
+
+    run_stereo(args, P)
 
 
 # ----------------------------------------------------------------------------------
