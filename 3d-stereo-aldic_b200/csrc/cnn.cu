@@ -404,6 +404,156 @@ __global__ void __launch_bounds__(kCorrThreads) corr_im2col_kernel(CorrSrc src, 
   for (int q = tid; q < kCorrRows / 16; q += kCorrThreads) outA[q] = reinterpret_cast<const uint4*>(rows)[q];
 }
 
+// conv1 and conv2 over one whole frame image in a single pass (prediction): CTA (bx, i2)
+// computes conv2's outputs (i2, 128 bx .. 128 bx + 127) of the (M2 x N2 x 32) map.  It loads
+// the 7 x 515 image pixels they depend on (BF16-rounded, zero outside the image) into shared
+// memory; for each output pixel the threads compute the 9 conv1 positions conv2's taps read
+// (32 channels each, FP32 sums in tap order, + bias, ReLU, BF16: the arithmetic of
+// conv1_kernel; zero outside conv1's map) straight into conv2's im2col row, written in the
+// 128-byte-swizzled K-major layout as 5 K-blocks of 64 columns (288 used, as conv2's GEMM);
+// conv2's weights are staged alike.  One thread issues the 20 tcgen05.mma (M 128, N 32,
+// K 16) of the GEMM's K order into 32 TMEM columns; the 4 warps read their rows back and
+// store bias + ReLU as BF16.  The results equal conv1_kernel + im2col + the tcgen05 GEMM
+// bit for bit.  The MMA wait is bounded (err bit 3 on time-out).
+constexpr int kFeatThreads = 128, kFeatCols = 4 * 128 + 3, kFeatKb = 5;
+constexpr int kFeatA = kFeatKb * 128 * 128, kFeatB = kFeatKb * 32 * 128;
+constexpr int kFeatSmem = 1024 + kFeatA + kFeatB + 7 * kFeatCols * 2;
+
+__global__ void __launch_bounds__(kFeatThreads) image_features_kernel(const float* __restrict__ img, int M, int N,
+                                                                      const bf16* __restrict__ W1,
+                                                                      const float* __restrict__ b1,
+                                                                      const bf16* __restrict__ W2,
+                                                                      const float* __restrict__ b2,
+                                                                      bf16* __restrict__ out, int* __restrict__ err) {
+  extern __shared__ unsigned char feat_raw[];
+  __shared__ float w1[32][9], bs1[32], bs2[32];
+  __shared__ __align__(8) uint64_t done;
+  __shared__ uint32_t s_tmem;
+  unsigned char* smem =
+      reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(feat_raw) + 1023) & ~uintptr_t(1023));
+  unsigned char* tA = smem;
+  unsigned char* tB = smem + kFeatA;
+  bf16* patch = reinterpret_cast<bf16*>(smem + kFeatA + kFeatB);  // [7][kFeatCols]
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int M1 = (M + 1) / 2, N1 = (N + 1) / 2, N2 = (N1 + 1) / 2;
+  const int i2 = blockIdx.y, j20 = blockIdx.x * 128;
+  const int pi0 = 4 * i2 - 3, pj0 = 4 * j20 - 3;  // image pixel (0-based) of patch (0, 0)
+  for (int q = tid; q < 32 * 9; q += kFeatThreads) w1[q / 9][q % 9] = __bfloat162float(W1[(q / 9) * 16 + q % 9]);
+  if (tid < 32) {
+    bs1[tid] = b1[tid];
+    bs2[tid] = b2[tid];
+  }
+  // image patch: column-major image, 7 consecutive rows per column
+  for (int q = tid; q < kFeatCols; q += kFeatThreads) {
+    const int j = pj0 + q;
+#pragma unroll
+    for (int a = 0; a < 7; ++a) {
+      const int i = pi0 + a;
+      const float v = (i >= 0 && i < M && j >= 0 && j < N) ? img[(size_t)i + (size_t)j * M] : 0.f;
+      patch[a * kFeatCols + q] = __float2bfloat16_rn(v);
+    }
+  }
+  // conv2 weights: K-block kb, row n, chunk c = columns 64 kb + 8 c .. + 7 (zero from 288)
+  for (int q = tid; q < kFeatKb * 32 * 8; q += kFeatThreads) {
+    const int kb = q / 256, n = (q / 8) % 32, c = q % 8, col = kb * 64 + c * 8;
+    const uint4 v = col < 288 ? *reinterpret_cast<const uint4*>(W2 + n * 288 + col) : make_uint4(0u, 0u, 0u, 0u);
+    *reinterpret_cast<uint4*>(tB + kb * 32 * 128 + n * 128 + ((c ^ (n & 7)) << 4)) = v;
+  }
+  if (tid == 0) {
+    mbar_init(&done, 1);
+    fence_barrier_init();
+  }
+  if (warp == 0) tmem_alloc(&s_tmem, 32);
+  __syncthreads();
+  // conv2's im2col row r (output pixel (i2, j20 + r)): tap t = (ky, kx) holds conv1 at
+  // (2 i2 - 1 + ky, 2 j2 - 1 + kx), 32 channels = 4 chunks at K-block t / 2, chunks
+  // 4 (t % 2) .. + 3; K-block 4's chunks 4..7 (columns 288..319) are zero.  Thread: channel
+  // group cg (8 channels, their weights in registers) of rows 4 rg .. 4 rg + 3.
+  {
+    const int cg = tid & 3, rg = tid >> 2;
+    float wr[8][9], br[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      br[k] = bs1[cg * 8 + k];
+#pragma unroll
+      for (int q = 0; q < 9; ++q) wr[k][q] = w1[cg * 8 + k][q];
+    }
+#pragma unroll 1
+    for (int rr = 0; rr < 4; ++rr) {
+      const int r = rg * 4 + rr, j2 = j20 + r;
+#pragma unroll 1
+      for (int t = 0; t < 9; ++t) {
+        const int ky = t / 3, kx = t % 3;
+        const int i1 = 2 * i2 - 1 + ky, j1 = 2 * j2 - 1 + kx;
+        const bool on_map = i1 >= 0 && i1 < M1 && j1 >= 0 && j1 < N1;
+        float x[9];
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+          for (int b = 0; b < 3; ++b)
+            x[a * 3 + b] = __bfloat162float(patch[(2 * ky + a) * kFeatCols + 4 * r + 2 * kx + b]);
+        __align__(16) bf16 o[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          float acc = 0.f;
+#pragma unroll
+          for (int q = 0; q < 9; ++q) acc = fmaf(wr[k][q], x[q], acc);
+          o[k] = __float2bfloat16_rn(on_map ? fmaxf(acc + br[k], 0.f) : 0.f);
+        }
+        const int chunk = (t % 2) * 4 + cg;
+        *reinterpret_cast<uint4*>(tA + (t / 2) * 128 * 128 + r * 128 + ((chunk ^ (r & 7)) << 4)) =
+            *reinterpret_cast<const uint4*>(o);
+      }
+      if (cg == 0) {
+        unsigned char* row = tA + 4 * 128 * 128 + r * 128;
+#pragma unroll
+        for (int chunk = 4; chunk < 8; ++chunk)
+          *reinterpret_cast<uint4*>(row + ((chunk ^ (r & 7)) << 4)) = make_uint4(0u, 0u, 0u, 0u);
+      }
+    }
+  }
+  fence_proxy_async_shared();
+  tcgen05_before_sync();
+  __syncthreads();
+  tcgen05_after_sync();
+  const uint32_t tmem = s_tmem;
+  if (tid == 0) {
+    constexpr uint32_t idesc = bf16_idesc(128, 32);
+    for (int kb = 0; kb < kFeatKb; ++kb) {
+      const uint32_t a = smem_u32(tA + kb * 128 * 128), b = smem_u32(tB + kb * 32 * 128);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) umma_bf16(tmem, sw128_desc(a + 32 * k), sw128_desc(b + 32 * k), idesc, kb > 0 || k > 0);
+    }
+    umma_commit(&done);
+  }
+  __syncwarp();
+  const bool ready = mbar_wait(&done, 0, kCorrWaitCycles);
+  if (!ready && lane == 0) atomicOr(err, 8);
+  tcgen05_after_sync();
+  {
+    const int r = warp * 32 + lane, j2 = j20 + r;
+    float v[32];
+    tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16), *reinterpret_cast<float(*)[16]>(v));
+    tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + 16u, *reinterpret_cast<float(*)[16]>(v + 16));
+    if (j2 < N2) {
+      uint4* dst = reinterpret_cast<uint4*>(out + ((size_t)i2 * N2 + j2) * 32);
+#pragma unroll
+      for (int g = 0; g < 4; ++g) {
+        __align__(16) bf16 o[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          const float x = v[g * 8 + k] + bs2[g * 8 + k];
+          o[k] = __float2bfloat16_rn(x > 0.f ? x : 0.f);
+        }
+        dst[g] = *reinterpret_cast<const uint4*>(o);
+      }
+    }
+  }
+  tcgen05_before_sync();
+  __syncthreads();
+  if (warp == 0) tmem_free(tmem, 32);
+}
+
 // out[c, r] = in[r, c] (BF16, 32 x 32 tiles through shared memory)
 __global__ void transpose_kernel(const bf16* __restrict__ in, bf16* __restrict__ out, long long R, long long Cn) {
   __shared__ bf16 t[32][33];
@@ -503,22 +653,6 @@ __global__ void patch_kernel(FrameDev fr, const double* __restrict__ coords, lon
   }
 }
 
-// A frame image (column-major M x N FP32) as a BF16 M x N row-major map (element (i, j) at
-// i N + j: image x along the map's rows), through 32 x 32 shared-memory tiles.
-__global__ void image_bf16_kernel(const float* __restrict__ img, int M, int N, bf16* __restrict__ out) {
-  __shared__ float t[32][33];
-  const int i0 = blockIdx.x * 32, j0 = blockIdx.y * 32;
-  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
-    const int i = i0 + threadIdx.x, j = j0 + k;
-    t[k][threadIdx.x] = (i < M && j < N) ? img[(size_t)i + (size_t)j * M] : 0.f;
-  }
-  __syncthreads();
-  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
-    const int i = i0 + k, j = j0 + threadIdx.x;
-    if (i < M && j < N) out[(size_t)i * N + j] = __float2bfloat16_rn(t[threadIdx.x][k]);
-  }
-}
-
 // Network outputs (scaled) -> IC-GN initial guess: U0 = (u, v), F0 = (du/dx, dv/dx, du/dy,
 // dv/dy).  With coords, the prediction belongs to the aligned centre (x = 1 mod 4) nearest the
 // subset's: U0 moves to the subset's own centre along F0; ok[t] = 0 gives NaN (no guess).
@@ -569,10 +703,10 @@ struct ProposalNet {
   bf16 *dY = nullptr, *dYt = nullptr;
   float *dAf = nullptr, *dHf = nullptr, *Y = nullptr, *loss = nullptr;
   uint8_t* ok = nullptr;  // per predicted subset: its feature crops lie inside the maps
-  // whole-image features for prediction (sized for the last frame size): the BF16 image,
-  // conv1's output, conv2's im2col rows, the reference and deformed maps
+  // whole-image features for prediction (sized for the last frame size): the reference and
+  // deformed conv2 maps
   int fM = 0, fN = 0;
-  bf16 *imgb = nullptr, *H1i = nullptr, *A2i = nullptr, *FR = nullptr, *FD = nullptr;
+  bf16 *FR = nullptr, *FD = nullptr;
   int* errflag = nullptr;
 };
 
@@ -871,7 +1005,7 @@ void aldic_net_destroy(aldic_net* net) {
   if (net->stream) cudaStreamSynchronize(net->stream);
   void* bufs[] = {net->w,  net->g,   net->m,   net->v,   net->wb,  net->Ht5, net->H6,     net->Ht6,
                   net->dZ6, net->dZt6, net->dY, net->dYt, net->Y, net->dAf, net->dHf, net->loss, net->ok,  net->errflag,
-                  net->imgb, net->H1i, net->A2i, net->FR, net->FD};
+                  net->FR, net->FD};
   for (void* p : bufs)
     if (p) cudaFree(p);
   for (int l = 0; l < 6; ++l)
@@ -994,38 +1128,32 @@ int aldic_net_status(aldic_net* net) {
 namespace aldic {
 // conv1 and conv2 over the whole reference and deformed images of frame fr into net->FR and
 // net->FD: (M + 3) / 4 x (N + 3) / 4 x 32 maps whose pixel (i, j) is centred on image pixel
-// (4 i + 1, 4 j + 1) (1-based)
+// (4 i + 1, 4 j + 1) (1-based); one image_features_kernel launch per image
 int image_features(ProposalNet* net, const FrameDev& fr) {
-  const int M = fr.M, N = fr.N, M1 = (M + 1) / 2, N1 = (N + 1) / 2, M2 = (M1 + 1) / 2, N2 = (N1 + 1) / 2;
-  const long long P1 = (long long)M1 * N1, P2 = (long long)M2 * N2;
+  const int M = fr.M, N = fr.N, M2 = (M + 3) / 4, N2 = (N + 3) / 4;
+  const size_t P2 = (size_t)M2 * N2;
   if (net->fM != M || net->fN != N) {
     NK(cudaStreamSynchronize(net->stream));
-    bf16** bufs[] = {&net->imgb, &net->H1i, &net->A2i, &net->FR, &net->FD};
+    bf16** bufs[] = {&net->FR, &net->FD};
     for (bf16** b : bufs) {
       if (*b) NK(cudaFree(*b));
       *b = nullptr;
     }
     net->fM = net->fN = 0;
-    NK(cudaMalloc(&net->imgb, (size_t)M * N * 2));
-    NK(cudaMalloc(&net->H1i, (size_t)P1 * 32 * 2));
-    NK(cudaMalloc(&net->A2i, (size_t)P2 * 288 * 2));
-    NK(cudaMalloc(&net->FR, (size_t)P2 * 32 * 2));
-    NK(cudaMalloc(&net->FD, (size_t)P2 * 32 * 2));
+    NK(cudaMalloc(&net->FR, P2 * 32 * 2));
+    NK(cudaMalloc(&net->FD, P2 * 32 * 2));
     net->fM = M;
     net->fN = N;
   }
-  const ConvI c1{0, M, N, 1, M1, N1, 32, 9, 16, 2}, c2{1, M1, N1, 32, M2, N2, 32, 288, 288, 2};
+  NK(cudaFuncSetAttribute(image_features_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kFeatSmem));
+  const dim3 grid((unsigned)((N2 + 127) / 128), (unsigned)M2);
   for (int side = 0; side < 2; ++side) {
-    const dim3 tg((unsigned)((M + 31) / 32), (unsigned)((N + 31) / 32));
-    image_bf16_kernel<<<tg, dim3(32, 8), 0, net->stream>>>(side ? fr.def : fr.ref, M, N, net->imgb);
+    image_features_kernel<<<grid, kFeatThreads, kFeatSmem, net->stream>>>(
+        side ? fr.def : fr.ref, M, N, net->wb + kL.w[0], net->w + kL.b[0], net->wb + kL.w[1], net->w + kL.b[1],
+        side ? net->FD : net->FR, net->errflag);
     ++net->launches;
-    conv1(net, net->imgb, View{0, 0, N, 1}, c1, P1, net->H1i);
-    im2col_kernel<<<blocks_for(P2 * 36), 256, 0, net->stream>>>(net->H1i, nhwc(M1, N1, 32), net->A2i, P2, c2);
-    ++net->launches;
-    const int rc = gemm(net, net->A2i, 288, net->wb + kL.w[1], 288, P2, 32, 288, kEpiBiasReluBf16, nullptr,
-                        side ? net->FD : net->FR, net->w + kL.b[1], 32, 1);
-    if (rc) return rc;
   }
+  NK(cudaGetLastError());
   return ALDIC_OK;
 }
 
