@@ -1,6 +1,7 @@
 """Multi-rank sharding on CPU (gloo, world size 2): every rank solves its range of subsets
-and the all-gather reassembles exactly the single-process result.  The per-rank solver is
-the FP64 oracle here (the device path is the same call on each rank's GPU)."""
+and the tensor all-gather reassembles exactly the single-process result.  The per-rank
+solver is the FP64 oracle here (the device path is the same call on each rank's GPU, its
+results gathered as CUDA tensors over NCCL)."""
 import os
 import socket
 
@@ -62,9 +63,19 @@ def _worker(rank, world, port, q):
         r = O.local_icgn(fr, c, u0, 20, 1e-3, variant=1, nthreads=1)
         return {k: r[k] for k in ("U", "F", "H", "conv")}
 
-    got = S.sharded_local_icgn(solve, coords, U0, cost=np.full(len(coords), 441.0))
+    fields = ("U", "F", "conv", "H")
+    # cost: window area x the iterations of a previous solve (uneven ranges)
+    prev = solve(coords, U0)["conv"]
+    got = S.sharded_local_icgn(solve, coords, U0, cost=S.icgn_cost(20, prev), fields=fields)
     full = solve(coords, U0)
-    ok = all(np.array_equal(got[k], full[k], equal_nan=True) for k in full)
+    ok = all(np.array_equal(got[k].numpy(), np.asarray(full[k]), equal_nan=True) for k in fields)
+    # a bare row gather with an uneven partition
+    import torch
+
+    parts = [(0, 3), (3, 10)]
+    s, e = parts[rank]
+    rows = S.gather_rows(torch.arange(s, e, dtype=torch.float64).reshape(-1, 1).repeat(1, 2), parts)
+    ok = ok and torch.equal(rows[:, 0], torch.arange(10, dtype=torch.float64))
     q.put((rank, ok, int(len(coords))))
     dist.barrier()
     dist.destroy_process_group()
