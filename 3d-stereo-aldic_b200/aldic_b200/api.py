@@ -323,6 +323,18 @@ class Context:
                     "aldic_subset_zncc")
         return z
 
+    def fallback_select(self, conv, zncc, zncc_min, out):
+        """Indices (0-based, in no fixed order) of the subsets with conv outside 1..100 or
+        zncc below zncc_min (or NaN) into `out` (int32, n entries of room: a CUDA tensor or a
+        writeable numpy array); returns their number (waits for the device)."""
+        k = _Keep()
+        n = int(conv.numel() if _is_torch(conv) else np.asarray(conv).size)
+        cnt = C.c_int64()
+        self._check(self.lib.aldic_fallback_select(self.h, n, k.ptr(conv, np.int32), k.ptr(zncc, np.float64),
+                                                   float(zncc_min), k.dst(out, np.int32, n), C.byref(cnt)),
+                    "aldic_fallback_select")
+        return int(cnt.value)
+
     def integer_search_list(self, search, gridx, gridy, winsize, step, grid_idx, out=None):
         """The integer search on the grid subsets grid_idx (i + j nX) only: dict of n-entry
         arrays x, y, u, v, phi in list order (or the CUDA tensors of `out`)."""

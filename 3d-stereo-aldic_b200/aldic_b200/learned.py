@@ -270,6 +270,7 @@ class LearnedInit:
         self.buf = {"U0": T.empty(2 * n, **f64), "F0": T.empty(4 * n, **f64), "U": T.empty(2 * n, **f64),
                     "F": T.empty(4 * n, **f64), "conv": T.empty(n, dtype=T.int32, device=dev),
                     "zncc": T.empty(n, **f64), "fallback": T.zeros(n, dtype=T.bool, device=dev)}
+        self.flist = T.empty(n, dtype=T.int32, device=dev)
         self.n_fallback = 0
         # (start, stop) CUDA event pairs recorded around the prediction and the main IC-GN call
         # when these are lists (timing hooks)
@@ -296,15 +297,14 @@ class LearnedInit:
                         lambda: ctx.local_icgn(self.variant, self.coords, b["U0"], self.w, self.tol, want_H=False,
                                                want_mark=False, out=b, F0=b["F0"]))
             ctx.subset_zncc(self.coords, b["U"], b["F"], self.w, out=b["zncc"])
-            c = b["conv"]
-            bad = (c < 1) | (c > 100) | ~(b["zncc"] >= self.zncc_min)
-            b["fallback"].copy_(bad)
-            idx = T.nonzero(bad).flatten()
-            nf = int(idx.numel())  # the host's one wait
+            nf = ctx.fallback_select(b["conv"], b["zncc"], self.zncc_min, self.flist)  # the host's one wait
+            b["fallback"].zero_()
             if nf:
+                il = self.flist[:nf]
+                idx = il.long()
+                b["fallback"][idx] = True
                 dev = self.coords.device
                 f64 = dict(dtype=T.float64, device=dev)
-                il = idx.to(T.int32)
                 r = {k: T.empty(nf, **f64) for k in ("x", "y", "u", "v", "phi")}
                 ctx.integer_search_list(self.search, self.gx, self.gy, self.w, self.step, il, out=r)
                 U0f = T.nan_to_num(T.stack([r["u"], r["v"]], 1), nan=0.0).reshape(-1).contiguous()

@@ -51,6 +51,7 @@ struct aldic_ctx {
   unsigned int* counter = nullptr;
   int npartials = 0;
   int* qcount = nullptr;
+  int* sel_count = nullptr;  // aldic_fallback_select's counter
   double* I1 = nullptr;
   double* I2 = nullptr;
   double* iitot = nullptr;
@@ -276,7 +277,7 @@ void aldic_destroy(aldic_ctx* c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   void* bufs[] = {c->img[0], c->img[1], c->mask, c->gx, c->gy, c->stats, c->partials, c->counter, c->qcount,
-                  c->I1, c->I2, c->iitot, c->tscratch, c->arena.base, c->sp2};
+                  c->I1, c->I2, c->iitot, c->tscratch, c->arena.base, c->sp2, c->sel_count};
   for (void* b : bufs)
     if (b) cudaFree(b);
   for (cudaEvent_t e : c->prof_ev) cudaEventDestroy(e);
@@ -810,6 +811,29 @@ int aldic_subset_zncc(aldic_ctx* c, int64_t n, const double* coords, const doubl
   if (rc) return rc;
   return finish(c, launch_subset_zncc(frame_of(c), n, (const double*)ac.dev, (const double*)au.dev,
                                       (const double*)af.dev, winsize, (double*)az.dev, c->stream));
+}
+
+int aldic_fallback_select(aldic_ctx* c, int64_t n, const int32_t* conv, const double* zncc, double zncc_min,
+                          int32_t* list, int64_t* count) {
+  if (!c) return ALDIC_ERR_ARG;
+  if (n < 0 || !count) return fail(c, ALDIC_ERR_ARG, "n >= 0 and count are required");
+  *count = 0;
+  if (n == 0) return ALDIC_OK;
+  if (!conv || !zncc || !list) return fail(c, ALDIC_ERR_ARG, "conv, zncc and list are required");
+  CK(cudaSetDevice(c->device));
+  if (!c->sel_count) CK(cudaMalloc(&c->sel_count, sizeof(int)));
+  Arg acv{conv, (size_t)n * 4, false, nullptr}, az{zncc, (size_t)n * 8, false, nullptr};
+  Arg al{list, (size_t)n * 4, true, nullptr};
+  int rc = stage(c, {&acv, &az, &al});
+  if (rc) return rc;
+  c->launches += launch_fallback_select((const int32_t*)acv.dev, (const double*)az.dev, n, zncc_min,
+                                        (int32_t*)al.dev, c->sel_count, c->stream);
+  int h = 0;
+  CK(cudaMemcpyAsync(&h, c->sel_count, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  rc = finish(c, 0);  // copies a host list back and waits
+  CK(cudaStreamSynchronize(c->stream));
+  *count = h;
+  return rc;
 }
 
 int aldic_net_predict(aldic_net* net, aldic_ctx* c, int64_t n, const double* coords, double* U0, double* F0) {

@@ -23,7 +23,8 @@
 // conv2 once over each whole image and the correlation and the rest per subset, on feature
 // crops at the subset's position (subset centres x = 1 mod 4 in both coordinates align the
 // two).  Every convolution, data gradient, weight gradient and fully connected layer is one
-// tcgen05 GEMM (cnn_gemm.cu) over im2col rows; the correlation and the rest are the small
+// tcgen05 GEMM (cnn_gemm.cu) over im2col rows (conv4, on a 4 x 4 map, as one dense 1024 x 1024
+// matrix on the flattened map instead); the correlation and the rest are the small
 // kernels below (im2col, col2im, correlation and its gradient, transposes, ReLU gradient, loss,
 // bias gradient, Adam, patch extraction).  Training: mean squared error on the scaled outputs
 // (u / 8, v / 8, F x 20), Adam.
@@ -443,21 +444,42 @@ __global__ void __launch_bounds__(kFeatThreads) image_features_kernel(const floa
     bs1[tid] = b1[tid];
     bs2[tid] = b2[tid];
   }
-  // image patch: column-major image, 7 consecutive rows per column
-  for (int q = tid; q < kFeatCols; q += kFeatThreads) {
-    const int j = pj0 + q;
+  // image patch: column-major image, 7 consecutive rows per column; every load of a thread is
+  // issued before any store (one round of memory latency, not five)
+  {
+    constexpr int kIters = (kFeatCols + kFeatThreads - 1) / kFeatThreads;
+    float v[kIters][7];
 #pragma unroll
-    for (int a = 0; a < 7; ++a) {
-      const int i = pi0 + a;
-      const float v = (i >= 0 && i < M && j >= 0 && j < N) ? img[(size_t)i + (size_t)j * M] : 0.f;
-      patch[a * kFeatCols + q] = __float2bfloat16_rn(v);
+    for (int it = 0; it < kIters; ++it) {
+      const int q = tid + it * kFeatThreads, j = pj0 + q;
+#pragma unroll
+      for (int a = 0; a < 7; ++a) {
+        const int i = pi0 + a;
+        v[it][a] = (q < kFeatCols && i >= 0 && i < M && j >= 0 && j < N) ? img[(size_t)i + (size_t)j * M] : 0.f;
+      }
+    }
+#pragma unroll
+    for (int it = 0; it < kIters; ++it) {
+      const int q = tid + it * kFeatThreads;
+      if (q < kFeatCols)
+#pragma unroll
+        for (int a = 0; a < 7; ++a) patch[a * kFeatCols + q] = __float2bfloat16_rn(v[it][a]);
     }
   }
   // conv2 weights: K-block kb, row n, chunk c = columns 64 kb + 8 c .. + 7 (zero from 288)
-  for (int q = tid; q < kFeatKb * 32 * 8; q += kFeatThreads) {
-    const int kb = q / 256, n = (q / 8) % 32, c = q % 8, col = kb * 64 + c * 8;
-    const uint4 v = col < 288 ? *reinterpret_cast<const uint4*>(W2 + n * 288 + col) : make_uint4(0u, 0u, 0u, 0u);
-    *reinterpret_cast<uint4*>(tB + kb * 32 * 128 + n * 128 + ((c ^ (n & 7)) << 4)) = v;
+  {
+    constexpr int kIters = kFeatKb * 32 * 8 / kFeatThreads;
+    uint4 v[kIters];
+#pragma unroll
+    for (int it = 0; it < kIters; ++it) {
+      const int q = tid + it * kFeatThreads, n = (q / 8) % 32, c = q % 8, col = (q / 256) * 64 + c * 8;
+      v[it] = col < 288 ? *reinterpret_cast<const uint4*>(W2 + n * 288 + col) : make_uint4(0u, 0u, 0u, 0u);
+    }
+#pragma unroll
+    for (int it = 0; it < kIters; ++it) {
+      const int q = tid + it * kFeatThreads, kb = q / 256, n = (q / 8) % 32, c = q % 8;
+      *reinterpret_cast<uint4*>(tB + kb * 32 * 128 + n * 128 + ((c ^ (n & 7)) << 4)) = v[it];
+    }
   }
   if (tid == 0) {
     mbar_init(&done, 1);
@@ -552,6 +574,44 @@ __global__ void __launch_bounds__(kFeatThreads) image_features_kernel(const floa
   tcgen05_before_sync();
   __syncthreads();
   if (warp == 0) tmem_free(tmem, 32);
+}
+
+// conv4 (3 x 3, stride 1, pad 1, 64 -> 64 channels on the 4 x 4 map) as one dense
+// 1024 x 1024 matrix on the flattened map (index (y 4 + x) 64 + c): W4d[(oy, ox, co)][(iy, ix,
+// ci)] = W4[co][(ky, kx, ci)] where (iy, ix) = (oy - 1 + ky, ox - 1 + kx), else 0; with its
+// transpose and the bias per output entry.  One thread per entry.
+__global__ void conv4_dense_kernel(const bf16* __restrict__ w4, const float* __restrict__ b4, bf16* __restrict__ W,
+                                   bf16* __restrict__ WT, float* __restrict__ bd) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < 1024 * 1024; e += gridDim.x * blockDim.x) {
+    const int r = e / 1024, c = e % 1024;
+    const int co = r % 64, oy = r / 256, ox = (r / 64) % 4;
+    const int ci = c % 64, iy = c / 256, ix = (c / 64) % 4;
+    const int ky = iy - oy + 1, kx = ix - ox + 1;
+    const bf16 v = (ky >= 0 && ky <= 2 && kx >= 0 && kx <= 2) ? w4[co * 576 + (ky * 3 + kx) * 64 + ci]
+                                                              : __float2bfloat16_rn(0.f);
+    W[(size_t)r * 1024 + c] = v;
+    WT[(size_t)c * 1024 + r] = v;
+    if (c == 0) bd[r] = b4[co];
+  }
+}
+
+// The conv4 weight gradient from the dense one: dW4[co][(ky, kx, ci)] sums dW4d over the
+// output positions whose tap (ky, kx) stays on the map (fixed order).
+__global__ void conv4_fold_kernel(const float* __restrict__ dWd, float* __restrict__ g) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < 64 * 576; e += gridDim.x * blockDim.x) {
+    const int co = e / 576, k = e % 576, tap = k / 64, ci = k % 64, ky = tap / 3, kx = tap % 3;
+    float acc = 0.f;
+    for (int oy = 0; oy < 4; ++oy) {
+      const int iy = oy - 1 + ky;
+      if (iy < 0 || iy >= 4) continue;
+      for (int ox = 0; ox < 4; ++ox) {
+        const int ix = ox - 1 + kx;
+        if (ix < 0 || ix >= 4) continue;
+        acc += dWd[(size_t)((oy * 4 + ox) * 64 + co) * 1024 + (iy * 4 + ix) * 64 + ci];
+      }
+    }
+    g[e] += acc;
+  }
 }
 
 // out[c, r] = in[r, c] (BF16, 32 x 32 tiles through shared memory)
@@ -700,6 +760,9 @@ struct ProposalNet {
   // gradient dY (dYt).  conv3's im2col rows A[kConv3] come straight from the correlation.
   bf16 *A[kNumConv] = {}, *At[kNumConv] = {}, *H[kNumConv] = {}, *dZ[kNumConv] = {}, *dZt[kNumConv] = {};
   bf16 *Ht5 = nullptr, *H6 = nullptr, *Ht6 = nullptr, *dZ6 = nullptr, *dZt6 = nullptr;
+  bf16 *W4d = nullptr, *W4dT = nullptr;  // conv4 as a dense 1024 x 1024 matrix and its transpose
+  float* b4d = nullptr;                   // its bias per output entry
+  bool w4d_valid = false;                 // W4d, W4dT, b4d match the current weights
   bf16 *dY = nullptr, *dYt = nullptr;
   float *dAf = nullptr, *dHf = nullptr, *Y = nullptr, *loss = nullptr;
   uint8_t* ok = nullptr;  // per predicted subset: its feature crops lie inside the maps
@@ -793,7 +856,16 @@ int head(ProposalNet* net, int batch) {
   const ConvI& L3 = kConv[kConv3];
   int rc = gemm(net, net->A[kConv3], L3.Kp, net->wb + kL.w[L3.layer], L3.Kp, P_of(kConv3, batch), L3.Cout, L3.Kp,
                 kEpiBiasReluBf16, nullptr, net->H[kConv3], net->w + kL.b[L3.layer], L3.Cout, 1);
-  if (!rc) rc = conv_forward(net, kConv4, batch, net->H[kConv3], nhwc(4, 4, 64));
+  if (!rc) {  // conv4 as one dense GEMM on conv3's flattened output (no im2col)
+    if (!net->w4d_valid) {  // rebuilt after every change of the weights
+      conv4_dense_kernel<<<512, 256, 0, net->stream>>>(net->wb + kL.w[3], net->w + kL.b[3], net->W4d, net->W4dT,
+                                                       net->b4d);
+      ++net->launches;
+      net->w4d_valid = true;
+    }
+    rc = gemm(net, net->H[kConv3], kFcIn, net->W4d, kFcIn, batch, kFcIn, kFcIn, kEpiBiasReluBf16, nullptr,
+              net->H[kConv4], net->b4d, kFcIn, 1);
+  }
   if (!rc)
     rc = gemm(net, net->H[kConv4], kFcIn, net->wb + kL.w[4], kFcIn, batch, kFcHid, kFcIn, kEpiBiasReluBf16, nullptr,
               net->H6, net->w + kL.b[4], kFcHid, 1);
@@ -896,7 +968,18 @@ int backward(ProposalNet* net, int batch, const bf16* X, const float* T) {
   if (rc) return rc;
   relu_grad(net, net->H[kConv4], net->dZ[kConv4], B * kFcIn);
   // conv4, conv3
-  if ((rc = conv_wgrad(net, kConv4, batch)) || (rc = conv_dgrad(net, kConv4, batch))) return rc;
+  // conv4 (dense): dW4d = dZ4^T H3 folded onto the 3 x 3 weights, db, dH3 = dZ4 W4d
+  transpose(net, net->dZ[kConv4], net->dZt[kConv4], B, kFcIn);
+  transpose(net, net->H[kConv3], net->At[kConv4], B, kFcIn);
+  rc = gemm(net, net->dZt[kConv4], B, net->At[kConv4], B, kFcIn, kFcIn, B, kEpiStore, net->dAf, nullptr, nullptr,
+            kFcIn, 1);
+  if (rc) return rc;
+  conv4_fold_kernel<<<144, 256, 0, st>>>(net->dAf, net->g + kL.w[3]);
+  bias_grad_kernel<<<148, 64, 0, st>>>(net->dZ[kConv4], B * 16, 64, net->g + kL.b[3]);
+  net->launches += 2;
+  rc = gemm(net, net->dZ[kConv4], kFcIn, net->W4dT, kFcIn, B, kFcIn, kFcIn, kEpiStore, net->dHf, nullptr, nullptr,
+            kFcIn, 1);
+  if (rc) return rc;
   relu_grad(net, net->H[kConv3], net->dZ[kConv3], B * 16 * 64);
   if ((rc = conv_wgrad(net, kConv3, batch)) || (rc = conv_dgrad(net, kConv3, batch))) return rc;
   // correlation: dHf holds dC (B, 8, 8, 81); the ReLUs of conv2's outputs folded in
@@ -964,7 +1047,7 @@ int aldic_net_create(aldic_net** out, int device, int max_batch) {
   if (e == cudaSuccess) e = cudaMalloc(&net->v, n * 4);
   if (e == cudaSuccess) e = cudaMalloc(&net->wb, n * 2);
   for (int l = 0; l < 6 && e == cudaSuccess; ++l) e = cudaMalloc(&net->wt[l], kL.rows[l] * kL.cols[l] * 2);
-  long long maxA = 0, maxH = B * kFcIn;
+  long long maxA = (long long)kFcIn * kFcIn, maxH = B * kFcIn;  // dAf also holds conv4's dense gradient
   for (int i = 0; i < kNumConv && e == cudaSuccess; ++i) {
     const ConvI& L = kConv[i];
     const long long P = P_of(i, (int)B);
@@ -977,6 +1060,9 @@ int aldic_net_create(aldic_net** out, int device, int max_batch) {
     if (e == cudaSuccess) e = cudaMalloc(&net->dZt[i], P * L.Cout * 2);
   }
   if (e == cudaSuccess) e = cudaMalloc(&net->Ht5, B * kFcIn * 2);
+  if (e == cudaSuccess) e = cudaMalloc(&net->W4d, kFcIn * kFcIn * 2);
+  if (e == cudaSuccess) e = cudaMalloc(&net->W4dT, kFcIn * kFcIn * 2);
+  if (e == cudaSuccess) e = cudaMalloc(&net->b4d, kFcIn * 4);
   if (e == cudaSuccess) e = cudaMalloc(&net->H6, B * kFcHid * 2);
   if (e == cudaSuccess) e = cudaMalloc(&net->Ht6, B * kFcHid * 2);
   if (e == cudaSuccess) e = cudaMalloc(&net->dZ6, B * kFcHid * 2);
@@ -1005,7 +1091,7 @@ void aldic_net_destroy(aldic_net* net) {
   if (net->stream) cudaStreamSynchronize(net->stream);
   void* bufs[] = {net->w,  net->g,   net->m,   net->v,   net->wb,  net->Ht5, net->H6,     net->Ht6,
                   net->dZ6, net->dZt6, net->dY, net->dYt, net->Y, net->dAf, net->dHf, net->loss, net->ok,  net->errflag,
-                  net->FR, net->FD};
+                  net->FR, net->FD, net->W4d, net->W4dT, net->b4d};
   for (void* p : bufs)
     if (p) cudaFree(p);
   for (int l = 0; l < 6; ++l)
@@ -1037,6 +1123,7 @@ int aldic_net_set_params(aldic_net* net, const float* params) {
   NK(cudaMemsetAsync(net->m, 0, sizeof(float) * kL.n, net->stream));
   NK(cudaMemsetAsync(net->v, 0, sizeof(float) * kL.n, net->stream));
   net->step_count = 0;
+  net->w4d_valid = false;
   ++net->launches;
   NK(cudaStreamSynchronize(net->stream));
   return ALDIC_OK;
@@ -1084,6 +1171,7 @@ int aldic_net_train_step(aldic_net* net, int batch, const void* x, const float* 
   adam_kernel<<<blocks_for(kL.n), 256, 0, net->stream>>>(net->w, net->wb, net->g, net->m, net->v, kL.n, lr, b1, b2,
                                                           1e-8f, bc1, bc2);
   ++net->launches;
+  net->w4d_valid = false;
   if (loss) {
     NK(cudaMemcpyAsync(loss, net->loss, sizeof(float), cudaMemcpyDefault, net->stream));
     NK(cudaStreamSynchronize(net->stream));

@@ -2095,6 +2095,27 @@ int launch_subset_zncc(const FrameDev& fr, long long n, const double* coords, co
   return 1;
 }
 
+// The subsets a learned initial guess failed: IC-GN did not converge (code outside 1..100) or
+// the final ZNCC is below zmin (or NaN).  Their indices are appended to list (in no fixed
+// order) and counted in *count (zeroed by the caller).
+__global__ void fallback_select_kernel(const int32_t* __restrict__ conv, const double* __restrict__ zncc, long long n,
+                                       double zmin, int32_t* __restrict__ list, int* __restrict__ count) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const int c = conv[t];
+    if (c < 1 || c > 100 || !(zncc[t] >= zmin)) list[atomicAdd(count, 1)] = (int32_t)t;
+  }
+}
+
+int launch_fallback_select(const int32_t* conv, const double* zncc, long long n, double zmin, int32_t* list,
+                           int* count, cudaStream_t st) {
+  if (n <= 0) return 0;
+  cudaMemsetAsync(count, 0, sizeof(int), st);
+  const long long blocks = (n + 255) / 256;
+  fallback_select_kernel<<<(unsigned)(blocks < 148 * 16 ? blocks : 148 * 16), 256, 0, st>>>(conv, zncc, n, zmin, list,
+                                                                                           count);
+  return 1;
+}
+
 int launch_subpb1(const Sub1Args& a, int wmax_x, int wmax_y, cudaStream_t st) {
   int launches = 0;
   cudaMemsetAsync(a.qcount, 0, 4 * sizeof(int), st);  // 2 queue counts, 2 work counters

@@ -119,6 +119,8 @@ size_t sub1_smem_bytes(int wx, int wy);
 int launch_icgn(const IcgnArgs& a, int wmax_enlarged, cudaStream_t st);
 // ZNCC of each subset's (w+1)^2 window of REF against DEF warped by P = [F U] (NaN where the
 // warped window leaves [3, M-2] x [3, N-2]); FP32 interpolation, FP64 sums.
+int launch_fallback_select(const int32_t* conv, const double* zncc, long long n, double zmin, int32_t* list,
+                           int* count, cudaStream_t st);
 int launch_subset_zncc(const FrameDev& fr, long long n, const double* coords, const double* U, const double* F,
                        int winsize, double* zncc, cudaStream_t st);
 // Proposal network (cnn.cu): the network input of n subsets (n x 64 x 64 x 2 BF16) from frame fr.

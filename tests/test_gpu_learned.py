@@ -134,6 +134,23 @@ def test_list_search_matches_the_whole_grid(env):
     assert np.array_equal(nodes[1], full["y"].ravel())
 
 
+def test_fallback_selection(env):
+    torch, ctx = env["torch"], env["ctx"]
+    rng = np.random.default_rng(5)
+    n = 5000
+    conv = rng.integers(-1, 103, n).astype(np.int32)
+    zncc = rng.uniform(0.5, 1.0, n)
+    zncc[rng.choice(n, 40, replace=False)] = np.nan
+    want = np.flatnonzero((conv < 1) | (conv > 100) | ~(zncc >= 0.9))
+    out = np.empty(n, dtype=np.int32)
+    k = ctx.fallback_select(conv, zncc, 0.9, out)
+    assert k == want.size and np.array_equal(np.sort(out[:k]), want)
+    dev = torch.device("cuda:0")
+    outd = torch.empty(n, dtype=torch.int32, device=dev)
+    k2 = ctx.fallback_select(torch.from_numpy(conv).to(dev), torch.from_numpy(zncc).to(dev), 0.9, outd)
+    assert k2 == k and np.array_equal(np.sort(outd[:k2].cpu().numpy()), want)
+
+
 def _patches_numpy(f, g, crd):
     M, N = f.shape
     out = np.zeros((crd.shape[0], 72, 72, 2))
