@@ -279,20 +279,20 @@ __device__ __forceinline__ bool corr_crops(const CorrSrc& s, long long t, const 
 }
 
 // The correlation volume of sample t (blockIdx.x) on the tensor cores and, from it, conv3's
-// im2col rows.  The 8 x 8 reference feature crop (64 rows of 32 BF16 channels) and the
-// 16 x 16 deformed crop (256 rows) are written to shared memory in the 128-byte-swizzled
-// K-major layout (only the first 64 bytes of each 128-byte row, the 32 channels the two
-// K = 16 steps read, are written; A rows 64..127 are not read back); one thread issues two
-// tcgen05.mma (M 128, N 256) into 256 TMEM columns: D[p, q] = fR[p] . fD[q] for every
-// reference / deformed position pair.  Warps 0 and 1 (TMEM lanes 0..63, the reference
-// positions p = 8 ii + j) then read the 12 deformed rows their 32 lanes touch (tcgen05.ld, 16
-// columns each) and keep, for their own row ii, the 9 offsets of each of deformed rows ii ..
-// ii + 8 (columns j .. j + 8, picked by a 3-stage rotation by j): the volume entries / 32,
-// rounded to BF16, each written straight to the (at most 4) places conv3's im2col rows use it,
-// in a shared-memory copy of the sample's 16 rows x 736 columns (zero elsewhere).  All 128
-// threads then copy those rows out with 16-byte stores.  ok[t] = 0 (whole-image crops
-// leaving the maps) gives a zero volume.  The MMA wait is bounded (err bit 2 on time-out,
-// the volume then undefined).
+// im2col rows.  The 8 x 8 reference feature crop (64 rows of 32 BF16 channels, written twice:
+// A rows p and 64 + p) and the 16 x 16 deformed crop (256 rows) are staged in shared memory in
+// the 128-byte-swizzled K-major layout (only the first 64 bytes of each 128-byte row, the 32
+// channels the two K = 16 steps read, are written); one thread issues two tcgen05.mma (M 128,
+// N 256) into 256 TMEM columns: D[p, q] = fR[p] . fD[q] for every reference / deformed
+// position pair.  Each warp w reads TMEM lanes 32 w .. (reference positions p = 8 ii + j,
+// rows 64.. repeating 0..63), 6 of the 12 deformed rows its lanes touch (tcgen05.ld, 16
+// columns each; warps w and w + 2 split them), and keeps, for its own row ii, the 9 offsets of
+// each deformed row within ii .. ii + 8 (columns j .. j + 8, picked by a 3-stage rotation by
+// j): the volume entries / 32, rounded to BF16, each written straight to the (at most 4)
+// places conv3's im2col rows use it, in a shared-memory copy of the sample's 16 rows x 736
+// columns (zero elsewhere).  All 128 threads then copy those rows out with 16-byte stores.
+// ok[t] = 0 (whole-image crops leaving the maps) gives a zero volume.  The MMA wait is bounded
+// (err bit 2 on time-out, the volume then undefined).
 constexpr int kCorrThreads = 128;
 constexpr int kCorrA = 128 * 128, kCorrB = 256 * 128;  // operand tiles (bytes)
 constexpr int kCorrRows = 16 * 736 * 2;                // conv3's im2col rows of the sample
@@ -334,10 +334,12 @@ __global__ void __launch_bounds__(kCorrThreads) corr_im2col_kernel(CorrSrc src, 
 #pragma unroll
     for (int i = 0; i < 10; ++i) {
       const int q = tid + i * kCorrThreads;
-      if (i < 2)
+      if (i < 2) {  // A rows p and p + 64 (a copy: TMEM lanes 64..127 for warps 2 and 3)
         put_chunk(tA, q / 4, q % 4, v[i]);
-      else
+        put_chunk(tA, 64 + q / 4, q % 4, v[i]);
+      } else {
         put_chunk(tB, (q - 256) / 4, q % 4, v[i]);
+      }
     }
   }
   // the im2col rows start at zero (padding taps and the 7 padding columns)
@@ -363,8 +365,10 @@ __global__ void __launch_bounds__(kCorrThreads) corr_im2col_kernel(CorrSrc src, 
   const bool ready = mbar_wait(&done, 0, kCorrWaitCycles);
   if (!ready && lane == 0) atomicOr(err, 4);
   tcgen05_after_sync();
-  if (warp < 2) {
-    const int p = warp * 32 + lane, ii = p / 8, j = p % 8, ii0 = warp * 4;
+  {
+    // warp w reads TMEM lanes 32 (w % 4) ..: reference positions p = 32 (w % 2) + lane (rows
+    // 64.. repeat 0..63); warps w and w + 2 split the 12 deformed rows their lanes touch
+    const int p = (warp % 2) * 32 + lane, ii = p / 8, j = p % 8, ii0 = (warp % 2) * 4, half = warp / 2;
     // the im2col places of volume position (ii, j): output (oy, ox) with 2 oy - 1 + ky = ii and
     // 2 ox - 1 + kx = j, tap (ky, kx); at most 2 per axis
     int base[4];
@@ -377,7 +381,7 @@ __global__ void __launch_bounds__(kCorrThreads) corr_im2col_kernel(CorrSrc src, 
                     : -1;
     }
 #pragma unroll 1
-    for (int rr = 0; rr < 12; ++rr) {
+    for (int rr = 6 * half; rr < 6 * half + 6; ++rr) {
       float v[16];
       tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)((ii0 + rr) * 16), v);
       const int di = ii0 + rr - ii;  // deformed row ii0 + rr = ii + di
@@ -417,7 +421,7 @@ __global__ void __launch_bounds__(kCorrThreads) corr_im2col_kernel(CorrSrc src, 
 // store bias + ReLU as BF16.  The results equal conv1_kernel + im2col + the tcgen05 GEMM
 // bit for bit.  The MMA wait is bounded (err bit 3 on time-out).
 constexpr int kFeatThreads = 128, kFeatCols = 4 * 128 + 3, kFeatKb = 5;
-constexpr int kFeatA = kFeatKb * 128 * 128, kFeatB = kFeatKb * 32 * 128;
+constexpr int kFeatA = 2 * 128 * 128, kFeatB = kFeatKb * 32 * 128;  // A: two K-block buffers
 constexpr int kFeatSmem = 1024 + kFeatA + kFeatB + 7 * kFeatCols * 2;
 
 __global__ void __launch_bounds__(kFeatThreads) image_features_kernel(const float* __restrict__ img, int M, int N,
@@ -428,7 +432,7 @@ __global__ void __launch_bounds__(kFeatThreads) image_features_kernel(const floa
                                                                       bf16* __restrict__ out, int* __restrict__ err) {
   extern __shared__ unsigned char feat_raw[];
   __shared__ float w1[32][9], bs1[32], bs2[32];
-  __shared__ __align__(8) uint64_t done;
+  __shared__ __align__(8) uint64_t kbar[2];  // MMAs of the K-blocks in A buffer 0 / 1 done
   __shared__ uint32_t s_tmem;
   unsigned char* smem =
       reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(feat_raw) + 1023) & ~uintptr_t(1023));
@@ -482,29 +486,50 @@ __global__ void __launch_bounds__(kFeatThreads) image_features_kernel(const floa
     }
   }
   if (tid == 0) {
-    mbar_init(&done, 1);
+    mbar_init(&kbar[0], 1);
+    mbar_init(&kbar[1], 1);
     fence_barrier_init();
   }
   if (warp == 0) tmem_alloc(&s_tmem, 32);
+  tcgen05_before_sync();
   __syncthreads();
+  tcgen05_after_sync();
   // conv2's im2col row r (output pixel (i2, j20 + r)): tap t = (ky, kx) holds conv1 at
   // (2 i2 - 1 + ky, 2 j2 - 1 + kx), 32 channels = 4 chunks at K-block t / 2, chunks
-  // 4 (t % 2) .. + 3; K-block 4's chunks 4..7 (columns 288..319) are zero.  Thread: channel
-  // group cg (8 channels, their weights in registers) of rows 4 rg .. 4 rg + 3.
-  {
-    const int cg = tid & 3, rg = tid >> 2;
-    float wr[8][9], br[8];
+  // 4 (t % 2) .. + 3; K-block 4's chunks 4..7 (columns 288..319) are zero.  K-blocks are built
+  // into two alternating buffers while the previous one's MMAs run.  Thread: channel group cg
+  // (8 channels, their weights in registers) of rows 4 rg .. 4 rg + 3.
+  const int cg = tid & 3, rg = tid >> 2;
+  float wr[8][9], br[8];
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      br[k] = bs1[cg * 8 + k];
+  for (int k = 0; k < 8; ++k) {
+    br[k] = bs1[cg * 8 + k];
 #pragma unroll
-      for (int q = 0; q < 9; ++q) wr[k][q] = w1[cg * 8 + k][q];
+    for (int q = 0; q < 9; ++q) wr[k][q] = w1[cg * 8 + k][q];
+  }
+  const uint32_t tmem = s_tmem;
+  bool ready = true;
+#pragma unroll 1
+  for (int kb = 0; kb < kFeatKb; ++kb) {
+    const int buf = kb & 1;
+    unsigned char* tAk = tA + buf * 128 * 128;
+    if (kb >= 2) {  // the MMAs of K-block kb - 2 read this buffer
+      ready = mbar_wait(&kbar[buf], (uint32_t)(((kb - 2) >> 1) & 1), kCorrWaitCycles) && ready;
+      tcgen05_after_sync();
     }
 #pragma unroll 1
     for (int rr = 0; rr < 4; ++rr) {
       const int r = rg * 4 + rr, j2 = j20 + r;
 #pragma unroll 1
-      for (int t = 0; t < 9; ++t) {
+      for (int t = 2 * kb; t < 2 * kb + 2; ++t) {
+        const int chunk0 = (t % 2) * 4;
+        if (t >= 9) {  // K columns 288..319
+          if (cg == 0)
+#pragma unroll
+            for (int chunk = 4; chunk < 8; ++chunk)
+              *reinterpret_cast<uint4*>(tAk + r * 128 + ((chunk ^ (r & 7)) << 4)) = make_uint4(0u, 0u, 0u, 0u);
+          continue;
+        }
         const int ky = t / 3, kx = t % 3;
         const int i1 = 2 * i2 - 1 + ky, j1 = 2 * j2 - 1 + kx;
         const bool on_map = i1 >= 0 && i1 < M1 && j1 >= 0 && j1 < N1;
@@ -522,34 +547,25 @@ __global__ void __launch_bounds__(kFeatThreads) image_features_kernel(const floa
           for (int q = 0; q < 9; ++q) acc = fmaf(wr[k][q], x[q], acc);
           o[k] = __float2bfloat16_rn(on_map ? fmaxf(acc + br[k], 0.f) : 0.f);
         }
-        const int chunk = (t % 2) * 4 + cg;
-        *reinterpret_cast<uint4*>(tA + (t / 2) * 128 * 128 + r * 128 + ((chunk ^ (r & 7)) << 4)) =
-            *reinterpret_cast<const uint4*>(o);
-      }
-      if (cg == 0) {
-        unsigned char* row = tA + 4 * 128 * 128 + r * 128;
-#pragma unroll
-        for (int chunk = 4; chunk < 8; ++chunk)
-          *reinterpret_cast<uint4*>(row + ((chunk ^ (r & 7)) << 4)) = make_uint4(0u, 0u, 0u, 0u);
+        const int chunk = chunk0 + cg;
+        *reinterpret_cast<uint4*>(tAk + r * 128 + ((chunk ^ (r & 7)) << 4)) = *reinterpret_cast<const uint4*>(o);
       }
     }
-  }
-  fence_proxy_async_shared();
-  tcgen05_before_sync();
-  __syncthreads();
-  tcgen05_after_sync();
-  const uint32_t tmem = s_tmem;
-  if (tid == 0) {
-    constexpr uint32_t idesc = bf16_idesc(128, 32);
-    for (int kb = 0; kb < kFeatKb; ++kb) {
-      const uint32_t a = smem_u32(tA + kb * 128 * 128), b = smem_u32(tB + kb * 32 * 128);
+    fence_proxy_async_shared();
+    tcgen05_before_sync();
+    __syncthreads();
+    tcgen05_after_sync();
+    if (tid == 0) {
+      constexpr uint32_t idesc = bf16_idesc(128, 32);
+      const uint32_t a = smem_u32(tAk), bb = smem_u32(tB + kb * 32 * 128);
 #pragma unroll
-      for (int k = 0; k < 4; ++k) umma_bf16(tmem, sw128_desc(a + 32 * k), sw128_desc(b + 32 * k), idesc, kb > 0 || k > 0);
+      for (int k = 0; k < 4; ++k) umma_bf16(tmem, sw128_desc(a + 32 * k), sw128_desc(bb + 32 * k), idesc, kb > 0 || k > 0);
+      umma_commit(&kbar[buf]);
     }
-    umma_commit(&done);
+    __syncwarp();
   }
-  __syncwarp();
-  const bool ready = mbar_wait(&done, 0, kCorrWaitCycles);
+  // K-block 4's commit (buffer 0, its third phase) covers every MMA issued before it
+  ready = mbar_wait(&kbar[0], 0u, kCorrWaitCycles) && ready;
   if (!ready && lane == 0) atomicOr(err, 8);
   tcgen05_after_sync();
   {
