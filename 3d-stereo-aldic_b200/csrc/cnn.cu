@@ -282,17 +282,18 @@ __device__ __forceinline__ bool corr_crops(const CorrSrc& s, long long t, const 
 // im2col rows.  The 8 x 8 reference feature crop (64 rows of 32 BF16 channels, written twice:
 // A rows p and 64 + p) and the 16 x 16 deformed crop (256 rows) are staged in shared memory in
 // the 128-byte-swizzled K-major layout (only the first 64 bytes of each 128-byte row, the 32
-// channels the two K = 16 steps read, are written); one thread issues two tcgen05.mma (M 128,
-// N 256) into 256 TMEM columns: D[p, q] = fR[p] . fD[q] for every reference / deformed
-// position pair.  Each warp w reads TMEM lanes 32 w .. (reference positions p = 8 ii + j,
-// rows 64.. repeating 0..63), 6 of the 12 deformed rows its lanes touch (tcgen05.ld, 16
-// columns each; warps w and w + 2 split them), and keeps, for its own row ii, the 9 offsets of
-// each deformed row within ii .. ii + 8 (columns j .. j + 8, picked by a 3-stage rotation by
-// j): the volume entries / 32, rounded to BF16, each written straight to the (at most 4)
-// places conv3's im2col rows use it, in a shared-memory copy of the sample's 16 rows x 736
-// columns (zero elsewhere).  All 128 threads then copy those rows out with 16-byte stores.
-// ok[t] = 0 (whole-image crops leaving the maps) gives a zero volume.  The MMA wait is bounded
-// (err bit 2 on time-out, the volume then undefined).
+// channels the two K = 16 steps read, are written).  In two passes (deformed rows 0..7, then
+// 8..15) one thread issues two tcgen05.mma (M 128, N 128) into 128 TMEM columns: D[p, q] =
+// fR[p] . fD[q] for the reference / deformed position pairs of the pass.  Each warp w reads
+// TMEM lanes 32 w .. (reference positions p = 8 ii + j, rows 64.. repeating 0..63) and takes,
+// with warp w + 2 or w - 2, the pass's deformed rows its lanes touch (tcgen05.ld, 16 columns
+// each); for its own row ii it keeps the 9 offsets of each deformed row within ii .. ii + 8
+// (columns j .. j + 8, picked by a 3-stage rotation by j): the volume entries / 32, rounded to
+// BF16, each written straight to the (at most 4) places conv3's im2col rows use it, in a
+// shared-memory copy of the sample's 16 rows x 736 columns (zero elsewhere).  All 128 threads
+// then copy those rows out with 16-byte stores.  128 TMEM columns and 73 KB of shared memory
+// let 3 CTAs share an SM.  ok[t] = 0 (whole-image crops leaving the maps) gives a zero volume.
+// The MMA waits are bounded (err bit 2 on time-out, the volume then undefined).
 constexpr int kCorrThreads = 128;
 constexpr int kCorrA = 128 * 128, kCorrB = 256 * 128;  // operand tiles (bytes)
 constexpr int kCorrRows = 16 * 736 * 2;                // conv3's im2col rows of the sample
@@ -348,43 +349,47 @@ __global__ void __launch_bounds__(kCorrThreads) corr_im2col_kernel(CorrSrc src, 
     mbar_init(&done, 1);
     fence_barrier_init();
   }
-  if (warp == 0) tmem_alloc(&s_tmem, 256);
+  if (warp == 0) tmem_alloc(&s_tmem, 128);
   fence_proxy_async_shared();  // the generic-proxy tile writes, visible to the tensor cores
   tcgen05_before_sync();
   __syncthreads();
   tcgen05_after_sync();
   const uint32_t tmem = s_tmem;
-  if (tid == 0) {
-    constexpr uint32_t idesc = bf16_idesc(128, 256);
-    const uint32_t a = smem_u32(tA), b = smem_u32(tB);
-    umma_bf16(tmem, sw128_desc(a), sw128_desc(b), idesc, false);
-    umma_bf16(tmem, sw128_desc(a + 32), sw128_desc(b + 32), idesc, true);
-    umma_commit(&done);
-  }
-  __syncwarp();
-  const bool ready = mbar_wait(&done, 0, kCorrWaitCycles);
-  if (!ready && lane == 0) atomicOr(err, 4);
-  tcgen05_after_sync();
-  {
-    // warp w reads TMEM lanes 32 (w % 4) ..: reference positions p = 32 (w % 2) + lane (rows
-    // 64.. repeat 0..63); warps w and w + 2 split the 12 deformed rows their lanes touch
-    const int p = (warp % 2) * 32 + lane, ii = p / 8, j = p % 8, ii0 = (warp % 2) * 4, half = warp / 2;
-    // the im2col places of volume position (ii, j): output (oy, ox) with 2 oy - 1 + ky = ii and
-    // 2 ox - 1 + kx = j, tap (ky, kx); at most 2 per axis
-    int base[4];
+  // warp w: reference positions p = 32 (w % 2) + lane (rows ii0 .. ii0 + 3), its half of the
+  // deformed rows it needs in each pass
+  const int p = (warp % 2) * 32 + lane, ii = p / 8, j = p % 8, ii0 = (warp % 2) * 4, half = warp / 2;
+  // the im2col places of volume position (ii, j): output (oy, ox) with 2 oy - 1 + ky = ii and
+  // 2 ox - 1 + kx = j, tap (ky, kx); at most 2 per axis
+  int base[4];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const int oy = ((ii + 1) >> 1) - (k >> 1), ox = ((j + 1) >> 1) - (k & 1);
-      const int ky = ii + 1 - 2 * oy, kx = j + 1 - 2 * ox;
-      base[k] = (oy >= 0 && oy < 4 && ox >= 0 && ox < 4 && ky >= 0 && ky <= 2 && kx >= 0 && kx <= 2)
-                    ? (oy * 4 + ox) * 736 + (ky * 3 + kx) * kDisp
-                    : -1;
-    }
+  for (int k = 0; k < 4; ++k) {
+    const int oy = ((ii + 1) >> 1) - (k >> 1), ox = ((j + 1) >> 1) - (k & 1);
+    const int ky = ii + 1 - 2 * oy, kx = j + 1 - 2 * ox;
+    base[k] = (oy >= 0 && oy < 4 && ox >= 0 && ox < 4 && ky >= 0 && ky <= 2 && kx >= 0 && kx <= 2)
+                  ? (oy * 4 + ox) * 736 + (ky * 3 + kx) * kDisp
+                  : -1;
+  }
+  bool ready = true;
 #pragma unroll 1
-    for (int rr = 6 * half; rr < 6 * half + 6; ++rr) {
+  for (int pass = 0; pass < 2; ++pass) {
+    if (tid == 0) {
+      constexpr uint32_t idesc = bf16_idesc(128, 128);
+      const uint32_t a = smem_u32(tA), b = smem_u32(tB + pass * 128 * 128);
+      umma_bf16(tmem, sw128_desc(a), sw128_desc(b), idesc, false);
+      umma_bf16(tmem, sw128_desc(a + 32), sw128_desc(b + 32), idesc, true);
+      umma_commit(&done);
+    }
+    __syncwarp();
+    ready = mbar_wait(&done, (uint32_t)pass, kCorrWaitCycles) && ready;
+    tcgen05_after_sync();
+    // deformed rows of this pass that rows ii0 .. ii0 + 3 touch, split between the two warps
+    const int lo = max(ii0, 8 * pass), hi = min(ii0 + 11, 8 * pass + 7);
+    const int mid = lo + (hi - lo + 2) / 2;
+#pragma unroll 1
+    for (int dr = half ? mid : lo; dr <= (half ? hi : mid - 1); ++dr) {
       float v[16];
-      tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)((ii0 + rr) * 16), v);
-      const int di = ii0 + rr - ii;  // deformed row ii0 + rr = ii + di
+      tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)((dr - 8 * pass) * 16), v);
+      const int di = dr - ii;  // deformed row dr = ii + di
       if (di < 0 || di > 8) continue;
       // rotate left by j (bits 4, 2, 1) so that v[0..8] = columns j .. j + 8
 #pragma unroll
@@ -401,10 +406,12 @@ __global__ void __launch_bounds__(kCorrThreads) corr_im2col_kernel(CorrSrc src, 
           if (base[k] >= 0) rows[base[k] + di * 9 + b] = x;
       }
     }
+    tcgen05_before_sync();
+    __syncthreads();
+    tcgen05_after_sync();
   }
-  tcgen05_before_sync();
-  __syncthreads();
-  if (warp == 0) tmem_free(tmem, 256);
+  if (!ready && lane == 0) atomicOr(err, 4);
+  if (warp == 0) tmem_free(tmem, 128);
   uint4* outA = reinterpret_cast<uint4*>(A3 + t * 16 * 736);
   for (int q = tid; q < kCorrRows / 16; q += kCorrThreads) outA[q] = reinterpret_cast<const uint4*>(rows)[q];
 }
