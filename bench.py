@@ -56,6 +56,8 @@ UNIT = "subsets/s"
 def workload_params(name):
     if name == "learned2048":  # learned vs FFT initial guess, held-out 2048 x 2048 smooth-field frames
         return dict(size=2048, w=32, step=16, search=16, tol=1e-3, roi=20, umax=12.0, gmax=0.05, frames=8)
+    if name == "learned1024":  # the same at 1024 x 1024 (profiling case)
+        return dict(size=1024, w=32, step=16, search=16, tol=1e-3, roi=20, umax=12.0, gmax=0.05, frames=8)
     if name == "quadtree2048":
         return dict(size=2048, w=32, step=16, s_temp=10, tol_temp=1e-3, mu=1e-3, admm=2, min_elem=4)
     if name == "stereo2048":
@@ -553,7 +555,8 @@ class LearnedBench:
         self.M, self.N = M, N
         self.gx, self.gy = [P["roi"] + 1, M - P["roi"]], [P["roi"] + 1, N - P["roi"]]
         di = device.index or 0
-        self.net = L.ProposalNet(di, max_batch=16384)
+        nodes = L.search_nodes(self.gx, self.gy, P["w"], P["step"])[0].shape[1]
+        self.net = L.ProposalNet(di, max_batch=min(16384, (nodes + 7) // 8 * 8))
         self.net.set_params(np.load(train_net.DEFAULT_WEIGHTS))
         self.ctx = A.Context(di)
         self.ctx.set_option(A.OPT_AUTOTUNE, 1)
@@ -860,7 +863,7 @@ def run_learned(args, P):
             "warmup": args.warmup, "ms_per_step": ms_l / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 (BF16 network, FP64 solve and re-decisions)",
             "data": "synthetic (seeded analytic speckle rendering; held-out frames, not in the training set)",
-            "config": {"workload": "learned2048", "subsets_per_frame": n, "frames_cycled": nF, **P,
+            "config": {"workload": args.workload, "subsets_per_frame": n, "frames_cycled": nF, **P,
                        "l2_flush": "each step a different frame; a step's working set (two 16 MiB FP32 images "
                                    "and gradients, 2 x 16 MiB feature maps, 356 MiB of conv3 input rows) "
                                    "exceeds the 126 MB L2"},
@@ -1110,7 +1113,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="learned2048",
-                    choices=["learned2048", "stereo2048", "stereo1024", "temporal512", "quadtree2048",
+                    choices=["learned2048", "learned1024", "stereo2048", "stereo1024", "temporal512", "quadtree2048",
                              "sequence4096"],
                     help="learned2048: learned vs FFT initial guess on held-out 2048 x 2048 frames (the "
                          "headline); stereo2048: the stereo + temporal + triangulation step; temporal512 and "
@@ -1133,7 +1136,7 @@ def main():
 
     if args.impl == "reference":
         if rank == 0:
-            if args.workload == "learned2048":
+            if args.workload in ("learned2048", "learned1024"):
                 run_reference_learned(args, P)
             elif args.workload in ("sequence4096", "temporal512", "quadtree2048"):
                 print(json.dumps({"impl": "reference", "unavailable": f"{args.workload} times the FP64 CPU oracle "
@@ -1142,7 +1145,7 @@ def main():
             else:
                 run_reference(args, P)
         return
-    if args.workload == "learned2048":
+    if args.workload in ("learned2048", "learned1024"):
         run_learned(args, P)
         return
     if args.workload == "sequence4096":
