@@ -546,7 +546,7 @@ class LearnedBench:
     Both on the same integer-search grid (ROI [roi+1, size-roi], winsize w, step), all work on
     one stream."""
 
-    def __init__(self, A, torch, P, device):
+    def __init__(self, A, torch, P, device, autotune=True):
         from aldic_b200 import learned as L
         from aldic_b200 import train_net
 
@@ -559,7 +559,7 @@ class LearnedBench:
         self.net = L.ProposalNet(di, max_batch=min(16384, (nodes + 7) // 8 * 8))
         self.net.set_params(np.load(train_net.DEFAULT_WEIGHTS))
         self.ctx = A.Context(di)
-        self.ctx.set_option(A.OPT_AUTOTUNE, 1)
+        self.ctx.set_option(A.OPT_AUTOTUNE, 1 if autotune else 0)
         self.li = L.LearnedInit(self.net, self.ctx, P["search"], self.gx, self.gy, P["w"], P["step"], P["tol"])
         self.stream = self.li.stream
         self.n, self.nx, self.ny = self.li.n, self.li.nx, self.li.ny
@@ -729,7 +729,7 @@ def run_learned(args, P):
     base = 50000 + 1000 * (args.seed + rank)
     pairs = learned_frames(P, [base + k for k in range(F)], dev)
     warm = learned_frames(P, [base + 900 + k for k in range(max(args.warmup, 3))], dev)
-    bench = LearnedBench(A, torch, P, dev)
+    bench = LearnedBench(A, torch, P, dev, autotune=not args.no_autotune)
     st = bench.stream
     for p in warm:  # warm-up: the autotuner's first calls, page-in
         bench.fft(p.ref, p.deff)
@@ -978,7 +978,7 @@ def run_stereo(args, P, emit=True):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     # weak scaling: every rank owns its own seeded frame set; no data-path collective
     scene = make_scene(args.workload, args.seed + rank)
-    pipe = StereoPipeline(A, torch, scene, P, dev)
+    pipe = StereoPipeline(A, torch, scene, P, dev, autotune=not args.no_autotune)
     stream = pipe.stream
     for _ in range(max(args.warmup, 3)):
         pipe.step()
@@ -1125,6 +1125,9 @@ def main():
     ap.add_argument("--cpu-per-pass", type=int, default=1200)
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-verify", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="the library's default configurations instead of the autotuner's (profiling runs: timings "
+                         "under a profiler would mislead the tuner)")
     ap.add_argument("--no-stereo", action="store_true",
                     help="learned2048: skip the stereo2048 step that the 1-GPU line carries as a sub-object")
     args = ap.parse_args()
