@@ -278,25 +278,27 @@ __device__ __forceinline__ bool corr_crops(const CorrSrc& s, long long t, const 
   return true;
 }
 
-// The correlation volume of sample t (blockIdx.x) on the tensor cores and, from it, conv3's
-// im2col rows.  The 8 x 8 reference feature crop (64 rows of 32 BF16 channels, written twice:
-// A rows p and 64 + p) and the 16 x 16 deformed crop (256 rows) are staged in shared memory in
-// the 128-byte-swizzled K-major layout (only the first 64 bytes of each 128-byte row, the 32
-// channels the two K = 16 steps read, are written).  In two passes (deformed rows 0..7, then
-// 8..15) one thread issues two tcgen05.mma (M 128, N 128) into 128 TMEM columns: D[p, q] =
-// fR[p] . fD[q] for the reference / deformed position pairs of the pass.  Each warp w reads
-// TMEM lanes 32 w .. (reference positions p = 8 ii + j, rows 64.. repeating 0..63) and takes,
-// with warp w + 2 or w - 2, the pass's deformed rows its lanes touch (tcgen05.ld, 16 columns
-// each); for its own row ii it keeps the 9 offsets of each deformed row within ii .. ii + 8
-// (columns j .. j + 8, picked by a 3-stage rotation by j): the volume entries / 32, rounded to
-// BF16, each written straight to the (at most 4) places conv3's im2col rows use it, in a
-// shared-memory copy of the sample's 16 rows x 736 columns (zero elsewhere).  All 128 threads
-// then copy those rows out with 16-byte stores.  128 TMEM columns and 73 KB of shared memory
-// let 3 CTAs share an SM.  ok[t] = 0 (whole-image crops leaving the maps) gives a zero volume.
-// The MMA waits are bounded (err bit 2 on time-out, the volume then undefined).
+// The correlation volumes of samples 0 .. nb - 1 on the tensor cores and, from them, conv3's
+// im2col rows; a persistent CTA takes samples blockIdx.x, + gridDim.x, ... and loads the next
+// sample's crops into registers while it works on the current one.  Per sample: the 8 x 8
+// reference feature crop (64 rows of 32 BF16 channels, written twice: A rows p and 64 + p) and
+// the 16 x 16 deformed crop (256 rows) are staged in shared memory in the 128-byte-swizzled
+// K-major layout (only the first 64 bytes of each 128-byte row, the 32 channels the two K = 16
+// steps read, are written).  In two passes (deformed rows 0..7, then 8..15) one thread issues
+// two tcgen05.mma (M 128, N 128) into 128 TMEM columns: D[p, q] = fR[p] . fD[q] for the
+// reference / deformed position pairs of the pass.  Each warp w reads TMEM lanes 32 w ..
+// (reference positions p = 8 ii + j, rows 64.. repeating 0..63) and takes, with warp w + 2 or
+// w - 2, the pass's deformed rows its lanes touch (tcgen05.ld, 16 columns each); for its own
+// row ii it keeps the 9 offsets of each deformed row within ii .. ii + 8 (columns j .. j + 8,
+// picked by a 3-stage rotation by j): the volume entries / 32, rounded to BF16, each written
+// straight to the (at most 4) places conv3's im2col rows use it, in a shared-memory copy of
+// the sample's 16 rows x 736 columns (zero elsewhere).  All 128 threads then copy those rows
+// out with 16-byte stores.  128 TMEM columns and 73 KB of shared memory let 3 CTAs share an
+// SM.  ok[t] = 0 (whole-image crops leaving the maps) gives a zero volume.  The MMA waits are
+// bounded (err bit 2 on time-out, the volumes then undefined).
 constexpr int kCorrThreads = 128;
 constexpr int kCorrA = 128 * 128, kCorrB = 256 * 128;  // operand tiles (bytes)
-constexpr int kCorrRows = 16 * 736 * 2;                // conv3's im2col rows of the sample
+constexpr int kCorrRows = 16 * 736 * 2;                // conv3's im2col rows of a sample
 constexpr int kCorrSmem = 1024 + kCorrA + kCorrB + kCorrRows;  // + alignment slack
 constexpr long long kCorrWaitCycles = 2000000000LL;
 
@@ -304,7 +306,22 @@ __device__ __forceinline__ void put_chunk(unsigned char* tile, int row, int chun
   *reinterpret_cast<uint4*>(tile + row * 128 + ((chunk ^ (row & 7)) << 4)) = v;
 }
 
-__global__ void __launch_bounds__(kCorrThreads) corr_im2col_kernel(CorrSrc src, bf16* __restrict__ A3,
+// this thread's 10 chunks of sample t's crops (A: chunks 0..255, B: 256..1279), zero outside
+__device__ __forceinline__ bool corr_fetch(const CorrSrc& src, long long t, int tid, uint4 (&v)[10]) {
+  const bf16 *r, *d;
+  long long rrow, drow;
+  const bool inside = corr_crops(src, t, r, rrow, d, drow);
+  const uint4 zero = make_uint4(0u, 0u, 0u, 0u);
+#pragma unroll
+  for (int i = 0; i < 10; ++i) {
+    const int q = tid + i * kCorrThreads, row = i < 2 ? q / 4 : (q - 256) / 4, ch = q % 4;
+    const bf16* src_row = i < 2 ? r + (row / 8) * rrow + (row % 8) * 32 : d + (row / 16) * drow + (row % 16) * 32;
+    v[i] = inside ? *reinterpret_cast<const uint4*>(src_row + ch * 8) : zero;
+  }
+  return inside;
+}
+
+__global__ void __launch_bounds__(kCorrThreads) corr_im2col_kernel(CorrSrc src, int nb, bf16* __restrict__ A3,
                                                                    uint8_t* __restrict__ ok, int* __restrict__ err) {
   extern __shared__ unsigned char corr_raw[];
   __shared__ __align__(8) uint64_t done;
@@ -314,43 +331,12 @@ __global__ void __launch_bounds__(kCorrThreads) corr_im2col_kernel(CorrSrc src, 
   unsigned char* tA = smem;
   unsigned char* tB = smem + kCorrA;
   bf16* rows = reinterpret_cast<bf16*>(smem + kCorrA + kCorrB);
-  const long long t = blockIdx.x;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const bf16 *r, *d;
-  long long rrow, drow;
-  const bool inside = corr_crops(src, t, r, rrow, d, drow);
-  if (ok && tid == 0) ok[t] = inside ? 1 : 0;
-  const uint4 zero = make_uint4(0u, 0u, 0u, 0u);
-  // A: reference rows 0..63 (crop row ii = p / 8, column j = p % 8); B: deformed rows
-  // q = 16 dr + dc; 4 chunks of 16 bytes per row, 256 + 1024 chunks: each thread issues its
-  // 10 loads before storing any (their latencies overlapped)
-  {
-    uint4 v[10];
-#pragma unroll
-    for (int i = 0; i < 10; ++i) {
-      const int q = tid + i * kCorrThreads, row = i < 2 ? q / 4 : (q - 256) / 4, ch = q % 4;
-      const bf16* src_row = i < 2 ? r + (row / 8) * rrow + (row % 8) * 32 : d + (row / 16) * drow + (row % 16) * 32;
-      v[i] = inside ? *reinterpret_cast<const uint4*>(src_row + ch * 8) : zero;
-    }
-#pragma unroll
-    for (int i = 0; i < 10; ++i) {
-      const int q = tid + i * kCorrThreads;
-      if (i < 2) {  // A rows p and p + 64 (a copy: TMEM lanes 64..127 for warps 2 and 3)
-        put_chunk(tA, q / 4, q % 4, v[i]);
-        put_chunk(tA, 64 + q / 4, q % 4, v[i]);
-      } else {
-        put_chunk(tB, (q - 256) / 4, q % 4, v[i]);
-      }
-    }
-  }
-  // the im2col rows start at zero (padding taps and the 7 padding columns)
-  for (int q = tid; q < kCorrRows / 16; q += kCorrThreads) reinterpret_cast<uint4*>(rows)[q] = zero;
   if (tid == 0) {
     mbar_init(&done, 1);
     fence_barrier_init();
   }
   if (warp == 0) tmem_alloc(&s_tmem, 128);
-  fence_proxy_async_shared();  // the generic-proxy tile writes, visible to the tensor cores
   tcgen05_before_sync();
   __syncthreads();
   tcgen05_after_sync();
@@ -370,50 +356,80 @@ __global__ void __launch_bounds__(kCorrThreads) corr_im2col_kernel(CorrSrc src, 
                   : -1;
   }
   bool ready = true;
+  uint4 v[10];
+  long long t = blockIdx.x;
+  bool inside = t < nb ? corr_fetch(src, t, tid, v) : false;
 #pragma unroll 1
-  for (int pass = 0; pass < 2; ++pass) {
-    if (tid == 0) {
-      constexpr uint32_t idesc = bf16_idesc(128, 128);
-      const uint32_t a = smem_u32(tA), b = smem_u32(tB + pass * 128 * 128);
-      umma_bf16(tmem, sw128_desc(a), sw128_desc(b), idesc, false);
-      umma_bf16(tmem, sw128_desc(a + 32), sw128_desc(b + 32), idesc, true);
-      umma_commit(&done);
-    }
-    __syncwarp();
-    ready = mbar_wait(&done, (uint32_t)pass, kCorrWaitCycles) && ready;
-    tcgen05_after_sync();
-    // deformed rows of this pass that rows ii0 .. ii0 + 3 touch, split between the two warps
-    const int lo = max(ii0, 8 * pass), hi = min(ii0 + 11, 8 * pass + 7);
-    const int mid = lo + (hi - lo + 2) / 2;
-#pragma unroll 1
-    for (int dr = half ? mid : lo; dr <= (half ? hi : mid - 1); ++dr) {
-      float v[16];
-      tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)((dr - 8 * pass) * 16), v);
-      const int di = dr - ii;  // deformed row dr = ii + di
-      if (di < 0 || di > 8) continue;
-      // rotate left by j (bits 4, 2, 1) so that v[0..8] = columns j .. j + 8
+  for (; t < nb; t += gridDim.x) {
+    // this sample's crops into the tiles (free: the previous sample's MMAs are complete), its
+    // im2col rows from zero (free: the previous copy-out finished before the loop's barrier)
 #pragma unroll
-      for (int k = 0; k < 12; ++k) v[k] = (j & 4) ? v[k + 4] : v[k];
-#pragma unroll
-      for (int k = 0; k < 10; ++k) v[k] = (j & 2) ? v[k + 2] : v[k];
-#pragma unroll
-      for (int k = 0; k < 9; ++k) v[k] = (j & 1) ? v[k + 1] : v[k];
-#pragma unroll
-      for (int b = 0; b < 9; ++b) {
-        const bf16 x = __float2bfloat16_rn(inside ? v[b] * (1.f / 32.f) : 0.f);
-#pragma unroll
-        for (int k = 0; k < 4; ++k)
-          if (base[k] >= 0) rows[base[k] + di * 9 + b] = x;
+    for (int i = 0; i < 10; ++i) {
+      const int q = tid + i * kCorrThreads;
+      if (i < 2) {  // A rows p and p + 64 (a copy: TMEM lanes 64..127 for warps 2 and 3)
+        put_chunk(tA, q / 4, q % 4, v[i]);
+        put_chunk(tA, 64 + q / 4, q % 4, v[i]);
+      } else {
+        put_chunk(tB, (q - 256) / 4, q % 4, v[i]);
       }
     }
+    for (int q = tid; q < kCorrRows / 16; q += kCorrThreads)
+      reinterpret_cast<uint4*>(rows)[q] = make_uint4(0u, 0u, 0u, 0u);
+    if (ok && tid == 0) ok[t] = inside ? 1 : 0;
+    const bool cur = inside;
+    if (t + gridDim.x < nb) inside = corr_fetch(src, t + gridDim.x, tid, v);  // in flight meanwhile
+    fence_proxy_async_shared();  // the generic-proxy tile writes, visible to the tensor cores
     tcgen05_before_sync();
     __syncthreads();
     tcgen05_after_sync();
+#pragma unroll 1
+    for (int pass = 0; pass < 2; ++pass) {
+      if (tid == 0) {
+        constexpr uint32_t idesc = bf16_idesc(128, 128);
+        const uint32_t a = smem_u32(tA), b = smem_u32(tB + pass * 128 * 128);
+        umma_bf16(tmem, sw128_desc(a), sw128_desc(b), idesc, false);
+        umma_bf16(tmem, sw128_desc(a + 32), sw128_desc(b + 32), idesc, true);
+        umma_commit(&done);
+      }
+      __syncwarp();
+      ready = mbar_wait(&done, (uint32_t)pass, kCorrWaitCycles) && ready;  // two phases per sample
+      tcgen05_after_sync();
+      // deformed rows of this pass that rows ii0 .. ii0 + 3 touch, split between the two warps
+      const int lo = max(ii0, 8 * pass), hi = min(ii0 + 11, 8 * pass + 7);
+      const int mid = lo + (hi - lo + 2) / 2;
+#pragma unroll 1
+      for (int dr = half ? mid : lo; dr <= (half ? hi : mid - 1); ++dr) {
+        float w[16];
+        tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)((dr - 8 * pass) * 16), w);
+        const int di = dr - ii;  // deformed row dr = ii + di
+        if (di < 0 || di > 8) continue;
+        // rotate left by j (bits 4, 2, 1) so that w[0..8] = columns j .. j + 8
+#pragma unroll
+        for (int k = 0; k < 12; ++k) w[k] = (j & 4) ? w[k + 4] : w[k];
+#pragma unroll
+        for (int k = 0; k < 10; ++k) w[k] = (j & 2) ? w[k + 2] : w[k];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) w[k] = (j & 1) ? w[k + 1] : w[k];
+#pragma unroll
+        for (int b = 0; b < 9; ++b) {
+          const bf16 x = __float2bfloat16_rn(cur ? w[b] * (1.f / 32.f) : 0.f);
+#pragma unroll
+          for (int k = 0; k < 4; ++k)
+            if (base[k] >= 0) rows[base[k] + di * 9 + b] = x;
+        }
+      }
+      tcgen05_before_sync();
+      __syncthreads();
+      tcgen05_after_sync();
+    }
+    uint4* outA = reinterpret_cast<uint4*>(A3 + t * 16 * 736);
+    for (int q = tid; q < kCorrRows / 16; q += kCorrThreads) outA[q] = reinterpret_cast<const uint4*>(rows)[q];
+    __syncthreads();  // the rows are read before the next sample zeroes them
   }
   if (!ready && lane == 0) atomicOr(err, 4);
+  tcgen05_before_sync();
+  __syncthreads();
   if (warp == 0) tmem_free(tmem, 128);
-  uint4* outA = reinterpret_cast<uint4*>(A3 + t * 16 * 736);
-  for (int q = tid; q < kCorrRows / 16; q += kCorrThreads) outA[q] = reinterpret_cast<const uint4*>(rows)[q];
 }
 
 // conv1 and conv2 over one whole frame image in a single pass (prediction): CTA (bx, i2)
@@ -908,9 +924,13 @@ void conv1(ProposalNet* net, const bf16* in, View v, const ConvI& L, long long P
 
 int corr_im2col(ProposalNet* net, const CorrSrc& src, int nb) {
   cudaFuncSetAttribute(corr_im2col_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kCorrSmem);
-  corr_im2col_kernel<<<(unsigned)nb, kCorrThreads, kCorrSmem, net->stream>>>(src, net->A[kConv3],
-                                                                             src.coords ? net->ok : nullptr,
-                                                                             net->errflag);
+  int dev = 0, sms = 148, per_sm = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, corr_im2col_kernel, kCorrThreads, kCorrSmem);
+  const int grid = std::max(1, std::min(nb, sms * std::max(per_sm, 1)));
+  corr_im2col_kernel<<<(unsigned)grid, kCorrThreads, kCorrSmem, net->stream>>>(
+      src, nb, net->A[kConv3], src.coords ? net->ok : nullptr, net->errflag);
   ++net->launches;
   return ALDIC_OK;
 }
