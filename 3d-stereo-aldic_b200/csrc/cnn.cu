@@ -924,11 +924,14 @@ void conv1(ProposalNet* net, const bf16* in, View v, const ConvI& L, long long P
 
 int corr_im2col(ProposalNet* net, const CorrSrc& src, int nb) {
   cudaFuncSetAttribute(corr_im2col_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kCorrSmem);
-  int dev = 0, sms = 148, per_sm = 1;
+  cudaFuncSetAttribute(corr_im2col_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+  int dev = 0, sms = 148, smem_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, corr_im2col_kernel, kCorrThreads, kCorrSmem);
-  const int grid = std::max(1, std::min(nb, sms * std::max(per_sm, 1)));
+  cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+  // CTAs per SM by shared memory (1 KB reserved per CTA); TMEM (128 of 512 columns) allows 4
+  const int per_sm = std::max(1, std::min(4, smem_sm / (kCorrSmem + 1024 + 64)));
+  const int grid = std::max(1, std::min(nb, sms * per_sm));
   corr_im2col_kernel<<<(unsigned)grid, kCorrThreads, kCorrSmem, net->stream>>>(
       src, nb, net->A[kConv3], src.coords ? net->ok : nullptr, net->errflag);
   ++net->launches;
