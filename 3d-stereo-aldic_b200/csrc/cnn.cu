@@ -292,9 +292,9 @@ __device__ __forceinline__ bool corr_crops(const CorrSrc& s, long long t, const 
 // row ii it keeps the 9 offsets of each deformed row within ii .. ii + 8 (columns j .. j + 8,
 // picked by a 3-stage rotation by j): the volume entries / 32, rounded to BF16, each written
 // straight to the (at most 4) places conv3's im2col rows use it, in a shared-memory copy of
-// the sample's 16 rows x 736 columns (zero elsewhere).  All 128 threads then copy those rows
-// out with 16-byte stores.  128 TMEM columns and 73 KB of shared memory let 3 CTAs share an
-// SM.  ok[t] = 0 (whole-image crops leaving the maps) gives a zero volume.  The MMA waits are
+// the sample's 16 rows x 736 columns (zeroed once: the other places are the same for every
+// sample).  All 128 threads then copy those rows out with 16-byte stores.  128 TMEM columns
+// and 73 KB of shared memory let 3 CTAs share an SM.  ok[t] = 0 (whole-image crops leaving the maps) gives a zero volume.  The MMA waits are
 // bounded (err bit 2 on time-out, the volumes then undefined).
 constexpr int kCorrThreads = 128;
 constexpr int kCorrA = 128 * 128, kCorrB = 256 * 128;  // operand tiles (bytes)
@@ -355,14 +355,18 @@ __global__ void __launch_bounds__(kCorrThreads) corr_im2col_kernel(CorrSrc src, 
                   ? (oy * 4 + ox) * 736 + (ky * 3 + kx) * kDisp
                   : -1;
   }
+  // the im2col rows start at zero (padding taps and the 7 padding columns); every sample
+  // rewrites the same (valid) places, so the zeros stay
+  for (int q = tid; q < kCorrRows / 16; q += kCorrThreads)
+    reinterpret_cast<uint4*>(rows)[q] = make_uint4(0u, 0u, 0u, 0u);
   bool ready = true;
   uint4 v[10];
   long long t = blockIdx.x;
   bool inside = t < nb ? corr_fetch(src, t, tid, v) : false;
 #pragma unroll 1
   for (; t < nb; t += gridDim.x) {
-    // this sample's crops into the tiles (free: the previous sample's MMAs are complete), its
-    // im2col rows from zero (free: the previous copy-out finished before the loop's barrier)
+    // this sample's crops into the tiles (free: the previous sample's MMAs are complete; its
+    // im2col rows are free too: the previous copy-out finished before the loop's barrier)
 #pragma unroll
     for (int i = 0; i < 10; ++i) {
       const int q = tid + i * kCorrThreads;
@@ -373,8 +377,6 @@ __global__ void __launch_bounds__(kCorrThreads) corr_im2col_kernel(CorrSrc src, 
         put_chunk(tB, (q - 256) / 4, q % 4, v[i]);
       }
     }
-    for (int q = tid; q < kCorrRows / 16; q += kCorrThreads)
-      reinterpret_cast<uint4*>(rows)[q] = make_uint4(0u, 0u, 0u, 0u);
     if (ok && tid == 0) ok[t] = inside ? 1 : 0;
     const bool cur = inside;
     if (t + gridDim.x < nb) inside = corr_fetch(src, t + gridDim.x, tid, v);  // in flight meanwhile
