@@ -85,7 +85,7 @@ SIGNATURES = {
     "aldic_net_status": (_i, [_vp]),
     "aldic_net_predict": (_i, [_vp, _vp, _i64, _vp, _vp, _vp]),
     "aldic_net_extract": (_i, [_vp, _i64, _vp, _vp]),
-    "aldic_local_icgn_guess": (_i, [_vp, _i, _i64, _vp, _vp, _vp, _i, _d, _vp, _vp, _vp, _vp, _vp]),
+    "aldic_local_icgn_guess": (_i, [_vp, _i, _i64, _vp, _vp, _vp, _i, _d, _vp, _vp, _vp, _vp, _vp, _vp]),
     "aldic_subset_zncc": (_i, [_vp, _i64, _vp, _vp, _vp, _i, _vp]),
     "aldic_fallback_select": (_i, [_vp, _i64, _vp, _vp, _d, _vp, _vp]),
     "aldic_integer_search_list": (_i, [_vp, _vp, _vp, _vp, _i, _i, _i64, _vp, _vp, _vp, _vp, _vp, _vp]),

@@ -278,23 +278,32 @@ class Context:
             return out
         return {nm: bufs[nm][0].reshape((ny, nx), order="F") for nm in ("x", "y", "u", "v", "phi")}
 
-    def local_icgn(self, variant, coords, U0, winsize, tol, want_H=True, want_mark=True, out=None, F0=None):
+    def local_icgn(self, variant, coords, U0, winsize, tol, want_H=True, want_mark=True, out=None, F0=None,
+                   want_zncc=False):
         """LocalICGN / LocalICGNQuadtree loop body; F0 (4n) starts IC-GN from [F0 U0] (the
-        learned initial guess) instead of the reference's [0 U0]."""
+        learned initial guess) instead of the reference's [0 U0].  want_zncc (with F0) also
+        returns each subset's ZNCC under its final warp, from IC-GN's last iteration (`zncc`; with `out`, into out["zncc"])."""
         k = _Keep()
         n = _count(coords, 2)
+        if want_zncc and F0 is None:
+            raise ValueError("want_zncc needs F0 (the learned-guess entry point)")
+        zncc, zp = None, None
         if out is None:
             U, up = k.out(2 * n, np.float64)
             F, fp = k.out(4 * n, np.float64)
             H, hp = k.out(21 * n, np.float64) if want_H else (None, None)
             conv, cp = k.out(n, np.int32)
             mark, mp = k.out(n, np.uint8) if (want_mark and variant == _lib.QUADTREE) else (None, None)
+            if want_zncc:
+                zncc, zp = k.out(n, np.float64)
         else:
             up = k.dst(out["U"], np.float64, 2 * n)
             fp = k.dst(out["F"], np.float64, 4 * n)
             hp = k.dst(out.get("H"), np.float64, 21 * n)
             cp = k.dst(out["conv"], np.int32, n)
             mp = k.dst(out.get("mark"), np.uint8, n)
+            if want_zncc:
+                zp = k.dst(out["zncc"], np.float64, n)
         if F0 is None:
             rc = self.lib.aldic_local_icgn(self.h, int(variant), n, k.ptr(coords, np.float64, numel=2 * n),
                                            k.ptr(U0, np.float64, "C", numel=2 * n), int(winsize), float(tol), up, fp,
@@ -303,11 +312,12 @@ class Context:
             rc = self.lib.aldic_local_icgn_guess(self.h, int(variant), n, k.ptr(coords, np.float64, numel=2 * n),
                                                  k.ptr(U0, np.float64, "C", numel=2 * n),
                                                  k.ptr(F0, np.float64, "C", numel=4 * n), int(winsize), float(tol), up,
-                                                 fp, hp, cp, mp)
+                                                 fp, hp, cp, mp, zp)
         self._check(rc, "aldic_local_icgn")
         if out is not None:
             return out
-        return dict(U=U, F=F, H=None if H is None else H.reshape((n, 21), order="F"), conv=conv, markHole=mark)
+        return dict(U=U, F=F, H=None if H is None else H.reshape((n, 21), order="F"), conv=conv, markHole=mark,
+                    zncc=zncc)
 
     def subset_zncc(self, coords, U, F, winsize, out=None):
         """ZNCC of each subset's window under the warp [F U] (NaN where it leaves the image)."""

@@ -293,10 +293,10 @@ class LearnedInit:
         T, ctx, b, n = self.T, self.ctx, self.buf, self.n
         with T.cuda.stream(self.stream):
             self._timed(self.predict_events, lambda: self.net.predict(ctx, self.coords, b))
+            # IC-GN from [F0 U0]; its last iteration's sums give each subset's ZNCC
             self._timed(self.icgn_events,
                         lambda: ctx.local_icgn(self.variant, self.coords, b["U0"], self.w, self.tol, want_H=False,
-                                               want_mark=False, out=b, F0=b["F0"]))
-            ctx.subset_zncc(self.coords, b["U"], b["F"], self.w, out=b["zncc"])
+                                               want_mark=False, out=b, F0=b["F0"], want_zncc=True))
             nf = ctx.fallback_select(b["conv"], b["zncc"], self.zncc_min, self.flist)  # the host's one wait
             b["fallback"].zero_()
             if nf:

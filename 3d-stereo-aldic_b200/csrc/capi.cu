@@ -708,7 +708,7 @@ static int tune_search(aldic_ctx* c, SearchArgs& a) {
 
 static int icgn_common(aldic_ctx* c, int variant, int64_t n, const double* coords, const double* U0, int winsize,
                        double tol, double* U, double* F, double* H, int32_t* conv, uint8_t* mark, double* znssd,
-                       const double* F0 = nullptr) {
+                       const double* F0 = nullptr, double* zncc = nullptr) {
   int rc = need_frame(c, true);
   if (rc) return rc;
   if (n < 0) return fail(c, ALDIC_ERR_ARG, "n < 0");
@@ -738,12 +738,15 @@ static int icgn_common(aldic_ctx* c, int variant, int64_t n, const double* coord
   Arg am{mark, mark ? (size_t)n : 0, true, nullptr};
   Arg az{znssd, znssd ? (size_t)n * 8 : 0, true, nullptr};
   Arg af0{F0, F0 ? (size_t)n * 4 * 8 : 0, false, nullptr};
+  Arg azc{zncc, zncc ? (size_t)n * 8 : 0, true, nullptr};
   // the work queue comes from the arena too: reserve room for it with the staged arguments
   c->arena.used = 0;
-  rc = arena_reserve(c, qbytes + 4096 + (size_t)n * (2 + 2 + 2 + 4 + 4 + 21 + 1 + 1 + 8) * 8 + 8192);
+  rc = arena_reserve(c, qbytes + 4096 + (size_t)n * (2 + 2 + 2 + 4 + 4 + 21 + 1 + 1 + 1 + 8) * 8 + 8192);
   if (rc) return rc;
-  rc = stage(c, {&ac, &au0, &au, &af, &ah, &acv, &am, &az, &af0});
+  rc = stage(c, {&ac, &au0, &au, &af, &ah, &acv, &am, &az, &af0, &azc});
   if (rc) return rc;
+  // subsets that no pass solves (their window leaves the image) keep a NaN ZNCC (all-ones bits)
+  if (zncc) CK(cudaMemsetAsync(azc.dev, 0xFF, (size_t)n * 8, c->stream));
   IcgnArgs a;
   a.fr = frame_of(c);
   a.variant = variant;
@@ -772,6 +775,7 @@ static int icgn_common(aldic_ctx* c, int variant, int64_t n, const double* coord
   a.slow_nw = c->slow_nw;
   a.slow_fp64 = c->slow_fp64;
   a.fp64_threads = c->fp64_threads;
+  a.zncc = (double*)azc.dev;
   if (c->autotune && !epi) {
     rc = tune_icgn(c, a, wmax);
     if (rc) return rc;
@@ -789,12 +793,12 @@ int aldic_local_icgn(aldic_ctx* c, int variant, int64_t n, const double* coords,
 
 int aldic_local_icgn_guess(aldic_ctx* c, int variant, int64_t n, const double* coords, const double* U0,
                            const double* F0, int winsize, double tol, double* U, double* F, double* H, int32_t* conv,
-                           uint8_t* markHole) {
+                           uint8_t* markHole, double* zncc) {
   if (!c) return ALDIC_ERR_ARG;
   if (variant != ALDIC_UNIFORM && variant != ALDIC_QUADTREE) return fail(c, ALDIC_ERR_ARG, "bad variant %d", variant);
   if (!F0) return fail(c, ALDIC_ERR_ARG, "F0 required (aldic_local_icgn starts from F = 0)");
   return icgn_common(c, variant, n, coords, U0, winsize, tol, U, F, H, conv,
-                     variant == ALDIC_QUADTREE ? markHole : nullptr, nullptr, F0);
+                     variant == ALDIC_QUADTREE ? markHole : nullptr, nullptr, F0, zncc);
 }
 
 int aldic_subset_zncc(aldic_ctx* c, int64_t n, const double* coords, const double* U, const double* F, int winsize,

@@ -3,15 +3,23 @@
 // contiguous BF16), the product the network's convolutions (implicit GEMM over im2col rows),
 // their data and weight gradients and its fully connected layers all reduce to.
 //
-// One CTA of 128 threads per (128-row, BN-column) tile and K range (split-K over grid.z):
-//   * one thread issues the TMA tile loads (A: 64 K x 128 rows, B: 64 K x BN rows, 128-byte
-//     swizzle, out-of-range rows and K read as zero) into a 4-stage ring and the tcgen05.mma
-//     instructions (M 128, N BN, K 16 each) into an FP32 accumulator of BN TMEM columns;
-//     tcgen05.commit on a per-stage mbarrier frees a stage for the next load;
-//   * the 4 warps then read their 32 accumulator rows back (tcgen05.ld 32x32b) and apply the
-//     epilogue: store (+ bias), atomic add (split-K), or bias + ReLU to BF16 (16-byte vector
-//     stores for whole 16-column runs at 16-byte aligned addresses).
-// Every wait is bounded; a time-out sets *err, stops issuing, drains and frees TMEM.
+// Persistent and warp-specialised: each CTA (192 threads) walks the output tiles
+// (128 rows x BN columns x one K range of the split-K division) t = blockIdx.x,
+// blockIdx.x + gridDim.x, ...; the N tiles of one row block are consecutive, so CTAs running
+// side by side share A tiles in L2.
+//   * warp 0 (one lane) issues the TMA loads (A: 64 K x 128 rows, B: 64 K x BN rows, 128-byte
+//     swizzle, out-of-range rows and K read as zero) into a 4-stage ring, across tile
+//     boundaries, each stage's refill gated by the tcgen05.commit of the MMAs that read it;
+//   * warp 1 (one lane) issues the tcgen05.mma instructions (M 128, N BN, K 16 each) into one
+//     of two FP32 TMEM accumulators of BN columns, alternating per tile, and commits each
+//     finished accumulator;
+//   * warps 2-5 read a finished accumulator back (tcgen05.ld 32x32b; warp w reads TMEM lanes
+//     32 (w mod 4) ..) while the next tile's MMAs fill the other one, release it, and apply
+//     the epilogue: store (+ bias), atomic add (split-K), or bias + ReLU to BF16 (16-byte
+//     vector stores for whole 16-column runs at 16-byte aligned addresses).
+// Every wait is bounded; a time-out sets *err and ends that role's loop (the others then
+// time out too), the producer waits for its loads in flight and the MMA warp for its MMAs
+// before the CTA frees TMEM and exits.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -26,7 +34,8 @@ namespace aldic {
 namespace {
 
 constexpr int kStages = 4;
-constexpr int kBK = 64;  // K per stage: one 128-byte swizzle row of BF16
+constexpr int kBK = 64;             // K per stage: one 128-byte swizzle row of BF16
+constexpr int kGemmThreads = 192;   // producer warp, MMA warp, 4 epilogue warps
 constexpr long long kGemmWaitCycles = 4000000000LL;
 
 template <int BN>
@@ -35,156 +44,208 @@ struct GemmSmem {
   static constexpr int b_bytes = BN * kBK * 2;
   static constexpr int stage_bytes = a_bytes + b_bytes;
   static constexpr int bytes = kStages * stage_bytes + 1024;  // + 1024 for the alignment
+  static constexpr uint32_t acc_cols = BN < 32 ? 32 : BN;     // TMEM columns of one accumulator
+  static constexpr int per_sm = (227 * 1024) / bytes < 4 ? (227 * 1024) / bytes : 4;
+};
+
+struct TileGrid {
+  int tiles_m, tiles_n, ntiles, kb_per_split, kb_total;
+  // tile t -> first row, first column and K-block range [kb0, kb1)
+  __device__ __forceinline__ void decode(int t, int& m0, int& n0, int& kb0, int& kb1) const {
+    const int nt = t % tiles_n, r = t / tiles_n, mt = r % tiles_m, sp = r / tiles_m;
+    m0 = mt * 128;
+    n0 = nt;  // scaled by BN by the caller
+    kb0 = sp * kb_per_split;
+    kb1 = min(kb_total, kb0 + kb_per_split);
+  }
 };
 
 template <int BN>
-__global__ void __launch_bounds__(128, 1)
+__device__ __forceinline__ void gemm_epilogue_tile(const GemmEpi& epi, uint32_t tacc, int row, int n0, int M, int N) {
+#pragma unroll 1
+  for (int c = 0; c < BN; c += 16) {
+    float v[16];
+    __syncwarp();  // tcgen05.ld is warp-collective: reconverge after the previous run's stores
+    tmem_ld16(tacc + (uint32_t)c, v);
+    const int col0 = n0 + c;
+    if (row < M && col0 + 16 <= N && epi.mode != kEpiAtomic) {  // 16 whole columns: vector stores
+      const size_t o = (size_t)row * epi.ldc + col0;
+      if (epi.mode == kEpiBiasReluBf16 && ((reinterpret_cast<uintptr_t>(epi.c16 + o) & 15) == 0)) {
+        __align__(16) __nv_bfloat16 h[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const float x = v[j] + (epi.bias ? epi.bias[col0 + j] : 0.f);
+          h[j] = __float2bfloat16_rn(x > 0.f ? x : 0.f);
+        }
+        uint4* dst = reinterpret_cast<uint4*>(epi.c16 + o);
+        dst[0] = reinterpret_cast<const uint4*>(h)[0];
+        dst[1] = reinterpret_cast<const uint4*>(h)[1];
+        continue;
+      }
+      if (epi.mode == kEpiStore && ((reinterpret_cast<uintptr_t>(epi.c32 + o) & 15) == 0)) {
+        float4* dst = reinterpret_cast<float4*>(epi.c32 + o);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          float4 q = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+          if (epi.bias) {
+            q.x += epi.bias[col0 + 4 * j];
+            q.y += epi.bias[col0 + 4 * j + 1];
+            q.z += epi.bias[col0 + 4 * j + 2];
+            q.w += epi.bias[col0 + 4 * j + 3];
+          }
+          dst[j] = q;
+        }
+        continue;
+      }
+    }
+    if (row < M) {
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const int col = n0 + c + j;
+        if (col >= N) continue;
+        float x = v[j];
+        const size_t o = (size_t)row * epi.ldc + col;
+        switch (epi.mode) {
+          case kEpiStore:
+            if (epi.bias) x += epi.bias[col];
+            epi.c32[o] = x;
+            break;
+          case kEpiAtomic:
+            atomicAdd(epi.c32 + o, x);
+            break;
+          case kEpiBiasReluBf16:
+            x += epi.bias ? epi.bias[col] : 0.f;
+            epi.c16[o] = __float2bfloat16_rn(x > 0.f ? x : 0.f);
+            break;
+          default:
+            break;
+        }
+      }
+    }
+  }
+}
+
+template <int BN>
+__global__ void __launch_bounds__(kGemmThreads, 1)
     umma_gemm_kernel(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb, GemmEpi epi,
-                     int M, int N, int kb_per_split, int kb_total) {
+                     int M, int N, TileGrid tg) {
   static_assert(BN % 16 == 0 && BN >= 16 && BN <= 256, "UMMA N");
-  constexpr uint32_t kCols = BN < 32 ? 32 : BN;  // TMEM columns (a power of two, >= 32)
+  constexpr uint32_t kCols = GemmSmem<BN>::acc_cols;
+  constexpr uint32_t kAlloc = 2 * kCols;  // two accumulators (a power of two, <= 512)
   constexpr uint32_t kIdesc = bf16_idesc(128, BN);
   extern __shared__ __align__(1024) unsigned char smem_raw[];
-  __shared__ __align__(8) uint64_t full[kStages], empty[kStages], done;
+  __shared__ __align__(8) uint64_t full[kStages], empty[kStages], acc_full[2], acc_empty[2], drain;
   __shared__ uint32_t s_tmem;
-  __shared__ int s_fail;
   unsigned char* smem =
       reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int m0 = blockIdx.x * 128, n0 = blockIdx.y * BN;
-  const int kb0 = blockIdx.z * kb_per_split;
-  const int kb1 = min(kb_total, kb0 + kb_per_split);
-  const int nkb = kb1 - kb0;
   if (tid == 0) {
     for (int s = 0; s < kStages; ++s) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
-    mbar_init(&done, 1);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&acc_full[b], 1);
+      mbar_init(&acc_empty[b], 4);  // one arrival per epilogue warp
+    }
+    mbar_init(&drain, 1);
     fence_barrier_init();
-    s_fail = 0;
   }
-  if (warp == 0) tmem_alloc(&s_tmem, kCols);
+  if (warp == 1) tmem_alloc(&s_tmem, kAlloc);
   tcgen05_before_sync();
   __syncthreads();
   tcgen05_after_sync();
   const uint32_t tmem = s_tmem;
-  if (tid == 0 && nkb > 0) {
-    auto a_at = [&](int s) { return smem + s * GemmSmem<BN>::stage_bytes; };
-    auto b_at = [&](int s) { return smem + s * GemmSmem<BN>::stage_bytes + GemmSmem<BN>::a_bytes; };
-    auto load = [&](int kb, int s) {
-      mbar_arrive_expect_tx(&full[s], (uint32_t)GemmSmem<BN>::stage_bytes);
-      tma_load_2d(a_at(s), &ta, kb * kBK, m0, &full[s]);
-      tma_load_2d(b_at(s), &tb, kb * kBK, n0, &full[s]);
-    };
-    const int pre = nkb < kStages ? nkb : kStages;
-    for (int i = 0; i < pre; ++i) load(kb0 + i, i);
-    bool ok = true;
-    for (int i = 0; i < nkb && ok; ++i) {
-      const int s = i % kStages;
-      const uint32_t ph = (uint32_t)(i / kStages) & 1u;
-      if (!mbar_wait(&full[s], ph, kGemmWaitCycles)) {
-        ok = false;
-        break;
-      }
-      tcgen05_after_sync();
-      const uint32_t a_addr = smem_u32(a_at(s)), b_addr = smem_u32(b_at(s));
-#pragma unroll
-      for (int k = 0; k < kBK / 16; ++k)  // 16 BF16 = 32 bytes along the swizzled row
-        umma_bf16(tmem, sw128_desc(a_addr + 32 * k), sw128_desc(b_addr + 32 * k), kIdesc, i > 0 || k > 0);
-      umma_commit(&empty[s]);
-      // refill the stage the previous MMAs read, once they are done (the MMAs just issued
-      // keep the tensor pipe busy meanwhile)
-      if (i >= 1) {
-        const int ip = i - 1, sp = ip % kStages;
-        if (ip + kStages < nkb) {
-          if (!mbar_wait(&empty[sp], (uint32_t)(ip / kStages) & 1u, kGemmWaitCycles)) {
+  auto a_at = [&](int s) { return smem + s * GemmSmem<BN>::stage_bytes; };
+  auto b_at = [&](int s) { return smem + s * GemmSmem<BN>::stage_bytes + GemmSmem<BN>::a_bytes; };
+  if (warp == 0) {
+    if (lane == 0) {
+      int it = 0;  // stage fills issued (stage it % kStages, its use number it / kStages)
+      bool ok = true;
+      for (int t = blockIdx.x; t < tg.ntiles && ok; t += gridDim.x) {
+        int m0, nt, kb0, kb1;
+        tg.decode(t, m0, nt, kb0, kb1);
+        for (int kb = kb0; kb < kb1; ++kb) {
+          const int s = it % kStages;
+          // the MMAs that read this stage's previous fill are done
+          if (it >= kStages && !mbar_wait(&empty[s], (uint32_t)((it / kStages) - 1) & 1u, kGemmWaitCycles)) {
             ok = false;
             break;
           }
-          load(kb0 + ip + kStages, sp);
+          mbar_arrive_expect_tx(&full[s], (uint32_t)GemmSmem<BN>::stage_bytes);
+          tma_load_2d(a_at(s), &ta, kb * kBK, m0, &full[s]);
+          tma_load_2d(b_at(s), &tb, kb * kBK, nt * BN, &full[s]);
+          ++it;
         }
       }
-    }
-    umma_commit(&done);  // arrives once every MMA issued above has completed
-    if (!ok) {
-      s_fail = 1;
-      atomicOr(epi.err, 1);
-    }
-  }
-  __syncthreads();
-  // accumulator ready (or nothing to do for an empty K range)
-  bool ready = nkb > 0;
-  if (ready) ready = mbar_wait(&done, 0, kGemmWaitCycles);
-  if (ready && !s_fail) {
-    tcgen05_after_sync();
-    const int row = m0 + warp * 32 + lane;
-#pragma unroll 1
-    for (int c = 0; c < BN; c += 16) {
-      float v[16];
-      tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, v);
-      const int col0 = n0 + c;
-      if (row < M && col0 + 16 <= N && epi.mode != kEpiAtomic) {  // 16 whole columns: vector stores
-        const size_t o = (size_t)row * epi.ldc + col0;
-        if (epi.mode == kEpiBiasReluBf16 && ((reinterpret_cast<uintptr_t>(epi.c16 + o) & 15) == 0)) {
-          __align__(16) __nv_bfloat16 h[16];
-#pragma unroll
-          for (int j = 0; j < 16; ++j) {
-            const float x = v[j] + (epi.bias ? epi.bias[col0 + j] : 0.f);
-            h[j] = __float2bfloat16_rn(x > 0.f ? x : 0.f);
-          }
-          uint4* dst = reinterpret_cast<uint4*>(epi.c16 + o);
-          dst[0] = reinterpret_cast<const uint4*>(h)[0];
-          dst[1] = reinterpret_cast<const uint4*>(h)[1];
-          continue;
-        }
-        if (epi.mode == kEpiStore && ((reinterpret_cast<uintptr_t>(epi.c32 + o) & 15) == 0)) {
-          float4* dst = reinterpret_cast<float4*>(epi.c32 + o);
-#pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            float4 q = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
-            if (epi.bias) {
-              q.x += epi.bias[col0 + 4 * j];
-              q.y += epi.bias[col0 + 4 * j + 1];
-              q.z += epi.bias[col0 + 4 * j + 2];
-              q.w += epi.bias[col0 + 4 * j + 3];
-            }
-            dst[j] = q;
-          }
-          continue;
-        }
-      }
-      if (row < M) {
-#pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          const int col = n0 + c + j;
-          if (col >= N) continue;
-          float x = v[j];
-          const size_t o = (size_t)row * epi.ldc + col;
-          switch (epi.mode) {
-            case kEpiStore:
-              if (epi.bias) x += epi.bias[col];
-              epi.c32[o] = x;
-              break;
-            case kEpiAtomic:
-              atomicAdd(epi.c32 + o, x);
-              break;
-            case kEpiBiasReluBf16:
-              x += epi.bias ? epi.bias[col] : 0.f;
-              epi.c16[o] = __float2bfloat16_rn(x > 0.f ? x : 0.f);
-              break;
-            default:
-              break;
-          }
-        }
+      if (!ok) atomicOr(epi.err, 1);
+      // loads still in flight (after a time-out elsewhere) land before the CTA exits
+      for (int s = 0; s < kStages && s < it; ++s) {
+        const int last = it - 1 - ((it - 1 - s) % kStages);  // the last fill of stage s
+        mbar_wait(&full[s], (uint32_t)(last / kStages) & 1u, kGemmWaitCycles);
       }
     }
-  } else if (nkb > 0 && !ready) {
-    atomicOr(epi.err, 2);
+  } else if (warp == 1) {
+    if (lane == 0) {
+      int it = 0, tc = 0;
+      bool ok = true, issued = false;
+      for (int t = blockIdx.x; t < tg.ntiles && ok; t += gridDim.x, ++tc) {
+        int m0, nt, kb0, kb1;
+        tg.decode(t, m0, nt, kb0, kb1);
+        const int b = tc & 1;
+        // the epilogue has read this accumulator's previous tile (tile tc - 2)
+        if (tc >= 2 && !mbar_wait(&acc_empty[b], (uint32_t)((tc >> 1) - 1) & 1u, kGemmWaitCycles)) {
+          ok = false;
+          break;
+        }
+        tcgen05_after_sync();
+        const uint32_t d = tmem + (uint32_t)b * kCols;
+        for (int kb = kb0; kb < kb1; ++kb) {
+          const int s = it % kStages;
+          if (!mbar_wait(&full[s], (uint32_t)(it / kStages) & 1u, kGemmWaitCycles)) {
+            ok = false;
+            break;
+          }
+          tcgen05_after_sync();
+          const uint32_t a_addr = smem_u32(a_at(s)), b_addr = smem_u32(b_at(s));
+#pragma unroll
+          for (int k = 0; k < kBK / 16; ++k)  // 16 BF16 = 32 bytes along the swizzled row
+            umma_bf16(d, sw128_desc(a_addr + 32 * k), sw128_desc(b_addr + 32 * k), kIdesc, kb > kb0 || k > 0);
+          umma_commit(&empty[s]);
+          issued = true;
+          ++it;
+        }
+        if (!ok) break;
+        umma_commit(&acc_full[b]);
+      }
+      if (!ok) atomicOr(epi.err, 1);
+      if (issued) {  // every MMA issued above has completed before TMEM is freed
+        umma_commit(&drain);
+        if (!mbar_wait(&drain, 0u, kGemmWaitCycles)) atomicOr(epi.err, 1);
+      }
+    }
+  } else {
+    const int q = warp & 3;  // TMEM lanes 32 q .. 32 q + 31 = tile rows
+    int tc = 0;
+    for (int t = blockIdx.x; t < tg.ntiles; t += gridDim.x, ++tc) {
+      int m0, nt, kb0, kb1;
+      tg.decode(t, m0, nt, kb0, kb1);
+      const int b = tc & 1;
+      if (!mbar_wait(&acc_full[b], (uint32_t)(tc >> 1) & 1u, kGemmWaitCycles)) {
+        if (lane == 0) atomicOr(epi.err, 2);
+        break;
+      }
+      tcgen05_after_sync();
+      gemm_epilogue_tile<BN>(epi, tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)b * kCols, m0 + q * 32 + lane,
+                             nt * BN, M, N);
+      tcgen05_before_sync();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&acc_empty[b]);
+    }
   }
   tcgen05_before_sync();
   __syncthreads();
-  if (warp == 0) tmem_free(tmem, kCols);
+  if (warp == 1) tmem_free(tmem, kAlloc);
 }
 
 // 2-D tensor map of a row-major BF16 matrix (rows x cols, cols contiguous with pitch ld
@@ -216,6 +277,18 @@ bool make_tmap_bf16(CUtensorMap* map, const void* base, long long rows, long lon
                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+int num_sms() {
+  static int sms = 0;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+      sms = 148;
+    cudaGetLastError();
+  });
+  return sms;
+}
+
 template <int BN>
 int launch_bn(const GemmArgs& g, cudaStream_t st) {
   CUtensorMap ta, tb;
@@ -226,12 +299,22 @@ int launch_bn(const GemmArgs& g, cudaStream_t st) {
   int splits = g.splits < 1 ? 1 : g.splits;
   if (splits > kb_total) splits = kb_total;
   const int per = (kb_total + splits - 1) / splits;
-  splits = (kb_total + per - 1) / per;
+  splits = (kb_total + per - 1) / per;  // every split holds at least one K block
   if (splits > 1 && g.epi.mode != kEpiAtomic) return -1;
-  const dim3 grid((unsigned)((g.M + 127) / 128), (unsigned)((g.N + BN - 1) / BN), (unsigned)splits);
+  TileGrid tg;
+  tg.tiles_m = (int)((g.M + 127) / 128);
+  tg.tiles_n = (int)((g.N + BN - 1) / BN);
+  tg.ntiles = tg.tiles_m * tg.tiles_n * splits;
+  tg.kb_per_split = per;
+  tg.kb_total = kb_total;
+  // persistent: as many CTAs as fit on the GPU at once (shared memory bound), at most one
+  // per tile
+  const long long slots = (long long)num_sms() * GemmSmem<BN>::per_sm;
+  const int grid = (int)(tg.ntiles < slots ? tg.ntiles : slots);
   auto k = umma_gemm_kernel<BN>;
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, GemmSmem<BN>::bytes);
-  k<<<grid, 128, GemmSmem<BN>::bytes, st>>>(ta, tb, g.epi, (int)g.M, (int)g.N, per, kb_total);
+  cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+  k<<<grid, kGemmThreads, GemmSmem<BN>::bytes, st>>>(ta, tb, g.epi, (int)g.M, (int)g.N, tg);
   return 1;
 }
 

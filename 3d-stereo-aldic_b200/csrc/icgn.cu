@@ -317,6 +317,7 @@ __global__ void __launch_bounds__(NT) icgn_solve_kernel(IcgnArgs a, int bucket) 
   const FrameDev& fr = a.fr;
   const bool quad = (a.variant == 1);
   const bool epi = (a.variant == 2);
+  const bool want_fg = epi || a.zncc != nullptr;  // sum f g: the epipolar ZNSSD, or the ZNCC
   const int count = a.qcount[bucket == 2 ? 4 : bucket];
   const int gM = fr.M - 6;
   for (int qi = blockIdx.x; qi < count; qi += gridDim.x) {
@@ -516,7 +517,7 @@ __global__ void __launch_bounds__(NT) icgn_solve_kernel(IcgnArgs a, int bucket) 
             ns += 1.f;
           }
           nz += (g == (G)0) ? 1.f : 0.f;
-          if (epi) fg = fma((G)s.f[p], g, fg);
+          if (want_fg) fg = fma((G)s.f[p], g, fg);
           aa += r_nt;
           bb += q_nt;
           if (aa >= W1) {
@@ -552,7 +553,7 @@ __global__ void __launch_bounds__(NT) icgn_solve_kernel(IcgnArgs a, int bucket) 
           gm = s.fbw8;
         }
         __syncthreads();
-        G C2[6] = {0, 0, 0, 0, 0, 0}, T1 = 0, T2 = 0;
+        G C2[6] = {0, 0, 0, 0, 0, 0}, T1 = 0, T2 = 0, TF = 0;
         float tn = 0.f, gs = 0.f;
         for (int p = tid; p < npx; p += NT) {
           const G dx = (G)(p % W1 - half), dy = (G)(p / W1 - half);
@@ -570,9 +571,10 @@ __global__ void __launch_bounds__(NT) icgn_solve_kernel(IcgnArgs a, int bucket) 
             tn += 1.f;
           }
           gs += gm[p] ? 1.f : 0.f;
+          if (want_fg) TF = fma((G)s.f[p], g, TF);
         }
-        double v2[10] = {C2[0], C2[1], C2[2], C2[3], C2[4], C2[5], T1, T2, tn, gs};
-        block_sum<10, NT>(v2, red, sums);
+        double v2[11] = {C2[0], C2[1], C2[2], C2[3], C2[4], C2[5], T1, T2, tn, gs, TF};
+        block_sum<11, NT>(v2, red, sums);
         if (tid == 0) c.gsum_prev = sums[9];
       }
       if (tid == 0) {
@@ -587,7 +589,7 @@ __global__ void __launch_bounds__(NT) icgn_solve_kernel(IcgnArgs a, int bucket) 
         }
         double b[6];
         for (int i = 0; i < 6; ++i) b[i] = c.bf * (c.A[i] - (sums[i] - meang * c.B[i]) / bg);
-        if (epi) c.znssd = 2.0 - 2.0 * (sums[10] - c.meanf * sums[6]) / (c.bf * bg);
+        if (want_fg) c.znssd = 2.0 - 2.0 * (sums[10] - c.meanf * sums[6]) / (c.bf * bg);
         double nn = 0;
         for (int i = 0; i < 6; ++i) nn += b[i] * b[i];
         c.normNew = sqrt(nn);
@@ -642,6 +644,7 @@ __global__ void __launch_bounds__(NT) icgn_solve_kernel(IcgnArgs a, int bucket) 
         a.U[2 * t] = c.P[4];
         a.U[2 * t + 1] = c.P[5];
         for (int k = 0; k < 4; ++k) a.F[4 * t + k] = c.P[k];
+        if (want_fg) a.zncc[t] = 1.0 - 0.5 * c.znssd;
         if (a.H)
           for (int k = 0; k < 21; ++k) a.H[t + a.n * k] = c.H[k];
       }
@@ -822,6 +825,7 @@ __global__ void __launch_bounds__(kWT, STAGED ? 2 : (NW == 1 ? 3 : 2))
   const FrameDev& fr = a.fr;
   const bool quad = (a.variant == 1);
   const bool epi = (a.variant == 2);
+  const bool want_fg = epi || a.zncc != nullptr;  // sum f g: the epipolar ZNSSD, or the ZNCC
   __shared__ int s_qi[NG];
   const int count = a.qcount[SLOW ? 1 : 0];
   const int gM = fr.M - 6;
@@ -1153,7 +1157,7 @@ __global__ void __launch_bounds__(kWT, STAGED ? 2 : (NW == 1 ? 3 : 2))
             }
             nz += (g.x == 0.f ? 1.f : 0.f) + (g.y == 0.f ? 1.f : 0.f);
           }
-          if (epi)
+          if (want_fg)
             fg2 = ffma2(make_float2(fr.ref[(r0 + aa) + (c0 + bb) * fr.M], fr.ref[(r0 + ab) + (c0 + bbb) * fr.M]), g,
                         fg2);
           aa = ab + r_nt;
@@ -1203,7 +1207,7 @@ __global__ void __launch_bounds__(kWT, STAGED ? 2 : (NW == 1 ? 3 : 2))
             v[6] += (double)g;
             v[7] += (double)g * (double)g;
           }
-          if (epi) v[10] += (double)fr.ref[(r0 + aa) + (c0 + bb) * fr.M] * (double)g;
+          if (want_fg) v[10] += (double)fr.ref[(r0 + aa) + (c0 + bb) * fr.M] * (double)g;
         }
         v[8] = ns;
         v[9] = nz;
@@ -1221,7 +1225,7 @@ __global__ void __launch_bounds__(kWT, STAGED ? 2 : (NW == 1 ? 3 : 2))
         meang = ALDIC_NAN;
         bgn = ALDIC_NAN;
       }
-      if (epi) znssd = 2.0 - 2.0 * (v[10] - meanf * v[6]) / (bf * bgn);
+      if (want_fg) znssd = 2.0 - 2.0 * (v[10] - meanf * v[6]) / (bf * bgn);
       double b[6];
       const double ibgn = 1.0 / bgn;  // one FP64 division per iteration instead of six
 #pragma unroll
@@ -1296,6 +1300,7 @@ __global__ void __launch_bounds__(kWT, STAGED ? 2 : (NW == 1 ? 3 : 2))
           a.U[2 * t] = P[4];
           a.U[2 * t + 1] = P[5];
           for (int k = 0; k < 4; ++k) a.F[4 * t + k] = P[k];
+          if (want_fg) a.zncc[t] = 1.0 - 0.5 * znssd;
           if (a.H)
             for (int k = 0; k < 21; ++k) a.H[t + a.n * k] = s_h[grp][k];
         }

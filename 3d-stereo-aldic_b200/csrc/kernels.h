@@ -51,6 +51,9 @@ struct IcgnArgs {
   int slow_fp64; // 1: subsets still iterating after warp_cap are re-solved in FP64 (not the epipolar
                  // variant, whose slow subsets always take the FP32 multi-warp pass)
   int fp64_threads;  // threads per subset of the FP64 re-solve kernel: 128 or 256
+  double* zncc;  // n or null (not epipolar): ZNCC of the window under the last evaluated warp,
+                 // which is the returned [F U] for a converged subset (the acceptance test of a
+                 // learned initial guess; sums of the last iteration, so no extra pass)
 };
 constexpr double kDefaultFp64Band = 1e-3;  // default IcgnArgs::band (plus the FP32 noise of |b|)
 constexpr double kDefaultFp64Noise = 4.0;  // default IcgnArgs::noise (2x the calibrated need)

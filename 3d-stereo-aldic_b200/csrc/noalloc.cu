@@ -147,6 +147,7 @@ extern "C" int aldic_local_icgn_noalloc(int variant, const float* ref, const flo
   a.slow_nw = 2;
   a.slow_fp64 = 0;
   a.fp64_threads = 128;
+  a.zncc = nullptr;
   aldic::launch_icgn(a, wmax, static_cast<cudaStream_t>(stream));
   return cudaGetLastError() == cudaSuccess ? ALDIC_OK : ALDIC_ERR_CUDA;
 }

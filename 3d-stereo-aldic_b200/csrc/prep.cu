@@ -12,8 +12,9 @@ __device__ __forceinline__ double load_px(const T* p, size_t k) {
 }
 
 // Sum of (x - shift)^power (power 1 or 2) over the ROI rows [gx0, gx1) x cols [gy0, gy1)
-// (0-based, half open).  Each block writes a partial; the last block to finish adds
-// the partials in a fixed order (deterministic) and stores
+// (0-based, half open), for floating-point images.  A block walks whole ROI columns
+// (contiguous rows, no per-pixel index division).  Each block writes a partial; the last
+// block to finish adds the partials in a fixed order (deterministic) and stores
 //   POWER 1: stats[0] = sum, stats[2] = mean;
 //   POWER 2: stats[1] = sum of squared deviations, stats[3] = std (N-1 normalised).
 template <typename T, int POWER>
@@ -23,14 +24,14 @@ __global__ void roi_moment_kernel(const T* __restrict__ img, int M, int gx0, int
   __shared__ double red[32];
   __shared__ bool last;
   const double shift = shift_ptr ? shift_ptr[0] : 0.0;
-  const int rows = gx1 - gx0;
-  const long long total = (long long)rows * (gy1 - gy0);
+  const int rows = gx1 - gx0, cols = gy1 - gy0;
   double s = 0;
-  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < total;
-       k += (long long)gridDim.x * blockDim.x) {
-    const int a = (int)(k % rows), b = (int)(k / rows);
-    const double v = load_px(img, (size_t)(gx0 + a) + (size_t)(gy0 + b) * M) - shift;
-    s += (POWER == 1) ? v : v * v;
+  for (int b = blockIdx.x; b < cols; b += gridDim.x) {
+    const T* col = img + (size_t)(gy0 + b) * M + gx0;
+    for (int r = threadIdx.x; r < rows; r += blockDim.x) {
+      const double v = load_px(col, (size_t)r) - shift;
+      s += (POWER == 1) ? v : v * v;
+    }
   }
   s = warp_sum(s);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -60,6 +61,77 @@ __global__ void roi_moment_kernel(const T* __restrict__ img, int M, int gx0, int
   }
 }
 
+__device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// The same statistics for integer images (u8, u16) in one pass: exact integer sums S1 = sum x
+// and S2 = sum x^2 over the ROI, then the sum of squared deviations (n S2 - S1^2) / n from
+// exact 128-bit integers, which the reference's two FP64 passes (the mean, then the squared
+// deviations from it; funNormalizeImg.m) approximate to within their rounding.  partials
+// holds 2 entries per block.
+template <typename T>
+__global__ void roi_moment_int_kernel(const T* __restrict__ img, int M, int gx0, int gx1, int gy0, int gy1,
+                                      unsigned long long* __restrict__ partials, unsigned int* __restrict__ counter,
+                                      double* __restrict__ stats, long long count) {
+  __shared__ unsigned long long red[2][32];
+  __shared__ bool last;
+  const int rows = gx1 - gx0, cols = gy1 - gy0;
+  unsigned long long s1 = 0, s2 = 0;
+  for (int b = blockIdx.x; b < cols; b += gridDim.x) {
+    const T* col = img + (size_t)(gy0 + b) * M + gx0;
+    for (int r = threadIdx.x; r < rows; r += blockDim.x) {
+      const unsigned long long v = col[r];
+      s1 += v;
+      s2 += v * v;
+    }
+  }
+  s1 = warp_sum_u64(s1);
+  s2 = warp_sum_u64(s2);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+    red[0][warp] = s1;
+    red[1][warp] = s2;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long t1 = 0, t2 = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      t1 += red[0][w];
+      t2 += red[1][w];
+    }
+    partials[2 * blockIdx.x] = t1;
+    partials[2 * blockIdx.x + 1] = t2;
+    __threadfence();
+    const unsigned int done = atomicAdd(counter, 1u);
+    last = (done == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (last && threadIdx.x < 32) {
+    unsigned long long t1 = 0, t2 = 0;
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += 32) {
+      t1 += ((volatile unsigned long long*)partials)[2 * i];
+      t2 += ((volatile unsigned long long*)partials)[2 * i + 1];
+    }
+    t1 = warp_sum_u64(t1);
+    t2 = warp_sum_u64(t2);
+    if (threadIdx.x == 0) {
+      const double n = (double)count;
+      const unsigned __int128 d =
+          (unsigned __int128)(unsigned long long)count * t2 - (unsigned __int128)t1 * t1;  // >= 0
+      const double nd = (double)(unsigned long long)(d >> 64) * 18446744073709551616.0 + (double)(unsigned long long)d;
+      const double ssd = nd / n;
+      stats[0] = (double)t1;  // exact: t1 < 2^53
+      stats[1] = ssd;
+      stats[2] = (double)t1 / n;
+      stats[3] = sqrt(ssd / (n - 1.0));
+      *counter = 0;  // re-arm for the next use
+    }
+  }
+}
+
 template <typename T>
 __global__ void normalize_map_kernel(const T* __restrict__ img, long long npx, const double* __restrict__ stats,
                                      const uint8_t* __restrict__ mask, float* __restrict__ out) {
@@ -69,6 +141,32 @@ __global__ void normalize_map_kernel(const T* __restrict__ img, long long npx, c
     if (mask && !mask[k]) v = 0.0;
     out[k] = (float)v;
   }
+}
+
+// u8 images take at most 256 values: each block tabulates (x - mean) / sd (the same FP64
+// division, so the same bits as normalize_map_kernel) and maps 4 pixels per thread step
+// (4-byte loads, 16-byte stores); vec = 0 when a pointer is not aligned for that.
+__global__ void normalize_u8_kernel(const uint8_t* __restrict__ img, long long npx, const double* __restrict__ stats,
+                                    const uint8_t* __restrict__ mask, float* __restrict__ out, int vec) {
+  __shared__ float lut[256];
+  const double mean = stats[2], sd = stats[3];
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) lut[i] = (float)(((double)i - mean) / sd);
+  __syncthreads();
+  const long long stride = (long long)gridDim.x * blockDim.x, first = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long n4 = vec ? npx / 4 : 0;
+  for (long long k = first; k < n4; k += stride) {
+    const uchar4 v = reinterpret_cast<const uchar4*>(img)[k];
+    float4 o = make_float4(lut[v.x], lut[v.y], lut[v.z], lut[v.w]);
+    if (mask) {
+      const uchar4 m = reinterpret_cast<const uchar4*>(mask)[k];
+      if (!m.x) o.x = 0.f;
+      if (!m.y) o.y = 0.f;
+      if (!m.z) o.z = 0.f;
+      if (!m.w) o.w = 0.f;
+    }
+    reinterpret_cast<float4*>(out)[k] = o;
+  }
+  for (long long k = 4 * n4 + first; k < npx; k += stride) out[k] = (mask && !mask[k]) ? 0.f : lut[img[k]];
 }
 
 __global__ void f64_to_f32_kernel(const double* __restrict__ in, long long n, float* __restrict__ out) {
@@ -88,15 +186,19 @@ __global__ void mask_binarize_kernel(const double* __restrict__ in, long long n,
 
 // funImgGradient (func/funImgGradient.m:52-78): correlation with
 // h = [-1 9 -45 0 45 -9 1]/60 along dim 1 (gx) and dim 2 (gy) at pixel (i+3, j+3),
-// times the mask there.  One thread per output pixel; columns of the output are
-// contiguous so a warp reads 32 consecutive rows (coalesced).
+// times the mask there.  One thread per output pixel; a block step covers 256 consecutive
+// rows of one output column (coalesced; the column and row come from one 32-bit division
+// per step, not per pixel).
 __global__ void gradient_kernel(const float* __restrict__ img, const uint8_t* __restrict__ mask, int M, int N,
                                 float* __restrict__ gx, float* __restrict__ gy) {
   const int gM = M - 6, gN = N - 6;
-  const long long total = (long long)gM * gN;
-  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < total;
-       k += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(k % gM) + 3, j = (int)(k / gM) + 3;
+  const int rb = (gM + 255) / 256;  // row steps per column
+  const int steps = rb * gN;
+  for (int st = blockIdx.x; st < steps; st += gridDim.x) {
+    const int jj = st / rb, i0 = (st - jj * rb) * 256;
+    const int ii = i0 + (int)threadIdx.x;
+    if (ii >= gM) continue;
+    const int i = ii + 3, j = jj + 3;
     const float* c = img + (size_t)i + (size_t)j * M;
     const float dx = ((__ldg(c + 3) - __ldg(c - 3)) - 9.0f * (__ldg(c + 2) - __ldg(c - 2)) +
                       45.0f * (__ldg(c + 1) - __ldg(c - 1))) * (1.0f / 60.0f);
@@ -104,6 +206,7 @@ __global__ void gradient_kernel(const float* __restrict__ img, const uint8_t* __
                       9.0f * (__ldg(c + 2 * (size_t)M) - __ldg(c - 2 * (size_t)M)) +
                       45.0f * (__ldg(c + (size_t)M) - __ldg(c - (size_t)M))) * (1.0f / 60.0f);
     const float mk = mask ? (float)mask[(size_t)i + (size_t)j * M] : 1.0f;
+    const size_t k = (size_t)ii + (size_t)jj * gM;
     gx[k] = dx * mk;
     gy[k] = dy * mk;
   }
@@ -146,24 +249,37 @@ int launch_normalize(const void* img, int dtype, int M, int N, int gx0, int gx1,
                      unsigned int* counter, cudaStream_t st) {
   const long long cnt = (long long)(gx1 - gx0) * (gy1 - gy0);
   const int th = 256;
-  const int g = grid_for(cnt, th, npartials);
+  const int cols = gy1 - gy0;
+  const int g = cols < npartials ? cols : npartials;            // FP partials: 1 per block
+  const int gi = cols < npartials / 2 ? cols : npartials / 2;   // integer partials: 2 per block
   const long long npx = (long long)M * N;
   const int gm = grid_for(npx, th, 4 * 148 * 4);
+  unsigned long long* ip = reinterpret_cast<unsigned long long*>(partials);
+  switch (dtype) {
+    case 0: {
+      roi_moment_int_kernel<uint8_t><<<gi, th, 0, st>>>((const uint8_t*)img, M, gx0, gx1, gy0, gy1, ip, counter,
+                                                        stats, cnt);
+      const int vec = ((uintptr_t)img % 4 == 0) && ((uintptr_t)out % 16 == 0) && ((uintptr_t)mask % 4 == 0);
+      normalize_u8_kernel<<<grid_for((npx + 3) / 4, th, 148 * 8), th, 0, st>>>((const uint8_t*)img, npx, stats,
+                                                                            mask, out, vec);
+      return 2;
+    }
+    case 1:
+      roi_moment_int_kernel<uint16_t><<<gi, th, 0, st>>>((const uint16_t*)img, M, gx0, gx1, gy0, gy1, ip, counter,
+                                                         stats, cnt);
+      normalize_map_kernel<uint16_t><<<gm, th, 0, st>>>((const uint16_t*)img, npx, stats, mask, out);
+      return 2;
 #define ALDIC_NORM_CASE(T)                                                                                        \
   roi_moment_kernel<T, 1><<<g, th, 0, st>>>((const T*)img, M, gx0, gx1, gy0, gy1, nullptr, partials, counter,    \
                                             stats, cnt);                                                        \
   roi_moment_kernel<T, 2><<<g, th, 0, st>>>((const T*)img, M, gx0, gx1, gy0, gy1, stats + 2, partials, counter,  \
                                             stats, cnt);                                                        \
   normalize_map_kernel<T><<<gm, th, 0, st>>>((const T*)img, npx, stats, mask, out);
-  switch (dtype) {
-    case 0: { ALDIC_NORM_CASE(uint8_t) break; }
-    case 1: { ALDIC_NORM_CASE(uint16_t) break; }
-    case 2: { ALDIC_NORM_CASE(float) break; }
-    case 3: { ALDIC_NORM_CASE(double) break; }
+    case 2: { ALDIC_NORM_CASE(float) return 3; }
+    case 3: { ALDIC_NORM_CASE(double) return 3; }
+#undef ALDIC_NORM_CASE
     default: return -1;
   }
-#undef ALDIC_NORM_CASE
-  return 3;  // kernels launched
 }
 
 int launch_f64_to_f32(const double* in, long long n, float* out, cudaStream_t st) {
@@ -182,8 +298,8 @@ int launch_mask_binarize(const double* in, long long n, uint8_t* out, cudaStream
 }
 
 int launch_gradient(const float* img, const uint8_t* mask, int M, int N, float* gx, float* gy, cudaStream_t st) {
-  const long long total = (long long)(M - 6) * (N - 6);
-  gradient_kernel<<<grid_for(total, 256, 148 * 16), 256, 0, st>>>(img, mask, M, N, gx, gy);
+  const long long steps = (long long)((M - 6 + 255) / 256) * (N - 6);
+  gradient_kernel<<<grid_for(steps, 1, 148 * 16), 256, 0, st>>>(img, mask, M, N, gx, gy);
   return 1;
 }
 

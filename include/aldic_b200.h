@@ -305,10 +305,14 @@ int aldic_net_predict(aldic_net* net, aldic_ctx* ctx, int64_t n, const double* c
  * training sets and checks of aldic_net_predict. */
 int aldic_net_extract(aldic_ctx* ctx, int64_t n, const double* coords, void* X);
 /* aldic_local_icgn from the initial guess P = [F0 U0] instead of [0 U0] (the reference starts
- * from F = 0, func/funICGN.m:46); everything else as aldic_local_icgn. */
+ * from F = 0, func/funICGN.m:46); everything else as aldic_local_icgn.  zncc (n, optional)
+ * receives each subset's zero-normalised cross-correlation of REF with DEF under the last
+ * warp IC-GN evaluated, which for a converged subset is the returned [F U] (its last
+ * iteration stops without an update): that iteration's sums, no extra pass (the acceptance
+ * test of a learned initial guess).  NaN where no pass solved the subset. */
 int aldic_local_icgn_guess(aldic_ctx* ctx, int variant, int64_t n, const double* coords, const double* U0,
                            const double* F0, int winsize, double tol, double* U, double* F, double* H, int32_t* conv,
-                           uint8_t* markHole);
+                           uint8_t* markHole, double* zncc);
 /* The fallback of a learned initial guess: the subsets whose IC-GN from it did not converge
  * (conv outside 1..100) or whose final ZNCC is below zncc_min (or NaN).  Their indices (0-based,
  * in no fixed order) go to list (n entries of room, host or device) and their number to

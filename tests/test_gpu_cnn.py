@@ -16,8 +16,11 @@ def _bf16_tensor(a, dev):
     return torch.from_numpy(np.ascontiguousarray(a, dtype=np.float32)).to(dev).to(torch.bfloat16)
 
 
+# the last three hold several tiles per persistent CTA (148 SMs): both TMEM accumulators and
+# the stage ring wrap around many times, with split-K atomics in the last
 @pytest.mark.parametrize("M,N,K,splits", [(300, 32, 24, 1), (256, 64, 288, 1), (128, 16, 128, 1),
-                                          (1000, 1024, 128, 1), (64, 288, 4096, 8), (32, 24, 131072, 64)])
+                                          (1000, 1024, 128, 1), (64, 288, 4096, 8), (32, 24, 131072, 64),
+                                          (113664, 64, 736, 1), (56832, 1024, 256, 1), (20000, 128, 4096, 4)])
 def test_tensor_core_gemm_matches_numpy(M, N, K, splits):
     import torch
 

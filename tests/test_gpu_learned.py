@@ -74,6 +74,32 @@ def test_zero_gradient_guess_is_the_reference_start(env):
         assert np.array_equal(a[k], b[k], equal_nan=True), k
 
 
+def test_icgn_zncc_output_is_the_final_warps_zncc(env):
+    """The ZNCC IC-GN returns from its last iteration's sums equals the ZNCC of the returned
+    [F U] (aldic_subset_zncc) on converged subsets, changes no other output, and is NaN for a
+    subset no pass solves (its window leaves the image)."""
+    A, ctx, pair = env["A"], env["ctx"], env["pair"]
+    crd = np.vstack([_nodes(pair.M, pair.N), [[6.0, 6.0]]])
+    n = crd.shape[0]
+    u, v = pair.field.disp(crd[:, 0], crd[:, 1])
+    rng = np.random.default_rng(5)
+    U0 = (np.stack([u, v], 1) + rng.uniform(-0.6, 0.6, (n, 2))).ravel()
+    F0 = (pair.field.grad(crd[:, 0], crd[:, 1]) + rng.uniform(-0.01, 0.01, (n, 4))).ravel()
+    for variant in (A.UNIFORM, A.QUADTREE):
+        a = ctx.local_icgn(variant, crd, U0, 32, 1e-3, F0=F0, want_H=False)
+        d = ctx.local_icgn(variant, crd, U0, 32, 1e-3, F0=F0, want_H=False, want_zncc=True)
+        for k in ("U", "F", "conv"):
+            assert np.array_equal(a[k], d[k], equal_nan=True), k
+        ok = (d["conv"] > 0) & (d["conv"] < 100)
+        assert ok[:-1].mean() > 0.95 and not ok[-1]
+        z = ctx.subset_zncc(crd, d["U"], d["F"], 32)
+        assert np.abs(d["zncc"] - z)[ok].max() < 1e-5
+        assert d["zncc"][ok].min() > 0.9
+        assert np.isnan(d["zncc"][-1])
+    with pytest.raises(ValueError):
+        ctx.local_icgn(A.UNIFORM, crd, U0, 32, 1e-3, want_zncc=True)
+
+
 def test_subset_zncc_matches_numpy(env):
     ctx, pair = env["ctx"], env["pair"]
     crd = _nodes(pair.M, pair.N)
