@@ -333,12 +333,21 @@ class Context:
                     "aldic_subset_zncc")
         return z
 
-    def fallback_select(self, conv, zncc, zncc_min, out):
+    def fallback_select(self, conv, zncc, zncc_min, out, count=None):
         """Indices (0-based, in no fixed order) of the subsets with conv outside 1..100 or
         zncc below zncc_min (or NaN) into `out` (int32, n entries of room: a CUDA tensor or a
-        writeable numpy array); returns their number (waits for the device)."""
+        writeable numpy array); returns their number (waits for the device).  With `count` (a
+        1-entry int64 CUDA tensor) the number goes there instead, queued on the context's
+        stream without a wait, and the call returns None."""
         k = _Keep()
         n = int(conv.numel() if _is_torch(conv) else np.asarray(conv).size)
+        if count is not None:
+            if not (_is_torch(count) and count.is_cuda):
+                raise ValueError("count must be a 1-entry int64 CUDA tensor")
+            self._check(self.lib.aldic_fallback_select(self.h, n, k.ptr(conv, np.int32), k.ptr(zncc, np.float64),
+                                                       float(zncc_min), k.dst(out, np.int32, n),
+                                                       k.ptr(count, np.int64, numel=1)), "aldic_fallback_select")
+            return None
         cnt = C.c_int64()
         self._check(self.lib.aldic_fallback_select(self.h, n, k.ptr(conv, np.int32), k.ptr(zncc, np.float64),
                                                    float(zncc_min), k.dst(out, np.int32, n), C.byref(cnt)),

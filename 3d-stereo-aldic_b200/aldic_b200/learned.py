@@ -251,9 +251,11 @@ class LearnedInit:
     whose final ZNCC is below zncc_min is searched (funIntegerSearchWholeField restricted to
     those grid subsets) and solved again from the search's [0 U0], as the reference's
     search-initialised path would.  Everything stays on ctx's stream; the host waits once, for
-    the number of fallback subsets."""
+    the number of fallback subsets.  run() = submit() (queue the frame) + complete() (that
+    wait, then queue the fallback); LearnedPipeline puts another frame between the two."""
 
-    def __init__(self, net, ctx, search, gridx, gridy, winsize, step, tol, zncc_min=0.9, variant=_lib.QUADTREE):
+    def __init__(self, net, ctx, search, gridx, gridy, winsize, step, tol, zncc_min=0.9, variant=_lib.QUADTREE,
+                 stream=None):
         import torch as T
 
         self.T, self.net, self.ctx = T, net, ctx
@@ -263,7 +265,9 @@ class LearnedInit:
         nodes, self.nx, self.ny = search_nodes(self.gx, self.gy, self.w, self.step)
         self.n = n = nodes.shape[1]
         dev = T.device("cuda", ctx.device if hasattr(ctx, "device") else T.cuda.current_device())
-        self.stream = T.cuda.Stream(dev)
+        # one stream for everything (a given one lets several contexts share the network's
+        # buffers in order, e.g. frames pipelined over two contexts)
+        self.stream = stream if stream is not None else T.cuda.Stream(dev)
         ctx.set_stream(self.stream.cuda_stream)
         f64 = dict(dtype=T.float64, device=dev)
         self.coords = T.from_numpy(np.ascontiguousarray(nodes)).to(dev)
@@ -271,6 +275,9 @@ class LearnedInit:
                     "F": T.empty(4 * n, **f64), "conv": T.empty(n, dtype=T.int32, device=dev),
                     "zncc": T.empty(n, **f64), "fallback": T.zeros(n, dtype=T.bool, device=dev)}
         self.flist = T.empty(n, dtype=T.int32, device=dev)
+        self.count_dev = T.zeros(1, dtype=T.int64, device=dev)
+        self.count_host = T.zeros(1, dtype=T.int64, pin_memory=True)
+        self.count_event = T.cuda.Event()
         self.n_fallback = 0
         # (start, stop) CUDA event pairs recorded around the prediction and the main IC-GN call
         # when these are lists (timing hooks)
@@ -290,14 +297,32 @@ class LearnedInit:
 
     def run(self):
         """One frame; returns the number of fallback subsets."""
-        T, ctx, b, n = self.T, self.ctx, self.buf, self.n
+        self.submit()
+        return self.complete()
+
+    def submit(self):
+        """Queue one frame on the stream without waiting: prediction, IC-GN from [F0 U0] (its
+        last iteration's sums give each subset's ZNCC) and the fallback selection, whose count
+        is copied to pinned host memory.  complete() finishes the frame; a caller may queue
+        another frame (on another context) in between."""
+        T, ctx, b = self.T, self.ctx, self.buf
         with T.cuda.stream(self.stream):
             self._timed(self.predict_events, lambda: self.net.predict(ctx, self.coords, b))
-            # IC-GN from [F0 U0]; its last iteration's sums give each subset's ZNCC
             self._timed(self.icgn_events,
                         lambda: ctx.local_icgn(self.variant, self.coords, b["U0"], self.w, self.tol, want_H=False,
                                                want_mark=False, out=b, F0=b["F0"], want_zncc=True))
-            nf = ctx.fallback_select(b["conv"], b["zncc"], self.zncc_min, self.flist)  # the host's one wait
+            ctx.fallback_select(b["conv"], b["zncc"], self.zncc_min, self.flist, count=self.count_dev)
+            self.count_host.copy_(self.count_dev, non_blocking=True)
+            self.count_event.record(self.stream)
+
+    def complete(self):
+        """Wait for the submitted frame's fallback count (the host's one wait per frame) and
+        queue the fallback: the integer search on those grid subsets and IC-GN from its
+        [0 U0].  Returns the number of fallback subsets."""
+        T, ctx, b, n = self.T, self.ctx, self.buf, self.n
+        self.count_event.synchronize()
+        nf = int(self.count_host[0])
+        with T.cuda.stream(self.stream):
             b["fallback"].zero_()
             if nf:
                 il = self.flist[:nf]
@@ -319,3 +344,46 @@ class LearnedInit:
                 b["F0"].view(n, 4)[idx] = 0.0
         self.n_fallback = nf
         return nf
+
+
+class LearnedPipeline:
+    """Frames through the learned initial guess with two contexts in flight: frame k is loaded
+    into one context and queued (LearnedInit.submit) before the host waits for frame k-1's
+    fallback count (LearnedInit.complete), so that wait, and the host's launches of frame k,
+    overlap the device's work instead of leaving it idle.  Both LearnedInit objects share the
+    network and one stream (the network's buffers are used in stream order).  Arguments after
+    `ctxs` (two contexts on the same device) are LearnedInit's."""
+
+    def __init__(self, net, ctxs, *args, **kw):
+        if len(ctxs) != 2:
+            raise ValueError("LearnedPipeline takes two contexts")
+        first = LearnedInit(net, ctxs[0], *args, **kw)
+        kw = dict(kw, stream=first.stream)
+        self.lis = [first, LearnedInit(net, ctxs[1], *args, **kw)]
+        self.stream = first.stream
+        self.turn = 0
+        self.pending = None
+
+    def push(self, load):
+        """load(ctx) queues the next frame's images into a context (on the stream); the frame
+        is then submitted and the previous one completed.  Returns the LearnedInit that holds
+        the previous frame's results (valid on the stream until the push after next), or None
+        for the first frame."""
+        import torch as T
+
+        li = self.lis[self.turn]
+        self.turn ^= 1
+        with T.cuda.stream(self.stream):
+            load(li.ctx)
+        li.submit()
+        done, self.pending = self.pending, li
+        if done is not None:
+            done.complete()
+        return done
+
+    def flush(self):
+        """Completes the last pushed frame; returns its LearnedInit (or None)."""
+        done, self.pending = self.pending, None
+        if done is not None:
+            done.complete()
+        return done

@@ -821,10 +821,14 @@ int aldic_fallback_select(aldic_ctx* c, int64_t n, const int32_t* conv, const do
                           int32_t* list, int64_t* count) {
   if (!c) return ALDIC_ERR_ARG;
   if (n < 0 || !count) return fail(c, ALDIC_ERR_ARG, "n >= 0 and count are required");
-  *count = 0;
-  if (n == 0) return ALDIC_OK;
-  if (!conv || !zncc || !list) return fail(c, ALDIC_ERR_ARG, "conv, zncc and list are required");
   CK(cudaSetDevice(c->device));
+  const bool dev_count = is_device_ptr(count);
+  if (!dev_count) *count = 0;
+  if (n == 0) {
+    if (dev_count) CK(cudaMemsetAsync(count, 0, sizeof(int64_t), c->stream));
+    return ALDIC_OK;
+  }
+  if (!conv || !zncc || !list) return fail(c, ALDIC_ERR_ARG, "conv, zncc and list are required");
   if (!c->sel_count) CK(cudaMalloc(&c->sel_count, sizeof(int)));
   Arg acv{conv, (size_t)n * 4, false, nullptr}, az{zncc, (size_t)n * 8, false, nullptr};
   Arg al{list, (size_t)n * 4, true, nullptr};
@@ -832,6 +836,12 @@ int aldic_fallback_select(aldic_ctx* c, int64_t n, const int32_t* conv, const do
   if (rc) return rc;
   c->launches += launch_fallback_select((const int32_t*)acv.dev, (const double*)az.dev, n, zncc_min,
                                         (int32_t*)al.dev, c->sel_count, c->stream);
+  if (dev_count) {
+    // the count stays on the device (little-endian: the int32 count is the int64's low word)
+    CK(cudaMemsetAsync(count, 0, sizeof(int64_t), c->stream));
+    CK(cudaMemcpyAsync(count, c->sel_count, sizeof(int), cudaMemcpyDeviceToDevice, c->stream));
+    return finish(c, 0);  // waits only to copy a host list back
+  }
   int h = 0;
   CK(cudaMemcpyAsync(&h, c->sel_count, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   rc = finish(c, 0);  // copies a host list back and waits

@@ -434,8 +434,8 @@ __global__ void __launch_bounds__(kCorrThreads) corr_im2col_kernel(CorrSrc src, 
   if (warp == 0) tmem_free(tmem, 128);
 }
 
-// conv1 and conv2 over one whole frame image in a single pass (prediction): CTA (bx, i2)
-// computes conv2's outputs (i2, 128 bx .. 128 bx + 127) of the (M2 x N2 x 32) map.  It loads
+// conv1 and conv2 over whole frame images in a single pass (prediction): CTA (bx, i2, z)
+// computes conv2's outputs (i2, 128 bx .. 128 bx + 127) of image z's (M2 x N2 x 32) map.  It loads
 // the 7 x 515 image pixels they depend on (BF16-rounded, zero outside the image) into shared
 // memory; for each output pixel the threads compute the 9 conv1 positions conv2's taps read
 // (32 channels each, FP32 sums in tap order, + bias, ReLU, BF16: the arithmetic of
@@ -449,12 +449,17 @@ constexpr int kFeatThreads = 128, kFeatCols = 4 * 128 + 3, kFeatKb = 5;
 constexpr int kFeatA = 2 * 128 * 128, kFeatB = kFeatKb * 32 * 128;  // A: two K-block buffers
 constexpr int kFeatSmem = 1024 + kFeatA + kFeatB + 7 * kFeatCols * 2;
 
-__global__ void __launch_bounds__(kFeatThreads) image_features_kernel(const float* __restrict__ img, int M, int N,
+__global__ void __launch_bounds__(kFeatThreads) image_features_kernel(const float* __restrict__ img0,
+                                                                      const float* __restrict__ img1, int M, int N,
                                                                       const bf16* __restrict__ W1,
                                                                       const float* __restrict__ b1,
                                                                       const bf16* __restrict__ W2,
                                                                       const float* __restrict__ b2,
-                                                                      bf16* __restrict__ out, int* __restrict__ err) {
+                                                                      bf16* __restrict__ out0,
+                                                                      bf16* __restrict__ out1, int* __restrict__ err) {
+  // grid.z selects the image: both images' CTAs in one launch (one tail, not two)
+  const float* __restrict__ img = blockIdx.z ? img1 : img0;
+  bf16* __restrict__ out = blockIdx.z ? out1 : out0;
   extern __shared__ unsigned char feat_raw[];
   __shared__ float w1[32][9], bs1[32], bs2[32];
   __shared__ __align__(8) uint64_t kbar[2];  // MMAs of the K-blocks in A buffer 0 / 1 done
@@ -1264,7 +1269,7 @@ int aldic_net_status(aldic_net* net) {
 namespace aldic {
 // conv1 and conv2 over the whole reference and deformed images of frame fr into net->FR and
 // net->FD: (M + 3) / 4 x (N + 3) / 4 x 32 maps whose pixel (i, j) is centred on image pixel
-// (4 i + 1, 4 j + 1) (1-based); one image_features_kernel launch per image
+// (4 i + 1, 4 j + 1) (1-based); one image_features_kernel launch for both images
 int image_features(ProposalNet* net, const FrameDev& fr) {
   const int M = fr.M, N = fr.N, M2 = (M + 3) / 4, N2 = (N + 3) / 4;
   const size_t P2 = (size_t)M2 * N2;
@@ -1282,13 +1287,11 @@ int image_features(ProposalNet* net, const FrameDev& fr) {
     net->fN = N;
   }
   NK(cudaFuncSetAttribute(image_features_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kFeatSmem));
-  const dim3 grid((unsigned)((N2 + 127) / 128), (unsigned)M2);
-  for (int side = 0; side < 2; ++side) {
-    image_features_kernel<<<grid, kFeatThreads, kFeatSmem, net->stream>>>(
-        side ? fr.def : fr.ref, M, N, net->wb + kL.w[0], net->w + kL.b[0], net->wb + kL.w[1], net->w + kL.b[1],
-        side ? net->FD : net->FR, net->errflag);
-    ++net->launches;
-  }
+  const dim3 grid((unsigned)((N2 + 127) / 128), (unsigned)M2, 2u);  // z: reference, deformed
+  image_features_kernel<<<grid, kFeatThreads, kFeatSmem, net->stream>>>(
+      fr.ref, fr.def, M, N, net->wb + kL.w[0], net->w + kL.b[0], net->wb + kL.w[1], net->w + kL.b[1], net->FR,
+      net->FD, net->errflag);
+  ++net->launches;
   NK(cudaGetLastError());
   return ALDIC_OK;
 }

@@ -316,7 +316,9 @@ int aldic_local_icgn_guess(aldic_ctx* ctx, int variant, int64_t n, const double*
 /* The fallback of a learned initial guess: the subsets whose IC-GN from it did not converge
  * (conv outside 1..100) or whose final ZNCC is below zncc_min (or NaN).  Their indices (0-based,
  * in no fixed order) go to list (n entries of room, host or device) and their number to
- * *count (host); the call waits for the device.  No counterpart in the reference. */
+ * *count: with a host count the call waits for the device; with a device count (and a
+ * device list) it is queued on the context's stream and returns at once, so a caller can
+ * queue the next frame before it reads the count.  No counterpart in the reference. */
 int aldic_fallback_select(aldic_ctx* ctx, int64_t n, const int32_t* conv, const double* zncc, double zncc_min,
                           int32_t* list, int64_t* count);
 /* Zero-normalised cross-correlation of each subset's (winsize+1)^2 window of REF with DEF under

@@ -175,6 +175,13 @@ def test_fallback_selection(env):
     outd = torch.empty(n, dtype=torch.int32, device=dev)
     k2 = ctx.fallback_select(torch.from_numpy(conv).to(dev), torch.from_numpy(zncc).to(dev), 0.9, outd)
     assert k2 == k and np.array_equal(np.sort(outd[:k2].cpu().numpy()), want)
+    # the count on the device: queued without a wait
+    cnt = torch.full((1,), -7, dtype=torch.int64, device=dev)
+    outd.fill_(-1)
+    assert ctx.fallback_select(torch.from_numpy(conv).to(dev), torch.from_numpy(zncc).to(dev), 0.9, outd,
+                               count=cnt) is None
+    ctx.synchronize()
+    assert int(cnt.item()) == k and np.array_equal(np.sort(outd[:k].cpu().numpy()), want)
 
 
 def _patches_numpy(f, g, crd):
@@ -322,3 +329,68 @@ def test_trained_network_gains_over_the_search_guess():
     finally:
         net.close()
         ctx.close()
+
+
+def test_pipelined_frames_equal_one_at_a_time():
+    """Frames pushed through LearnedPipeline (two contexts; the host's wait for a frame's
+    fallback count sits behind the next frame's launches) get, frame by frame, the results
+    of LearnedInit.run on that frame alone, fallbacks included (forced by a ZNCC threshold
+    at the 10th percentile of the converged subsets)."""
+    import os
+
+    import torch
+
+    import aldic_b200 as A
+    from aldic_b200 import learned as L
+    from aldic_b200 import synth_gpu, train_net
+
+    if not os.path.exists(train_net.DEFAULT_WEIGHTS):
+        pytest.skip("no trained weights shipped")
+    ctxs = [A.Context(0) for _ in range(3)]
+    net = L.ProposalNet(0, max_batch=4096)
+    try:
+        net.set_params(np.load(train_net.DEFAULT_WEIGHTS))
+        M = N = 512
+        gx, gy, w, st, s = [21, M - 20], [21, N - 20], 32, 16, 16
+        pairs = [synth_gpu.field_pair(seed, M=M, N=N) for seed in (31, 32, 33)]
+
+        def load(ctx, p):
+            ctx.load_image_raw(0, p.ref, gx, gy, want_stats=False, shape=(M, N))
+            ctx.load_image_raw(1, p.deff, gx, gy, want_stats=False, shape=(M, N))
+            ctx.compute_gradients()
+
+        one = L.LearnedInit(net, ctxs[2], s, gx, gy, w, st, 1e-3)
+
+        def run_one(p):
+            with torch.cuda.stream(one.stream):
+                load(ctxs[2], p)
+            nf = one.run()
+            one.stream.synchronize()
+            return nf, {k: v.cpu().numpy() for k, v in one.buf.items()}
+
+        _, b0 = run_one(pairs[0])
+        ok = (b0["conv"] > 0) & (b0["conv"] < 100)
+        zmin = float(np.quantile(b0["zncc"][ok], 0.1))
+        one.zncc_min = zmin
+        want = [run_one(p) for p in pairs]
+        assert all(nf > 0 for nf, _ in want)
+        pipe = L.LearnedPipeline(net, ctxs[:2], s, gx, gy, w, st, 1e-3, zncc_min=zmin)
+        got = []
+
+        def keep(done):
+            if done is not None:
+                pipe.stream.synchronize()
+                got.append((done.n_fallback, {k: v.cpu().numpy() for k, v in done.buf.items()}))
+
+        for p in pairs:
+            keep(pipe.push(lambda ctx, p=p: load(ctx, p)))
+        keep(pipe.flush())
+        assert len(got) == len(pairs)
+        for (nf_w, bw), (nf_g, bg) in zip(want, got):
+            assert nf_w == nf_g
+            for k in ("U0", "F0", "U", "F", "conv", "fallback"):
+                assert np.array_equal(bw[k], bg[k], equal_nan=True), k
+    finally:
+        net.close()
+        for c in ctxs:
+            c.close()
