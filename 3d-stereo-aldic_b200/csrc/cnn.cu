@@ -282,9 +282,8 @@ __device__ __forceinline__ bool corr_crops(const CorrSrc& s, long long t, const 
 // im2col rows; a persistent CTA takes samples blockIdx.x, + gridDim.x, ... and loads the next
 // sample's crops into registers while it works on the current one.  Per sample: the 8 x 8
 // reference feature crop (64 rows of 32 BF16 channels, written twice: A rows p and 64 + p) and
-// the 16 x 16 deformed crop (256 rows) are staged in shared memory in the 128-byte-swizzled
-// K-major layout (only the first 64 bytes of each 128-byte row, the 32 channels the two K = 16
-// steps read, are written).  In two passes (deformed rows 0..7, then 8..15) one thread issues
+// the 16 x 16 deformed crop (256 rows) are staged in shared memory in the 64-byte-swizzled
+// K-major layout (a row: the 32 channels, the two K = 16 steps).  In two passes (deformed rows 0..7, then 8..15) one thread issues
 // two tcgen05.mma (M 128, N 128) into 128 TMEM columns: D[p, q] = fR[p] . fD[q] for the
 // reference / deformed position pairs of the pass.  Each warp w reads TMEM lanes 32 w ..
 // (reference positions p = 8 ii + j, rows 64.. repeating 0..63) and takes, with warp w + 2 or
@@ -294,16 +293,17 @@ __device__ __forceinline__ bool corr_crops(const CorrSrc& s, long long t, const 
 // straight to the (at most 4) places conv3's im2col rows use it, in a shared-memory copy of
 // the sample's 16 rows x 736 columns (zeroed once: the other places are the same for every
 // sample).  All 128 threads then copy those rows out with 16-byte stores.  128 TMEM columns
-// and 73 KB of shared memory let 3 CTAs share an SM.  ok[t] = 0 (whole-image crops leaving the maps) gives a zero volume.  The MMA waits are
+// and 48 KB of shared memory let 4 CTAs share an SM.  ok[t] = 0 (whole-image crops leaving the maps) gives a zero volume.  The MMA waits are
 // bounded (err bit 2 on time-out, the volumes then undefined).
 constexpr int kCorrThreads = 128;
-constexpr int kCorrA = 128 * 128, kCorrB = 256 * 128;  // operand tiles (bytes)
+constexpr int kCorrA = 128 * 64, kCorrB = 256 * 64;  // operand tiles (bytes): 64-byte rows
 constexpr int kCorrRows = 16 * 736 * 2;                // conv3's im2col rows of a sample
 constexpr int kCorrSmem = 1024 + kCorrA + kCorrB + kCorrRows;  // + alignment slack
 constexpr long long kCorrWaitCycles = 2000000000LL;
 
-__device__ __forceinline__ void put_chunk(unsigned char* tile, int row, int chunk, uint4 v) {
-  *reinterpret_cast<uint4*>(tile + row * 128 + ((chunk ^ (row & 7)) << 4)) = v;
+// chunk (16 bytes, 0..3) of a 64-byte-swizzled row (sw64_desc)
+__device__ __forceinline__ void put_chunk64(unsigned char* tile, int row, int chunk, uint4 v) {
+  *reinterpret_cast<uint4*>(tile + row * 64 + ((chunk ^ ((row >> 1) & 3)) << 4)) = v;
 }
 
 // this thread's 10 chunks of sample t's crops (A: chunks 0..255, B: 256..1279), zero outside
@@ -371,10 +371,10 @@ __global__ void __launch_bounds__(kCorrThreads) corr_im2col_kernel(CorrSrc src, 
     for (int i = 0; i < 10; ++i) {
       const int q = tid + i * kCorrThreads;
       if (i < 2) {  // A rows p and p + 64 (a copy: TMEM lanes 64..127 for warps 2 and 3)
-        put_chunk(tA, q / 4, q % 4, v[i]);
-        put_chunk(tA, 64 + q / 4, q % 4, v[i]);
+        put_chunk64(tA, q / 4, q % 4, v[i]);
+        put_chunk64(tA, 64 + q / 4, q % 4, v[i]);
       } else {
-        put_chunk(tB, (q - 256) / 4, q % 4, v[i]);
+        put_chunk64(tB, (q - 256) / 4, q % 4, v[i]);
       }
     }
     if (ok && tid == 0) ok[t] = inside ? 1 : 0;
@@ -388,9 +388,9 @@ __global__ void __launch_bounds__(kCorrThreads) corr_im2col_kernel(CorrSrc src, 
     for (int pass = 0; pass < 2; ++pass) {
       if (tid == 0) {
         constexpr uint32_t idesc = bf16_idesc(128, 128);
-        const uint32_t a = smem_u32(tA), b = smem_u32(tB + pass * 128 * 128);
-        umma_bf16(tmem, sw128_desc(a), sw128_desc(b), idesc, false);
-        umma_bf16(tmem, sw128_desc(a + 32), sw128_desc(b + 32), idesc, true);
+        const uint32_t a = smem_u32(tA), b = smem_u32(tB + pass * 128 * 64);
+        umma_bf16(tmem, sw64_desc(a), sw64_desc(b), idesc, false);
+        umma_bf16(tmem, sw64_desc(a + 32), sw64_desc(b + 32), idesc, true);
         umma_commit(&done);
       }
       __syncwarp();

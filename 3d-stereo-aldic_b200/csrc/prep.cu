@@ -47,16 +47,19 @@ __global__ void roi_moment_kernel(const T* __restrict__ img, int M, int gx0, int
   }
   __syncthreads();
   if (last) {
-    // fixed-order sum of the partials by one warp
-    if (threadIdx.x < 32) {
-      double t = 0;
-      for (int i = threadIdx.x; i < (int)gridDim.x; i += 32) t += ((volatile double*)partials)[i];
-      t = warp_sum(t);
-      if (threadIdx.x == 0) {
-        stats[POWER - 1] = t;
-        stats[POWER + 1] = (POWER == 1) ? t / (double)count : sqrt(t / (double)(count - 1));
-        *counter = 0;  // re-arm for the next use
-      }
+    // fixed-order sum of the partials by the whole block (a few L2 reads per thread, then
+    // the warp and block sums in a fixed tree)
+    double t = 0;
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) t += __ldcg(partials + i);
+    t = warp_sum(t);
+    if (lane == 0) red[warp] = t;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double u = 0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) u += red[w];
+      stats[POWER - 1] = u;
+      stats[POWER + 1] = (POWER == 1) ? u / (double)count : sqrt(u / (double)(count - 1));
+      *counter = 0;  // re-arm for the next use
     }
   }
 }
@@ -109,15 +112,27 @@ __global__ void roi_moment_int_kernel(const T* __restrict__ img, int M, int gx0,
     last = (done == gridDim.x - 1);
   }
   __syncthreads();
-  if (last && threadIdx.x < 32) {
+  if (last) {
+    // the whole block sums the partials (L2 reads; integer sums, so any order is exact)
     unsigned long long t1 = 0, t2 = 0;
-    for (int i = threadIdx.x; i < (int)gridDim.x; i += 32) {
-      t1 += ((volatile unsigned long long*)partials)[2 * i];
-      t2 += ((volatile unsigned long long*)partials)[2 * i + 1];
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) {
+      t1 += __ldcg(partials + 2 * i);
+      t2 += __ldcg(partials + 2 * i + 1);
     }
     t1 = warp_sum_u64(t1);
     t2 = warp_sum_u64(t2);
+    if (lane == 0) {
+      red[0][warp] = t1;
+      red[1][warp] = t2;
+    }
+    __syncthreads();
     if (threadIdx.x == 0) {
+      t1 = 0;
+      t2 = 0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+        t1 += red[0][w];
+        t2 += red[1][w];
+      }
       const double n = (double)count;
       const unsigned __int128 d =
           (unsigned __int128)(unsigned long long)count * t2 - (unsigned __int128)t1 * t1;  // >= 0
@@ -186,29 +201,38 @@ __global__ void mask_binarize_kernel(const double* __restrict__ in, long long n,
 
 // funImgGradient (func/funImgGradient.m:52-78): correlation with
 // h = [-1 9 -45 0 45 -9 1]/60 along dim 1 (gx) and dim 2 (gy) at pixel (i+3, j+3),
-// times the mask there.  One thread per output pixel; a block step covers 256 consecutive
-// rows of one output column (coalesced; the column and row come from one 32-bit division
-// per step, not per pixel).
-__global__ void gradient_kernel(const float* __restrict__ img, const uint8_t* __restrict__ mask, int M, int N,
-                                float* __restrict__ gx, float* __restrict__ gy) {
+// times the mask there.  A block computes a 64-row x 32-column output tile from a 70 x 38
+// input tile staged in shared memory (each input pixel read from memory about 1.3 times
+// instead of once per tap column); thread (r, g) computes rows r, columns 8 g .. 8 g + 7,
+// consecutive threads consecutive rows (coalesced stores, conflict-free shared reads).
+constexpr int kGradTR = 64, kGradTC = 32, kGradPR = kGradTR + 6, kGradPC = kGradTC + 6;
+__global__ void __launch_bounds__(256) gradient_kernel(const float* __restrict__ img, const uint8_t* __restrict__ mask,
+                                                       int M, int N, float* __restrict__ gx, float* __restrict__ gy) {
+  __shared__ float t[kGradPC][kGradPR];
   const int gM = M - 6, gN = N - 6;
-  const int rb = (gM + 255) / 256;  // row steps per column
-  const int steps = rb * gN;
-  for (int st = blockIdx.x; st < steps; st += gridDim.x) {
-    const int jj = st / rb, i0 = (st - jj * rb) * 256;
-    const int ii = i0 + (int)threadIdx.x;
-    if (ii >= gM) continue;
-    const int i = ii + 3, j = jj + 3;
-    const float* c = img + (size_t)i + (size_t)j * M;
-    const float dx = ((__ldg(c + 3) - __ldg(c - 3)) - 9.0f * (__ldg(c + 2) - __ldg(c - 2)) +
-                      45.0f * (__ldg(c + 1) - __ldg(c - 1))) * (1.0f / 60.0f);
-    const float dy = ((__ldg(c + 3 * (size_t)M) - __ldg(c - 3 * (size_t)M)) -
-                      9.0f * (__ldg(c + 2 * (size_t)M) - __ldg(c - 2 * (size_t)M)) +
-                      45.0f * (__ldg(c + (size_t)M) - __ldg(c - (size_t)M))) * (1.0f / 60.0f);
-    const float mk = mask ? (float)mask[(size_t)i + (size_t)j * M] : 1.0f;
-    const size_t k = (size_t)ii + (size_t)jj * gM;
-    gx[k] = dx * mk;
-    gy[k] = dy * mk;
+  const int i0 = blockIdx.x * kGradTR, j0 = blockIdx.y * kGradTC;  // output tile origin
+  // input rows i0 .. i0 + 69, columns j0 .. j0 + 37 (output (ii, jj) centres on (ii + 3, jj + 3))
+  for (int q = threadIdx.x; q < kGradPR * kGradPC; q += blockDim.x) {
+    const int r = q % kGradPR, c = q / kGradPR, i = i0 + r, j = j0 + c;
+    t[c][r] = (i < M && j < N) ? __ldg(img + (size_t)i + (size_t)j * M) : 0.f;
+  }
+  __syncthreads();
+  const int r = threadIdx.x % kGradTR, g = threadIdx.x / kGradTR;
+  const int ii = i0 + r;
+  if (ii >= gM) return;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const int c = g * 8 + k, jj = j0 + c;
+    if (jj >= gN) break;
+    const int R = r + 3, Cc = c + 3;
+    const float dx = ((t[Cc][R + 3] - t[Cc][R - 3]) - 9.0f * (t[Cc][R + 2] - t[Cc][R - 2]) +
+                      45.0f * (t[Cc][R + 1] - t[Cc][R - 1])) * (1.0f / 60.0f);
+    const float dy = ((t[Cc + 3][R] - t[Cc - 3][R]) - 9.0f * (t[Cc + 2][R] - t[Cc - 2][R]) +
+                      45.0f * (t[Cc + 1][R] - t[Cc - 1][R])) * (1.0f / 60.0f);
+    const float mk = mask ? (float)mask[(size_t)(ii + 3) + (size_t)(jj + 3) * M] : 1.0f;
+    const size_t o = (size_t)ii + (size_t)jj * gM;
+    gx[o] = dx * mk;
+    gy[o] = dy * mk;
   }
 }
 
@@ -298,8 +322,8 @@ int launch_mask_binarize(const double* in, long long n, uint8_t* out, cudaStream
 }
 
 int launch_gradient(const float* img, const uint8_t* mask, int M, int N, float* gx, float* gy, cudaStream_t st) {
-  const long long steps = (long long)((M - 6 + 255) / 256) * (N - 6);
-  gradient_kernel<<<grid_for(steps, 1, 148 * 16), 256, 0, st>>>(img, mask, M, N, gx, gy);
+  const dim3 grid((unsigned)((M - 6 + kGradTR - 1) / kGradTR), (unsigned)((N - 6 + kGradTC - 1) / kGradTC));
+  gradient_kernel<<<grid, 256, 0, st>>>(img, mask, M, N, gx, gy);
   return 1;
 }
 

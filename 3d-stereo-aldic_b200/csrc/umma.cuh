@@ -40,6 +40,19 @@ __device__ __forceinline__ uint64_t sw128_desc(uint32_t smem_addr) {
   return d;
 }
 
+// The same for a K-major tile of 32 BF16 per row in the 64-byte swizzle layout: rows of 64
+// bytes, 8-row core groups 512 bytes apart, chunk c (16 bytes) of row r stored at
+// r * 64 + ((c ^ ((r >> 1) & 3)) << 4), the tile 512-byte aligned; layout 4 = 64-byte swizzle.
+__device__ __forceinline__ uint64_t sw64_desc(uint32_t smem_addr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((smem_addr >> 4) & 0x3FFFu);
+  d |= (uint64_t)1u << 16;
+  d |= (uint64_t)((512u >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1u << 46;
+  d |= (uint64_t)4u << 61;
+  return d;
+}
+
 // Instruction descriptor of kind::f16 with BF16 A and B, FP32 D, both K-major, M x N:
 // [4,6) D format (1 = F32), [7,10) A format (1 = BF16), [10,13) B format (1 = BF16),
 // [15] A major (0 = K), [16] B major (0 = K), [17,23) N >> 3, [24,29) M >> 4.
