@@ -75,6 +75,8 @@ __device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v)
 // exact 128-bit integers, which the reference's two FP64 passes (the mean, then the squared
 // deviations from it; funNormalizeImg.m) approximate to within their rounding.  partials
 // holds 2 entries per block.
+constexpr int kMomentCols = 8;  // ROI columns per block step of roi_moment_int_kernel
+
 template <typename T>
 __global__ void roi_moment_int_kernel(const T* __restrict__ img, int M, int gx0, int gx1, int gy0, int gy1,
                                       unsigned long long* __restrict__ partials, unsigned int* __restrict__ counter,
@@ -82,13 +84,22 @@ __global__ void roi_moment_int_kernel(const T* __restrict__ img, int M, int gx0,
   __shared__ unsigned long long red[2][32];
   __shared__ bool last;
   const int rows = gx1 - gx0, cols = gy1 - gy0;
+  // a block step covers kMomentCols ROI columns: each thread's loads of those columns are
+  // independent, so they are all in flight at once (a loop of one load per step would wait
+  // out each load's latency before issuing the next)
   unsigned long long s1 = 0, s2 = 0;
-  for (int b = blockIdx.x; b < cols; b += gridDim.x) {
-    const T* col = img + (size_t)(gy0 + b) * M + gx0;
+  for (int b0 = blockIdx.x * kMomentCols; b0 < cols; b0 += gridDim.x * kMomentCols) {
+    const T* col = img + (size_t)(gy0 + b0) * M + gx0;
+    const int nc = min(kMomentCols, cols - b0);
     for (int r = threadIdx.x; r < rows; r += blockDim.x) {
-      const unsigned long long v = col[r];
-      s1 += v;
-      s2 += v * v;
+      unsigned int v[kMomentCols];
+#pragma unroll
+      for (int k = 0; k < kMomentCols; ++k) v[k] = k < nc ? (unsigned int)col[(size_t)k * M + r] : 0u;
+#pragma unroll
+      for (int k = 0; k < kMomentCols; ++k) {
+        s1 += v[k];
+        s2 += (unsigned long long)v[k] * v[k];
+      }
     }
   }
   s1 = warp_sum_u64(s1);
@@ -275,7 +286,8 @@ int launch_normalize(const void* img, int dtype, int M, int N, int gx0, int gx1,
   const int th = 256;
   const int cols = gy1 - gy0;
   const int g = cols < npartials ? cols : npartials;            // FP partials: 1 per block
-  const int gi = cols < npartials / 2 ? cols : npartials / 2;   // integer partials: 2 per block
+  const int csteps = (cols + kMomentCols - 1) / kMomentCols;   // integer kernel: column groups
+  const int gi = csteps < npartials / 2 ? csteps : npartials / 2;  // integer partials: 2 per block
   const long long npx = (long long)M * N;
   const int gm = grid_for(npx, th, 4 * 148 * 4);
   unsigned long long* ip = reinterpret_cast<unsigned long long*>(partials);
