@@ -539,12 +539,13 @@ LEARNED_METRIC = "converged IC-GN subsets/s at <=0.01 px vs FP64 oracle; learned
 class LearnedBench:
     """The two initial-guess paths on one device, each a pass over one frame pair (uint8
     2048 x 2048, resident): load + normalise + gradients, then
-      learned: network prediction -> IC-GN from [F0 U0] -> ZNCC check -> integer search + IC-GN
-               on the failed subsets (the fallback);
+      learned: network prediction -> IC-GN from [F0 U0] (its last iteration gives the ZNCC
+               check) -> integer search + IC-GN on the failed subsets (the fallback);
       fft:     whole-field integer search -> outlier removal -> Init (inpaint) -> IC-GN from
                [0 U0] (LocalICGN's reference path).
     Both on the same integer-search grid (ROI [roi+1, size-roi], winsize w, step), all work on
-    one stream."""
+    one stream.  The learned path's timed frames go through a LearnedPipeline over two
+    contexts (frame k queued before the host reads frame k-1's fallback count)."""
 
     def __init__(self, A, torch, P, device, autotune=True):
         from aldic_b200 import learned as L
