@@ -124,3 +124,37 @@ def test_organize_matched_pairs():
     assert np.array_equal(P[0], np.concatenate([C, Cr], 1))
     assert np.array_equal(P[1][:, :2], C + [1.0, 2.0]) and np.array_equal(P[1][:, 2:], Cr + [0.5, -1.0])
     assert np.array_equal(P[2][:, :2], C + [1.5, 2.5]) and np.array_equal(P[2][:, 2:], Cr)
+
+
+def test_learned_pipeline_order(monkeypatch):
+    """LearnedPipeline (two contexts, one stream): each push loads and submits a frame on the
+    other context before completing the previous frame (the host's wait for its fallback
+    count), returns that previous frame, and flush completes the last one."""
+    from aldic_b200 import learned as L
+
+    log = []
+
+    class FakeInit:
+        def __init__(self, net, ctx, *args, stream=None, **kw):
+            self.ctx, self.stream, self.n_fallback = ctx, stream, 0
+
+        def submit(self):
+            log.append(("submit", self.ctx))
+
+        def complete(self):
+            log.append(("complete", self.ctx))
+            return 0
+
+    monkeypatch.setattr(L, "LearnedInit", FakeInit)
+    with pytest.raises(ValueError):
+        L.LearnedPipeline("net", ["A"], 16, [1, 99], [1, 99], 32, 16, 1e-3)
+    pipe = L.LearnedPipeline("net", ["A", "B"], 16, [1, 99], [1, 99], 32, 16, 1e-3)
+    assert pipe.lis[1].stream is pipe.lis[0].stream
+    done = [pipe.push(lambda ctx, k=k: log.append(("load", ctx, k))) for k in range(3)]
+    last = pipe.flush()
+    assert log == [("load", "A", 0), ("submit", "A"),
+                   ("load", "B", 1), ("submit", "B"), ("complete", "A"),
+                   ("load", "A", 2), ("submit", "A"), ("complete", "B"),
+                   ("complete", "A")]
+    assert done[0] is None and done[1].ctx == "A" and done[2].ctx == "B" and last.ctx == "A"
+    assert pipe.flush() is None
