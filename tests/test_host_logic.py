@@ -158,3 +158,29 @@ def test_learned_pipeline_order(monkeypatch):
                    ("complete", "A")]
     assert done[0] is None and done[1].ctx == "A" and done[2].ctx == "B" and last.ctx == "A"
     assert pipe.flush() is None
+
+
+def test_exact_integer_roi_statistics():
+    """The arithmetic of roi_moment_int_kernel (prep.cu) on integer frames: exact sums
+    S1 = sum x, S2 = sum x^2, the squared deviations (n S2 - S1^2) / n from the exact integer
+    numerator split into 64-bit halves before the FP64 conversion, as the kernel does.  It
+    equals numpy's two-pass FP64 mean and N-1 standard deviation to rounding, also where
+    n S2 needs more than 64 bits (a u16 frame)."""
+    import math
+
+    rng = np.random.default_rng(0)
+    for dtype, hi, shape in ((np.uint8, 256, (513, 257)), (np.uint16, 65536, (2048, 1024))):
+        x = rng.integers(0, hi, size=shape).astype(dtype)
+        n = x.size
+        s1 = int(x.astype(np.int64).sum())
+        s2 = int((x.astype(np.uint64) * x.astype(np.uint64)).sum(dtype=np.uint64))
+        d = n * s2 - s1 * s1
+        assert d >= 0
+        if dtype == np.uint16:
+            assert n * s2 >= 2 ** 64  # the high word is in use
+        nd = float(d >> 64) * 18446744073709551616.0 + float(d & (2 ** 64 - 1))
+        ssd = nd / n
+        mean, sd = s1 / n, math.sqrt(ssd / (n - 1))
+        xf = x.astype(np.float64)
+        assert abs(mean - xf.mean()) <= 4e-16 * abs(xf.mean())
+        assert abs(sd - xf.std(ddof=1)) <= 1e-14 * xf.std(ddof=1)
